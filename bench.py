@@ -1,0 +1,400 @@
+"""Benchmark of the B200 batch step on the mixed-precision IMS workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one GPU): 1,048,576 ions of 200 Da, +1, HSS cross-section 150 A^2,
+in N2 at 300 K and 1000 Pa, uniform E at 20 Td, Boris push, dt = 5e-10 s,
+collisions by the null-collision HSS scheme with Philox; velocities, field
+and collision arithmetic in FP32, positions and time in FP64.  One bench
+step = 1,000 engine steps of all ions (the engine's snapshot interval), so
+the default 100 timed steps are the workload's full 100,000-step run.
+Inputs are synthetic (the reference's own ion loader semantics, seed 123).
+
+Metric: ion-steps/s (whole job).  Timed on the device with CUDA events on
+the launching stream, L2 flushed (256 MB write) between timed steps, barrier
++ synchronize around the timed loop, max over ranks.  Under torchrun each
+rank advances its own 1,048,576 ions (weak scaling; ion ids offset by rank)
+and the per-snapshot ensemble moments are all-reduced over NCCL.
+
+--impl reference runs the reference's own CPU code (oracle/_ref/ref_harness,
+compiled from the reference sources) on all host cores for the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+N_IONS = 1_048_576
+STEPS_PER_BENCH_STEP = 1000
+DT = 5e-10
+EN_TD = 20.0
+METRIC = "ion-steps/s on 1 B200: mixed-prec vs plain FP64 at <=0.3% K0 error"
+WORKLOAD = "IMS drift, 1,048,576 ions (200 Da, +1, 150 A^2 HSS) in N2 300 K 1000 Pa, 20 Td, Boris + HSS, dt 5e-10 s"
+# bytes each ion moves per launch of the fused kernel:
+# read x,y,z(24) v(12) S,U(8) mass,charge(16) flags(1) t_arr(8); write x,y,z(24) v(12) S,U(8) flags(1)
+BYTES_PER_ION_LAUNCH = {"mixed": 114, "hilo": 114, "fp64": 69 + 12 + 8 + 45 + 12 + 8}
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        if shutil.which("nvidia-smi") is None:
+            return
+        self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                      "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                     stderr=subprocess.DEVNULL, text=True)
+        self.thr = threading.Thread(target=self._read, daemon=True)
+        self.thr.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# reference CPU code (oracle/_ref/ref_harness)
+# ---------------------------------------------------------------------------
+REF_DOMAIN = dict(instrument="IMS", origin_z=-0.01, length=0.1, radius=0.05, T=300, P=1000, gas="N2", EN_Td=EN_TD)
+
+
+def _harness():
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc  # noqa: E402  (CPU-baseline leg only)
+    return orc
+
+
+def reference_sample(n_ions: int, n_steps: int, threads: int, state_path: Path | None = None) -> dict:
+    """Run the reference's Boris + HSS code (best CPU form: one OpenMP loop per
+    step) on n_ions for n_steps; returns the harness's own loop timing."""
+    orc = _harness()
+    with tempfile.TemporaryDirectory() as td:
+        sp = Path(td) / "s.bin"
+        orc.harness("init", seed=123, n=n_ions, sigma_pos=5e-4, T=300, mass=repr(200.0 * 1.66053906660e-27), out=sp)
+        out = orc.harness("run", **{"in": sp, "out": Path(td) / "o.bin"}, **REF_DOMAIN, integrator="boris",
+                          collision="hss", dt=DT, steps=n_steps, threads=threads, seed=123)
+    return json.loads(out.strip().splitlines()[-1])
+
+
+def cpu_baseline(budget_s: float = 15.0) -> dict:
+    """Bounded sample of the same workload on the host cores (rank 0, N=1)."""
+    orc = _harness()
+    threads = cpu_threads()
+    n = 65536
+    if not orc.have_harness():
+        return {"value": None, "unit": "ion-steps/s", "cores": threads, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/ref_harness was not built"}
+    probe = reference_sample(n, 20, threads)
+    rate = max(probe["ion_steps_per_s"], 1.0)
+    steps = int(min(max(budget_s * rate / n, 20), 100000))
+    r = reference_sample(n, steps, threads)
+    return {"value": r["ion_steps_per_s"], "unit": "ion-steps/s", "cores": threads, "kind": "reference",
+            "sample": f"{n} ions x {steps} steps of the same physics (reference BorisStrategy + HSSCollisionHandler, "
+                      f"OpenMP over ions, {threads} threads, {r['wall_s']:.1f} s)"}
+
+
+def run_reference_arm(args) -> None:
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return
+    orc = _harness()
+    threads = cpu_threads()
+    line = {"impl": "reference", "metric": METRIC, "unit": "ion-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic"}
+    if not orc.have_harness():
+        line["unavailable"] = "reference CPU code was not compiled (oracle/_ref/ref_harness missing)"
+        print(json.dumps(line))
+        return
+    n = 65536
+    probe = reference_sample(n, 10, threads)
+    rate = max(probe["ion_steps_per_s"], 1.0)
+    per_step_s = min(1.0, 150.0 / max(args.steps + args.warmup, 1))
+    sub = int(max(5, per_step_s * rate / n))
+    for _ in range(args.warmup):
+        reference_sample(n, sub, threads)
+    wall, ion_steps = 0.0, 0
+    for _ in range(args.steps):
+        r = reference_sample(n, sub, threads)
+        wall += r["wall_s"]
+        ion_steps += r["ion_steps"]
+    value = ion_steps / wall
+    line.update({"value": value, "ms_per_step": 1e3 * wall / args.steps,
+                 "config": {"workload": WORKLOAD, "ions": n, "engine_steps_per_bench_step": sub,
+                            "sample": f"{n} of {N_IONS} ions per step (bounded CPU sample)"},
+                 "cpu_baseline": {"value": value, "unit": "ion-steps/s", "cores": threads, "kind": "reference",
+                                  "sample": f"{n} ions x {sub} engine steps per bench step"},
+                 "e2e": {"value": value, "unit": "ion-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    sys.path.insert(0, str(ROOT))
+    from icarion_b200 import _capi as capi
+    from icarion_b200 import config as cfg
+    from icarion_b200 import parallel
+    from icarion_b200.sim import IonState, Simulation, generate_ions
+
+    rank, world, local = _env_rank()
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    prec_id = {"mixed": capi.PREC_MIXED, "fp64": capi.PREC_FP64, "hilo": capi.PREC_MIXED_HILO}[args.precision]
+
+    domain = {"instrument": "IMS", "geometry": {"origin_m": [0.0, 0.0, -0.01], "length_m": 0.1, "radius_m": 0.05},
+              "env": {"temperature_K": 300.0, "pressure_Pa": 1000.0, "gas_species": "N2"},
+              "fields": {"DC": {"EN_Td": EN_TD}}}
+    ens = cfg.ensemble_params(domain, 150e-20, DT, detector_z_m=2.0e-3)
+    spec = cfg.species_spec(N_IONS, 200.0 * cfg.AMU_TO_KG, cfg.ELEM_CHARGE_C,
+                            {"type": "gaussian", "center": [0, 0, 0], "std": [5e-4] * 3},
+                            {"type": "thermal", "temperature_K": 300.0})
+    st0 = generate_ions(123, [spec])
+    first_id = rank * N_IONS
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def make_sim(prec, K=args.steps_per_launch):
+        s = Simulation([ens], precision=prec, integrator=capi.INTEGRATOR_BORIS, collision=capi.COLLISION_HSS,
+                       rng_seed=123, device=dev, steps_per_launch=K, block_size=args.block,
+                       pending_threshold=args.pending)
+        s.set_stream(stream.cuda_stream)
+        s.upload(st0, first_id=first_id)
+        return s
+
+    def timed_loop(sim, n_steps, steps_per_bench, allreduce=True):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n_steps)]
+        kernel_ms, launches, timed_launches = 0.0, 0, 0
+        stats_tot = {"candidates": 0, "collisions": 0}
+        for i in range(n_steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            rs = sim.advance(steps_per_bench)
+            ev[i][1].record(stream)
+            if allreduce and world > 1:
+                parallel.allreduce_moments(sim.moments())
+            kernel_ms += rs["step_kernel_ms"]
+            launches += rs["kernel_launches"]
+            timed_launches += min(math.ceil(steps_per_bench / sim_K(sim)), 64)
+            for k in stats_tot:
+                stats_tot[k] += rs[k]
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev)
+        return ms, kernel_ms, launches, timed_launches, stats_tot
+
+    def sim_K(sim):
+        return args.steps_per_launch if args.steps_per_launch > 0 else 1000
+
+    sim = make_sim(prec_id)
+    # warm-up (same workload), then restart from the initial state
+    for _ in range(args.warmup):
+        sim.advance(STEPS_PER_BENCH_STEP)
+    sim.upload(st0, first_id=first_id)
+    sim.set_clock(0, np.zeros(1))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)).split(",")[0]) if world == 1 else dev)
+    clocks.start()
+    ms, kernel_ms, launches, timed_launches, stt = timed_loop(sim, args.steps, STEPS_PER_BENCH_STEP)
+    clk = clocks.stop()
+    if world > 1:
+        dist.barrier()
+    ms_max = parallel.max_over_ranks(ms)
+    ion_steps = N_IONS * STEPS_PER_BENCH_STEP * args.steps * world
+    value = ion_steps / (ms_max * 1e-3)
+
+    # roofline of the dominant (fused step) kernel: algorithmic bytes per launch / mean launch duration
+    peaks = measured_peaks()
+    avg_launch_ms = kernel_ms / max(timed_launches, 1)
+    bpl = BYTES_PER_ION_LAUNCH[args.precision] * N_IONS
+    achieved = bpl / (avg_launch_ms * 1e-3) / 1e9
+
+    # the same kernel in per-step form (one engine step per launch; state round-trips HBM every step)
+    sim1 = make_sim(prec_id, K=1)
+    for _ in range(3):
+        sim1.advance(10)
+    torch.cuda.synchronize()
+    r1 = sim1.advance(50)
+    avg1 = r1["step_kernel_ms"] / 50
+    ach1 = bpl / (avg1 * 1e-3) / 1e9
+    sim1.close()
+
+    # plain FP64 form of the same kernel (same algorithm), a shorter timed run
+    fp64_line = None
+    if args.precision != "fp64" and args.fp64_steps > 0:
+        s64 = make_sim(capi.PREC_FP64)
+        s64.advance(STEPS_PER_BENCH_STEP)
+        s64.upload(st0, first_id=first_id)
+        torch.cuda.synchronize()
+        ms64, _, _, _, _ = timed_loop(s64, args.fp64_steps, STEPS_PER_BENCH_STEP, allreduce=False)
+        ms64 = parallel.max_over_ranks(ms64)
+        v64 = N_IONS * STEPS_PER_BENCH_STEP * args.fp64_steps * world / (ms64 * 1e-3)
+        fp64_line = {"value": v64, "unit": "ion-steps/s", "steps": args.fp64_steps, "speedup_mixed_over_fp64": value / v64}
+        s64.close()
+
+    # end to end through the C ABI with host buffers: H2D state from pinned
+    # memory, advance one snapshot interval, D2H state, every step
+    e2e_steps = min(args.steps, args.e2e_steps)
+    pin = {k: torch.empty(N_IONS, dtype=torch.float64, pin_memory=True).numpy() for k in ("x", "y", "z", "vx", "vy", "vz")}
+    pin_act = torch.empty(N_IONS, dtype=torch.uint8, pin_memory=True).numpy()
+    for k in pin:
+        pin[k][:] = getattr(st0, k)
+    pin_act[:] = 1
+    host = IonState(x=pin["x"], y=pin["y"], z=pin["z"], vx=pin["vx"], vy=pin["vy"], vz=pin["vz"], mass=st0.mass,
+                    charge=st0.charge, active=pin_act, t_death=None, t_arrival=None)
+    sim.upload(st0, first_id=first_id)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sim.update_state(host)
+        sim.advance(STEPS_PER_BENCH_STEP)
+        capi.check(capi.lib().icb_download_ions(sim._h, capi.dptr(host.x), capi.dptr(host.y), capi.dptr(host.z),
+                                                capi.dptr(host.vx), capi.dptr(host.vy), capi.dptr(host.vz),
+                                                capi.u8ptr(host.active), None, None))
+    torch.cuda.synchronize()
+    e2e_s = parallel.max_over_ranks(time.perf_counter() - t0)
+    e2e_value = N_IONS * STEPS_PER_BENCH_STEP * e2e_steps * world / e2e_s
+    sim.close()
+
+    cpu = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "ion-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {"mixed": "f32 (v, field, collisions) + f64 (x, t)", "fp64": "f64",
+                                       "hilo": "f32 (v) + f32 hi/lo (x)"}[args.precision],
+        "data": "synthetic (reference ion-loader semantics, seed 123)",
+        "config": {"workload": WORKLOAD, "ions_per_gpu": N_IONS, "engine_steps_per_bench_step": STEPS_PER_BENCH_STEP,
+                   "total_engine_steps": STEPS_PER_BENCH_STEP * args.steps, "precision": args.precision,
+                   "steps_per_launch": sim_K(None), "collisions": "HSS null-collision, Philox4x32-10",
+                   "parallelism": f"ions sharded, {world} GPU(s)", "l2": "flushed between timed steps (256 MB write)",
+                   "collision_fraction": stt["collisions"] / max(ion_steps / world, 1)},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"],
+                     "kernel": f"k_step<{args.precision},boris,hss,uniform> fused {sim_K(None)} steps/launch",
+                     "bytes_per_launch": bpl, "avg_launch_ms": avg_launch_ms,
+                     "note": "fused K-step kernel: state crosses HBM once per launch, so it is instruction-issue "
+                             "bound, not HBM bound; see roofline_per_step and profiles/"},
+        "roofline_per_step": {"bound": "hbm", "achieved": ach1, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                              "frac": ach1 / peaks["hbm_gbs"], "avg_launch_ms": avg1,
+                              "kernel": f"k_step<{args.precision},boris,hss,uniform> 1 step/launch",
+                              "ion_steps_per_s": N_IONS / (avg1 * 1e-3)},
+        "fp64_form": fp64_line,
+        "e2e": {"value": e2e_value, "unit": "ion-steps/s", "h2d_bytes_per_step": 6 * 8 * N_IONS,
+                "d2h_bytes_per_step": 6 * 8 * N_IONS + N_IONS, "steps": e2e_steps,
+                "path": "icb_update_state (pinned host) -> icb_advance(1000) -> icb_download_ions (pinned host)"},
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["mixed", "fp64", "hilo"], default="mixed")
+    ap.add_argument("--steps-per-launch", type=int, default=1000)
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--pending", type=int, default=0)
+    ap.add_argument("--fp64-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

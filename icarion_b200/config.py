@@ -1,0 +1,236 @@
+"""ICARION JSON config (the unchanged reference schema) -> ensemble parameters.
+
+Only the subset on the uniform-dt batch step is read: ``simulation``
+(dt_s, total_time_s, write_interval, integrator, enable_gpu, rng_seed),
+``physics.collision_model``, ``domains[]`` (instrument, geometry, env,
+fields.DC / RF / magnetic) and ``ions.species[]``.  Derived values are
+computed with the reference loader's arithmetic:
+
+* n = P / (kB T)                       EnvironmentConfig.h:152
+* axial_V = (E/N [Td] * 1e-21 * n) * L  DomainConfigLoader.cpp:417-431
+* mass = mass_amu * AMU_TO_KG, q = charge * e, CCS = CCS_A2 * 1e-20
+                                        SpeciesConfig.h:72-84
+* gas mass from the species constants  EnvironmentConfig.h:164-200, utils/constants.h
+
+Knobs that are not part of the reference schema (precision mode, steps per
+launch, detector plane, ...) are passed separately, never inside the JSON.
+"""
+from __future__ import annotations
+
+import copy
+import json
+import math
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Any
+
+from . import _capi as capi
+
+# utils/constants.h
+AMU_TO_KG = 1.66053906660e-27
+ELEM_CHARGE_C = 1.602176634e-19
+BOLTZMANN_CONSTANT = 1.380649e-23
+ANGSTROM_TO_M = 1e-10
+ANGSTROM2_TO_M2 = 1e-20
+ANGSTROM3_TO_M3 = 1e-30
+STP_TEMP = 273.15
+STP_PRESSURE = 101325.0
+EPSILON_0 = 8.854187817e-12
+
+GAS_MASS_KG = {
+    "He": 4.002602 * AMU_TO_KG,
+    "Ar": 39.948 * AMU_TO_KG,
+    "CO2": 44.0095 * AMU_TO_KG,
+    "Ne": 20.1797 * AMU_TO_KG,
+    "N2": 28.0134 * AMU_TO_KG,
+    "O2": 31.9988 * AMU_TO_KG,
+    "H2O": 18.01528 * AMU_TO_KG,
+}
+GAS_POLARIZABILITY_M3 = {
+    "He": 0.195e-30, "Ar": 1.596e-30, "CO2": 2.612e-30, "Ne": 0.352e-30,
+    "N2": 1.74e-30, "O2": 1.567e-30, "H2O": 1.45e-30,
+}
+
+INSTRUMENTS = {"IMS": capi.INSTRUMENT_IMS, "FTICR": capi.INSTRUMENT_FTICR,
+               "QuadrupoleRF": capi.INSTRUMENT_QUADRUPOLE_RF}
+INTEGRATORS = {"Boris": capi.INTEGRATOR_BORIS, "RK4": capi.INTEGRATOR_RK4}
+COLLISIONS = {"None": capi.COLLISION_NONE, "none": capi.COLLISION_NONE, "HSS": capi.COLLISION_HSS,
+              "IPM": capi.COLLISION_IPM_TABLE}
+
+
+def gas_density(pressure_pa: float, temperature_k: float) -> float:
+    """n = P / (kB T) (EnvironmentConfig::compute_derived_properties)."""
+    return pressure_pa / (BOLTZMANN_CONSTANT * temperature_k)
+
+
+def axial_voltage_from_en(en_td: float, pressure_pa: float, temperature_k: float, length_m: float) -> float:
+    """E/N [Td] -> axial_V exactly as DomainConfigLoader::load_dc_fields."""
+    k_b = 1.380649e-23
+    n = pressure_pa / (k_b * temperature_k)
+    e_vm = en_td * 1e-21 * n
+    return e_vm * length_m
+
+
+def thermal_width(temperature_k: float, mass_kg: float) -> float:
+    return math.sqrt(BOLTZMANN_CONSTANT * temperature_k / mass_kg)
+
+
+def n0_loschmidt() -> float:
+    """N0 = 101325 / (kB * 273.15) used to reduce mobilities to K0."""
+    return STP_PRESSURE / (BOLTZMANN_CONSTANT * STP_TEMP)
+
+
+@dataclass
+class Species:
+    species_id: str
+    mass_kg: float
+    charge_C: float
+    ccs_m2: float
+    ccs_hss_m2: dict = field(default_factory=dict)
+
+    def sigma_for_gas(self, gas: str) -> float:
+        return self.ccs_hss_m2.get(gas, self.ccs_m2)
+
+
+def species_from_db_entry(sid: str, e: dict) -> Species:
+    ccs = e.get("CCS_A2")
+    return Species(
+        species_id=sid,
+        mass_kg=float(e["mass_amu"]) * AMU_TO_KG,
+        charge_C=int(e["charge"]) * ELEM_CHARGE_C,
+        ccs_m2=(float(ccs) * ANGSTROM2_TO_M2) if ccs is not None else 0.0,
+        ccs_hss_m2={g: float(v) * ANGSTROM2_TO_M2 for g, v in e.get("CCS_HSS", {}).items()},
+    )
+
+
+def ensemble_params(domain: dict, sigma_m2: float, dt_s: float, detector_z_m: float = 1e30,
+                    ipm_bmax_m: float = 0.0) -> dict:
+    """One ensemble (domain + env + ion cross-section + dt) as a plain dict."""
+    geom = domain.get("geometry", {})
+    env = domain.get("env", domain.get("environment", {}))
+    fields = domain.get("fields", {})
+    dc = fields.get("DC", fields.get("dc", {}))
+    rf = fields.get("RF", fields.get("rf", {}))
+    mag = fields.get("magnetic", {})
+    T = float(env.get("temperature_K", 300.0))
+    P = float(env.get("pressure_Pa", 101325.0))
+    gas = env.get("gas_species", "He")
+    L = float(geom.get("length_m", 0.1))
+    axial = 0.0
+    if "EN_Td" in dc:
+        axial = axial_voltage_from_en(float(dc["EN_Td"]), P, T, L)
+    if "axial_V" in dc:
+        axial = float(dc["axial_V"])
+    return {
+        "instrument": INSTRUMENTS[domain.get("instrument", "IMS")],
+        "magnetic_enabled": int(bool(mag.get("enabled", False))),
+        "origin_m": [float(v) for v in geom.get("origin_m", [0.0, 0.0, 0.0])],
+        "length_m": L,
+        "radius_m": float(geom.get("radius_m", 0.05)),
+        "axial_V": axial,
+        "radial_V": float(dc.get("radial_V", 0.0)),
+        "dc_quad_V": float(dc.get("quad_V", 0.0)),
+        "rf_voltage_V": float(rf.get("voltage_V", 0.0)),
+        "rf_frequency_Hz": float(rf.get("frequency_Hz", 0.0)),
+        "B_T": [float(v) for v in mag.get("field_strength_T", [0.0, 0.0, 0.0])],
+        "temperature_K": T,
+        "gas_density_m3": gas_density(P, T),
+        "gas_mass_kg": GAS_MASS_KG[gas],
+        "gas_velocity_m_s": [float(v) for v in env.get("gas_velocity_m_s", [0.0, 0.0, 0.0])],
+        "gas_polarizability_m3": GAS_POLARIZABILITY_M3.get(gas, 0.0),
+        "sigma_m2": float(sigma_m2),
+        "ipm_bmax_m": float(ipm_bmax_m),
+        "dt_s": float(dt_s),
+        "detector_z_m": float(detector_z_m),
+    }
+
+
+def to_struct(p: dict) -> capi.EnsembleParams:
+    s = capi.EnsembleParams()
+    for k, _ in capi.EnsembleParams._fields_:
+        v = p[k]
+        if isinstance(v, (list, tuple)):
+            getattr(s, k)[:] = [float(x) for x in v]
+        else:
+            setattr(s, k, v)
+    return s
+
+
+def species_spec(count: int, mass_kg: float, charge_C: float, position: dict, velocity: dict) -> capi.SpeciesSpec:
+    """IonSpeciesConfig position/velocity blocks -> icb_species_spec."""
+    s = capi.SpeciesSpec()
+    s.count = int(count)
+    s.mass_kg = mass_kg
+    s.charge_C = charge_C
+    ptype = position.get("type", "point").lower()
+    s.position_type = {"point": capi.POS_POINT, "gaussian": capi.POS_GAUSSIAN,
+                       "uniform_sphere": capi.POS_UNIFORM_SPHERE, "uniform_cylinder": capi.POS_UNIFORM_CYLINDER,
+                       "uniform_box": capi.POS_UNIFORM_BOX}[ptype]
+    s.center_m[:] = [float(v) for v in position.get("center", [0.0, 0.0, 0.0])]
+    s.std_m[:] = [float(v) for v in position.get("std", [0.0, 0.0, 0.0])]
+    s.radius_m = float(position.get("radius", 0.0))
+    s.length_m = float(position.get("length", 0.0))
+    s.box_min_m[:] = [float(v) for v in position.get("min", [0.0, 0.0, 0.0])]
+    s.box_max_m[:] = [float(v) for v in position.get("max", [0.0, 0.0, 0.0])]
+    vtype = velocity.get("type", "fixed").lower()
+    s.velocity_type = {"fixed": capi.VEL_FIXED, "thermal": capi.VEL_THERMAL}[vtype]
+    s.velocity_m_s[:] = [float(v) for v in velocity.get("value", [0.0, 0.0, 0.0])]
+    s.temperature_K = float(velocity.get("temperature_K", 300.0))
+    return s
+
+
+@dataclass
+class RunConfig:
+    """The parts of a reference config the batch step needs."""
+    dt_s: float
+    total_time_s: float
+    write_interval: int
+    integrator: int
+    collision_model: int
+    rng_seed: int
+    enable_gpu: bool
+    domain: dict
+    species: list            # list[(Species, count, position, velocity)]
+    raw: dict
+
+    @property
+    def n_steps(self) -> int:
+        return int(round(self.total_time_s / self.dt_s))
+
+
+def load(cfg: Any, species_db: dict | None = None) -> RunConfig:
+    """Read a reference config (path or dict).  ``species_db`` is the parsed
+    species database (``{"species": {...}}``); inline entries in it override
+    the file named by the config's ``species_database``."""
+    if isinstance(cfg, (str, Path)):
+        path = Path(cfg)
+        raw = json.loads(path.read_text())
+        base = path.parent
+    else:
+        raw = copy.deepcopy(cfg)
+        base = Path(".")
+    db = {}
+    if "species_database" in raw and species_db is None:
+        dbp = base / raw["species_database"]
+        if dbp.exists():
+            db = json.loads(dbp.read_text()).get("species", {})
+    if species_db:
+        db.update(species_db.get("species", species_db))
+    sim = raw["simulation"]
+    phys = raw.get("physics", {})
+    species = []
+    for sp in raw.get("ions", {}).get("species", []):
+        spc = species_from_db_entry(sp["id"], db[sp["id"]])
+        species.append((spc, int(sp["count"]), sp.get("position", {}), sp.get("velocity", {})))
+    return RunConfig(
+        dt_s=float(sim["dt_s"]),
+        total_time_s=float(sim["total_time_s"]),
+        write_interval=int(sim.get("write_interval", 1000)),
+        integrator=INTEGRATORS[sim.get("integrator", "RK4")],
+        collision_model=COLLISIONS[phys.get("collision_model", "None")],
+        rng_seed=int(sim.get("rng_seed", 0)),
+        enable_gpu=bool(sim.get("enable_gpu", False)),
+        domain=raw["domains"][0],
+        species=species,
+        raw=raw,
+    )

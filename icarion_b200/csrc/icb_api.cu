@@ -1,0 +1,844 @@
+// icb_api.cu — the C ABI (include/icarion_b200.h): handle lifetime, device
+// resident SoA ion state, launch sequencing, the device engine clock and the
+// deterministic per-ensemble moment reduction.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/icarion_b200.h"
+#include "icb_internal.h"
+#include "icb_params.h"
+#include "icb_rng.cuh"
+
+using namespace icb;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+namespace {
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define ICB_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t err_ = (call);                                                       \
+        if (err_ != cudaSuccess) {                                                       \
+            return fail(err_ == cudaErrorMemoryAllocation ? ICB_ERR_OUT_OF_MEMORY        \
+                                                          : ICB_ERR_CUDA,                \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(err_),        \
+                        __FILE__, __LINE__);                                             \
+        }                                                                                \
+    } while (0)
+
+constexpr double kGeomEps = 1e-12;          // CylindricalGeometry.h:245
+constexpr double kMinVoltage = 1e-12;       // AnalyticalFieldModel voltage threshold
+constexpr double kBoltzmann = 1.380649e-23; // utils/constants.h:15
+constexpr double kMeanChi3 = 1.5957691216057308;  // E|N(0,I3)| = 2 sqrt(2/pi)
+constexpr int kMomItemIons = 8192;
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t alloc(size_t count) {
+        if (p) { cudaFree(p); p = nullptr; n = 0; }
+        if (count == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        return e;
+    }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// auxiliary kernels
+// ---------------------------------------------------------------------------
+namespace {
+
+// Initial collision clocks: S = 1, U = uniform of Philox(id, 0, 3, 0).x.
+template <class R>
+__global__ void k_clock_init(R* S, R* U, uint64_t n, uint64_t first_id, uint64_t seed) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const U4 r = philox4x32_10(static_cast<uint32_t>(first_id + i), 0u, 3u, 0u,
+                               static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32));
+    S[i] = R(1);
+    if constexpr (sizeof(R) == 8) U[i] = unit_d(r.x);
+    else U[i] = unit_f(r.x);
+}
+
+// Device engine clock: step += K and t_e += dt_e, K times (accumulated like
+// the engine's per-step t += dt, SimulationEngineLifecycle.cpp:162).
+__global__ void k_clock_advance(unsigned long long* step, double* t, const double* dt, int n_ens, uint32_t K) {
+    const int e = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (e == 0) *step += K;
+    if (e >= n_ens) return;
+    double te = t[e];
+    const double d = dt[e];
+    for (uint32_t k = 0; k < K; ++k) te = te + d;
+    t[e] = te;
+}
+
+// Upload conversion: staged doubles -> working precision.
+__global__ void k_to_float(const double* __restrict__ src, float* __restrict__ dst, uint64_t n) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = static_cast<float>(src[i]);
+}
+__global__ void k_to_hilo(const double* __restrict__ src, float* __restrict__ hi, float* __restrict__ lo, uint64_t n) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const float h = static_cast<float>(src[i]);
+        hi[i] = h;
+        lo[i] = static_cast<float>(src[i] - static_cast<double>(h));
+    }
+}
+__global__ void k_from_float(const float* __restrict__ src, double* __restrict__ dst, uint64_t n) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = static_cast<double>(src[i]);
+}
+__global__ void k_from_hilo(const float* __restrict__ hi, const float* __restrict__ lo, double* __restrict__ dst, uint64_t n) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = static_cast<double>(hi[i]) + static_cast<double>(lo[i]);
+}
+__global__ void k_flags_in(const uint8_t* __restrict__ active, const double* __restrict__ birth, uint8_t* __restrict__ flags,
+                           double* __restrict__ t_death, double* __restrict__ t_arr, uint64_t n) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool born = birth == nullptr || birth[i] <= 0.0;
+    uint8_t f = 0;
+    if (born) f |= kFlagBorn;
+    if (born && active[i]) f |= kFlagActive;
+    flags[i] = f;
+    t_death[i] = -1.0;
+    t_arr[i] = -1.0;
+}
+__global__ void k_flags_update(const uint8_t* __restrict__ active, uint8_t* __restrict__ flags, uint64_t n) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint8_t f = flags[i];
+    if ((f & kFlagBorn) != 0) f = active[i] ? static_cast<uint8_t>(f | kFlagActive) : static_cast<uint8_t>(f & ~kFlagActive);
+    flags[i] = f;
+}
+__global__ void k_flags_out(const uint8_t* __restrict__ flags, uint8_t* __restrict__ active, uint64_t n) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) active[i] = (flags[i] & kFlagActive) ? 1 : 0;
+}
+
+// Moments: one block per work item (a slice of one ensemble's ions), a
+// fixed-order block reduction into partials[item], then one block per
+// ensemble sums its items in order.  Deterministic for a given item split.
+struct MomItem { uint64_t begin, end; };
+
+template <class R, bool HILO>
+__global__ void __launch_bounds__(256) k_moments_partial(const MomItem* __restrict__ items,
+                                                         const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                                                         const float* __restrict__ xh, const float* __restrict__ xl,
+                                                         const float* __restrict__ yh, const float* __restrict__ yl,
+                                                         const float* __restrict__ zh, const float* __restrict__ zl,
+                                                         const R* __restrict__ vx, const R* __restrict__ vy, const R* __restrict__ vz,
+                                                         const double* __restrict__ xr, const double* __restrict__ yr, const double* __restrict__ zr,
+                                                         const uint8_t* __restrict__ flags, const double* __restrict__ t_death,
+                                                         const double* __restrict__ t_arr, double* __restrict__ partials) {
+    __shared__ double red[8][ICB_N_MOMENTS];
+    const MomItem it = items[blockIdx.x];
+    double acc[ICB_N_MOMENTS];
+#pragma unroll
+    for (int j = 0; j < ICB_N_MOMENTS; ++j) acc[j] = 0.0;
+    for (uint64_t i = it.begin + threadIdx.x; i < it.end; i += blockDim.x) {
+        const uint8_t f = flags[i];
+        if (t_arr[i] >= 0.0) acc[11] += 1.0;
+        if (!(f & kFlagActive)) {
+            if (t_death[i] >= 0.0) acc[12] += 1.0;
+            continue;
+        }
+        double px, py, pz;
+        if constexpr (HILO) {
+            px = static_cast<double>(xh[i]) + static_cast<double>(xl[i]);
+            py = static_cast<double>(yh[i]) + static_cast<double>(yl[i]);
+            pz = static_cast<double>(zh[i]) + static_cast<double>(zl[i]);
+        } else {
+            px = x[i]; py = y[i]; pz = z[i];
+        }
+        const double ux = static_cast<double>(vx[i]), uy = static_cast<double>(vy[i]), uz = static_cast<double>(vz[i]);
+        acc[0] += 1.0;
+        acc[1] += px; acc[2] += py; acc[3] += pz;
+        acc[4] += px * px; acc[5] += py * py; acc[6] += pz * pz;
+        acc[7] += ux; acc[8] += uy; acc[9] += uz;
+        acc[10] += ux * ux + uy * uy + uz * uz;
+        acc[13] += pz * uz;
+        const double dx = px - xr[i], dy = py - yr[i], dz = pz - zr[i];
+        acc[14] += dx; acc[15] += dy; acc[16] += dz;
+        acc[17] += dx * dx; acc[18] += dy * dy; acc[19] += dz * dz;
+    }
+#pragma unroll
+    for (int j = 0; j < ICB_N_MOMENTS; ++j) {
+        double v = acc[j];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        acc[j] = v;
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+#pragma unroll
+        for (int j = 0; j < ICB_N_MOMENTS; ++j) red[w][j] = acc[j];
+    }
+    __syncthreads();
+    if (threadIdx.x < ICB_N_MOMENTS) {
+        double s = 0.0;
+        const int nw = static_cast<int>(blockDim.x >> 5);
+        for (int k = 0; k < nw; ++k) s += red[k][threadIdx.x];
+        partials[static_cast<size_t>(blockIdx.x) * ICB_N_MOMENTS + threadIdx.x] = s;
+    }
+}
+
+__global__ void k_moments_final(const double* __restrict__ partials, const int* __restrict__ item_off,
+                                int n_ens, double* __restrict__ out) {
+    const int e = blockIdx.x;
+    if (e >= n_ens || threadIdx.x >= ICB_N_MOMENTS) return;
+    double s = 0.0;
+    for (int it = item_off[e]; it < item_off[e + 1]; ++it) s += partials[static_cast<size_t>(it) * ICB_N_MOMENTS + threadIdx.x];
+    out[static_cast<size_t>(e) * ICB_N_MOMENTS + threadIdx.x] = s;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------
+struct icb_handle {
+    icb_config cfg{};
+    std::vector<icb_ensemble_params> ens;
+    std::vector<EnsConst> ens_const;
+    int field_kind = kFieldUniform;
+    bool magnetic = false;
+    int coll = kCollNone;
+    int block = 256;
+    uint32_t K = 1000;
+    uint32_t pend = 20;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> kev;      // per-launch events of the step kernel
+    uint64_t launches = 0;             // kernels launched by the current call
+
+    uint64_t n = 0;
+    uint64_t first_id = 0;
+    std::vector<uint64_t> ens_off;
+
+    DevBuf<double> x, y, z;
+    DevBuf<double> xr, yr, zr;   // displacement reference positions
+    DevBuf<float> xh, xl, yh, yl, zh, zl;
+    DevBuf<double> vxd, vyd, vzd;
+    DevBuf<float> vxf, vyf, vzf;
+    DevBuf<double> Sd, Ud;
+    DevBuf<float> Sf, Uf;
+    DevBuf<double> mass, charge, t_death, t_arr, birth;
+    DevBuf<uint8_t> flags, active_stage;
+    DevBuf<double> stage;
+    DevBuf<unsigned long long> counters, step_dev;
+    DevBuf<double> t_dev, dt_dev;
+    DevBuf<MomItem> mom_items;
+    DevBuf<int> mom_item_off;
+    DevBuf<double> mom_partials, mom_out;
+    int n_mom_items = 0;
+    bool has_birth = false;
+
+    bool fp64() const { return cfg.precision == ICB_PREC_FP64; }
+    bool hilo() const { return cfg.precision == ICB_PREC_MIXED_HILO; }
+    void* vx() const { return fp64() ? static_cast<void*>(vxd.p) : static_cast<void*>(vxf.p); }
+    void* vy() const { return fp64() ? static_cast<void*>(vyd.p) : static_cast<void*>(vyf.p); }
+    void* vz() const { return fp64() ? static_cast<void*>(vzd.p) : static_cast<void*>(vzf.p); }
+    ~icb_handle() {
+        for (cudaEvent_t e : kev) cudaEventDestroy(e);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+};
+
+namespace {
+
+int check_handle(icb_handle* h) {
+    if (!h) return fail(ICB_ERR_INVALID_ARGUMENT, "null handle");
+    cudaError_t e = cudaSetDevice(h->cfg.device);
+    if (e != cudaSuccess) return fail(ICB_ERR_CUDA, "cudaSetDevice(%d): %s", h->cfg.device, cudaGetErrorString(e));
+    return ICB_OK;
+}
+
+// Per-ensemble constants exactly as the reference derives them.
+int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, bool& mag, int coll) {
+    std::memset(&C, 0, sizeof(C));
+    if (!(P.length_m > 0.0) || !(P.radius_m > 0.0)) return fail(ICB_ERR_INVALID_ARGUMENT, "ensemble geometry needs length_m > 0 and radius_m > 0");
+    if (!(P.dt_s > 0.0)) return fail(ICB_ERR_INVALID_ARGUMENT, "ensemble dt_s must be > 0");
+    int kind = kFieldUniform;
+    const bool rf = std::fabs(P.rf_voltage_V) > kMinVoltage;
+    switch (P.instrument) {
+        case ICB_INSTRUMENT_IMS:            // AnalyticalFieldModel.cpp:136-161
+            C.E0[2] = P.axial_V / P.length_m;
+            if (rf) kind = kFieldLinearRF;
+            break;
+        case ICB_INSTRUMENT_QUADRUPOLE_RF:  // AnalyticalFieldModel.cpp:219-248
+            if (std::fabs(P.axial_V) > kMinVoltage) C.E0[2] = P.axial_V / P.length_m;
+            if (rf) kind = kFieldLinearRF;
+            break;
+        case ICB_INSTRUMENT_FTICR: {        // AnalyticalFieldModel.cpp:174-186
+            const double L = P.length_m, r = P.radius_m;
+            const double d = std::sqrt((L * L / 8.0) + (r * r / 4.0));
+            const double factor = P.radial_V / (d * d);
+            C.G[0] = factor; C.G[1] = factor; C.G[2] = -2.0 * factor;
+            C.c[2] = 0.5 * L;
+            kind = kFieldLinear;
+            break;
+        }
+        default:
+            return fail(ICB_ERR_UNSUPPORTED, "instrument %d not supported", P.instrument);
+    }
+    if (rf) {
+        C.rf = 1;
+        C.rf_U0 = P.dc_quad_V;
+        C.rf_V = P.rf_voltage_V;
+        C.rf_omega = 2.0 * M_PI * P.rf_frequency_Hz;
+        C.r0sq = P.radius_m * P.radius_m;
+    }
+    field_kind = std::max(field_kind, kind);
+    if (P.magnetic_enabled) {
+        C.magnetic = 1;
+        for (int a = 0; a < 3; ++a) C.B[a] = P.B_T[a];
+        if (P.B_T[0] != 0.0 || P.B_T[1] != 0.0 || P.B_T[2] != 0.0) mag = true;
+    }
+    C.ox = P.origin_m[0]; C.oy = P.origin_m[1]; C.oz = P.origin_m[2];
+    C.zmax_local = P.length_m + kGeomEps;
+    C.rmax2 = (P.radius_m + kGeomEps) * (P.radius_m + kGeomEps);
+    C.dt = P.dt_s;
+    if (coll != kCollNone) {
+        if (!(P.gas_mass_kg > 0.0) || !(P.temperature_K > 0.0))
+            return fail(ICB_ERR_INVALID_ARGUMENT, "collisions need gas_mass_kg > 0 and temperature_K > 0");
+        if (!(P.sigma_m2 > 0.0) || !(P.gas_density_m3 >= 0.0))
+            return fail(ICB_ERR_INVALID_ARGUMENT, "collisions need sigma_m2 > 0 and gas_density_m3 >= 0");
+        C.A = P.gas_density_m3 * P.sigma_m2 * P.dt_s;
+        C.sig_n = std::sqrt(kBoltzmann * P.temperature_K / P.gas_mass_kg);
+        C.mean_th = C.sig_n * kMeanChi3;
+        C.m_gas = P.gas_mass_kg;
+        for (int a = 0; a < 3; ++a) C.ug[a] = P.gas_velocity_m_s[a];
+    }
+    C.zdet = P.detector_z_m;
+    return ICB_OK;
+}
+
+inline unsigned grid_for(uint64_t n, int block) { return static_cast<unsigned>((n + block - 1) / block); }
+
+int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_finalize) {
+    const int n_ens = static_cast<int>(h->ens.size());
+    for (int e0 = 0; e0 < n_ens; e0 += kMaxLaunchEns) {
+        const int ne = std::min(kMaxLaunchEns, n_ens - e0);
+        const uint64_t b = h->ens_off[static_cast<size_t>(e0)];
+        const uint64_t en = h->ens_off[static_cast<size_t>(e0 + ne)];
+        if (en <= b) continue;
+        StepParams p;
+        std::memset(&p, 0, sizeof(p));
+        p.x = h->x.p; p.y = h->y.p; p.z = h->z.p;
+        p.xh = h->xh.p; p.xl = h->xl.p; p.yh = h->yh.p; p.yl = h->yl.p; p.zh = h->zh.p; p.zl = h->zl.p;
+        p.vx = h->vx(); p.vy = h->vy(); p.vz = h->vz();
+        p.clkS = h->fp64() ? static_cast<void*>(h->Sd.p) : static_cast<void*>(h->Sf.p);
+        p.clkU = h->fp64() ? static_cast<void*>(h->Ud.p) : static_cast<void*>(h->Uf.p);
+        p.mass = h->mass.p; p.charge = h->charge.p; p.flags = h->flags.p;
+        p.t_death = h->t_death.p; p.t_arr = h->t_arr.p;
+        p.birth = h->has_birth ? h->birth.p : nullptr;
+        p.counters = h->counters.p;
+        p.step_dev = h->step_dev.p;
+        p.t_dev = h->t_dev.p;
+        p.first_id = h->first_id;
+        p.seed = h->cfg.rng_seed;
+        p.n_steps = K;
+        p.pend_threshold = h->pend;
+        p.ens_base = static_cast<uint32_t>(e0);
+        p.n_ens = static_cast<uint32_t>(ne);
+        p.do_push = do_push; p.do_collide = do_collide; p.do_finalize = do_finalize;
+        for (int e = 0; e <= ne; ++e) p.ens_off[e] = h->ens_off[static_cast<size_t>(e0 + e)];
+        for (int e = 0; e < ne; ++e) p.ens[e] = h->ens_const[static_cast<size_t>(e0 + e)];
+        const dim3 grid(grid_for(en - b, h->block)), block(static_cast<unsigned>(h->block));
+        cudaError_t err;
+        switch (h->cfg.precision) {
+            case ICB_PREC_FP64: err = launch_step_fp64(h->cfg.integrator, h->coll, h->field_kind, h->magnetic, p, grid, block, h->stream); break;
+            case ICB_PREC_MIXED: err = launch_step_mixed(h->cfg.integrator, h->coll, h->field_kind, h->magnetic, p, grid, block, h->stream); break;
+            default: err = launch_step_hilo(h->cfg.integrator, h->coll, h->field_kind, h->magnetic, p, grid, block, h->stream); break;
+        }
+        ++h->launches;
+        if (err == cudaErrorNotSupported)
+            return fail(ICB_ERR_UNSUPPORTED, "no kernel for precision %d integrator %d collision %d",
+                        h->cfg.precision, h->cfg.integrator, h->cfg.collision_model);
+        if (err != cudaSuccess) return fail(ICB_ERR_CUDA, "step kernel launch: %s", cudaGetErrorString(err));
+    }
+    return ICB_OK;
+}
+
+int read_stats(icb_handle* h, icb_run_stats* st, uint64_t steps, size_t n_timed_launches) {
+    unsigned long long c[kNumCounters];
+    ICB_CUDA(cudaMemcpyAsync(c, h->counters.p, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
+    float ms = 0.f;
+    ICB_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    double kms = 0.0;
+    for (size_t j = 0; j < n_timed_launches; ++j) {
+        float m = 0.f;
+        ICB_CUDA(cudaEventElapsedTime(&m, h->kev[2 * j], h->kev[2 * j + 1]));
+        kms += m;
+    }
+    st->step_kernel_ms = kms;
+    st->kernel_launches = h->launches;
+    st->steps = steps;
+    st->candidates = c[kCntCandidates];
+    st->collisions = c[kCntCollisions];
+    st->rate_overflows = c[kCntOverflow];
+    st->deaths = c[kCntDeaths];
+    st->arrivals = c[kCntArrivals];
+    st->device_ms = static_cast<double>(ms);
+    return ICB_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int icb_abi_version(void) { return ICB_ABI_VERSION; }
+
+const char* icb_last_error(void) { return g_last_error.c_str(); }
+
+int icb_device_count(int* count) {
+    if (!count) return fail(ICB_ERR_INVALID_ARGUMENT, "null count");
+    int c = 0;
+    cudaError_t e = cudaGetDeviceCount(&c);
+    if (e != cudaSuccess) {
+        *count = 0;
+        return fail(ICB_ERR_NO_DEVICE, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    }
+    *count = c;
+    return ICB_OK;
+}
+
+int icb_create(const icb_config* cfg, icb_handle** out) {
+    if (!cfg || !out) return fail(ICB_ERR_INVALID_ARGUMENT, "null config or output pointer");
+    *out = nullptr;
+    if (cfg->n_ensembles < 1 || cfg->n_ensembles > ICB_MAX_ENSEMBLES || !cfg->ensembles)
+        return fail(ICB_ERR_INVALID_ARGUMENT, "n_ensembles must be in [1, %d] with a parameter array", ICB_MAX_ENSEMBLES);
+    if (cfg->precision < ICB_PREC_FP64 || cfg->precision > ICB_PREC_MIXED_HILO)
+        return fail(ICB_ERR_INVALID_ARGUMENT, "unknown precision %d", cfg->precision);
+    if (cfg->integrator != ICB_INTEGRATOR_BORIS && cfg->integrator != ICB_INTEGRATOR_RK4)
+        return fail(ICB_ERR_INVALID_ARGUMENT, "unknown integrator %d", cfg->integrator);
+    if (cfg->precision == ICB_PREC_MIXED_HILO && cfg->integrator != ICB_INTEGRATOR_BORIS)
+        return fail(ICB_ERR_UNSUPPORTED, "the hi/lo position variant is built for the Boris pusher only");
+    int coll;
+    switch (cfg->collision_model) {
+        case ICB_COLLISION_NONE: coll = kCollNone; break;
+        case ICB_COLLISION_HSS: coll = kCollHSS; break;
+        default: return fail(ICB_ERR_UNSUPPORTED, "collision model %d not available", cfg->collision_model);
+    }
+    int ndev = 0;
+    cudaError_t ce = cudaGetDeviceCount(&ndev);
+    if (ce != cudaSuccess || ndev == 0) return fail(ICB_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(ce));
+    if (cfg->device < 0 || cfg->device >= ndev) return fail(ICB_ERR_INVALID_ARGUMENT, "device %d out of range (%d devices)", cfg->device, ndev);
+    std::unique_ptr<icb_handle> h(new icb_handle());
+    h->cfg = *cfg;
+    h->cfg.ensembles = nullptr;
+    h->coll = coll;
+    h->ens.assign(cfg->ensembles, cfg->ensembles + cfg->n_ensembles);
+    h->ens_const.resize(h->ens.size());
+    for (size_t e = 0; e < h->ens.size(); ++e) {
+        int r = build_ens_const(h->ens[e], h->ens_const[e], h->field_kind, h->magnetic, coll);
+        if (r != ICB_OK) return r;
+    }
+    if (cfg->block_size > 0) {
+        if (cfg->block_size % 32 != 0 || cfg->block_size > 256)
+            return fail(ICB_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 and <= 256");
+        h->block = cfg->block_size;
+    }
+    if (cfg->steps_per_launch > 0) h->K = static_cast<uint32_t>(cfg->steps_per_launch);
+    if (cfg->pending_threshold > 0) h->pend = static_cast<uint32_t>(std::min(cfg->pending_threshold, 32));
+    ICB_CUDA(cudaSetDevice(cfg->device));
+    ICB_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    h->stream = h->own_stream;
+    ICB_CUDA(cudaEventCreate(&h->ev0));
+    ICB_CUDA(cudaEventCreate(&h->ev1));
+    ICB_CUDA(h->counters.alloc(kNumCounters));
+    ICB_CUDA(h->step_dev.alloc(1));
+    ICB_CUDA(h->t_dev.alloc(h->ens.size()));
+    ICB_CUDA(h->dt_dev.alloc(h->ens.size()));
+    std::vector<double> dts(h->ens.size()), zeros(h->ens.size(), 0.0);
+    for (size_t e = 0; e < h->ens.size(); ++e) dts[e] = h->ens[e].dt_s;
+    ICB_CUDA(cudaMemcpy(h->dt_dev.p, dts.data(), dts.size() * sizeof(double), cudaMemcpyHostToDevice));
+    ICB_CUDA(cudaMemcpy(h->t_dev.p, zeros.data(), zeros.size() * sizeof(double), cudaMemcpyHostToDevice));
+    ICB_CUDA(cudaMemset(h->step_dev.p, 0, sizeof(unsigned long long)));
+    ICB_CUDA(cudaMemset(h->counters.p, 0, kNumCounters * sizeof(unsigned long long)));
+    ICB_CUDA(h->mom_out.alloc(h->ens.size() * ICB_N_MOMENTS));
+    *out = h.release();
+    return ICB_OK;
+}
+
+int icb_destroy(icb_handle* h) {
+    if (!h) return ICB_OK;
+    cudaSetDevice(h->cfg.device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    delete h;
+    return ICB_OK;
+}
+
+int icb_set_stream(icb_handle* h, void* cuda_stream) {
+    if (int r = check_handle(h)) return r;
+    h->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : h->own_stream;
+    return ICB_OK;
+}
+
+int icb_synchronize(icb_handle* h) {
+    if (int r = check_handle(h)) return r;
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
+    return ICB_OK;
+}
+
+uint64_t icb_ion_count(icb_handle* h) { return h ? h->n : 0; }
+
+int icb_upload_ions(icb_handle* h, uint64_t n,
+                    const double* x, const double* y, const double* z,
+                    const double* vx, const double* vy, const double* vz,
+                    const double* mass_kg, const double* charge_C,
+                    const uint8_t* active, const double* birth_time_s,
+                    const uint64_t* ens_offsets, uint64_t first_ion_id) {
+    if (int r = check_handle(h)) return r;
+    if (n == 0) return fail(ICB_ERR_INVALID_ARGUMENT, "no ions");
+    if (!x || !y || !z || !vx || !vy || !vz || !mass_kg || !charge_C || !active)
+        return fail(ICB_ERR_INVALID_ARGUMENT, "state arrays must not be NULL");
+    if (first_ion_id + n > (1ull << 32)) return fail(ICB_ERR_INVALID_ARGUMENT, "ion ids must fit in 32 bits");
+    const size_t ne = h->ens.size();
+    std::vector<uint64_t> off(ne + 1);
+    if (ens_offsets) {
+        for (size_t e = 0; e <= ne; ++e) off[e] = ens_offsets[e];
+        if (off[0] != 0 || off[ne] != n) return fail(ICB_ERR_INVALID_ARGUMENT, "ens_offsets must start at 0 and end at n");
+        for (size_t e = 0; e < ne; ++e)
+            if (off[e + 1] < off[e]) return fail(ICB_ERR_INVALID_ARGUMENT, "ens_offsets must be non-decreasing");
+    } else {
+        if (ne != 1) return fail(ICB_ERR_INVALID_ARGUMENT, "ens_offsets required with %zu ensembles", ne);
+        off[0] = 0; off[1] = n;
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+        if (!(mass_kg[i] > 0.0)) return fail(ICB_ERR_INVALID_ARGUMENT, "ion %llu: mass must be > 0", static_cast<unsigned long long>(i));
+    }
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->n != n) {
+        const bool f64 = h->fp64(), hl = h->hilo();
+        ICB_CUDA(h->x.alloc(hl ? 0 : n)); ICB_CUDA(h->y.alloc(hl ? 0 : n)); ICB_CUDA(h->z.alloc(hl ? 0 : n));
+        ICB_CUDA(h->xh.alloc(hl ? n : 0)); ICB_CUDA(h->xl.alloc(hl ? n : 0));
+        ICB_CUDA(h->yh.alloc(hl ? n : 0)); ICB_CUDA(h->yl.alloc(hl ? n : 0));
+        ICB_CUDA(h->zh.alloc(hl ? n : 0)); ICB_CUDA(h->zl.alloc(hl ? n : 0));
+        ICB_CUDA(h->vxd.alloc(f64 ? n : 0)); ICB_CUDA(h->vyd.alloc(f64 ? n : 0)); ICB_CUDA(h->vzd.alloc(f64 ? n : 0));
+        ICB_CUDA(h->vxf.alloc(f64 ? 0 : n)); ICB_CUDA(h->vyf.alloc(f64 ? 0 : n)); ICB_CUDA(h->vzf.alloc(f64 ? 0 : n));
+        const bool clk = h->coll != kCollNone;
+        ICB_CUDA(h->Sd.alloc(clk && f64 ? n : 0)); ICB_CUDA(h->Ud.alloc(clk && f64 ? n : 0));
+        ICB_CUDA(h->Sf.alloc(clk && !f64 ? n : 0)); ICB_CUDA(h->Uf.alloc(clk && !f64 ? n : 0));
+        ICB_CUDA(h->xr.alloc(n)); ICB_CUDA(h->yr.alloc(n)); ICB_CUDA(h->zr.alloc(n));
+        ICB_CUDA(h->mass.alloc(n)); ICB_CUDA(h->charge.alloc(n));
+        ICB_CUDA(h->t_death.alloc(n)); ICB_CUDA(h->t_arr.alloc(n)); ICB_CUDA(h->birth.alloc(n));
+        ICB_CUDA(h->flags.alloc(n)); ICB_CUDA(h->active_stage.alloc(n));
+        ICB_CUDA(h->stage.alloc(f64 ? 0 : n));
+        h->n = n;
+    }
+    h->first_id = first_ion_id;
+    h->ens_off = off;
+    cudaStream_t s = h->stream;
+    const unsigned g = grid_for(n, 256);
+    const size_t bytes = n * sizeof(double);
+    // positions
+    const double* pos[3] = {x, y, z};
+    DevBuf<double>* pd[3] = {&h->x, &h->y, &h->z};
+    DevBuf<float>* ph[3] = {&h->xh, &h->yh, &h->zh};
+    DevBuf<float>* pl[3] = {&h->xl, &h->yl, &h->zl};
+    for (int a = 0; a < 3; ++a) {
+        if (h->hilo()) {
+            ICB_CUDA(cudaMemcpyAsync(h->stage.p, pos[a], bytes, cudaMemcpyHostToDevice, s));
+            k_to_hilo<<<g, 256, 0, s>>>(h->stage.p, ph[a]->p, pl[a]->p, n);
+            ICB_CUDA(cudaGetLastError());
+        } else {
+            ICB_CUDA(cudaMemcpyAsync(pd[a]->p, pos[a], bytes, cudaMemcpyHostToDevice, s));
+        }
+    }
+    DevBuf<double>* pr[3] = {&h->xr, &h->yr, &h->zr};
+    for (int a = 0; a < 3; ++a) ICB_CUDA(cudaMemcpyAsync(pr[a]->p, pos[a], bytes, cudaMemcpyHostToDevice, s));
+    const double* vel[3] = {vx, vy, vz};
+    DevBuf<double>* vd[3] = {&h->vxd, &h->vyd, &h->vzd};
+    DevBuf<float>* vf[3] = {&h->vxf, &h->vyf, &h->vzf};
+    for (int a = 0; a < 3; ++a) {
+        if (h->fp64()) {
+            ICB_CUDA(cudaMemcpyAsync(vd[a]->p, vel[a], bytes, cudaMemcpyHostToDevice, s));
+        } else {
+            ICB_CUDA(cudaMemcpyAsync(h->stage.p, vel[a], bytes, cudaMemcpyHostToDevice, s));
+            k_to_float<<<g, 256, 0, s>>>(h->stage.p, vf[a]->p, n);
+            ICB_CUDA(cudaGetLastError());
+        }
+    }
+    ICB_CUDA(cudaMemcpyAsync(h->mass.p, mass_kg, bytes, cudaMemcpyHostToDevice, s));
+    ICB_CUDA(cudaMemcpyAsync(h->charge.p, charge_C, bytes, cudaMemcpyHostToDevice, s));
+    ICB_CUDA(cudaMemcpyAsync(h->active_stage.p, active, n, cudaMemcpyHostToDevice, s));
+    h->has_birth = birth_time_s != nullptr;
+    if (birth_time_s) ICB_CUDA(cudaMemcpyAsync(h->birth.p, birth_time_s, bytes, cudaMemcpyHostToDevice, s));
+    k_flags_in<<<g, 256, 0, s>>>(h->active_stage.p, h->has_birth ? h->birth.p : nullptr, h->flags.p, h->t_death.p, h->t_arr.p, n);
+    ICB_CUDA(cudaGetLastError());
+    if (h->coll != kCollNone) {
+        if (h->fp64()) k_clock_init<double><<<g, 256, 0, s>>>(h->Sd.p, h->Ud.p, n, first_ion_id, h->cfg.rng_seed);
+        else k_clock_init<float><<<g, 256, 0, s>>>(h->Sf.p, h->Uf.p, n, first_ion_id, h->cfg.rng_seed);
+        ICB_CUDA(cudaGetLastError());
+    }
+    // moment work items: slices of <= kMomItemIons ions, never crossing an ensemble
+    std::vector<MomItem> items;
+    std::vector<int> item_off(ne + 1, 0);
+    for (size_t e = 0; e < ne; ++e) {
+        item_off[e] = static_cast<int>(items.size());
+        for (uint64_t b = off[e]; b < off[e + 1]; b += kMomItemIons)
+            items.push_back(MomItem{b, std::min<uint64_t>(off[e + 1], b + kMomItemIons)});
+    }
+    item_off[ne] = static_cast<int>(items.size());
+    h->n_mom_items = static_cast<int>(items.size());
+    ICB_CUDA(h->mom_items.alloc(std::max<size_t>(items.size(), 1)));
+    ICB_CUDA(h->mom_item_off.alloc(ne + 1));
+    ICB_CUDA(h->mom_partials.alloc(std::max<size_t>(items.size(), 1) * ICB_N_MOMENTS));
+    if (!items.empty()) ICB_CUDA(cudaMemcpyAsync(h->mom_items.p, items.data(), items.size() * sizeof(MomItem), cudaMemcpyHostToDevice, s));
+    ICB_CUDA(cudaMemcpyAsync(h->mom_item_off.p, item_off.data(), item_off.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
+    return ICB_OK;
+}
+
+int icb_update_state(icb_handle* h, const double* x, const double* y, const double* z,
+                     const double* vx, const double* vy, const double* vz, const uint8_t* active) {
+    if (int r = check_handle(h)) return r;
+    if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
+    cudaStream_t s = h->stream;
+    const uint64_t n = h->n;
+    const unsigned g = grid_for(n, 256);
+    const size_t bytes = n * sizeof(double);
+    const double* pos[3] = {x, y, z};
+    DevBuf<double>* pd[3] = {&h->x, &h->y, &h->z};
+    DevBuf<float>* ph[3] = {&h->xh, &h->yh, &h->zh};
+    DevBuf<float>* pl[3] = {&h->xl, &h->yl, &h->zl};
+    for (int a = 0; a < 3; ++a) {
+        if (!pos[a]) continue;
+        if (h->hilo()) {
+            ICB_CUDA(cudaMemcpyAsync(h->stage.p, pos[a], bytes, cudaMemcpyHostToDevice, s));
+            k_to_hilo<<<g, 256, 0, s>>>(h->stage.p, ph[a]->p, pl[a]->p, n);
+            ICB_CUDA(cudaGetLastError());
+        } else {
+            ICB_CUDA(cudaMemcpyAsync(pd[a]->p, pos[a], bytes, cudaMemcpyHostToDevice, s));
+        }
+    }
+    const double* vel[3] = {vx, vy, vz};
+    DevBuf<double>* vd[3] = {&h->vxd, &h->vyd, &h->vzd};
+    DevBuf<float>* vf[3] = {&h->vxf, &h->vyf, &h->vzf};
+    for (int a = 0; a < 3; ++a) {
+        if (!vel[a]) continue;
+        if (h->fp64()) {
+            ICB_CUDA(cudaMemcpyAsync(vd[a]->p, vel[a], bytes, cudaMemcpyHostToDevice, s));
+        } else {
+            ICB_CUDA(cudaMemcpyAsync(h->stage.p, vel[a], bytes, cudaMemcpyHostToDevice, s));
+            k_to_float<<<g, 256, 0, s>>>(h->stage.p, vf[a]->p, n);
+            ICB_CUDA(cudaGetLastError());
+        }
+    }
+    if (active) {
+        ICB_CUDA(cudaMemcpyAsync(h->active_stage.p, active, n, cudaMemcpyHostToDevice, s));
+        k_flags_update<<<g, 256, 0, s>>>(h->active_stage.p, h->flags.p, n);
+        ICB_CUDA(cudaGetLastError());
+    }
+    return ICB_OK;
+}
+
+int icb_download_ions(icb_handle* h, double* x, double* y, double* z,
+                      double* vx, double* vy, double* vz,
+                      uint8_t* active, double* death_time_s, double* arrival_time_s) {
+    if (int r = check_handle(h)) return r;
+    if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
+    cudaStream_t s = h->stream;
+    const uint64_t n = h->n;
+    const unsigned g = grid_for(n, 256);
+    const size_t bytes = n * sizeof(double);
+    double* pos[3] = {x, y, z};
+    DevBuf<double>* pd[3] = {&h->x, &h->y, &h->z};
+    DevBuf<float>* ph[3] = {&h->xh, &h->yh, &h->zh};
+    DevBuf<float>* pl[3] = {&h->xl, &h->yl, &h->zl};
+    for (int a = 0; a < 3; ++a) {
+        if (!pos[a]) continue;
+        if (h->hilo()) {
+            k_from_hilo<<<g, 256, 0, s>>>(ph[a]->p, pl[a]->p, h->stage.p, n);
+            ICB_CUDA(cudaGetLastError());
+            ICB_CUDA(cudaMemcpyAsync(pos[a], h->stage.p, bytes, cudaMemcpyDeviceToHost, s));
+            ICB_CUDA(cudaStreamSynchronize(s));
+        } else {
+            ICB_CUDA(cudaMemcpyAsync(pos[a], pd[a]->p, bytes, cudaMemcpyDeviceToHost, s));
+        }
+    }
+    double* vel[3] = {vx, vy, vz};
+    DevBuf<double>* vd[3] = {&h->vxd, &h->vyd, &h->vzd};
+    DevBuf<float>* vf[3] = {&h->vxf, &h->vyf, &h->vzf};
+    for (int a = 0; a < 3; ++a) {
+        if (!vel[a]) continue;
+        if (h->fp64()) {
+            ICB_CUDA(cudaMemcpyAsync(vel[a], vd[a]->p, bytes, cudaMemcpyDeviceToHost, s));
+        } else {
+            k_from_float<<<g, 256, 0, s>>>(vf[a]->p, h->stage.p, n);
+            ICB_CUDA(cudaGetLastError());
+            ICB_CUDA(cudaMemcpyAsync(vel[a], h->stage.p, bytes, cudaMemcpyDeviceToHost, s));
+            ICB_CUDA(cudaStreamSynchronize(s));
+        }
+    }
+    if (active) {
+        k_flags_out<<<g, 256, 0, s>>>(h->flags.p, h->active_stage.p, n);
+        ICB_CUDA(cudaGetLastError());
+        ICB_CUDA(cudaMemcpyAsync(active, h->active_stage.p, n, cudaMemcpyDeviceToHost, s));
+    }
+    if (death_time_s) ICB_CUDA(cudaMemcpyAsync(death_time_s, h->t_death.p, bytes, cudaMemcpyDeviceToHost, s));
+    if (arrival_time_s) ICB_CUDA(cudaMemcpyAsync(arrival_time_s, h->t_arr.p, bytes, cudaMemcpyDeviceToHost, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
+    return ICB_OK;
+}
+
+int icb_advance(icb_handle* h, uint64_t n_steps, icb_run_stats* stats) {
+    if (int r = check_handle(h)) return r;
+    if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
+    cudaStream_t s = h->stream;
+    ICB_CUDA(cudaMemsetAsync(h->counters.p, 0, kNumCounters * sizeof(unsigned long long), s));
+    ICB_CUDA(cudaEventRecord(h->ev0, s));
+    h->launches = 0;
+    const int ne = static_cast<int>(h->ens.size());
+    // Per-launch events around the step kernels when statistics are asked
+    // for (at most 64 launches are timed individually per call).
+    const size_t n_launch = static_cast<size_t>((n_steps + h->K - 1) / h->K);
+    const size_t n_timed = stats ? std::min<size_t>(n_launch, 64) : 0;
+    while (h->kev.size() < 2 * n_timed) {
+        cudaEvent_t e;
+        ICB_CUDA(cudaEventCreate(&e));
+        h->kev.push_back(e);
+    }
+    uint64_t left = n_steps;
+    size_t j = 0;
+    while (left > 0) {
+        const uint32_t K = static_cast<uint32_t>(std::min<uint64_t>(left, h->K));
+        if (j < n_timed) ICB_CUDA(cudaEventRecord(h->kev[2 * j], s));
+        if (int r = launch_step(h, K, 1, 1, 1)) return r;
+        if (j < n_timed) ICB_CUDA(cudaEventRecord(h->kev[2 * j + 1], s));
+        k_clock_advance<<<(ne + 127) / 128, 128, 0, s>>>(h->step_dev.p, h->t_dev.p, h->dt_dev.p, ne, K);
+        ICB_CUDA(cudaGetLastError());
+        ++h->launches;
+        left -= K;
+        ++j;
+    }
+    ICB_CUDA(cudaEventRecord(h->ev1, s));
+    if (stats) return read_stats(h, stats, n_steps, n_timed);
+    return ICB_OK;
+}
+
+static int single_part(icb_handle* h, int push, int collide, int finalize, icb_run_stats* stats) {
+    if (int r = check_handle(h)) return r;
+    if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
+    cudaStream_t s = h->stream;
+    ICB_CUDA(cudaMemsetAsync(h->counters.p, 0, kNumCounters * sizeof(unsigned long long), s));
+    ICB_CUDA(cudaEventRecord(h->ev0, s));
+    h->launches = 0;
+    if (int r = launch_step(h, 1, push, collide, finalize)) return r;
+    if (finalize) {
+        const int ne = static_cast<int>(h->ens.size());
+        k_clock_advance<<<(ne + 127) / 128, 128, 0, s>>>(h->step_dev.p, h->t_dev.p, h->dt_dev.p, ne, 1);
+        ICB_CUDA(cudaGetLastError());
+        ++h->launches;
+    }
+    ICB_CUDA(cudaEventRecord(h->ev1, s));
+    if (stats) return read_stats(h, stats, finalize ? 1 : 0, 0);
+    return ICB_OK;
+}
+
+int icb_push(icb_handle* h) { return single_part(h, 1, 0, 0, nullptr); }
+int icb_collide(icb_handle* h, icb_run_stats* stats) { return single_part(h, 0, 1, 0, stats); }
+int icb_finalize(icb_handle* h, icb_run_stats* stats) { return single_part(h, 0, 0, 1, stats); }
+
+int icb_get_clock(icb_handle* h, uint64_t* step, double* time_s) {
+    if (int r = check_handle(h)) return r;
+    unsigned long long st = 0;
+    ICB_CUDA(cudaMemcpyAsync(&st, h->step_dev.p, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+    if (time_s) ICB_CUDA(cudaMemcpyAsync(time_s, h->t_dev.p, h->ens.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
+    if (step) *step = st;
+    return ICB_OK;
+}
+
+int icb_set_clock(icb_handle* h, uint64_t step, const double* time_s) {
+    if (int r = check_handle(h)) return r;
+    unsigned long long st = step;
+    ICB_CUDA(cudaMemcpyAsync(h->step_dev.p, &st, sizeof(st), cudaMemcpyHostToDevice, h->stream));
+    if (time_s) ICB_CUDA(cudaMemcpyAsync(h->t_dev.p, time_s, h->ens.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
+    return ICB_OK;
+}
+
+int icb_moments(icb_handle* h, double* out) {
+    if (int r = check_handle(h)) return r;
+    if (!out) return fail(ICB_ERR_INVALID_ARGUMENT, "null output");
+    if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
+    cudaStream_t s = h->stream;
+    const int ne = static_cast<int>(h->ens.size());
+    if (h->n_mom_items > 0) {
+        if (h->fp64()) {
+            k_moments_partial<double, false><<<h->n_mom_items, 256, 0, s>>>(
+                h->mom_items.p, h->x.p, h->y.p, h->z.p, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                h->vxd.p, h->vyd.p, h->vzd.p, h->xr.p, h->yr.p, h->zr.p, h->flags.p, h->t_death.p, h->t_arr.p, h->mom_partials.p);
+        } else if (h->hilo()) {
+            k_moments_partial<float, true><<<h->n_mom_items, 256, 0, s>>>(
+                h->mom_items.p, nullptr, nullptr, nullptr, h->xh.p, h->xl.p, h->yh.p, h->yl.p, h->zh.p, h->zl.p,
+                h->vxf.p, h->vyf.p, h->vzf.p, h->xr.p, h->yr.p, h->zr.p, h->flags.p, h->t_death.p, h->t_arr.p, h->mom_partials.p);
+        } else {
+            k_moments_partial<float, false><<<h->n_mom_items, 256, 0, s>>>(
+                h->mom_items.p, h->x.p, h->y.p, h->z.p, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                h->vxf.p, h->vyf.p, h->vzf.p, h->xr.p, h->yr.p, h->zr.p, h->flags.p, h->t_death.p, h->t_arr.p, h->mom_partials.p);
+        }
+        ICB_CUDA(cudaGetLastError());
+    }
+    k_moments_final<<<ne, 32, 0, s>>>(h->mom_partials.p, h->mom_item_off.p, ne, h->mom_out.p);
+    ICB_CUDA(cudaGetLastError());
+    ICB_CUDA(cudaMemcpyAsync(out, h->mom_out.p, static_cast<size_t>(ne) * ICB_N_MOMENTS * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ICB_CUDA(cudaStreamSynchronize(s));
+    return ICB_OK;
+}
+
+int icb_mark_reference(icb_handle* h) {
+    if (int r = check_handle(h)) return r;
+    if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
+    cudaStream_t s = h->stream;
+    const uint64_t n = h->n;
+    if (h->hilo()) {
+        const unsigned g = grid_for(n, 256);
+        k_from_hilo<<<g, 256, 0, s>>>(h->xh.p, h->xl.p, h->xr.p, n);
+        k_from_hilo<<<g, 256, 0, s>>>(h->yh.p, h->yl.p, h->yr.p, n);
+        k_from_hilo<<<g, 256, 0, s>>>(h->zh.p, h->zl.p, h->zr.p, n);
+        ICB_CUDA(cudaGetLastError());
+    } else {
+        ICB_CUDA(cudaMemcpyAsync(h->xr.p, h->x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        ICB_CUDA(cudaMemcpyAsync(h->yr.p, h->y.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        ICB_CUDA(cudaMemcpyAsync(h->zr.p, h->z.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    return ICB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,18 @@
+// icb_internal.h — host-side declarations shared by the library's .cu files.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "icb_params.h"
+
+namespace icb {
+
+// Kernel launchers, one per precision translation unit.  Each returns the
+// launch's cudaError_t (cudaErrorNotSupported for an absent combination).
+cudaError_t launch_step_fp64(int integ, int coll, int field, bool mag, const StepParams& p,
+                             dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t launch_step_mixed(int integ, int coll, int field, bool mag, const StepParams& p,
+                              dim3 grid, dim3 block, cudaStream_t s);
+cudaError_t launch_step_hilo(int integ, int coll, int field, bool mag, const StepParams& p,
+                             dim3 grid, dim3 block, cudaStream_t s);
+
+}  // namespace icb

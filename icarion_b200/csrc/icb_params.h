@@ -1,0 +1,78 @@
+// icb_params.h — plain structs shared by the host library and the kernels.
+//
+// Per-ensemble constants travel in the kernel's parameter block (a constant
+// bank on the device, up to 32 KB), so every launch sees its ensembles'
+// field, geometry and gas constants in constant memory without a
+// per-handle __constant__ symbol (several handles may coexist in one process).
+#pragma once
+#include <cstdint>
+
+namespace icb {
+
+constexpr int kMaxLaunchEns = 64;   // ensembles per launch chunk (param space bound)
+
+enum FieldKind : int { kFieldUniform = 0, kFieldLinear = 1, kFieldLinearRF = 2 };
+enum CollKind : int { kCollNone = 0, kCollHSS = 1 };
+enum PrecKind : int { kPrecFP64 = 0, kPrecMixed = 1, kPrecHiLo = 2 };
+enum IntegKind : int { kBoris = 0, kRK4 = 1 };
+
+// Counter slots (uint64 each) accumulated by the stepping kernels.
+enum CounterSlot : int {
+    kCntCandidates = 0, kCntCollisions = 1, kCntOverflow = 2, kCntDeaths = 3, kCntArrivals = 4, kNumCounters = 8
+};
+
+// Flags byte per ion.
+constexpr uint8_t kFlagActive = 1u;
+constexpr uint8_t kFlagBorn = 2u;
+
+struct EnsConst {
+    // Electric field E = E0 + G .* (x - c); with rf: E_x, E_y from the
+    // quadrupole term -2 x U(t)/r0^2, 2 y U(t)/r0^2, U = U0 + V cos(w t).
+    double E0[3];
+    double G[3];
+    double c[3];
+    double rf_U0, rf_V, rf_omega, r0sq;
+    double B[3];
+    // Cylinder (no rotation): local = x - origin; inside iff
+    // -eps <= lz < L + eps and lx^2 + ly^2 <= (R + eps)^2.
+    double ox, oy, oz, zmax_local, rmax2;
+    double dt;
+    // Gas: A = n sigma dt, mean thermal speed <|th|> = sigma_n 2 sqrt(2/pi).
+    double A, mean_th, sig_n;
+    double ug[3];
+    double m_gas;
+    double zdet;
+    int32_t magnetic;
+    int32_t rf;
+};
+
+struct StepParams {
+    // FP64 / mixed positions
+    double* x; double* y; double* z;
+    // hi/lo positions (mixed hi/lo mode)
+    float* xh; float* xl; float* yh; float* yl; float* zh; float* zl;
+    // velocities (double in FP64 mode, float otherwise)
+    void* vx; void* vy; void* vz;
+    // null-collision clock: survival S and threshold U (same type as v)
+    void* clkS; void* clkU;
+    const double* mass;
+    const double* charge;
+    uint8_t* flags;
+    double* t_death;
+    double* t_arr;
+    const double* birth;               // nullable
+    unsigned long long* counters;      // kNumCounters
+    const unsigned long long* step_dev;// engine step index at launch start
+    const double* t_dev;               // engine time per ensemble at launch start
+    uint64_t first_id;
+    uint64_t seed;
+    uint32_t n_steps;
+    uint32_t pend_threshold;
+    uint32_t ens_base;                 // global index of this chunk's ensemble 0
+    uint32_t n_ens;
+    uint32_t do_push, do_collide, do_finalize, pad;
+    uint64_t ens_off[kMaxLaunchEns + 1];  // absolute ion offsets of the chunk's ensembles
+    EnsConst ens[kMaxLaunchEns];
+};
+
+}  // namespace icb

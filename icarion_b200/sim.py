@@ -1,0 +1,223 @@
+"""Host mirror of the reference's batch-step plug points over the C ABI.
+
+``Simulation`` owns one ``icb_handle``: the device-resident ion SoA plus the
+per-ensemble constants.  It exposes the reference's call pattern:
+
+* ``step_batch(t, dt)``  -> IIntegrationStrategy::step_batch (push only)
+* ``handle_batch(dt)``   -> ICollisionHandler::handle_batch (collisions only)
+* ``finalize()``         -> SimulationEngine::finalize_ions_after_integration
+* ``advance(n)``         -> n fused engine steps (SimulationEngine::process_timestep)
+
+and ``run(n_steps, write_interval)`` for the engine's snapshot loop.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi as capi
+from . import config as cfgmod
+
+
+@dataclass
+class IonState:
+    """IonEnsemble hot/cold SoA arrays (IonEnsemble.h:267-330) on the host."""
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    vx: np.ndarray
+    vy: np.ndarray
+    vz: np.ndarray
+    mass: np.ndarray
+    charge: np.ndarray
+    active: np.ndarray
+    birth: np.ndarray | None = None
+    t_death: np.ndarray | None = None
+    t_arrival: np.ndarray | None = None
+
+    @property
+    def n(self) -> int:
+        return int(self.x.shape[0])
+
+    def copy(self) -> "IonState":
+        return IonState(**{k: (None if v is None else np.array(v, copy=True)) for k, v in self.__dict__.items()})
+
+    @staticmethod
+    def empty(n: int) -> "IonState":
+        z = lambda: np.zeros(n, dtype=np.float64)  # noqa: E731
+        return IonState(z(), z(), z(), z(), z(), z(), z(), z(), np.ones(n, dtype=np.uint8),
+                        None, np.full(n, -1.0), np.full(n, -1.0))
+
+    @staticmethod
+    def concat(states: list["IonState"]) -> "IonState":
+        out = {}
+        for k in ("x", "y", "z", "vx", "vy", "vz", "mass", "charge", "active"):
+            out[k] = np.ascontiguousarray(np.concatenate([getattr(s, k) for s in states]))
+        n = sum(s.n for s in states)
+        out["t_death"] = np.full(n, -1.0)
+        out["t_arrival"] = np.full(n, -1.0)
+        return IonState(**out)
+
+
+def generate_ions(rng_seed: int, specs: list[capi.SpeciesSpec]) -> IonState:
+    """Initial cloud with the reference IonLoader semantics (host C++)."""
+    n = sum(int(s.count) for s in specs)
+    st = IonState.empty(n)
+    arr = (capi.SpeciesSpec * len(specs))(*specs)
+    capi.check(capi.lib().icb_generate_ions(
+        C.c_uint32(rng_seed & 0xFFFFFFFF), len(specs), arr,
+        capi.dptr(st.x), capi.dptr(st.y), capi.dptr(st.z), capi.dptr(st.vx), capi.dptr(st.vy), capi.dptr(st.vz),
+        capi.dptr(st.mass), capi.dptr(st.charge)))
+    return st
+
+
+def device_count() -> int:
+    c = C.c_int(0)
+    rc = capi.lib().icb_device_count(C.byref(c))
+    return c.value if rc == 0 else 0
+
+
+class Simulation:
+    """One device-resident population of ions in one or more ensembles."""
+
+    def __init__(self, ensembles: list[dict], precision: int = capi.PREC_MIXED,
+                 integrator: int = capi.INTEGRATOR_BORIS, collision: int = capi.COLLISION_HSS,
+                 rng_seed: int = 123, device: int = 0, block_size: int = 0, steps_per_launch: int = 0,
+                 pending_threshold: int = 0, use_graphs: int = 0):
+        self._lib = capi.lib()
+        self.n_ens = len(ensembles)
+        self._ens = (capi.EnsembleParams * self.n_ens)(*[cfgmod.to_struct(e) for e in ensembles])
+        cfg = capi.Config()
+        cfg.precision = precision
+        cfg.integrator = integrator
+        cfg.collision_model = collision
+        cfg.n_ensembles = self.n_ens
+        cfg.ensembles = C.cast(self._ens, C.POINTER(capi.EnsembleParams))
+        cfg.rng_seed = rng_seed
+        cfg.device = device
+        cfg.block_size = block_size
+        cfg.steps_per_launch = steps_per_launch
+        cfg.pending_threshold = pending_threshold
+        cfg.use_graphs = use_graphs
+        self._h = C.c_void_p()
+        capi.check(self._lib.icb_create(C.byref(cfg), C.byref(self._h)))
+        self.ensembles = ensembles
+        self.precision = precision
+        self.n = 0
+
+    # -- lifetime ------------------------------------------------------------
+    def close(self) -> None:
+        if self._h:
+            self._lib.icb_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state ---------------------------------------------------------------
+    def upload(self, st: IonState, ens_offsets: np.ndarray | None = None, first_id: int = 0) -> None:
+        off = None if ens_offsets is None else np.ascontiguousarray(ens_offsets, dtype=np.uint64)
+        capi.check(self._lib.icb_upload_ions(
+            self._h, st.n, capi.dptr(st.x), capi.dptr(st.y), capi.dptr(st.z),
+            capi.dptr(st.vx), capi.dptr(st.vy), capi.dptr(st.vz), capi.dptr(st.mass), capi.dptr(st.charge),
+            capi.u8ptr(st.active), capi.dptr(st.birth), capi.u64ptr(off), first_id))
+        self.n = st.n
+
+    def update_state(self, st: IonState) -> None:
+        capi.check(self._lib.icb_update_state(
+            self._h, capi.dptr(st.x), capi.dptr(st.y), capi.dptr(st.z),
+            capi.dptr(st.vx), capi.dptr(st.vy), capi.dptr(st.vz), capi.u8ptr(st.active)))
+
+    def download(self, into: IonState | None = None) -> IonState:
+        st = into if into is not None else IonState.empty(self.n)
+        if st.t_death is None:
+            st.t_death = np.full(self.n, -1.0)
+        if st.t_arrival is None:
+            st.t_arrival = np.full(self.n, -1.0)
+        capi.check(self._lib.icb_download_ions(
+            self._h, capi.dptr(st.x), capi.dptr(st.y), capi.dptr(st.z),
+            capi.dptr(st.vx), capi.dptr(st.vy), capi.dptr(st.vz), capi.u8ptr(st.active),
+            capi.dptr(st.t_death), capi.dptr(st.t_arrival)))
+        return st
+
+    # -- stepping -------------------------------------------------------------
+    def advance(self, n_steps: int) -> dict:
+        rs = capi.RunStats()
+        capi.check(self._lib.icb_advance(self._h, int(n_steps), C.byref(rs)))
+        return rs.as_dict()
+
+    def advance_async(self, n_steps: int) -> None:
+        capi.check(self._lib.icb_advance(self._h, int(n_steps), None))
+
+    def step_batch(self) -> bool:
+        """IIntegrationStrategy::step_batch: push every active ion once."""
+        capi.check(self._lib.icb_push(self._h))
+        return True
+
+    def handle_batch(self) -> dict:
+        """ICollisionHandler::handle_batch: one collision test per active ion."""
+        rs = capi.RunStats()
+        capi.check(self._lib.icb_collide(self._h, C.byref(rs)))
+        return rs.as_dict()
+
+    def finalize(self) -> dict:
+        rs = capi.RunStats()
+        capi.check(self._lib.icb_finalize(self._h, C.byref(rs)))
+        return rs.as_dict()
+
+    def synchronize(self) -> None:
+        capi.check(self._lib.icb_synchronize(self._h))
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        capi.check(self._lib.icb_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def clock(self) -> tuple[int, np.ndarray]:
+        st = C.c_uint64(0)
+        t = np.zeros(self.n_ens)
+        capi.check(self._lib.icb_get_clock(self._h, C.byref(st), capi.dptr(t)))
+        return st.value, t
+
+    def set_clock(self, step: int, t: np.ndarray) -> None:
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        capi.check(self._lib.icb_set_clock(self._h, int(step), capi.dptr(t)))
+
+    def moments(self) -> np.ndarray:
+        out = np.zeros((self.n_ens, capi.N_MOMENTS))
+        capi.check(self._lib.icb_moments(self._h, capi.dptr(out)))
+        return out
+
+    def mark_reference(self) -> None:
+        capi.check(self._lib.icb_mark_reference(self._h))
+
+    def run(self, n_steps: int, write_interval: int, ref_step: int = 0) -> tuple[np.ndarray, np.ndarray, dict]:
+        """Advance n_steps, taking moments every write_interval steps (the
+        engine's snapshot cadence).  Displacement moments are relative to the
+        positions after ref_step steps (a multiple of write_interval).
+        Returns (snapshot step indices, moments [snap, ens, 20], totals)."""
+        if ref_step % write_interval:
+            raise ValueError("ref_step must be a multiple of write_interval")
+        steps, moms = [], []
+        tot = {"candidates": 0, "collisions": 0, "rate_overflows": 0, "deaths": 0, "arrivals": 0, "device_ms": 0.0}
+        done = 0
+        while done < n_steps:
+            k = min(write_interval, n_steps - done)
+            rs = self.advance(k)
+            for key in tot:
+                tot[key] += rs[key]
+            done += k
+            if done == ref_step:
+                self.mark_reference()
+            steps.append(done)
+            moms.append(self.moments())
+        return np.asarray(steps), np.stack(moms), tot

@@ -1,0 +1,232 @@
+/*
+ * icarion_b200.h — C ABI of the B200-native ICARION uniform-dt batch step.
+ *
+ * One handle owns one device-resident ion population (SoA in HBM) and the
+ * per-ensemble constants of the physics (domain, fields, gas, time step).
+ * Every entry point returns an int status (ICB_OK == 0); nothing throws
+ * across the ABI.  On failure icb_last_error() gives a readable message.
+ * Handles are not thread-safe: one host thread drives one handle, as one
+ * SimulationEngine drives one IIntegrationStrategy / ICollisionHandler.
+ *
+ * Interfaces replaced (reference paths are relative to the ICARION tree):
+ *   IIntegrationStrategy::step_batch
+ *       src/core/integrator/strategies/IIntegrationStrategy.h:119-132
+ *       -> icb_upload_ions + icb_advance(push only / fused) + icb_download_ions
+ *   ICollisionHandler::handle_batch
+ *       src/core/physics/collisions/ICollisionHandler.h:121-134
+ *       -> icb_collide (unfused) or folded into icb_advance (fused)
+ *   SimulationEngine::process_timestep's per-step order
+ *       src/core/integrator/SimulationEngine.cpp:374-428
+ *       -> icb_advance(n_steps): push -> collide -> finalize -> t += dt, n times
+ */
+#ifndef ICARION_B200_H
+#define ICARION_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ICB_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    ICB_OK = 0,
+    ICB_ERR_INVALID_ARGUMENT = 1,
+    ICB_ERR_CUDA = 2,
+    ICB_ERR_OUT_OF_MEMORY = 3,
+    ICB_ERR_UNSUPPORTED = 4,
+    ICB_ERR_STATE = 5,
+    ICB_ERR_NO_DEVICE = 6,
+    ICB_ERR_TIMEOUT = 7
+};
+
+/* ---- enums ------------------------------------------------------------- */
+enum { ICB_PREC_FP64 = 0, ICB_PREC_MIXED = 1, ICB_PREC_MIXED_HILO = 2 };
+enum { ICB_INTEGRATOR_BORIS = 0, ICB_INTEGRATOR_RK4 = 1 };
+enum {
+    ICB_COLLISION_NONE = 0,
+    ICB_COLLISION_HSS = 1,
+    ICB_COLLISION_IPM_TABLE = 2,
+    ICB_COLLISION_IPM_MLP = 3,
+    ICB_COLLISION_LANGEVIN = 4
+};
+enum {
+    ICB_INSTRUMENT_IMS = 0,          /* AnalyticalFieldModel.cpp:136-161 */
+    ICB_INSTRUMENT_FTICR = 1,        /* AnalyticalFieldModel.cpp:174-186 */
+    ICB_INSTRUMENT_QUADRUPOLE_RF = 2 /* AnalyticalFieldModel.cpp:219-248 */
+};
+
+/* Number of doubles per ensemble returned by icb_moments:
+ *  0 n_active  1 sum x   2 sum y   3 sum z   4 sum x^2  5 sum y^2  6 sum z^2
+ *  7 sum vx    8 sum vy  9 sum vz  10 sum |v|^2  11 n_arrived  12 n_dead
+ *  13 sum z*vz
+ *  14..16 sum of displacement (x - x_ref) per axis, 17..19 sum of its square,
+ *  where x_ref is the position at upload or at the last icb_mark_reference.
+ *  Drift and diffusion are fitted from the displacement moments, which do
+ *  not carry the initial cloud's spread.                                   */
+#define ICB_N_MOMENTS 20
+
+/* One ensemble = one domain + environment + ion species + dt.  The fields
+ * follow DomainConfig / EnvironmentConfig of the reference; derived values
+ * (gas density, axial_V from E/N) are computed by the caller exactly as the
+ * reference loader does (DomainConfigLoader.cpp:410-440,
+ * EnvironmentConfig.h:152). */
+typedef struct icb_ensemble_params {
+    int32_t instrument;        /* ICB_INSTRUMENT_* */
+    int32_t magnetic_enabled;  /* fields.magnetic.enabled */
+    double origin_m[3];        /* geometry.origin_m (no rotation) */
+    double length_m;           /* geometry.length_m */
+    double radius_m;           /* geometry.radius_m */
+    double axial_V;            /* fields.DC.axial_V */
+    double radial_V;           /* fields.DC.radial_V (FTICR trap) */
+    double dc_quad_V;          /* fields.DC.quad_V */
+    double rf_voltage_V;       /* fields.RF.voltage_V */
+    double rf_frequency_Hz;    /* fields.RF.frequency_Hz */
+    double B_T[3];             /* fields.magnetic.field_strength_T */
+    double temperature_K;      /* env.temperature_K */
+    double gas_density_m3;     /* env.particle_density_m_3 = P/(kB T) */
+    double gas_mass_kg;        /* env.gas_mass_kg */
+    double gas_velocity_m_s[3];/* env.gas_velocity_m_s (constant flow) */
+    double gas_polarizability_m3; /* Langevin capture (alpha') */
+    double sigma_m2;           /* HSS cross-section of this ensemble's ions */
+    double ipm_bmax_m;         /* IPM: event cross-section pi*b_max^2 */
+    double dt_s;               /* uniform time step of this ensemble */
+    double detector_z_m;       /* arrival plane (first crossing, global z) */
+} icb_ensemble_params;
+
+typedef struct icb_config {
+    int32_t precision;         /* ICB_PREC_* */
+    int32_t integrator;        /* ICB_INTEGRATOR_* */
+    int32_t collision_model;   /* ICB_COLLISION_* */
+    int32_t n_ensembles;       /* 1 .. ICB_MAX_ENSEMBLES */
+    const icb_ensemble_params* ensembles; /* copied at icb_create */
+    uint64_t rng_seed;         /* simulation.rng_seed */
+    int32_t device;            /* CUDA device ordinal */
+    int32_t block_size;        /* threads per block, 0 = tuned default */
+    int32_t steps_per_launch;  /* steps fused per kernel launch, 0 = default */
+    int32_t pending_threshold; /* deferred-collision batch size per warp, 0 = default */
+    int32_t use_graphs;        /* capture launch sequences in CUDA graphs */
+    int32_t reserved[7];
+} icb_config;
+
+#define ICB_MAX_ENSEMBLES 256
+
+typedef struct icb_run_stats {
+    uint64_t steps;            /* time steps advanced by the call */
+    uint64_t candidates;       /* null-collision candidates tested */
+    uint64_t collisions;       /* accepted collisions */
+    uint64_t rate_overflows;   /* steps whose candidate probability was clamped to 1 */
+    uint64_t deaths;           /* ions deactivated (domain exit or non-finite state) */
+    uint64_t arrivals;         /* first detector-plane crossings */
+    double device_ms;          /* device time of the call (CUDA events) */
+    double step_kernel_ms;     /* device time inside the fused step kernel launches */
+    uint64_t kernel_launches;  /* kernels this call launched */
+} icb_run_stats;
+
+/* ---- ion cloud generation (IonLoader semantics) ------------------------ */
+enum {
+    ICB_POS_POINT = 0, ICB_POS_GAUSSIAN = 1, ICB_POS_UNIFORM_SPHERE = 2,
+    ICB_POS_UNIFORM_CYLINDER = 3, ICB_POS_UNIFORM_BOX = 4
+};
+enum { ICB_VEL_FIXED = 0, ICB_VEL_THERMAL = 1 };
+
+typedef struct icb_species_spec {
+    uint64_t count;
+    double mass_kg;
+    double charge_C;
+    int32_t position_type;     /* ICB_POS_* (PositionDistribution) */
+    int32_t velocity_type;     /* ICB_VEL_* (VelocityDistribution) */
+    double center_m[3];
+    double std_m[3];           /* gaussian */
+    double radius_m;           /* uniform_sphere / uniform_cylinder */
+    double length_m;           /* uniform_cylinder */
+    double box_min_m[3];
+    double box_max_m[3];
+    double velocity_m_s[3];    /* fixed */
+    double temperature_K;      /* thermal */
+} icb_species_spec;
+
+/* Generate the initial ion cloud of all species in order from one
+ * std::mt19937(rng_seed), as IonLoader::generate_species does
+ * (IonLoader.cpp:183-238, sample_position/sample_velocity :246-313).
+ * Output arrays hold sum(count) entries. */
+int icb_generate_ions(uint32_t rng_seed, int32_t n_species, const icb_species_spec* specs,
+                      double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                      double* mass_kg, double* charge_C);
+
+/* ---- library ----------------------------------------------------------- */
+int icb_abi_version(void);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* icb_last_error(void);
+int icb_device_count(int* count);
+
+/* ---- handle lifetime --------------------------------------------------- */
+int icb_create(const icb_config* cfg, struct icb_handle** out);
+int icb_destroy(struct icb_handle* h);
+/* Launch on this stream (a cudaStream_t); NULL = the handle's own stream. */
+int icb_set_stream(struct icb_handle* h, void* cuda_stream);
+int icb_synchronize(struct icb_handle* h);
+
+/* ---- ion state (IonEnsemble SoA, IonEnsemble.h:267-330) ----------------
+ * Ions must be grouped by ensemble: ions [ens_offsets[e], ens_offsets[e+1])
+ * belong to ensemble e.  ens_offsets may be NULL when n_ensembles == 1.
+ * birth_time_s may be NULL (all born at t = 0).  Ion ids (the Philox key
+ * component) are first_ion_id + index. */
+int icb_upload_ions(struct icb_handle* h, uint64_t n,
+                    const double* x, const double* y, const double* z,
+                    const double* vx, const double* vy, const double* vz,
+                    const double* mass_kg, const double* charge_C,
+                    const uint8_t* active, const double* birth_time_s,
+                    const uint64_t* ens_offsets, uint64_t first_ion_id);
+/* Copy positions/velocities back; every pointer may be NULL.  death and
+ * arrival times are -1 where the event has not happened. */
+int icb_download_ions(struct icb_handle* h,
+                      double* x, double* y, double* z,
+                      double* vx, double* vy, double* vz,
+                      uint8_t* active, double* death_time_s,
+                      double* arrival_time_s);
+/* Overwrite positions/velocities only (engine-side edits between steps);
+ * collision clocks, ids and flags stay. */
+int icb_update_state(struct icb_handle* h,
+                     const double* x, const double* y, const double* z,
+                     const double* vx, const double* vy, const double* vz,
+                     const uint8_t* active);
+uint64_t icb_ion_count(struct icb_handle* h);
+
+/* ---- stepping ---------------------------------------------------------- */
+/* Fused uniform-dt batch step, n_steps times: push (Boris/RK4) -> collision
+ * -> domain/NaN finalize -> t += dt (SimulationEngine.cpp:374-428). */
+int icb_advance(struct icb_handle* h, uint64_t n_steps, icb_run_stats* stats);
+/* Unfused parts of one step, for the per-step plug points:
+ * icb_push   = IIntegrationStrategy::step_batch (push only, no finalize)
+ * icb_collide = ICollisionHandler::handle_batch (collision only)
+ * icb_finalize = SimulationEngine::finalize_ions_after_integration + t += dt */
+int icb_push(struct icb_handle* h);
+int icb_collide(struct icb_handle* h, icb_run_stats* stats);
+int icb_finalize(struct icb_handle* h, icb_run_stats* stats);
+/* Engine clock: step index and time of ensemble 0 (all ensembles share the
+ * step index; time_s[e] = accumulated dt of ensemble e). */
+int icb_get_clock(struct icb_handle* h, uint64_t* step, double* time_s);
+int icb_set_clock(struct icb_handle* h, uint64_t step, const double* time_s);
+/* Per-ensemble moments of the active ions (ICB_N_MOMENTS doubles each). */
+int icb_moments(struct icb_handle* h, double* out);
+/* Store every ion's current position as its displacement reference. */
+int icb_mark_reference(struct icb_handle* h);
+
+/* ---- counter-based RNG check ------------------------------------------ */
+/* Evaluate the device Philox4x32-10 (use_curand = 0) or cuRAND's
+ * curand_Philox4x32_10 (use_curand = 1) on n host counters (4 words each)
+ * under key (lo32(seed), hi32(seed)) on `device`; results to out (4n).
+ * Replaces nothing in the reference: it pins the stateless RNG that stands
+ * in for PhysicsRng (CollisionTypes.h:31-49). */
+int icb_philox_eval(int device, uint64_t n, const uint32_t* counters, uint64_t seed,
+                    int use_curand, uint32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ICARION_B200_H */

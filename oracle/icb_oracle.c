@@ -1,0 +1,522 @@
+/*
+ * ORACLE — test infrastructure only.  Nothing in the icarion_b200 product
+ * links, loads or calls this file; only tests/, __graft_entry__.smoke() and
+ * bench.py's cpu_baseline leg use it, as the checker.
+ *
+ * CPU restatement (plain C, IEEE double, no FP contraction) of ICARION's
+ * uniform-dt batch step, written from the reference's behaviour:
+ *
+ *   - engine order per step: domain check of unborn/outside ions, push,
+ *     collision, finalize (domain exit -> inactive + death time, NaN ->
+ *     inactive), t += dt          SimulationEngine.cpp:374-428,
+ *                                 SimulationEngineLifecycle.cpp:72-195
+ *   - Boris push with x += v_plus*dt     BorisStrategy.cpp:18-98
+ *   - RK4 batch                          RK4Strategy.cpp:181-361
+ *   - analytic E of IMS / FTICR / QuadrupoleRF
+ *                                        AnalyticalFieldModel.cpp:136-248
+ *   - magnetic force for RK4             MagneticFieldForce.cpp:61-118
+ *   - cylinder containment (eps 1e-12)   CylindricalGeometry.h:35-40
+ *   - reference HSS: full Maxwell-Boltzmann neutral every step, P=1-exp,
+ *     isotropic COM scatter              HSSCollisionHandler.cpp:257-376,
+ *                                        VelocitySampling.cpp:9-66,
+ *                                        CollisionKernels.cpp:139-169,383-397
+ *   - per-ion std::mt19937_64 seeded rng_seed + ion index, uniform01 via
+ *     libstdc++ generate_canonical<double,53>
+ *                                        CollisionTypes.h:31-49, RngUtils.cpp:51-53
+ *   - the product's null-collision HSS (same per-step collision law in
+ *     distribution) with Philox4x32-10 keyed on (seed, ion id, step), FP64,
+ *     so GPU FP64 trajectories can be compared ion by ion.
+ *
+ * Pinned against golden vectors produced by the reference's own code
+ * (oracle/ref_harness.cpp compiled from the reference sources), see
+ * tests/golden/make_golden.py.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+#define ORC_N_MOMENTS 20
+#define ORC_KB 1.380649e-23          /* utils/constants.h:15 */
+#define ORC_GEOM_EPS 1e-12           /* CylindricalGeometry.h:245 */
+#define ORC_MIN_REL_VEL 1e-10        /* HSSCollisionHandler.cpp:20 */
+#define ORC_MIN_VEL_MAG 1e-12        /* CollisionKernels.h:172 */
+#define ORC_MIN_VOLTAGE 1e-12        /* threshold on |rf voltage| (AnalyticalFieldModel) */
+
+/* Same layout as icb_ensemble_params (include/icarion_b200.h): the oracle
+ * defines its own copy so it does not depend on the product headers. */
+typedef struct orc_domain {
+    int32_t instrument;
+    int32_t magnetic_enabled;
+    double origin_m[3];
+    double length_m;
+    double radius_m;
+    double axial_V;
+    double radial_V;
+    double dc_quad_V;
+    double rf_voltage_V;
+    double rf_frequency_Hz;
+    double B_T[3];
+    double temperature_K;
+    double gas_density_m3;
+    double gas_mass_kg;
+    double gas_velocity_m_s[3];
+    double gas_polarizability_m3;
+    double sigma_m2;
+    double ipm_bmax_m;
+    double dt_s;
+    double detector_z_m;
+} orc_domain;
+
+/* ======================================================================
+ * mt19937_64 (Matsumoto & Nishimura, ACM TOMACS 2000; 64-bit variant of
+ * Nishimura 2000), restated from the published algorithm.
+ * ==================================================================== */
+typedef struct { uint64_t mt[312]; int mti; } orc_mt64;
+
+static void mt64_seed(orc_mt64* s, uint64_t seed) {
+    s->mt[0] = seed;
+    for (int i = 1; i < 312; ++i)
+        s->mt[i] = 6364136223846793005ULL * (s->mt[i - 1] ^ (s->mt[i - 1] >> 62)) + (uint64_t)i;
+    s->mti = 312;
+}
+
+static uint64_t mt64_next(orc_mt64* s) {
+    const uint64_t UM = 0xFFFFFFFF80000000ULL, LM = 0x7FFFFFFFULL;
+    const uint64_t MATRIX_A = 0xB5026F5AA96619E9ULL;
+    if (s->mti >= 312) {
+        int i;
+        for (i = 0; i < 312 - 156; ++i) {
+            uint64_t x = (s->mt[i] & UM) | (s->mt[i + 1] & LM);
+            s->mt[i] = s->mt[i + 156] ^ (x >> 1) ^ ((x & 1ULL) ? MATRIX_A : 0ULL);
+        }
+        for (; i < 311; ++i) {
+            uint64_t x = (s->mt[i] & UM) | (s->mt[i + 1] & LM);
+            s->mt[i] = s->mt[i + (156 - 312)] ^ (x >> 1) ^ ((x & 1ULL) ? MATRIX_A : 0ULL);
+        }
+        uint64_t x = (s->mt[311] & UM) | (s->mt[0] & LM);
+        s->mt[311] = s->mt[155] ^ (x >> 1) ^ ((x & 1ULL) ? MATRIX_A : 0ULL);
+        s->mti = 0;
+    }
+    uint64_t x = s->mt[s->mti++];
+    x ^= (x >> 29) & 0x5555555555555555ULL;
+    x ^= (x << 17) & 0x71D67FFFEDA60000ULL;
+    x ^= (x << 37) & 0xFFF7EEE000000000ULL;
+    x ^= (x >> 43);
+    return x;
+}
+
+/* uniform_real_distribution<double>(0,1) over a 64-bit engine: one draw,
+ * value / 2^64, clamped below 1 (generate_canonical<double, 53>). */
+static double mt64_uniform01(orc_mt64* s) {
+    double r = (double)mt64_next(s) / 18446744073709551616.0;
+    if (r >= 1.0) r = nextafter(1.0, 0.0);
+    return r;
+}
+
+void orc_mt64_uniforms(uint64_t seed, int64_t n, double* out) {
+    orc_mt64 s;
+    mt64_seed(&s, seed);
+    for (int64_t i = 0; i < n; ++i) out[i] = mt64_uniform01(&s);
+}
+
+/* ======================================================================
+ * Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel Random Numbers: As
+ * Easy as 1, 2, 3", SC'11), restated from the paper.
+ * ==================================================================== */
+static void philox4x32_10(const uint32_t c_in[4], const uint32_t k_in[2], uint32_t out[4]) {
+    uint32_t c0 = c_in[0], c1 = c_in[1], c2 = c_in[2], c3 = c_in[3];
+    uint32_t k0 = k_in[0], k1 = k_in[1];
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    philox4x32_10(ctr, key, out);
+}
+
+void orc_philox_many(int64_t n, const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+    for (int64_t i = 0; i < n; ++i) philox4x32_10(ctr + 4 * i, key, out + 4 * i);
+}
+
+/* 32-bit word -> double uniform on (0, 1]: (w + 1) * 2^-32 (exact). */
+static double u32_to_unit(uint32_t w) { return ((double)w + 1.0) * 2.3283064365386963e-10; }
+
+/* Philox stream layout of the product (icarion_b200/csrc/icb_rng.cuh):
+ * key = (lo32(seed), hi32(seed)), counter = (ion id, step, substream, 0). */
+static void draw4(uint64_t seed, uint32_t ion_id, uint32_t step, uint32_t sub, double u[4]) {
+    uint32_t c[4] = {ion_id, step, sub, 0u};
+    uint32_t k[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t o[4];
+    philox4x32_10(c, k, o);
+    for (int i = 0; i < 4; ++i) u[i] = u32_to_unit(o[i]);
+}
+
+void orc_unit_uniforms(uint64_t seed, uint32_t ion_id, uint32_t step, uint32_t sub, double* out4) {
+    draw4(seed, ion_id, step, sub, out4);
+}
+
+/* ======================================================================
+ * Fields and geometry
+ * ==================================================================== */
+static void field_E(const orc_domain* d, const double p[3], double t, double E[3]) {
+    E[0] = E[1] = E[2] = 0.0;
+    if (d->instrument == 0) {               /* IMS: AnalyticalFieldModel.cpp:136-161 */
+        E[2] = d->axial_V / d->length_m;
+        if (fabs(d->rf_voltage_V) > ORC_MIN_VOLTAGE) {
+            double r0_sq = d->radius_m * d->radius_m;
+            double omega = 2.0 * M_PI * d->rf_frequency_Hz;
+            double U = d->dc_quad_V + d->rf_voltage_V * cos(omega * t);
+            E[0] = -2.0 * p[0] * U / r0_sq;
+            E[1] = 2.0 * p[1] * U / r0_sq;
+        }
+    } else if (d->instrument == 1) {        /* FTICR: AnalyticalFieldModel.cpp:174-186 */
+        double L = d->length_m, r = d->radius_m;
+        double dd = sqrt((L * L / 8.0) + (r * r / 4.0));
+        double factor = d->radial_V / (dd * dd);
+        double zc = p[2] - 0.5 * L;
+        E[0] = factor * p[0];
+        E[1] = factor * p[1];
+        E[2] = -2.0 * factor * zc;
+    } else if (d->instrument == 2) {        /* QuadrupoleRF: AnalyticalFieldModel.cpp:219-248 */
+        if (fabs(d->rf_voltage_V) > ORC_MIN_VOLTAGE) {
+            double r0_sq = d->radius_m * d->radius_m;
+            double omega = 2.0 * M_PI * d->rf_frequency_Hz;
+            double U = d->dc_quad_V + d->rf_voltage_V * cos(omega * t);
+            E[0] = -2.0 * p[0] * U / r0_sq;
+            E[1] = 2.0 * p[1] * U / r0_sq;
+        }
+        if (fabs(d->axial_V) > ORC_MIN_VOLTAGE) E[2] = d->axial_V / d->length_m;
+    }
+}
+
+void orc_field(const orc_domain* d, const double p[3], double t, double E[3]) { field_E(d, p, t, E); }
+
+static int contains(const orc_domain* d, const double p[3]) {
+    double lx = p[0] - d->origin_m[0], ly = p[1] - d->origin_m[1], lz = p[2] - d->origin_m[2];
+    if (lz < -ORC_GEOM_EPS || lz >= d->length_m + ORC_GEOM_EPS) return 0;
+    double r2 = lx * lx + ly * ly;
+    return r2 <= (d->radius_m + ORC_GEOM_EPS) * (d->radius_m + ORC_GEOM_EPS);
+}
+
+/* ======================================================================
+ * Pushers
+ * ==================================================================== */
+static void boris_step(const orc_domain* d, double x[3], double v[3], double m, double q,
+                       double t, double dt) {
+    double E[3];
+    field_E(d, x, t, E);
+    double F[3] = {E[0] * q, E[1] * q, E[2] * q};          /* ElectricFieldForce: E * q */
+    double a[3] = {F[0] / m, F[1] / m, F[2] / m};          /* F / mass */
+    double B[3] = {0.0, 0.0, 0.0};
+    if (d->magnetic_enabled) { B[0] = d->B_T[0]; B[1] = d->B_T[1]; B[2] = d->B_T[2]; }
+    double qm = q / m;
+    double h = dt * 0.5;
+    double vm[3] = {v[0] + a[0] * h, v[1] + a[1] * h, v[2] + a[2] * h};
+    double ts = qm * dt * 0.5;
+    double tv[3] = {B[0] * ts, B[1] * ts, B[2] * ts};
+    double t2 = tv[0] * tv[0] + tv[1] * tv[1] + tv[2] * tv[2];
+    double sf = 2.0 / (1.0 + t2);
+    double sv[3] = {tv[0] * sf, tv[1] * sf, tv[2] * sf};
+    double c1[3] = {vm[1] * tv[2] - vm[2] * tv[1], vm[2] * tv[0] - vm[0] * tv[2], vm[0] * tv[1] - vm[1] * tv[0]};
+    double vp_[3] = {vm[0] + c1[0], vm[1] + c1[1], vm[2] + c1[2]};
+    double c2[3] = {vp_[1] * sv[2] - vp_[2] * sv[1], vp_[2] * sv[0] - vp_[0] * sv[2], vp_[0] * sv[1] - vp_[1] * sv[0]};
+    double vplus[3] = {vm[0] + c2[0], vm[1] + c2[1], vm[2] + c2[2]};
+    x[0] += vplus[0] * dt; x[1] += vplus[1] * dt; x[2] += vplus[2] * dt;
+    v[0] = vplus[0] + a[0] * h; v[1] = vplus[1] + a[1] * h; v[2] = vplus[2] + a[2] * h;
+}
+
+/* total force / m for RK4: E force, then magnetic force when enabled
+ * (PhysicsSetup.cpp:206 adds MagneticFieldForce for non-Boris integrators),
+ * times (1/mass) (RK4Strategy.cpp:242). */
+static void rk4_acc(const orc_domain* d, const double x[3], const double v[3], double m, double q,
+                    double t, double acc[3]) {
+    double E[3];
+    field_E(d, x, t, E);
+    double F[3] = {E[0] * q, E[1] * q, E[2] * q};
+    if (d->magnetic_enabled) {
+        const double* B = d->B_T;
+        double vxb[3] = {v[1] * B[2] - v[2] * B[1], v[2] * B[0] - v[0] * B[2], v[0] * B[1] - v[1] * B[0]};
+        double Fb[3] = {vxb[0] * q, vxb[1] * q, vxb[2] * q};
+        F[0] += Fb[0]; F[1] += Fb[1]; F[2] += Fb[2];
+    }
+    double im = 1.0 / m;
+    acc[0] = F[0] * im; acc[1] = F[1] * im; acc[2] = F[2] * im;
+}
+
+static void rk4_step(const orc_domain* d, double x[3], double v[3], double m, double q,
+                     double t, double dt) {
+    double h = dt * 0.5;
+    double bx[3] = {x[0], x[1], x[2]}, bv[3] = {v[0], v[1], v[2]};
+    double k1v[3] = {bv[0], bv[1], bv[2]}, k1a[3];
+    rk4_acc(d, bx, bv, m, q, t, k1a);
+    double p2[3], v2[3], k2a[3];
+    for (int i = 0; i < 3; ++i) { p2[i] = bx[i] + k1v[i] * h; v2[i] = bv[i] + k1a[i] * h; }
+    rk4_acc(d, p2, v2, m, q, t + h, k2a);
+    double p3[3], v3[3], k3a[3];
+    for (int i = 0; i < 3; ++i) { p3[i] = bx[i] + v2[i] * h; v3[i] = bv[i] + k2a[i] * h; }
+    rk4_acc(d, p3, v3, m, q, t + h, k3a);
+    double p4[3], v4[3], k4a[3];
+    for (int i = 0; i < 3; ++i) { p4[i] = bx[i] + v3[i] * dt; v4[i] = bv[i] + k3a[i] * dt; }
+    rk4_acc(d, p4, v4, m, q, t + dt, k4a);
+    double s = dt / 6.0;
+    for (int i = 0; i < 3; ++i) {
+        x[i] = bx[i] + (k1v[i] + v2[i] * 2.0 + v3[i] * 2.0 + v4[i]) * s;
+        v[i] = bv[i] + (k1a[i] + k2a[i] * 2.0 + k3a[i] * 2.0 + k4a[i]) * s;
+    }
+}
+
+/* ======================================================================
+ * Collisions
+ * ==================================================================== */
+/* Reference HSS, single gas (HSSCollisionHandler.cpp:257-376). */
+static int hss_reference(const orc_domain* d, double v[3], double mi, orc_mt64* rng) {
+    double sig_n = sqrt(ORC_KB * d->temperature_K / d->gas_mass_kg);
+    double vn[3];
+    for (int c = 0; c < 3; ++c) {
+        double u1 = mt64_uniform01(rng), u2 = mt64_uniform01(rng);
+        vn[c] = sig_n * sqrt(-2.0 * log(u1)) * cos(2.0 * M_PI * u2);
+    }
+    for (int c = 0; c < 3; ++c) vn[c] = vn[c] + d->gas_velocity_m_s[c];
+    double vr[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
+    double g = sqrt(vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]);
+    if (g < ORC_MIN_REL_VEL) return 0;
+    double P = 1.0 - exp(-d->gas_density_m3 * d->sigma_m2 * g * d->dt_s);
+    if (mt64_uniform01(rng) >= P) return 0;
+    /* CollisionKernels::hss_collision */
+    double mn = d->gas_mass_kg;
+    double vr2[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
+    double gm = sqrt(vr2[0] * vr2[0] + vr2[1] * vr2[1] + vr2[2] * vr2[2]);
+    if (gm <= ORC_MIN_VEL_MAG) {
+        double u1 = mt64_uniform01(rng), u2 = mt64_uniform01(rng);
+        (void)u1; (void)u2;
+        gm = ORC_MIN_VEL_MAG;
+    }
+    double u1 = mt64_uniform01(rng), u2 = mt64_uniform01(rng);
+    double ct = 2.0 * u1 - 1.0;
+    double st = sqrt(fmax(0.0, 1.0 - ct * ct));
+    double ph = 2.0 * M_PI * u2;
+    double dir[3] = {st * cos(ph), st * sin(ph), ct};
+    double mt = mi + mn, inv = 1.0 / mt;
+    double fac = mn * inv;
+    for (int c = 0; c < 3; ++c) {
+        double vcom = (v[c] * mi + vn[c] * mn) * inv;
+        v[c] = vcom + (dir[c] * gm) * fac;
+    }
+    return 1;
+}
+
+/* Null-collision HSS with Philox (the product's algorithm, FP64).
+ * Per step: Q = n*sigma*dt*(|v-u| + <|th|>), survival S *= (1-Q); a
+ * candidate fires when S < U.  The neutral's thermal part th is drawn from
+ * the mixture f(th)(|v-u| + |th|)/(|v-u| + <|th|>) and accepted with
+ * (1-exp(-n sigma g dt)) / (n sigma dt (|v-u|+|th|)) <= 1; the joint law of
+ * (collide, v_n) per step is then f(v_n)(1-exp(-n sigma g dt)), i.e. the
+ * reference's.  Return: 0 none, 1 candidate rejected, 2 collision. */
+static int hss_nullcoll(const orc_domain* d, double v[3], double mi, uint64_t seed, uint32_t id,
+                        uint32_t step, double* S, double* U, uint64_t* overflow) {
+    const double mn = d->gas_mass_kg;
+    const double sig_n = sqrt(ORC_KB * d->temperature_K / mn);
+    const double mean_th = sig_n * 1.5957691216057308;   /* E|th| = sigma*2*sqrt(2/pi) */
+    const double A = d->gas_density_m3 * d->sigma_m2 * d->dt_s;
+    const double* ug = d->gas_velocity_m_s;
+    double w[3] = {v[0] - ug[0], v[1] - ug[1], v[2] - ug[2]};
+    double gu = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    double Q = A * (gu + mean_th);
+    if (Q > 1.0) { Q = 1.0; ++*overflow; }
+    *S = *S - *S * Q;
+    if (!(*S < *U)) return 0;
+    double r0[4], r1[4], r2[4];
+    draw4(seed, id, step, 0u, r0);
+    draw4(seed, id, step, 1u, r1);
+    draw4(seed, id, step, 2u, r2);
+    *U = r0[0];
+    *S = 1.0;
+    double th[3];
+    if (r0[1] * (gu + mean_th) < gu) {
+        double ra = sqrt(-2.0 * log(r1[0]));
+        double pa = 2.0 * M_PI * r1[1];
+        double rb = sqrt(-2.0 * log(r1[2]));
+        double pb = 2.0 * M_PI * r1[3];
+        th[0] = sig_n * (ra * cos(pa));
+        th[1] = sig_n * (ra * sin(pa));
+        th[2] = sig_n * (rb * cos(pb));
+    } else {
+        double rad = sig_n * sqrt(-2.0 * log(r1[0] * r1[1]));
+        double ct = 2.0 * r1[2] - 1.0;
+        double st = sqrt(fmax(0.0, 1.0 - ct * ct));
+        double ph = 2.0 * M_PI * r1[3];
+        th[0] = rad * (st * cos(ph));
+        th[1] = rad * (st * sin(ph));
+        th[2] = rad * ct;
+    }
+    double thm = sqrt(th[0] * th[0] + th[1] * th[1] + th[2] * th[2]);
+    double vn[3] = {ug[0] + th[0], ug[1] + th[1], ug[2] + th[2]};
+    double gv[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
+    double g = sqrt(gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2]);
+    double q = A * (gu + thm);
+    double p = -expm1(-A * g);
+    if (!(r0[2] * q < p)) return 1;
+    double ct = 2.0 * r0[3] - 1.0;
+    double st = sqrt(fmax(0.0, 1.0 - ct * ct));
+    double ph = 2.0 * M_PI * r2[0];
+    double dir[3] = {st * cos(ph), st * sin(ph), ct};
+    double inv = 1.0 / (mi + mn);
+    double fac = mn * inv;
+    for (int c = 0; c < 3; ++c) {
+        double vcom = (v[c] * mi + vn[c] * mn) * inv;
+        v[c] = vcom + (dir[c] * g) * fac;
+    }
+    return 2;
+}
+
+void orc_clock_init(uint64_t seed, int64_t n, uint64_t first_id, double* S, double* U) {
+    for (int64_t i = 0; i < n; ++i) {
+        double r[4];
+        draw4(seed, (uint32_t)(first_id + (uint64_t)i), 0u, 3u, r);
+        S[i] = 1.0;
+        U[i] = r[0];
+    }
+}
+
+/* ======================================================================
+ * Engine loop (one domain)
+ * ==================================================================== */
+static void add_moments(double* m, const double x[3], const double v[3], const double r[3]) {
+    m[0] += 1.0;
+    m[1] += x[0]; m[2] += x[1]; m[3] += x[2];
+    m[4] += x[0] * x[0]; m[5] += x[1] * x[1]; m[6] += x[2] * x[2];
+    m[7] += v[0]; m[8] += v[1]; m[9] += v[2];
+    m[10] += v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    m[13] += x[2] * v[2];
+    for (int c = 0; c < 3; ++c) {
+        double d = x[c] - r[c];
+        m[14 + c] += d;
+        m[17 + c] += d * d;
+    }
+}
+
+/*
+ * Run n_steps engine steps for n ions of one domain.
+ *   integrator: 0 Boris, 1 RK4
+ *   collision:  0 none, 1 reference HSS (mt19937_64 seeded seed + id),
+ *               2 null-collision HSS (Philox; needs clk_S/clk_U)
+ *   step0/t0:   engine step index and time at entry
+ *   snap_every: moments of the active ions are accumulated after every
+ *               snap_every-th step into moments[(k/snap_every) * 14 + ...]
+ *               (slot 11 counts arrivals so far, slot 12 deaths so far)
+ *               (slots 14..19: displacement moments from the position after
+ *               ref_step steps; before that, from the entry position)
+ *   counters:   [candidates, collisions, rate_overflows] (nullable)
+ * Ions are independent without space charge, so the loop runs ion-major
+ * (parallel over ions with OpenMP when n_threads > 1).
+ */
+int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
+            int64_t n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+            const double* mass, const double* charge, uint8_t* active,
+            double* t_death, double* t_arr, double* clk_S, double* clk_U,
+            uint64_t first_id, uint64_t step0, double t0, int64_t n_steps,
+            int64_t snap_every, int64_t ref_step, double* moments, uint64_t* counters, int n_threads) {
+    if (collision == 2 && (!clk_S || !clk_U)) return 1;
+    const int64_t n_snap = (snap_every > 0) ? n_steps / snap_every : 0;
+    if (n_snap > 0 && moments) memset(moments, 0, sizeof(double) * (size_t)(n_snap * ORC_N_MOMENTS));
+    uint64_t cand_tot = 0, coll_tot = 0, ovf_tot = 0;
+    const double dt = d->dt_s;
+    const double zdet = d->detector_z_m;
+#ifdef _OPENMP
+    if (n_threads < 1) n_threads = 1;
+#else
+    (void)n_threads;
+#endif
+#pragma omp parallel num_threads(n_threads) reduction(+ : cand_tot, coll_tot, ovf_tot)
+    {
+        double* mom = NULL;
+        if (n_snap > 0 && moments) mom = (double*)calloc((size_t)(n_snap * ORC_N_MOMENTS), sizeof(double));
+        orc_mt64* rng = (collision == 1) ? (orc_mt64*)malloc(sizeof(orc_mt64)) : NULL;
+#pragma omp for schedule(static)
+        for (int64_t i = 0; i < n; ++i) {
+            double p[3] = {x[i], y[i], z[i]}, v[3] = {vx[i], vy[i], vz[i]};
+            double m = mass[i], q = charge[i];
+            uint8_t act = active[i];
+            double S = clk_S ? clk_S[i] : 1.0, U = clk_U ? clk_U[i] : 0.0;
+            uint32_t id = (uint32_t)(first_id + (uint64_t)i);
+            if (collision == 1) mt64_seed(rng, seed + first_id + (uint64_t)i);
+            double t = t0;
+            double ref[3] = {p[0], p[1], p[2]};
+            for (int64_t k = 0; k < n_steps; ++k) {
+                if (act) {
+                    if (!contains(d, p)) {            /* prepare_ions_for_integration */
+                        act = 0;
+                        t_death[i] = t;
+                    }
+                }
+                if (act) {
+                    double zold = p[2];
+                    if (integrator == 0) boris_step(d, p, v, m, q, t, dt);
+                    else rk4_step(d, p, v, m, q, t, dt);
+                    if (collision == 1) {
+                        coll_tot += (uint64_t)hss_reference(d, v, m, rng);
+                    } else if (collision == 2) {
+                        uint64_t ov = 0;
+                        int r = hss_nullcoll(d, v, m, seed, id, (uint32_t)(step0 + (uint64_t)k), &S, &U, &ov);
+                        ovf_tot += ov;
+                        if (r > 0) ++cand_tot;
+                        if (r == 2) ++coll_tot;
+                    }
+                    if (t_arr[i] < 0.0 && zold < zdet && p[2] >= zdet)
+                        t_arr[i] = t + dt * ((zdet - zold) / (p[2] - zold));
+                    if (!contains(d, p)) {
+                        act = 0;
+                        t_death[i] = t;
+                    } else if (!(isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]) &&
+                                 isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]))) {
+                        act = 0;
+                        t_death[i] = t;
+                    }
+                }
+                t = t + dt;
+                if (k + 1 == ref_step) { ref[0] = p[0]; ref[1] = p[1]; ref[2] = p[2]; }
+                if (mom && ((k + 1) % snap_every) == 0) {
+                    double* ms = mom + ((k + 1) / snap_every - 1) * ORC_N_MOMENTS;
+                    if (act) add_moments(ms, p, v, ref);
+                    if (t_arr[i] >= 0.0) ms[11] += 1.0;
+                    if (!act && t_death[i] >= 0.0) ms[12] += 1.0;
+                }
+            }
+            x[i] = p[0]; y[i] = p[1]; z[i] = p[2];
+            vx[i] = v[0]; vy[i] = v[1]; vz[i] = v[2];
+            active[i] = act;
+            if (clk_S) clk_S[i] = S;
+            if (clk_U) clk_U[i] = U;
+        }
+        if (mom) {
+#pragma omp critical
+            for (int64_t j = 0; j < n_snap * ORC_N_MOMENTS; ++j) moments[j] += mom[j];
+            free(mom);
+        }
+        free(rng);
+    }
+    if (counters) { counters[0] = cand_tot; counters[1] = coll_tot; counters[2] = ovf_tot; }
+    return 0;
+}
+
+/* Thermal width sqrt(kB T / m) (VelocitySampling.cpp:48-55). */
+double orc_thermal_width(double T, double m) { return sqrt(ORC_KB * T / m); }

@@ -1,0 +1,394 @@
+// ORACLE — test infrastructure only (never linked into the product).
+//
+// Drives the reference's own hot-path code, compiled from its sources by
+// oracle/Makefile, with the engine's per-step order restated here because
+// SimulationEngine itself needs HDF5/jsoncpp which this image lacks:
+//
+//   per step (SimulationEngine::process_timestep, SimulationEngine.cpp:374-428):
+//     prepare:   ion outside the domain -> inactive, death = t
+//                (SimulationEngineLifecycle.cpp:72-121)
+//     integrate: BorisStrategy::step per ion (SimulationEngineIntegration.cpp:114-146)
+//                or RK4Strategy::step_batch (uniform dt, :26-45)
+//     collide:   HSSCollisionHandler::handle_collision per ion with
+//                PhysicsRng(rng_seed + ion index) (RngUtils.cpp:51-53)
+//     finalize:  domain exit -> inactive, death = t; non-finite -> inactive
+//                (SimulationEngineLifecycle.cpp:123-195);  t += dt
+//   arrival time = first crossing of the detector plane, linearly
+//   interpolated within the step (analysis/ims_mobility.py:290-322 convention).
+//
+// Modes (key=value arguments):
+//   uniforms seed= n= out=             PhysicsRng(seed).uniform01() x n
+//   init     seed= n= sigma_pos= T= mass= charge= ccs= out=
+//            ion cloud as IonLoader::sample_position/sample_velocity
+//            (gaussian at the origin, thermal), std::mt19937(seed)
+//   derive   <domain keys>             print the loader-derived constants
+//   run      in= out= <domain keys> integrator= collision= steps= snap=
+//            ref_step= threads= seed= schedule=static|faithful mom=
+//            moments (20 per snapshot, layout of ICB_N_MOMENTS) of the
+//            active ions; slots 14..19 are displacement moments from the
+//            positions after ref_step steps.
+#include "core/integrator/strategies/BorisStrategy.h"
+#include "core/integrator/strategies/RK4Strategy.h"
+#include "core/physics/collisions/HSSCollisionHandler.h"
+#include "core/physics/forces/ElectricFieldForce.h"
+#include "core/physics/forces/MagneticFieldForce.h"
+#include "core/config/types/AnalyticalFieldModel.h"
+#include "core/config/types/CylindricalGeometry.h"
+#include "core/types/IonEnsemble.h"
+#include "core/types/CollisionTypes.h"
+#include "utils/constants.h"
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+using namespace ICARION;
+
+namespace {
+
+using Args = std::map<std::string, std::string>;
+
+double num(const Args& a, const char* k, double def) {
+    auto it = a.find(k);
+    return it == a.end() ? def : std::strtod(it->second.c_str(), nullptr);
+}
+std::string str(const Args& a, const char* k, const char* def) {
+    auto it = a.find(k);
+    return it == a.end() ? std::string(def) : it->second;
+}
+
+// Ion state file: int64 n, then 12 arrays of n doubles:
+// x y z vx vy vz mass charge ccs active t_death t_arrival
+struct State {
+    int64_t n = 0;
+    std::vector<double> a[12];
+};
+
+State read_state(const std::string& path) {
+    State s;
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw std::runtime_error("cannot open " + path);
+    if (std::fread(&s.n, sizeof(int64_t), 1, f) != 1) throw std::runtime_error("bad state file");
+    for (auto& v : s.a) {
+        v.resize(static_cast<size_t>(s.n));
+        if (std::fread(v.data(), sizeof(double), v.size(), f) != v.size()) throw std::runtime_error("short state file");
+    }
+    std::fclose(f);
+    return s;
+}
+
+void write_state(const std::string& path, const State& s) {
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot write " + path);
+    std::fwrite(&s.n, sizeof(int64_t), 1, f);
+    for (const auto& v : s.a) std::fwrite(v.data(), sizeof(double), v.size(), f);
+    std::fclose(f);
+}
+
+// Domain exactly as the loader builds it: E/N -> axial_V via N = P/(kB T)
+// (DomainConfigLoader.cpp:417-431), density and gas mass from
+// EnvironmentConfig::compute_derived_properties.
+config::DomainConfig make_domain(const Args& a) {
+    config::DomainConfig d;
+    const std::string inst = str(a, "instrument", "IMS");
+    if (inst == "IMS") d.instrument = config::Instrument::IMS;
+    else if (inst == "FTICR") d.instrument = config::Instrument::FTICR;
+    else if (inst == "QuadrupoleRF") d.instrument = config::Instrument::QuadrupoleRF;
+    else throw std::runtime_error("unsupported instrument " + inst);
+    d.geometry.origin_m = Vec3{num(a, "origin_x", 0.0), num(a, "origin_y", 0.0), num(a, "origin_z", 0.0)};
+    d.geometry.length_m = num(a, "length", 0.1);
+    d.geometry.radius_m = num(a, "radius", 0.05);
+    d.environment.temperature_K = num(a, "T", 300.0);
+    d.environment.pressure_Pa = num(a, "P", 1000.0);
+    d.environment.gas_species = str(a, "gas", "N2");
+    d.environment.compute_derived_properties();
+    if (a.count("EN_Td")) {
+        const double EN_Td = num(a, "EN_Td", 0.0);
+        const double k_B = 1.380649e-23;
+        const double N = d.environment.pressure_Pa / (k_B * d.environment.temperature_K);
+        const double E_Vm = EN_Td * 1e-21 * N;
+        d.fields.dc.axial_V.constant_value = E_Vm * d.geometry.length_m;
+    }
+    if (a.count("axial_V")) d.fields.dc.axial_V.constant_value = num(a, "axial_V", 0.0);
+    d.fields.dc.radial_V.constant_value = num(a, "radial_V", 0.0);
+    d.fields.dc.quad_V.constant_value = num(a, "dc_quad_V", 0.0);
+    d.fields.rf.voltage_V.constant_value = num(a, "rf_V", 0.0);
+    d.fields.rf.frequency_Hz.constant_value = num(a, "rf_f", 0.0);
+    d.fields.magnetic.enabled = num(a, "magnetic", 0.0) != 0.0;
+    d.fields.magnetic.field_strength_T = Vec3{num(a, "B_x", 0.0), num(a, "B_y", 0.0), num(a, "B_z", 0.0)};
+    return d;
+}
+
+int mode_uniforms(const Args& a) {
+    physics::PhysicsRng rng(static_cast<uint64_t>(std::strtoull(str(a, "seed", "123").c_str(), nullptr, 10)));
+    const int64_t n = static_cast<int64_t>(num(a, "n", 64));
+    std::vector<double> u(static_cast<size_t>(n));
+    for (auto& x : u) x = rng.uniform01();
+    FILE* f = std::fopen(str(a, "out", "uniforms.bin").c_str(), "wb");
+    std::fwrite(u.data(), sizeof(double), u.size(), f);
+    std::fclose(f);
+    return 0;
+}
+
+int mode_init(const Args& a) {
+    std::mt19937 rng(static_cast<uint32_t>(std::strtoul(str(a, "seed", "123").c_str(), nullptr, 10)));
+    const int64_t n = static_cast<int64_t>(num(a, "n", 4096));
+    const double sp = num(a, "sigma_pos", 5e-4);
+    const double T = num(a, "T", 300.0);
+    const double m = num(a, "mass", 200.0 * AMU_TO_KG);
+    State s;
+    s.n = n;
+    for (auto& v : s.a) v.assign(static_cast<size_t>(n), 0.0);
+    for (int64_t i = 0; i < n; ++i) {
+        // IonLoader::sample_position (Gaussian) then sample_velocity (Thermal),
+        // each with fresh distribution objects (IonLoader.cpp:246-313).
+        std::normal_distribution<double> np(0.0, 1.0);
+        const double px = 0.0 + np(rng) * sp;
+        const double py = 0.0 + np(rng) * sp;
+        const double pz = 0.0 + np(rng) * sp;
+        std::normal_distribution<double> nv(0.0, 1.0);
+        const double sig = std::sqrt(BOLTZMANN_CONSTANT * T / m);
+        const double vx = nv(rng) * sig;
+        const double vy = nv(rng) * sig;
+        const double vz = nv(rng) * sig;
+        const size_t k = static_cast<size_t>(i);
+        s.a[0][k] = px; s.a[1][k] = py; s.a[2][k] = pz;
+        s.a[3][k] = vx; s.a[4][k] = vy; s.a[5][k] = vz;
+        s.a[6][k] = m;
+        s.a[7][k] = num(a, "charge", ELEM_CHARGE_C);
+        s.a[8][k] = num(a, "ccs", 150e-20);
+        s.a[9][k] = 1.0;
+        s.a[10][k] = -1.0;
+        s.a[11][k] = -1.0;
+    }
+    write_state(str(a, "out", "state.bin"), s);
+    return 0;
+}
+
+int mode_derive(const Args& a) {
+    auto d = make_domain(a);
+    std::printf("{\"gas_density_m3\": %.17g, \"gas_mass_kg\": %.17g, \"axial_V\": %.17g, "
+                "\"E_z\": %.17g}\n",
+                d.environment.particle_density_m_3, d.environment.gas_mass_kg,
+                d.fields.dc.axial_V.constant_value.value_or(0.0),
+                d.fields.dc.axial_V.constant_value.value_or(0.0) / d.geometry.length_m);
+    return 0;
+}
+
+int mode_run(const Args& a) {
+    State s = read_state(str(a, "in", "state.bin"));
+    const int64_t n = s.n;
+    config::DomainConfig d = make_domain(a);
+    const double dt = num(a, "dt", 5e-10);
+    const int64_t steps = static_cast<int64_t>(num(a, "steps", 1000));
+    const int64_t snap = static_cast<int64_t>(num(a, "snap", 0));
+    const int64_t ref_step = static_cast<int64_t>(num(a, "ref_step", 0));
+    const double zdet = num(a, "zdet", 1e30);
+    const uint64_t seed = std::strtoull(str(a, "seed", "123").c_str(), nullptr, 10);
+    const std::string integ = str(a, "integrator", "boris");
+    const std::string coll = str(a, "collision", "none");
+    const bool faithful = str(a, "schedule", "static") == "faithful";
+    const int threads = static_cast<int>(num(a, "threads", 1));
+#ifdef _OPENMP
+    omp_set_num_threads(threads);
+#else
+    (void)threads;
+#endif
+
+    std::vector<IonState> ions(static_cast<size_t>(n));
+    for (int64_t i = 0; i < n; ++i) {
+        auto& ion = ions[static_cast<size_t>(i)];
+        const size_t k = static_cast<size_t>(i);
+        ion.pos = Vec3{s.a[0][k], s.a[1][k], s.a[2][k]};
+        ion.vel = Vec3{s.a[3][k], s.a[4][k], s.a[5][k]};
+        ion.mass_kg = s.a[6][k];
+        ion.ion_charge_C = s.a[7][k];
+        ion.CCS_m2 = s.a[8][k];
+        ion.active = s.a[9][k] != 0.0;
+        ion.born = true;
+        ion.birth_time_s = 0.0;
+        ion.species_id = "ion";
+    }
+    core::IonEnsemble ens = core::IonEnsemble::from_legacy(ions);
+
+    config::AnalyticalFieldModel field_model(d);
+    auto reg = std::make_shared<physics::ForceRegistry>(d);
+    reg->add_force(std::make_unique<physics::ElectricFieldForce>(d));
+    if (d.fields.magnetic.enabled && integ != "boris")
+        reg->add_force(std::make_unique<physics::MagneticFieldForce>(d.fields.magnetic));
+    reg->set_field_model(&field_model);
+    std::vector<std::shared_ptr<physics::ForceRegistry>> regs{reg};
+    config::CylindricalGeometry geom(d);
+
+    integrator::BorisStrategy boris;
+    integrator::RK4Strategy rk4;
+    rk4.set_parallel_enabled(threads > 1);
+    physics::HSSCollisionHandler hss(false, nullptr);
+    std::vector<physics::PhysicsRng> rng;
+    rng.reserve(static_cast<size_t>(n));
+    for (int64_t i = 0; i < n; ++i) rng.emplace_back(seed + static_cast<uint64_t>(i));
+
+    auto* px = ens.pos_x_data(); auto* py = ens.pos_y_data(); auto* pz = ens.pos_z_data();
+    auto* vx = ens.vel_x_data(); auto* vy = ens.vel_y_data(); auto* vz = ens.vel_z_data();
+    auto* active = ens.active_data();
+    std::vector<double>& t_death = s.a[10];
+    std::vector<double>& t_arr = s.a[11];
+    std::vector<double> zold(static_cast<size_t>(n));
+    std::vector<int> dom(static_cast<size_t>(n), 0);
+    const int64_t n_snap = snap > 0 ? steps / snap : 0;
+    std::vector<double> mom(static_cast<size_t>(n_snap * 20), 0.0);
+    std::vector<double> rx(px, px + n), ry(py, py + n), rz(pz, pz + n);
+    uint64_t collisions = 0;
+
+    double t = num(a, "t0", 0.0);
+    const auto wall0 = std::chrono::steady_clock::now();
+    for (int64_t k = 0; k < steps; ++k) {
+        // prepare_ions_for_integration
+        for (int64_t i = 0; i < n; ++i) {
+            if (!active[i]) { dom[static_cast<size_t>(i)] = -1; continue; }
+            if (!geom.contains(Vec3{px[i], py[i], pz[i]})) {
+                active[i] = 0;
+                t_death[static_cast<size_t>(i)] = t;
+                dom[static_cast<size_t>(i)] = -1;
+            } else {
+                dom[static_cast<size_t>(i)] = 0;
+            }
+            zold[static_cast<size_t>(i)] = pz[i];
+        }
+        if (integ == "rk4") {
+            rk4.step_batch(ens, t, dt, regs, dom);
+            if (coll == "hss") {
+#pragma omp parallel for schedule(static) reduction(+ : collisions)
+                for (int64_t i = 0; i < n; ++i) {
+                    if (!active[i]) continue;
+                    auto cv = ens.collision_data(static_cast<size_t>(i));
+                    collisions += hss.handle_collision(cv, dt, rng[static_cast<size_t>(i)], d.environment) ? 1 : 0;
+                }
+            }
+        } else if (faithful) {
+            // Engine order as written: serial Boris loop, OpenMP collision loop.
+            for (int64_t i = 0; i < n; ++i)
+                if (active[i]) boris.step(ens, static_cast<size_t>(i), t, dt, *reg);
+            if (coll == "hss") {
+#pragma omp parallel for schedule(guided, 128) reduction(+ : collisions)
+                for (int64_t i = 0; i < n; ++i) {
+                    if (!active[i]) continue;
+                    auto cv = ens.collision_data(static_cast<size_t>(i));
+                    collisions += hss.handle_collision(cv, dt, rng[static_cast<size_t>(i)], d.environment) ? 1 : 0;
+                }
+            }
+        } else {
+            // Best CPU form of the reference code: one OpenMP loop, push then collide.
+#pragma omp parallel for schedule(static) reduction(+ : collisions)
+            for (int64_t i = 0; i < n; ++i) {
+                if (!active[i]) continue;
+                boris.step(ens, static_cast<size_t>(i), t, dt, *reg);
+                if (coll == "hss") {
+                    auto cv = ens.collision_data(static_cast<size_t>(i));
+                    collisions += hss.handle_collision(cv, dt, rng[static_cast<size_t>(i)], d.environment) ? 1 : 0;
+                }
+            }
+        }
+        // finalize_ions_after_integration (+ arrival-plane crossing)
+        for (int64_t i = 0; i < n; ++i) {
+            const size_t k2 = static_cast<size_t>(i);
+            if (dom[k2] < 0) continue;
+            const double zo = zold[k2];
+            if (t_arr[k2] < 0.0 && zo < zdet && pz[i] >= zdet)
+                t_arr[k2] = t + dt * ((zdet - zo) / (pz[i] - zo));
+            const Vec3 p{px[i], py[i], pz[i]};
+            if (!geom.contains(p)) {
+                active[i] = 0;
+                t_death[k2] = t;
+                continue;
+            }
+            if (!(std::isfinite(p.x) && std::isfinite(p.y) && std::isfinite(p.z) &&
+                  std::isfinite(vx[i]) && std::isfinite(vy[i]) && std::isfinite(vz[i]))) {
+                active[i] = 0;
+                t_death[k2] = t;
+            }
+        }
+        t = t + dt;
+        if (k + 1 == ref_step) {
+            std::copy(px, px + n, rx.begin());
+            std::copy(py, py + n, ry.begin());
+            std::copy(pz, pz + n, rz.begin());
+        }
+        if (snap > 0 && (k + 1) % snap == 0) {
+            double* m = &mom[static_cast<size_t>(((k + 1) / snap - 1) * 20)];
+            for (int64_t i = 0; i < n; ++i) {
+                const size_t k2 = static_cast<size_t>(i);
+                if (t_arr[k2] >= 0.0) m[11] += 1.0;
+                if (!active[i]) { if (t_death[k2] >= 0.0) m[12] += 1.0; continue; }
+                m[0] += 1.0;
+                m[1] += px[i]; m[2] += py[i]; m[3] += pz[i];
+                m[4] += px[i] * px[i]; m[5] += py[i] * py[i]; m[6] += pz[i] * pz[i];
+                m[7] += vx[i]; m[8] += vy[i]; m[9] += vz[i];
+                m[10] += vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i];
+                m[13] += pz[i] * vz[i];
+                const double d[3] = {px[i] - rx[k2], py[i] - ry[k2], pz[i] - rz[k2]};
+                for (int c = 0; c < 3; ++c) {
+                    m[14 + c] += d[c];
+                    m[17 + c] += d[c] * d[c];
+                }
+            }
+        }
+    }
+    const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
+
+    for (int64_t i = 0; i < n; ++i) {
+        const size_t k = static_cast<size_t>(i);
+        s.a[0][k] = px[i]; s.a[1][k] = py[i]; s.a[2][k] = pz[i];
+        s.a[3][k] = vx[i]; s.a[4][k] = vy[i]; s.a[5][k] = vz[i];
+        s.a[9][k] = active[i] ? 1.0 : 0.0;
+    }
+    write_state(str(a, "out", "state_out.bin"), s);
+    if (snap > 0) {
+        FILE* f = std::fopen(str(a, "mom", "moments.bin").c_str(), "wb");
+        std::fwrite(mom.data(), sizeof(double), mom.size(), f);
+        std::fclose(f);
+    }
+    std::printf("{\"ion_steps\": %lld, \"wall_s\": %.6f, \"ion_steps_per_s\": %.6g, \"threads\": %d, "
+                "\"collisions\": %llu, \"t_end\": %.17g}\n",
+                static_cast<long long>(n * steps), wall, static_cast<double>(n * steps) / wall, threads,
+                static_cast<unsigned long long>(collisions), t);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 2) {
+        std::fprintf(stderr, "usage: ref_harness uniforms|init|derive|run key=value...\n");
+        return 2;
+    }
+    Args a;
+    for (int i = 2; i < argc; ++i) {
+        const char* eq = std::strchr(argv[i], '=');
+        if (!eq) { std::fprintf(stderr, "bad argument %s\n", argv[i]); return 2; }
+        a[std::string(argv[i], static_cast<size_t>(eq - argv[i]))] = std::string(eq + 1);
+    }
+    try {
+        const std::string mode = argv[1];
+        if (mode == "uniforms") return mode_uniforms(a);
+        if (mode == "init") return mode_init(a);
+        if (mode == "derive") return mode_derive(a);
+        if (mode == "run") return mode_run(a);
+        std::fprintf(stderr, "unknown mode %s\n", argv[1]);
+        return 2;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "ref_harness: %s\n", e.what());
+        return 1;
+    }
+}

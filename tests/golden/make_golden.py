@@ -1,0 +1,135 @@
+"""Generate the golden fixtures of tests/golden/ from the reference's own code.
+
+    make -C oracle && python tests/golden/make_golden.py [--quick]
+
+Every fixture is produced by ``oracle/_ref/ref_harness`` — the reference's
+hot-path sources (BorisStrategy, RK4Strategy, HSSCollisionHandler,
+CollisionKernels, VelocitySampling, PhysicsRng, ForceRegistry, the analytic
+field model and CylindricalGeometry) compiled unchanged by oracle/Makefile —
+driven through the reference engine's per-step order.  The reference tree is
+needed only here; the fixtures travel with the repository.
+
+Fixtures
+  rng_mt64.npz          PhysicsRng(seed).uniform01() streams (seeds 123, 4219)
+  ions_init.npz         IonLoader gaussian/thermal cloud from std::mt19937(123)
+  derived.json          loader-derived n, gas mass, axial_V, E_z (config 0)
+  push_<case>.npz       collision-free Boris / RK4 runs (IMS, FTICR, QuadrupoleRF)
+  hss_ref.npz           Boris + reference HSS, 64 ions x 2000 steps
+  ims_config0.npz       config 0: 4096 ions x 100k steps, moments every 1000
+                        steps, displacement reference after 20k steps,
+                        arrival (z = 2 mm) and death times, OpenMP timing
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT / "oracle"))
+import oracle as orc  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+AMU = 1.66053906660e-27
+E = 1.602176634e-19
+
+# config 0: IMS drift of 200 Da, 150 A^2 ions in N2, 300 K, 1000 Pa, 20 Td
+IMS_DOMAIN = dict(instrument="IMS", origin_z=-0.01, length=0.1, radius=0.05, T=300, P=1000, gas="N2", EN_Td=20)
+FTICR_DOMAIN = dict(instrument="FTICR", origin_z=0.0, length=0.05, radius=0.025, T=300, P=1e-7, gas="He",
+                    radial_V=1.0, magnetic=1, B_z=7.0)
+QUAD_DOMAIN = dict(instrument="QuadrupoleRF", origin_z=-0.05, length=0.1, radius=0.005, T=300, P=1.0, gas="He",
+                   rf_V=200.0, rf_f=1.0e6, dc_quad_V=5.0, axial_V=1.0)
+
+
+def init_state(n: int, seed: int = 123, mass_amu: float = 200.0, sigma_pos: float = 5e-4) -> dict:
+    st_path = OUT / "_tmp_init.bin"
+    orc.harness("init", seed=seed, n=n, sigma_pos=sigma_pos, T=300, mass=repr(mass_amu * AMU), out=st_path)
+    st = orc.read_state(st_path)
+    st_path.unlink()
+    return st
+
+
+def fticr_state(n: int) -> dict:
+    """Ions on 2 mm cyclotron orbits about the trap centre (0, 0, L/2),
+    m/z uniform over 500-1500 (fixed seed)."""
+    rng = np.random.default_rng(7)
+    m = rng.uniform(500.0, 1500.0, n) * AMU
+    wc = E * 7.0 / m
+    phase = rng.uniform(0, 2 * np.pi, n)
+    r = 2e-3
+    st = {
+        "x": r * np.cos(phase) + rng.normal(0, 1e-4, n), "y": r * np.sin(phase) + rng.normal(0, 1e-4, n),
+        "z": 0.025 + rng.normal(0, 1e-4, n),
+        "vx": -wc * r * np.sin(phase), "vy": wc * r * np.cos(phase), "vz": rng.normal(0, 5.0, n),
+        "mass": m, "charge": np.full(n, E), "ccs": np.full(n, 150e-20), "active": np.ones(n),
+        "t_death": np.full(n, -1.0), "t_arrival": np.full(n, -1.0),
+    }
+    return st
+
+
+def save(name: str, **arrays) -> None:
+    np.savez_compressed(OUT / name, **arrays)
+    print("wrote", name, flush=True)
+
+
+def main(quick: bool) -> None:
+    if not orc.have_harness():
+        raise SystemExit("oracle/_ref/ref_harness missing: run `make -C oracle` with the reference tree present")
+
+    # 1. PhysicsRng streams
+    streams = {}
+    for seed in (123, 4219):
+        p = OUT / "_u.bin"
+        orc.harness("uniforms", seed=seed, n=256, out=p)
+        streams[f"seed_{seed}"] = np.fromfile(p, dtype=np.float64)
+        p.unlink()
+    save("rng_mt64.npz", **streams)
+
+    # 2. ion cloud
+    st = init_state(64)
+    save("ions_init.npz", **{k: st[k] for k in ("x", "y", "z", "vx", "vy", "vz", "mass")},
+         seed=123, sigma_pos=5e-4, T=300.0, mass_amu=200.0)
+
+    # 3. derived constants
+    d = json.loads(orc.harness("derive", **IMS_DOMAIN))
+    (OUT / "derived.json").write_text(json.dumps(d, indent=1) + "\n")
+
+    # 4. collision-free pushes
+    cases = {
+        "boris_ims": (IMS_DOMAIN, "boris", init_state(64), 5000, 5e-10),
+        "rk4_ims": (IMS_DOMAIN, "rk4", init_state(64), 5000, 5e-10),
+        "boris_fticr": (FTICR_DOMAIN, "boris", fticr_state(64), 20000, 1e-9),
+        "rk4_fticr": (FTICR_DOMAIN, "rk4", fticr_state(64), 5000, 1e-9),
+        "boris_quadrf": (QUAD_DOMAIN, "boris", init_state(64, mass_amu=100.0, sigma_pos=2e-4), 4000, 1e-9),
+    }
+    for name, (dom, integ, s0, steps, dt) in cases.items():
+        fin, stats, _ = orc.harness_run(s0, steps, dom, integrator=integ, collision="none", dt=dt)
+        save(f"push_{name}.npz", **{f"in_{k}": s0[k] for k in orc.STATE_KEYS},
+             **{f"out_{k}": fin[k] for k in orc.STATE_KEYS}, steps=steps, dt=dt,
+             domain=json.dumps(dom), integrator=integ)
+
+    # 5. Boris + reference HSS, bit-level fixture for the restatement
+    s0 = init_state(64)
+    fin, stats, _ = orc.harness_run(s0, 2000, IMS_DOMAIN, integrator="boris", collision="hss", dt=5e-10, seed=123)
+    save("hss_ref.npz", **{f"in_{k}": s0[k] for k in orc.STATE_KEYS},
+         **{f"out_{k}": fin[k] for k in orc.STATE_KEYS}, steps=2000, dt=5e-10, seed=123,
+         collisions=stats["collisions"], domain=json.dumps(IMS_DOMAIN))
+
+    # 6. config 0 statistics
+    n, steps = (1024, 20000) if quick else (4096, 100000)
+    s0 = init_state(n)
+    fin, stats, mom = orc.harness_run(s0, steps, IMS_DOMAIN, integrator="boris", collision="hss", dt=5e-10,
+                                      seed=123, snap=1000, ref_step=steps // 5, zdet=2.0e-3, threads=8)
+    save("ims_config0.npz", moments=mom, snap_every=1000, ref_step=steps // 5, steps=steps, dt=5e-10,
+         n_ions=n, t_arrival=fin["t_arrival"], t_death=fin["t_death"], zdet=2.0e-3,
+         final_vz=fin["vz"], ion_steps_per_s=stats["ion_steps_per_s"], threads=stats["threads"],
+         collisions=stats["collisions"], domain=json.dumps(IMS_DOMAIN))
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--quick", action="store_true")
+    main(ap.parse_args().quick)

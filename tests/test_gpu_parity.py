@@ -1,0 +1,210 @@
+"""Device parity through the C ABI against the reference's own outputs and
+the CPU oracle.
+
+Tolerances (stated per test):
+  * FP64 collision-free push: <= 1e-12 relative; the
+    uniform-field and linear-field cases are additionally bit-identical.
+  * FP64 null-collision HSS vs the FP64 oracle with the same Philox streams:
+    >= 99% of ions agree to 1e-9 relative after 3000 steps (transcendental
+    functions differ by an ulp between CUDA and glibc, which can flip a rare
+    accept/reject decision).
+  * Mixed precision push: <= 2e-5 (IMS) / 2e-3 (FT-ICR, RF) relative.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as orc
+from helpers import config0_ensemble, config0_ions, ensemble_from_golden, golden_state, oracle_state
+from icarion_b200 import _capi as capi
+from icarion_b200.sim import IonState, Simulation, device_count
+
+pytestmark = pytest.mark.gpu
+
+PUSH_CASES = ["boris_ims", "rk4_ims", "boris_fticr", "rk4_fticr", "boris_quadrf"]
+BIT_EXACT = {"boris_ims", "rk4_ims", "boris_fticr", "rk4_fticr"}
+KEYS = ("x", "y", "z", "vx", "vy", "vz")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    assert device_count() > 0, "these tests need a CUDA device"
+
+
+def vec_rel_err(out: IonState, z, prefix="out_") -> float:
+    """max over ions of |a - b| / |b| per 3-vector (position and velocity)."""
+    worst = 0.0
+    for grp in (("x", "y", "z"), ("vx", "vy", "vz")):
+        a = np.stack([getattr(out, k) for k in grp])
+        b = np.stack([z[prefix + k] for k in grp])
+        scale = np.maximum(np.linalg.norm(b, axis=0), 1e-300)
+        worst = max(worst, float(np.max(np.linalg.norm(a - b, axis=0) / scale)))
+    return worst
+
+
+def run_push(z, precision, integrator) -> IonState:
+    e = ensemble_from_golden(z)
+    with Simulation([e], precision=precision, integrator=integrator, collision=capi.COLLISION_NONE) as sim:
+        sim.upload(golden_state(z))
+        sim.advance(int(z["steps"]))
+        return sim.download()
+
+
+@pytest.mark.parametrize("case", PUSH_CASES)
+def test_fp64_push_matches_reference(golden, case):
+    z = golden(f"push_{case}.npz")
+    integ = capi.INTEGRATOR_BORIS if case.startswith("boris") else capi.INTEGRATOR_RK4
+    out = run_push(z, capi.PREC_FP64, integ)
+    err = vec_rel_err(out, z)
+    assert err <= 1e-12, err
+    if case in BIT_EXACT:
+        for k in KEYS:
+            assert np.array_equal(getattr(out, k), z[f"out_{k}"]), k
+    assert np.array_equal(out.active, z["out_active"].astype(np.uint8))
+
+
+@pytest.mark.parametrize("case", PUSH_CASES)
+def test_mixed_push_close_to_reference(golden, case):
+    z = golden(f"push_{case}.npz")
+    integ = capi.INTEGRATOR_BORIS if case.startswith("boris") else capi.INTEGRATOR_RK4
+    tol = 2e-5 if case.endswith("ims") else 2e-3
+    err = vec_rel_err(run_push(z, capi.PREC_MIXED, integ), z)
+    assert err <= tol, err
+    if case.startswith("boris"):
+        err_hl = vec_rel_err(run_push(z, capi.PREC_MIXED_HILO, integ), z)
+        assert err_hl <= tol, err_hl
+
+
+def test_philox_device_matches_oracle_and_curand():
+    rng = np.random.default_rng(11)
+    n = 4096
+    ctr = rng.integers(0, 2**32, size=(n, 4), dtype=np.uint64).astype(np.uint32)
+    seed = 0x0123456789ABCDEF
+    ref = orc.philox(ctr, seed)
+    for use_curand in (0, 1):
+        out = np.zeros_like(ctr)
+        capi.check(capi.lib().icb_philox_eval(0, n, capi.u32ptr(np.ascontiguousarray(ctr)), seed, use_curand,
+                                              capi.u32ptr(out)))
+        assert np.array_equal(out, ref), f"use_curand={use_curand}"
+
+
+def _hss_gpu(st0: IonState, e: dict, steps: int, **kw) -> tuple[IonState, dict]:
+    with Simulation([e], precision=kw.pop("precision", capi.PREC_FP64), integrator=capi.INTEGRATOR_BORIS,
+                    collision=capi.COLLISION_HSS, rng_seed=123, **kw) as sim:
+        sim.upload(st0)
+        rs = sim.advance(steps)
+        return sim.download(), rs
+
+
+def test_fp64_hss_trajectories_match_oracle():
+    n, steps = 512, 3000
+    e = config0_ensemble()
+    st0 = config0_ions(n)
+    ost = oracle_state(st0)
+    r = orc.run(e, ost, steps, integrator=0, collision=2, seed=123)
+    out, rs = _hss_gpu(st0, e, steps)
+    pos = np.stack([out.x, out.y, out.z])
+    opos = np.stack([ost["x"], ost["y"], ost["z"]])
+    vel = np.stack([out.vx, out.vy, out.vz])
+    ovel = np.stack([ost["vx"], ost["vy"], ost["vz"]])
+    rel = np.maximum(np.linalg.norm(pos - opos, axis=0) / np.linalg.norm(opos, axis=0),
+                     np.linalg.norm(vel - ovel, axis=0) / np.linalg.norm(ovel, axis=0))
+    frac = float(np.mean(rel < 1e-9))
+    assert frac >= 0.99, (frac, np.sort(rel)[-5:])
+    assert abs(rs["collisions"] - r["collisions"]) <= 0.01 * r["collisions"]
+    assert r["collisions"] > 0.05 * n * steps      # ~9% of ion-steps collide at config 0
+
+
+def test_results_independent_of_launch_shape():
+    """Same Philox counters and per-lane step order: block size, steps per
+    launch and the deferred-collision threshold do not change results."""
+    n, steps = 3000, 1500
+    e = config0_ensemble()
+    st0 = config0_ions(n)
+    outs = []
+    for bs, K, pend in ((256, 1000, 20), (64, 7, 1), (128, 333, 32)):
+        out, _ = _hss_gpu(st0, e, steps, block_size=bs, steps_per_launch=K, pending_threshold=pend)
+        outs.append(out)
+    for o in outs[1:]:
+        for k in KEYS:
+            assert np.array_equal(getattr(o, k), getattr(outs[0], k)), k
+
+
+def test_unfused_plug_points_equal_fused_step():
+    """push (step_batch) -> collide (handle_batch) -> finalize, one call each
+    per step, gives the fused icb_advance result bit for bit (FP64)."""
+    n, steps = 1024, 200
+    e = config0_ensemble()
+    st0 = config0_ions(n)
+    fused, _ = _hss_gpu(st0, e, steps)
+    with Simulation([e], precision=capi.PREC_FP64, collision=capi.COLLISION_HSS, rng_seed=123) as sim:
+        sim.upload(st0)
+        for _ in range(steps):
+            sim.step_batch()
+            sim.handle_batch()
+            sim.finalize()
+        parts = sim.download()
+        step, t = sim.clock()
+    assert step == steps
+    for k in KEYS:
+        assert np.array_equal(getattr(parts, k), getattr(fused, k)), k
+
+
+def test_domain_exit_death_times_match_oracle():
+    """Ions leaving a small cylinder are deactivated with death time = start
+    of the step (SimulationEngineLifecycle.cpp:139-147); FP64 vs oracle."""
+    n, steps = 256, 4000
+    e = config0_ensemble()
+    e.update(radius_m=6e-4, length_m=2.6e-3, origin_m=[0.0, 0.0, -1.3e-3])
+    st0 = config0_ions(n)
+    ost = oracle_state(st0)
+    orc.run(e, ost, steps, integrator=0, collision=2, seed=123)
+    out, rs = _hss_gpu(st0, e, steps)
+    dead = ost["active"] == 0
+    assert dead.sum() > n // 4
+    agree = np.mean((out.active == ost["active"]) & (out.t_death == ost["t_death"]))
+    assert agree >= 0.98, agree
+    assert rs["deaths"] == int(np.sum(out.active == 0))
+
+
+def test_outside_and_nonfinite_ions_are_deactivated():
+    e = config0_ensemble()
+    st = config0_ions(64)
+    st.z[3] = 0.5                 # outside the cylinder before the first step
+    st.vx[5] = np.nan             # non-finite velocity
+    for prec in (capi.PREC_FP64, capi.PREC_MIXED):
+        out, rs = _hss_gpu(st, e, 10, precision=prec)
+        assert out.active[3] == 0 and out.t_death[3] == 0.0
+        assert out.active[5] == 0 and out.t_death[5] == 0.0
+        assert int(out.active.sum()) == 62
+
+
+def test_births_wait_until_birth_time():
+    e = config0_ensemble()
+    st = config0_ions(32)
+    st.birth = np.zeros(32)
+    st.birth[:8] = 1.0            # never born within the run
+    st.birth[8:16] = 50 * 5e-10   # born at step 50
+    with Simulation([e], precision=capi.PREC_FP64, collision=capi.COLLISION_HSS) as sim:
+        sim.upload(st)
+        sim.advance(49)
+        mid = sim.download()
+        sim.advance(51)
+        end = sim.download()
+    assert np.array_equal(mid.z[:16], st.z[:16]) and not mid.active[:16].any()
+    assert not end.active[:8].any() and np.array_equal(end.z[:8], st.z[:8])
+    assert end.active[8:].all() and not np.array_equal(end.z[8:16], st.z[8:16])
+
+
+def test_invalid_inputs_raise():
+    e = config0_ensemble()
+    with Simulation([e], precision=capi.PREC_MIXED) as sim:
+        st = config0_ions(16)
+        st.mass[2] = 0.0
+        with pytest.raises(capi.IcbError):
+            sim.upload(st)
+        with pytest.raises(capi.IcbError):
+            sim.advance(10)       # nothing uploaded
+    with pytest.raises(capi.IcbError):
+        Simulation([dict(e, dt_s=0.0)])
