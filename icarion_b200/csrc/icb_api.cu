@@ -229,9 +229,9 @@ struct icb_handle {
     int field_kind = kFieldUniform;
     bool magnetic = false;
     int coll = kCollNone;
-    int block = 256;
+    int block = 128;
     uint32_t K = 1000;
-    uint32_t pend = 20;
+    uint32_t pend = 16;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -249,7 +249,7 @@ struct icb_handle {
     DevBuf<float> vxf, vyf, vzf;
     DevBuf<double> Sd, Ud;
     DevBuf<float> Sf, Uf;
-    DevBuf<double> mass, charge, t_death, t_arr, birth;
+    DevBuf<double> mass, charge, t_death, t_arr, birth, zprev;
     DevBuf<uint8_t> flags, active_stage;
     DevBuf<double> stage;
     DevBuf<unsigned long long> counters, step_dev;
@@ -326,6 +326,7 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
     C.ox = P.origin_m[0]; C.oy = P.origin_m[1]; C.oz = P.origin_m[2];
     C.zmax_local = P.length_m + kGeomEps;
     C.rmax2 = (P.radius_m + kGeomEps) * (P.radius_m + kGeomEps);
+    C.rmax = P.radius_m + kGeomEps;
     C.dt = P.dt_s;
     if (coll != kCollNone) {
         if (!(P.gas_mass_kg > 0.0) || !(P.temperature_K > 0.0))
@@ -361,6 +362,7 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.mass = h->mass.p; p.charge = h->charge.p; p.flags = h->flags.p;
         p.t_death = h->t_death.p; p.t_arr = h->t_arr.p;
         p.birth = h->has_birth ? h->birth.p : nullptr;
+        p.zprev = h->zprev.p;
         p.counters = h->counters.p;
         p.step_dev = h->step_dev.p;
         p.t_dev = h->t_dev.p;
@@ -468,11 +470,15 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
         if (r != ICB_OK) return r;
     }
     if (cfg->block_size > 0) {
-        if (cfg->block_size % 32 != 0 || cfg->block_size > 256)
-            return fail(ICB_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 and <= 256");
+        if (cfg->block_size % 32 != 0 || cfg->block_size > 128)
+            return fail(ICB_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 and <= 128");
         h->block = cfg->block_size;
     }
-    if (cfg->steps_per_launch > 0) h->K = static_cast<uint32_t>(cfg->steps_per_launch);
+    if (cfg->steps_per_launch > 0) {
+        if (cfg->steps_per_launch > static_cast<int32_t>(kMaxStepsPerLaunch))
+            return fail(ICB_ERR_INVALID_ARGUMENT, "steps_per_launch must be <= %u", kMaxStepsPerLaunch);
+        h->K = static_cast<uint32_t>(cfg->steps_per_launch);
+    }
     if (cfg->pending_threshold > 0) h->pend = static_cast<uint32_t>(std::min(cfg->pending_threshold, 32));
     ICB_CUDA(cudaSetDevice(cfg->device));
     ICB_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
@@ -556,6 +562,7 @@ int icb_upload_ions(icb_handle* h, uint64_t n,
         ICB_CUDA(h->xr.alloc(n)); ICB_CUDA(h->yr.alloc(n)); ICB_CUDA(h->zr.alloc(n));
         ICB_CUDA(h->mass.alloc(n)); ICB_CUDA(h->charge.alloc(n));
         ICB_CUDA(h->t_death.alloc(n)); ICB_CUDA(h->t_arr.alloc(n)); ICB_CUDA(h->birth.alloc(n));
+        ICB_CUDA(h->zprev.alloc(n));
         ICB_CUDA(h->flags.alloc(n)); ICB_CUDA(h->active_stage.alloc(n));
         ICB_CUDA(h->stage.alloc(f64 ? 0 : n));
         h->n = n;

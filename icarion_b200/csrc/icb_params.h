@@ -10,6 +10,10 @@
 namespace icb {
 
 constexpr int kMaxLaunchEns = 64;   // ensembles per launch chunk (param space bound)
+// Steps per launch are bounded so that the float accumulation of a lane's
+// drift length between exact boundary checks stays within 0.1% (the check
+// triggers at 99% of the distance to the nearest boundary).
+constexpr uint32_t kMaxStepsPerLaunch = 16384;
 
 enum FieldKind : int { kFieldUniform = 0, kFieldLinear = 1, kFieldLinearRF = 2 };
 enum CollKind : int { kCollNone = 0, kCollHSS = 1 };
@@ -35,7 +39,7 @@ struct EnsConst {
     double B[3];
     // Cylinder (no rotation): local = x - origin; inside iff
     // -eps <= lz < L + eps and lx^2 + ly^2 <= (R + eps)^2.
-    double ox, oy, oz, zmax_local, rmax2;
+    double ox, oy, oz, zmax_local, rmax2, rmax;
     double dt;
     // Gas: A = n sigma dt, mean thermal speed <|th|> = sigma_n 2 sqrt(2/pi).
     double A, mean_th, sig_n;
@@ -61,6 +65,7 @@ struct StepParams {
     double* t_death;
     double* t_arr;
     const double* birth;               // nullable
+    double* zprev;                     // z before the push, kept between unfused calls
     unsigned long long* counters;      // kNumCounters
     const unsigned long long* step_dev;// engine step index at launch start
     const double* t_dev;               // engine time per ensemble at launch start

@@ -8,7 +8,10 @@ namespace icb {
 
 template <int PREC, int INTEG, int COLL, int FIELD, bool MAG>
 cudaError_t launch_one(const StepParams& p, dim3 grid, dim3 block, cudaStream_t s) {
-    k_step<PREC, INTEG, COLL, FIELD, MAG><<<grid, block, 0, s>>>(p);
+    if (p.do_push && p.do_collide && p.do_finalize)
+        k_step<PREC, INTEG, COLL, FIELD, MAG, true><<<grid, block, 0, s>>>(p);
+    else
+        k_step<PREC, INTEG, COLL, FIELD, MAG, false><<<grid, block, 0, s>>>(p);
     return cudaGetLastError();
 }
 

@@ -209,8 +209,9 @@ __device__ __forceinline__ void efield(const Consts<R>& k, const Pos& x, double 
 
 // ---- pushers ------------------------------------------------------------------
 // Boris exactly as BorisStrategy.cpp:50-97, including x += v_plus * dt.
+// Returns |v_plus|_1, the L1 speed of this step's drift.
 template <class R, int FIELD, bool MAG, class Pos>
-__device__ __forceinline__ void boris(const Consts<R>& k, Pos& x, R v[3], double t) {
+__device__ __forceinline__ R boris(const Consts<R>& k, Pos& x, R v[3], double t) {
     R a[3];
     if (FIELD == kFieldUniform) {
         a[0] = k.a_uni[0]; a[1] = k.a_uni[1]; a[2] = k.a_uni[2];
@@ -244,6 +245,7 @@ __device__ __forceinline__ void boris(const Consts<R>& k, Pos& x, R v[3], double
     x.drift(vp[0], vp[1], vp[2], k.dt);
 #pragma unroll
     for (int c = 0; c < 3; ++c) v[c] = vp[c] + a[c] * k.h;
+    return fabs(vp[0]) + fabs(vp[1]) + fabs(vp[2]);
 }
 
 // RK4 acceleration: (E q [+ (v x B) q]) * (1/m)  (RK4Strategy.cpp:236-243,
@@ -265,8 +267,9 @@ __device__ __forceinline__ void rk4_acc(const Consts<R>& k, const Pos& x, const 
     for (int c = 0; c < 3; ++c) acc[c] = F[c] * k.inv_m;
 }
 
+// Returns the L1 norm of the step's displacement divided by dt.
 template <class R, int FIELD, bool MAG, class Pos>
-__device__ __forceinline__ void rk4(const Consts<R>& k, Pos& x, R v[3], double t) {
+__device__ __forceinline__ R rk4(const Consts<R>& k, Pos& x, R v[3], double t) {
     const double dt = k.dt;
     const double hd = dt * 0.5;
     const R h = k.h;
@@ -295,6 +298,7 @@ __device__ __forceinline__ void rk4(const Consts<R>& k, Pos& x, R v[3], double t
     const R s = static_cast<R>(dt / 6.0);
 #pragma unroll
     for (int c = 0; c < 3; ++c) v[c] = v0[c] + (k1a[c] + k2a[c] * R(2.0) + k3a[c] * R(2.0) + k4a[c]) * s;
+    return (fabs(dv[0]) + fabs(dv[1]) + fabs(dv[2])) * R(1.0 / 6.0);
 }
 
 // ---- null-collision HSS -------------------------------------------------------
@@ -312,8 +316,20 @@ __device__ __forceinline__ bool clock_tick(const Consts<R>& k, const R v[3], R& 
 // Candidate processing (the same steps as the oracle's hss_nullcoll).
 // Returns true when the collision is accepted (v updated).
 template <class R>
-__device__ __forceinline__ bool candidate(const Consts<R>& k, R v[3], R& S, R& U, R gu,
+__device__ __forceinline__ bool candidate(const EnsConst& C, R v[3], R& S, R& U, R gu, double mi_d,
                                           uint64_t seed, uint32_t id, uint32_t step) {
+    struct {
+        R A, mean_th, sig_n, ug[3], mi, mn, inv_mt, fac;
+    } k;
+    k.A = static_cast<R>(C.A);
+    k.mean_th = static_cast<R>(C.mean_th);
+    k.sig_n = static_cast<R>(C.sig_n);
+    k.ug[0] = static_cast<R>(C.ug[0]); k.ug[1] = static_cast<R>(C.ug[1]); k.ug[2] = static_cast<R>(C.ug[2]);
+    k.mi = static_cast<R>(mi_d);
+    k.mn = static_cast<R>(C.m_gas);
+    const double inv = 1.0 / (mi_d + C.m_gas);
+    k.inv_mt = static_cast<R>(inv);
+    k.fac = static_cast<R>(C.m_gas * inv);
     const uint32_t k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32);
     const U4 r0 = philox4x32_10(id, step, 0u, 0u, k0, k1);
     const U4 r1 = philox4x32_10(id, step, 1u, 0u, k0, k1);
@@ -377,10 +393,29 @@ __device__ __forceinline__ unsigned long long warp_sum_u32(uint32_t v) {
 }
 
 // ---- the kernel -----------------------------------------------------------------
-template <int PREC, int INTEG, int COLL, int FIELD, bool MAG>
-__global__ void __launch_bounds__(256) k_step(const __grid_constant__ StepParams p) {
+// Exact per-step finalize of the reference (domain exit -> death at the step
+// start time, non-finite state -> death, first detector-plane crossing) is
+// evaluated only when it can change anything: each lane accumulates the L1
+// length of its drifts since its last exact check (acc) and re-checks once acc
+// may exceed 99% of the distance to the nearest wall, end face or (not yet
+// crossed) detector plane (lim).  The L1 length bounds the true path, so no
+// exit or crossing is missed; NaN or Inf makes acc non-finite and forces the
+// check.  Float accumulation error over <= 16384 steps per launch is < 0.1%.
+constexpr int kCheapStepsPerVote = 4;
+
+template <int PREC>
+struct KernelShape { static constexpr int kMinBlocks = 6; };
+template <>
+struct KernelShape<kPrecFP64> { static constexpr int kMinBlocks = 4; };
+
+template <int PREC, int INTEG, int COLL, int FIELD, bool MAG, bool FUSED>
+__global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(const __grid_constant__ StepParams p) {
     using R = typename PrecT<PREC>::R;
     using Pos = typename PosOf<PREC>::T;
+    // FP64 keeps the engine clock as the accumulated sum t += dt (bit-exact
+    // death and arrival times); the float paths form t = t0 + k*dt when an
+    // event needs it, unless the field itself is time dependent.
+    constexpr bool kAccumT = (PREC == kPrecFP64) || (FIELD == kFieldLinearRF);
 
     const uint64_t i = p.ens_off[0] + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const bool in_range = i < p.ens_off[p.n_ens];
@@ -394,12 +429,16 @@ __global__ void __launch_bounds__(256) k_step(const __grid_constant__ StepParams
         e = lo;
     }
     const EnsConst& C = p.ens[e];
+    const bool do_push = FUSED || p.do_push;
+    const bool do_coll = FUSED || p.do_collide;
+    const bool do_fin = FUSED || p.do_finalize;
 
     uint8_t flags = 0;
     Pos x{};
     R v[3] = {R(0), R(0), R(0)};
     R S = R(1), U = R(0);
     double q = 1.0, m = 1.0, birth = 0.0;
+    bool had_arrival = false;
     if (in_range) {
         flags = p.flags[i];
         x.load(p, i);
@@ -413,6 +452,7 @@ __global__ void __launch_bounds__(256) k_step(const __grid_constant__ StepParams
         q = p.charge[i];
         m = p.mass[i];
         if (p.birth) birth = p.birth[i];
+        had_arrival = p.t_arr[i] >= 0.0;
     }
     Consts<R> k;
     load_consts<R, FIELD, MAG>(k, C, q, m);
@@ -423,35 +463,60 @@ __global__ void __launch_bounds__(256) k_step(const __grid_constant__ StepParams
 
     const uint32_t id = static_cast<uint32_t>(p.first_id + i);
     const uint32_t step0 = static_cast<uint32_t>(*p.step_dev);
-    double t = p.t_dev[p.ens_base + e];
+    const double t0 = p.t_dev[p.ens_base + e];
     const double dt = C.dt;
+    const R dt_r = static_cast<R>(dt);
     const double zdet = C.zdet;
+    double t = t0;            // accumulated clock (used when kAccumT)
     double tdeath = -1.0, tarr = -1.0;
     bool dead_now = false, arr_now = false;
-
-    bool live = in_range && (flags & kFlagActive);
-    bool waiting = in_range && !(flags & kFlagBorn);
-    // prepare_ions_for_integration: an ion already outside is deactivated.
-    if (live && p.do_finalize && !inside(C, x)) {
-        live = false;
-        flags &= static_cast<uint8_t>(~kFlagActive);
-        tdeath = t;
-        dead_now = true;
-    }
-
-    uint32_t n_cand = 0, n_coll = 0, n_ovf = 0, n_dead = dead_now ? 1u : 0u, n_arr = 0;
-    bool had_arrival = in_range && p.t_arr[i] >= 0.0;
+    uint32_t n_cand = 0, n_coll = 0, n_ovf = 0, n_dead = 0, n_arr = 0;
     const uint32_t K = p.n_steps;
     uint32_t kk = 0;
     bool pending = false;
     R gu = R(0);
     double zold = 0.0;
+    R acc = R(0), lim = R(0);
 
+    auto t_step = [&]() -> double { return kAccumT ? t : fma(static_cast<double>(kk), dt, t0); };
+    auto kill = [&](double when) {
+        flags &= static_cast<uint8_t>(~kFlagActive);
+        tdeath = when;
+        dead_now = true;
+        ++n_dead;
+    };
+    // distance to the nearest wall, end face or pending detector plane
+    auto new_limit = [&]() {
+        const double z = x.gz();
+        const double lz = z - C.oz;
+        double d = fmin(lz + 1e-12, C.zmax_local - lz);
+        const double lx = x.gx() - C.ox, ly = x.gy() - C.oy;
+        d = fmin(d, C.rmax - sqrt(lx * lx + ly * ly));
+        if (!had_arrival) d = fmin(d, fabs(zdet - z));
+        lim = static_cast<R>(0.99 * d);
+        acc = R(0);
+    };
+
+    bool live = in_range && (flags & kFlagActive);
+    bool waiting = in_range && !(flags & kFlagBorn);
+    if (live && (do_fin || do_push)) {
+        if (!inside(C, x)) {       // prepare_ions_for_integration: outside -> inactive
+            live = false;
+            kill(t0);
+        } else {
+            new_limit();
+        }
+    }
+
+    // exact finalize of the current step (SimulationEngineLifecycle.cpp:123-195)
     auto finalize_step = [&]() {
-        if (p.do_finalize) {
+        // the unfused finalize call has no drift history: always exact
+        if (do_fin && (!FUSED || !(acc <= lim))) {
+            if (!FUSED && !do_push) zold = p.zprev[i];
+            const double ts = t_step();
             const double znew = x.gz();
             if (!had_arrival && zold < zdet && znew >= zdet) {
-                tarr = t + dt * ((zdet - zold) / (znew - zold));
+                tarr = ts + dt * ((zdet - zold) / (znew - zold));
                 had_arrival = true;
                 arr_now = true;
                 ++n_arr;
@@ -460,44 +525,48 @@ __global__ void __launch_bounds__(256) k_step(const __grid_constant__ StepParams
             if (ok) ok = x.finite() && isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]);
             if (!ok) {
                 live = false;
-                flags &= static_cast<uint8_t>(~kFlagActive);
-                tdeath = t;
-                dead_now = true;
-                ++n_dead;
+                kill(ts);
+            } else {
+                new_limit();
             }
         }
         ++kk;
-        t = t + dt;
+        if (kAccumT) t = t + dt;
+    };
+
+    auto cheap_step = [&]() {
+        if (waiting) {
+            if (t_step() >= birth) {      // prepare_ions_for_integration birth rule
+                waiting = false;
+                flags |= static_cast<uint8_t>(kFlagBorn | kFlagActive);
+                live = inside(C, x);
+                if (!live) kill(t_step());
+                else new_limit();
+            }
+        }
+        if (waiting || !live) {
+            ++kk;
+            if (kAccumT) t = t + dt;
+            return;
+        }
+        zold = x.gz();
+        if (!FUSED && do_push) p.zprev[i] = zold;
+        if (do_push) {
+            R l1;
+            if (INTEG == kBoris) l1 = boris<R, FIELD, MAG>(k, x, v, t_step());
+            else l1 = rk4<R, FIELD, MAG>(k, x, v, t_step());
+            acc += l1 * dt_r;
+        }
+        if (COLL != kCollNone && do_coll) pending = clock_tick<R>(k, v, S, U, gu, n_ovf);
+        if (!pending) finalize_step();
     };
 
     while (true) {
-        // cheap phase: one step for every lane that can step without a collision
-        if ((live || waiting) && !pending && kk < K) {
-            if (waiting) {
-                if (t >= birth) {      // prepare_ions_for_integration birth rule
-                    waiting = false;
-                    flags |= static_cast<uint8_t>(kFlagBorn | kFlagActive);
-                    live = inside(C, x);
-                    if (!live) {
-                        flags &= static_cast<uint8_t>(~kFlagActive);
-                        tdeath = t; dead_now = true; ++n_dead;
-                    }
-                }
-            }
-            if (waiting || !live) {
-                ++kk;
-                t = t + dt;
-            } else {
-                zold = x.gz();
-                if (p.do_push) {
-                    if (INTEG == kBoris) boris<R, FIELD, MAG>(k, x, v, t);
-                    else rk4<R, FIELD, MAG>(k, x, v, t);
-                }
-                if (COLL != kCollNone && p.do_collide) {
-                    pending = clock_tick<R>(k, v, S, U, gu, n_ovf);
-                }
-                if (!pending) finalize_step();
-            }
+        // cheap phase: up to kCheapStepsPerVote steps for every lane that can
+        // step without a collision
+#pragma unroll 1
+        for (int j = 0; j < kCheapStepsPerVote; ++j) {
+            if ((live || waiting) && !pending && kk < K) cheap_step();
         }
         const unsigned pend_mask = __ballot_sync(0xffffffffu, pending);
         const unsigned run_mask = __ballot_sync(0xffffffffu, (live || waiting) && !pending && kk < K);
@@ -505,7 +574,7 @@ __global__ void __launch_bounds__(256) k_step(const __grid_constant__ StepParams
             (run_mask == 0u || static_cast<uint32_t>(__popc(pend_mask)) >= p.pend_threshold)) {
             if (pending) {
                 ++n_cand;
-                if (candidate<R>(k, v, S, U, gu, p.seed, id, step0 + kk)) ++n_coll;
+                if (candidate<R>(C, v, S, U, gu, m, p.seed, id, step0 + kk)) ++n_coll;
                 pending = false;
                 finalize_step();
             }
