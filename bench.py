@@ -233,7 +233,7 @@ def run_ours(args) -> None:
     def make_sim(prec, K=args.steps_per_launch):
         s = Simulation([ens], precision=prec, integrator=capi.INTEGRATOR_BORIS, collision=capi.COLLISION_HSS,
                        rng_seed=123, device=dev, steps_per_launch=K, block_size=args.block,
-                       pending_threshold=args.pending)
+                       pending_threshold=args.pending, steps_per_vote=args.spv)
         s.set_stream(stream.cuda_stream)
         s.upload(st0, first_id=first_id)
         return s
@@ -384,6 +384,7 @@ def main():
     ap.add_argument("--steps-per-launch", type=int, default=1000)
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--pending", type=int, default=0)
+    ap.add_argument("--spv", type=int, default=0, help="collision-free steps between warp votes")
     ap.add_argument("--fp64-steps", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")

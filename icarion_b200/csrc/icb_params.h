@@ -75,7 +75,7 @@ struct StepParams {
     uint32_t pend_threshold;
     uint32_t ens_base;                 // global index of this chunk's ensemble 0
     uint32_t n_ens;
-    uint32_t do_push, do_collide, do_finalize, pad;
+    uint32_t do_push, do_collide, do_finalize, steps_per_vote;
     uint64_t ens_off[kMaxLaunchEns + 1];  // absolute ion offsets of the chunk's ensembles
     EnsConst ens[kMaxLaunchEns];
 };

@@ -140,8 +140,7 @@ struct Consts {
     R q, m, qm, inv_m;
     double dt;
     R h;                     // dt/2 in working precision
-    R A, mean_th, sig_n, ug[3];
-    R mi, mn, inv_mt, fac;
+    R A, mean_th, ug[3];     // collision clock
 };
 
 template <class R, int FIELD, bool MAG>
@@ -161,10 +160,24 @@ __device__ void load_consts(Consts<R>& k, const EnsConst& C, double q, double m)
     k.h = static_cast<R>(C.dt * 0.5);
     k.q = static_cast<R>(q);
     k.m = static_cast<R>(m);
-    // Reference: qm = charge / mass; t = B * (qm * dt * 0.5); s = 2 t / (1 + t^2).
-    const double qm = q / m;
+    // Reference: qm = charge / mass; t = B * (qm * dt * 0.5); s = 2 t / (1 + t^2);
+    // uniform field a = (E * q) / m (ElectricFieldForce.cpp:66-83,
+    // BorisStrategy.cpp:50), constant for the whole launch.  FP64 keeps the
+    // reference's divisions; the float paths use one reciprocal.
+    double qm, inv_m;
+    if constexpr (sizeof(R) == 8) {
+        qm = q / m;
+        inv_m = 1.0 / m;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) k.a_uni[a] = static_cast<R>((C.E0[a] * q) / m);
+    } else {
+        inv_m = 1.0 / m;
+        qm = q * inv_m;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) k.a_uni[a] = static_cast<R>((C.E0[a] * q) * inv_m);
+    }
     k.qm = static_cast<R>(qm);
-    k.inv_m = static_cast<R>(1.0 / m);
+    k.inv_m = static_cast<R>(inv_m);
     if (MAG) {
         const double ts = qm * C.dt * 0.5;
         const double tv0 = C.B[0] * ts, tv1 = C.B[1] * ts, tv2 = C.B[2] * ts;
@@ -173,18 +186,8 @@ __device__ void load_consts(Consts<R>& k, const EnsConst& C, double q, double m)
         k.tv[0] = static_cast<R>(tv0); k.tv[1] = static_cast<R>(tv1); k.tv[2] = static_cast<R>(tv2);
         k.sv[0] = static_cast<R>(tv0 * sf); k.sv[1] = static_cast<R>(tv1 * sf); k.sv[2] = static_cast<R>(tv2 * sf);
     }
-    // Uniform field: F = E * q, a = F / m (ElectricFieldForce.cpp:66-83,
-    // BorisStrategy.cpp:50), constant for the whole launch.
-#pragma unroll
-    for (int a = 0; a < 3; ++a) k.a_uni[a] = static_cast<R>((C.E0[a] * q) / m);
     k.A = static_cast<R>(C.A);
     k.mean_th = static_cast<R>(C.mean_th);
-    k.sig_n = static_cast<R>(C.sig_n);
-    k.mi = static_cast<R>(m);
-    k.mn = static_cast<R>(C.m_gas);
-    const double inv = 1.0 / (m + C.m_gas);
-    k.inv_mt = static_cast<R>(inv);
-    k.fac = static_cast<R>(C.m_gas * inv);
 }
 
 // ---- fields -----------------------------------------------------------------
@@ -401,7 +404,6 @@ __device__ __forceinline__ unsigned long long warp_sum_u32(uint32_t v) {
 // crossed) detector plane (lim).  The L1 length bounds the true path, so no
 // exit or crossing is missed; NaN or Inf makes acc non-finite and forces the
 // check.  Float accumulation error over <= 16384 steps per launch is < 0.1%.
-constexpr int kCheapStepsPerVote = 4;
 
 template <int PREC>
 struct KernelShape { static constexpr int kMinBlocks = 6; };
@@ -485,8 +487,12 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
         dead_now = true;
         ++n_dead;
     };
+    // Short launches (the per-step form) check exactly every step instead of
+    // setting up a displacement budget (lim stays 0).
+    const bool budget = FUSED && K >= 8;
     // distance to the nearest wall, end face or pending detector plane
     auto new_limit = [&]() {
+        if (!budget) return;
         const double z = x.gz();
         const double lz = z - C.oz;
         double d = fmin(lz + 1e-12, C.zmax_local - lz);
@@ -562,10 +568,10 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
     };
 
     while (true) {
-        // cheap phase: up to kCheapStepsPerVote steps for every lane that can
+        // cheap phase: up to steps_per_vote steps for every lane that can
         // step without a collision
 #pragma unroll 1
-        for (int j = 0; j < kCheapStepsPerVote; ++j) {
+        for (uint32_t j = 0; j < p.steps_per_vote; ++j) {
             if ((live || waiting) && !pending && kk < K) cheap_step();
         }
         const unsigned pend_mask = __ballot_sync(0xffffffffu, pending);

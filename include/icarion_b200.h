@@ -109,7 +109,8 @@ typedef struct icb_config {
     int32_t steps_per_launch;  /* steps fused per kernel launch, 0 = default */
     int32_t pending_threshold; /* deferred-collision batch size per warp, 0 = default */
     int32_t use_graphs;        /* capture launch sequences in CUDA graphs */
-    int32_t reserved[7];
+    int32_t steps_per_vote;    /* collision-free steps between warp votes, 0 = default */
+    int32_t reserved[6];
 } icb_config;
 
 #define ICB_MAX_ENSEMBLES 256
