@@ -339,6 +339,11 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
         C.mean_th = C.sig_n * kMeanChi3;
         C.m_gas = P.gas_mass_kg;
         for (int a = 0; a < 3; ++a) C.ug[a] = P.gas_velocity_m_s[a];
+        C.fA = static_cast<float>(C.A);
+        C.fmean_th = static_cast<float>(C.mean_th);
+        C.fsig_n = static_cast<float>(C.sig_n);
+        C.fm_gas = static_cast<float>(C.m_gas);
+        for (int a = 0; a < 3; ++a) C.fug[a] = static_cast<float>(C.ug[a]);
     }
     C.zdet = P.detector_z_m;
     return ICB_OK;

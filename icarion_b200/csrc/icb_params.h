@@ -48,6 +48,10 @@ struct EnsConst {
     double zdet;
     int32_t magnetic;
     int32_t rf;
+    // float copies for the float collision path
+    float fA, fmean_th, fsig_n, fm_gas;
+    float fug[3];
+    float pad_;
 };
 
 struct StepParams {

@@ -12,7 +12,8 @@
 // Precision policies:
 //   FP64       double everywhere.  Compiled without FMA contraction so that
 //              the collision-free push is bit-identical to the reference.
-//   MIXED      float velocity, field, collision; double position and time.
+//   MIXED      float velocity, field, collision; position = double anchor +
+//              float offset (folded into the anchor every ~4 um of path).
 //   HILO       float velocity; position as a compensated float hi/lo pair.
 //
 // Deferred collisions.  A collision candidate fires in ~10% of ion-steps;
@@ -26,6 +27,7 @@
 #pragma once
 #include <cstdint>
 #include <cmath>
+#include <type_traits>
 #include "icb_params.h"
 #include "icb_rng.cuh"
 
@@ -43,15 +45,25 @@ __device__ __forceinline__ double m_log(double x) { return log(x); }
 __device__ __forceinline__ float m_log(float x) { return __logf(x); }
 __device__ __forceinline__ double m_expm1(double x) { return expm1(x); }
 __device__ __forceinline__ float m_expm1(float x) { return expm1f(x); }
-__device__ __forceinline__ double m_cos(double x) { return cos(x); }
 __device__ __forceinline__ double m_fmax(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ float m_fmax(float a, float b) { return fmaxf(a, b); }
-__device__ __forceinline__ double unit(uint32_t w, double) { return unit_d(w); }
-__device__ __forceinline__ float unit(uint32_t w, float) { return unit_f(w); }
 
-// (cos, sin) of the angle 2*pi*u.  FP64 keeps the oracle's 2*pi*u; the
-// float path uses the equally uniform angle 2*pi*(u - 1/2) in (-pi, pi],
-// the accurate range of the hardware sin/cos.
+// Uniforms from Philox words.  FP64: (w + 1) 2^-32 in (0, 1] and, for a
+// 16-bit half k, (k + 1/2) 2^-16 -- the oracle's conversions.  Float: the
+// same intervals built from the exponent field (no int->float convert):
+// 23-bit words in (0, 1] and the identical (k + 1/2) 2^-16 halves.
+__device__ __forceinline__ double u32(uint32_t w, double) { return unit_d(w); }
+__device__ __forceinline__ float u32(uint32_t w, float) {
+    return 2.0f - __uint_as_float(0x3f800000u | (w >> 9));
+}
+__device__ __forceinline__ double u16(uint32_t k, double) { return (static_cast<double>(k) + 0.5) * 1.52587890625e-05; }
+__device__ __forceinline__ float u16(uint32_t k, float) {
+    return __uint_as_float(0x3f800000u | (k << 7)) - 0.99999237060546875f;
+}
+
+// (cos, sin) of a uniform angle.  FP64 uses 2*pi*u like the oracle; the
+// float path uses the equally uniform 2*pi*(u - 1/2) in (-pi, pi], the
+// accurate range of the hardware sin/cos.
 __device__ __forceinline__ void angle_cs(double u, double& c, double& s) {
     const double ph = 2.0 * 3.14159265358979323846 * u;
     c = cos(ph);
@@ -62,14 +74,19 @@ __device__ __forceinline__ void angle_cs(float u, float& c, float& s) {
 }
 
 // ---- positions --------------------------------------------------------------
-// Double position (FP64 and MIXED).
+// Double position (FP64).
 struct PosD {
+    static constexpr double kFoldLimit = 1e300;
+    using Snap = double;
     double x, y, z;
     __device__ void load(const StepParams& p, uint64_t i) { x = p.x[i]; y = p.y[i]; z = p.z[i]; }
     __device__ void store(const StepParams& p, uint64_t i) const { p.x[i] = x; p.y[i] = y; p.z[i] = z; }
     __device__ double gx() const { return x; }
     __device__ double gy() const { return y; }
     __device__ double gz() const { return z; }
+    __device__ Snap snap_z() const { return z; }
+    __device__ double z_of(Snap s) const { return s; }
+    __device__ void fold() {}
     template <class R> __device__ R rel(int a, double c) const {
         const double v = (a == 0) ? x : (a == 1) ? y : z;
         return static_cast<R>(v - c);
@@ -77,12 +94,45 @@ struct PosD {
     __device__ void drift(double vx, double vy, double vz, double dt) {
         x += vx * dt; y += vy * dt; z += vz * dt;
     }
-    __device__ void drift(float vx, float vy, float vz, double dt) {
-        x = fma(static_cast<double>(vx), dt, x);
-        y = fma(static_cast<double>(vy), dt, y);
-        z = fma(static_cast<double>(vz), dt, z);
-    }
     __device__ bool finite() const { return isfinite(x) && isfinite(y) && isfinite(z); }
+};
+
+// Double anchor + float offset (MIXED).  A step adds v*dt to the float
+// offset (one FFMA per axis, no conversion); the offset is folded into the
+// anchor at the lane's exact checks, which the displacement budget forces
+// at least every kFoldLimit metres of path, so the offset stays below
+// ~4 um and its rounding below ~2e-13 m per step.
+struct PosA {
+    static constexpr double kFoldLimit = 3.814697265625e-06;   // 2^-18 m
+    using Snap = float;
+    double ax, ay, az;
+    float dx, dy, dz;
+    __device__ void load(const StepParams& p, uint64_t i) {
+        ax = p.x[i]; ay = p.y[i]; az = p.z[i];
+        dx = dy = dz = 0.0f;
+    }
+    __device__ void store(const StepParams& p, uint64_t i) const { p.x[i] = gx(); p.y[i] = gy(); p.z[i] = gz(); }
+    __device__ double gx() const { return ax + static_cast<double>(dx); }
+    __device__ double gy() const { return ay + static_cast<double>(dy); }
+    __device__ double gz() const { return az + static_cast<double>(dz); }
+    __device__ Snap snap_z() const { return dz; }
+    __device__ double z_of(Snap s) const { return az + static_cast<double>(s); }
+    __device__ void fold() {
+        ax += static_cast<double>(dx); ay += static_cast<double>(dy); az += static_cast<double>(dz);
+        dx = dy = dz = 0.0f;
+    }
+    template <class R> __device__ R rel(int a, double c) const {
+        const double an = (a == 0) ? ax : (a == 1) ? ay : az;
+        const float d = (a == 0) ? dx : (a == 1) ? dy : dz;
+        return static_cast<R>(static_cast<float>(an - c) + d);
+    }
+    __device__ void drift(float vx, float vy, float vz, double dt) {
+        const float d = static_cast<float>(dt);
+        dx = fmaf(vx, d, dx); dy = fmaf(vy, d, dy); dz = fmaf(vz, d, dz);
+    }
+    __device__ bool finite() const {
+        return isfinite(ax) && isfinite(ay) && isfinite(az) && isfinite(dx) && isfinite(dy) && isfinite(dz);
+    }
 };
 
 // Compensated float pair: value = hi + lo, |lo| <= ulp(hi)/2.
@@ -96,7 +146,11 @@ __device__ __forceinline__ void two_sum_acc(float& hi, float& lo, float d) {
     hi = h2;
 }
 
+// Compensated float hi/lo position (HILO), TwoSum update (Knuth, TAOCP
+// vol. 2, 4.2.2).
 struct PosHL {
+    static constexpr double kFoldLimit = 1e300;
+    using Snap = double;
     float xh, xl, yh, yl, zh, zl;
     __device__ void load(const StepParams& p, uint64_t i) {
         xh = p.xh[i]; xl = p.xl[i]; yh = p.yh[i]; yl = p.yl[i]; zh = p.zh[i]; zl = p.zl[i];
@@ -107,6 +161,9 @@ struct PosHL {
     __device__ double gx() const { return static_cast<double>(xh) + static_cast<double>(xl); }
     __device__ double gy() const { return static_cast<double>(yh) + static_cast<double>(yl); }
     __device__ double gz() const { return static_cast<double>(zh) + static_cast<double>(zl); }
+    __device__ Snap snap_z() const { return gz(); }
+    __device__ double z_of(Snap s) const { return s; }
+    __device__ void fold() {}
     template <class R> __device__ R rel(int a, double c) const {
         const float h = (a == 0) ? xh : (a == 1) ? yh : zh;
         const float l = (a == 0) ? xl : (a == 1) ? yl : zl;
@@ -125,22 +182,25 @@ struct PosHL {
     }
 };
 
-template <int PREC> struct PosOf { using T = PosD; };
+template <int PREC> struct PosOf;
+template <> struct PosOf<kPrecFP64> { using T = PosD; };
+template <> struct PosOf<kPrecMixed> { using T = PosA; };
 template <> struct PosOf<kPrecHiLo> { using T = PosHL; };
 
-// ---- per-thread copy of the ensemble constants in the working precision --
+// ---- per-thread constants in the working precision ------------------------
 template <class R>
 struct Consts {
     R E0[3], G[3];
     double c[3];
     R rfU0, rfV, r0sq;
     double rfw;
-    R tv[3], sv[3];          // Boris rotation vectors for this ion
+    R tv[3], sv[3];          // Boris rotation vectors (RK4: B itself in tv)
     R a_uni[3];              // acceleration of a uniform field for this ion
-    R q, m, qm, inv_m;
+    R q, qm, inv_m;
+    double m;
     double dt;
     R h;                     // dt/2 in working precision
-    R A, mean_th, ug[3];     // collision clock
+    R A, Amean, ug[3];       // collision clock: Q = A |v - u| + A <|th|>
 };
 
 template <class R, int FIELD, bool MAG>
@@ -159,7 +219,7 @@ __device__ void load_consts(Consts<R>& k, const EnsConst& C, double q, double m)
     k.dt = C.dt;
     k.h = static_cast<R>(C.dt * 0.5);
     k.q = static_cast<R>(q);
-    k.m = static_cast<R>(m);
+    k.m = m;
     // Reference: qm = charge / mass; t = B * (qm * dt * 0.5); s = 2 t / (1 + t^2);
     // uniform field a = (E * q) / m (ElectricFieldForce.cpp:66-83,
     // BorisStrategy.cpp:50), constant for the whole launch.  FP64 keeps the
@@ -187,7 +247,7 @@ __device__ void load_consts(Consts<R>& k, const EnsConst& C, double q, double m)
         k.sv[0] = static_cast<R>(tv0 * sf); k.sv[1] = static_cast<R>(tv1 * sf); k.sv[2] = static_cast<R>(tv2 * sf);
     }
     k.A = static_cast<R>(C.A);
-    k.mean_th = static_cast<R>(C.mean_th);
+    k.Amean = static_cast<R>(C.A * C.mean_th);
 }
 
 // ---- fields -----------------------------------------------------------------
@@ -198,7 +258,7 @@ __device__ __forceinline__ void efield(const Consts<R>& k, const Pos& x, double 
         return;
     } else {
 #pragma unroll
-    for (int a = 0; a < 3; ++a) E[a] = k.E0[a] + k.G[a] * x.template rel<R>(a, k.c[a]);
+        for (int a = 0; a < 3; ++a) E[a] = k.E0[a] + k.G[a] * x.template rel<R>(a, k.c[a]);
     }
     if constexpr (FIELD == kFieldLinearRF) {
         // AnalyticalFieldModel.cpp:152-158: U = dc_quad + V cos(w t);
@@ -216,14 +276,14 @@ __device__ __forceinline__ void efield(const Consts<R>& k, const Pos& x, double 
 template <class R, int FIELD, bool MAG, class Pos>
 __device__ __forceinline__ R boris(const Consts<R>& k, Pos& x, R v[3], double t) {
     R a[3];
-    if (FIELD == kFieldUniform) {
+    if constexpr (FIELD == kFieldUniform) {
         a[0] = k.a_uni[0]; a[1] = k.a_uni[1]; a[2] = k.a_uni[2];
     } else {
         R E[3];
         efield<R, FIELD>(k, x, t, E);
-        if (sizeof(R) == 8) {
+        if constexpr (sizeof(R) == 8) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) a[c] = (E[c] * k.q) / k.m;
+            for (int c = 0; c < 3; ++c) a[c] = (E[c] * k.q) / static_cast<R>(k.m);
         } else {
 #pragma unroll
             for (int c = 0; c < 3; ++c) a[c] = E[c] * k.qm;
@@ -233,7 +293,7 @@ __device__ __forceinline__ R boris(const Consts<R>& k, Pos& x, R v[3], double t)
 #pragma unroll
     for (int c = 0; c < 3; ++c) vm[c] = v[c] + a[c] * k.h;
     R vp[3];
-    if (MAG) {
+    if constexpr (MAG) {
         const R c1x = vm[1] * k.tv[2] - vm[2] * k.tv[1];
         const R c1y = vm[2] * k.tv[0] - vm[0] * k.tv[2];
         const R c1z = vm[0] * k.tv[1] - vm[1] * k.tv[0];
@@ -259,8 +319,8 @@ __device__ __forceinline__ void rk4_acc(const Consts<R>& k, const Pos& x, const 
     R E[3];
     efield<R, FIELD>(k, x, t, E);
     R F[3] = {E[0] * k.q, E[1] * k.q, E[2] * k.q};
-    if (MAG) {
-        const R B0 = k.tv[0], B1 = k.tv[1], B2 = k.tv[2];  // holds B itself for RK4 (see load)
+    if constexpr (MAG) {
+        const R B0 = k.tv[0], B1 = k.tv[1], B2 = k.tv[2];
         const R cx = v[1] * B2 - v[2] * B1;
         const R cy = v[2] * B0 - v[0] * B2;
         const R cz = v[0] * B1 - v[1] * B0;
@@ -270,7 +330,8 @@ __device__ __forceinline__ void rk4_acc(const Consts<R>& k, const Pos& x, const 
     for (int c = 0; c < 3; ++c) acc[c] = F[c] * k.inv_m;
 }
 
-// Returns the L1 norm of the step's displacement divided by dt.
+// RK4 batch stages (RK4Strategy.cpp:255-358).  Returns the L1 norm of the
+// step's displacement divided by dt.
 template <class R, int FIELD, bool MAG, class Pos>
 __device__ __forceinline__ R rk4(const Consts<R>& k, Pos& x, R v[3], double t) {
     const double dt = k.dt;
@@ -305,83 +366,99 @@ __device__ __forceinline__ R rk4(const Consts<R>& k, Pos& x, R v[3], double t) {
 }
 
 // ---- null-collision HSS -------------------------------------------------------
-// Clock update after the push.  Returns true when a candidate fires.
+// The reference draws a Maxwell-Boltzmann neutral every step and collides
+// with probability p = 1 - exp(-n sigma |v - v_n| dt).  Here each step has a
+// candidate with probability Q = A (b + <|th|>) (A = n sigma dt, b >= |v - u|,
+// th = v_n - u the neutral's thermal part); a candidate draws th from
+// f(th) (b + |th|) / (b + <|th|>) and is accepted with p / (A (b + |th|)) <= 1,
+// so the joint law of (collision, v_n) per step is f(v_n) p, the reference's.
+// The mixture is sampled without branches: |th|^2/sigma^2 = -2 ln u1 -
+// 2 ln u2 * s with s = cos^2(2 pi u3) (chi^2_3, the thermal part, probability
+// b/(b+<|th|>)) or s = 1 (chi^2_4, the |th|-weighted part), and an isotropic
+// direction.
+//
+// FP64 uses b = |v - u| (exact sqrt, as the oracle).  The float path uses
+// the sqrt-free bound b = (w^2 + c^2) / (2c) >= |w| (AM-GM), c = |w| at the
+// lane's last candidate, which keeps Q within ~0.1% of the tight value.
 template <class R>
-__device__ __forceinline__ bool clock_tick(const Consts<R>& k, const R v[3], R& S, R U, R& gu, uint32_t& ovf) {
+struct ClockBound {
+    R inv2c, halfc;      // b = w2 * inv2c + halfc  (float path)
+    __device__ void set(R w2) {
+        const R c = m_fmax(m_sqrt(w2), R(1e-3));
+        inv2c = R(0.5) / c;
+        halfc = R(0.5) * c;
+    }
+};
+
+template <class R>
+__device__ __forceinline__ bool clock_tick(const Consts<R>& k, const R v[3], R& S, R U, R& b,
+                                           const ClockBound<R>& cb, uint32_t& ovf) {
     const R wx = v[0] - k.ug[0], wy = v[1] - k.ug[1], wz = v[2] - k.ug[2];
-    gu = m_sqrt(wx * wx + wy * wy + wz * wz);
-    R Q = k.A * (gu + k.mean_th);
+    const R w2 = wx * wx + wy * wy + wz * wz;
+    if constexpr (sizeof(R) == 8) b = m_sqrt(w2);
+    else b = w2 * cb.inv2c + cb.halfc;
+    R Q = k.A * b + k.Amean;
     if (Q > R(1)) { Q = R(1); ++ovf; }
     S = S - S * Q;
     return S < U;
 }
 
-// Candidate processing (the same steps as the oracle's hss_nullcoll).
-// Returns true when the collision is accepted (v updated).
+// Candidate processing (the steps of the oracle's hss_nullcoll).  Returns
+// true when the collision is accepted (v updated).
 template <class R>
-__device__ __forceinline__ bool candidate(const EnsConst& C, R v[3], R& S, R& U, R gu, double mi_d,
+__device__ __forceinline__ bool candidate(const EnsConst& C, R v[3], R& S, R& U, R b, double mi_d,
                                           uint64_t seed, uint32_t id, uint32_t step) {
-    struct {
-        R A, mean_th, sig_n, ug[3], mi, mn, inv_mt, fac;
-    } k;
-    k.A = static_cast<R>(C.A);
-    k.mean_th = static_cast<R>(C.mean_th);
-    k.sig_n = static_cast<R>(C.sig_n);
-    k.ug[0] = static_cast<R>(C.ug[0]); k.ug[1] = static_cast<R>(C.ug[1]); k.ug[2] = static_cast<R>(C.ug[2]);
-    k.mi = static_cast<R>(mi_d);
-    k.mn = static_cast<R>(C.m_gas);
-    const double inv = 1.0 / (mi_d + C.m_gas);
-    k.inv_mt = static_cast<R>(inv);
-    k.fac = static_cast<R>(C.m_gas * inv);
+    R A, mean_th, sig_n, ug[3], mi, mn, inv_mt, fac;
+    if constexpr (sizeof(R) == 8) {
+        A = C.A; mean_th = C.mean_th; sig_n = C.sig_n;
+        ug[0] = C.ug[0]; ug[1] = C.ug[1]; ug[2] = C.ug[2];
+        mi = mi_d; mn = C.m_gas;
+        inv_mt = 1.0 / (mi_d + C.m_gas);
+        fac = mn * inv_mt;
+    } else {
+        A = C.fA; mean_th = C.fmean_th; sig_n = C.fsig_n;
+        ug[0] = C.fug[0]; ug[1] = C.fug[1]; ug[2] = C.fug[2];
+        mi = static_cast<float>(mi_d); mn = C.fm_gas;
+        inv_mt = __frcp_rn(mi + mn);
+        fac = mn * inv_mt;
+    }
     const uint32_t k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32);
     const U4 r0 = philox4x32_10(id, step, 0u, 0u, k0, k1);
     const U4 r1 = philox4x32_10(id, step, 1u, 0u, k0, k1);
-    U = unit(r0.x, R(0));
+    U = u32(r0.x, R(0));
     S = R(1);
-    R th[3];
-    if (unit(r0.y, R(0)) * (gu + k.mean_th) < gu) {
-        const R ra = m_sqrt(R(-2.0) * m_log(unit(r1.x, R(0))));
-        const R rb = m_sqrt(R(-2.0) * m_log(unit(r1.z, R(0))));
-        R ca, sa, cb, sb;
-        angle_cs(unit(r1.y, R(0)), ca, sa);
-        angle_cs(unit(r1.w, R(0)), cb, sb);
-        th[0] = k.sig_n * (ra * ca);
-        th[1] = k.sig_n * (ra * sa);
-        th[2] = k.sig_n * (rb * cb);
-    } else {
-        const R rad = k.sig_n * m_sqrt(R(-2.0) * m_log(unit(r1.x, R(0)) * unit(r1.y, R(0))));
-        const R ct = R(2.0) * unit(r1.z, R(0)) - R(1.0);
-        const R st = m_sqrt(m_fmax(R(0), R(1.0) - ct * ct));
-        R cp, sp;
-        angle_cs(unit(r1.w, R(0)), cp, sp);
-        th[0] = rad * (st * cp);
-        th[1] = rad * (st * sp);
-        th[2] = rad * ct;
-    }
-    const R thm = m_sqrt(th[0] * th[0] + th[1] * th[1] + th[2] * th[2]);
-    const R vn[3] = {k.ug[0] + th[0], k.ug[1] + th[1], k.ug[2] + th[2]};
-    const R gx = v[0] - vn[0], gy = v[1] - vn[1], gz = v[2] - vn[2];
-    const R g = m_sqrt(gx * gx + gy * gy + gz * gz);
-    const R q = k.A * (gu + thm);
-    const R pc = -m_expm1(-k.A * g);
-    if (!(unit(r0.z, R(0)) * q < pc)) return false;
-    const U4 r2 = philox4x32_10(id, step, 2u, 0u, k0, k1);
-    const R ct = R(2.0) * unit(r0.w, R(0)) - R(1.0);
+    const bool thermal = u32(r0.y, R(0)) * (b + mean_th) < b;
+    R c3, s3;
+    angle_cs(u16(r1.y >> 16, R(0)), c3, s3);
+    const R sfac = thermal ? c3 * c3 : R(1);
+    const R r2 = R(-2.0) * (m_log(u32(r0.w, R(0))) + m_log(u32(r1.x, R(0))) * sfac);
+    const R rad = sig_n * m_sqrt(r2);
+    const R ct = R(2.0) * u16(r1.y & 0xffffu, R(0)) - R(1.0);
     const R st = m_sqrt(m_fmax(R(0), R(1.0) - ct * ct));
     R cp, sp;
-    angle_cs(unit(r2.x, R(0)), cp, sp);
-    const R dir[3] = {st * cp, st * sp, ct};
+    angle_cs(u16(r1.z >> 16, R(0)), cp, sp);
+    const R vn[3] = {ug[0] + rad * (st * cp), ug[1] + rad * (st * sp), ug[2] + rad * ct};
+    const R gx = v[0] - vn[0], gy = v[1] - vn[1], gz = v[2] - vn[2];
+    const R g = m_sqrt(gx * gx + gy * gy + gz * gz);
+    const R q = A * (b + rad);
+    const R pc = -m_expm1(-A * g);
+    if (!(u32(r0.z, R(0)) * q < pc)) return false;
+    const R ct2 = R(2.0) * u16(r1.z & 0xffffu, R(0)) - R(1.0);
+    const R st2 = m_sqrt(m_fmax(R(0), R(1.0) - ct2 * ct2));
+    R cp2, sp2;
+    angle_cs(u16(r1.w >> 16, R(0)), cp2, sp2);
+    const R dir[3] = {st2 * cp2, st2 * sp2, ct2};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const R vcom = (v[c] * k.mi + vn[c] * k.mn) * k.inv_mt;
-        v[c] = vcom + (dir[c] * g) * k.fac;
+        const R vcom = (v[c] * mi + vn[c] * mn) * inv_mt;
+        v[c] = vcom + (dir[c] * g) * fac;
     }
     return true;
 }
 
 // ---- finalize ------------------------------------------------------------------
 // CylindricalGeometry::contains (CylindricalGeometry.h:35-40) on the global
-// position; returns false for positions outside or non-finite.
+// position; false for positions outside or non-finite.
 template <class Pos>
 __device__ __forceinline__ bool inside(const EnsConst& C, const Pos& x) {
     const double lz = x.gz() - C.oz;
@@ -403,8 +480,7 @@ __device__ __forceinline__ unsigned long long warp_sum_u32(uint32_t v) {
 // may exceed 99% of the distance to the nearest wall, end face or (not yet
 // crossed) detector plane (lim).  The L1 length bounds the true path, so no
 // exit or crossing is missed; NaN or Inf makes acc non-finite and forces the
-// check.  Float accumulation error over <= 16384 steps per launch is < 0.1%.
-
+// check.  Float accumulation error over <= kMaxStepsPerLaunch steps is < 0.1%.
 template <int PREC>
 struct KernelShape { static constexpr int kMinBlocks = 6; };
 template <>
@@ -414,6 +490,7 @@ template <int PREC, int INTEG, int COLL, int FIELD, bool MAG, bool FUSED>
 __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(const __grid_constant__ StepParams p) {
     using R = typename PrecT<PREC>::R;
     using Pos = typename PosOf<PREC>::T;
+    using Snap = typename Pos::Snap;
     // FP64 keeps the engine clock as the accumulated sum t += dt (bit-exact
     // death and arrival times); the float paths form t = t0 + k*dt when an
     // event needs it, unless the field itself is time dependent.
@@ -459,8 +536,12 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
     Consts<R> k;
     load_consts<R, FIELD, MAG>(k, C, q, m);
     if (INTEG == kRK4 && MAG) {
-        // rk4_acc reads B from tv[] (no rotation vectors needed for RK4).
         k.tv[0] = static_cast<R>(C.B[0]); k.tv[1] = static_cast<R>(C.B[1]); k.tv[2] = static_cast<R>(C.B[2]);
+    }
+    ClockBound<R> cb;
+    if constexpr (sizeof(R) == 4) {
+        const R wx = v[0] - k.ug[0], wy = v[1] - k.ug[1], wz = v[2] - k.ug[2];
+        cb.set(wx * wx + wy * wy + wz * wz);
     }
 
     const uint32_t id = static_cast<uint32_t>(p.first_id + i);
@@ -476,8 +557,8 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
     const uint32_t K = p.n_steps;
     uint32_t kk = 0;
     bool pending = false;
-    R gu = R(0);
-    double zold = 0.0;
+    R b = R(0);
+    Snap zold{};
     R acc = R(0), lim = R(0);
 
     auto t_step = [&]() -> double { return kAccumT ? t : fma(static_cast<double>(kk), dt, t0); };
@@ -499,7 +580,8 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
         const double lx = x.gx() - C.ox, ly = x.gy() - C.oy;
         d = fmin(d, C.rmax - sqrt(lx * lx + ly * ly));
         if (!had_arrival) d = fmin(d, fabs(zdet - z));
-        lim = static_cast<R>(0.99 * d);
+        d = fmin(0.99 * d, Pos::kFoldLimit);
+        lim = static_cast<R>(d);
         acc = R(0);
     };
 
@@ -518,11 +600,13 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
     auto finalize_step = [&]() {
         // the unfused finalize call has no drift history: always exact
         if (do_fin && (!FUSED || !(acc <= lim))) {
-            if (!FUSED && !do_push) zold = p.zprev[i];
+            double zo = x.z_of(zold);
+            if (!FUSED && !do_push) zo = p.zprev[i];
+            x.fold();
             const double ts = t_step();
             const double znew = x.gz();
-            if (!had_arrival && zold < zdet && znew >= zdet) {
-                tarr = ts + dt * ((zdet - zold) / (znew - zold));
+            if (!had_arrival && zo < zdet && znew >= zdet) {
+                tarr = ts + dt * ((zdet - zo) / (znew - zo));
                 had_arrival = true;
                 arr_now = true;
                 ++n_arr;
@@ -540,54 +624,70 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
         if (kAccumT) t = t + dt;
     };
 
-    auto cheap_step = [&]() {
-        if (waiting) {
-            if (t_step() >= birth) {      // prepare_ions_for_integration birth rule
-                waiting = false;
-                flags |= static_cast<uint8_t>(kFlagBorn | kFlagActive);
-                live = inside(C, x);
-                if (!live) kill(t_step());
-                else new_limit();
-            }
-        }
-        if (waiting || !live) {
-            ++kk;
-            if (kAccumT) t = t + dt;
-            return;
-        }
-        zold = x.gz();
-        if (!FUSED && do_push) p.zprev[i] = zold;
+    // one collision-free step (or a step that leaves the lane pending)
+    auto push_and_tick = [&]() {
+        zold = x.snap_z();
+        if (!FUSED && do_push) p.zprev[i] = x.z_of(zold);
         if (do_push) {
             R l1;
             if (INTEG == kBoris) l1 = boris<R, FIELD, MAG>(k, x, v, t_step());
             else l1 = rk4<R, FIELD, MAG>(k, x, v, t_step());
             acc += l1 * dt_r;
         }
-        if (COLL != kCollNone && do_coll) pending = clock_tick<R>(k, v, S, U, gu, n_ovf);
+        if (COLL != kCollNone && do_coll) pending = clock_tick<R>(k, v, S, U, b, cb, n_ovf);
         if (!pending) finalize_step();
     };
 
-    while (true) {
-        // cheap phase: up to steps_per_vote steps for every lane that can
-        // step without a collision
+    auto run = [&](auto births) {
+        constexpr bool kBirths = decltype(births)::value;
+        while (true) {
+            // cheap phase: up to steps_per_vote steps for every lane that can
+            // step without a collision
 #pragma unroll 1
-        for (uint32_t j = 0; j < p.steps_per_vote; ++j) {
-            if ((live || waiting) && !pending && kk < K) cheap_step();
-        }
-        const unsigned pend_mask = __ballot_sync(0xffffffffu, pending);
-        const unsigned run_mask = __ballot_sync(0xffffffffu, (live || waiting) && !pending && kk < K);
-        if (pend_mask != 0u &&
-            (run_mask == 0u || static_cast<uint32_t>(__popc(pend_mask)) >= p.pend_threshold)) {
-            if (pending) {
-                ++n_cand;
-                if (candidate<R>(C, v, S, U, gu, m, p.seed, id, step0 + kk)) ++n_coll;
-                pending = false;
-                finalize_step();
+            for (uint32_t j = 0; j < p.steps_per_vote; ++j) {
+                if constexpr (kBirths) {
+                    if (!((live || waiting) && !pending && kk < K)) continue;
+                    if (waiting) {
+                        if (t_step() >= birth) {      // prepare_ions_for_integration birth rule
+                            waiting = false;
+                            flags |= static_cast<uint8_t>(kFlagBorn | kFlagActive);
+                            live = inside(C, x);
+                            if (!live) kill(t_step());
+                            else new_limit();
+                        }
+                    }
+                    if (waiting || !live) {
+                        ++kk;
+                        if (kAccumT) t = t + dt;
+                        continue;
+                    }
+                    push_and_tick();
+                } else {
+                    if (live && !pending && kk < K) push_and_tick();
+                }
             }
-            continue;
+            const bool can_step = (kBirths ? (live || waiting) : live) && !pending && kk < K;
+            const unsigned pend_mask = __ballot_sync(0xffffffffu, pending);
+            const unsigned run_mask = __ballot_sync(0xffffffffu, can_step);
+            if (pend_mask != 0u &&
+                (run_mask == 0u || static_cast<uint32_t>(__popc(pend_mask)) >= p.pend_threshold)) {
+                if (pending) {
+                    ++n_cand;
+                    if (candidate<R>(C, v, S, U, b, m, p.seed, id, step0 + kk)) ++n_coll;
+                    if constexpr (sizeof(R) == 4) {
+                        const R wx = v[0] - k.ug[0], wy = v[1] - k.ug[1], wz = v[2] - k.ug[2];
+                        cb.set(wx * wx + wy * wy + wz * wz);
+                    }
+                    pending = false;
+                    finalize_step();
+                }
+                continue;
+            }
+            if (run_mask == 0u) break;
         }
-        if (run_mask == 0u) break;
-    }
+    };
+    if (__any_sync(0xffffffffu, waiting)) run(std::true_type{});
+    else run(std::false_type{});
 
     if (in_range) {
         x.store(p, i);

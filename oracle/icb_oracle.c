@@ -325,60 +325,61 @@ static int hss_reference(const orc_domain* d, double v[3], double mi, orc_mt64* 
 }
 
 /* Null-collision HSS with Philox (the product's algorithm, FP64).
- * Per step: Q = n*sigma*dt*(|v-u| + <|th|>), survival S *= (1-Q); a
+ * Per step: Q = A |v-u| + A <|th|> (A = n sigma dt), survival S *= (1-Q); a
  * candidate fires when S < U.  The neutral's thermal part th is drawn from
- * the mixture f(th)(|v-u| + |th|)/(|v-u| + <|th|>) and accepted with
- * (1-exp(-n sigma g dt)) / (n sigma dt (|v-u|+|th|)) <= 1; the joint law of
- * (collide, v_n) per step is then f(v_n)(1-exp(-n sigma g dt)), i.e. the
- * reference's.  Return: 0 none, 1 candidate rejected, 2 collision. */
+ * the mixture f(th)(|v-u| + |th|)/(|v-u| + <|th|>) -- |th|^2/sigma^2 =
+ * -2 ln u1 - 2 ln u2 * s with s = cos^2(2 pi u3) (chi^2_3, probability
+ * |v-u|/(|v-u|+<|th|>)) or s = 1 (chi^2_4), isotropic direction -- and
+ * accepted with (1-exp(-n sigma g dt)) / (A (|v-u|+|th|)) <= 1; the joint
+ * law of (collide, v_n) per step is then f(v_n)(1-exp(-n sigma g dt)), the
+ * reference's.  Words: r0 = (U, choice, accept, u1), r1 = (u2, u3|cos th,
+ * phi th|cos scatter, phi scatter|-), 16-bit halves as (k + 1/2) 2^-16.
+ * Return: 0 none, 1 candidate rejected, 2 collision. */
+static double u16_to_unit(uint32_t k) { return ((double)k + 0.5) * 1.52587890625e-05; }
+
+static void philox_words(uint64_t seed, uint32_t ion_id, uint32_t step, uint32_t sub, uint32_t o[4]) {
+    uint32_t c[4] = {ion_id, step, sub, 0u};
+    uint32_t k[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    philox4x32_10(c, k, o);
+}
+
 static int hss_nullcoll(const orc_domain* d, double v[3], double mi, uint64_t seed, uint32_t id,
                         uint32_t step, double* S, double* U, uint64_t* overflow) {
     const double mn = d->gas_mass_kg;
     const double sig_n = sqrt(ORC_KB * d->temperature_K / mn);
     const double mean_th = sig_n * 1.5957691216057308;   /* E|th| = sigma*2*sqrt(2/pi) */
     const double A = d->gas_density_m3 * d->sigma_m2 * d->dt_s;
+    const double Amean = A * mean_th;
     const double* ug = d->gas_velocity_m_s;
     double w[3] = {v[0] - ug[0], v[1] - ug[1], v[2] - ug[2]};
     double gu = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
-    double Q = A * (gu + mean_th);
+    double Q = A * gu + Amean;
     if (Q > 1.0) { Q = 1.0; ++*overflow; }
     *S = *S - *S * Q;
     if (!(*S < *U)) return 0;
-    double r0[4], r1[4], r2[4];
-    draw4(seed, id, step, 0u, r0);
-    draw4(seed, id, step, 1u, r1);
-    draw4(seed, id, step, 2u, r2);
-    *U = r0[0];
+    uint32_t r0[4], r1[4];
+    philox_words(seed, id, step, 0u, r0);
+    philox_words(seed, id, step, 1u, r1);
+    *U = u32_to_unit(r0[0]);
     *S = 1.0;
-    double th[3];
-    if (r0[1] * (gu + mean_th) < gu) {
-        double ra = sqrt(-2.0 * log(r1[0]));
-        double pa = 2.0 * M_PI * r1[1];
-        double rb = sqrt(-2.0 * log(r1[2]));
-        double pb = 2.0 * M_PI * r1[3];
-        th[0] = sig_n * (ra * cos(pa));
-        th[1] = sig_n * (ra * sin(pa));
-        th[2] = sig_n * (rb * cos(pb));
-    } else {
-        double rad = sig_n * sqrt(-2.0 * log(r1[0] * r1[1]));
-        double ct = 2.0 * r1[2] - 1.0;
-        double st = sqrt(fmax(0.0, 1.0 - ct * ct));
-        double ph = 2.0 * M_PI * r1[3];
-        th[0] = rad * (st * cos(ph));
-        th[1] = rad * (st * sin(ph));
-        th[2] = rad * ct;
-    }
-    double thm = sqrt(th[0] * th[0] + th[1] * th[1] + th[2] * th[2]);
-    double vn[3] = {ug[0] + th[0], ug[1] + th[1], ug[2] + th[2]};
+    const int thermal = u32_to_unit(r0[1]) * (gu + mean_th) < gu;
+    const double c3 = cos(2.0 * M_PI * u16_to_unit(r1[1] >> 16));
+    const double sfac = thermal ? c3 * c3 : 1.0;
+    const double r2 = -2.0 * (log(u32_to_unit(r0[3])) + log(u32_to_unit(r1[0])) * sfac);
+    const double rad = sig_n * sqrt(r2);
+    const double ct = 2.0 * u16_to_unit(r1[1] & 0xffffu) - 1.0;
+    const double st = sqrt(fmax(0.0, 1.0 - ct * ct));
+    const double ph = 2.0 * M_PI * u16_to_unit(r1[2] >> 16);
+    double vn[3] = {ug[0] + rad * (st * cos(ph)), ug[1] + rad * (st * sin(ph)), ug[2] + rad * ct};
     double gv[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
     double g = sqrt(gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2]);
-    double q = A * (gu + thm);
+    double q = A * (gu + rad);
     double p = -expm1(-A * g);
-    if (!(r0[2] * q < p)) return 1;
-    double ct = 2.0 * r0[3] - 1.0;
-    double st = sqrt(fmax(0.0, 1.0 - ct * ct));
-    double ph = 2.0 * M_PI * r2[0];
-    double dir[3] = {st * cos(ph), st * sin(ph), ct};
+    if (!(u32_to_unit(r0[2]) * q < p)) return 1;
+    const double ct2 = 2.0 * u16_to_unit(r1[2] & 0xffffu) - 1.0;
+    const double st2 = sqrt(fmax(0.0, 1.0 - ct2 * ct2));
+    const double ph2 = 2.0 * M_PI * u16_to_unit(r1[3] >> 16);
+    double dir[3] = {st2 * cos(ph2), st2 * sin(ph2), ct2};
     double inv = 1.0 / (mi + mn);
     double fac = mn * inv;
     for (int c = 0; c < 3; ++c) {
