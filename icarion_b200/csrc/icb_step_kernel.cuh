@@ -76,7 +76,6 @@ __device__ __forceinline__ void angle_cs(float u, float& c, float& s) {
 // ---- positions --------------------------------------------------------------
 // Double position (FP64).
 struct PosD {
-    static constexpr double kFoldLimit = 1e300;
     using Snap = double;
     double x, y, z;
     __device__ void load(const StepParams& p, uint64_t i) { x = p.x[i]; y = p.y[i]; z = p.z[i]; }
@@ -98,12 +97,10 @@ struct PosD {
 };
 
 // Double anchor + float offset (MIXED).  A step adds v*dt to the float
-// offset (one FFMA per axis, no conversion); the offset is folded into the
-// anchor at the lane's exact checks, which the displacement budget forces
-// at least every kFoldLimit metres of path, so the offset stays below
-// ~4 um and its rounding below ~2e-13 m per step.
+// offset (one FFMA per axis, no conversion); every lane folds the offset
+// into the anchor at each warp vote (every steps_per_vote steps), so the
+// offset stays below ~1 um and its rounding below ~1e-13 m per step.
 struct PosA {
-    static constexpr double kFoldLimit = 3.814697265625e-06;   // 2^-18 m
     using Snap = float;
     double ax, ay, az;
     float dx, dy, dz;
@@ -149,7 +146,6 @@ __device__ __forceinline__ void two_sum_acc(float& hi, float& lo, float d) {
 // Compensated float hi/lo position (HILO), TwoSum update (Knuth, TAOCP
 // vol. 2, 4.2.2).
 struct PosHL {
-    static constexpr double kFoldLimit = 1e300;
     using Snap = double;
     float xh, xl, yh, yl, zh, zl;
     __device__ void load(const StepParams& p, uint64_t i) {
@@ -580,8 +576,7 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
         const double lx = x.gx() - C.ox, ly = x.gy() - C.oy;
         d = fmin(d, C.rmax - sqrt(lx * lx + ly * ly));
         if (!had_arrival) d = fmin(d, fabs(zdet - z));
-        d = fmin(0.99 * d, Pos::kFoldLimit);
-        lim = static_cast<R>(d);
+        lim = static_cast<R>(0.99 * d);
         acc = R(0);
     };
 
@@ -666,6 +661,9 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
                     if (live && !pending && kk < K) push_and_tick();
                 }
             }
+            // warp-uniform fold of the float position offsets (anchor mode);
+            // pending lanes keep theirs until their step is finalized
+            if (!pending) x.fold();
             const bool can_step = (kBirths ? (live || waiting) : live) && !pending && kk < K;
             const unsigned pend_mask = __ballot_sync(0xffffffffu, pending);
             const unsigned run_mask = __ballot_sync(0xffffffffu, can_step);
