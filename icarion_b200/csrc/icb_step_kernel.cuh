@@ -13,7 +13,7 @@
 //   FP64       double everywhere.  Compiled without FMA contraction so that
 //              the collision-free push is bit-identical to the reference.
 //   MIXED      float velocity, field, collision; position = double anchor +
-//              float offset (folded into the anchor every ~4 um of path).
+//              float offset (folded into the anchor at every warp vote).
 //   HILO       float velocity; position as a compensated float hi/lo pair.
 //
 // Deferred collisions.  A collision candidate fires in ~10% of ion-steps;
@@ -90,7 +90,7 @@ struct PosD {
         const double v = (a == 0) ? x : (a == 1) ? y : z;
         return static_cast<R>(v - c);
     }
-    __device__ void drift(double vx, double vy, double vz, double dt) {
+    __device__ void drift(double vx, double vy, double vz, double dt, double) {
         x += vx * dt; y += vy * dt; z += vz * dt;
     }
     __device__ bool finite() const { return isfinite(x) && isfinite(y) && isfinite(z); }
@@ -123,8 +123,7 @@ struct PosA {
         const float d = (a == 0) ? dx : (a == 1) ? dy : dz;
         return static_cast<R>(static_cast<float>(an - c) + d);
     }
-    __device__ void drift(float vx, float vy, float vz, double dt) {
-        const float d = static_cast<float>(dt);
+    __device__ void drift(float vx, float vy, float vz, double, float d) {
         dx = fmaf(vx, d, dx); dy = fmaf(vy, d, dy); dz = fmaf(vz, d, dz);
     }
     __device__ bool finite() const {
@@ -146,7 +145,7 @@ __device__ __forceinline__ void two_sum_acc(float& hi, float& lo, float d) {
 // Compensated float hi/lo position (HILO), TwoSum update (Knuth, TAOCP
 // vol. 2, 4.2.2).
 struct PosHL {
-    using Snap = double;
+    struct Snap { float h, l; };
     float xh, xl, yh, yl, zh, zl;
     __device__ void load(const StepParams& p, uint64_t i) {
         xh = p.xh[i]; xl = p.xl[i]; yh = p.yh[i]; yl = p.yl[i]; zh = p.zh[i]; zl = p.zl[i];
@@ -157,8 +156,8 @@ struct PosHL {
     __device__ double gx() const { return static_cast<double>(xh) + static_cast<double>(xl); }
     __device__ double gy() const { return static_cast<double>(yh) + static_cast<double>(yl); }
     __device__ double gz() const { return static_cast<double>(zh) + static_cast<double>(zl); }
-    __device__ Snap snap_z() const { return gz(); }
-    __device__ double z_of(Snap s) const { return s; }
+    __device__ Snap snap_z() const { return Snap{zh, zl}; }
+    __device__ double z_of(Snap s) const { return static_cast<double>(s.h) + static_cast<double>(s.l); }
     __device__ void fold() {}
     template <class R> __device__ R rel(int a, double c) const {
         const float h = (a == 0) ? xh : (a == 1) ? yh : zh;
@@ -167,8 +166,7 @@ struct PosHL {
         const float cl = static_cast<float>(c - static_cast<double>(ch));
         return static_cast<R>(((h - ch) + l) - cl);
     }
-    __device__ void drift(float vx, float vy, float vz, double dt) {
-        const float d = static_cast<float>(dt);
+    __device__ void drift(float vx, float vy, float vz, double, float d) {
         two_sum_acc(xh, xl, vx * d);
         two_sum_acc(yh, yl, vy * d);
         two_sum_acc(zh, zl, vz * d);
@@ -194,8 +192,8 @@ struct Consts {
     R a_uni[3];              // acceleration of a uniform field for this ion
     R q, qm, inv_m;
     double m;
-    double dt;
-    R h;                     // dt/2 in working precision
+    double dt, hd, dt6;      // dt, dt/2, dt/6
+    R dt_r, h, dt6_r;        // the same in working precision
     R A, Amean, ug[3];       // collision clock: Q = A |v - u| + A <|th|>
 };
 
@@ -213,7 +211,11 @@ __device__ void load_consts(Consts<R>& k, const EnsConst& C, double q, double m)
     k.r0sq = static_cast<R>(C.r0sq);
     k.rfw = C.rf_omega;
     k.dt = C.dt;
+    k.hd = C.dt * 0.5;
+    k.dt6 = C.dt / 6.0;
+    k.dt_r = static_cast<R>(C.dt);
     k.h = static_cast<R>(C.dt * 0.5);
+    k.dt6_r = static_cast<R>(C.dt / 6.0);
     k.q = static_cast<R>(q);
     k.m = m;
     // Reference: qm = charge / mass; t = B * (qm * dt * 0.5); s = 2 t / (1 + t^2);
@@ -301,7 +303,7 @@ __device__ __forceinline__ R boris(const Consts<R>& k, Pos& x, R v[3], double t)
     } else {
         vp[0] = vm[0]; vp[1] = vm[1]; vp[2] = vm[2];
     }
-    x.drift(vp[0], vp[1], vp[2], k.dt);
+    x.drift(vp[0], vp[1], vp[2], k.dt, k.dt_r);
 #pragma unroll
     for (int c = 0; c < 3; ++c) v[c] = vp[c] + a[c] * k.h;
     return fabs(vp[0]) + fabs(vp[1]) + fabs(vp[2]);
@@ -331,22 +333,22 @@ __device__ __forceinline__ void rk4_acc(const Consts<R>& k, const Pos& x, const 
 template <class R, int FIELD, bool MAG, class Pos>
 __device__ __forceinline__ R rk4(const Consts<R>& k, Pos& x, R v[3], double t) {
     const double dt = k.dt;
-    const double hd = dt * 0.5;
+    const double hd = k.hd;
     const R h = k.h;
-    const R dtr = static_cast<R>(dt);
+    const R dtr = k.dt_r;
     const Pos x0 = x;
     const R v0[3] = {v[0], v[1], v[2]};
     R k1a[3], k2a[3], k3a[3], k4a[3], v2[3], v3[3], v4[3];
     rk4_acc<R, FIELD, MAG>(k, x0, v0, t, k1a);
-    Pos p2 = x0; p2.drift(v0[0], v0[1], v0[2], hd);
+    Pos p2 = x0; p2.drift(v0[0], v0[1], v0[2], hd, h);
 #pragma unroll
     for (int c = 0; c < 3; ++c) v2[c] = v0[c] + k1a[c] * h;
     rk4_acc<R, FIELD, MAG>(k, p2, v2, t + hd, k2a);
-    Pos p3 = x0; p3.drift(v2[0], v2[1], v2[2], hd);
+    Pos p3 = x0; p3.drift(v2[0], v2[1], v2[2], hd, h);
 #pragma unroll
     for (int c = 0; c < 3; ++c) v3[c] = v0[c] + k2a[c] * h;
     rk4_acc<R, FIELD, MAG>(k, p3, v3, t + hd, k3a);
-    Pos p4 = x0; p4.drift(v3[0], v3[1], v3[2], dt);
+    Pos p4 = x0; p4.drift(v3[0], v3[1], v3[2], dt, dtr);
 #pragma unroll
     for (int c = 0; c < 3; ++c) v4[c] = v0[c] + k3a[c] * dtr;
     rk4_acc<R, FIELD, MAG>(k, p4, v4, t + dt, k4a);
@@ -354,8 +356,8 @@ __device__ __forceinline__ R rk4(const Consts<R>& k, Pos& x, R v[3], double t) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) dv[c] = v0[c] + v2[c] * R(2.0) + v3[c] * R(2.0) + v4[c];
     x = x0;
-    x.drift(dv[0], dv[1], dv[2], dt / 6.0);
-    const R s = static_cast<R>(dt / 6.0);
+    x.drift(dv[0], dv[1], dv[2], k.dt6, k.dt6_r);
+    const R s = k.dt6_r;
 #pragma unroll
     for (int c = 0; c < 3; ++c) v[c] = v0[c] + (k1a[c] + k2a[c] * R(2.0) + k3a[c] * R(2.0) + k4a[c]) * s;
     return (fabs(dv[0]) + fabs(dv[1]) + fabs(dv[2])) * R(1.0 / 6.0);
@@ -625,8 +627,10 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
         if (!FUSED && do_push) p.zprev[i] = x.z_of(zold);
         if (do_push) {
             R l1;
-            if (INTEG == kBoris) l1 = boris<R, FIELD, MAG>(k, x, v, t_step());
-            else l1 = rk4<R, FIELD, MAG>(k, x, v, t_step());
+            double tn = 0.0;   // only a time-dependent field reads the clock
+            if constexpr (FIELD == kFieldLinearRF) tn = t_step();
+            if (INTEG == kBoris) l1 = boris<R, FIELD, MAG>(k, x, v, tn);
+            else l1 = rk4<R, FIELD, MAG>(k, x, v, tn);
             acc += l1 * dt_r;
         }
         if (COLL != kCollNone && do_coll) pending = clock_tick<R>(k, v, S, U, b, cb, n_ovf);
