@@ -73,16 +73,27 @@ struct DevBuf {
 // ---------------------------------------------------------------------------
 namespace {
 
-// Initial collision clocks: S = 1, U = uniform of Philox(id, 0, 3, 0).x.
+// Initial collision clocks from u = uniform of Philox(id, 0, 3, 0).x:
+// per-step clock S = 1, U = u; skip clock tau = -ln u, restart pending.
 template <class R>
-__global__ void k_clock_init(R* S, R* U, uint64_t n, uint64_t first_id, uint64_t seed) {
+__global__ void k_clock_init(R* S, R* U, uint32_t* nxt, uint32_t* start, uint64_t n, uint64_t first_id,
+                             uint64_t seed, int skip) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const U4 r = philox4x32_10(static_cast<uint32_t>(first_id + i), 0u, 3u, 0u,
                                static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32));
-    S[i] = R(1);
-    if constexpr (sizeof(R) == 8) U[i] = unit_d(r.x);
-    else U[i] = unit_f(r.x);
+    R u;
+    if constexpr (sizeof(R) == 8) u = unit_d(r.x);
+    else u = 2.0f - __uint_as_float(0x3f800000u | (r.x >> 9));
+    if (skip) {
+        S[i] = -log(u);
+        U[i] = R(0);
+        nxt[i] = 0xFFFFFFFFu;
+        start[i] = 0u;
+    } else {
+        S[i] = R(1);
+        U[i] = u;
+    }
 }
 
 // Device engine clock: step += K and t_e += dt_e, K times (accumulated like
@@ -238,6 +249,7 @@ struct icb_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<cudaEvent_t> kev;      // per-launch events of the step kernel
     uint64_t launches = 0;             // kernels launched by the current call
+    uint64_t host_step = 0;            // host mirror of the engine step index
 
     uint64_t n = 0;
     uint64_t first_id = 0;
@@ -250,6 +262,7 @@ struct icb_handle {
     DevBuf<float> vxf, vyf, vzf;
     DevBuf<double> Sd, Ud;
     DevBuf<float> Sf, Uf;
+    DevBuf<uint32_t> clk_next, clk_start;   // skip clock (Boris + collisions)
     DevBuf<double> mass, charge, t_death, t_arr, birth, zprev;
     DevBuf<uint8_t> flags, active_stage;
     DevBuf<double> stage;
@@ -262,6 +275,7 @@ struct icb_handle {
     bool has_birth = false;
 
     bool fp64() const { return cfg.precision == ICB_PREC_FP64; }
+    bool skip_clock() const { return coll != kCollNone && cfg.integrator == ICB_INTEGRATOR_BORIS; }
     bool hilo() const { return cfg.precision == ICB_PREC_MIXED_HILO; }
     void* vx() const { return fp64() ? static_cast<void*>(vxd.p) : static_cast<void*>(vxf.p); }
     void* vy() const { return fp64() ? static_cast<void*>(vyd.p) : static_cast<void*>(vyf.p); }
@@ -281,6 +295,24 @@ int check_handle(icb_handle* h) {
     cudaError_t e = cudaSetDevice(h->cfg.device);
     if (e != cudaSuccess) return fail(ICB_ERR_CUDA, "cudaSetDevice(%d): %s", h->cfg.device, cudaGetErrorString(e));
     return ICB_OK;
+}
+
+// Upper bound of |E| over the cylinder for E = E0 + G .* (x - c) plus the
+// RF quadrupole term: |E0| + |G .* max|x - c|| + 2 (|U0| + |V|) r_axis / r0^2.
+// The CPU oracle evaluates the same expression (orc_field_bound).
+double field_bound(const EnsConst& C, const icb_ensemble_params& P) {
+    const double Rp = P.radius_m + kGeomEps;
+    double e = std::sqrt(C.E0[0] * C.E0[0] + C.E0[1] * C.E0[1] + C.E0[2] * C.E0[2]);
+    const double ex = std::fabs(C.ox - C.c[0]) + Rp;
+    const double ey = std::fabs(C.oy - C.c[1]) + Rp;
+    const double ez = std::fmax(std::fabs(C.oz - C.c[2]), std::fabs(C.oz + C.zmax_local - C.c[2]));
+    const double gx = C.G[0] * ex, gy = C.G[1] * ey, gz = C.G[2] * ez;
+    e = e + std::sqrt(gx * gx + gy * gy + gz * gz);
+    if (C.rf) {
+        const double raxis = std::sqrt(C.ox * C.ox + C.oy * C.oy) + Rp;
+        e = e + 2.0 * (std::fabs(C.rf_U0) + std::fabs(C.rf_V)) * raxis / C.r0sq;
+    }
+    return e;
 }
 
 // Per-ensemble constants exactly as the reference derives them.
@@ -346,6 +378,7 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
         for (int a = 0; a < 3; ++a) C.fug[a] = static_cast<float>(C.ug[a]);
     }
     C.zdet = P.detector_z_m;
+    C.Emax = field_bound(C, P);
     return ICB_OK;
 }
 
@@ -365,6 +398,8 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.vx = h->vx(); p.vy = h->vy(); p.vz = h->vz();
         p.clkS = h->fp64() ? static_cast<void*>(h->Sd.p) : static_cast<void*>(h->Sf.p);
         p.clkU = h->fp64() ? static_cast<void*>(h->Ud.p) : static_cast<void*>(h->Uf.p);
+        p.clk_next = h->clk_next.p;
+        p.clk_start = h->clk_start.p;
         p.mass = h->mass.p; p.charge = h->charge.p; p.flags = h->flags.p;
         p.t_death = h->t_death.p; p.t_arr = h->t_arr.p;
         p.birth = h->has_birth ? h->birth.p : nullptr;
@@ -374,6 +409,7 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.t_dev = h->t_dev.p;
         p.first_id = h->first_id;
         p.seed = h->cfg.rng_seed;
+        philox_round_keys(h->cfg.rng_seed, p.rk);
         p.n_steps = K;
         p.pend_threshold = h->pend;
         p.steps_per_vote = h->spv;
@@ -570,6 +606,8 @@ int icb_upload_ions(icb_handle* h, uint64_t n,
         const bool clk = h->coll != kCollNone;
         ICB_CUDA(h->Sd.alloc(clk && f64 ? n : 0)); ICB_CUDA(h->Ud.alloc(clk && f64 ? n : 0));
         ICB_CUDA(h->Sf.alloc(clk && !f64 ? n : 0)); ICB_CUDA(h->Uf.alloc(clk && !f64 ? n : 0));
+        // event-step arrays of the skip clock (read by the Boris kernels only)
+        ICB_CUDA(h->clk_next.alloc(clk ? n : 0)); ICB_CUDA(h->clk_start.alloc(clk ? n : 0));
         ICB_CUDA(h->xr.alloc(n)); ICB_CUDA(h->yr.alloc(n)); ICB_CUDA(h->zr.alloc(n));
         ICB_CUDA(h->mass.alloc(n)); ICB_CUDA(h->charge.alloc(n));
         ICB_CUDA(h->t_death.alloc(n)); ICB_CUDA(h->t_arr.alloc(n)); ICB_CUDA(h->birth.alloc(n));
@@ -619,8 +657,13 @@ int icb_upload_ions(icb_handle* h, uint64_t n,
     k_flags_in<<<g, 256, 0, s>>>(h->active_stage.p, h->has_birth ? h->birth.p : nullptr, h->flags.p, h->t_death.p, h->t_arr.p, n);
     ICB_CUDA(cudaGetLastError());
     if (h->coll != kCollNone) {
-        if (h->fp64()) k_clock_init<double><<<g, 256, 0, s>>>(h->Sd.p, h->Ud.p, n, first_ion_id, h->cfg.rng_seed);
-        else k_clock_init<float><<<g, 256, 0, s>>>(h->Sf.p, h->Uf.p, n, first_ion_id, h->cfg.rng_seed);
+        const int skip = h->skip_clock() ? 1 : 0;
+        if (h->fp64())
+            k_clock_init<double><<<g, 256, 0, s>>>(h->Sd.p, h->Ud.p, h->clk_next.p, h->clk_start.p, n, first_ion_id,
+                                                   h->cfg.rng_seed, skip);
+        else
+            k_clock_init<float><<<g, 256, 0, s>>>(h->Sf.p, h->Uf.p, h->clk_next.p, h->clk_start.p, n, first_ion_id,
+                                                  h->cfg.rng_seed, skip);
         ICB_CUDA(cudaGetLastError());
     }
     // moment work items: slices of <= kMomItemIons ions, never crossing an ensemble
@@ -737,6 +780,10 @@ int icb_download_ions(icb_handle* h, double* x, double* y, double* z,
 int icb_advance(icb_handle* h, uint64_t n_steps, icb_run_stats* stats) {
     if (int r = check_handle(h)) return r;
     if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
+    // Philox counters and clock events use 31-bit global step indices.
+    if (h->host_step + n_steps >= (1ull << 31))
+        return fail(ICB_ERR_INVALID_ARGUMENT, "runs are limited to 2^31 engine steps");
+    h->host_step += n_steps;
     cudaStream_t s = h->stream;
     ICB_CUDA(cudaMemsetAsync(h->counters.p, 0, kNumCounters * sizeof(unsigned long long), s));
     ICB_CUDA(cudaEventRecord(h->ev0, s));
@@ -772,6 +819,9 @@ int icb_advance(icb_handle* h, uint64_t n_steps, icb_run_stats* stats) {
 static int single_part(icb_handle* h, int push, int collide, int finalize, icb_run_stats* stats) {
     if (int r = check_handle(h)) return r;
     if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
+    if (h->host_step + 1 >= (1ull << 31))
+        return fail(ICB_ERR_INVALID_ARGUMENT, "runs are limited to 2^31 engine steps");
+    if (finalize) h->host_step += 1;
     cudaStream_t s = h->stream;
     ICB_CUDA(cudaMemsetAsync(h->counters.p, 0, kNumCounters * sizeof(unsigned long long), s));
     ICB_CUDA(cudaEventRecord(h->ev0, s));
@@ -804,6 +854,8 @@ int icb_get_clock(icb_handle* h, uint64_t* step, double* time_s) {
 
 int icb_set_clock(icb_handle* h, uint64_t step, const double* time_s) {
     if (int r = check_handle(h)) return r;
+    if (step >= (1ull << 31)) return fail(ICB_ERR_INVALID_ARGUMENT, "step index must be < 2^31");
+    h->host_step = step;
     unsigned long long st = step;
     ICB_CUDA(cudaMemcpyAsync(h->step_dev.p, &st, sizeof(st), cudaMemcpyHostToDevice, h->stream));
     if (time_s) ICB_CUDA(cudaMemcpyAsync(h->t_dev.p, time_s, h->ens.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));

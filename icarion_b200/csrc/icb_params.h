@@ -46,6 +46,9 @@ struct EnsConst {
     double ug[3];
     double m_gas;
     double zdet;
+    // Upper bound of |E| inside the domain: the skip clock bounds the ion
+    // speed change per step by |q/m| Emax dt.
+    double Emax;
     int32_t magnetic;
     int32_t rf;
     // float copies for the float collision path
@@ -61,8 +64,14 @@ struct StepParams {
     float* xh; float* xl; float* yh; float* yl; float* zh; float* zl;
     // velocities (double in FP64 mode, float otherwise)
     void* vx; void* vy; void* vz;
-    // null-collision clock: survival S and threshold U (same type as v)
+    // null-collision clock (same type as v): per-step clock (RK4): survival S
+    // and threshold U; skip clock (Boris): optical depth tau at the last
+    // restart and the majorant Q*.
     void* clkS; void* clkU;
+    // skip clock: global step of the next clock event (bit 31 set = horizon
+    // refresh, 0xFFFFFFFF = restart needed) and of the last restart
+    uint32_t* clk_next;
+    uint32_t* clk_start;
     const double* mass;
     const double* charge;
     uint8_t* flags;
@@ -75,6 +84,7 @@ struct StepParams {
     const double* t_dev;               // engine time per ensemble at launch start
     uint64_t first_id;
     uint64_t seed;
+    uint32_t rk[20];                   // Philox round keys of the seed
     uint32_t n_steps;
     uint32_t pend_threshold;
     uint32_t ens_base;                 // global index of this chunk's ensemble 0

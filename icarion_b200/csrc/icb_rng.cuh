@@ -41,6 +41,35 @@ ICB_HD U4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint
     return U4{c0, c1, c2, c3};
 }
 
+// Round keys (k0 + r W0, k1 + r W1), r = 0..9, of a fixed key: computed
+// once per launch so the rounds need no key arithmetic.
+inline void philox_round_keys(uint64_t seed, uint32_t rk[20]) {
+    uint32_t k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32);
+    for (int r = 0; r < 10; ++r) {
+        rk[2 * r] = k0;
+        rk[2 * r + 1] = k1;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+// Philox4x32-10 with precomputed round keys; identical output to
+// philox4x32_10(c, k0, k1).
+ICB_HD U4 philox4x32_10_rk(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, const uint32_t* rk) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * c0;
+        const uint64_t p1 = static_cast<uint64_t>(0xCD9E8D57u) * c2;
+        const uint32_t hi0 = static_cast<uint32_t>(p0 >> 32), lo0 = static_cast<uint32_t>(p0);
+        const uint32_t hi1 = static_cast<uint32_t>(p1 >> 32), lo1 = static_cast<uint32_t>(p1);
+        c0 = hi1 ^ c1 ^ rk[2 * r];
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ rk[2 * r + 1];
+        c3 = lo0;
+    }
+    return U4{c0, c1, c2, c3};
+}
+
 // 32-bit word -> double in (0, 1]: (w + 1) * 2^-32, exact.
 ICB_HD double unit_d(uint32_t w) { return (static_cast<double>(w) + 1.0) * 2.3283064365386963e-10; }
 // 32-bit word -> float in (0, 1]: (top 24 bits + 1) * 2^-24, exact.

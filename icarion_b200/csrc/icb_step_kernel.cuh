@@ -43,6 +43,8 @@ __device__ __forceinline__ double m_sqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float m_sqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double m_log(double x) { return log(x); }
 __device__ __forceinline__ float m_log(float x) { return __logf(x); }
+__device__ __forceinline__ double m_log1p(double x) { return log1p(x); }
+__device__ __forceinline__ float m_log1p(float x) { return log1pf(x); }
 __device__ __forceinline__ double m_expm1(double x) { return expm1(x); }
 __device__ __forceinline__ float m_expm1(float x) { return expm1f(x); }
 __device__ __forceinline__ double m_fmax(double a, double b) { return fmax(a, b); }
@@ -401,11 +403,15 @@ __device__ __forceinline__ bool clock_tick(const Consts<R>& k, const R v[3], R& 
     return S < U;
 }
 
-// Candidate processing (the steps of the oracle's hss_nullcoll).  Returns
-// true when the collision is accepted (v updated).
-template <class R>
-__device__ __forceinline__ bool candidate(const EnsConst& C, R v[3], R& S, R& U, R b, double mi_d,
-                                          uint64_t seed, uint32_t id, uint32_t step) {
+// Candidate processing (the steps of the oracle's hss_nullcoll).
+// SKIP (skip clock): the event is first thinned with Q(b)/Q*, b = |v - u|
+// exact; clk receives the new optical depth.  Otherwise (per-step clock) b
+// is the clock's bound and clk receives the new threshold U.
+// Returns 0 when the skip-clock event is thinned away, 1 when the candidate
+// is rejected, 2 on a collision (v updated).
+template <class R, bool SKIP>
+__device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qstar, R Amean, R b, double mi_d,
+                                         const uint32_t* rk, uint32_t id, uint32_t step) {
     R A, mean_th, sig_n, ug[3], mi, mn, inv_mt, fac;
     if constexpr (sizeof(R) == 8) {
         A = C.A; mean_th = C.mean_th; sig_n = C.sig_n;
@@ -420,12 +426,20 @@ __device__ __forceinline__ bool candidate(const EnsConst& C, R v[3], R& S, R& U,
         inv_mt = __frcp_rn(mi + mn);
         fac = mn * inv_mt;
     }
-    const uint32_t k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32);
-    const U4 r0 = philox4x32_10(id, step, 0u, 0u, k0, k1);
-    const U4 r1 = philox4x32_10(id, step, 1u, 0u, k0, k1);
-    U = u32(r0.x, R(0));
-    S = R(1);
-    const bool thermal = u32(r0.y, R(0)) * (b + mean_th) < b;
+    const U4 r0 = philox4x32_10_rk(id, step, 0u, 0u, rk);
+    R uc = u32(r0.y, R(0));
+    if constexpr (SKIP) {
+        clk = -m_log(u32(r0.x, R(0)));
+        const R wx = v[0] - ug[0], wy = v[1] - ug[1], wz = v[2] - ug[2];
+        b = m_sqrt(wx * wx + wy * wy + wz * wz);
+        const R Q = A * b + Amean;
+        if (!(uc * qstar < Q)) return 0;
+        uc = uc * qstar / Q;          // uniform on (0, 1) given the acceptance
+    } else {
+        clk = u32(r0.x, R(0));
+    }
+    const U4 r1 = philox4x32_10_rk(id, step, 1u, 0u, rk);
+    const bool thermal = uc * (b + mean_th) < b;
     R c3, s3;
     angle_cs(u16(r1.y >> 16, R(0)), c3, s3);
     const R sfac = thermal ? c3 * c3 : R(1);
@@ -440,7 +454,7 @@ __device__ __forceinline__ bool candidate(const EnsConst& C, R v[3], R& S, R& U,
     const R g = m_sqrt(gx * gx + gy * gy + gz * gz);
     const R q = A * (b + rad);
     const R pc = -m_expm1(-A * g);
-    if (!(u32(r0.z, R(0)) * q < pc)) return false;
+    if (!(u32(r0.z, R(0)) * q < pc)) return 1;
     const R ct2 = R(2.0) * u16(r1.z & 0xffffu, R(0)) - R(1.0);
     const R st2 = m_sqrt(m_fmax(R(0), R(1.0) - ct2 * ct2));
     R cp2, sp2;
@@ -451,7 +465,7 @@ __device__ __forceinline__ bool candidate(const EnsConst& C, R v[3], R& S, R& U,
         const R vcom = (v[c] * mi + vn[c] * mn) * inv_mt;
         v[c] = vcom + (dir[c] * g) * fac;
     }
-    return true;
+    return 2;
 }
 
 // ---- finalize ------------------------------------------------------------------
@@ -544,6 +558,45 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
 
     const uint32_t id = static_cast<uint32_t>(p.first_id + i);
     const uint32_t step0 = static_cast<uint32_t>(*p.step_dev);
+    uint32_t n_cand = 0, n_coll = 0, n_ovf = 0, n_dead = 0, n_arr = 0;
+
+    // Skip clock (Boris): S holds the exponential optical depth tau left at
+    // the last restart, U the majorant Q* = A b* + A <|th|> of the current
+    // horizon, b* >= |v - u| for every step of the horizon because Boris
+    // changes |v| by at most |q/m| Emax dt per step.  A restart computes the
+    // step at which tau is used up at rate -ln(1 - Q*) per step (the clock
+    // event) or, if that lies beyond the horizon of H steps, a refresh at the
+    // horizon's last step; restarts happen at global step indices fixed by
+    // the lane's own history, so results do not depend on launch shape.
+    constexpr bool kSkip = (INTEG == kBoris) && (COLL != kCollNone);
+    constexpr uint32_t kRefresh = 0x80000000u, kNeedRestart = 0xFFFFFFFFu;
+    uint32_t g_next = kNeedRestart, g_start = 0u, nk = 0xFFFFFFFFu, H = 1u;
+    R lam = R(0), dvmax = R(0), absu = R(0);
+    if constexpr (kSkip) {
+        if (in_range) { g_next = p.clk_next[i]; g_start = p.clk_start[i]; }
+        dvmax = static_cast<R>(fabs(k.qm) * static_cast<R>(C.Emax) * static_cast<R>(C.dt));
+        absu = m_sqrt(k.ug[0] * k.ug[0] + k.ug[1] * k.ug[1] + k.ug[2] * k.ug[2]);
+        // horizon minimising the majorant's excess plus refreshes: 1/sqrt(A dv)
+        R hz = R(1) / m_sqrt(k.A * dvmax);
+        if (!(hz < R(4096))) hz = R(4096);
+        if (hz < R(16)) hz = R(16);
+        H = static_cast<uint32_t>(hz);
+        if (U > R(0)) lam = -m_log1p(-U);
+        if (g_next != kNeedRestart) nk = (g_next & ~kRefresh) - step0;
+    }
+    auto clock_restart = [&](uint32_t gs) {
+        const R v0 = m_sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        const R bstar = (v0 + absu + static_cast<R>(H) * dvmax) * R(1.000001);
+        R qs = k.A * bstar + k.Amean;
+        if (qs > R(0.99999904632568359375)) { qs = R(0.99999904632568359375); ++n_ovf; }
+        U = qs;
+        lam = -m_log1p(-qs);
+        const R nf = ceil(S / lam);
+        g_start = gs;
+        if (nf <= static_cast<R>(H)) g_next = gs + (nf < R(1) ? 1u : static_cast<uint32_t>(nf)) - 1u;
+        else g_next = (gs + H - 1u) | kRefresh;
+        nk = (g_next & ~kRefresh) - step0;
+    };
     const double t0 = p.t_dev[p.ens_base + e];
     const double dt = C.dt;
     const R dt_r = static_cast<R>(dt);
@@ -551,10 +604,10 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
     double t = t0;            // accumulated clock (used when kAccumT)
     double tdeath = -1.0, tarr = -1.0;
     bool dead_now = false, arr_now = false;
-    uint32_t n_cand = 0, n_coll = 0, n_ovf = 0, n_dead = 0, n_arr = 0;
     const uint32_t K = p.n_steps;
     uint32_t kk = 0;
-    bool pending = false;
+    bool pending = false;     // lane stopped at this step until the deferred phase
+    bool cand = false;        // ... because a collision candidate fired
     R b = R(0);
     Snap zold{};
     R acc = R(0), lim = R(0);
@@ -591,6 +644,9 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
         } else {
             new_limit();
         }
+    }
+    if constexpr (kSkip) {
+        if (live && do_coll && g_next == kNeedRestart) clock_restart(step0);
     }
 
     // exact finalize of the current step (SimulationEngineLifecycle.cpp:123-195)
@@ -633,8 +689,19 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
             else l1 = rk4<R, FIELD, MAG>(k, x, v, tn);
             acc += l1 * dt_r;
         }
-        if (COLL != kCollNone && do_coll) pending = clock_tick<R>(k, v, S, U, b, cb, n_ovf);
-        if (!pending) finalize_step();
+        if constexpr (kSkip) {
+            if (do_coll) cand = (kk == nk);
+        } else if constexpr (COLL != kCollNone) {
+            if (do_coll) cand = clock_tick<R>(k, v, S, U, b, cb, n_ovf);
+        }
+        // A collision candidate or an exhausted displacement budget stops the
+        // lane at this step; both are handled in the warp's deferred phase,
+        // which keeps the rare exact check out of the per-step path.
+        pending = cand || (do_fin && (!FUSED || !(acc <= lim)));
+        if (!pending) {
+            ++kk;
+            if (kAccumT) t = t + dt;
+        }
     };
 
     auto run = [&](auto births) {
@@ -651,8 +718,14 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
                             waiting = false;
                             flags |= static_cast<uint8_t>(kFlagBorn | kFlagActive);
                             live = inside(C, x);
-                            if (!live) kill(t_step());
-                            else new_limit();
+                            if (!live) {
+                                kill(t_step());
+                            } else {
+                                new_limit();
+                                if constexpr (kSkip) {
+                                    if (do_coll && g_next == kNeedRestart) clock_restart(step0 + kk);
+                                }
+                            }
                         }
                     }
                     if (waiting || !live) {
@@ -674,11 +747,28 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
             if (pend_mask != 0u &&
                 (run_mask == 0u || static_cast<uint32_t>(__popc(pend_mask)) >= p.pend_threshold)) {
                 if (pending) {
-                    ++n_cand;
-                    if (candidate<R>(C, v, S, U, b, m, p.seed, id, step0 + kk)) ++n_coll;
-                    if constexpr (sizeof(R) == 4) {
-                        const R wx = v[0] - k.ug[0], wy = v[1] - k.ug[1], wz = v[2] - k.ug[2];
-                        cb.set(wx * wx + wy * wy + wz * wz);
+                    if (cand) {
+                        const uint32_t gs = step0 + kk;
+                        if constexpr (kSkip) {
+                            if (g_next & kRefresh) {
+                                // horizon end without an event: consume its steps
+                                S = S - static_cast<R>(gs + 1u - g_start) * lam;
+                            } else {
+                                const int st = candidate<R, true>(C, v, S, U, k.Amean, b, m, p.rk, id, gs);
+                                if (st >= 1) ++n_cand;
+                                if (st == 2) ++n_coll;
+                            }
+                            clock_restart(gs + 1u);
+                        } else {
+                            ++n_cand;
+                            if (candidate<R, false>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs) == 2) ++n_coll;
+                            S = R(1);
+                            if constexpr (sizeof(R) == 4) {
+                                const R wx = v[0] - k.ug[0], wy = v[1] - k.ug[1], wz = v[2] - k.ug[2];
+                                cb.set(wx * wx + wy * wy + wz * wz);
+                            }
+                        }
+                        cand = false;
                     }
                     pending = false;
                     finalize_step();
@@ -699,6 +789,10 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
         if (COLL != kCollNone) {
             static_cast<R*>(p.clkS)[i] = S;
             static_cast<R*>(p.clkU)[i] = U;
+        }
+        if constexpr (kSkip) {
+            p.clk_next[i] = g_next;
+            p.clk_start[i] = g_start;
         }
         p.flags[i] = flags;
         if (dead_now) p.t_death[i] = tdeath;

@@ -325,16 +325,25 @@ static int hss_reference(const orc_domain* d, double v[3], double mi, orc_mt64* 
 }
 
 /* Null-collision HSS with Philox (the product's algorithm, FP64).
- * Per step: Q = A |v-u| + A <|th|> (A = n sigma dt), survival S *= (1-Q); a
- * candidate fires when S < U.  The neutral's thermal part th is drawn from
- * the mixture f(th)(|v-u| + |th|)/(|v-u| + <|th|>) -- |th|^2/sigma^2 =
- * -2 ln u1 - 2 ln u2 * s with s = cos^2(2 pi u3) (chi^2_3, probability
- * |v-u|/(|v-u|+<|th|>)) or s = 1 (chi^2_4), isotropic direction -- and
- * accepted with (1-exp(-n sigma g dt)) / (A (|v-u|+|th|)) <= 1; the joint
- * law of (collide, v_n) per step is then f(v_n)(1-exp(-n sigma g dt)), the
- * reference's.  Words: r0 = (U, choice, accept, u1), r1 = (u2, u3|cos th,
- * phi th|cos scatter, phi scatter|-), 16-bit halves as (k + 1/2) 2^-16.
- * Return: 0 none, 1 candidate rejected, 2 collision. */
+ * Each step has a candidate with probability Q = A b + A <|th|> (A = n sigma
+ * dt, b = |v-u|).  The neutral's thermal part th is drawn from the mixture
+ * f(th)(b + |th|)/(b + <|th|>) -- |th|^2/sigma^2 = -2 ln u1 - 2 ln u2 * s with
+ * s = cos^2(2 pi u3) (chi^2_3, probability b/(b+<|th|>)) or s = 1 (chi^2_4),
+ * isotropic direction -- and accepted with (1-exp(-n sigma g dt)) /
+ * (A (b+|th|)) <= 1; the joint law of (collide, v_n) per step is then
+ * f(v_n)(1-exp(-n sigma g dt)), the reference's.
+ *
+ * Two clocks decide the candidate steps:
+ *  - per-step clock (RK4): survival S *= (1-Q), candidate when S < U;
+ *  - skip clock (Boris): an exponential optical depth tau is spent at rate
+ *    -ln(1-Q*) per step over horizons of H steps, with Q* = A b* + A<|th|>
+ *    and b* = (|v| + |u| + H |q/m| Emax dt)(1 + 1e-6) >= |v-u| for every step
+ *    of the horizon; at the step where tau runs out the event is thinned with
+ *    Q(b)/Q*; at the end of a horizon without event tau is reduced and the
+ *    horizon restarted.
+ * Words: r0 = (U or tau, choice (thinning), accept, u1), r1 = (u2,
+ * u3|cos th, phi th|cos scatter, phi scatter|-), 16-bit halves as
+ * (k + 1/2) 2^-16.  Return: 0 thinned away, 1 candidate rejected, 2 collision. */
 static double u16_to_unit(uint32_t k) { return ((double)k + 0.5) * 1.52587890625e-05; }
 
 static void philox_words(uint64_t seed, uint32_t ion_id, uint32_t step, uint32_t sub, uint32_t o[4]) {
@@ -343,43 +352,55 @@ static void philox_words(uint64_t seed, uint32_t ion_id, uint32_t step, uint32_t
     philox4x32_10(c, k, o);
 }
 
-static int hss_nullcoll(const orc_domain* d, double v[3], double mi, uint64_t seed, uint32_t id,
-                        uint32_t step, double* S, double* U, uint64_t* overflow) {
-    const double mn = d->gas_mass_kg;
-    const double sig_n = sqrt(ORC_KB * d->temperature_K / mn);
-    const double mean_th = sig_n * 1.5957691216057308;   /* E|th| = sigma*2*sqrt(2/pi) */
-    const double A = d->gas_density_m3 * d->sigma_m2 * d->dt_s;
-    const double Amean = A * mean_th;
-    const double* ug = d->gas_velocity_m_s;
-    double w[3] = {v[0] - ug[0], v[1] - ug[1], v[2] - ug[2]};
-    double gu = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
-    double Q = A * gu + Amean;
-    if (Q > 1.0) { Q = 1.0; ++*overflow; }
-    *S = *S - *S * Q;
-    if (!(*S < *U)) return 0;
+typedef struct { double A, Amean, mean_th, sig_n, mn, ug[3]; } gas_consts;
+
+static gas_consts gas_of(const orc_domain* d) {
+    gas_consts g;
+    g.mn = d->gas_mass_kg;
+    g.sig_n = sqrt(ORC_KB * d->temperature_K / g.mn);
+    g.mean_th = g.sig_n * 1.5957691216057308;   /* E|th| = sigma*2*sqrt(2/pi) */
+    g.A = d->gas_density_m3 * d->sigma_m2 * d->dt_s;
+    g.Amean = g.A * g.mean_th;
+    for (int c = 0; c < 3; ++c) g.ug[c] = d->gas_velocity_m_s[c];
+    return g;
+}
+
+static int nullcoll_candidate(const gas_consts* G, double v[3], double mi, uint64_t seed, uint32_t id,
+                              uint32_t step, int skip, double* clk, double qstar, double b) {
+    const double* ug = G->ug;
     uint32_t r0[4], r1[4];
     philox_words(seed, id, step, 0u, r0);
+    double uc = u32_to_unit(r0[1]);
+    if (skip) {
+        *clk = -log(u32_to_unit(r0[0]));
+        double w[3] = {v[0] - ug[0], v[1] - ug[1], v[2] - ug[2]};
+        b = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+        const double Q = G->A * b + G->Amean;
+        if (!(uc * qstar < Q)) return 0;
+        uc = uc * qstar / Q;
+    } else {
+        *clk = u32_to_unit(r0[0]);
+    }
     philox_words(seed, id, step, 1u, r1);
-    *U = u32_to_unit(r0[0]);
-    *S = 1.0;
-    const int thermal = u32_to_unit(r0[1]) * (gu + mean_th) < gu;
+    const int thermal = uc * (b + G->mean_th) < b;
     const double c3 = cos(2.0 * M_PI * u16_to_unit(r1[1] >> 16));
     const double sfac = thermal ? c3 * c3 : 1.0;
     const double r2 = -2.0 * (log(u32_to_unit(r0[3])) + log(u32_to_unit(r1[0])) * sfac);
-    const double rad = sig_n * sqrt(r2);
+    const double rad = G->sig_n * sqrt(r2);
     const double ct = 2.0 * u16_to_unit(r1[1] & 0xffffu) - 1.0;
     const double st = sqrt(fmax(0.0, 1.0 - ct * ct));
     const double ph = 2.0 * M_PI * u16_to_unit(r1[2] >> 16);
     double vn[3] = {ug[0] + rad * (st * cos(ph)), ug[1] + rad * (st * sin(ph)), ug[2] + rad * ct};
     double gv[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
     double g = sqrt(gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2]);
-    double q = A * (gu + rad);
-    double p = -expm1(-A * g);
+    double q = G->A * (b + rad);
+    double p = -expm1(-G->A * g);
     if (!(u32_to_unit(r0[2]) * q < p)) return 1;
     const double ct2 = 2.0 * u16_to_unit(r1[2] & 0xffffu) - 1.0;
     const double st2 = sqrt(fmax(0.0, 1.0 - ct2 * ct2));
     const double ph2 = 2.0 * M_PI * u16_to_unit(r1[3] >> 16);
     double dir[3] = {st2 * cos(ph2), st2 * sin(ph2), ct2};
+    const double mn = G->mn;
     double inv = 1.0 / (mi + mn);
     double fac = mn * inv;
     for (int c = 0; c < 3; ++c) {
@@ -389,12 +410,103 @@ static int hss_nullcoll(const orc_domain* d, double v[3], double mi, uint64_t se
     return 2;
 }
 
-void orc_clock_init(uint64_t seed, int64_t n, uint64_t first_id, double* S, double* U) {
+/* Per-step clock (RK4). */
+static int hss_nullcoll(const orc_domain* d, double v[3], double mi, uint64_t seed, uint32_t id,
+                        uint32_t step, double* S, double* U, uint64_t* overflow) {
+    const gas_consts G = gas_of(d);
+    double w[3] = {v[0] - G.ug[0], v[1] - G.ug[1], v[2] - G.ug[2]};
+    double gu = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    double Q = G.A * gu + G.Amean;
+    if (Q > 1.0) { Q = 1.0; ++*overflow; }
+    *S = *S - *S * Q;
+    if (!(*S < *U)) return -1;
+    const int r = nullcoll_candidate(&G, v, mi, seed, id, step, 0, U, 0.0, gu);
+    *S = 1.0;
+    return r;
+}
+
+/* Upper bound of |E| over the cylinder (same expression as the product's
+ * field_bound): |E0| + |G .* max|x - c|| + 2 (|U0| + |V|) r_axis / r0^2. */
+double orc_field_bound(const orc_domain* d) {
+    double E0[3] = {0.0, 0.0, 0.0}, Gv[3] = {0.0, 0.0, 0.0}, c[3] = {0.0, 0.0, 0.0};
+    int rf = fabs(d->rf_voltage_V) > ORC_MIN_VOLTAGE;
+    if (d->instrument == 0) {
+        E0[2] = d->axial_V / d->length_m;
+    } else if (d->instrument == 2) {
+        if (fabs(d->axial_V) > ORC_MIN_VOLTAGE) E0[2] = d->axial_V / d->length_m;
+    } else if (d->instrument == 1) {
+        double L = d->length_m, r = d->radius_m;
+        double dd = sqrt((L * L / 8.0) + (r * r / 4.0));
+        double factor = d->radial_V / (dd * dd);
+        Gv[0] = factor; Gv[1] = factor; Gv[2] = -2.0 * factor;
+        c[2] = 0.5 * L;
+    }
+    const double Rp = d->radius_m + ORC_GEOM_EPS;
+    const double ox = d->origin_m[0], oy = d->origin_m[1], oz = d->origin_m[2];
+    const double zmax_local = d->length_m + ORC_GEOM_EPS;
+    double e = sqrt(E0[0] * E0[0] + E0[1] * E0[1] + E0[2] * E0[2]);
+    const double ex = fabs(ox - c[0]) + Rp;
+    const double ey = fabs(oy - c[1]) + Rp;
+    const double ez = fmax(fabs(oz - c[2]), fabs(oz + zmax_local - c[2]));
+    const double gx = Gv[0] * ex, gy = Gv[1] * ey, gz = Gv[2] * ez;
+    e = e + sqrt(gx * gx + gy * gy + gz * gz);
+    if (rf) {
+        const double raxis = sqrt(ox * ox + oy * oy) + Rp;
+        e = e + 2.0 * (fabs(d->dc_quad_V) + fabs(d->rf_voltage_V)) * raxis / (d->radius_m * d->radius_m);
+    }
+    return e;
+}
+
+/* Skip clock of one ion (Boris). */
+typedef struct {
+    double tau, qstar, lam, dvmax, absu;
+    uint32_t next, start, H;
+} skip_clock;
+
+#define ORC_REFRESH 0x80000000u
+#define ORC_NEED_RESTART 0xFFFFFFFFu
+#define ORC_QCAP 0.99999904632568359375
+
+static void skip_setup(skip_clock* k, const orc_domain* d, const gas_consts* G, double q, double m) {
+    const double qm = q / m;
+    k->dvmax = fabs(qm) * orc_field_bound(d) * d->dt_s;
+    k->absu = sqrt(G->ug[0] * G->ug[0] + G->ug[1] * G->ug[1] + G->ug[2] * G->ug[2]);
+    double hz = 1.0 / sqrt(G->A * k->dvmax);
+    if (!(hz < 4096.0)) hz = 4096.0;
+    if (hz < 16.0) hz = 16.0;
+    k->H = (uint32_t)hz;
+    k->lam = (k->qstar > 0.0) ? -log1p(-k->qstar) : 0.0;
+}
+
+static void skip_restart(skip_clock* k, const gas_consts* G, const double v[3], uint32_t gs, uint64_t* overflow) {
+    const double v0 = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const double bstar = (v0 + k->absu + (double)k->H * k->dvmax) * 1.000001;
+    double qs = G->A * bstar + G->Amean;
+    if (qs > ORC_QCAP) { qs = ORC_QCAP; ++*overflow; }
+    k->qstar = qs;
+    k->lam = -log1p(-qs);
+    const double nf = ceil(k->tau / k->lam);
+    k->start = gs;
+    if (nf <= (double)k->H) k->next = gs + (nf < 1.0 ? 1u : (uint32_t)nf) - 1u;
+    else k->next = (gs + k->H - 1u) | ORC_REFRESH;
+}
+
+/* Initial clocks from u = uniform of Philox(id, 0, 3, 0).x: per-step clock
+ * S = 1, U = u; skip clock (skip != 0) tau = -ln u, restart pending. */
+void orc_clock_init(uint64_t seed, int64_t n, uint64_t first_id, double* S, double* U,
+                    uint32_t* next, uint32_t* start, int skip) {
     for (int64_t i = 0; i < n; ++i) {
         double r[4];
         draw4(seed, (uint32_t)(first_id + (uint64_t)i), 0u, 3u, r);
-        S[i] = 1.0;
-        U[i] = r[0];
+        if (skip) {
+            S[i] = -log(r[0]);
+            U[i] = 0.0;
+            next[i] = ORC_NEED_RESTART;
+            start[i] = 0u;
+        } else {
+            S[i] = 1.0;
+            U[i] = r[0];
+        }
     }
 }
 
@@ -419,7 +531,8 @@ static void add_moments(double* m, const double x[3], const double v[3], const d
  * Run n_steps engine steps for n ions of one domain.
  *   integrator: 0 Boris, 1 RK4
  *   collision:  0 none, 1 reference HSS (mt19937_64 seeded seed + id),
- *               2 null-collision HSS (Philox; needs clk_S/clk_U)
+ *               2 null-collision HSS (Philox; needs clk_S/clk_U, and for
+ *               Boris the skip-clock event arrays clk_next/clk_start)
  *   step0/t0:   engine step index and time at entry
  *   snap_every: moments of the active ions are accumulated after every
  *               snap_every-th step into moments[(k/snap_every) * 14 + ...]
@@ -434,9 +547,12 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
             int64_t n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
             const double* mass, const double* charge, uint8_t* active,
             double* t_death, double* t_arr, double* clk_S, double* clk_U,
+            uint32_t* clk_next, uint32_t* clk_start,
             uint64_t first_id, uint64_t step0, double t0, int64_t n_steps,
             int64_t snap_every, int64_t ref_step, double* moments, uint64_t* counters, int n_threads) {
     if (collision == 2 && (!clk_S || !clk_U)) return 1;
+    if (collision == 2 && integrator == 0 && (!clk_next || !clk_start)) return 1;
+    const gas_consts G = gas_of(d);
     const int64_t n_snap = (snap_every > 0) ? n_steps / snap_every : 0;
     if (n_snap > 0 && moments) memset(moments, 0, sizeof(double) * (size_t)(n_snap * ORC_N_MOMENTS));
     uint64_t cand_tot = 0, coll_tot = 0, ovf_tot = 0;
@@ -460,6 +576,21 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
             double S = clk_S ? clk_S[i] : 1.0, U = clk_U ? clk_U[i] : 0.0;
             uint32_t id = (uint32_t)(first_id + (uint64_t)i);
             if (collision == 1) mt64_seed(rng, seed + first_id + (uint64_t)i);
+            skip_clock sk;
+            memset(&sk, 0, sizeof(sk));
+            const int skip = (collision == 2 && integrator == 0);
+            if (skip) {
+                sk.tau = S;
+                sk.qstar = U;
+                sk.next = clk_next[i];
+                sk.start = clk_start[i];
+                skip_setup(&sk, d, &G, q, m);
+                if (act && contains(d, p) && sk.next == ORC_NEED_RESTART) {
+                    uint64_t ov = 0;
+                    skip_restart(&sk, &G, v, (uint32_t)step0, &ov);
+                    ovf_tot += ov;
+                }
+            }
             double t = t0;
             double ref[3] = {p[0], p[1], p[2]};
             for (int64_t k = 0; k < n_steps; ++k) {
@@ -475,11 +606,25 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                     else rk4_step(d, p, v, m, q, t, dt);
                     if (collision == 1) {
                         coll_tot += (uint64_t)hss_reference(d, v, m, rng);
+                    } else if (collision == 2 && skip) {
+                        const uint32_t gs = (uint32_t)(step0 + (uint64_t)k);
+                        if (sk.next != ORC_NEED_RESTART && gs == (sk.next & ~ORC_REFRESH)) {
+                            uint64_t ov = 0;
+                            if (sk.next & ORC_REFRESH) {
+                                sk.tau = sk.tau - (double)(gs + 1u - sk.start) * sk.lam;
+                            } else {
+                                int r = nullcoll_candidate(&G, v, m, seed, id, gs, 1, &sk.tau, sk.qstar, 0.0);
+                                if (r >= 1) ++cand_tot;
+                                if (r == 2) ++coll_tot;
+                            }
+                            skip_restart(&sk, &G, v, gs + 1u, &ov);
+                            ovf_tot += ov;
+                        }
                     } else if (collision == 2) {
                         uint64_t ov = 0;
                         int r = hss_nullcoll(d, v, m, seed, id, (uint32_t)(step0 + (uint64_t)k), &S, &U, &ov);
                         ovf_tot += ov;
-                        if (r > 0) ++cand_tot;
+                        if (r >= 1) ++cand_tot;
                         if (r == 2) ++coll_tot;
                     }
                     if (t_arr[i] < 0.0 && zold < zdet && p[2] >= zdet)
@@ -505,6 +650,12 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
             x[i] = p[0]; y[i] = p[1]; z[i] = p[2];
             vx[i] = v[0]; vy[i] = v[1]; vz[i] = v[2];
             active[i] = act;
+            if (skip) {
+                S = sk.tau;
+                U = sk.qstar;
+                clk_next[i] = sk.next;
+                clk_start[i] = sk.start;
+            }
             if (clk_S) clk_S[i] = S;
             if (clk_U) clk_U[i] = U;
         }

@@ -77,11 +77,13 @@ def lib() -> C.CDLL:
         L.orc_philox_many.argtypes = [C.c_int64, U32P, U32P, U32P]
         L.orc_unit_uniforms.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, DP]
         L.orc_field.argtypes = [C.POINTER(Domain), DP, C.c_double, DP]
-        L.orc_clock_init.argtypes = [C.c_uint64, C.c_int64, C.c_uint64, DP, DP]
+        L.orc_clock_init.argtypes = [C.c_uint64, C.c_int64, C.c_uint64, DP, DP, U32P, U32P, C.c_int]
+        L.orc_field_bound.argtypes = [C.POINTER(Domain)]
+        L.orc_field_bound.restype = C.c_double
         L.orc_thermal_width.argtypes = [C.c_double, C.c_double]
         L.orc_thermal_width.restype = C.c_double
         L.orc_run.argtypes = [C.POINTER(Domain), C.c_int, C.c_int, C.c_uint64, C.c_int64,
-                              DP, DP, DP, DP, DP, DP, DP, DP, U8P, DP, DP, DP, DP,
+                              DP, DP, DP, DP, DP, DP, DP, DP, U8P, DP, DP, DP, DP, U32P, U32P,
                               C.c_uint64, C.c_uint64, C.c_double, C.c_int64, C.c_int64, C.c_int64,
                               DP, U64P, C.c_int]
         L.orc_run.restype = C.c_int
@@ -91,6 +93,10 @@ def lib() -> C.CDLL:
 
 def _dp(a):
     return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _u32(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_uint32))
 
 
 def mt64_uniforms(seed: int, n: int) -> np.ndarray:
@@ -114,19 +120,22 @@ def run(domain: dict, state: dict, n_steps: int, *, integrator: int = 0, collisi
     """Run the restatement.  ``state`` holds float64 arrays x..vz, mass, charge,
     uint8 active and optional t_death / t_arrival; it is updated in place.
     collision: 0 none, 1 reference HSS (mt19937_64 per ion), 2 null-collision
-    HSS with Philox (needs ``clock`` = (S, U) arrays or None to initialise)."""
+    HSS with Philox (``clock`` = (S, U, next, start) arrays from a previous
+    call, or None to initialise; Boris uses the skip clock, RK4 the per-step
+    clock)."""
     d = domain_struct(domain)
     n = state["x"].shape[0]
     for k in ("t_death", "t_arrival"):
         if state.get(k) is None:
             state[k] = np.full(n, -1.0)
-    S = U = None
+    S = U = nxt = start = None
     if collision == 2:
         if clock is None:
             S, U = np.zeros(n), np.zeros(n)
-            lib().orc_clock_init(seed, n, first_id, _dp(S), _dp(U))
+            nxt, start = np.zeros(n, dtype=np.uint32), np.zeros(n, dtype=np.uint32)
+            lib().orc_clock_init(seed, n, first_id, _dp(S), _dp(U), _u32(nxt), _u32(start), 1 if integrator == 0 else 0)
         else:
-            S, U = clock
+            S, U, nxt, start = clock
     n_snap = n_steps // snap_every if snap_every > 0 else 0
     mom = np.zeros((max(n_snap, 1), N_MOMENTS))
     cnt = np.zeros(3, dtype=np.uint64)
@@ -135,13 +144,13 @@ def run(domain: dict, state: dict, n_steps: int, *, integrator: int = 0, collisi
                        _dp(state["vx"]), _dp(state["vy"]), _dp(state["vz"]),
                        _dp(state["mass"]), _dp(state["charge"]),
                        state["active"].ctypes.data_as(C.POINTER(C.c_uint8)),
-                       _dp(state["t_death"]), _dp(state["t_arrival"]), _dp(S), _dp(U),
+                       _dp(state["t_death"]), _dp(state["t_arrival"]), _dp(S), _dp(U), _u32(nxt), _u32(start),
                        first_id, step0, t0, n_steps, snap_every, ref_step,
                        _dp(mom) if n_snap else None, cnt.ctypes.data_as(C.POINTER(C.c_uint64)), threads)
     if rc != 0:
         raise RuntimeError(f"orc_run failed ({rc})")
     return {"moments": mom[:n_snap], "candidates": int(cnt[0]), "collisions": int(cnt[1]),
-            "rate_overflows": int(cnt[2]), "clock": (S, U)}
+            "rate_overflows": int(cnt[2]), "clock": (S, U, nxt, start)}
 
 
 # ---------------------------------------------------------------------------

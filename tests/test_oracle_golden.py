@@ -90,3 +90,28 @@ def test_nullcoll_scheme_reproduces_reference_collision_law():
     p = rates[1]
     se = np.sqrt(p * (1 - p) / (5 * n))
     assert abs(rates[2] - rates[1]) < 5 * np.sqrt(2) * se, rates
+
+
+def test_nullcoll_oracle_tracks_reference_code_over_20k_steps(golden):
+    """The null-collision scheme with the skip clock (oracle, FP64, Philox)
+    against the reference's own Boris + HSS run (golden ims_config0.npz) on
+    the same 4,096-ion cloud over the first 20,000 steps: collision fraction
+    within 1% and drift velocity within 4 combined standard errors."""
+    from helpers import config0_ensemble
+    from icarion_b200 import observables as ob
+    z = golden("ims_config0.npz")
+    n = int(z["n_ions"])
+    steps = 20000
+    e = config0_ensemble(detector_z_m=2.0e-3)
+    st = oracle_state(config0_ions(n))
+    r = orc.run(e, st, steps, integrator=0, collision=2, seed=123, snap_every=1000, ref_step=int(z["ref_step"]),
+                threads=8)
+    dt = float(z["dt"])
+    t = np.arange(1, steps // 1000 + 1) * 1000 * dt
+    mine = ob.fit_transport(t[3:], r["moments"][3:], t_ref=0.0)
+    ref = ob.fit_transport(t[3:], z["moments"][3:steps // 1000], t_ref=0.0)
+    assert abs(mine["v_drift"] - ref["v_drift"]) <= 4 * np.hypot(mine["se_v_drift"], ref["se_v_drift"]), (mine, ref)
+    # the reference collides in 8.8% of ion-steps at config 0
+    f_ref = float(z["collisions"]) / (n * int(z["steps"]))
+    f_me = r["collisions"] / (n * steps)
+    assert abs(f_me - f_ref) / f_ref < 0.01, (f_me, f_ref)
