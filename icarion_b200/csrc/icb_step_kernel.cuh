@@ -646,7 +646,9 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
         }
     }
     if constexpr (kSkip) {
-        if (live && do_coll && g_next == kNeedRestart) clock_restart(step0);
+        // restart from the velocity before this step's push (the unfused
+        // push call restarts for the collide call that follows)
+        if (live && (do_coll || do_push) && g_next == kNeedRestart) clock_restart(step0);
     }
 
     // exact finalize of the current step (SimulationEngineLifecycle.cpp:123-195)
@@ -723,7 +725,7 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
                             } else {
                                 new_limit();
                                 if constexpr (kSkip) {
-                                    if (do_coll && g_next == kNeedRestart) clock_restart(step0 + kk);
+                                    if ((do_coll || do_push) && g_next == kNeedRestart) clock_restart(step0 + kk);
                                 }
                             }
                         }
