@@ -43,9 +43,15 @@ DT = 5e-10
 EN_TD = 20.0
 METRIC = "ion-steps/s on 1 B200: mixed-prec vs plain FP64 at <=0.3% K0 error"
 WORKLOAD = "IMS drift, 1,048,576 ions (200 Da, +1, 150 A^2 HSS) in N2 300 K 1000 Pa, 20 Td, Boris + HSS, dt 5e-10 s"
-# bytes each ion moves per launch of the fused kernel:
-# read x,y,z(24) v(12) S,U(8) mass,charge(16) flags(1) t_arr(8); write x,y,z(24) v(12) S,U(8) flags(1)
-BYTES_PER_ION_LAUNCH = {"mixed": 114, "hilo": 114, "fp64": 69 + 12 + 8 + 45 + 12 + 8}
+# Algorithmic bytes each ion moves per launch of the fused kernel:
+# read  x,y,z(24) v(12) tau,Q*(8) next,start(8) mass,charge(16) flags(1) t_arr(8) = 77
+# write x,y,z(24) v(12) tau,Q*(8) next,start(8) flags(1)                          = 53
+# (hi/lo: positions 6 floats = 24 B as well; FP64: v and the clock are doubles: 97 + 73)
+BYTES_PER_ION_LAUNCH = {"mixed": 130, "hilo": 130, "fp64": 170}
+# DRAM bytes of one fused mixed launch at 1,048,576 ions from the ncu capture
+# summarised in profiles/k_step_mixed_fused_ims_1M.md (dram__bytes_read.sum +
+# dram__bytes_write.sum; writes still in L2 at kernel end are not counted).
+NCU_TRAFFIC_PER_LAUNCH = {"mixed": 81.245952e6 + 8.287232e6}
 
 
 def _env_rank():
@@ -355,7 +361,9 @@ def run_ours(args) -> None:
                    "collision_fraction": stt["collisions"] / max(ion_steps / world, 1)},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"],
+                     "frac": achieved / peaks["hbm_gbs"],
+                     "traffic": NCU_TRAFFIC_PER_LAUNCH.get(args.precision) if args.steps_per_launch == 1000 else None,
+                     "traffic_unit": "bytes per launch (ncu)", "peak_source": peaks["source"],
                      "kernel": f"k_step<{args.precision},boris,hss,uniform> fused {sim_K(None)} steps/launch",
                      "bytes_per_launch": bpl, "avg_launch_ms": avg_launch_ms,
                      "note": "fused K-step kernel: state crosses HBM once per launch, so it is instruction-issue "
