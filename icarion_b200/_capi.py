@@ -119,6 +119,9 @@ SIGNATURES = {
     "icb_mark_reference": (C.c_int, [_H]),
     "icb_generate_ions": (C.c_int, [C.c_uint32, C.c_int32, _P(SpeciesSpec), _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
     "icb_philox_eval": (C.c_int, [C.c_int, C.c_uint64, _U32P, C.c_uint64, C.c_int, _U32P]),
+    "icb_moments_noalloc": (C.c_int, [C.c_int, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

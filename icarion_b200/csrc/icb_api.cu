@@ -68,6 +68,11 @@ struct DevBuf {
 
 }  // namespace
 
+int icb::set_error(int code, const char* msg) {
+    g_last_error = msg;
+    return code;
+}
+
 // ---------------------------------------------------------------------------
 // auxiliary kernels
 // ---------------------------------------------------------------------------

@@ -15,4 +15,8 @@ cudaError_t launch_step_mixed(int integ, int coll, int field, bool mag, const St
 cudaError_t launch_step_hilo(int integ, int coll, int field, bool mag, const StepParams& p,
                              dim3 grid, dim3 block, cudaStream_t s);
 
+// Records the message icb_last_error() returns on this host thread and
+// passes `code` through.
+int set_error(int code, const char* msg);
+
 }  // namespace icb

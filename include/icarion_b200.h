@@ -217,6 +217,25 @@ int icb_moments(struct icb_handle* h, double* out);
 /* Store every ion's current position as its displacement reference. */
 int icb_mark_reference(struct icb_handle* h);
 
+/* ---- moments without device allocation -------------------------------- */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (an engine whose allocator reserves all device memory up front, or a
+ * fixed device-memory budget): the ICB_N_MOMENTS moments of one population
+ * from caller-owned device arrays (positions, velocities, displacement
+ * reference positions, active flags; arrival/death times may be NULL, then
+ * slots 11/12 are 0) into `out` (device, ICB_N_MOMENTS doubles), launched on
+ * `cuda_stream` (NULL = default stream).  Allocates nothing: partial sums go
+ * to a 640 KB file-scope device array, so n <= 33,554,432 ions (larger n is
+ * rejected with ICB_ERR_INVALID_ARGUMENT).  The first call on a device
+ * resolves that array's address and should come before any stream capture.
+ * All calls on a device share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller. */
+int icb_moments_noalloc(int device, uint64_t n, const double* x, const double* y, const double* z,
+                        const double* vx, const double* vy, const double* vz,
+                        const double* x_ref, const double* y_ref, const double* z_ref,
+                        const uint8_t* active, const double* arrival_time_s,
+                        const double* death_time_s, double* out, void* cuda_stream);
+
 /* ---- counter-based RNG check ------------------------------------------ */
 /* Evaluate the device Philox4x32-10 (use_curand = 0) or cuRAND's
  * curand_Philox4x32_10 (use_curand = 1) on n host counters (4 words each)
