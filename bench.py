@@ -42,6 +42,9 @@ STEPS_PER_BENCH_STEP = 1000
 DT = 5e-10
 EN_TD = 20.0
 METRIC = "ion-steps/s on 1 B200: mixed-prec vs plain FP64 at <=0.3% K0 error"
+SWEEP_WORKLOAD = ("E/N sweep, 64 ensembles (2-100 Td log-spaced, N2 300 K 1000 Pa), species 100/500/2000 Da "
+                  "(100/250/600 A^2) round-robin, {n:,} ions (log-uniform 1k-256k per ensemble, seed 123), "
+                  "dt = 0.1/nu_max per ensemble, Boris + HSS")
 WORKLOAD = "IMS drift, 1,048,576 ions (200 Da, +1, 150 A^2 HSS) in N2 300 K 1000 Pa, 20 Td, Boris + HSS, dt 5e-10 s"
 # Algorithmic bytes each ion moves per launch of the fused kernel:
 # read  x,y,z(24) v(12) tau,Q*(8) next,start(8) mass,charge(16) flags(1) t_arr(8) = 77
@@ -224,24 +227,36 @@ def run_ours(args) -> None:
     dev = torch.cuda.current_device()
     prec_id = {"mixed": capi.PREC_MIXED, "fp64": capi.PREC_FP64, "hilo": capi.PREC_MIXED_HILO}[args.precision]
 
-    domain = {"instrument": "IMS", "geometry": {"origin_m": [0.0, 0.0, -0.01], "length_m": 0.1, "radius_m": 0.05},
-              "env": {"temperature_K": 300.0, "pressure_Pa": 1000.0, "gas_species": "N2"},
-              "fields": {"DC": {"EN_Td": EN_TD}}}
-    ens = cfg.ensemble_params(domain, 150e-20, DT, detector_z_m=2.0e-3)
-    spec = cfg.species_spec(N_IONS, 200.0 * cfg.AMU_TO_KG, cfg.ELEM_CHARGE_C,
-                            {"type": "gaussian", "center": [0, 0, 0], "std": [5e-4] * 3},
-                            {"type": "thermal", "temperature_K": 300.0})
-    st0 = generate_ions(123, [spec])
-    first_id = rank * N_IONS
-    stream = torch.cuda.current_stream()
+    if args.workload == "en-sweep":
+        # batched E/N sweep: 64 ensembles in one launch sequence (CUDA graphs, autotuned shape)
+        from icarion_b200 import sweep
+        sw = sweep.en_sweep()
+        ensembles, st0, offsets, n_ions = sw.ensembles, sw.ions, sw.offsets, sw.n_ions
+        workload = SWEEP_WORKLOAD.format(n=n_ions)
+        args.graphs, args.autotune = True, True
+    else:
+        domain = {"instrument": "IMS", "geometry": {"origin_m": [0.0, 0.0, -0.01], "length_m": 0.1, "radius_m": 0.05},
+                  "env": {"temperature_K": 300.0, "pressure_Pa": 1000.0, "gas_species": "N2"},
+                  "fields": {"DC": {"EN_Td": EN_TD}}}
+        ensembles = [cfg.ensemble_params(domain, 150e-20, DT, detector_z_m=2.0e-3)]
+        spec = cfg.species_spec(N_IONS, 200.0 * cfg.AMU_TO_KG, cfg.ELEM_CHARGE_C,
+                                {"type": "gaussian", "center": [0, 0, 0], "std": [5e-4] * 3},
+                                {"type": "thermal", "temperature_K": 300.0})
+        st0, offsets, n_ions, workload = generate_ions(123, [spec]), None, N_IONS, WORKLOAD
+    first_id = rank * n_ions
+    n_ens = len(ensembles)
+    # a dedicated (non-default) stream: the library launches on it, and the
+    # timing events and the L2 flush are recorded on it too
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def make_sim(prec, K=args.steps_per_launch):
-        s = Simulation([ens], precision=prec, integrator=capi.INTEGRATOR_BORIS, collision=capi.COLLISION_HSS,
+        s = Simulation(ensembles, precision=prec, integrator=capi.INTEGRATOR_BORIS, collision=capi.COLLISION_HSS,
                        rng_seed=123, device=dev, steps_per_launch=K, block_size=args.block,
-                       pending_threshold=args.pending, steps_per_vote=args.spv)
+                       pending_threshold=args.pending, steps_per_vote=args.spv, use_graphs=int(args.graphs))
         s.set_stream(stream.cuda_stream)
-        s.upload(st0, first_id=first_id)
+        s.upload(st0, ens_offsets=offsets, first_id=first_id)
         return s
 
     def timed_loop(sim, n_steps, steps_per_bench, allreduce=True):
@@ -268,11 +283,12 @@ def run_ours(args) -> None:
         return args.steps_per_launch if args.steps_per_launch > 0 else 1000
 
     sim = make_sim(prec_id)
+    tuning = sim.autotune(500) if args.autotune else None
     # warm-up (same workload), then restart from the initial state
     for _ in range(args.warmup):
         sim.advance(STEPS_PER_BENCH_STEP)
-    sim.upload(st0, first_id=first_id)
-    sim.set_clock(0, np.zeros(1))
+    sim.upload(st0, ens_offsets=offsets, first_id=first_id)
+    sim.set_clock(0, np.zeros(n_ens))
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -284,13 +300,13 @@ def run_ours(args) -> None:
     if world > 1:
         dist.barrier()
     ms_max = parallel.max_over_ranks(ms)
-    ion_steps = N_IONS * STEPS_PER_BENCH_STEP * args.steps * world
+    ion_steps = n_ions * STEPS_PER_BENCH_STEP * args.steps * world
     value = ion_steps / (ms_max * 1e-3)
 
     # roofline of the dominant (fused step) kernel: algorithmic bytes per launch / mean launch duration
     peaks = measured_peaks()
     avg_launch_ms = kernel_ms / max(timed_launches, 1)
-    bpl = BYTES_PER_ION_LAUNCH[args.precision] * N_IONS
+    bpl = BYTES_PER_ION_LAUNCH[args.precision] * n_ions
     achieved = bpl / (avg_launch_ms * 1e-3) / 1e9
 
     # the same kernel in per-step form (one engine step per launch; state round-trips HBM every step)
@@ -308,25 +324,25 @@ def run_ours(args) -> None:
     if args.precision != "fp64" and args.fp64_steps > 0:
         s64 = make_sim(capi.PREC_FP64)
         s64.advance(STEPS_PER_BENCH_STEP)
-        s64.upload(st0, first_id=first_id)
+        s64.upload(st0, ens_offsets=offsets, first_id=first_id)
         torch.cuda.synchronize()
         ms64, _, _, _, _ = timed_loop(s64, args.fp64_steps, STEPS_PER_BENCH_STEP, allreduce=False)
         ms64 = parallel.max_over_ranks(ms64)
-        v64 = N_IONS * STEPS_PER_BENCH_STEP * args.fp64_steps * world / (ms64 * 1e-3)
+        v64 = n_ions * STEPS_PER_BENCH_STEP * args.fp64_steps * world / (ms64 * 1e-3)
         fp64_line = {"value": v64, "unit": "ion-steps/s", "steps": args.fp64_steps, "speedup_mixed_over_fp64": value / v64}
         s64.close()
 
     # end to end through the C ABI with host buffers: H2D state from pinned
     # memory, advance one snapshot interval, D2H state, every step
     e2e_steps = min(args.steps, args.e2e_steps)
-    pin = {k: torch.empty(N_IONS, dtype=torch.float64, pin_memory=True).numpy() for k in ("x", "y", "z", "vx", "vy", "vz")}
-    pin_act = torch.empty(N_IONS, dtype=torch.uint8, pin_memory=True).numpy()
+    pin = {k: torch.empty(n_ions, dtype=torch.float64, pin_memory=True).numpy() for k in ("x", "y", "z", "vx", "vy", "vz")}
+    pin_act = torch.empty(n_ions, dtype=torch.uint8, pin_memory=True).numpy()
     for k in pin:
         pin[k][:] = getattr(st0, k)
     pin_act[:] = 1
     host = IonState(x=pin["x"], y=pin["y"], z=pin["z"], vx=pin["vx"], vy=pin["vy"], vz=pin["vz"], mass=st0.mass,
                     charge=st0.charge, active=pin_act, t_death=None, t_arrival=None)
-    sim.upload(st0, first_id=first_id)
+    sim.upload(st0, ens_offsets=offsets, first_id=first_id)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -339,10 +355,12 @@ def run_ours(args) -> None:
                                                 capi.u8ptr(host.active), None, None))
     torch.cuda.synchronize()
     e2e_s = parallel.max_over_ranks(time.perf_counter() - t0)
-    e2e_value = N_IONS * STEPS_PER_BENCH_STEP * e2e_steps * world / e2e_s
+    e2e_value = n_ions * STEPS_PER_BENCH_STEP * e2e_steps * world / e2e_s
     sim.close()
 
-    cpu = cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    # the CPU sample is the single-ensemble IMS workload; no CPU line for the sweep
+    cpu = (cpu_baseline() if (rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "ims-1M")
+           else None)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -354,11 +372,12 @@ def run_ours(args) -> None:
         "vs_baseline": None, "dtype": {"mixed": "f32 (v, field, collisions) + f64 (x, t)", "fp64": "f64",
                                        "hilo": "f32 (v) + f32 hi/lo (x)"}[args.precision],
         "data": "synthetic (reference ion-loader semantics, seed 123)",
-        "config": {"workload": WORKLOAD, "ions_per_gpu": N_IONS, "engine_steps_per_bench_step": STEPS_PER_BENCH_STEP,
+        "config": {"workload": workload, "ions_per_gpu": n_ions, "engine_steps_per_bench_step": STEPS_PER_BENCH_STEP,
                    "total_engine_steps": STEPS_PER_BENCH_STEP * args.steps, "precision": args.precision,
                    "steps_per_launch": sim_K(None), "collisions": "HSS null-collision, Philox4x32-10",
                    "parallelism": f"ions sharded, {world} GPU(s)", "l2": "flushed between timed steps (256 MB write)",
-                   "collision_fraction": stt["collisions"] / max(ion_steps / world, 1)},
+                   "collision_fraction": stt["collisions"] / max(ion_steps / world, 1),
+                   "cuda_graphs": bool(args.graphs), "autotuned": tuning},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"],
@@ -371,10 +390,10 @@ def run_ours(args) -> None:
         "roofline_per_step": {"bound": "hbm", "achieved": ach1, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                               "frac": ach1 / peaks["hbm_gbs"], "avg_launch_ms": avg1,
                               "kernel": f"k_step<{args.precision},boris,hss,uniform> 1 step/launch",
-                              "ion_steps_per_s": N_IONS / (avg1 * 1e-3)},
+                              "ion_steps_per_s": n_ions / (avg1 * 1e-3)},
         "fp64_form": fp64_line,
-        "e2e": {"value": e2e_value, "unit": "ion-steps/s", "h2d_bytes_per_step": 6 * 8 * N_IONS,
-                "d2h_bytes_per_step": 6 * 8 * N_IONS + N_IONS, "steps": e2e_steps,
+        "e2e": {"value": e2e_value, "unit": "ion-steps/s", "h2d_bytes_per_step": 6 * 8 * n_ions,
+                "d2h_bytes_per_step": 6 * 8 * n_ions + n_ions, "steps": e2e_steps,
                 "path": "icb_update_state (pinned host) -> icb_advance(1000) -> icb_download_ions (pinned host)"},
         "clocks": clk,
         "cpu_baseline": cpu,
@@ -393,6 +412,10 @@ def main():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--pending", type=int, default=0)
     ap.add_argument("--spv", type=int, default=0, help="collision-free steps between warp votes")
+    ap.add_argument("--workload", choices=["ims-1M", "en-sweep"], default="ims-1M",
+                    help="ims-1M: the 1,048,576-ion IMS run (default); en-sweep: the batched 64-ensemble E/N sweep")
+    ap.add_argument("--autotune", action="store_true", help="pick the launch shape with icb_autotune first")
+    ap.add_argument("--graphs", action="store_true", help="replay icb_advance through CUDA graphs")
     ap.add_argument("--fp64-steps", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")

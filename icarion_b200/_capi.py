@@ -80,6 +80,17 @@ class RunStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Tuning(C.Structure):
+    _fields_ = [
+        ("block_size", C.c_int32), ("steps_per_vote", C.c_int32), ("pending_threshold", C.c_int32),
+        ("steps_per_launch", C.c_int32), ("trials", C.c_int32), ("reserved", C.c_int32),
+        ("ion_steps_per_s", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class SpeciesSpec(C.Structure):
     _fields_ = [
         ("count", C.c_uint64), ("mass_kg", C.c_double), ("charge_C", C.c_double),
@@ -117,6 +128,7 @@ SIGNATURES = {
     "icb_set_clock": (C.c_int, [_H, C.c_uint64, _DP]),
     "icb_moments": (C.c_int, [_H, _DP]),
     "icb_mark_reference": (C.c_int, [_H]),
+    "icb_autotune": (C.c_int, [_H, C.c_uint64, _P(Tuning)]),
     "icb_generate_ions": (C.c_int, [C.c_uint32, C.c_int32, _P(SpeciesSpec), _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
     "icb_philox_eval": (C.c_int, [C.c_int, C.c_uint64, _U32P, C.c_uint64, C.c_int, _U32P]),
     "icb_moments_noalloc": (C.c_int, [C.c_int, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

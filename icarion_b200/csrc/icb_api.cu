@@ -285,7 +285,21 @@ struct icb_handle {
     void* vx() const { return fp64() ? static_cast<void*>(vxd.p) : static_cast<void*>(vxf.p); }
     void* vy() const { return fp64() ? static_cast<void*>(vyd.p) : static_cast<void*>(vyf.p); }
     void* vz() const { return fp64() ? static_cast<void*>(vzd.p) : static_cast<void*>(vzf.p); }
+    // CUDA graph of one icb_advance(graph_steps) launch sequence; rebuilt when
+    // anything baked into it changes (state arrays, stream, launch shape).
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_steps = 0;
+    uint64_t graph_gen = 0;
+    uint64_t graph_launches = 0;
+    uint64_t gen = 1;                  // bumped whenever the graph goes stale
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        graph_steps = 0;
+    }
+
     ~icb_handle() {
+        drop_graph();
         for (cudaEvent_t e : kev) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -439,6 +453,30 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
     return ICB_OK;
 }
 
+// The launch sequence of icb_advance(n_steps): counter reset, then per chunk
+// of at most K steps the fused step kernel(s) and the device clock update.
+// The first n_timed chunks are bracketed by events for per-kernel timing.
+int enqueue_advance(icb_handle* h, uint64_t n_steps, size_t n_timed) {
+    cudaStream_t s = h->stream;
+    ICB_CUDA(cudaMemsetAsync(h->counters.p, 0, kNumCounters * sizeof(unsigned long long), s));
+    h->launches = 0;
+    const int ne = static_cast<int>(h->ens.size());
+    uint64_t left = n_steps;
+    size_t j = 0;
+    while (left > 0) {
+        const uint32_t K = static_cast<uint32_t>(std::min<uint64_t>(left, h->K));
+        if (j < n_timed) ICB_CUDA(cudaEventRecord(h->kev[2 * j], s));
+        if (int r = launch_step(h, K, 1, 1, 1)) return r;
+        if (j < n_timed) ICB_CUDA(cudaEventRecord(h->kev[2 * j + 1], s));
+        k_clock_advance<<<(ne + 127) / 128, 128, 0, s>>>(h->step_dev.p, h->t_dev.p, h->dt_dev.p, ne, K);
+        ICB_CUDA(cudaGetLastError());
+        ++h->launches;
+        left -= K;
+        ++j;
+    }
+    return ICB_OK;
+}
+
 int read_stats(icb_handle* h, icb_run_stats* st, uint64_t steps, size_t n_timed_launches) {
     unsigned long long c[kNumCounters];
     ICB_CUDA(cudaMemcpyAsync(c, h->counters.p, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
@@ -461,6 +499,27 @@ int read_stats(icb_handle* h, icb_run_stats* st, uint64_t steps, size_t n_timed_
     st->arrivals = c[kCntArrivals];
     st->device_ms = static_cast<double>(ms);
     return ICB_OK;
+}
+
+template <class T>
+void add_state(std::vector<std::pair<void*, size_t>>& v, DevBuf<T>& b) {
+    if (b.p) v.emplace_back(static_cast<void*>(b.p), b.n * sizeof(T));
+}
+
+// Device buffers that a step changes (allocated ones only), for the
+// autotuner's save/restore.
+std::vector<std::pair<void*, size_t>> mutable_state(icb_handle* h) {
+    std::vector<std::pair<void*, size_t>> v;
+    add_state(v, h->x); add_state(v, h->y); add_state(v, h->z);
+    add_state(v, h->xh); add_state(v, h->xl); add_state(v, h->yh);
+    add_state(v, h->yl); add_state(v, h->zh); add_state(v, h->zl);
+    add_state(v, h->vxd); add_state(v, h->vyd); add_state(v, h->vzd);
+    add_state(v, h->vxf); add_state(v, h->vyf); add_state(v, h->vzf);
+    add_state(v, h->Sd); add_state(v, h->Ud); add_state(v, h->Sf); add_state(v, h->Uf);
+    add_state(v, h->clk_next); add_state(v, h->clk_start);
+    add_state(v, h->flags); add_state(v, h->t_death); add_state(v, h->t_arr); add_state(v, h->zprev);
+    add_state(v, h->step_dev); add_state(v, h->t_dev);
+    return v;
 }
 
 }  // namespace
@@ -563,6 +622,7 @@ int icb_destroy(icb_handle* h) {
 int icb_set_stream(icb_handle* h, void* cuda_stream) {
     if (int r = check_handle(h)) return r;
     h->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : h->own_stream;
+    ++h->gen;
     return ICB_OK;
 }
 
@@ -622,6 +682,7 @@ int icb_upload_ions(icb_handle* h, uint64_t n,
         h->n = n;
     }
     h->first_id = first_ion_id;
+    ++h->gen;
     h->ens_off = off;
     cudaStream_t s = h->stream;
     const unsigned g = grid_for(n, 256);
@@ -790,10 +851,39 @@ int icb_advance(icb_handle* h, uint64_t n_steps, icb_run_stats* stats) {
         return fail(ICB_ERR_INVALID_ARGUMENT, "runs are limited to 2^31 engine steps");
     h->host_step += n_steps;
     cudaStream_t s = h->stream;
-    ICB_CUDA(cudaMemsetAsync(h->counters.p, 0, kNumCounters * sizeof(unsigned long long), s));
+    if (h->cfg.use_graphs) {
+        // Replay one captured graph per distinct n_steps: counters reset, the
+        // fused step launches and the device clock updates.
+        if (!h->graph || h->graph_steps != n_steps || h->graph_gen != h->gen) {
+            h->drop_graph();
+            // Captured on the handle's own non-blocking stream (capture is
+            // not allowed on the legacy default stream); replayed on h->stream.
+            cudaGraph_t g = nullptr;
+            ICB_CUDA(cudaStreamBeginCapture(h->own_stream, cudaStreamCaptureModeThreadLocal));
+            h->stream = h->own_stream;
+            int r = enqueue_advance(h, n_steps, 0);
+            h->stream = s;
+            cudaError_t ce = cudaStreamEndCapture(h->own_stream, &g);
+            if (r != ICB_OK) { if (g) cudaGraphDestroy(g); return r; }
+            if (ce != cudaSuccess) return fail(ICB_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+            ce = cudaGraphInstantiate(&h->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) { h->graph = nullptr; return fail(ICB_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(ce)); }
+            h->graph_steps = n_steps;
+            h->graph_gen = h->gen;
+            h->graph_launches = h->launches;
+        }
+        ICB_CUDA(cudaEventRecord(h->ev0, s));
+        ICB_CUDA(cudaGraphLaunch(h->graph, s));
+        ICB_CUDA(cudaEventRecord(h->ev1, s));
+        h->launches = h->graph_launches;
+        if (stats) {
+            if (int r = read_stats(h, stats, n_steps, 0)) return r;
+            stats->step_kernel_ms = stats->device_ms;   // kernels are not timed one by one inside a graph
+        }
+        return ICB_OK;
+    }
     ICB_CUDA(cudaEventRecord(h->ev0, s));
-    h->launches = 0;
-    const int ne = static_cast<int>(h->ens.size());
     // Per-launch events around the step kernels when statistics are asked
     // for (at most 64 launches are timed individually per call).
     const size_t n_launch = static_cast<size_t>((n_steps + h->K - 1) / h->K);
@@ -803,21 +893,93 @@ int icb_advance(icb_handle* h, uint64_t n_steps, icb_run_stats* stats) {
         ICB_CUDA(cudaEventCreate(&e));
         h->kev.push_back(e);
     }
-    uint64_t left = n_steps;
-    size_t j = 0;
-    while (left > 0) {
-        const uint32_t K = static_cast<uint32_t>(std::min<uint64_t>(left, h->K));
-        if (j < n_timed) ICB_CUDA(cudaEventRecord(h->kev[2 * j], s));
-        if (int r = launch_step(h, K, 1, 1, 1)) return r;
-        if (j < n_timed) ICB_CUDA(cudaEventRecord(h->kev[2 * j + 1], s));
-        k_clock_advance<<<(ne + 127) / 128, 128, 0, s>>>(h->step_dev.p, h->t_dev.p, h->dt_dev.p, ne, K);
-        ICB_CUDA(cudaGetLastError());
-        ++h->launches;
-        left -= K;
-        ++j;
-    }
+    if (int r = enqueue_advance(h, n_steps, n_timed)) return r;
     ICB_CUDA(cudaEventRecord(h->ev1, s));
     if (stats) return read_stats(h, stats, n_steps, n_timed);
+    return ICB_OK;
+}
+
+int icb_autotune(icb_handle* h, uint64_t trial_steps, icb_tuning* out) {
+    if (int r = check_handle(h)) return r;
+    if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
+    if (trial_steps == 0) trial_steps = 500;
+    if (trial_steps > 100000) return fail(ICB_ERR_INVALID_ARGUMENT, "trial_steps must be <= 100000");
+    if (h->host_step + trial_steps >= (1ull << 31))
+        return fail(ICB_ERR_INVALID_ARGUMENT, "runs are limited to 2^31 engine steps");
+    cudaStream_t s = h->stream;
+    // Save the state once; every trial starts from it and it is put back at
+    // the end, so the handle's trajectory is unchanged by tuning.
+    const auto bufs = mutable_state(h);
+    size_t total = 0;
+    for (const auto& b : bufs) total += (b.second + 255) & ~size_t(255);
+    DevBuf<uint8_t> saved;
+    ICB_CUDA(saved.alloc(total));
+    auto copy_all = [&](bool save) -> cudaError_t {
+        size_t off = 0;
+        for (const auto& b : bufs) {
+            void* dst = save ? static_cast<void*>(saved.p + off) : b.first;
+            const void* src = save ? b.first : static_cast<const void*>(saved.p + off);
+            cudaError_t e = cudaMemcpyAsync(dst, src, b.second, cudaMemcpyDeviceToDevice, s);
+            if (e != cudaSuccess) return e;
+            off += (b.second + 255) & ~size_t(255);
+        }
+        return cudaSuccess;
+    };
+    ICB_CUDA(copy_all(true));
+    const int blk0 = h->block;
+    const uint32_t spv0 = h->spv, pend0 = h->pend;
+    const int blocks[] = {64, 128};
+    const uint32_t spvs[] = {4, 8, 16};
+    const uint32_t pends[] = {6, 10, 14};
+    const bool coll = h->coll != kCollNone;
+    double best_ms = 1e300;
+    int best_blk = blk0;
+    uint32_t best_spv = spv0, best_pend = pend0;
+    int trials = 0;
+    auto timed = [&](int blk, uint32_t spv, uint32_t pend, float* ms) -> int {
+        h->block = blk; h->spv = spv; h->pend = pend;
+        ICB_CUDA(copy_all(false));
+        ICB_CUDA(cudaEventRecord(h->ev0, s));
+        if (int r = enqueue_advance(h, trial_steps, 0)) return r;
+        ICB_CUDA(cudaEventRecord(h->ev1, s));
+        ICB_CUDA(cudaEventSynchronize(h->ev1));
+        ICB_CUDA(cudaEventElapsedTime(ms, h->ev0, h->ev1));
+        return ICB_OK;
+    };
+    int rc = ICB_OK;
+    float ms = 0.f;
+    rc = timed(blk0, spv0, pend0, &ms);   // warm-up
+    for (int blk : blocks) {
+        for (uint32_t spv : spvs) {
+            for (uint32_t pend : pends) {
+                if (rc != ICB_OK) break;
+                if (!coll && pend != pends[0]) continue;   // the threshold only matters with collisions
+                const uint32_t pe = coll ? pend : pend0;
+                float m0 = 0.f, m1 = 0.f;
+                if ((rc = timed(blk, spv, pe, &m0)) != ICB_OK) break;
+                if ((rc = timed(blk, spv, pe, &m1)) != ICB_OK) break;
+                ++trials;
+                const double m = std::min(m0, m1);
+                if (m < best_ms) { best_ms = m; best_blk = blk; best_spv = spv; best_pend = pe; }
+            }
+        }
+    }
+    // Back to the saved state with the chosen shape (or the old one on error).
+    if (rc == ICB_OK) { h->block = best_blk; h->spv = best_spv; h->pend = best_pend; }
+    else { h->block = blk0; h->spv = spv0; h->pend = pend0; }
+    ICB_CUDA(copy_all(false));
+    ICB_CUDA(cudaStreamSynchronize(s));
+    ++h->gen;
+    if (rc != ICB_OK) return rc;
+    if (out) {
+        std::memset(out, 0, sizeof(*out));
+        out->block_size = h->block;
+        out->steps_per_vote = static_cast<int32_t>(h->spv);
+        out->pending_threshold = static_cast<int32_t>(h->pend);
+        out->steps_per_launch = static_cast<int32_t>(h->K);
+        out->trials = trials;
+        out->ion_steps_per_s = static_cast<double>(h->n) * static_cast<double>(trial_steps) / (best_ms * 1e-3);
+    }
     return ICB_OK;
 }
 

@@ -201,6 +201,13 @@ class Simulation:
     def mark_reference(self) -> None:
         capi.check(self._lib.icb_mark_reference(self._h))
 
+    def autotune(self, trial_steps: int = 0) -> dict:
+        """Pick the fastest launch shape on the uploaded ions; the state and
+        clock are restored, so the run continues unchanged (see icb_autotune)."""
+        t = capi.Tuning()
+        capi.check(self._lib.icb_autotune(self._h, trial_steps, C.byref(t)))
+        return t.as_dict()
+
     def run(self, n_steps: int, write_interval: int, ref_step: int = 0) -> tuple[np.ndarray, np.ndarray, dict]:
         """Advance n_steps, taking moments every write_interval steps (the
         engine's snapshot cadence).  Displacement moments are relative to the

@@ -217,6 +217,26 @@ int icb_moments(struct icb_handle* h, double* out);
 /* Store every ion's current position as its displacement reference. */
 int icb_mark_reference(struct icb_handle* h);
 
+/* ---- launch-shape tuning ----------------------------------------------- */
+typedef struct icb_tuning {
+    int32_t block_size;        /* threads per block chosen */
+    int32_t steps_per_vote;    /* collision-free steps between warp votes chosen */
+    int32_t pending_threshold; /* deferred-collision batch size chosen */
+    int32_t steps_per_launch;  /* unchanged by tuning */
+    int32_t trials;            /* launch shapes timed */
+    int32_t reserved;
+    double ion_steps_per_s;    /* trial throughput of the chosen shape */
+} icb_tuning;
+/* No counterpart in the reference (its batch path has no launch shape).
+ * Times trial_steps (0 = 500) fused steps of the uploaded ions under each
+ * launch shape (block 64/128 x steps per vote 4/8/16 x pending threshold
+ * 6/10/14), each from the same saved copy of the state, keeps the fastest
+ * and restores the state and clock: the trajectory continues as if the call
+ * had not been made.  In FP64 every shape gives bit-identical results; in
+ * the float forms the shape moves where float position offsets are folded
+ * into the double anchor, so results change at float rounding level. */
+int icb_autotune(struct icb_handle* h, uint64_t trial_steps, icb_tuning* out);
+
 /* ---- moments without device allocation -------------------------------- */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (an engine whose allocator reserves all device memory up front, or a

@@ -133,6 +133,54 @@ def test_results_independent_of_launch_shape():
             assert np.array_equal(getattr(o, k), getattr(outs[0], k)), k
 
 
+def _chunks(st0, e, chunks, precision, **kw):
+    with Simulation([e], precision=precision, integrator=capi.INTEGRATOR_BORIS, collision=capi.COLLISION_HSS,
+                    rng_seed=123, **kw) as sim:
+        sim.upload(st0)
+        stats = [sim.advance(k) for k in chunks]
+        return sim.download(), sim.clock(), stats
+
+
+@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_MIXED])
+def test_graph_replay_equals_direct_launches(precision):
+    """icb_advance through a captured CUDA graph (replayed for repeated
+    n_steps, recaptured when n_steps changes) gives the direct-launch result
+    bit for bit, with the same counters and device clock."""
+    e = config0_ensemble()
+    st0 = config0_ions(3000)
+    chunks = (300, 300, 300, 125, 300)
+    direct, c0, s0 = _chunks(st0, e, chunks, precision, steps_per_launch=128)
+    graph, c1, s1 = _chunks(st0, e, chunks, precision, steps_per_launch=128, use_graphs=1)
+    for k in KEYS:
+        assert np.array_equal(getattr(graph, k), getattr(direct, k)), k
+    assert c0[0] == c1[0] == sum(chunks) and np.array_equal(c0[1], c1[1])
+    for a, b in zip(s0, s1):
+        assert (a["collisions"], a["candidates"], a["kernel_launches"]) == \
+               (b["collisions"], b["candidates"], b["kernel_launches"])
+
+
+def test_autotune_restores_state_and_keeps_fp64_results():
+    """icb_autotune times launch shapes from a saved copy of the state and
+    puts it back: an FP64 run tuned half way equals an untuned run bit for bit."""
+    e = config0_ensemble()
+    st0 = config0_ions(4000)
+    plain, c0, _ = _chunks(st0, e, (400, 600), capi.PREC_FP64)
+    with Simulation([e], precision=capi.PREC_FP64, integrator=capi.INTEGRATOR_BORIS, collision=capi.COLLISION_HSS,
+                    rng_seed=123) as sim:
+        sim.upload(st0)
+        sim.advance(400)
+        t = sim.autotune(trial_steps=200)
+        assert sim.clock()[0] == 400
+        sim.advance(600)
+        tuned = sim.download()
+        c1 = sim.clock()
+    assert t["trials"] == 18 and t["block_size"] in (64, 128) and t["ion_steps_per_s"] > 0
+    assert t["steps_per_vote"] in (4, 8, 16) and t["pending_threshold"] in (6, 10, 14)
+    for k in KEYS:
+        assert np.array_equal(getattr(tuned, k), getattr(plain, k)), k
+    assert c0[0] == c1[0] and np.array_equal(c0[1], c1[1])
+
+
 def test_unfused_plug_points_equal_fused_step():
     """push (step_batch) -> collide (handle_batch) -> finalize, one call each
     per step, gives the fused icb_advance result bit for bit (FP64)."""
