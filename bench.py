@@ -401,6 +401,108 @@ def run_ours(args) -> None:
     print(json.dumps(line))
 
 
+def run_fticr(args) -> None:
+    """FT-ICR cell with space charge (262,144 ions, P3M on a 128^3 mesh, one
+    solve per engine step): ion-steps/s of the whole step and the P3M solve
+    time per step.  One GPU, replicas only under torchrun."""
+    import torch
+
+    sys.path.insert(0, str(ROOT))
+    from icarion_b200 import _capi as capi
+    from icarion_b200 import fticr
+    from icarion_b200.sim import Simulation
+
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local if world > 1 else 0)
+    dev = torch.cuda.current_device()
+    prec_id = {"mixed": capi.PREC_MIXED, "fp64": capi.PREC_FP64}[args.precision if args.precision != "hilo" else "mixed"]
+    cell = fticr.fticr_cell()
+    n = cell.ions.n
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    steps_per = 100
+    sim = Simulation([cell.ensemble], precision=prec_id, integrator=capi.INTEGRATOR_BORIS,
+                     collision=capi.COLLISION_LANGEVIN, rng_seed=123, device=dev, use_graphs=int(args.graphs))
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(cell.ions, first_id=rank * n)
+    fticr.configure(sim, cell)
+    for _ in range(args.warmup):
+        sim.advance(steps_per)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)).split(",")[0]) if world == 1 else dev)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sc_ms, sc_n, step_ms, step_n, launches = 0.0, 0, 0.0, 0, 0
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        rs = sim.advance(steps_per)
+        ev[i][1].record(stream)
+        sc_ms += rs["spacecharge_ms"]
+        sc_n += rs["spacecharge_solves_timed"]
+        step_ms += rs["step_kernel_ms"]
+        step_n += min(steps_per, 64)
+        launches += rs["kernel_launches"]
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    value = n * steps_per * args.steps / (ms * 1e-3)
+    p3m_ms = sc_ms / max(sc_n, 1)
+    # algorithmic HBM bytes of one isolated P3M solve on the (2*128)^3 grid:
+    # deposit write, forward FFT read+write, 3 x (kernel multiply: 2 reads +
+    # 1 write, inverse FFT read+write) of the real (8 B) / half-complex
+    # (16 B x (M/2+1)/M) grids, plus per ion position/charge reads, keys and
+    # the 8-node x 3-component gather
+    M = 2 * cell.sc_grid[0]
+    real_b = 8.0 * M ** 3
+    cplx_b = 16.0 * M * M * (M // 2 + 1)
+    grid_bytes = real_b + (real_b + cplx_b) + 3 * (3 * cplx_b) + 3 * (cplx_b + real_b)
+    ion_bytes = n * (33 + 32 + 24 + 192 + 24)
+    p3m_bytes = grid_bytes + ion_bytes
+    achieved = p3m_bytes / (p3m_ms * 1e-3) / 1e9
+    peaks = measured_peaks()
+    # end to end: host state in, steps_per steps, host state out, per bench step
+    e2e_steps = min(args.steps, args.e2e_steps)
+    host = sim.download()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sim.update_state(host)
+        sim.advance(steps_per)
+        sim.download(into=host)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    sim.close()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "ion-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {capi.PREC_MIXED: "f32 (v, field) + f64 (x, t, space charge)",
+                                       capi.PREC_FP64: "f64"}[prec_id],
+        "data": "synthetic (reference ion-loader semantics, seed 123; m/z uniform 500-1500)",
+        "config": {"workload": "FT-ICR cell, 262,144 ions (+1, m/z 500-1500), 7 T, 1 V quadrupolar trap, "
+                               "He 1e-7 Pa Langevin capture, Boris dt 1e-9 s, P3M space charge 128^3 CIC "
+                               "(isolated, 2-cell particle-particle cutoff) solved every step",
+                   "ions_per_gpu": n, "engine_steps_per_bench_step": steps_per, "precision": args.precision,
+                   "parallelism": "replicas" if world > 1 else "1 GPU", "l2": "flushed between timed steps",
+                   "cuda_graphs": bool(args.graphs), "p3m_ms_per_step": p3m_ms,
+                   "push_ms_per_step": step_ms / max(step_n, 1)},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"],
+                     "kernel": "isolated P3M solve (bin, sort, deposit, FFTs, kernel multiplies, gather + PP)",
+                     "bytes_per_solve": p3m_bytes},
+        "e2e": {"value": n * steps_per * e2e_steps / e2e_s, "unit": "ion-steps/s", "h2d_bytes_per_step": 6 * 8 * n + n,
+                "d2h_bytes_per_step": 6 * 8 * n + n + 2 * 8 * n, "steps": e2e_steps},
+        "clocks": clk,
+        "cpu_baseline": None,
+        "cpu_baseline_note": "the reference's CPU space charge is an O(N^2) direct sum; no bounded sample of this "
+                             "workload is timed",
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -412,8 +514,9 @@ def main():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--pending", type=int, default=0)
     ap.add_argument("--spv", type=int, default=0, help="collision-free steps between warp votes")
-    ap.add_argument("--workload", choices=["ims-1M", "en-sweep"], default="ims-1M",
-                    help="ims-1M: the 1,048,576-ion IMS run (default); en-sweep: the batched 64-ensemble E/N sweep")
+    ap.add_argument("--workload", choices=["ims-1M", "en-sweep", "fticr-sc"], default="ims-1M",
+                    help="ims-1M: the 1,048,576-ion IMS run (default); en-sweep: the batched 64-ensemble E/N "
+                         "sweep; fticr-sc: the 262,144-ion FT-ICR cell with P3M space charge")
     ap.add_argument("--autotune", action="store_true", help="pick the launch shape with icb_autotune first")
     ap.add_argument("--graphs", action="store_true", help="replay icb_advance through CUDA graphs")
     ap.add_argument("--fp64-steps", type=int, default=10)
@@ -424,6 +527,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.workload == "fticr-sc":
+        run_fticr(args)
     else:
         run_ours(args)
 

@@ -27,6 +27,7 @@ PREC_FP64, PREC_MIXED, PREC_MIXED_HILO = 0, 1, 2
 INTEGRATOR_BORIS, INTEGRATOR_RK4 = 0, 1
 COLLISION_NONE, COLLISION_HSS, COLLISION_IPM_TABLE, COLLISION_IPM_MLP, COLLISION_LANGEVIN = 0, 1, 2, 3, 4
 INSTRUMENT_IMS, INSTRUMENT_FTICR, INSTRUMENT_QUADRUPOLE_RF = 0, 1, 2
+SC_OFF, SC_P3M_ISOLATED, SC_PM_PERIODIC_REF = 0, 1, 2
 POS_POINT, POS_GAUSSIAN, POS_UNIFORM_SPHERE, POS_UNIFORM_CYLINDER, POS_UNIFORM_BOX = 0, 1, 2, 3, 4
 VEL_FIXED, VEL_THERMAL = 0, 1
 N_MOMENTS = 20
@@ -74,10 +75,19 @@ class RunStats(C.Structure):
         ("steps", C.c_uint64), ("candidates", C.c_uint64), ("collisions", C.c_uint64),
         ("rate_overflows", C.c_uint64), ("deaths", C.c_uint64), ("arrivals", C.c_uint64),
         ("device_ms", C.c_double), ("step_kernel_ms", C.c_double), ("kernel_launches", C.c_uint64),
+        ("spacecharge_ms", C.c_double), ("spacecharge_solves_timed", C.c_uint64),
     ]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class SpaceChargeConfig(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int32), ("grid_n", C.c_int32 * 3), ("box_min_m", D3), ("box_max_m", D3),
+        ("alpha_h", C.c_double), ("pp_cutoff_cells", C.c_double), ("softening_m", C.c_double),
+        ("field_bound_V_m", C.c_double), ("reserved", C.c_int32 * 8),
+    ]
 
 
 class Tuning(C.Structure):
@@ -129,6 +139,8 @@ SIGNATURES = {
     "icb_moments": (C.c_int, [_H, _DP]),
     "icb_mark_reference": (C.c_int, [_H]),
     "icb_autotune": (C.c_int, [_H, C.c_uint64, _P(Tuning)]),
+    "icb_spacecharge_configure": (C.c_int, [_H, _P(SpaceChargeConfig)]),
+    "icb_spacecharge_field": (C.c_int, [_H, _DP, _DP, _DP]),
     "icb_generate_ions": (C.c_int, [C.c_uint32, C.c_int32, _P(SpeciesSpec), _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
     "icb_philox_eval": (C.c_int, [C.c_int, C.c_uint64, _U32P, C.c_uint64, C.c_int, _U32P]),
     "icb_moments_noalloc": (C.c_int, [C.c_int, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

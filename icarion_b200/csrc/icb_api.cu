@@ -49,6 +49,7 @@ int fail(int code, const char* fmt, ...) {
 constexpr double kGeomEps = 1e-12;          // CylindricalGeometry.h:245
 constexpr double kMinVoltage = 1e-12;       // AnalyticalFieldModel voltage threshold
 constexpr double kBoltzmann = 1.380649e-23; // utils/constants.h:15
+constexpr double kEps0 = 8.854187817e-12;   // utils/constants.h:19
 constexpr double kMeanChi3 = 1.5957691216057308;  // E|N(0,I3)| = 2 sqrt(2/pi)
 constexpr int kMomItemIons = 8192;
 
@@ -292,6 +293,11 @@ struct icb_handle {
     uint64_t graph_gen = 0;
     uint64_t graph_launches = 0;
     uint64_t gen = 1;                  // bumped whenever the graph goes stale
+    // space charge (solved before every step when configured)
+    SpaceChargeSolver* sc = nullptr;
+    double sc_emax_base = 0.0;         // ensemble 0's field bound without space charge
+    std::vector<cudaEvent_t> sc_ev;    // per-solve events (first 64 solves of a call)
+    size_t sc_timed = 0;
     void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
@@ -300,6 +306,8 @@ struct icb_handle {
 
     ~icb_handle() {
         drop_graph();
+        if (sc) sc_destroy(sc);
+        for (cudaEvent_t e : sc_ev) cudaEventDestroy(e);
         for (cudaEvent_t e : kev) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -383,9 +391,17 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
     if (coll != kCollNone) {
         if (!(P.gas_mass_kg > 0.0) || !(P.temperature_K > 0.0))
             return fail(ICB_ERR_INVALID_ARGUMENT, "collisions need gas_mass_kg > 0 and temperature_K > 0");
-        if (!(P.sigma_m2 > 0.0) || !(P.gas_density_m3 >= 0.0))
-            return fail(ICB_ERR_INVALID_ARGUMENT, "collisions need sigma_m2 > 0 and gas_density_m3 >= 0");
-        C.A = P.gas_density_m3 * P.sigma_m2 * P.dt_s;
+        if (!(P.gas_density_m3 >= 0.0)) return fail(ICB_ERR_INVALID_ARGUMENT, "collisions need gas_density_m3 >= 0");
+        if (coll == kCollLangevin) {
+            // nu = n pi |q| sqrt(alpha' / (4 pi eps0 mu)) (sigma_L v of DampingForce.cpp:170-176)
+            if (!(P.gas_polarizability_m3 > 0.0))
+                return fail(ICB_ERR_INVALID_ARGUMENT, "Langevin collisions need gas_polarizability_m3 > 0");
+            C.A = 0.0;
+            C.lang_c = P.gas_density_m3 * P.dt_s * M_PI * std::sqrt(P.gas_polarizability_m3 / (4.0 * M_PI * kEps0));
+        } else {
+            if (!(P.sigma_m2 > 0.0)) return fail(ICB_ERR_INVALID_ARGUMENT, "collisions need sigma_m2 > 0");
+            C.A = P.gas_density_m3 * P.sigma_m2 * P.dt_s;
+        }
         C.sig_n = std::sqrt(kBoltzmann * P.temperature_K / P.gas_mass_kg);
         C.mean_th = C.sig_n * kMeanChi3;
         C.m_gas = P.gas_mass_kg;
@@ -422,6 +438,9 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.mass = h->mass.p; p.charge = h->charge.p; p.flags = h->flags.p;
         p.t_death = h->t_death.p; p.t_arr = h->t_arr.p;
         p.birth = h->has_birth ? h->birth.p : nullptr;
+        p.escx = h->sc ? sc_field(h->sc, 0) : nullptr;
+        p.escy = h->sc ? sc_field(h->sc, 1) : nullptr;
+        p.escz = h->sc ? sc_field(h->sc, 2) : nullptr;
         p.zprev = h->zprev.p;
         p.counters = h->counters.p;
         p.step_dev = h->step_dev.p;
@@ -453,6 +472,15 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
     return ICB_OK;
 }
 
+// Space-charge field of the current positions (before a push).
+int solve_space_charge(icb_handle* h) {
+    std::string err;
+    const int r = sc_solve(h->sc, h->x.p, h->y.p, h->z.p, h->charge.p, h->flags.p, h->n, h->stream, err);
+    if (r != ICB_OK) return fail(r, "space charge: %s", err.c_str());
+    h->launches += static_cast<uint64_t>(sc_kernel_count(h->sc));
+    return ICB_OK;
+}
+
 // The launch sequence of icb_advance(n_steps): counter reset, then per chunk
 // of at most K steps the fused step kernel(s) and the device clock update.
 // The first n_timed chunks are bracketed by events for per-kernel timing.
@@ -463,8 +491,18 @@ int enqueue_advance(icb_handle* h, uint64_t n_steps, size_t n_timed) {
     const int ne = static_cast<int>(h->ens.size());
     uint64_t left = n_steps;
     size_t j = 0;
+    h->sc_timed = 0;
     while (left > 0) {
-        const uint32_t K = static_cast<uint32_t>(std::min<uint64_t>(left, h->K));
+        // with space charge every launch advances one step, after the solve
+        // of the field at the step's start positions
+        const uint32_t K = h->sc ? 1u : static_cast<uint32_t>(std::min<uint64_t>(left, h->K));
+        if (h->sc) {
+            const bool timed = n_timed > 0 && h->sc_timed < 64;
+            if (timed) ICB_CUDA(cudaEventRecord(h->sc_ev[2 * h->sc_timed], s));
+            if (int r = solve_space_charge(h)) return r;
+            if (timed) ICB_CUDA(cudaEventRecord(h->sc_ev[2 * h->sc_timed + 1], s));
+            if (timed) ++h->sc_timed;
+        }
         if (j < n_timed) ICB_CUDA(cudaEventRecord(h->kev[2 * j], s));
         if (int r = launch_step(h, K, 1, 1, 1)) return r;
         if (j < n_timed) ICB_CUDA(cudaEventRecord(h->kev[2 * j + 1], s));
@@ -490,6 +528,14 @@ int read_stats(icb_handle* h, icb_run_stats* st, uint64_t steps, size_t n_timed_
         kms += m;
     }
     st->step_kernel_ms = kms;
+    double scms = 0.0;
+    for (size_t j = 0; j < h->sc_timed; ++j) {
+        float m = 0.f;
+        ICB_CUDA(cudaEventElapsedTime(&m, h->sc_ev[2 * j], h->sc_ev[2 * j + 1]));
+        scms += m;
+    }
+    st->spacecharge_ms = scms;
+    st->spacecharge_solves_timed = h->sc_timed;
     st->kernel_launches = h->launches;
     st->steps = steps;
     st->candidates = c[kCntCandidates];
@@ -560,6 +606,11 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
     switch (cfg->collision_model) {
         case ICB_COLLISION_NONE: coll = kCollNone; break;
         case ICB_COLLISION_HSS: coll = kCollHSS; break;
+        case ICB_COLLISION_LANGEVIN:
+            if (cfg->integrator != ICB_INTEGRATOR_BORIS)
+                return fail(ICB_ERR_UNSUPPORTED, "Langevin capture collisions are built for the Boris pusher");
+            coll = kCollLangevin;
+            break;
         default: return fail(ICB_ERR_UNSUPPORTED, "collision model %d not available", cfg->collision_model);
     }
     int ndev = 0;
@@ -886,16 +937,75 @@ int icb_advance(icb_handle* h, uint64_t n_steps, icb_run_stats* stats) {
     ICB_CUDA(cudaEventRecord(h->ev0, s));
     // Per-launch events around the step kernels when statistics are asked
     // for (at most 64 launches are timed individually per call).
-    const size_t n_launch = static_cast<size_t>((n_steps + h->K - 1) / h->K);
+    const uint64_t k_eff = h->sc ? 1u : h->K;
+    const size_t n_launch = static_cast<size_t>((n_steps + k_eff - 1) / k_eff);
     const size_t n_timed = stats ? std::min<size_t>(n_launch, 64) : 0;
-    while (h->kev.size() < 2 * n_timed) {
+    while (h->kev.size() < 2 * n_timed || (h->sc && h->sc_ev.size() < 128)) {
         cudaEvent_t e;
         ICB_CUDA(cudaEventCreate(&e));
-        h->kev.push_back(e);
+        if (h->kev.size() < 2 * n_timed) h->kev.push_back(e);
+        else h->sc_ev.push_back(e);
     }
     if (int r = enqueue_advance(h, n_steps, n_timed)) return r;
     ICB_CUDA(cudaEventRecord(h->ev1, s));
     if (stats) return read_stats(h, stats, n_steps, n_timed);
+    return ICB_OK;
+}
+
+int icb_spacecharge_configure(icb_handle* h, const icb_spacecharge_config* cfg) {
+    if (int r = check_handle(h)) return r;
+    if (!cfg) return fail(ICB_ERR_INVALID_ARGUMENT, "null space-charge config");
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->sc) {
+        sc_destroy(h->sc);
+        h->sc = nullptr;
+        h->ens_const[0].Emax = h->sc_emax_base;
+    }
+    ++h->gen;
+    if (cfg->mode == ICB_SC_OFF) return ICB_OK;
+    if (h->n == 0) return fail(ICB_ERR_STATE, "upload the ions before configuring space charge");
+    if (h->ens.size() != 1) return fail(ICB_ERR_UNSUPPORTED, "space charge couples one ensemble's ions: use one ensemble");
+    if (h->cfg.integrator != ICB_INTEGRATOR_BORIS)
+        return fail(ICB_ERR_UNSUPPORTED, "space charge needs the Boris pusher (RK4 refreshes it per stage)");
+    if (h->hilo()) return fail(ICB_ERR_UNSUPPORTED, "space charge is built for the FP64 and mixed position forms");
+    std::string err;
+    SpaceChargeSolver* sc = nullptr;
+    int r = sc_create(*cfg, h->n, h->stream, &sc, err);
+    if (r != ICB_OK) return fail(r, "space charge: %s", err.c_str());
+    h->sc = sc;
+    h->sc_emax_base = h->ens_const[0].Emax;
+    double bound = cfg->field_bound_V_m;
+    if (!(bound > 0.0)) {
+        // 4 x the largest field of the configured state
+        r = sc_solve(h->sc, h->x.p, h->y.p, h->z.p, h->charge.p, h->flags.p, h->n, h->stream, err);
+        if (r != ICB_OK) return fail(r, "space charge: %s", err.c_str());
+        std::vector<double> e[3];
+        for (int a = 0; a < 3; ++a) {
+            e[a].resize(h->n);
+            ICB_CUDA(cudaMemcpyAsync(e[a].data(), sc_field(h->sc, a), h->n * sizeof(double), cudaMemcpyDeviceToHost,
+                                     h->stream));
+        }
+        ICB_CUDA(cudaStreamSynchronize(h->stream));
+        double mx = 0.0;
+        for (uint64_t i = 0; i < h->n; ++i)
+            mx = std::max(mx, std::sqrt(e[0][i] * e[0][i] + e[1][i] * e[1][i] + e[2][i] * e[2][i]));
+        bound = 4.0 * mx;
+    }
+    h->ens_const[0].Emax = h->sc_emax_base + bound;
+    return ICB_OK;
+}
+
+int icb_spacecharge_field(icb_handle* h, double* ex, double* ey, double* ez) {
+    if (int r = check_handle(h)) return r;
+    if (!h->sc) return fail(ICB_ERR_STATE, "space charge is not configured");
+    h->launches = 0;
+    if (int r = solve_space_charge(h)) return r;
+    double* out[3] = {ex, ey, ez};
+    for (int a = 0; a < 3; ++a)
+        if (out[a])
+            ICB_CUDA(cudaMemcpyAsync(out[a], sc_field(h->sc, a), h->n * sizeof(double), cudaMemcpyDeviceToHost,
+                                     h->stream));
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
     return ICB_OK;
 }
 
@@ -993,6 +1103,10 @@ static int single_part(icb_handle* h, int push, int collide, int finalize, icb_r
     ICB_CUDA(cudaMemsetAsync(h->counters.p, 0, kNumCounters * sizeof(unsigned long long), s));
     ICB_CUDA(cudaEventRecord(h->ev0, s));
     h->launches = 0;
+    h->sc_timed = 0;
+    if (push && h->sc) {
+        if (int r = solve_space_charge(h)) return r;
+    }
     if (int r = launch_step(h, 1, push, collide, finalize)) return r;
     if (finalize) {
         const int ne = static_cast<int>(h->ens.size());

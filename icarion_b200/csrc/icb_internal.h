@@ -2,6 +2,9 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <string>
+
+#include "../../include/icarion_b200.h"
 #include "icb_params.h"
 
 namespace icb {
@@ -14,6 +17,17 @@ cudaError_t launch_step_mixed(int integ, int coll, int field, bool mag, const St
                               dim3 grid, dim3 block, cudaStream_t s);
 cudaError_t launch_step_hilo(int integ, int coll, int field, bool mag, const StepParams& p,
                              dim3 grid, dim3 block, cudaStream_t s);
+
+// Space-charge solver (icb_p3m.cu).  Functions return ICB_* status codes
+// and put a message into `err` on failure.
+struct SpaceChargeSolver;
+int sc_create(const icb_spacecharge_config& cfg, uint64_t n_ions, cudaStream_t s, SpaceChargeSolver** out,
+              std::string& err);
+void sc_destroy(SpaceChargeSolver* sc);
+int sc_solve(SpaceChargeSolver* sc, const double* x, const double* y, const double* z, const double* q,
+             const uint8_t* flags, uint64_t n, cudaStream_t s, std::string& err);
+const double* sc_field(const SpaceChargeSolver* sc, int axis);
+int sc_kernel_count(const SpaceChargeSolver* sc);
 
 // Records the message icb_last_error() returns on this host thread and
 // passes `code` through.

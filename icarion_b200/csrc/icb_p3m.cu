@@ -1,0 +1,559 @@
+// icb_p3m.cu — space-charge field of the ion cloud (ISpaceChargeModel,
+// ISpaceChargeModel.h:22-46), solved once per step before the push.
+//
+// Two solvers share one pipeline:
+//   bin     ions -> mesh base cell key (CIC cell of the lower corner)
+//   sort    (key, ion) pairs, stable radix sort (CUB)
+//   bounds  first sorted slot of every cell key (binary search)
+//   deposit every mesh node gathers the CIC charge of the ions in the eight
+//           cells around it, in a fixed order (deterministic, no atomics)
+//   solve   isolated P3M: zero-padded (2n)^3 FFT convolution with the
+//           transformed long-range field kernel (three inverse FFTs, one per
+//           field component); periodic PM (the reference's solver as it is,
+//           GPUSpaceChargeP3M.cu:36-339): periodic Poisson solve, 1/N scale,
+//           central differences
+//   gather  per ion (in cell order): CIC interpolation of the mesh field,
+//           plus, for P3M, the particle-particle correction over the ions in
+//           the cells within the cutoff
+// All arithmetic is FP64; the periodic solver keeps the reference's float
+// CIC weights and float field output.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <memory>
+#include <string>
+
+#include "../../include/icarion_b200.h"
+#include "icb_internal.h"
+
+namespace icb {
+
+namespace {
+
+constexpr double kCoulomb = 8.987551787e9;     // utils/constants.h:20
+constexpr double kEps0 = 8.854187817e-12;      // utils/constants.h:19
+constexpr double kPi = 3.14159265358979323846;
+
+struct MeshGeom {
+    int n0, n1, n2;          // mesh nodes
+    int m0, m1, m2;          // FFT grid
+    double lo0, lo1, lo2;
+    double ih0, ih1, ih2;    // grid coordinate scale (1/h, or n/extent for the periodic solver)
+    uint32_t ncell;          // n0*n1*n2 (also the key of excluded ions)
+};
+
+__device__ __forceinline__ bool grid_coords(const MeshGeom& g, double x, double y, double z, double f[3]) {
+    f[0] = (x - g.lo0) * g.ih0;
+    f[1] = (y - g.lo1) * g.ih1;
+    f[2] = (z - g.lo2) * g.ih2;
+    // false for NaN as well
+    return f[0] >= 0.0 && f[0] < g.n0 - 1 && f[1] >= 0.0 && f[1] < g.n1 - 1 && f[2] >= 0.0 && f[2] < g.n2 - 1;
+}
+
+__global__ void k_sc_bin(MeshGeom g, const double* __restrict__ x, const double* __restrict__ y,
+                         const double* __restrict__ z, const uint8_t* __restrict__ flags, uint32_t n, int all_ions,
+                         uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t key = g.ncell;
+    const bool use = all_ions || ((flags[i] & 3u) == 3u);   // active and born
+    double f[3];
+    if (use && grid_coords(g, x[i], y[i], z[i], f)) {
+        const int c0 = static_cast<int>(f[0]), c1 = static_cast<int>(f[1]), c2 = static_cast<int>(f[2]);
+        key = (static_cast<uint32_t>(c0) * g.n1 + static_cast<uint32_t>(c1)) * g.n2 + static_cast<uint32_t>(c2);
+    }
+    keys[i] = key;
+    vals[i] = i;
+}
+
+// start[c] = first sorted slot whose key is >= c, for c in [0, ncell].
+__global__ void k_sc_cell_start(const uint32_t* __restrict__ keys, uint32_t n, uint32_t ncell,
+                                uint32_t* __restrict__ start) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > ncell) return;
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if (keys[mid] < c) lo = mid + 1; else hi = mid;
+    }
+    start[c] = lo;
+}
+
+// CIC weight of corner (ox, oy, oz) of a cell for fractions fr (taken left
+// to right: x, y, z).
+template <class W>
+__device__ __forceinline__ W cic_w(int ox, int oy, int oz, W fx, W fy, W fz) {
+    const W one = W(1);
+    return (ox ? fx : one - fx) * (oy ? fy : one - fy) * (oz ? fz : one - fz);
+}
+
+// Charge per mesh node (C); nodes of the FFT grid outside the mesh are 0.
+template <bool REF_WEIGHTS>
+__global__ void k_sc_deposit(MeshGeom g, const double* __restrict__ x, const double* __restrict__ y,
+                             const double* __restrict__ z, const double* __restrict__ q,
+                             const uint32_t* __restrict__ vals, const uint32_t* __restrict__ start,
+                             double* __restrict__ rho) {
+    const size_t total = static_cast<size_t>(g.m0) * g.m1 * g.m2;
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int c = static_cast<int>(idx % g.m2);
+    const size_t t = idx / g.m2;
+    const int b = static_cast<int>(t % g.m1);
+    const int a = static_cast<int>(t / g.m1);
+    double acc = 0.0;
+    if (a < g.n0 && b < g.n1 && c < g.n2) {
+        for (int ci = a - 1; ci <= a; ++ci) {
+            if (ci < 0 || ci > g.n0 - 2) continue;
+            for (int cj = b - 1; cj <= b; ++cj) {
+                if (cj < 0 || cj > g.n1 - 2) continue;
+                for (int ck = c - 1; ck <= c; ++ck) {
+                    if (ck < 0 || ck > g.n2 - 2) continue;
+                    const uint32_t key = (static_cast<uint32_t>(ci) * g.n1 + static_cast<uint32_t>(cj)) * g.n2 +
+                                         static_cast<uint32_t>(ck);
+                    const uint32_t s1 = start[key + 1];
+                    for (uint32_t s = start[key]; s < s1; ++s) {
+                        const uint32_t j = vals[s];
+                        const double fx = (x[j] - g.lo0) * g.ih0 - ci;
+                        const double fy = (y[j] - g.lo1) * g.ih1 - cj;
+                        const double fz = (z[j] - g.lo2) * g.ih2 - ck;
+                        double w;
+                        if (REF_WEIGHTS) {
+                            w = static_cast<double>(cic_w<float>(a - ci, b - cj, c - ck, static_cast<float>(fx),
+                                                                 static_cast<float>(fy), static_cast<float>(fz)));
+                        } else {
+                            w = cic_w<double>(a - ci, b - cj, c - ck, fx, fy, fz);
+                        }
+                        acc += w * q[j];
+                    }
+                }
+            }
+        }
+    }
+    rho[idx] = acc;
+}
+
+// out = a * b (complex), n entries
+__global__ void k_sc_cmul(const cufftDoubleComplex* __restrict__ a, const cufftDoubleComplex* __restrict__ b,
+                          cufftDoubleComplex* __restrict__ out, size_t n) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const cufftDoubleComplex u = a[i], v = b[i];
+    out[i] = make_cuDoubleComplex(u.x * v.x - u.y * v.y, u.x * v.y + u.y * v.x);
+}
+
+__device__ __forceinline__ double e_long(double r, double alpha) {
+    // long-range part of a unit charge's field / Coulomb constant:
+    // erf(a r)/r^2 - (2a/sqrt(pi)) exp(-a^2 r^2)/r
+    const double ar = alpha * r;
+    return erf(ar) / (r * r) - (2.0 * alpha / sqrt(kPi)) * exp(-ar * ar) / r;
+}
+
+// Component `comp` of the sampled long-range field of a unit charge on the
+// zero-padded grid: displacement index s wrapped to (-n, n); s == n is never
+// reached by mesh data and is 0, as is the origin.
+__global__ void k_sc_green(MeshGeom g, double h0, double h1, double h2, double alpha, int comp,
+                           double* __restrict__ out) {
+    const size_t total = static_cast<size_t>(g.m0) * g.m1 * g.m2;
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int c = static_cast<int>(idx % g.m2);
+    const size_t t = idx / g.m2;
+    const int b = static_cast<int>(t % g.m1);
+    const int a = static_cast<int>(t / g.m1);
+    double v = 0.0;
+    if (a != g.n0 && b != g.n1 && c != g.n2) {
+        const double dx = (a < g.n0 ? a : a - g.m0) * h0;
+        const double dy = (b < g.n1 ? b : b - g.m1) * h1;
+        const double dz = (c < g.n2 ? c : c - g.m2) * h2;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 > 0.0) {
+            const double r = sqrt(r2);
+            const double f = kCoulomb * e_long(r, alpha) / r;
+            v = f * (comp == 0 ? dx : (comp == 1 ? dy : dz));
+        }
+    }
+    out[idx] = v;
+}
+
+// Scale a transformed kernel by 1 / (grid size): cuFFT's inverse is
+// unnormalised.
+__global__ void k_sc_normalize(MeshGeom g, cufftDoubleComplex* __restrict__ gh) {
+    const size_t total = static_cast<size_t>(g.m0) * g.m1 * (g.m2 / 2 + 1);
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const double scale = 1.0 / (static_cast<double>(g.m0) * g.m1 * g.m2);
+    gh[idx].x *= scale;
+    gh[idx].y *= scale;
+}
+
+// The reference's Fourier-space Poisson step (GPUSpaceChargeP3M.cu:114-161):
+// phi_hat = rho_hat / (eps0 k^2 V), k = 0 -> 0, its z length (nz/2+1) 2 dz.
+__global__ void k_sc_poisson_ref(MeshGeom g, double dx, double dy, double dz, cufftDoubleComplex* __restrict__ rh) {
+    const int nx = g.n0, ny = g.n1, nz_half = g.n2 / 2 + 1;
+    const int total = nx * ny * nz_half;
+    const int mode_idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mode_idx >= total) return;
+    const int i = mode_idx / (ny * nz_half);
+    const int j = (mode_idx % (ny * nz_half)) / nz_half;
+    const int k = mode_idx % nz_half;
+    const double Lx = nx * dx, Ly = ny * dy, Lz = nz_half * 2 * dz;
+    const double kx = (i < nx / 2) ? (2.0 * kPi * i / Lx) : (2.0 * kPi * (i - nx) / Lx);
+    const double ky = (j < ny / 2) ? (2.0 * kPi * j / Ly) : (2.0 * kPi * (j - ny) / Ly);
+    const double kz = 2.0 * kPi * k / Lz;
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    if (k2 < 1e-10) {
+        rh[mode_idx].x = 0.0;
+        rh[mode_idx].y = 0.0;
+        return;
+    }
+    const double scale = 1.0 / (kEps0 * k2 * (dx * dy * dz));
+    rh[mode_idx].x = rh[mode_idx].x * scale;
+    rh[mode_idx].y = rh[mode_idx].y * scale;
+}
+
+// E = -grad(phi * s) by central differences, one-sided at the edges
+// (GPUSpaceChargeP3M.cu:176-248).
+__global__ void k_sc_efield_ref(MeshGeom g, double dx, double dy, double dz, double s, const double* __restrict__ phi,
+                                double* __restrict__ ex, double* __restrict__ ey, double* __restrict__ ez) {
+    const int nx = g.n0, ny = g.n1, nz = g.n2;
+    const int total = nx * ny * nz;
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= total) return;
+    const int i = cell / (ny * nz);
+    const int j = (cell % (ny * nz)) / nz;
+    const int k = cell % nz;
+    const int sy = nz, sx = ny * nz;
+    auto P = [&](int a, int b, int c) { return phi[a * sx + b * sy + c] * s; };
+    if (i == 0) ex[cell] = -(P(i + 1, j, k) - P(i, j, k)) / dx;
+    else if (i == nx - 1) ex[cell] = -(P(i, j, k) - P(i - 1, j, k)) / dx;
+    else ex[cell] = -(P(i + 1, j, k) - P(i - 1, j, k)) / (2.0 * dx);
+    if (j == 0) ey[cell] = -(P(i, j + 1, k) - P(i, j, k)) / dy;
+    else if (j == ny - 1) ey[cell] = -(P(i, j, k) - P(i, j - 1, k)) / dy;
+    else ey[cell] = -(P(i, j + 1, k) - P(i, j - 1, k)) / (2.0 * dy);
+    if (k == 0) ez[cell] = -(P(i, j, k + 1) - P(i, j, k)) / dz;
+    else if (k == nz - 1) ez[cell] = -(P(i, j, k) - P(i, j, k - 1)) / dz;
+    else ez[cell] = -(P(i, j, k + 1) - P(i, j, k - 1)) / (2.0 * dz);
+}
+
+struct PPParams {
+    int on;
+    int r0, r1, r2;          // neighbour cell reach per axis
+    double rc2, alpha, eps2, min_d2;
+};
+
+// Field of every ion: CIC interpolation of the mesh field (+ particle-
+// particle correction).  Thread s handles the ion in sorted slot s.
+template <bool REF_WEIGHTS>
+__global__ void k_sc_gather(MeshGeom g, PPParams pp, const double* __restrict__ x, const double* __restrict__ y,
+                            const double* __restrict__ z, const double* __restrict__ q,
+                            const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                            const uint32_t* __restrict__ start, uint32_t n, const double* __restrict__ gx,
+                            const double* __restrict__ gy, const double* __restrict__ gz, double* __restrict__ ex,
+                            double* __restrict__ ey, double* __restrict__ ez) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint32_t i = vals[s];
+    const uint32_t key = keys[s];
+    if (key >= g.ncell) {
+        ex[i] = 0.0; ey[i] = 0.0; ez[i] = 0.0;
+        return;
+    }
+    const int ck = static_cast<int>(key % g.n2);
+    const uint32_t t = key / g.n2;
+    const int cj = static_cast<int>(t % g.n1);
+    const int ci = static_cast<int>(t / g.n1);
+    const double xi = x[i], yi = y[i], zi = z[i];
+    const double fx = (xi - g.lo0) * g.ih0 - ci;
+    const double fy = (yi - g.lo1) * g.ih1 - cj;
+    const double fz = (zi - g.lo2) * g.ih2 - ck;
+    double E[3] = {0.0, 0.0, 0.0};
+    const double* grid[3] = {gx, gy, gz};
+    // corners in the reference's order w000, w100, w010, w110, w001, ... (x fastest)
+    for (int oz = 0; oz < 2; ++oz) {
+        for (int oy = 0; oy < 2; ++oy) {
+            for (int ox = 0; ox < 2; ++ox) {
+                double w;
+                if (REF_WEIGHTS) {
+                    w = static_cast<double>(cic_w<float>(ox, oy, oz, static_cast<float>(fx), static_cast<float>(fy),
+                                                         static_cast<float>(fz)));
+                } else {
+                    w = cic_w<double>(ox, oy, oz, fx, fy, fz);
+                }
+                const size_t node = (static_cast<size_t>(ci + ox) * g.m1 + static_cast<size_t>(cj + oy)) * g.m2 +
+                                    static_cast<size_t>(ck + oz);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) E[c] += w * grid[c][node];
+            }
+        }
+    }
+    if (REF_WEIGHTS) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) E[c] = static_cast<double>(static_cast<float>(E[c]));
+    }
+    if (pp.on) {
+        const double c2a = 2.0 * pp.alpha / sqrt(kPi);
+        const int x0 = max(ci - pp.r0, 0), x1 = min(ci + pp.r0, g.n0 - 2);
+        const int y0 = max(cj - pp.r1, 0), y1 = min(cj + pp.r1, g.n1 - 2);
+        const int z0 = max(ck - pp.r2, 0), z1 = min(ck + pp.r2, g.n2 - 2);
+        for (int cx = x0; cx <= x1; ++cx) {
+            for (int cy = y0; cy <= y1; ++cy) {
+                const uint32_t row = (static_cast<uint32_t>(cx) * g.n1 + static_cast<uint32_t>(cy)) * g.n2;
+                const uint32_t sa = start[row + static_cast<uint32_t>(z0)];
+                const uint32_t sb = start[row + static_cast<uint32_t>(z1) + 1u];
+                for (uint32_t s2 = sa; s2 < sb; ++s2) {
+                    const uint32_t j = vals[s2];
+                    if (j == i) continue;
+                    const double dx = xi - x[j], dy = yi - y[j], dz = zi - z[j];
+                    const double r2 = dx * dx + dy * dy + dz * dz;
+                    if (r2 < pp.min_d2 || r2 >= pp.rc2) continue;
+                    const double r = sqrt(r2);
+                    const double ar = pp.alpha * r;
+                    const double el = erf(ar) / r2 - c2a * exp(-ar * ar) / r;
+                    const double sc = kCoulomb * (1.0 / (r2 + pp.eps2) - el) / r * q[j];
+                    E[0] += dx * sc;
+                    E[1] += dy * sc;
+                    E[2] += dz * sc;
+                }
+            }
+        }
+    }
+    ex[i] = E[0]; ey[i] = E[1]; ez[i] = E[2];
+}
+
+template <class T>
+cudaError_t dev_alloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) return cudaSuccess;
+    return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+}
+
+inline unsigned blocks_for(size_t n, int threads) { return static_cast<unsigned>((n + threads - 1) / threads); }
+
+}  // namespace
+
+struct SpaceChargeSolver {
+    int mode = ICB_SC_OFF;
+    MeshGeom g{};
+    double h[3] = {0, 0, 0};
+    PPParams pp{};
+    uint32_t cap = 0;
+    int key_bits = 1;
+    uint32_t* keys = nullptr;
+    uint32_t* keys_sorted = nullptr;
+    uint32_t* vals = nullptr;
+    uint32_t* vals_sorted = nullptr;
+    uint32_t* start = nullptr;
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    double* rho = nullptr;
+    cufftDoubleComplex* rho_hat = nullptr;
+    cufftDoubleComplex* tmp_hat = nullptr;
+    double* egrid[3] = {nullptr, nullptr, nullptr};
+    cufftDoubleComplex* ghat[3] = {nullptr, nullptr, nullptr};
+    double* esc[3] = {nullptr, nullptr, nullptr};
+    cufftHandle fwd = 0, inv = 0;
+    bool have_fwd = false, have_inv = false;
+    double max_field = 0.0;
+
+    ~SpaceChargeSolver() {
+        if (have_fwd) cufftDestroy(fwd);
+        if (have_inv) cufftDestroy(inv);
+        for (void* p : {static_cast<void*>(keys), static_cast<void*>(keys_sorted), static_cast<void*>(vals),
+                        static_cast<void*>(vals_sorted), static_cast<void*>(start), cub_tmp,
+                        static_cast<void*>(rho), static_cast<void*>(rho_hat), static_cast<void*>(tmp_hat)})
+            if (p) cudaFree(p);
+        for (int c = 0; c < 3; ++c) {
+            if (egrid[c]) cudaFree(egrid[c]);
+            if (ghat[c]) cudaFree(ghat[c]);
+            if (esc[c]) cudaFree(esc[c]);
+        }
+    }
+    size_t real_size() const { return static_cast<size_t>(g.m0) * g.m1 * g.m2; }
+    size_t cplx_size() const { return static_cast<size_t>(g.m0) * g.m1 * (g.m2 / 2 + 1); }
+};
+
+#define SC_CUDA(expr)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (expr);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            err = std::string(#expr) + ": " + cudaGetErrorString(e_);                          \
+            return e_ == cudaErrorMemoryAllocation ? ICB_ERR_OUT_OF_MEMORY : ICB_ERR_CUDA;     \
+        }                                                                                      \
+    } while (0)
+#define SC_FFT(expr)                                                                           \
+    do {                                                                                       \
+        cufftResult r_ = (expr);                                                               \
+        if (r_ != CUFFT_SUCCESS) {                                                             \
+            err = std::string(#expr) + ": cuFFT error " + std::to_string(static_cast<int>(r_)); \
+            return r_ == CUFFT_ALLOC_FAILED ? ICB_ERR_OUT_OF_MEMORY : ICB_ERR_CUDA;            \
+        }                                                                                      \
+    } while (0)
+
+int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, cudaStream_t s, SpaceChargeSolver** out,
+              std::string& err) {
+    *out = nullptr;
+    if (c.mode != ICB_SC_P3M_ISOLATED && c.mode != ICB_SC_PM_PERIODIC_REF) {
+        err = "unknown space-charge mode";
+        return ICB_ERR_INVALID_ARGUMENT;
+    }
+    const bool iso = c.mode == ICB_SC_P3M_ISOLATED;
+    const int nmax = iso ? 256 : 512;
+    for (int a = 0; a < 3; ++a) {
+        if (c.grid_n[a] < 8 || c.grid_n[a] > nmax) {
+            err = "grid_n must be in [8, " + std::to_string(nmax) + "] per axis";
+            return ICB_ERR_INVALID_ARGUMENT;
+        }
+        if (!(c.box_max_m[a] > c.box_min_m[a])) {
+            err = "box_max_m must exceed box_min_m on every axis";
+            return ICB_ERR_INVALID_ARGUMENT;
+        }
+    }
+    if (n_ions == 0 || n_ions >= (1ull << 31)) {
+        err = "space charge needs 1 .. 2^31-1 ions";
+        return ICB_ERR_INVALID_ARGUMENT;
+    }
+    auto sv = std::make_unique<SpaceChargeSolver>();
+    SpaceChargeSolver& S = *sv;
+    S.mode = c.mode;
+    MeshGeom& g = S.g;
+    g.n0 = c.grid_n[0]; g.n1 = c.grid_n[1]; g.n2 = c.grid_n[2];
+    g.m0 = iso ? 2 * g.n0 : g.n0; g.m1 = iso ? 2 * g.n1 : g.n1; g.m2 = iso ? 2 * g.n2 : g.n2;
+    g.lo0 = c.box_min_m[0]; g.lo1 = c.box_min_m[1]; g.lo2 = c.box_min_m[2];
+    double hmax = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        const double ext = c.box_max_m[a] - c.box_min_m[a];
+        S.h[a] = ext / c.grid_n[a];
+        hmax = std::max(hmax, S.h[a]);
+    }
+    if (iso) {
+        g.ih0 = 1.0 / S.h[0]; g.ih1 = 1.0 / S.h[1]; g.ih2 = 1.0 / S.h[2];
+    } else {
+        // GPUSpaceChargeP3M.cu: inv_spacing = grid_n / domain_size
+        g.ih0 = c.grid_n[0] / (c.box_max_m[0] - c.box_min_m[0]);
+        g.ih1 = c.grid_n[1] / (c.box_max_m[1] - c.box_min_m[1]);
+        g.ih2 = c.grid_n[2] / (c.box_max_m[2] - c.box_min_m[2]);
+    }
+    g.ncell = static_cast<uint32_t>(g.n0) * g.n1 * g.n2;
+    S.key_bits = 1;
+    while ((1ull << S.key_bits) <= g.ncell) ++S.key_bits;
+    S.pp.on = iso ? 1 : 0;
+    if (iso) {
+        const double ah = c.alpha_h > 0.0 ? c.alpha_h : 1.0;
+        const double rcc = c.pp_cutoff_cells > 0.0 ? c.pp_cutoff_cells : 2.0;
+        const double soft = c.softening_m < 0.0 ? 1e-10 : c.softening_m;
+        S.pp.alpha = ah / hmax;
+        const double rc = rcc * hmax;
+        S.pp.rc2 = rc * rc;
+        S.pp.r0 = static_cast<int>(std::ceil(rc / S.h[0]));
+        S.pp.r1 = static_cast<int>(std::ceil(rc / S.h[1]));
+        S.pp.r2 = static_cast<int>(std::ceil(rc / S.h[2]));
+        S.pp.eps2 = soft * soft;
+        S.pp.min_d2 = std::max(soft * soft * 1e-4, 1e-30);
+    }
+    S.cap = static_cast<uint32_t>(n_ions);
+    SC_CUDA(dev_alloc(&S.keys, S.cap));
+    SC_CUDA(dev_alloc(&S.keys_sorted, S.cap));
+    SC_CUDA(dev_alloc(&S.vals, S.cap));
+    SC_CUDA(dev_alloc(&S.vals_sorted, S.cap));
+    SC_CUDA(dev_alloc(&S.start, static_cast<size_t>(g.ncell) + 1));
+    SC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, S.cub_bytes, S.keys, S.keys_sorted, S.vals, S.vals_sorted,
+                                            static_cast<int>(S.cap), 0, S.key_bits, s));
+    SC_CUDA(cudaMalloc(&S.cub_tmp, std::max<size_t>(S.cub_bytes, 16)));
+    SC_CUDA(dev_alloc(&S.rho, S.real_size()));
+    SC_CUDA(dev_alloc(&S.rho_hat, S.cplx_size()));
+    for (int a = 0; a < 3; ++a) {
+        SC_CUDA(dev_alloc(&S.egrid[a], S.real_size()));
+        SC_CUDA(dev_alloc(&S.esc[a], S.cap));
+    }
+    SC_FFT(cufftPlan3d(&S.fwd, g.m0, g.m1, g.m2, CUFFT_D2Z));
+    S.have_fwd = true;
+    SC_FFT(cufftPlan3d(&S.inv, g.m0, g.m1, g.m2, CUFFT_Z2D));
+    S.have_inv = true;
+    SC_FFT(cufftSetStream(S.fwd, s));
+    SC_FFT(cufftSetStream(S.inv, s));
+    if (iso) {
+        SC_CUDA(dev_alloc(&S.tmp_hat, S.cplx_size()));
+        for (int a = 0; a < 3; ++a) {
+            SC_CUDA(dev_alloc(&S.ghat[a], S.cplx_size()));
+            k_sc_green<<<blocks_for(S.real_size(), 256), 256, 0, s>>>(g, S.h[0], S.h[1], S.h[2], S.pp.alpha, a, S.rho);
+            SC_CUDA(cudaGetLastError());
+            SC_FFT(cufftExecD2Z(S.fwd, S.rho, S.ghat[a]));
+            k_sc_normalize<<<blocks_for(S.cplx_size(), 256), 256, 0, s>>>(g, S.ghat[a]);
+            SC_CUDA(cudaGetLastError());
+        }
+    }
+    SC_CUDA(cudaStreamSynchronize(s));
+    *out = sv.release();
+    return ICB_OK;
+}
+
+void sc_destroy(SpaceChargeSolver* S) { delete S; }
+
+int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const double* z, const double* q,
+             const uint8_t* flags, uint64_t n, cudaStream_t s, std::string& err) {
+    if (n > S->cap) {
+        err = "more ions than the space-charge solver was configured for";
+        return ICB_ERR_STATE;
+    }
+    const MeshGeom& g = S->g;
+    const bool iso = S->mode == ICB_SC_P3M_ISOLATED;
+    const uint32_t nn = static_cast<uint32_t>(n);
+    SC_FFT(cufftSetStream(S->fwd, s));
+    SC_FFT(cufftSetStream(S->inv, s));
+    k_sc_bin<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, flags, nn, iso ? 0 : 1, S->keys, S->vals);
+    SC_CUDA(cudaGetLastError());
+    size_t bytes = S->cub_bytes;
+    SC_CUDA(cub::DeviceRadixSort::SortPairs(S->cub_tmp, bytes, S->keys, S->keys_sorted, S->vals, S->vals_sorted,
+                                            static_cast<int>(nn), 0, S->key_bits, s));
+    k_sc_cell_start<<<blocks_for(static_cast<size_t>(g.ncell) + 1, 256), 256, 0, s>>>(S->keys_sorted, nn, g.ncell,
+                                                                                      S->start);
+    SC_CUDA(cudaGetLastError());
+    if (iso) {
+        k_sc_deposit<false><<<blocks_for(S->real_size(), 256), 256, 0, s>>>(g, x, y, z, q, S->vals_sorted, S->start,
+                                                                             S->rho);
+        SC_CUDA(cudaGetLastError());
+        SC_FFT(cufftExecD2Z(S->fwd, S->rho, S->rho_hat));
+        for (int a = 0; a < 3; ++a) {
+            k_sc_cmul<<<blocks_for(S->cplx_size(), 256), 256, 0, s>>>(S->rho_hat, S->ghat[a], S->tmp_hat,
+                                                                       S->cplx_size());
+            SC_CUDA(cudaGetLastError());
+            SC_FFT(cufftExecZ2D(S->inv, S->tmp_hat, S->egrid[a]));
+        }
+        k_sc_gather<false><<<blocks_for(nn, 128), 128, 0, s>>>(g, S->pp, x, y, z, q, S->keys_sorted, S->vals_sorted,
+                                                                S->start, nn, S->egrid[0], S->egrid[1], S->egrid[2],
+                                                                S->esc[0], S->esc[1], S->esc[2]);
+        SC_CUDA(cudaGetLastError());
+    } else {
+        k_sc_deposit<true><<<blocks_for(S->real_size(), 256), 256, 0, s>>>(g, x, y, z, q, S->vals_sorted, S->start,
+                                                                            S->rho);
+        SC_CUDA(cudaGetLastError());
+        SC_FFT(cufftExecD2Z(S->fwd, S->rho, S->rho_hat));
+        k_sc_poisson_ref<<<blocks_for(S->cplx_size(), 256), 256, 0, s>>>(g, S->h[0], S->h[1], S->h[2], S->rho_hat);
+        SC_CUDA(cudaGetLastError());
+        // the potential lands in rho (no longer needed after the forward FFT)
+        SC_FFT(cufftExecZ2D(S->inv, S->rho_hat, S->rho));
+        const double scale = 1.0 / static_cast<double>(S->real_size());
+        k_sc_efield_ref<<<blocks_for(S->real_size(), 256), 256, 0, s>>>(g, S->h[0], S->h[1], S->h[2], scale, S->rho,
+                                                                         S->egrid[0], S->egrid[1], S->egrid[2]);
+        SC_CUDA(cudaGetLastError());
+        k_sc_gather<true><<<blocks_for(nn, 128), 128, 0, s>>>(g, S->pp, x, y, z, q, S->keys_sorted, S->vals_sorted,
+                                                               S->start, nn, S->egrid[0], S->egrid[1], S->egrid[2],
+                                                               S->esc[0], S->esc[1], S->esc[2]);
+        SC_CUDA(cudaGetLastError());
+    }
+    return ICB_OK;
+}
+
+const double* sc_field(const SpaceChargeSolver* S, int axis) { return S->esc[axis]; }
+
+int sc_kernel_count(const SpaceChargeSolver* S) {
+    // kernels of one solve that this library launches (cuFFT and CUB not counted)
+    return S->mode == ICB_SC_P3M_ISOLATED ? 3 + 1 + 3 + 1 : 3 + 1 + 1 + 1 + 1;
+}
+
+}  // namespace icb

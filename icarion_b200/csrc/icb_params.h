@@ -16,7 +16,7 @@ constexpr int kMaxLaunchEns = 64;   // ensembles per launch chunk (param space b
 constexpr uint32_t kMaxStepsPerLaunch = 16384;
 
 enum FieldKind : int { kFieldUniform = 0, kFieldLinear = 1, kFieldLinearRF = 2 };
-enum CollKind : int { kCollNone = 0, kCollHSS = 1 };
+enum CollKind : int { kCollNone = 0, kCollHSS = 1, kCollLangevin = 2 };
 enum PrecKind : int { kPrecFP64 = 0, kPrecMixed = 1, kPrecHiLo = 2 };
 enum IntegKind : int { kBoris = 0, kRK4 = 1 };
 
@@ -49,6 +49,9 @@ struct EnsConst {
     // Upper bound of |E| inside the domain: the skip clock bounds the ion
     // speed change per step by |q/m| Emax dt.
     double Emax;
+    // Langevin capture: per-step event probability parameter
+    // lambda_i = lang_c |q_i| / sqrt(mu_i)
+    double lang_c;
     int32_t magnetic;
     int32_t rf;
     // float copies for the float collision path
@@ -78,6 +81,9 @@ struct StepParams {
     double* t_death;
     double* t_arr;
     const double* birth;               // nullable
+    // space-charge field of this step per ion (nullable; launches with
+    // space charge advance one step, the field is solved before each)
+    const double* escx; const double* escy; const double* escz;
     double* zprev;                     // z before the push, kept between unfused calls
     unsigned long long* counters;      // kNumCounters
     const unsigned long long* step_dev;// engine step index at launch start

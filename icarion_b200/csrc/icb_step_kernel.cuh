@@ -197,6 +197,8 @@ struct Consts {
     double dt, hd, dt6;      // dt, dt/2, dt/6
     R dt_r, h, dt6_r;        // the same in working precision
     R A, Amean, ug[3];       // collision clock: Q = A |v - u| + A <|th|>
+    R escq[3];               // space-charge force E_sc q of this step
+    bool sc;                 // space charge on (one step per launch)
 };
 
 template <class R, int FIELD, bool MAG>
@@ -281,12 +283,23 @@ __device__ __forceinline__ R boris(const Consts<R>& k, Pos& x, R v[3], double t)
     } else {
         R E[3];
         efield<R, FIELD>(k, x, t, E);
+        // total force q E + q E_sc, then / m (ForceRegistry.cpp:76-87)
         if constexpr (sizeof(R) == 8) {
+            if (k.sc) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) a[c] = (E[c] * k.q) / static_cast<R>(k.m);
+                for (int c = 0; c < 3; ++c) a[c] = (E[c] * k.q + k.escq[c]) / static_cast<R>(k.m);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) a[c] = (E[c] * k.q) / static_cast<R>(k.m);
+            }
         } else {
+            if (k.sc) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) a[c] = E[c] * k.qm;
+                for (int c = 0; c < 3; ++c) a[c] = (E[c] * k.q + k.escq[c]) * k.inv_m;
+            } else {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) a[c] = E[c] * k.qm;
+            }
         }
     }
     R vm[3];
@@ -409,7 +422,7 @@ __device__ __forceinline__ bool clock_tick(const Consts<R>& k, const R v[3], R& 
 // is the clock's bound and clk receives the new threshold U.
 // Returns 0 when the skip-clock event is thinned away, 1 when the candidate
 // is rejected, 2 on a collision (v updated).
-template <class R, bool SKIP>
+template <class R, bool SKIP, bool LANG>
 __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qstar, R Amean, R b, double mi_d,
                                          const uint32_t* rk, uint32_t id, uint32_t step) {
     R A, mean_th, sig_n, ug[3], mi, mn, inv_mt, fac;
@@ -439,7 +452,8 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
         clk = u32(r0.x, R(0));
     }
     const U4 r1 = philox4x32_10_rk(id, step, 1u, 0u, rk);
-    const bool thermal = uc * (b + mean_th) < b;
+    // Langevin capture: Maxwellian neutral (the thermal branch), every event collides
+    const bool thermal = LANG || (uc * (b + mean_th) < b);
     R c3, s3;
     angle_cs(u16(r1.y >> 16, R(0)), c3, s3);
     const R sfac = thermal ? c3 * c3 : R(1);
@@ -454,7 +468,7 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
     const R g = m_sqrt(gx * gx + gy * gy + gz * gz);
     const R q = A * (b + rad);
     const R pc = -m_expm1(-A * g);
-    if (!(u32(r0.z, R(0)) * q < pc)) return 1;
+    if (!LANG && !(u32(r0.z, R(0)) * q < pc)) return 1;
     const R ct2 = R(2.0) * u16(r1.z & 0xffffu, R(0)) - R(1.0);
     const R st2 = m_sqrt(m_fmax(R(0), R(1.0) - ct2 * ct2));
     R cp2, sp2;
@@ -547,6 +561,27 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
     }
     Consts<R> k;
     load_consts<R, FIELD, MAG>(k, C, q, m);
+    if constexpr (COLL == kCollLangevin) {
+        // speed-independent capture rate nu_i: event probability per step
+        // Q = 1 - exp(-nu_i dt) (A = 0)
+        const double mu = m * C.m_gas / (m + C.m_gas);
+        k.A = R(0);
+        k.Amean = static_cast<R>(-expm1(-C.lang_c * fabs(q) / sqrt(mu)));
+    }
+    k.sc = false;
+    if (p.escx != nullptr && in_range) {
+        // space charge: this launch advances one step with the field solved
+        // for the step's start positions; the uniform-field acceleration
+        // becomes (E0 q + E_sc q) / m
+        const double es[3] = {p.escx[i], p.escy[i], p.escz[i]};
+        k.sc = true;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            k.escq[a] = static_cast<R>(es[a] * q);
+            if constexpr (sizeof(R) == 8) k.a_uni[a] = static_cast<R>((C.E0[a] * q + es[a] * q) / m);
+            else k.a_uni[a] = static_cast<R>((C.E0[a] * q + es[a] * q) * (1.0 / m));
+        }
+    }
     if (INTEG == kRK4 && MAG) {
         k.tv[0] = static_cast<R>(C.B[0]); k.tv[1] = static_cast<R>(C.B[1]); k.tv[2] = static_cast<R>(C.B[2]);
     }
@@ -756,14 +791,14 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
                                 // horizon end without an event: consume its steps
                                 S = S - static_cast<R>(gs + 1u - g_start) * lam;
                             } else {
-                                const int st = candidate<R, true>(C, v, S, U, k.Amean, b, m, p.rk, id, gs);
+                                const int st = candidate<R, true, COLL == kCollLangevin>(C, v, S, U, k.Amean, b, m, p.rk, id, gs);
                                 if (st >= 1) ++n_cand;
                                 if (st == 2) ++n_coll;
                             }
                             clock_restart(gs + 1u);
                         } else {
                             ++n_cand;
-                            if (candidate<R, false>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs) == 2) ++n_coll;
+                            if (candidate<R, false, COLL == kCollLangevin>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs) == 2) ++n_coll;
                             S = R(1);
                             if constexpr (sizeof(R) == 4) {
                                 const R wx = v[0] - k.ug[0], wy = v[1] - k.ug[1], wz = v[2] - k.ug[2];

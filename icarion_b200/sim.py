@@ -201,6 +201,28 @@ class Simulation:
     def mark_reference(self) -> None:
         capi.check(self._lib.icb_mark_reference(self._h))
 
+    def configure_space_charge(self, mode: int, grid_n, box_min, box_max, alpha_h: float = 0.0,
+                               pp_cutoff_cells: float = 0.0, softening_m: float = -1.0,
+                               field_bound: float = 0.0) -> None:
+        """Space charge solved before every step (see icb_spacecharge_configure)."""
+        c = capi.SpaceChargeConfig()
+        c.mode = mode
+        c.grid_n[:] = [int(v) for v in grid_n]
+        c.box_min_m[:] = [float(v) for v in box_min]
+        c.box_max_m[:] = [float(v) for v in box_max]
+        c.alpha_h = alpha_h
+        c.pp_cutoff_cells = pp_cutoff_cells
+        c.softening_m = softening_m
+        c.field_bound_V_m = field_bound
+        capi.check(self._lib.icb_spacecharge_configure(self._h, C.byref(c)))
+
+    def space_charge_field(self) -> np.ndarray:
+        """[3, n] space-charge field (V/m) of the current state."""
+        out = np.zeros((3, self.n))
+        capi.check(self._lib.icb_spacecharge_field(self._h, capi.dptr(out[0]), capi.dptr(out[1]),
+                                                   capi.dptr(out[2])))
+        return out
+
     def autotune(self, trial_steps: int = 0) -> dict:
         """Pick the fastest launch shape on the uploaded ions; the state and
         clock are restored, so the run continues unchanged (see icb_autotune)."""

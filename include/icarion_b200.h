@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define ICB_ABI_VERSION 1
+#define ICB_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -125,6 +125,8 @@ typedef struct icb_run_stats {
     double device_ms;          /* device time of the call (CUDA events) */
     double step_kernel_ms;     /* device time inside the fused step kernel launches */
     uint64_t kernel_launches;  /* kernels this call launched */
+    double spacecharge_ms;     /* device time of the space-charge solves timed (the first 64 of the call) */
+    uint64_t spacecharge_solves_timed;
 } icb_run_stats;
 
 /* ---- ion cloud generation (IonLoader semantics) ------------------------ */
@@ -216,6 +218,44 @@ int icb_set_clock(struct icb_handle* h, uint64_t step, const double* time_s);
 int icb_moments(struct icb_handle* h, double* out);
 /* Store every ion's current position as its displacement reference. */
 int icb_mark_reference(struct icb_handle* h);
+
+/* ---- space charge (ISpaceChargeModel, ISpaceChargeModel.h:22-46) --------
+ * Replaces the GPU space-charge model the factory builds when
+ * physics.enable_space_charge_gpu is set (SpaceChargeModelFactory.cpp:29-95,
+ * GPUSpaceChargeP3M.h:61-92 for the configuration).  Once configured, every
+ * step of icb_advance / icb_push first solves the field of the current ion
+ * positions (ISpaceChargeModel::update_fields, once per step before the push,
+ * SimulationEngineLifecycle.cpp:16-32) and the push adds q E_sc to the force
+ * (ForceRegistry.cpp:76-87).  Needs one ensemble and the Boris pusher (the
+ * reference's RK4 refreshes space charge per stage).
+ *   ICB_SC_P3M_ISOLATED: P3M with free-space boundaries: CIC charges on the
+ *     mesh, zero-padded FFT convolution with the long-range part of the
+ *     Coulomb field of a Gaussian-screened charge (screening alpha), CIC
+ *     interpolation, plus a particle-particle correction to the softened
+ *     direct-sum field (SpaceChargeDirectModel.cpp:20-66) within
+ *     pp_cutoff_cells mesh cells.  Active ions inside the mesh take part.
+ *   ICB_SC_PM_PERIODIC_REF: the reference's GPU particle-mesh solver as it is
+ *     (GPUSpaceChargeP3M.cu:36-339): periodic FFT Poisson solve, central
+ *     differences, no particle-particle part, all ions deposit.
+ * Ions outside the mesh (a grid coordinate outside [0, n-1)) get no field
+ * and deposit nothing, as in the reference solver. */
+enum { ICB_SC_OFF = 0, ICB_SC_P3M_ISOLATED = 1, ICB_SC_PM_PERIODIC_REF = 2 };
+typedef struct icb_spacecharge_config {
+    int32_t mode;              /* ICB_SC_* */
+    int32_t grid_n[3];         /* mesh nodes per axis (8 .. 512), GPUSpaceChargeP3M::Config::grid_n* */
+    double box_min_m[3];       /* domain_min */
+    double box_max_m[3];       /* domain_max; node spacing h = (max - min) / n */
+    double alpha_h;            /* isolated: screening alpha times max(h); 0 = 1.0 */
+    double pp_cutoff_cells;    /* isolated: particle-particle cutoff in units of max(h); 0 = 2 */
+    double softening_m;        /* isolated: direct-sum softening; < 0 = 1e-10 (SpaceChargeModelFactory.h:26) */
+    double field_bound_V_m;    /* bound on |E_sc| added to the collision majorant's field bound;
+                                  0 = 4 x the largest |E_sc| of the configured state */
+    int32_t reserved[8];
+} icb_spacecharge_config;
+int icb_spacecharge_configure(struct icb_handle* h, const icb_spacecharge_config* cfg);
+/* Solve the field of the current state and copy E_sc (V/m) of every ion to
+ * host arrays (any may be NULL): ISpaceChargeModel::sample_electric_field. */
+int icb_spacecharge_field(struct icb_handle* h, double* ex, double* ey, double* ez);
 
 /* ---- launch-shape tuning ----------------------------------------------- */
 typedef struct icb_tuning {

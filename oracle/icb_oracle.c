@@ -45,6 +45,7 @@
 
 #define ORC_N_MOMENTS 20
 #define ORC_KB 1.380649e-23          /* utils/constants.h:15 */
+#define ORC_EPS0 8.854187817e-12     /* utils/constants.h:19 */
 #define ORC_GEOM_EPS 1e-12           /* CylindricalGeometry.h:245 */
 #define ORC_MIN_REL_VEL 1e-10        /* HSSCollisionHandler.cpp:20 */
 #define ORC_MIN_VEL_MAG 1e-12        /* CollisionKernels.h:172 */
@@ -366,7 +367,7 @@ static gas_consts gas_of(const orc_domain* d) {
 }
 
 static int nullcoll_candidate(const gas_consts* G, double v[3], double mi, uint64_t seed, uint32_t id,
-                              uint32_t step, int skip, double* clk, double qstar, double b) {
+                              uint32_t step, int skip, double* clk, double qstar, double b, int langevin) {
     const double* ug = G->ug;
     uint32_t r0[4], r1[4];
     philox_words(seed, id, step, 0u, r0);
@@ -382,7 +383,8 @@ static int nullcoll_candidate(const gas_consts* G, double v[3], double mi, uint6
         *clk = u32_to_unit(r0[0]);
     }
     philox_words(seed, id, step, 1u, r1);
-    const int thermal = uc * (b + G->mean_th) < b;
+    /* Langevin capture: a Maxwellian neutral (thermal branch), every event collides */
+    const int thermal = langevin ? 1 : (uc * (b + G->mean_th) < b);
     const double c3 = cos(2.0 * M_PI * u16_to_unit(r1[1] >> 16));
     const double sfac = thermal ? c3 * c3 : 1.0;
     const double r2 = -2.0 * (log(u32_to_unit(r0[3])) + log(u32_to_unit(r1[0])) * sfac);
@@ -395,7 +397,7 @@ static int nullcoll_candidate(const gas_consts* G, double v[3], double mi, uint6
     double g = sqrt(gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2]);
     double q = G->A * (b + rad);
     double p = -expm1(-G->A * g);
-    if (!(u32_to_unit(r0[2]) * q < p)) return 1;
+    if (!langevin && !(u32_to_unit(r0[2]) * q < p)) return 1;
     const double ct2 = 2.0 * u16_to_unit(r1[2] & 0xffffu) - 1.0;
     const double st2 = sqrt(fmax(0.0, 1.0 - ct2 * ct2));
     const double ph2 = 2.0 * M_PI * u16_to_unit(r1[3] >> 16);
@@ -420,9 +422,21 @@ static int hss_nullcoll(const orc_domain* d, double v[3], double mi, uint64_t se
     if (Q > 1.0) { Q = 1.0; ++*overflow; }
     *S = *S - *S * Q;
     if (!(*S < *U)) return -1;
-    const int r = nullcoll_candidate(&G, v, mi, seed, id, step, 0, U, 0.0, gu);
+    const int r = nullcoll_candidate(&G, v, mi, seed, id, step, 0, U, 0.0, gu, 0);
     *S = 1.0;
     return r;
+}
+
+/* Langevin capture (collision 3): a speed-independent rate per ion,
+ * nu = n pi |q| sqrt(alpha' / (4 pi eps0 mu)) — sigma_L(v) v of
+ * DampingForce.cpp:170-176 — so the per-step probability is the constant
+ * 1 - exp(-nu dt); the skip clock runs with A = 0 and Amean = nu dt, each
+ * event draws a Maxwellian neutral and scatters isotropically in the COM
+ * frame. */
+static double langevin_lambda(const orc_domain* d, double q, double m) {
+    const double mu = m * d->gas_mass_kg / (m + d->gas_mass_kg);
+    const double c = d->gas_density_m3 * d->dt_s * M_PI * sqrt(d->gas_polarizability_m3 / (4.0 * M_PI * ORC_EPS0));
+    return c * fabs(q) / sqrt(mu);
 }
 
 /* Upper bound of |E| over the cylinder (same expression as the product's
@@ -550,8 +564,10 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
             uint32_t* clk_next, uint32_t* clk_start,
             uint64_t first_id, uint64_t step0, double t0, int64_t n_steps,
             int64_t snap_every, int64_t ref_step, double* moments, uint64_t* counters, int n_threads) {
-    if (collision == 2 && (!clk_S || !clk_U)) return 1;
-    if (collision == 2 && integrator == 0 && (!clk_next || !clk_start)) return 1;
+    const int clocked = (collision == 2 || collision == 3);
+    if (clocked && (!clk_S || !clk_U)) return 1;
+    if (clocked && integrator == 0 && (!clk_next || !clk_start)) return 1;
+    if (collision == 3 && integrator != 0) return 1;
     const gas_consts G = gas_of(d);
     const int64_t n_snap = (snap_every > 0) ? n_steps / snap_every : 0;
     if (n_snap > 0 && moments) memset(moments, 0, sizeof(double) * (size_t)(n_snap * ORC_N_MOMENTS));
@@ -578,16 +594,21 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
             if (collision == 1) mt64_seed(rng, seed + first_id + (uint64_t)i);
             skip_clock sk;
             memset(&sk, 0, sizeof(sk));
-            const int skip = (collision == 2 && integrator == 0);
+            const int skip = (clocked && integrator == 0);
+            gas_consts Gi = G;
+            if (collision == 3) {
+                Gi.A = 0.0;
+                Gi.Amean = -expm1(-langevin_lambda(d, q, m));   /* per-step probability */
+            }
             if (skip) {
                 sk.tau = S;
                 sk.qstar = U;
                 sk.next = clk_next[i];
                 sk.start = clk_start[i];
-                skip_setup(&sk, d, &G, q, m);
+                skip_setup(&sk, d, &Gi, q, m);
                 if (act && contains(d, p) && sk.next == ORC_NEED_RESTART) {
                     uint64_t ov = 0;
-                    skip_restart(&sk, &G, v, (uint32_t)step0, &ov);
+                    skip_restart(&sk, &Gi, v, (uint32_t)step0, &ov);
                     ovf_tot += ov;
                 }
             }
@@ -606,18 +627,19 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                     else rk4_step(d, p, v, m, q, t, dt);
                     if (collision == 1) {
                         coll_tot += (uint64_t)hss_reference(d, v, m, rng);
-                    } else if (collision == 2 && skip) {
+                    } else if (skip) {
                         const uint32_t gs = (uint32_t)(step0 + (uint64_t)k);
                         if (sk.next != ORC_NEED_RESTART && gs == (sk.next & ~ORC_REFRESH)) {
                             uint64_t ov = 0;
                             if (sk.next & ORC_REFRESH) {
                                 sk.tau = sk.tau - (double)(gs + 1u - sk.start) * sk.lam;
                             } else {
-                                int r = nullcoll_candidate(&G, v, m, seed, id, gs, 1, &sk.tau, sk.qstar, 0.0);
+                                int r = nullcoll_candidate(&Gi, v, m, seed, id, gs, 1, &sk.tau, sk.qstar, 0.0,
+                                                           collision == 3);
                                 if (r >= 1) ++cand_tot;
                                 if (r == 2) ++coll_tot;
                             }
-                            skip_restart(&sk, &G, v, gs + 1u, &ov);
+                            skip_restart(&sk, &Gi, v, gs + 1u, &ov);
                             ovf_tot += ov;
                         }
                     } else if (collision == 2) {

@@ -122,14 +122,14 @@ def run(domain: dict, state: dict, n_steps: int, *, integrator: int = 0, collisi
     collision: 0 none, 1 reference HSS (mt19937_64 per ion), 2 null-collision
     HSS with Philox (``clock`` = (S, U, next, start) arrays from a previous
     call, or None to initialise; Boris uses the skip clock, RK4 the per-step
-    clock)."""
+    clock), 3 Langevin capture with Philox (Boris, skip clock)."""
     d = domain_struct(domain)
     n = state["x"].shape[0]
     for k in ("t_death", "t_arrival"):
         if state.get(k) is None:
             state[k] = np.full(n, -1.0)
     S = U = nxt = start = None
-    if collision == 2:
+    if collision in (2, 3):
         if clock is None:
             S, U = np.zeros(n), np.zeros(n)
             nxt, start = np.zeros(n, dtype=np.uint32), np.zeros(n, dtype=np.uint32)

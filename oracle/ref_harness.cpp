@@ -35,6 +35,7 @@
 #include "core/config/types/AnalyticalFieldModel.h"
 #include "core/config/types/CylindricalGeometry.h"
 #include "core/types/IonEnsemble.h"
+#include "core/physics/spacecharge/SpaceChargeDirectModel.h"
 #include "core/types/CollisionTypes.h"
 #include "utils/constants.h"
 
@@ -183,6 +184,40 @@ int mode_derive(const Args& a) {
                 d.environment.particle_density_m_3, d.environment.gas_mass_kg,
                 d.fields.dc.axial_V.constant_value.value_or(0.0),
                 d.fields.dc.axial_V.constant_value.value_or(0.0) / d.geometry.length_m);
+    return 0;
+}
+
+// Space-charge field of every ion from the reference's direct summation
+// (SpaceChargeDirectModel::update_fields, SpaceChargeDirectModel.cpp:20-66,
+// softening as the factory builds it, SpaceChargeModelFactory.h:26).
+// Output file: 3n doubles (Ex[n], Ey[n], Ez[n]).
+int mode_direct(const Args& a) {
+    State s = read_state(str(a, "in", "state.bin"));
+    std::vector<IonState> ions(static_cast<size_t>(s.n));
+    for (int64_t i = 0; i < s.n; ++i) {
+        auto& ion = ions[static_cast<size_t>(i)];
+        const size_t k = static_cast<size_t>(i);
+        ion.pos = Vec3{s.a[0][k], s.a[1][k], s.a[2][k]};
+        ion.vel = Vec3{s.a[3][k], s.a[4][k], s.a[5][k]};
+        ion.mass_kg = s.a[6][k];
+        ion.ion_charge_C = s.a[7][k];
+        ion.active = s.a[9][k] != 0.0;
+        ion.born = true;
+        ion.species_id = "ion";
+    }
+    core::IonEnsemble ens = core::IonEnsemble::from_legacy(ions);
+    physics::SpaceChargeDirectModel model(num(a, "softening", 1e-10));
+    model.update_fields(ens, 0.0);
+    FILE* f = std::fopen(str(a, "out", "field.bin").c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot write field file");
+    for (int c = 0; c < 3; ++c) {
+        for (int64_t i = 0; i < s.n; ++i) {
+            const Vec3 e = model.sample_electric_field(static_cast<size_t>(i));
+            const double v = c == 0 ? e.x : (c == 1 ? e.y : e.z);
+            std::fwrite(&v, sizeof(double), 1, f);
+        }
+    }
+    std::fclose(f);
     return 0;
 }
 
@@ -385,6 +420,7 @@ int main(int argc, char** argv) {
         if (mode == "init") return mode_init(a);
         if (mode == "derive") return mode_derive(a);
         if (mode == "run") return mode_run(a);
+        if (mode == "direct") return mode_direct(a);
         std::fprintf(stderr, "unknown mode %s\n", argv[1]);
         return 2;
     } catch (const std::exception& e) {

@@ -93,7 +93,7 @@ def test_philox_device_matches_oracle_and_curand():
 
 def _hss_gpu(st0: IonState, e: dict, steps: int, **kw) -> tuple[IonState, dict]:
     with Simulation([e], precision=kw.pop("precision", capi.PREC_FP64), integrator=capi.INTEGRATOR_BORIS,
-                    collision=capi.COLLISION_HSS, rng_seed=123, **kw) as sim:
+                    collision=kw.pop("collision", capi.COLLISION_HSS), rng_seed=123, **kw) as sim:
         sim.upload(st0)
         rs = sim.advance(steps)
         return sim.download(), rs
@@ -116,6 +116,28 @@ def test_fp64_hss_trajectories_match_oracle():
     assert frac >= 0.99, (frac, np.sort(rel)[-5:])
     assert abs(rs["collisions"] - r["collisions"]) <= 0.01 * r["collisions"]
     assert r["collisions"] > 0.05 * n * steps      # ~9% of ion-steps collide at config 0
+
+
+def test_fp64_langevin_trajectories_match_oracle():
+    """Langevin capture collisions (constant rate per ion, Maxwellian
+    neutral, isotropic COM scatter) against the oracle with the same Philox
+    streams: >= 99 % of ions to 1e-9 after 3000 steps; same collision count
+    within 1 %."""
+    n, steps = 512, 3000
+    e = config0_ensemble()
+    st0 = config0_ions(n)
+    ost = oracle_state(st0)
+    r = orc.run(e, ost, steps, integrator=0, collision=3, seed=123)
+    out, rs = _hss_gpu(st0, e, steps, collision=capi.COLLISION_LANGEVIN)
+    pos = np.stack([out.x, out.y, out.z])
+    opos = np.stack([ost["x"], ost["y"], ost["z"]])
+    vel = np.stack([out.vx, out.vy, out.vz])
+    ovel = np.stack([ost["vx"], ost["vy"], ost["vz"]])
+    rel = np.maximum(np.linalg.norm(pos - opos, axis=0) / np.linalg.norm(opos, axis=0),
+                     np.linalg.norm(vel - ovel, axis=0) / np.linalg.norm(ovel, axis=0))
+    assert float(np.mean(rel < 1e-9)) >= 0.99, np.sort(rel)[-5:]
+    assert abs(rs["collisions"] - r["collisions"]) <= 0.01 * r["collisions"]
+    assert r["collisions"] == r["candidates"] > 0.02 * n * steps
 
 
 def test_results_independent_of_launch_shape():
