@@ -448,7 +448,8 @@ def run_fticr(args) -> None:
     clk = clocks.stop()
     ms = sum(a.elapsed_time(b) for a, b in ev)
     value = n * steps_per * args.steps / (ms * 1e-3)
-    p3m_ms = sc_ms / max(sc_n, 1)
+    # solves are timed one by one only outside CUDA graphs
+    p3m_ms = sc_ms / sc_n if sc_n else None
     # algorithmic HBM bytes of one isolated P3M solve on the (2*128)^3 grid:
     # deposit write, forward FFT read+write, 3 x (kernel multiply: 2 reads +
     # 1 write, inverse FFT read+write) of the real (8 B) / half-complex
@@ -460,7 +461,7 @@ def run_fticr(args) -> None:
     grid_bytes = real_b + (real_b + cplx_b) + 3 * (3 * cplx_b) + 3 * (cplx_b + real_b)
     ion_bytes = n * (33 + 32 + 24 + 192 + 24)
     p3m_bytes = grid_bytes + ion_bytes
-    achieved = p3m_bytes / (p3m_ms * 1e-3) / 1e9
+    achieved = p3m_bytes / (p3m_ms * 1e-3) / 1e9 if p3m_ms else None
     peaks = measured_peaks()
     # end to end: host state in, steps_per steps, host state out, per bench step
     e2e_steps = min(args.steps, args.e2e_steps)
@@ -490,7 +491,8 @@ def run_fticr(args) -> None:
                    "push_ms_per_step": step_ms / max(step_n, 1)},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"],
+                     "frac": achieved / peaks["hbm_gbs"] if achieved else None, "traffic": None,
+                     "peak_source": peaks["source"],
                      "kernel": "isolated P3M solve (bin, sort, deposit, FFTs, kernel multiplies, gather + PP)",
                      "bytes_per_solve": p3m_bytes},
         "e2e": {"value": n * steps_per * e2e_steps / e2e_s, "unit": "ion-steps/s", "h2d_bytes_per_step": 6 * 8 * n + n,

@@ -28,6 +28,7 @@ INTEGRATOR_BORIS, INTEGRATOR_RK4 = 0, 1
 COLLISION_NONE, COLLISION_HSS, COLLISION_IPM_TABLE, COLLISION_IPM_MLP, COLLISION_LANGEVIN = 0, 1, 2, 3, 4
 INSTRUMENT_IMS, INSTRUMENT_FTICR, INSTRUMENT_QUADRUPOLE_RF = 0, 1, 2
 SC_OFF, SC_P3M_ISOLATED, SC_PM_PERIODIC_REF = 0, 1, 2
+MLP_HIDDEN, MLP_N_PARAMS = 64, 4417
 POS_POINT, POS_GAUSSIAN, POS_UNIFORM_SPHERE, POS_UNIFORM_CYLINDER, POS_UNIFORM_BOX = 0, 1, 2, 3, 4
 VEL_FIXED, VEL_THERMAL = 0, 1
 N_MOMENTS = 20
@@ -90,6 +91,21 @@ class SpaceChargeConfig(C.Structure):
     ]
 
 
+class IpmPotential(C.Structure):
+    _fields_ = [("epsilon_J", C.c_double), ("r_m_m", C.c_double), ("polarizability_m3", C.c_double),
+                ("charge_C", C.c_double)]
+
+
+class IpmConfig(C.Structure):
+    _fields_ = [("potential", IpmPotential), ("b_max_m", C.c_double), ("E_min_J", C.c_double),
+                ("E_max_J", C.c_double), ("n_E", C.c_int32), ("n_b", C.c_int32), ("reserved", C.c_int32 * 6)]
+
+
+class MlpTrainConfig(C.Structure):
+    _fields_ = [("epochs", C.c_int32), ("batch", C.c_int32), ("lr", C.c_double), ("lr_min", C.c_double),
+                ("seed", C.c_uint64), ("bf16_forward", C.c_int32), ("reserved", C.c_int32 * 5)]
+
+
 class Tuning(C.Structure):
     _fields_ = [
         ("block_size", C.c_int32), ("steps_per_vote", C.c_int32), ("pending_threshold", C.c_int32),
@@ -112,6 +128,7 @@ class SpeciesSpec(C.Structure):
 
 _P = C.POINTER
 _DP = _P(C.c_double)
+_FP = _P(C.c_float)
 _U8P = _P(C.c_uint8)
 _U32P = _P(C.c_uint32)
 _U64P = _P(C.c_uint64)
@@ -141,6 +158,14 @@ SIGNATURES = {
     "icb_autotune": (C.c_int, [_H, C.c_uint64, _P(Tuning)]),
     "icb_spacecharge_configure": (C.c_int, [_H, _P(SpaceChargeConfig)]),
     "icb_spacecharge_field": (C.c_int, [_H, _DP, _DP, _DP]),
+    "icb_ipm_deflection": (C.c_int, [C.c_int, _P(IpmPotential), C.c_uint64, _DP, _DP, _DP]),
+    "icb_ipm_configure": (C.c_int, [_H, _P(IpmConfig)]),
+    "icb_ipm_table": (C.c_int, [_H, _FP]),
+    "icb_ipm_set_mlp": (C.c_int, [_H, _FP]),
+    "icb_mlp_init": (C.c_int, [C.c_uint64, _FP]),
+    "icb_mlp_train": (C.c_int, [C.c_int, _P(MlpTrainConfig), C.c_uint64, _FP, _FP, _FP, _DP]),
+    "icb_mlp_forward": (C.c_int, [C.c_int, _FP, C.c_uint64, _FP, _FP, C.c_int]),
+    "icb_mlp_gradients": (C.c_int, [C.c_int, _FP, C.c_uint64, _FP, _FP, _FP, _DP]),
     "icb_generate_ions": (C.c_int, [C.c_uint32, C.c_int32, _P(SpeciesSpec), _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
     "icb_philox_eval": (C.c_int, [C.c_int, C.c_uint64, _U32P, C.c_uint64, C.c_int, _U32P]),
     "icb_moments_noalloc": (C.c_int, [C.c_int, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -172,6 +197,13 @@ def check(rc: int) -> None:
     if rc != ICB_OK:
         msg = lib().icb_last_error().decode(errors="replace")
         raise IcbError(rc, msg)
+
+
+def fptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_FP)
 
 
 def dptr(a: np.ndarray | None):

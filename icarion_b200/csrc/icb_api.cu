@@ -293,6 +293,13 @@ struct icb_handle {
     uint64_t graph_gen = 0;
     uint64_t graph_launches = 0;
     uint64_t gen = 1;                  // bumped whenever the graph goes stale
+    // interaction-potential collisions: cos(chi) table and learned model
+    DevBuf<float> ipm_tab;
+    int ipm_nE = 0, ipm_nb = 0;
+    double ipm_lnEmin = 0.0, ipm_inv_dlnE = 0.0, ipm_bmax = 0.0, ipm_Emin = 0.0, ipm_Emax = 0.0;
+    DevBuf<uint32_t> mlp_w2;
+    DevBuf<float> mlp_f;
+    bool mlp_ready = false;
     // space charge (solved before every step when configured)
     SpaceChargeSolver* sc = nullptr;
     double sc_emax_base = 0.0;         // ensemble 0's field bound without space charge
@@ -398,6 +405,11 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
                 return fail(ICB_ERR_INVALID_ARGUMENT, "Langevin collisions need gas_polarizability_m3 > 0");
             C.A = 0.0;
             C.lang_c = P.gas_density_m3 * P.dt_s * M_PI * std::sqrt(P.gas_polarizability_m3 / (4.0 * M_PI * kEps0));
+        } else if (coll == kCollIPMTable || coll == kCollIPMMLP) {
+            // event cross-section pi b_max^2 (InteractionPotentialCollisionHandler.cpp:443-447)
+            if (!(P.ipm_bmax_m > 0.0))
+                return fail(ICB_ERR_INVALID_ARGUMENT, "interaction-potential collisions need ipm_bmax_m > 0");
+            C.A = P.gas_density_m3 * (M_PI * P.ipm_bmax_m * P.ipm_bmax_m) * P.dt_s;
         } else {
             if (!(P.sigma_m2 > 0.0)) return fail(ICB_ERR_INVALID_ARGUMENT, "collisions need sigma_m2 > 0");
             C.A = P.gas_density_m3 * P.sigma_m2 * P.dt_s;
@@ -421,6 +433,10 @@ inline unsigned grid_for(uint64_t n, int block) { return static_cast<unsigned>((
 
 int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_finalize) {
     const int n_ens = static_cast<int>(h->ens.size());
+    if ((h->coll == kCollIPMTable || h->coll == kCollIPMMLP) && h->ipm_nE == 0)
+        return fail(ICB_ERR_STATE, "interaction-potential collisions need icb_ipm_configure first");
+    if (h->coll == kCollIPMMLP && !h->mlp_ready)
+        return fail(ICB_ERR_STATE, "the learned deflection needs icb_ipm_set_mlp first");
     for (int e0 = 0; e0 < n_ens; e0 += kMaxLaunchEns) {
         const int ne = std::min(kMaxLaunchEns, n_ens - e0);
         const uint64_t b = h->ens_off[static_cast<size_t>(e0)];
@@ -442,6 +458,13 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.escy = h->sc ? sc_field(h->sc, 1) : nullptr;
         p.escz = h->sc ? sc_field(h->sc, 2) : nullptr;
         p.zprev = h->zprev.p;
+        p.ipm_tab = h->ipm_tab.p;
+        p.ipm_nE = h->ipm_nE;
+        p.ipm_nb = h->ipm_nb;
+        p.ipm_lnEmin = h->ipm_lnEmin;
+        p.ipm_inv_dlnE = h->ipm_inv_dlnE;
+        p.mlp_w2 = h->mlp_w2.p;
+        p.mlp_f = h->mlp_f.p;
         p.counters = h->counters.p;
         p.step_dev = h->step_dev.p;
         p.t_dev = h->t_dev.p;
@@ -606,6 +629,12 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
     switch (cfg->collision_model) {
         case ICB_COLLISION_NONE: coll = kCollNone; break;
         case ICB_COLLISION_HSS: coll = kCollHSS; break;
+        case ICB_COLLISION_IPM_TABLE:
+        case ICB_COLLISION_IPM_MLP:
+            if (cfg->integrator != ICB_INTEGRATOR_BORIS)
+                return fail(ICB_ERR_UNSUPPORTED, "interaction-potential collisions are built for the Boris pusher");
+            coll = cfg->collision_model == ICB_COLLISION_IPM_TABLE ? kCollIPMTable : kCollIPMMLP;
+            break;
         case ICB_COLLISION_LANGEVIN:
             if (cfg->integrator != ICB_INTEGRATOR_BORIS)
                 return fail(ICB_ERR_UNSUPPORTED, "Langevin capture collisions are built for the Boris pusher");
@@ -992,6 +1021,63 @@ int icb_spacecharge_configure(icb_handle* h, const icb_spacecharge_config* cfg) 
         bound = 4.0 * mx;
     }
     h->ens_const[0].Emax = h->sc_emax_base + bound;
+    return ICB_OK;
+}
+
+int icb_ipm_configure(icb_handle* h, const icb_ipm_config* cfg) {
+    if (int r = check_handle(h)) return r;
+    if (!cfg) return fail(ICB_ERR_INVALID_ARGUMENT, "null IPM config");
+    if (cfg->n_E < 2 || cfg->n_b < 2 || cfg->n_E > 16384 || cfg->n_b > 16384)
+        return fail(ICB_ERR_INVALID_ARGUMENT, "IPM table needs 2 <= n_E, n_b <= 16384");
+    if (!(cfg->E_min_J > 0.0) || !(cfg->E_max_J > cfg->E_min_J) || !(cfg->b_max_m > 0.0))
+        return fail(ICB_ERR_INVALID_ARGUMENT, "IPM table needs 0 < E_min < E_max and b_max > 0");
+    for (const auto& e : h->ens)
+        if (std::fabs(e.ipm_bmax_m - cfg->b_max_m) > 1e-12 * cfg->b_max_m)
+            return fail(ICB_ERR_INVALID_ARGUMENT, "b_max_m must equal every ensemble's ipm_bmax_m");
+    std::string err;
+    IpmPotential P{};
+    if (int r = ipm_potential_from(cfg->potential, P, err)) return fail(r, "%s", err.c_str());
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
+    ICB_CUDA(h->ipm_tab.alloc(static_cast<size_t>(cfg->n_E) * cfg->n_b));
+    int r = ipm_build_table(h->cfg.device, P, cfg->n_E, cfg->n_b, cfg->E_min_J, cfg->E_max_J, cfg->b_max_m,
+                            h->ipm_tab.p, h->stream, err);
+    if (r != ICB_OK) {
+        h->ipm_nE = 0;
+        return fail(r, "%s", err.c_str());
+    }
+    h->ipm_nE = cfg->n_E;
+    h->ipm_nb = cfg->n_b;
+    h->ipm_lnEmin = std::log(cfg->E_min_J);
+    h->ipm_inv_dlnE = (cfg->n_E - 1) / (std::log(cfg->E_max_J) - h->ipm_lnEmin);
+    h->ipm_bmax = cfg->b_max_m;
+    h->ipm_Emin = cfg->E_min_J;
+    h->ipm_Emax = cfg->E_max_J;
+    ++h->gen;
+    return ICB_OK;
+}
+
+int icb_ipm_set_mlp(icb_handle* h, const float* params) {
+    if (int r = check_handle(h)) return r;
+    if (!params) return fail(ICB_ERR_INVALID_ARGUMENT, "null params");
+    std::vector<uint32_t> frag;
+    std::vector<float> fb;
+    mlp_pack(params, frag, fb);
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
+    ICB_CUDA(h->mlp_w2.alloc(frag.size()));
+    ICB_CUDA(h->mlp_f.alloc(fb.size()));
+    ICB_CUDA(cudaMemcpy(h->mlp_w2.p, frag.data(), frag.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    ICB_CUDA(cudaMemcpy(h->mlp_f.p, fb.data(), fb.size() * sizeof(float), cudaMemcpyHostToDevice));
+    h->mlp_ready = true;
+    ++h->gen;
+    return ICB_OK;
+}
+
+int icb_ipm_table(icb_handle* h, float* out) {
+    if (int r = check_handle(h)) return r;
+    if (h->ipm_nE == 0) return fail(ICB_ERR_STATE, "no IPM table");
+    if (!out) return fail(ICB_ERR_INVALID_ARGUMENT, "null output");
+    ICB_CUDA(cudaMemcpyAsync(out, h->ipm_tab.p, h->ipm_tab.n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
     return ICB_OK;
 }
 

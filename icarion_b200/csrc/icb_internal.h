@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/icarion_b200.h"
 #include "icb_params.h"
@@ -28,6 +29,14 @@ int sc_solve(SpaceChargeSolver* sc, const double* x, const double* y, const doub
              const uint8_t* flags, uint64_t n, cudaStream_t s, std::string& err);
 const double* sc_field(const SpaceChargeSolver* sc, int axis);
 int sc_kernel_count(const SpaceChargeSolver* sc);
+
+// Interaction-potential physics (icb_ipm.cu).
+int ipm_potential_from(const icb_ipm_potential& p, IpmPotential& P, std::string& err);
+int ipm_build_table(int device, const IpmPotential& P, int nE, int nb, double Emin, double Emax, double bmax,
+                    float* dev_table, cudaStream_t s, std::string& err);
+
+// Learned deflection (icb_mlp.cu): the collision path's parameter blocks.
+void mlp_pack(const float* params, std::vector<uint32_t>& frag, std::vector<float>& fblock);
 
 // Records the message icb_last_error() returns on this host thread and
 // passes `code` through.

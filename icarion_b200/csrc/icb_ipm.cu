@@ -1,0 +1,226 @@
+// icb_ipm.cu — interaction-potential collisions: the classical deflection
+// function of the ion-neutral potential by quadrature on the device, and the
+// cos(chi) table the stepping kernel samples.
+//
+// Potential (one isotropic site, the reference's LJ1264 form:
+// interaction_potential_precompute.cpp:1386-1420 and :1457-1508):
+//     V(r) = c12 / r^12 - c6 / r^6 - c4 / r^4,
+//     c12 = 4 eps sigma^12, c6 = 4 eps sigma^6, sigma = r_m 2^(-1/6),
+//     c4 = 1/2 alpha' k q^2 (:905, :929).
+// Deflection at centre-of-mass energy E and impact parameter b:
+//     chi = pi - 2 b \int_{r0}^inf dr / (r^2 sqrt(F(r))),  F = 1 - b^2/r^2 - V/E,
+// r0 the outermost zero of F.  With r = r0 / u and u = 1 - s^2 the integrand
+// is regular at the turning point:
+//     chi = pi - 2 (b / r0) \int_0^1 2 s ds / sqrt(F(r0 / (1 - s^2))),
+// evaluated with 64-point Gauss-Legendre.  r0 is bracketed by stepping
+// inwards by 2 % from 4 (b + sigma) and refined by bisection.  This replaces
+// the reference's per-trajectory velocity-Verlet integration (:1672-1796);
+// the two agree to a few 1e-4 in cos(chi) away from orbiting.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/icarion_b200.h"
+#include "icb_internal.h"
+
+namespace icb {
+
+namespace {
+
+constexpr double kCoulomb = 8.987551787e9;   // utils/constants.h:20
+constexpr int kGL = 64;
+
+struct GLNodes {
+    double s[kGL];   // nodes on [0, 1]
+    double w[kGL];   // weights on [0, 1]
+};
+
+// Gauss-Legendre nodes and weights on [-1, 1] by Newton iteration on P_n
+// (Golub-Welsch-free textbook recurrence), mapped to [0, 1].
+GLNodes make_gl() {
+    GLNodes g{};
+    const int n = kGL;
+    for (int i = 0; i < n; ++i) {
+        double x = std::cos(M_PI * (i + 0.75) / (n + 0.5));
+        double dp = 0.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = x;
+            for (int k = 2; k <= n; ++k) {
+                const double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (x * p1 - p0) / (x * x - 1.0);
+            const double dx = p1 / dp;
+            x -= dx;
+            if (std::fabs(dx) < 1e-16) break;
+        }
+        const double w = 2.0 / ((1.0 - x * x) * dp * dp);
+        g.s[i] = 0.5 * (x + 1.0);
+        g.w[i] = 0.5 * w;
+    }
+    return g;
+}
+
+__device__ __forceinline__ double ipm_F(const IpmPotential& P, double E, double b, double r) {
+    const double ir2 = 1.0 / (r * r);
+    const double ir4 = ir2 * ir2, ir6 = ir4 * ir2, ir12 = ir6 * ir6;
+    const double V = P.c12 * ir12 - P.c6 * ir6 - P.c4 * ir4;
+    return 1.0 - b * b * ir2 - V / E;
+}
+
+__device__ double ipm_cos_chi(const IpmPotential& P, const GLNodes& gl, double E, double b) {
+    if (!(E > 0.0)) return 1.0;
+    double r = 4.0 * (b + P.sigma);
+    int it = 0;
+    while (ipm_F(P, E, b, r * 0.98) > 0.0 && it < 4000) {
+        r *= 0.98;
+        ++it;
+    }
+    double lo = r * 0.98, hi = r;
+    for (int k = 0; k < 200 && hi - lo > 1e-15 * hi; ++k) {
+        const double mid = 0.5 * (lo + hi);
+        if (ipm_F(P, E, b, mid) > 0.0) hi = mid; else lo = mid;
+    }
+    const double r0 = hi;
+    double I = 0.0;
+    for (int k = 0; k < kGL; ++k) {
+        const double s = gl.s[k];
+        const double u = 1.0 - s * s;
+        const double F = fmax(ipm_F(P, E, b, r0 / u), 1e-300);
+        I += gl.w[k] * 2.0 * s / sqrt(F);
+    }
+    const double chi = M_PI - 2.0 * (b / r0) * I;
+    return cos(chi);
+}
+
+__global__ void k_ipm_deflection(IpmPotential P, const GLNodes* __restrict__ gl, uint64_t n,
+                                 const double* __restrict__ E, const double* __restrict__ b, double* __restrict__ out) {
+    __shared__ GLNodes sg;
+    for (int k = threadIdx.x; k < kGL; k += blockDim.x) {
+        sg.s[k] = gl->s[k];
+        sg.w[k] = gl->w[k];
+    }
+    __syncthreads();
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = ipm_cos_chi(P, sg, E[i], b[i]);
+}
+
+// cos(chi) on the table grid: E_k = E_min (E_max/E_min)^(k/(nE-1)),
+// b_j = b_max j / (nb - 1); row-major [k][j].
+__global__ void k_ipm_table(IpmPotential P, const GLNodes* __restrict__ gl, int nE, int nb, double lnEmin,
+                            double dlnE, double db, float* __restrict__ tab) {
+    __shared__ GLNodes sg;
+    for (int k = threadIdx.x; k < kGL; k += blockDim.x) {
+        sg.s[k] = gl->s[k];
+        sg.w[k] = gl->w[k];
+    }
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nE * nb) return;
+    const int k = i / nb, j = i % nb;
+    const double E = exp(lnEmin + k * dlnE);
+    tab[i] = static_cast<float>(ipm_cos_chi(P, sg, E, j * db));
+}
+
+std::mutex g_gl_mutex;
+GLNodes* g_gl_dev[64] = {};
+
+int gl_nodes(int device, const GLNodes** out, std::string& err) {
+    std::lock_guard<std::mutex> lock(g_gl_mutex);
+    if (device < 0 || device >= 64) {
+        err = "device ordinal out of range";
+        return ICB_ERR_INVALID_ARGUMENT;
+    }
+    if (!g_gl_dev[device]) {
+        const GLNodes h = make_gl();
+        GLNodes* d = nullptr;
+        cudaError_t e = cudaMalloc(&d, sizeof(GLNodes));
+        if (e == cudaSuccess) e = cudaMemcpy(d, &h, sizeof(GLNodes), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            err = std::string("Gauss-Legendre nodes: ") + cudaGetErrorString(e);
+            if (d) cudaFree(d);
+            return ICB_ERR_CUDA;
+        }
+        g_gl_dev[device] = d;
+    }
+    *out = g_gl_dev[device];
+    return ICB_OK;
+}
+
+}  // namespace
+
+int ipm_potential_from(const icb_ipm_potential& p, IpmPotential& P, std::string& err) {
+    if (!(p.epsilon_J >= 0.0) || !(p.r_m_m > 0.0) || !(p.polarizability_m3 >= 0.0)) {
+        err = "IPM potential needs epsilon_J >= 0, r_m_m > 0, polarizability_m3 >= 0";
+        return ICB_ERR_INVALID_ARGUMENT;
+    }
+    const double sigma = p.r_m_m * std::pow(2.0, -1.0 / 6.0);
+    const double s6 = std::pow(sigma, 6.0);
+    P.c12 = 4.0 * p.epsilon_J * s6 * s6;
+    P.c6 = 4.0 * p.epsilon_J * s6;
+    P.c4 = 0.5 * p.polarizability_m3 * kCoulomb * p.charge_C * p.charge_C;
+    P.sigma = sigma;
+    if (!(P.c12 > 0.0)) {
+        err = "IPM potential needs a repulsive wall (epsilon_J > 0)";
+        return ICB_ERR_INVALID_ARGUMENT;
+    }
+    return ICB_OK;
+}
+
+int ipm_build_table(int device, const IpmPotential& P, int nE, int nb, double Emin, double Emax, double bmax,
+                    float* dev_table, cudaStream_t s, std::string& err) {
+    const GLNodes* gl = nullptr;
+    if (int r = gl_nodes(device, &gl, err)) return r;
+    const double lnEmin = std::log(Emin);
+    const double dlnE = (std::log(Emax) - lnEmin) / (nE - 1);
+    const double db = bmax / (nb - 1);
+    const int total = nE * nb;
+    k_ipm_table<<<(total + 127) / 128, 128, 0, s>>>(P, gl, nE, nb, lnEmin, dlnE, db, dev_table);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        err = std::string("IPM table: ") + cudaGetErrorString(e);
+        return ICB_ERR_CUDA;
+    }
+    return ICB_OK;
+}
+
+}  // namespace icb
+
+using namespace icb;
+
+extern "C" int icb_ipm_deflection(int device, const icb_ipm_potential* pot, uint64_t n, const double* E_J,
+                                  const double* b_m, double* cos_chi) {
+    if (!pot || (n > 0 && (!E_J || !b_m || !cos_chi))) return set_error(ICB_ERR_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return ICB_OK;
+    std::string err;
+    IpmPotential P{};
+    if (int r = ipm_potential_from(*pot, P, err)) return set_error(r, err.c_str());
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return set_error(ICB_ERR_NO_DEVICE, cudaGetErrorString(e));
+    const GLNodes* gl = nullptr;
+    if (int r = gl_nodes(device, &gl, err)) return set_error(r, err.c_str());
+    double *dE = nullptr, *db = nullptr, *dout = nullptr;
+    const size_t bytes = n * sizeof(double);
+    e = cudaMalloc(&dE, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&db, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(dE, E_J, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(db, b_m, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_ipm_deflection<<<static_cast<unsigned>((n + 127) / 128), 128>>>(P, gl, n, dE, db, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(cos_chi, dout, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(dE);
+    cudaFree(db);
+    cudaFree(dout);
+    if (e != cudaSuccess) return set_error(ICB_ERR_CUDA, cudaGetErrorString(e));
+    return ICB_OK;
+}

@@ -27,6 +27,7 @@
 #include <cstdio>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "../../include/icarion_b200.h"
 #include "icb_internal.h"
@@ -84,6 +85,23 @@ __global__ void k_sc_cell_start(const uint32_t* __restrict__ keys, uint32_t n, u
     start[c] = lo;
 }
 
+// Positions and charges in sorted (cell) order: the deposit and the
+// particle-particle loops then read contiguous memory.
+// A float copy of the positions relative to the mesh origin serves as the
+// particle-particle loop's distance prefilter.
+__global__ void k_sc_permute(MeshGeom g, const double* __restrict__ x, const double* __restrict__ y,
+                             const double* __restrict__ z, const double* __restrict__ q,
+                             const uint32_t* __restrict__ vals, uint32_t n, double4* __restrict__ ps,
+                             float4* __restrict__ pf) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint32_t j = vals[s];
+    const double4 v = make_double4(x[j], y[j], z[j], q[j]);
+    ps[s] = v;
+    pf[s] = make_float4(static_cast<float>(v.x - g.lo0), static_cast<float>(v.y - g.lo1),
+                        static_cast<float>(v.z - g.lo2), 0.f);
+}
+
 // CIC weight of corner (ox, oy, oz) of a cell for fractions fr (taken left
 // to right: x, y, z).
 template <class W>
@@ -92,58 +110,61 @@ __device__ __forceinline__ W cic_w(int ox, int oy, int oz, W fx, W fy, W fz) {
     return (ox ? fx : one - fx) * (oy ? fy : one - fy) * (oz ? fz : one - fz);
 }
 
-// Charge per mesh node (C); nodes of the FFT grid outside the mesh are 0.
+// Charge per mesh node (C), written into the FFT grid (whose nodes outside
+// the mesh were zeroed before).  One thread per mesh node.
 template <bool REF_WEIGHTS>
-__global__ void k_sc_deposit(MeshGeom g, const double* __restrict__ x, const double* __restrict__ y,
-                             const double* __restrict__ z, const double* __restrict__ q,
-                             const uint32_t* __restrict__ vals, const uint32_t* __restrict__ start,
+__global__ void k_sc_deposit(MeshGeom g, const double4* __restrict__ ps, const uint32_t* __restrict__ start,
                              double* __restrict__ rho) {
-    const size_t total = static_cast<size_t>(g.m0) * g.m1 * g.m2;
+    const size_t total = static_cast<size_t>(g.n0) * g.n1 * g.n2;
     const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= total) return;
-    const int c = static_cast<int>(idx % g.m2);
-    const size_t t = idx / g.m2;
-    const int b = static_cast<int>(t % g.m1);
-    const int a = static_cast<int>(t / g.m1);
+    const int c = static_cast<int>(idx % g.n2);
+    const size_t t = idx / g.n2;
+    const int b = static_cast<int>(t % g.n1);
+    const int a = static_cast<int>(t / g.n1);
     double acc = 0.0;
-    if (a < g.n0 && b < g.n1 && c < g.n2) {
-        for (int ci = a - 1; ci <= a; ++ci) {
-            if (ci < 0 || ci > g.n0 - 2) continue;
-            for (int cj = b - 1; cj <= b; ++cj) {
-                if (cj < 0 || cj > g.n1 - 2) continue;
-                for (int ck = c - 1; ck <= c; ++ck) {
-                    if (ck < 0 || ck > g.n2 - 2) continue;
-                    const uint32_t key = (static_cast<uint32_t>(ci) * g.n1 + static_cast<uint32_t>(cj)) * g.n2 +
-                                         static_cast<uint32_t>(ck);
-                    const uint32_t s1 = start[key + 1];
-                    for (uint32_t s = start[key]; s < s1; ++s) {
-                        const uint32_t j = vals[s];
-                        const double fx = (x[j] - g.lo0) * g.ih0 - ci;
-                        const double fy = (y[j] - g.lo1) * g.ih1 - cj;
-                        const double fz = (z[j] - g.lo2) * g.ih2 - ck;
-                        double w;
-                        if (REF_WEIGHTS) {
-                            w = static_cast<double>(cic_w<float>(a - ci, b - cj, c - ck, static_cast<float>(fx),
-                                                                 static_cast<float>(fy), static_cast<float>(fz)));
-                        } else {
-                            w = cic_w<double>(a - ci, b - cj, c - ck, fx, fy, fz);
-                        }
-                        acc += w * q[j];
+    for (int ci = a - 1; ci <= a; ++ci) {
+        if (ci < 0 || ci > g.n0 - 2) continue;
+        for (int cj = b - 1; cj <= b; ++cj) {
+            if (cj < 0 || cj > g.n1 - 2) continue;
+            for (int ck = c - 1; ck <= c; ++ck) {
+                if (ck < 0 || ck > g.n2 - 2) continue;
+                const uint32_t key = (static_cast<uint32_t>(ci) * g.n1 + static_cast<uint32_t>(cj)) * g.n2 +
+                                     static_cast<uint32_t>(ck);
+                const uint32_t s1 = start[key + 1];
+                for (uint32_t s = start[key]; s < s1; ++s) {
+                    const double4 pj = ps[s];
+                    const double fx = (pj.x - g.lo0) * g.ih0 - ci;
+                    const double fy = (pj.y - g.lo1) * g.ih1 - cj;
+                    const double fz = (pj.z - g.lo2) * g.ih2 - ck;
+                    double w;
+                    if (REF_WEIGHTS) {
+                        w = static_cast<double>(cic_w<float>(a - ci, b - cj, c - ck, static_cast<float>(fx),
+                                                             static_cast<float>(fy), static_cast<float>(fz)));
+                    } else {
+                        w = cic_w<double>(a - ci, b - cj, c - ck, fx, fy, fz);
                     }
+                    acc += w * pj.w;
                 }
             }
         }
     }
-    rho[idx] = acc;
+    rho[(static_cast<size_t>(a) * g.m1 + static_cast<size_t>(b)) * g.m2 + static_cast<size_t>(c)] = acc;
 }
 
-// out = a * b (complex), n entries
-__global__ void k_sc_cmul(const cufftDoubleComplex* __restrict__ a, const cufftDoubleComplex* __restrict__ b,
-                          cufftDoubleComplex* __restrict__ out, size_t n) {
+// out_c = a * b_c (complex) for the three field components, n entries each
+__global__ void k_sc_cmul3(const cufftDoubleComplex* __restrict__ a, const cufftDoubleComplex* __restrict__ b0,
+                           const cufftDoubleComplex* __restrict__ b1, const cufftDoubleComplex* __restrict__ b2,
+                           cufftDoubleComplex* __restrict__ out, size_t n) {
     const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const cufftDoubleComplex u = a[i], v = b[i];
-    out[i] = make_cuDoubleComplex(u.x * v.x - u.y * v.y, u.x * v.y + u.y * v.x);
+    const cufftDoubleComplex u = a[i];
+    const cufftDoubleComplex* bs[3] = {b0, b1, b2};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const cufftDoubleComplex v = bs[c][i];
+        out[c * n + i] = make_cuDoubleComplex(u.x * v.x - u.y * v.y, u.x * v.y + u.y * v.x);
+    }
 }
 
 __device__ __forceinline__ double e_long(double r, double alpha) {
@@ -244,17 +265,30 @@ struct PPParams {
     int on;
     int r0, r1, r2;          // neighbour cell reach per axis
     double rc2, alpha, eps2, min_d2;
+    float rc2_pre;           // float prefilter bound, slightly above rc^2
+    double inv_dr;           // table intervals per metre
+    const double* table;     // L(r) at r = k / inv_dr, k = 0..kPPTable
 };
+
+// Particle-particle table: L(r) = r^2 E_long(r) / k = erf(a r) - (2 a r /
+// sqrt(pi)) exp(-a^2 r^2) on kPPTable equal intervals of [0, r_c], linearly
+// interpolated (relative error ~ (a r_c / kPPTable)^2 / 8 ~ 3e-8 at a r_c = 2).
+constexpr int kPPTable = 4096;
 
 // Field of every ion: CIC interpolation of the mesh field (+ particle-
 // particle correction).  Thread s handles the ion in sorted slot s.
 template <bool REF_WEIGHTS>
-__global__ void k_sc_gather(MeshGeom g, PPParams pp, const double* __restrict__ x, const double* __restrict__ y,
-                            const double* __restrict__ z, const double* __restrict__ q,
+__global__ void __launch_bounds__(256) k_sc_gather(MeshGeom g, PPParams pp, const double4* __restrict__ ps,
+                            const float4* __restrict__ pf,
                             const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                             const uint32_t* __restrict__ start, uint32_t n, const double* __restrict__ gx,
                             const double* __restrict__ gy, const double* __restrict__ gz, double* __restrict__ ex,
                             double* __restrict__ ey, double* __restrict__ ez) {
+    __shared__ double tab[REF_WEIGHTS ? 1 : kPPTable + 1];
+    if (!REF_WEIGHTS && pp.on) {
+        for (int k = threadIdx.x; k <= kPPTable; k += blockDim.x) tab[k] = pp.table[k];
+        __syncthreads();
+    }
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const uint32_t i = vals[s];
@@ -267,7 +301,8 @@ __global__ void k_sc_gather(MeshGeom g, PPParams pp, const double* __restrict__ 
     const uint32_t t = key / g.n2;
     const int cj = static_cast<int>(t % g.n1);
     const int ci = static_cast<int>(t / g.n1);
-    const double xi = x[i], yi = y[i], zi = z[i];
+    const double4 pi4 = ps[s];
+    const double xi = pi4.x, yi = pi4.y, zi = pi4.z;
     const double fx = (xi - g.lo0) * g.ih0 - ci;
     const double fy = (yi - g.lo1) * g.ih1 - cj;
     const double fz = (zi - g.lo2) * g.ih2 - ck;
@@ -295,8 +330,9 @@ __global__ void k_sc_gather(MeshGeom g, PPParams pp, const double* __restrict__ 
 #pragma unroll
         for (int c = 0; c < 3; ++c) E[c] = static_cast<double>(static_cast<float>(E[c]));
     }
-    if (pp.on) {
-        const double c2a = 2.0 * pp.alpha / sqrt(kPi);
+    if (!REF_WEIGHTS && pp.on) {
+        const float4 own = pf[s];
+        const float fxi = own.x, fyi = own.y, fzi = own.z;
         const int x0 = max(ci - pp.r0, 0), x1 = min(ci + pp.r0, g.n0 - 2);
         const int y0 = max(cj - pp.r1, 0), y1 = min(cj + pp.r1, g.n1 - 2);
         const int z0 = max(ck - pp.r2, 0), z1 = min(ck + pp.r2, g.n2 - 2);
@@ -306,15 +342,20 @@ __global__ void k_sc_gather(MeshGeom g, PPParams pp, const double* __restrict__ 
                 const uint32_t sa = start[row + static_cast<uint32_t>(z0)];
                 const uint32_t sb = start[row + static_cast<uint32_t>(z1) + 1u];
                 for (uint32_t s2 = sa; s2 < sb; ++s2) {
-                    const uint32_t j = vals[s2];
-                    if (j == i) continue;
-                    const double dx = xi - x[j], dy = yi - y[j], dz = zi - z[j];
+                    const float4 qf = pf[s2];
+                    const float ex0 = fxi - qf.x, ey0 = fyi - qf.y, ez0 = fzi - qf.z;
+                    if (ex0 * ex0 + ey0 * ey0 + ez0 * ez0 >= pp.rc2_pre) continue;
+                    const double4 pj = ps[s2];
+                    const double dx = xi - pj.x, dy = yi - pj.y, dz = zi - pj.z;
                     const double r2 = dx * dx + dy * dy + dz * dz;
-                    if (r2 < pp.min_d2 || r2 >= pp.rc2) continue;
+                    if (s2 == s || r2 < pp.min_d2 || r2 >= pp.rc2) continue;
                     const double r = sqrt(r2);
-                    const double ar = pp.alpha * r;
-                    const double el = erf(ar) / r2 - c2a * exp(-ar * ar) / r;
-                    const double sc = kCoulomb * (1.0 / (r2 + pp.eps2) - el) / r * q[j];
+                    const double u = r * pp.inv_dr;
+                    const int kt = min(static_cast<int>(u), kPPTable - 1);
+                    const double fr = u - kt;
+                    const double L = fma(fr, tab[kt + 1] - tab[kt], tab[kt]);
+                    // softened direct field minus the mesh's long-range part, / r
+                    const double sc = kCoulomb * (1.0 / (r2 + pp.eps2) - L / r2) / r * pj.w;
                     E[0] += dx * sc;
                     E[1] += dy * sc;
                     E[2] += dz * sc;
@@ -348,6 +389,9 @@ struct SpaceChargeSolver {
     uint32_t* vals = nullptr;
     uint32_t* vals_sorted = nullptr;
     uint32_t* start = nullptr;
+    double4* ps = nullptr;
+    float4* pf = nullptr;
+    double* pp_table = nullptr;
     void* cub_tmp = nullptr;
     size_t cub_bytes = 0;
     double* rho = nullptr;
@@ -356,19 +400,21 @@ struct SpaceChargeSolver {
     double* egrid[3] = {nullptr, nullptr, nullptr};
     cufftDoubleComplex* ghat[3] = {nullptr, nullptr, nullptr};
     double* esc[3] = {nullptr, nullptr, nullptr};
-    cufftHandle fwd = 0, inv = 0;
-    bool have_fwd = false, have_inv = false;
+    cufftHandle fwd = 0, inv = 0, inv3 = 0;
+    bool have_fwd = false, have_inv = false, have_inv3 = false;
     double max_field = 0.0;
 
     ~SpaceChargeSolver() {
         if (have_fwd) cufftDestroy(fwd);
         if (have_inv) cufftDestroy(inv);
+        if (have_inv3) cufftDestroy(inv3);
         for (void* p : {static_cast<void*>(keys), static_cast<void*>(keys_sorted), static_cast<void*>(vals),
-                        static_cast<void*>(vals_sorted), static_cast<void*>(start), cub_tmp,
+                        static_cast<void*>(vals_sorted), static_cast<void*>(start), static_cast<void*>(ps), static_cast<void*>(pf), static_cast<void*>(pp_table),
+                        cub_tmp,
                         static_cast<void*>(rho), static_cast<void*>(rho_hat), static_cast<void*>(tmp_hat)})
             if (p) cudaFree(p);
+        if (egrid[0]) cudaFree(egrid[0]);   // one block holds the three grids
         for (int c = 0; c < 3; ++c) {
-            if (egrid[c]) cudaFree(egrid[c]);
             if (ghat[c]) cudaFree(ghat[c]);
             if (esc[c]) cudaFree(esc[c]);
         }
@@ -454,6 +500,10 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, cudaStream_t s, 
         S.pp.r2 = static_cast<int>(std::ceil(rc / S.h[2]));
         S.pp.eps2 = soft * soft;
         S.pp.min_d2 = std::max(soft * soft * 1e-4, 1e-30);
+        S.pp.inv_dr = kPPTable / rc;
+        // float positions relative to the mesh origin carry an absolute error
+        // below 1e-7 of the box; the margin keeps every pair under r_c
+        S.pp.rc2_pre = static_cast<float>(rc * rc * 1.001 + 1e-6 * 3.0 * (c.box_max_m[0] - c.box_min_m[0]) * rc);
     }
     S.cap = static_cast<uint32_t>(n_ions);
     SC_CUDA(dev_alloc(&S.keys, S.cap));
@@ -461,13 +511,27 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, cudaStream_t s, 
     SC_CUDA(dev_alloc(&S.vals, S.cap));
     SC_CUDA(dev_alloc(&S.vals_sorted, S.cap));
     SC_CUDA(dev_alloc(&S.start, static_cast<size_t>(g.ncell) + 1));
+    SC_CUDA(dev_alloc(&S.ps, S.cap));
+    SC_CUDA(dev_alloc(&S.pf, S.cap));
+    if (iso) {
+        std::vector<double> tab(kPPTable + 1);
+        const double a = S.pp.alpha;
+        for (int k = 0; k <= kPPTable; ++k) {
+            const double r = k / S.pp.inv_dr;
+            tab[k] = std::erf(a * r) - (2.0 * a * r / std::sqrt(kPi)) * std::exp(-a * a * r * r);
+        }
+        SC_CUDA(dev_alloc(&S.pp_table, tab.size()));
+        SC_CUDA(cudaMemcpy(S.pp_table, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+        S.pp.table = S.pp_table;
+    }
     SC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, S.cub_bytes, S.keys, S.keys_sorted, S.vals, S.vals_sorted,
                                             static_cast<int>(S.cap), 0, S.key_bits, s));
     SC_CUDA(cudaMalloc(&S.cub_tmp, std::max<size_t>(S.cub_bytes, 16)));
     SC_CUDA(dev_alloc(&S.rho, S.real_size()));
     SC_CUDA(dev_alloc(&S.rho_hat, S.cplx_size()));
+    SC_CUDA(dev_alloc(&S.egrid[0], 3 * S.real_size()));
     for (int a = 0; a < 3; ++a) {
-        SC_CUDA(dev_alloc(&S.egrid[a], S.real_size()));
+        S.egrid[a] = S.egrid[0] + a * S.real_size();
         SC_CUDA(dev_alloc(&S.esc[a], S.cap));
     }
     SC_FFT(cufftPlan3d(&S.fwd, g.m0, g.m1, g.m2, CUFFT_D2Z));
@@ -477,7 +541,12 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, cudaStream_t s, 
     SC_FFT(cufftSetStream(S.fwd, s));
     SC_FFT(cufftSetStream(S.inv, s));
     if (iso) {
-        SC_CUDA(dev_alloc(&S.tmp_hat, S.cplx_size()));
+        // the three field components go through one batched inverse transform
+        int dims[3] = {g.m0, g.m1, g.m2};
+        SC_FFT(cufftPlanMany(&S.inv3, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 3));
+        S.have_inv3 = true;
+        SC_FFT(cufftSetStream(S.inv3, s));
+        SC_CUDA(dev_alloc(&S.tmp_hat, 3 * S.cplx_size()));
         for (int a = 0; a < 3; ++a) {
             SC_CUDA(dev_alloc(&S.ghat[a], S.cplx_size()));
             k_sc_green<<<blocks_for(S.real_size(), 256), 256, 0, s>>>(g, S.h[0], S.h[1], S.h[2], S.pp.alpha, a, S.rho);
@@ -505,6 +574,7 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
     const uint32_t nn = static_cast<uint32_t>(n);
     SC_FFT(cufftSetStream(S->fwd, s));
     SC_FFT(cufftSetStream(S->inv, s));
+    if (S->have_inv3) SC_FFT(cufftSetStream(S->inv3, s));
     k_sc_bin<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, flags, nn, iso ? 0 : 1, S->keys, S->vals);
     SC_CUDA(cudaGetLastError());
     size_t bytes = S->cub_bytes;
@@ -513,24 +583,24 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
     k_sc_cell_start<<<blocks_for(static_cast<size_t>(g.ncell) + 1, 256), 256, 0, s>>>(S->keys_sorted, nn, g.ncell,
                                                                                       S->start);
     SC_CUDA(cudaGetLastError());
+    k_sc_permute<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, q, S->vals_sorted, nn, S->ps, S->pf);
+    SC_CUDA(cudaGetLastError());
+    const size_t mesh_nodes = static_cast<size_t>(g.n0) * g.n1 * g.n2;
     if (iso) {
-        k_sc_deposit<false><<<blocks_for(S->real_size(), 256), 256, 0, s>>>(g, x, y, z, q, S->vals_sorted, S->start,
-                                                                             S->rho);
+        SC_CUDA(cudaMemsetAsync(S->rho, 0, S->real_size() * sizeof(double), s));
+        k_sc_deposit<false><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho);
         SC_CUDA(cudaGetLastError());
         SC_FFT(cufftExecD2Z(S->fwd, S->rho, S->rho_hat));
-        for (int a = 0; a < 3; ++a) {
-            k_sc_cmul<<<blocks_for(S->cplx_size(), 256), 256, 0, s>>>(S->rho_hat, S->ghat[a], S->tmp_hat,
-                                                                       S->cplx_size());
-            SC_CUDA(cudaGetLastError());
-            SC_FFT(cufftExecZ2D(S->inv, S->tmp_hat, S->egrid[a]));
-        }
-        k_sc_gather<false><<<blocks_for(nn, 128), 128, 0, s>>>(g, S->pp, x, y, z, q, S->keys_sorted, S->vals_sorted,
+        k_sc_cmul3<<<blocks_for(S->cplx_size(), 256), 256, 0, s>>>(S->rho_hat, S->ghat[0], S->ghat[1], S->ghat[2],
+                                                                    S->tmp_hat, S->cplx_size());
+        SC_CUDA(cudaGetLastError());
+        SC_FFT(cufftExecZ2D(S->inv3, S->tmp_hat, S->egrid[0]));
+        k_sc_gather<false><<<blocks_for(nn, 256), 256, 0, s>>>(g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted,
                                                                 S->start, nn, S->egrid[0], S->egrid[1], S->egrid[2],
                                                                 S->esc[0], S->esc[1], S->esc[2]);
         SC_CUDA(cudaGetLastError());
     } else {
-        k_sc_deposit<true><<<blocks_for(S->real_size(), 256), 256, 0, s>>>(g, x, y, z, q, S->vals_sorted, S->start,
-                                                                            S->rho);
+        k_sc_deposit<true><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho);
         SC_CUDA(cudaGetLastError());
         SC_FFT(cufftExecD2Z(S->fwd, S->rho, S->rho_hat));
         k_sc_poisson_ref<<<blocks_for(S->cplx_size(), 256), 256, 0, s>>>(g, S->h[0], S->h[1], S->h[2], S->rho_hat);
@@ -541,7 +611,7 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
         k_sc_efield_ref<<<blocks_for(S->real_size(), 256), 256, 0, s>>>(g, S->h[0], S->h[1], S->h[2], scale, S->rho,
                                                                          S->egrid[0], S->egrid[1], S->egrid[2]);
         SC_CUDA(cudaGetLastError());
-        k_sc_gather<true><<<blocks_for(nn, 128), 128, 0, s>>>(g, S->pp, x, y, z, q, S->keys_sorted, S->vals_sorted,
+        k_sc_gather<true><<<blocks_for(nn, 256), 256, 0, s>>>(g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted,
                                                                S->start, nn, S->egrid[0], S->egrid[1], S->egrid[2],
                                                                S->esc[0], S->esc[1], S->esc[2]);
         SC_CUDA(cudaGetLastError());
@@ -553,7 +623,7 @@ const double* sc_field(const SpaceChargeSolver* S, int axis) { return S->esc[axi
 
 int sc_kernel_count(const SpaceChargeSolver* S) {
     // kernels of one solve that this library launches (cuFFT and CUB not counted)
-    return S->mode == ICB_SC_P3M_ISOLATED ? 3 + 1 + 3 + 1 : 3 + 1 + 1 + 1 + 1;
+    return S->mode == ICB_SC_P3M_ISOLATED ? 4 + 1 + 1 + 1 : 4 + 1 + 1 + 1 + 1;
 }
 
 }  // namespace icb

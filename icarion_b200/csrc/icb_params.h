@@ -16,7 +16,7 @@ constexpr int kMaxLaunchEns = 64;   // ensembles per launch chunk (param space b
 constexpr uint32_t kMaxStepsPerLaunch = 16384;
 
 enum FieldKind : int { kFieldUniform = 0, kFieldLinear = 1, kFieldLinearRF = 2 };
-enum CollKind : int { kCollNone = 0, kCollHSS = 1, kCollLangevin = 2 };
+enum CollKind : int { kCollNone = 0, kCollHSS = 1, kCollLangevin = 2, kCollIPMTable = 3, kCollIPMMLP = 4 };
 enum PrecKind : int { kPrecFP64 = 0, kPrecMixed = 1, kPrecHiLo = 2 };
 enum IntegKind : int { kBoris = 0, kRK4 = 1 };
 
@@ -60,6 +60,11 @@ struct EnsConst {
     float pad_;
 };
 
+// Ion-neutral interaction potential V = c12/r^12 - c6/r^6 - c4/r^4 (SI).
+struct IpmPotential {
+    double c12, c6, c4, sigma;
+};
+
 struct StepParams {
     // FP64 / mixed positions
     double* x; double* y; double* z;
@@ -85,6 +90,15 @@ struct StepParams {
     // space charge advance one step, the field is solved before each)
     const double* escx; const double* escy; const double* escz;
     double* zprev;                     // z before the push, kept between unfused calls
+    // interaction-potential collisions: cos(chi) table [nE][nb] over
+    // ln E = lnEmin + k / inv_dlnE and b = b_max j / (nb - 1)
+    const float* ipm_tab;
+    int32_t ipm_nE, ipm_nb;
+    double ipm_lnEmin, ipm_inv_dlnE;
+    // learned deflection (MLP 2-64-64-1): packed BF16 weights and FP32
+    // biases (nullable unless the MLP model is selected)
+    const uint32_t* mlp_w2;            // W2 as mma B fragments
+    const float* mlp_f;                // W1 (128), b1 (64), b2 (64), W3 (64), b3 (1)
     unsigned long long* counters;      // kNumCounters
     const unsigned long long* step_dev;// engine step index at launch start
     const double* t_dev;               // engine time per ensemble at launch start

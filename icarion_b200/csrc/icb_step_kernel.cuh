@@ -30,6 +30,7 @@
 #include <type_traits>
 #include "icb_params.h"
 #include "icb_rng.cuh"
+#include "icb_mlp.cuh"
 
 namespace icb {
 
@@ -49,6 +50,8 @@ __device__ __forceinline__ double m_expm1(double x) { return expm1(x); }
 __device__ __forceinline__ float m_expm1(float x) { return expm1f(x); }
 __device__ __forceinline__ double m_fmax(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ float m_fmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double m_fmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float m_fmin(float a, float b) { return fminf(a, b); }
 
 // Uniforms from Philox words.  FP64: (w + 1) 2^-32 in (0, 1] and, for a
 // 16-bit half k, (k + 1/2) 2^-16 -- the oracle's conversions.  Float: the
@@ -422,9 +425,75 @@ __device__ __forceinline__ bool clock_tick(const Consts<R>& k, const R v[3], R& 
 // is the clock's bound and clk receives the new threshold U.
 // Returns 0 when the skip-clock event is thinned away, 1 when the candidate
 // is rejected, 2 on a collision (v updated).
-template <class R, bool SKIP, bool LANG>
+// cos(chi) from the interaction-potential table: bilinear in (ln E, b),
+// E clamped to the table range.
+template <class R>
+__device__ __forceinline__ R ipm_table_cos(const StepParams& p, R E, R bn) {
+    const int nE = p.ipm_nE, nb = p.ipm_nb;
+    R t = (m_log(E) - static_cast<R>(p.ipm_lnEmin)) * static_cast<R>(p.ipm_inv_dlnE);
+    t = m_fmin(m_fmax(t, R(0)), static_cast<R>(nE - 1));
+    const int k = min(static_cast<int>(t), nE - 2);
+    const R ft = t - static_cast<R>(k);
+    const R u = bn * static_cast<R>(nb - 1);
+    const int j = min(static_cast<int>(u), nb - 2);
+    const R fu = u - static_cast<R>(j);
+    const float* r0 = p.ipm_tab + static_cast<size_t>(k) * nb + j;
+    const float* r1 = r0 + nb;
+    const R c00 = static_cast<R>(__ldg(r0)), c01 = static_cast<R>(__ldg(r0 + 1));
+    const R c10 = static_cast<R>(__ldg(r1)), c11 = static_cast<R>(__ldg(r1 + 1));
+    const R lo = c00 + fu * (c01 - c00);
+    const R hi = c10 + fu * (c11 - c10);
+    return lo + ft * (hi - lo);
+}
+
+// Relative velocity g turned by the polar angle chi (cos cx, sin sx) about
+// its own direction, azimuth (cp, sp) (Bird 1994, eq. 2.22).
+template <class R>
+__device__ __forceinline__ void deflect(const R g3[3], R g, R cx, R sx, R cp, R sp, R out[3]) {
+    const R gyz = m_sqrt(g3[1] * g3[1] + g3[2] * g3[2]);
+    if (gyz > R(1e-6) * g) {
+        const R ig = R(1) / gyz;
+        out[0] = g3[0] * cx + sx * sp * gyz;
+        out[1] = g3[1] * cx + sx * (g * g3[2] * cp - g3[0] * g3[1] * sp) * ig;
+        out[2] = g3[2] * cx - sx * (g * g3[1] * cp + g3[0] * g3[2] * sp) * ig;
+    } else {
+        out[0] = g3[0] * cx;
+        out[1] = g * sx * cp;
+        out[2] = g * sx * sp;
+    }
+}
+
+// A collision whose deflection waits for the warp's network evaluation.
+template <class R>
+struct IpmPend {
+    R g3[3], g, vn[3], E, bn, cp, sp;
+};
+
+// v after an elastic deflection of the relative velocity by chi.
+template <class R>
+__device__ __forceinline__ void ipm_apply(const EnsConst& C, R v[3], const IpmPend<R>& ip, R cx, double mi_d) {
+    R mi, mn, inv_mt;
+    if constexpr (sizeof(R) == 8) {
+        mi = mi_d; mn = C.m_gas; inv_mt = 1.0 / (mi_d + C.m_gas);
+    } else {
+        mi = static_cast<float>(mi_d); mn = C.fm_gas; inv_mt = __frcp_rn(mi + mn);
+    }
+    const R fac = mn * inv_mt;
+    const R sx = m_sqrt(m_fmax(R(0), R(1) - cx * cx));
+    R gp[3];
+    deflect<R>(ip.g3, ip.g, cx, sx, ip.cp, ip.sp, gp);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const R vcom = (v[c] * mi + ip.vn[c] * mn) * inv_mt;
+        v[c] = vcom + gp[c] * fac;
+    }
+}
+
+template <class R, bool SKIP, int COLL>
 __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qstar, R Amean, R b, double mi_d,
-                                         const uint32_t* rk, uint32_t id, uint32_t step) {
+                                         const uint32_t* rk, uint32_t id, uint32_t step, const StepParams& p,
+                                         IpmPend<R>* ip) {
+    constexpr bool LANG = COLL == kCollLangevin;
     R A, mean_th, sig_n, ug[3], mi, mn, inv_mt, fac;
     if constexpr (sizeof(R) == 8) {
         A = C.A; mean_th = C.mean_th; sig_n = C.sig_n;
@@ -469,6 +538,36 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
     const R q = A * (b + rad);
     const R pc = -m_expm1(-A * g);
     if (!LANG && !(u32(r0.z, R(0)) * q < pc)) return 1;
+    if constexpr (COLL == kCollIPMMLP) {
+        // deflection after the warp's network evaluation
+        const R mu = mi * mn * inv_mt;
+        ip->E = R(0.5) * mu * (g * g);
+        ip->bn = m_sqrt(u16(r1.z & 0xffffu, R(0)));
+        angle_cs(u16(r1.w >> 16, R(0)), ip->cp, ip->sp);
+        ip->g3[0] = gx; ip->g3[1] = gy; ip->g3[2] = gz;
+        ip->g = g;
+        ip->vn[0] = vn[0]; ip->vn[1] = vn[1]; ip->vn[2] = vn[2];
+        return 3;
+    }
+    if constexpr (COLL == kCollIPMTable) {
+        // elastic deflection by chi(E, b): b uniform in area below b_max
+        const R mu = mi * mn * inv_mt;
+        const R E = R(0.5) * mu * (g * g);
+        const R bn = m_sqrt(u16(r1.z & 0xffffu, R(0)));
+        const R cx = ipm_table_cos<R>(p, E, bn);
+        const R sx = m_sqrt(m_fmax(R(0), R(1) - cx * cx));
+        R cp2, sp2;
+        angle_cs(u16(r1.w >> 16, R(0)), cp2, sp2);
+        const R g3[3] = {gx, gy, gz};
+        R gp[3];
+        deflect<R>(g3, g, cx, sx, cp2, sp2, gp);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const R vcom = (v[c] * mi + vn[c] * mn) * inv_mt;
+            v[c] = vcom + gp[c] * fac;
+        }
+        return 2;
+    }
     const R ct2 = R(2.0) * u16(r1.z & 0xffffu, R(0)) - R(1.0);
     const R st2 = m_sqrt(m_fmax(R(0), R(1.0) - ct2 * ct2));
     R cp2, sp2;
@@ -783,22 +882,53 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
             const unsigned run_mask = __ballot_sync(0xffffffffu, can_step);
             if (pend_mask != 0u &&
                 (run_mask == 0u || static_cast<uint32_t>(__popc(pend_mask)) >= p.pend_threshold)) {
+                IpmPend<R> ip;
+                bool need_net = false;
+                const uint32_t gs = step0 + kk;
+                if (pending && cand) {
+                    if constexpr (kSkip) {
+                        if (g_next & kRefresh) {
+                            // horizon end without an event: consume its steps
+                            S = S - static_cast<R>(gs + 1u - g_start) * lam;
+                        } else {
+                            const int st = candidate<R, true, COLL>(C, v, S, U, k.Amean, b, m, p.rk, id, gs, p, &ip);
+                            if (st >= 1) ++n_cand;
+                            if (st >= 2) ++n_coll;
+                            need_net = st == 3;
+                        }
+                    } else {
+                        ++n_cand;
+                        const int st = candidate<R, false, COLL>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs, p, &ip);
+                        if (st >= 2) ++n_coll;
+                        need_net = st == 3;
+                    }
+                }
+                if constexpr (COLL == kCollIPMMLP) {
+                    // the warp's accepted collisions share one tensor-core
+                    // evaluation of the deflection network; energies outside
+                    // the trained range use the table
+                    if (__any_sync(0xffffffffu, need_net)) {
+                        R t = R(0);
+                        bool in_dom = false;
+                        if (need_net) {
+                            t = (m_log(ip.E) - static_cast<R>(p.ipm_lnEmin)) * static_cast<R>(p.ipm_inv_dlnE);
+                            in_dom = t >= R(0) && t <= static_cast<R>(p.ipm_nE - 1);
+                        }
+                        const float x0 = static_cast<float>(R(2) * t / static_cast<R>(p.ipm_nE - 1) - R(1));
+                        const float x1 = static_cast<float>(R(2) * ip.bn - R(1));
+                        const float y = mlp_warp_eval(p.mlp_w2, p.mlp_f, x0, x1, need_net && in_dom);
+                        if (need_net) {
+                            R cx = in_dom ? m_fmin(m_fmax(static_cast<R>(y), R(-1)), R(1))
+                                          : ipm_table_cos<R>(p, ip.E, ip.bn);
+                            ipm_apply<R>(C, v, ip, cx, m);
+                        }
+                    }
+                }
                 if (pending) {
                     if (cand) {
-                        const uint32_t gs = step0 + kk;
                         if constexpr (kSkip) {
-                            if (g_next & kRefresh) {
-                                // horizon end without an event: consume its steps
-                                S = S - static_cast<R>(gs + 1u - g_start) * lam;
-                            } else {
-                                const int st = candidate<R, true, COLL == kCollLangevin>(C, v, S, U, k.Amean, b, m, p.rk, id, gs);
-                                if (st >= 1) ++n_cand;
-                                if (st == 2) ++n_coll;
-                            }
                             clock_restart(gs + 1u);
                         } else {
-                            ++n_cand;
-                            if (candidate<R, false, COLL == kCollLangevin>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs) == 2) ++n_coll;
                             S = R(1);
                             if constexpr (sizeof(R) == 4) {
                                 const R wx = v[0] - k.ug[0], wy = v[1] - k.ug[1], wz = v[2] - k.ug[2];

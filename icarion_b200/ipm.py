@@ -1,0 +1,136 @@
+"""Interaction-potential collisions: the ion-neutral potential, its
+deflection function (device quadrature), the cos(chi) table of a handle and
+the learned deflection network (training, evaluation, loading).
+
+Default potential: the reference's LJ1264 form (interaction_potential_
+precompute.cpp:1386-1508) for an ion in N2 with a 12-6 well of 5 meV at
+r_m = 4 A plus the induced-dipole term of the N2 polarisability 1.74 A^3
+(utils/constants.h:54) for a singly charged ion; ion mass 300 Da.  The
+collision event cross-section is pi b_max^2 with b_max = 12 A; the table
+and the network cover centre-of-mass energies 1 meV - 10 eV.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _capi as capi
+from . import config as cfg
+
+EV_J = 1.602176634e-19
+
+
+@dataclass
+class IpmSetup:
+    epsilon_J: float = 5e-3 * EV_J
+    r_m_m: float = 4e-10
+    polarizability_m3: float = 1.74e-30
+    charge_C: float = cfg.ELEM_CHARGE_C
+    b_max_m: float = 12e-10
+    E_min_J: float = 1e-3 * EV_J
+    E_max_J: float = 10.0 * EV_J
+    n_E: int = 512
+    n_b: int = 256
+
+    def potential(self) -> capi.IpmPotential:
+        p = capi.IpmPotential()
+        p.epsilon_J = self.epsilon_J
+        p.r_m_m = self.r_m_m
+        p.polarizability_m3 = self.polarizability_m3
+        p.charge_C = self.charge_C
+        return p
+
+    def config(self) -> capi.IpmConfig:
+        c = capi.IpmConfig()
+        c.potential = self.potential()
+        c.b_max_m = self.b_max_m
+        c.E_min_J = self.E_min_J
+        c.E_max_J = self.E_max_J
+        c.n_E = self.n_E
+        c.n_b = self.n_b
+        return c
+
+    def coefficients(self) -> tuple[float, float, float]:
+        """(c12, c6, c4) of V = c12/r^12 - c6/r^6 - c4/r^4."""
+        sigma = self.r_m_m * 2.0 ** (-1.0 / 6.0)
+        c12 = 4.0 * self.epsilon_J * sigma ** 12
+        c6 = 4.0 * self.epsilon_J * sigma ** 6
+        c4 = 0.5 * self.polarizability_m3 * 8.987551787e9 * self.charge_C ** 2
+        return c12, c6, c4
+
+
+def deflection(setup: IpmSetup, E_J: np.ndarray, b_m: np.ndarray, device: int = 0) -> np.ndarray:
+    """cos(chi) of the device quadrature."""
+    E = np.ascontiguousarray(E_J, dtype=np.float64)
+    b = np.ascontiguousarray(b_m, dtype=np.float64)
+    out = np.zeros_like(E)
+    pot = setup.potential()
+    capi.check(capi.lib().icb_ipm_deflection(device, C.byref(pot), E.size, capi.dptr(E), capi.dptr(b),
+                                             capi.dptr(out)))
+    return out
+
+
+def normalize(setup: IpmSetup, E_J: np.ndarray, b_m: np.ndarray) -> np.ndarray:
+    """Network inputs (2n float32): 2 (ln E - ln E_min)/(ln E_max - ln E_min) - 1, 2 b/b_max - 1."""
+    lo, hi = math.log(setup.E_min_J), math.log(setup.E_max_J)
+    x0 = 2.0 * (np.log(E_J) - lo) / (hi - lo) - 1.0
+    x1 = 2.0 * np.asarray(b_m) / setup.b_max_m - 1.0
+    return np.ascontiguousarray(np.stack([x0, x1], axis=1).ravel(), dtype=np.float32)
+
+
+def training_set(setup: IpmSetup, n: int = 2 ** 20, seed: int = 2024, device: int = 0):
+    """n (E, b) pairs, E log-uniform over [E_min, E_max], b uniform over
+    [0, b_max], with cos(chi) from the quadrature: (x, y, E, b)."""
+    rng = np.random.default_rng(seed)
+    E = np.exp(rng.uniform(math.log(setup.E_min_J), math.log(setup.E_max_J), n))
+    b = rng.uniform(0.0, setup.b_max_m, n)
+    y = deflection(setup, E, b, device).astype(np.float32)
+    return normalize(setup, E, b), y, E, b
+
+
+def init_params(seed: int = 7) -> np.ndarray:
+    p = np.zeros(capi.MLP_N_PARAMS, dtype=np.float32)
+    capi.check(capi.lib().icb_mlp_init(seed, capi.fptr(p)))
+    return p
+
+
+def train(x: np.ndarray, y: np.ndarray, params: np.ndarray | None = None, epochs: int = 30, batch: int = 1024,
+          lr: float = 3e-3, lr_min: float = 1e-5, seed: int = 7, bf16_forward: bool = True,
+          device: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Adam on the device; returns (params, loss per epoch)."""
+    p = init_params(seed) if params is None else np.array(params, dtype=np.float32, copy=True)
+    c = capi.MlpTrainConfig()
+    c.epochs = epochs
+    c.batch = batch
+    c.lr = lr
+    c.lr_min = lr_min
+    c.seed = seed
+    c.bf16_forward = int(bf16_forward)
+    losses = np.zeros(epochs)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    capi.check(capi.lib().icb_mlp_train(device, C.byref(c), y.size, capi.fptr(x), capi.fptr(y), capi.fptr(p),
+                                        capi.dptr(losses)))
+    return p, losses
+
+
+def forward(params: np.ndarray, x: np.ndarray, mode: int = 1, device: int = 0) -> np.ndarray:
+    """mode 0: FP32 arithmetic; mode 1: the collision path's BF16 tensor-core evaluation."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.zeros(x.size // 2, dtype=np.float32)
+    capi.check(capi.lib().icb_mlp_forward(device, capi.fptr(np.ascontiguousarray(params, dtype=np.float32)),
+                                          y.size, capi.fptr(x), capi.fptr(y), mode))
+    return y
+
+
+def gradients(params: np.ndarray, x: np.ndarray, y: np.ndarray, device: int = 0) -> tuple[np.ndarray, float]:
+    g = np.zeros(capi.MLP_N_PARAMS, dtype=np.float32)
+    loss = C.c_double(0.0)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    capi.check(capi.lib().icb_mlp_gradients(device, capi.fptr(np.ascontiguousarray(params, dtype=np.float32)),
+                                            y.size, capi.fptr(x), capi.fptr(y), capi.fptr(g), C.byref(loss)))
+    return g, loss.value

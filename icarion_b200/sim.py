@@ -223,6 +223,21 @@ class Simulation:
                                                    capi.dptr(out[2])))
         return out
 
+    def configure_ipm(self, setup) -> None:
+        """Build the interaction-potential cos(chi) table (an ipm.IpmSetup)."""
+        c = setup.config()
+        capi.check(self._lib.icb_ipm_configure(self._h, C.byref(c)))
+        self._ipm_shape = (setup.n_E, setup.n_b)
+
+    def ipm_table(self) -> np.ndarray:
+        out = np.zeros(self._ipm_shape, dtype=np.float32)
+        capi.check(self._lib.icb_ipm_table(self._h, capi.fptr(out.reshape(-1))))
+        return out
+
+    def set_mlp(self, params: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        capi.check(self._lib.icb_ipm_set_mlp(self._h, capi.fptr(p)))
+
     def autotune(self, trial_steps: int = 0) -> dict:
         """Pick the fastest launch shape on the uploaded ions; the state and
         clock are restored, so the run continues unchanged (see icb_autotune)."""

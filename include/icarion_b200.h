@@ -257,6 +257,79 @@ int icb_spacecharge_configure(struct icb_handle* h, const icb_spacecharge_config
  * host arrays (any may be NULL): ISpaceChargeModel::sample_electric_field. */
 int icb_spacecharge_field(struct icb_handle* h, double* ex, double* ey, double* ez);
 
+/* ---- interaction-potential collisions ----------------------------------
+ * Replaces InteractionPotentialCollisionHandler::handle_collision
+ * (InteractionPotentialCollisionHandler.cpp:298-552) and its offline table
+ * (InteractionPotentialOfflineSampleSet.h:16-98) for an isotropic ion-neutral
+ * potential: the reference's LJ1264 form V = c12/r^12 - c6/r^6 - c4/r^4
+ * (interaction_potential_precompute.cpp:1386-1508), c12 = 4 eps sigma^12,
+ * c6 = 4 eps sigma^6, sigma = r_m 2^(-1/6), c4 = 1/2 alpha' k q^2.
+ * A collision event happens at rate n g pi b_max^2 (sigma_event, the
+ * ensemble's ipm_bmax_m); the impact parameter is uniform in area below
+ * b_max and the relative velocity is deflected elastically by chi(E, b),
+ * E = mu g^2 / 2, with a uniform azimuth (the reference applies the
+ * equivalent momentum transfer mu (v_out - v0) from its trajectory samples). */
+typedef struct icb_ipm_potential {
+    double epsilon_J;          /* LJ well depth */
+    double r_m_m;              /* LJ minimum position */
+    double polarizability_m3;  /* neutral polarizability volume alpha' */
+    double charge_C;           /* ion charge in the induced-dipole term */
+} icb_ipm_potential;
+/* cos(chi) at n (E, b) pairs by the device quadrature (chi = pi - 2 b
+ * int dr / (r^2 sqrt(1 - b^2/r^2 - V/E)) from the outermost turning point);
+ * host arrays.  Replaces the trajectory integration of
+ * interaction_potential_precompute.cpp:1672-1835. */
+int icb_ipm_deflection(int device, const icb_ipm_potential* pot, uint64_t n, const double* E_J,
+                       const double* b_m, double* cos_chi);
+typedef struct icb_ipm_config {
+    icb_ipm_potential potential;
+    double b_max_m;            /* must equal every ensemble's ipm_bmax_m */
+    double E_min_J, E_max_J;   /* table range (log-spaced); energies outside are clamped */
+    int32_t n_E, n_b;          /* table size (>= 2 each) */
+    int32_t reserved[6];
+} icb_ipm_config;
+/* Build the cos(chi) table of the handle on its device (collision models
+ * ICB_COLLISION_IPM_TABLE and ICB_COLLISION_IPM_MLP need it; the learned
+ * model falls back to it outside [E_min, E_max]). */
+int icb_ipm_configure(struct icb_handle* h, const icb_ipm_config* cfg);
+/* Copy the table (n_E * n_b floats, row-major [E][b]) to the host. */
+int icb_ipm_table(struct icb_handle* h, float* out);
+
+/* ---- learned deflection (MLP 2 -> 64 -> 64 -> 1, tanh) ------------------
+ * No counterpart in the reference: a network trained on the quadrature's
+ * cos(chi) replaces the table lookup in the collision path.  Inputs
+ * x0 = 2 (ln E - ln E_min) / (ln E_max - ln E_min) - 1, x1 = 2 b / b_max - 1;
+ * output cos(chi).  Parameters (ICB_MLP_N_PARAMS floats, in order):
+ * W1[64][2], b1[64], W2[64][64], b2[64], W3[64], b3.  In the collision path
+ * the weights are BF16 and the 64x64 layer runs on the tensor cores
+ * (mma.sync m16n8k16, FP32 accumulation), the warp's colliding ions forming
+ * the rows. */
+#define ICB_MLP_HIDDEN 64
+#define ICB_MLP_N_PARAMS 4417
+typedef struct icb_mlp_train_config {
+    int32_t epochs;
+    int32_t batch;             /* samples per Adam step */
+    double lr;                 /* initial learning rate (cosine decay to lr_min) */
+    double lr_min;
+    uint64_t seed;             /* initialisation and shuffling */
+    int32_t bf16_forward;      /* train through the BF16 forward of the collision path */
+    int32_t reserved[5];
+} icb_mlp_train_config;
+/* Xavier-uniform initial parameters from `seed`. */
+int icb_mlp_init(uint64_t seed, float* params);
+/* Adam on the mean squared error over n samples (x: 2n floats, y: n floats,
+ * host); params in/out; loss_per_epoch (epochs doubles) may be NULL. */
+int icb_mlp_train(int device, const icb_mlp_train_config* cfg, uint64_t n, const float* x, const float* y,
+                  float* params, double* loss_per_epoch);
+/* Network output for n inputs: mode 0 = FP32 reference arithmetic, mode 1 =
+ * the collision path's BF16 tensor-core evaluation. */
+int icb_mlp_forward(int device, const float* params, uint64_t n, const float* x, float* y, int mode);
+/* Gradient of the mean squared error (FP32 arithmetic) and the loss. */
+int icb_mlp_gradients(int device, const float* params, uint64_t n, const float* x, const float* y,
+                      float* grad, double* loss);
+/* Load network parameters into the handle (ICB_COLLISION_IPM_MLP). */
+int icb_ipm_set_mlp(struct icb_handle* h, const float* params);
+
 /* ---- launch-shape tuning ----------------------------------------------- */
 typedef struct icb_tuning {
     int32_t block_size;        /* threads per block chosen */

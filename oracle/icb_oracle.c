@@ -366,8 +366,60 @@ static gas_consts gas_of(const orc_domain* d) {
     return g;
 }
 
+/* Interaction-potential table (collision 4): cos(chi) [nE][nb] over
+ * ln E = lnEmin + k / inv_dlnE, b = b_max j / (nb - 1); bilinear in
+ * (ln E, b) with E clamped, as the product samples it. */
+static const float* g_ipm_tab = NULL;
+static int g_ipm_nE = 0, g_ipm_nb = 0;
+static double g_ipm_lnEmin = 0.0, g_ipm_inv_dlnE = 0.0;
+
+void orc_set_ipm_table(const float* tab, int nE, int nb, double lnEmin, double inv_dlnE) {
+    g_ipm_tab = tab;
+    g_ipm_nE = nE;
+    g_ipm_nb = nb;
+    g_ipm_lnEmin = lnEmin;
+    g_ipm_inv_dlnE = inv_dlnE;
+}
+
+static double ipm_table_cos(double E, double bn) {
+    double t = (log(E) - g_ipm_lnEmin) * g_ipm_inv_dlnE;
+    t = fmin(fmax(t, 0.0), (double)(g_ipm_nE - 1));
+    int k = (int)t;
+    if (k > g_ipm_nE - 2) k = g_ipm_nE - 2;
+    const double ft = t - (double)k;
+    const double u = bn * (double)(g_ipm_nb - 1);
+    int j = (int)u;
+    if (j > g_ipm_nb - 2) j = g_ipm_nb - 2;
+    const double fu = u - (double)j;
+    const float* r0 = g_ipm_tab + (size_t)k * g_ipm_nb + j;
+    const float* r1 = r0 + g_ipm_nb;
+    const double c00 = r0[0], c01 = r0[1], c10 = r1[0], c11 = r1[1];
+    const double lo = c00 + fu * (c01 - c00);
+    const double hi = c10 + fu * (c11 - c10);
+    return lo + ft * (hi - lo);
+}
+
+/* Relative velocity g turned by chi about its own direction with azimuth
+ * (cp, sp): Bird, Molecular Gas Dynamics and the Direct Simulation of Gas
+ * Flows (1994), eq. 2.22. */
+static void deflect(const double g3[3], double g, double cx, double sx, double cp, double sp, double out[3]) {
+    const double gyz = sqrt(g3[1] * g3[1] + g3[2] * g3[2]);
+    if (gyz > 1e-6 * g) {
+        const double ig = 1.0 / gyz;
+        out[0] = g3[0] * cx + sx * sp * gyz;
+        out[1] = g3[1] * cx + sx * (g * g3[2] * cp - g3[0] * g3[1] * sp) * ig;
+        out[2] = g3[2] * cx - sx * (g * g3[1] * cp + g3[0] * g3[2] * sp) * ig;
+    } else {
+        out[0] = g3[0] * cx;
+        out[1] = g * sx * cp;
+        out[2] = g * sx * sp;
+    }
+}
+
+/* model: 0 hard sphere, 1 Langevin capture, 2 interaction-potential table */
 static int nullcoll_candidate(const gas_consts* G, double v[3], double mi, uint64_t seed, uint32_t id,
-                              uint32_t step, int skip, double* clk, double qstar, double b, int langevin) {
+                              uint32_t step, int skip, double* clk, double qstar, double b, int model) {
+    const int langevin = model == 1;
     const double* ug = G->ug;
     uint32_t r0[4], r1[4];
     philox_words(seed, id, step, 0u, r0);
@@ -398,6 +450,24 @@ static int nullcoll_candidate(const gas_consts* G, double v[3], double mi, uint6
     double q = G->A * (b + rad);
     double p = -expm1(-G->A * g);
     if (!langevin && !(u32_to_unit(r0[2]) * q < p)) return 1;
+    if (model == 2) {
+        const double mn = G->mn;
+        const double inv = 1.0 / (mi + mn);
+        const double fac = mn * inv;
+        const double mu = mi * mn * inv;
+        const double E = 0.5 * mu * (g * g);
+        const double bn = sqrt(u16_to_unit(r1[2] & 0xffffu));
+        const double cx = ipm_table_cos(E, bn);
+        const double sx = sqrt(fmax(0.0, 1.0 - cx * cx));
+        const double phi = 2.0 * M_PI * u16_to_unit(r1[3] >> 16);
+        double gp[3];
+        deflect(gv, g, cx, sx, cos(phi), sin(phi), gp);
+        for (int c = 0; c < 3; ++c) {
+            double vcom = (v[c] * mi + vn[c] * mn) * inv;
+            v[c] = vcom + gp[c] * fac;
+        }
+        return 2;
+    }
     const double ct2 = 2.0 * u16_to_unit(r1[2] & 0xffffu) - 1.0;
     const double st2 = sqrt(fmax(0.0, 1.0 - ct2 * ct2));
     const double ph2 = 2.0 * M_PI * u16_to_unit(r1[3] >> 16);
@@ -564,10 +634,11 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
             uint32_t* clk_next, uint32_t* clk_start,
             uint64_t first_id, uint64_t step0, double t0, int64_t n_steps,
             int64_t snap_every, int64_t ref_step, double* moments, uint64_t* counters, int n_threads) {
-    const int clocked = (collision == 2 || collision == 3);
+    const int clocked = (collision == 2 || collision == 3 || collision == 4);
     if (clocked && (!clk_S || !clk_U)) return 1;
     if (clocked && integrator == 0 && (!clk_next || !clk_start)) return 1;
-    if (collision == 3 && integrator != 0) return 1;
+    if ((collision == 3 || collision == 4) && integrator != 0) return 1;
+    if (collision == 4 && !g_ipm_tab) return 1;
     const gas_consts G = gas_of(d);
     const int64_t n_snap = (snap_every > 0) ? n_steps / snap_every : 0;
     if (n_snap > 0 && moments) memset(moments, 0, sizeof(double) * (size_t)(n_snap * ORC_N_MOMENTS));
@@ -599,6 +670,9 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
             if (collision == 3) {
                 Gi.A = 0.0;
                 Gi.Amean = -expm1(-langevin_lambda(d, q, m));   /* per-step probability */
+            } else if (collision == 4) {
+                Gi.A = d->gas_density_m3 * (M_PI * d->ipm_bmax_m * d->ipm_bmax_m) * d->dt_s;
+                Gi.Amean = Gi.A * Gi.mean_th;
             }
             if (skip) {
                 sk.tau = S;
@@ -635,7 +709,7 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                                 sk.tau = sk.tau - (double)(gs + 1u - sk.start) * sk.lam;
                             } else {
                                 int r = nullcoll_candidate(&Gi, v, m, seed, id, gs, 1, &sk.tau, sk.qstar, 0.0,
-                                                           collision == 3);
+                                                           collision == 3 ? 1 : (collision == 4 ? 2 : 0));
                                 if (r >= 1) ++cand_tot;
                                 if (r == 2) ++coll_tot;
                             }
@@ -694,3 +768,98 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
 
 /* Thermal width sqrt(kB T / m) (VelocitySampling.cpp:48-55). */
 double orc_thermal_width(double T, double m) { return sqrt(ORC_KB * T / m); }
+
+/* ---- interaction potential: classical deflection by trajectory ---------
+ * Restates the reference's offline IPM physics for one isotropic site at
+ * the origin: LJ 12-6 V = c12/r^12 - c6/r^6 (compute_vdw_force_and_potential,
+ * interaction_potential_precompute.cpp:1386-1420) plus the isotropic
+ * induced-dipole term -c4/r^4, c4 = 1/2 alpha' k q^2 (:1457-1508, :905/:929);
+ * velocity-Verlet with the adaptive step of integrate_trajectory (:1672-1796:
+ * dt <= eta sqrt(m r / |F|), halve when the per-step relative energy drift
+ * exceeds tol_high, grow by 1.1 after relax_steps steps under tol_low, stop
+ * outbound beyond r_cut once potential and force are negligible); the start
+ * point (b, 0, -(b + 50 A)) and the deflection cos(theta) = v0 . v_out / |v0|^2
+ * of deflection_weight_for_b (:1798-1835).  max_step_m > 0 is the tool's
+ * optional cap |v| dt <= max_step_m (TrajectoryConfig::max_step_m, :504,
+ * :1718-1724); without it the first step can jump over the interaction
+ * region at high energy.  Returns cos(chi), or NAN when the trajectory did
+ * not reach the asymptotic region within max_steps (200000, :503). */
+static void ipm_force(double c12, double c6, double c4, const double r[3], double f[3], double* pot) {
+    const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    const double rn = sqrt(r2);
+    const double ir = 1.0 / rn;
+    const double ir2 = ir * ir, ir4 = ir2 * ir2, ir6 = ir4 * ir2, ir12 = ir6 * ir6;
+    const double ir7 = ir6 * ir, ir13 = ir12 * ir, ir5 = ir4 * ir;
+    *pot = c12 * ir12 - c6 * ir6 - c4 * ir4;
+    const double dVdr = -12.0 * c12 * ir13 + 6.0 * c6 * ir7 + 4.0 * c4 * ir5;
+    const double scale = -dVdr * ir;
+    for (int a = 0; a < 3; ++a) f[a] = r[a] * scale;
+}
+
+double orc_ipm_cos_chi_trajectory(double c12, double c6, double c4, double m_red, double E, double b,
+                                  double max_step_m) {
+    const double eta = 0.02, tol_high = 1e-6, tol_low = 1e-8;
+    const int relax_steps = 100, max_steps = 200000;
+    const double margin = 50e-10;
+    const double r_cut = b + margin;
+    const double v_rel = sqrt(2.0 * E / m_red);
+    double r[3] = {b, 0.0, -(b + margin)}, v[3] = {0.0, 0.0, v_rel};
+    double f[3], pot;
+    ipm_force(c12, c6, c4, r, f, &pot);
+    const double inv_m = 1.0 / m_red;
+    double e_prev = 0.5 * m_red * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + pot;
+    const double kin0 = 0.5 * m_red * v_rel * v_rel;
+    const double e_floor = fmax(1e-30, kin0 * 1e-12);
+    double e_scale = fmax(e_floor, fmax(fabs(e_prev), kin0));
+    double dt = 0.0;
+    int good = 0, approached = 0;
+    for (int step = 0; step < max_steps; ++step) {
+        const double rn = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        const double fn = sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+        if (fn > 0.0 && rn > 0.0) {
+            const double dtf = eta * sqrt(m_red * rn / fn);
+            dt = (dt <= 0.0) ? dtf : fmin(dt, dtf);
+        }
+        if (max_step_m > 0.0) {
+            const double vn = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            if (vn > 1e-12) {
+                const double dts = max_step_m / vn;
+                dt = (dt <= 0.0) ? dts : fmin(dt, dts);
+            }
+        }
+        if (dt <= 0.0) dt = 1e-15;
+        double vh[3], rt[3], fnw[3], pn;
+        for (int a = 0; a < 3; ++a) {
+            vh[a] = v[a] + f[a] * (0.5 * dt * inv_m);
+            rt[a] = r[a] + vh[a] * dt;
+        }
+        ipm_force(c12, c6, c4, rt, fnw, &pn);
+        double vt[3];
+        for (int a = 0; a < 3; ++a) vt[a] = vh[a] + fnw[a] * (0.5 * dt * inv_m);
+        const double e_new = 0.5 * m_red * (vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]) + pn;
+        const double drift = fabs(e_new - e_prev) / e_scale;
+        if (drift > tol_high) {
+            dt *= 0.5;
+            continue;
+        }
+        for (int a = 0; a < 3; ++a) { r[a] = rt[a]; v[a] = vt[a]; f[a] = fnw[a]; }
+        pot = pn;
+        e_prev = e_new;
+        if (drift < tol_low) {
+            if (++good >= relax_steps) { dt *= 1.1; good = 0; }
+        } else {
+            good = 0;
+        }
+        const double kin = 0.5 * m_red * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        const double rn2 = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        const double fn2 = sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+        const double asym = fmax(e_floor, kin);
+        const double radial = r[0] * v[0] + r[1] * v[1] + r[2] * v[2];
+        if (radial < 0.0) approached = 1;
+        if (approached && radial > 0.0 && rn2 > r_cut && fabs(pot) / asym < 1e-6 && (fn2 * rn2) / asym < 1e-6) {
+            const double c = (v[2] * v_rel) / fmax(1e-12, v_rel * v_rel);
+            return fmax(-1.0, fmin(1.0, c));
+        }
+    }
+    return NAN;
+}

@@ -87,6 +87,9 @@ def lib() -> C.CDLL:
                               C.c_uint64, C.c_uint64, C.c_double, C.c_int64, C.c_int64, C.c_int64,
                               DP, U64P, C.c_int]
         L.orc_run.restype = C.c_int
+        L.orc_set_ipm_table.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_double, C.c_double]
+        L.orc_ipm_cos_chi_trajectory.argtypes = [C.c_double] * 7
+        L.orc_ipm_cos_chi_trajectory.restype = C.c_double
         _lib = L
     return _lib
 
@@ -97,6 +100,22 @@ def _dp(a):
 
 def _u32(a):
     return None if a is None else a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+_ipm_table_ref = None
+
+
+def set_ipm_table(tab: np.ndarray, n_E: int, n_b: int, ln_E_min: float, inv_dlnE: float) -> None:
+    """Interaction-potential table for collision model 4 (kept alive here)."""
+    global _ipm_table_ref
+    _ipm_table_ref = np.ascontiguousarray(tab, dtype=np.float32)
+    lib().orc_set_ipm_table(_ipm_table_ref.ctypes.data_as(C.POINTER(C.c_float)), n_E, n_b, ln_E_min, inv_dlnE)
+
+
+def ipm_cos_chi_trajectory(c12: float, c6: float, c4: float, m_red: float, E: float, b: float,
+                           max_step_m: float = 0.05e-10) -> float:
+    """cos(chi) from the restated reference trajectory integrator."""
+    return lib().orc_ipm_cos_chi_trajectory(c12, c6, c4, m_red, E, b, max_step_m)
 
 
 def mt64_uniforms(seed: int, n: int) -> np.ndarray:
@@ -122,14 +141,16 @@ def run(domain: dict, state: dict, n_steps: int, *, integrator: int = 0, collisi
     collision: 0 none, 1 reference HSS (mt19937_64 per ion), 2 null-collision
     HSS with Philox (``clock`` = (S, U, next, start) arrays from a previous
     call, or None to initialise; Boris uses the skip clock, RK4 the per-step
-    clock), 3 Langevin capture with Philox (Boris, skip clock)."""
+    clock), 3 Langevin capture with Philox (Boris, skip clock), 4
+    interaction-potential table collisions (Boris, skip clock; table from
+    set_ipm_table)."""
     d = domain_struct(domain)
     n = state["x"].shape[0]
     for k in ("t_death", "t_arrival"):
         if state.get(k) is None:
             state[k] = np.full(n, -1.0)
     S = U = nxt = start = None
-    if collision in (2, 3):
+    if collision in (2, 3, 4):
         if clock is None:
             S, U = np.zeros(n), np.zeros(n)
             nxt, start = np.zeros(n, dtype=np.uint32), np.zeros(n, dtype=np.uint32)

@@ -2,9 +2,11 @@
 the numpy oracle of both solvers, the reference's own two-ion GPU test, and
 a pushed two-ion system (momentum and energy).
 
-Tolerances: the isolated P3M field equals the oracle's to 1e-10 of the
-cloud's RMS field (FFT and summation-order rounding only); the reference
-periodic solver's float output to 1e-6 of its largest field."""
+Tolerances: the isolated P3M field equals the oracle's to 1e-6 of the
+cloud's RMS field (the particle-particle term is interpolated from a
+4,096-interval table of the long-range kernel, ~3e-8 relative; FFT and
+summation order add rounding only); the reference periodic solver's float
+output to 1e-6 of its largest field."""
 from __future__ import annotations
 
 import numpy as np
@@ -74,7 +76,7 @@ def test_isolated_p3m_matches_oracle():
         again = sim.space_charge_field()
     assert np.array_equal(got, again)                      # deterministic (no atomics)
     rms = np.sqrt(np.mean(np.sum(want ** 2, axis=0)))
-    assert np.max(np.abs(got - want)) <= 1e-10 * rms
+    assert np.max(np.abs(got - want)) <= 1e-6 * rms
     assert np.all(got[:, act == 0] == 0.0)
 
 
