@@ -505,6 +505,129 @@ def run_fticr(args) -> None:
     print(json.dumps(line))
 
 
+def run_ipm(args) -> None:
+    """Learned interaction-potential collisions: train the deflection network
+    on 2^20 quadrature samples, then advance 1,048,576 ions of 300 Da in N2
+    (three ensembles at 10, 40 and 80 Td) with the table and with the
+    network, reporting ion-steps/s of both and their K0."""
+    import torch
+
+    sys.path.insert(0, str(ROOT))
+    from icarion_b200 import _capi as capi
+    from icarion_b200 import config as cfg
+    from icarion_b200 import ipm, sweep
+    from icarion_b200.sim import Simulation, generate_ions
+
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local if world > 1 else 0)
+    dev = torch.cuda.current_device()
+    setup = ipm.IpmSetup()
+    t0 = time.perf_counter()
+    x, y, _, _ = ipm.training_set(setup, n=1 << 20, seed=2024, device=dev)
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    params, losses = ipm.train(x, y, epochs=20, batch=1024, lr=3e-3, seed=7, device=dev)
+    t_train = time.perf_counter() - t0
+    xv, yv, _, _ = ipm.training_set(setup, n=1 << 16, seed=99, device=dev)
+    val_rms = float(np.sqrt(np.mean((ipm.forward(params, xv, mode=1, device=dev) - yv) ** 2)))
+
+    en = (10.0, 40.0, 80.0)
+    n_total = N_IONS
+    counts = [n_total // 3 + (1 if k < n_total % 3 else 0) for k in range(3)]
+    m_ion = 300.0 * cfg.AMU_TO_KG
+    sigma_ev = math.pi * setup.b_max_m ** 2
+    ensembles, specs = [], []
+    for e_td, c in zip(en, counts):
+        nu = sweep.collision_frequency_max(e_td, m_ion, sigma_ev, cfg.GAS_MASS_KG["N2"], 300.0, 1000.0)
+        domain = {"instrument": "IMS", "geometry": {"origin_m": [0.0, 0.0, -0.01], "length_m": 0.1, "radius_m": 0.05},
+                  "env": {"temperature_K": 300.0, "pressure_Pa": 1000.0, "gas_species": "N2"},
+                  "fields": {"DC": {"EN_Td": e_td}}}
+        ensembles.append(cfg.ensemble_params(domain, 0.0, 0.1 / nu, ipm_bmax_m=setup.b_max_m))
+        specs.append(cfg.species_spec(c, m_ion, cfg.ELEM_CHARGE_C,
+                                      {"type": "gaussian", "center": [0, 0, 0], "std": [5e-4] * 3},
+                                      {"type": "thermal", "temperature_K": 300.0}))
+    st0 = generate_ions(123, specs)
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    results = {}
+    launches = 0
+    clocks = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)).split(",")[0]) if world == 1 else dev)
+    clocks.start()
+    for name, model in (("table", capi.COLLISION_IPM_TABLE), ("mlp", capi.COLLISION_IPM_MLP)):
+        sim = Simulation(ensembles, precision=capi.PREC_MIXED, collision=model, rng_seed=123, device=dev)
+        sim.set_stream(stream.cuda_stream)
+        sim.upload(st0, ens_offsets=offsets, first_id=rank * n_total)
+        sim.configure_ipm(setup)
+        if model == capi.COLLISION_IPM_MLP:
+            sim.set_mlp(params)
+        for _ in range(args.warmup):
+            sim.advance(STEPS_PER_BENCH_STEP)
+        sim.upload(st0, ens_offsets=offsets, first_id=rank * n_total)
+        sim.set_clock(0, np.zeros(3))
+        torch.cuda.synchronize()
+        ms, kms, nl, coll = 0.0, 0.0, 0, 0
+        for _ in range(args.steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            rs = sim.advance(STEPS_PER_BENCH_STEP)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms += a.elapsed_time(b)
+            kms += rs["step_kernel_ms"]
+            nl += rs["kernel_launches"]
+            coll += rs["collisions"]
+        launches += nl
+        mom = sim.moments()
+        _, tcl = sim.clock()
+        k0 = []
+        for e in range(3):
+            dz = mom[e][16] / mom[e][0]
+            v_d = dz / tcl[e]
+            n_gas = ensembles[e]["gas_density_m3"]
+            E = en[e] * 1e-21 * n_gas
+            k0.append(v_d / E * (n_gas / cfg.n0_loschmidt()) * 1e4)
+        results[name] = {"ion_steps_per_s": n_total * STEPS_PER_BENCH_STEP * args.steps / (ms * 1e-3),
+                         "ms_per_step": ms / args.steps, "K0_cm2_Vs": k0,
+                         "collision_fraction": coll / (n_total * STEPS_PER_BENCH_STEP * args.steps)}
+        sim.close()
+    clk = clocks.stop()
+    if rank != 0:
+        return
+    peaks = measured_peaks()
+    mlp = results["mlp"]
+    bpl = BYTES_PER_ION_LAUNCH["mixed"] * n_total
+    achieved = bpl / (mlp["ms_per_step"] * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": mlp["ion_steps_per_s"], "unit": "ion-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mlp["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (v, field, collisions) + bf16 MMA (network) + f64 (x, t)",
+        "data": "synthetic (reference ion-loader semantics, seed 123; training pairs seed 2024)",
+        "config": {"workload": "learned interaction-potential collisions: LJ 12-6 (5 meV, r_m 4 A) + C4 "
+                               "(N2 1.74 A^3) ion-N2 potential, 300 Da, 1,048,576 ions in three ensembles at "
+                               "10/40/80 Td, N2 300 K 1000 Pa, b_max 12 A, dt = 0.1/nu_max",
+                   "ions_per_gpu": n_total, "engine_steps_per_bench_step": STEPS_PER_BENCH_STEP,
+                   "table": results["table"], "mlp": mlp,
+                   "K0_shift_mlp_vs_table": [m / t - 1.0 for m, t in zip(mlp["K0_cm2_Vs"], results["table"]["K0_cm2_Vs"])],
+                   "training": {"samples": 1 << 20, "epochs": 20, "batch": 1024, "data_s": t_data,
+                                "train_s": t_train, "final_loss": float(losses[-1]),
+                                "validation_rms_cos_chi": val_rms},
+                   "l2": "flushed between timed steps"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"],
+                     "kernel": "k_step<mixed,boris,ipm-mlp,uniform> fused 1000 steps/launch",
+                     "note": "state crosses HBM once per 1000-step launch: issue bound, not HBM bound"},
+        "e2e": None,
+        "clocks": clk,
+        "cpu_baseline": None,
+        "cpu_baseline_note": "the reference's IPM handler needs its HDF5 offline tables (not buildable here)",
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -516,9 +639,10 @@ def main():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--pending", type=int, default=0)
     ap.add_argument("--spv", type=int, default=0, help="collision-free steps between warp votes")
-    ap.add_argument("--workload", choices=["ims-1M", "en-sweep", "fticr-sc"], default="ims-1M",
+    ap.add_argument("--workload", choices=["ims-1M", "en-sweep", "fticr-sc", "ipm"], default="ims-1M",
                     help="ims-1M: the 1,048,576-ion IMS run (default); en-sweep: the batched 64-ensemble E/N "
-                         "sweep; fticr-sc: the 262,144-ion FT-ICR cell with P3M space charge")
+                         "sweep; fticr-sc: the 262,144-ion FT-ICR cell with P3M space charge; ipm: learned "
+                         "interaction-potential collisions vs the table")
     ap.add_argument("--autotune", action="store_true", help="pick the launch shape with icb_autotune first")
     ap.add_argument("--graphs", action="store_true", help="replay icb_advance through CUDA graphs")
     ap.add_argument("--fp64-steps", type=int, default=10)
@@ -531,6 +655,8 @@ def main():
         run_reference_arm(args)
     elif args.workload == "fticr-sc":
         run_fticr(args)
+    elif args.workload == "ipm":
+        run_ipm(args)
     else:
         run_ours(args)
 
