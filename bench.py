@@ -51,9 +51,9 @@ WORKLOAD = "IMS drift, 1,048,576 ions (200 Da, +1, 150 A^2 HSS) in N2 300 K 1000
 # write x,y,z(24) v(12) tau,Q*(8) next,start(8) flags(1)                          = 53
 # (hi/lo: positions 6 floats = 24 B as well; FP64: v and the clock are doubles: 97 + 73)
 BYTES_PER_ION_LAUNCH = {"mixed": 130, "hilo": 130, "fp64": 170}
-# DRAM bytes of one fused mixed launch at 1,048,576 ions from the ncu capture
-# summarised in profiles/k_step_mixed_fused_ims_1M.md (dram__bytes_read.sum +
-# dram__bytes_write.sum; writes still in L2 at kernel end are not counted).
+# DRAM bytes of one fused mixed launch at 1,048,576 ions from an ncu capture
+# of that launch (dram__bytes_read.sum + dram__bytes_write.sum; writes still
+# in L2 at kernel end are not counted).
 NCU_TRAFFIC_PER_LAUNCH = {"mixed": 81.245952e6 + 8.287232e6}
 
 

@@ -104,8 +104,15 @@ def species_from_db_entry(sid: str, e: dict) -> Species:
 
 
 def ensemble_params(domain: dict, sigma_m2: float, dt_s: float, detector_z_m: float = 1e30,
-                    ipm_bmax_m: float = 0.0) -> dict:
-    """One ensemble (domain + env + ion cross-section + dt) as a plain dict."""
+                    ipm_bmax_m: float = 0.0, sigma_by_gas: dict | None = None) -> dict:
+    """One ensemble (domain + env + ion cross-section + dt) as a plain dict.
+
+    ``env.gas_mixture`` (a list of {species, mole_fraction[, cross_section_m2]})
+    becomes the HSS mixture: densities f_i P/(kB T) with the fractions
+    normalised as EnvironmentConfig::compute_derived_properties does
+    (EnvironmentConfig.h:155-170), cross-sections from the component's
+    override, else ``sigma_by_gas[species]``, else ``sigma_m2``
+    (HSSCollisionHandler.cpp:136-176)."""
     geom = domain.get("geometry", {})
     env = domain.get("env", domain.get("environment", {}))
     fields = domain.get("fields", {})
@@ -116,6 +123,20 @@ def ensemble_params(domain: dict, sigma_m2: float, dt_s: float, detector_z_m: fl
     P = float(env.get("pressure_Pa", 101325.0))
     gas = env.get("gas_species", "He")
     L = float(geom.get("length_m", 0.1))
+    mix = env.get("gas_mixture", []) or []
+    n_mix = len(mix) if len(mix) >= 2 else 0
+    if n_mix > 4:
+        raise ValueError("at most 4 gas mixture components")
+    dens, mass, sig = [0.0] * 4, [0.0] * 4, [0.0] * 4
+    if n_mix:
+        fsum = sum(float(c.get("mole_fraction", 0.0)) for c in mix)
+        norm = fsum if fsum > 0.0 else 1.0
+        n_tot = gas_density(P, T)
+        for i, c in enumerate(mix):
+            dens[i] = float(c.get("mole_fraction", 0.0)) / norm * n_tot
+            mass[i] = GAS_MASS_KG.get(c["species"], GAS_MASS_KG["He"])
+            override = float(c.get("cross_section_m2", -1.0))
+            sig[i] = override if override > 0.0 else float((sigma_by_gas or {}).get(c["species"], sigma_m2))
     axial = 0.0
     if "EN_Td" in dc:
         axial = axial_voltage_from_en(float(dc["EN_Td"]), P, T, L)
@@ -142,6 +163,11 @@ def ensemble_params(domain: dict, sigma_m2: float, dt_s: float, detector_z_m: fl
         "ipm_bmax_m": float(ipm_bmax_m),
         "dt_s": float(dt_s),
         "detector_z_m": float(detector_z_m),
+        "n_gas": n_mix,
+        "reserved_": 0,
+        "gas_mix_density_m3": dens,
+        "gas_mix_mass_kg": mass,
+        "gas_mix_sigma_m2": sig,
     }
 
 

@@ -299,6 +299,7 @@ struct icb_handle {
     double ipm_lnEmin = 0.0, ipm_inv_dlnE = 0.0, ipm_bmax = 0.0, ipm_Emin = 0.0, ipm_Emax = 0.0;
     DevBuf<uint32_t> mlp_w2;
     DevBuf<float> mlp_f;
+    DevBuf<MixConst> mix;              // HSS gas mixtures, per ensemble
     bool mlp_ready = false;
     // space charge (solved before every step when configured)
     SpaceChargeSolver* sc = nullptr;
@@ -350,6 +351,30 @@ double field_bound(const EnsConst& C, const icb_ensemble_params& P) {
 }
 
 // Per-ensemble constants exactly as the reference derives them.
+// HSS mixture constants of one ensemble (a single gas becomes n = 1).
+int build_mix(const icb_ensemble_params& P, MixConst& M) {
+    std::memset(&M, 0, sizeof(M));
+    const bool mixture = P.n_gas >= 2;
+    if (P.n_gas > kMaxGas) return fail(ICB_ERR_INVALID_ARGUMENT, "at most %d gas components", kMaxGas);
+    M.n = mixture ? P.n_gas : 1;
+    for (int i = 0; i < M.n; ++i) {
+        const double n = mixture ? P.gas_mix_density_m3[i] : P.gas_density_m3;
+        const double m = mixture ? P.gas_mix_mass_kg[i] : P.gas_mass_kg;
+        const double sg = mixture ? P.gas_mix_sigma_m2[i] : P.sigma_m2;
+        if (!(n >= 0.0) || !(m > 0.0) || !(sg > 0.0))
+            return fail(ICB_ERR_INVALID_ARGUMENT, "gas component %d needs density >= 0, mass > 0, sigma > 0", i);
+        M.A[i] = n * sg * P.dt_s;
+        M.sig_n[i] = std::sqrt(kBoltzmann * P.temperature_K / m);
+        M.mean_th[i] = M.sig_n[i] * kMeanChi3;
+        M.m[i] = m;
+        M.fA[i] = static_cast<float>(M.A[i]);
+        M.fsig_n[i] = static_cast<float>(M.sig_n[i]);
+        M.fmean_th[i] = static_cast<float>(M.mean_th[i]);
+        M.fm[i] = static_cast<float>(m);
+    }
+    return ICB_OK;
+}
+
 int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, bool& mag, int coll) {
     std::memset(&C, 0, sizeof(C));
     if (!(P.length_m > 0.0) || !(P.radius_m > 0.0)) return fail(ICB_ERR_INVALID_ARGUMENT, "ensemble geometry needs length_m > 0 and radius_m > 0");
@@ -410,6 +435,8 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
             if (!(P.ipm_bmax_m > 0.0))
                 return fail(ICB_ERR_INVALID_ARGUMENT, "interaction-potential collisions need ipm_bmax_m > 0");
             C.A = P.gas_density_m3 * (M_PI * P.ipm_bmax_m * P.ipm_bmax_m) * P.dt_s;
+        } else if (coll == kCollHSSMix && P.n_gas >= 2) {
+            C.A = 0.0;   // the mixture's totals are set below
         } else {
             if (!(P.sigma_m2 > 0.0)) return fail(ICB_ERR_INVALID_ARGUMENT, "collisions need sigma_m2 > 0");
             C.A = P.gas_density_m3 * P.sigma_m2 * P.dt_s;
@@ -423,6 +450,20 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
         C.fsig_n = static_cast<float>(C.sig_n);
         C.fm_gas = static_cast<float>(C.m_gas);
         for (int a = 0; a < 3; ++a) C.fug[a] = static_cast<float>(C.ug[a]);
+        if (coll == kCollHSSMix) {
+            // clock totals of the mixture: A = sum A_i, A <|th|> = sum A_i <|th_i|>
+            MixConst M;
+            if (int r = build_mix(P, M)) return r;
+            double A = 0.0, Am = 0.0;
+            for (int i = 0; i < M.n; ++i) {
+                A += M.A[i];
+                Am += M.A[i] * M.mean_th[i];
+            }
+            C.A = A;
+            C.mean_th = A > 0.0 ? Am / A : 0.0;
+            C.fA = static_cast<float>(C.A);
+            C.fmean_th = static_cast<float>(C.mean_th);
+        }
     }
     C.zdet = P.detector_z_m;
     C.Emax = field_bound(C, P);
@@ -465,6 +506,7 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.ipm_inv_dlnE = h->ipm_inv_dlnE;
         p.mlp_w2 = h->mlp_w2.p;
         p.mlp_f = h->mlp_f.p;
+        p.mix = h->mix.p;
         p.counters = h->counters.p;
         p.step_dev = h->step_dev.p;
         p.t_dev = h->t_dev.p;
@@ -628,7 +670,14 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
     int coll;
     switch (cfg->collision_model) {
         case ICB_COLLISION_NONE: coll = kCollNone; break;
-        case ICB_COLLISION_HSS: coll = kCollHSS; break;
+        case ICB_COLLISION_HSS: {
+            coll = kCollHSS;
+            for (int32_t e = 0; e < cfg->n_ensembles; ++e)
+                if (cfg->ensembles[e].n_gas >= 2) coll = kCollHSSMix;
+            if (coll == kCollHSSMix && cfg->integrator != ICB_INTEGRATOR_BORIS)
+                return fail(ICB_ERR_UNSUPPORTED, "HSS gas mixtures are built for the Boris pusher");
+            break;
+        }
         case ICB_COLLISION_IPM_TABLE:
         case ICB_COLLISION_IPM_MLP:
             if (cfg->integrator != ICB_INTEGRATOR_BORIS)
@@ -655,6 +704,12 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
     for (size_t e = 0; e < h->ens.size(); ++e) {
         int r = build_ens_const(h->ens[e], h->ens_const[e], h->field_kind, h->magnetic, coll);
         if (r != ICB_OK) return r;
+    }
+    std::vector<MixConst> mixes;
+    if (coll == kCollHSSMix) {
+        mixes.resize(h->ens.size());
+        for (size_t e = 0; e < h->ens.size(); ++e)
+            if (int r = build_mix(h->ens[e], mixes[e])) return r;
     }
     if (cfg->block_size > 0) {
         if (cfg->block_size % 32 != 0 || cfg->block_size > 128)
@@ -687,6 +742,10 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
     ICB_CUDA(cudaMemset(h->step_dev.p, 0, sizeof(unsigned long long)));
     ICB_CUDA(cudaMemset(h->counters.p, 0, kNumCounters * sizeof(unsigned long long)));
     ICB_CUDA(h->mom_out.alloc(h->ens.size() * ICB_N_MOMENTS));
+    if (!mixes.empty()) {
+        ICB_CUDA(h->mix.alloc(mixes.size()));
+        ICB_CUDA(cudaMemcpy(h->mix.p, mixes.data(), mixes.size() * sizeof(MixConst), cudaMemcpyHostToDevice));
+    }
     *out = h.release();
     return ICB_OK;
 }

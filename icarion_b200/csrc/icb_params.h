@@ -16,7 +16,7 @@ constexpr int kMaxLaunchEns = 64;   // ensembles per launch chunk (param space b
 constexpr uint32_t kMaxStepsPerLaunch = 16384;
 
 enum FieldKind : int { kFieldUniform = 0, kFieldLinear = 1, kFieldLinearRF = 2 };
-enum CollKind : int { kCollNone = 0, kCollHSS = 1, kCollLangevin = 2, kCollIPMTable = 3, kCollIPMMLP = 4 };
+enum CollKind : int { kCollNone = 0, kCollHSS = 1, kCollLangevin = 2, kCollIPMTable = 3, kCollIPMMLP = 4, kCollHSSMix = 5 };
 enum PrecKind : int { kPrecFP64 = 0, kPrecMixed = 1, kPrecHiLo = 2 };
 enum IntegKind : int { kBoris = 0, kRK4 = 1 };
 
@@ -60,6 +60,18 @@ struct EnsConst {
     float pad_;
 };
 
+// HSS gas mixture of one ensemble (read by the candidate step only):
+// A_i = n_i sigma_i dt, thermal widths and masses per component.  The
+// ensemble's EnsConst carries the totals (A = sum A_i, A mean_th =
+// sum A_i mean_th_i) for the collision clock.
+constexpr int kMaxGas = 4;
+struct MixConst {
+    int32_t n;
+    int32_t pad_;
+    double A[kMaxGas], mean_th[kMaxGas], sig_n[kMaxGas], m[kMaxGas];
+    float fA[kMaxGas], fmean_th[kMaxGas], fsig_n[kMaxGas], fm[kMaxGas];
+};
+
 // Ion-neutral interaction potential V = c12/r^12 - c6/r^6 - c4/r^4 (SI).
 struct IpmPotential {
     double c12, c6, c4, sigma;
@@ -99,6 +111,7 @@ struct StepParams {
     // biases (nullable unless the MLP model is selected)
     const uint32_t* mlp_w2;            // W2 as mma B fragments
     const float* mlp_f;                // W1 (128), b1 (64), b2 (64), W3 (64), b3 (1)
+    const MixConst* mix;               // per ensemble (global index), HSS mixtures
     unsigned long long* counters;      // kNumCounters
     const unsigned long long* step_dev;// engine step index at launch start
     const double* t_dev;               // engine time per ensemble at launch start

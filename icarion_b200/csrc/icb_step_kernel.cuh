@@ -581,6 +581,108 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
     return 2;
 }
 
+// Candidate of an HSS gas mixture (HSSCollisionHandler.cpp:105-249): the
+// reference draws a neutral of every component, collides with probability
+// 1 - exp(-K), K = sum_j n_j sigma_j |v - v_j| dt, and picks component i
+// with probability k_i / K.  Here the candidate (majorant Q = sum_i A_i
+// (b + <|th_i|>)) picks component i with probability A_i (b + <|th_i|>) / Q,
+// draws its neutral from the size-biased mixture as in the single-gas case,
+// draws the other components' neutrals from their Maxwellians (Philox
+// substreams 4 + j), and accepts with g_i (1 - exp(-K)) / (K (b + |th_i|)):
+// the joint law of (collision, component, v_n) per step is the reference's.
+template <class R, bool SKIP>
+__device__ __forceinline__ int candidate_mix(const EnsConst& C, const MixConst& M, R v[3], R& clk, R qstar,
+                                             R Amean, R b, double mi_d, const uint32_t* rk, uint32_t id,
+                                             uint32_t step) {
+    constexpr bool D = sizeof(R) == 8;
+    R ug[3], mi;
+    if constexpr (D) {
+        ug[0] = C.ug[0]; ug[1] = C.ug[1]; ug[2] = C.ug[2];
+        mi = mi_d;
+    } else {
+        ug[0] = C.fug[0]; ug[1] = C.fug[1]; ug[2] = C.fug[2];
+        mi = static_cast<float>(mi_d);
+    }
+    const int n = M.n;
+    auto Ai = [&](int i) -> R { if constexpr (D) return M.A[i]; else return M.fA[i]; };
+    auto Mi = [&](int i) -> R { if constexpr (D) return M.mean_th[i]; else return M.fmean_th[i]; };
+    auto Si = [&](int i) -> R { if constexpr (D) return M.sig_n[i]; else return M.fsig_n[i]; };
+    auto Gm = [&](int i) -> R { if constexpr (D) return M.m[i]; else return M.fm[i]; };
+    const U4 r0 = philox4x32_10_rk(id, step, 0u, 0u, rk);
+    R uc = u32(r0.y, R(0));
+    if constexpr (SKIP) {
+        clk = -m_log(u32(r0.x, R(0)));
+        const R wx = v[0] - ug[0], wy = v[1] - ug[1], wz = v[2] - ug[2];
+        b = m_sqrt(wx * wx + wy * wy + wz * wz);
+        const R A = D ? static_cast<R>(C.A) : static_cast<R>(C.fA);
+        const R Q = A * b + Amean;
+        if (!(uc * qstar < Q)) return 0;
+        uc = uc * qstar / Q;
+    } else {
+        clk = u32(r0.x, R(0));
+    }
+    // component choice
+    R qtot = R(0);
+    for (int i = 0; i < n; ++i) qtot += Ai(i) * (b + Mi(i));
+    const R target = uc * qtot;
+    int ci = n - 1;
+    R cum = R(0);
+    for (int i = 0; i < n - 1; ++i) {
+        const R qi = Ai(i) * (b + Mi(i));
+        if (target < cum + qi) { ci = i; break; }
+        cum += qi;
+    }
+    const R qsel = Ai(ci) * (b + Mi(ci));
+    const R uci = m_fmin((target - cum) / qsel, R(1));
+    const U4 r1 = philox4x32_10_rk(id, step, 1u, 0u, rk);
+    const bool thermal = uci * (b + Mi(ci)) < b;
+    R c3, s3;
+    angle_cs(u16(r1.y >> 16, R(0)), c3, s3);
+    const R sfac = thermal ? c3 * c3 : R(1);
+    const R r2 = R(-2.0) * (m_log(u32(r0.w, R(0))) + m_log(u32(r1.x, R(0))) * sfac);
+    const R rad = Si(ci) * m_sqrt(r2);
+    const R ct = R(2.0) * u16(r1.y & 0xffffu, R(0)) - R(1.0);
+    const R st = m_sqrt(m_fmax(R(0), R(1.0) - ct * ct));
+    R cp, sp;
+    angle_cs(u16(r1.z >> 16, R(0)), cp, sp);
+    const R vn[3] = {ug[0] + rad * (st * cp), ug[1] + rad * (st * sp), ug[2] + rad * ct};
+    const R gx = v[0] - vn[0], gy = v[1] - vn[1], gz = v[2] - vn[2];
+    const R g = m_sqrt(gx * gx + gy * gy + gz * gz);
+    R K = Ai(ci) * g;
+    for (int j = 0; j < n; ++j) {
+        if (j == ci) continue;
+        const U4 rj = philox4x32_10_rk(id, step, 4u + static_cast<uint32_t>(j), 0u, rk);
+        const R ra = m_sqrt(R(-2.0) * m_log(u32(rj.x, R(0))));
+        const R rb = m_sqrt(R(-2.0) * m_log(u32(rj.y, R(0))));
+        R ca, sa, cb2, sb2;
+        angle_cs(u16(rj.z >> 16, R(0)), ca, sa);
+        angle_cs(u16(rj.z & 0xffffu, R(0)), cb2, sb2);
+        const R s = Si(j);
+        const R hx = v[0] - (ug[0] + s * ra * ca);
+        const R hy = v[1] - (ug[1] + s * ra * sa);
+        const R hz = v[2] - (ug[2] + s * rb * cb2);
+        K += Ai(j) * m_sqrt(hx * hx + hy * hy + hz * hz);
+    }
+    const R pc = -m_expm1(-K);
+    if (!(u32(r0.z, R(0)) * K * (b + rad) < g * pc)) return 1;
+    const R mn = Gm(ci);
+    R inv_mt;
+    if constexpr (D) inv_mt = R(1) / (mi + mn);
+    else inv_mt = __frcp_rn(mi + mn);
+    const R fac = mn * inv_mt;
+    const R ct2 = R(2.0) * u16(r1.z & 0xffffu, R(0)) - R(1.0);
+    const R st2 = m_sqrt(m_fmax(R(0), R(1.0) - ct2 * ct2));
+    R cp2, sp2;
+    angle_cs(u16(r1.w >> 16, R(0)), cp2, sp2);
+    const R dir[3] = {st2 * cp2, st2 * sp2, ct2};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const R vcom = (v[c] * mi + vn[c] * mn) * inv_mt;
+        v[c] = vcom + (dir[c] * g) * fac;
+    }
+    return 2;
+}
+
 // ---- finalize ------------------------------------------------------------------
 // CylindricalGeometry::contains (CylindricalGeometry.h:35-40) on the global
 // position; false for positions outside or non-finite.
@@ -891,14 +993,22 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
                             // horizon end without an event: consume its steps
                             S = S - static_cast<R>(gs + 1u - g_start) * lam;
                         } else {
-                            const int st = candidate<R, true, COLL>(C, v, S, U, k.Amean, b, m, p.rk, id, gs, p, &ip);
+                            int st;
+                            if constexpr (COLL == kCollHSSMix)
+                                st = candidate_mix<R, true>(C, p.mix[p.ens_base + e], v, S, U, k.Amean, b, m, p.rk, id, gs);
+                            else
+                                st = candidate<R, true, COLL>(C, v, S, U, k.Amean, b, m, p.rk, id, gs, p, &ip);
                             if (st >= 1) ++n_cand;
                             if (st >= 2) ++n_coll;
                             need_net = st == 3;
                         }
                     } else {
                         ++n_cand;
-                        const int st = candidate<R, false, COLL>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs, p, &ip);
+                        int st;
+                        if constexpr (COLL == kCollHSSMix)
+                            st = candidate_mix<R, false>(C, p.mix[p.ens_base + e], v, U, R(0), k.Amean, b, m, p.rk, id, gs);
+                        else
+                            st = candidate<R, false, COLL>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs, p, &ip);
                         if (st >= 2) ++n_coll;
                         need_net = st == 3;
                     }

@@ -245,11 +245,14 @@ class Simulation:
         capi.check(self._lib.icb_autotune(self._h, trial_steps, C.byref(t)))
         return t.as_dict()
 
-    def run(self, n_steps: int, write_interval: int, ref_step: int = 0) -> tuple[np.ndarray, np.ndarray, dict]:
+    def run(self, n_steps: int, write_interval: int, ref_step: int = 0,
+            writer=None) -> tuple[np.ndarray, np.ndarray, dict]:
         """Advance n_steps, taking moments every write_interval steps (the
         engine's snapshot cadence).  Displacement moments are relative to the
-        positions after ref_step steps (a multiple of write_interval).
-        Returns (snapshot step indices, moments [snap, ens, 20], totals)."""
+        positions after ref_step steps (a multiple of write_interval).  With a
+        ``snapshots.TrajectoryWriter`` every snapshot's state is also written
+        (time of ensemble 0).  Returns (snapshot step indices, moments
+        [snap, ens, 20], totals)."""
         if ref_step % write_interval:
             raise ValueError("ref_step must be a multiple of write_interval")
         steps, moms = [], []
@@ -265,4 +268,6 @@ class Simulation:
                 self.mark_reference()
             steps.append(done)
             moms.append(self.moments())
+            if writer is not None:
+                writer.append(float(self.clock()[1][0]), self.download())
         return np.asarray(steps), np.stack(moms), tot

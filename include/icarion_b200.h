@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define ICB_ABI_VERSION 2
+#define ICB_ABI_VERSION 3
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -95,7 +95,17 @@ typedef struct icb_ensemble_params {
     double ipm_bmax_m;         /* IPM: event cross-section pi*b_max^2 */
     double dt_s;               /* uniform time step of this ensemble */
     double detector_z_m;       /* arrival plane (first crossing, global z) */
+    /* Gas mixture (env.gas_mixture, EnvironmentConfig.h:31-44, 155-205):
+     * n_gas = 2..ICB_MAX_GAS components replace gas_density_m3 /
+     * gas_mass_kg / sigma_m2 above for HSS collisions
+     * (HSSCollisionHandler.cpp:105-249); 0 or 1 = the single gas above. */
+    int32_t n_gas;
+    int32_t reserved_;
+    double gas_mix_density_m3[4];
+    double gas_mix_mass_kg[4];
+    double gas_mix_sigma_m2[4];
 } icb_ensemble_params;
+#define ICB_MAX_GAS 4
 
 typedef struct icb_config {
     int32_t precision;         /* ICB_PREC_* */

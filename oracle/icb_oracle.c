@@ -74,6 +74,11 @@ typedef struct orc_domain {
     double ipm_bmax_m;
     double dt_s;
     double detector_z_m;
+    int32_t n_gas;
+    int32_t reserved_;
+    double gas_mix_density_m3[4];
+    double gas_mix_mass_kg[4];
+    double gas_mix_sigma_m2[4];
 } orc_domain;
 
 /* ======================================================================
@@ -482,6 +487,84 @@ static int nullcoll_candidate(const gas_consts* G, double v[3], double mi, uint6
     return 2;
 }
 
+/* HSS gas mixture candidate (collision 5), the product's exact restatement
+ * of HSSCollisionHandler.cpp:105-249: component i chosen with probability
+ * A_i (b + <|th_i|>) / sum, its neutral from the size-biased mixture, the
+ * other components' neutrals Maxwellian from Philox substreams 4 + j, accept
+ * with g_i (1 - exp(-K)) / (K (b + |th_i|)), K = sum_j A_j |v - v_j|. */
+static int mix_candidate(const orc_domain* d, const gas_consts* G, double v[3], double mi, uint64_t seed,
+                         uint32_t id, uint32_t step, double* clk, double qstar) {
+    const int n = d->n_gas;
+    double A[4], mean[4], sig[4];
+    for (int i = 0; i < n; ++i) {
+        A[i] = d->gas_mix_density_m3[i] * d->gas_mix_sigma_m2[i] * d->dt_s;
+        sig[i] = sqrt(ORC_KB * d->temperature_K / d->gas_mix_mass_kg[i]);
+        mean[i] = sig[i] * 1.5957691216057308;
+    }
+    const double* ug = G->ug;
+    uint32_t r0[4], r1[4];
+    philox_words(seed, id, step, 0u, r0);
+    double uc = u32_to_unit(r0[1]);
+    *clk = -log(u32_to_unit(r0[0]));
+    double w[3] = {v[0] - ug[0], v[1] - ug[1], v[2] - ug[2]};
+    const double b = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    const double Q = G->A * b + G->Amean;
+    if (!(uc * qstar < Q)) return 0;
+    uc = uc * qstar / Q;
+    double qtot = 0.0;
+    for (int i = 0; i < n; ++i) qtot += A[i] * (b + mean[i]);
+    const double target = uc * qtot;
+    int ci = n - 1;
+    double cum = 0.0;
+    for (int i = 0; i < n - 1; ++i) {
+        const double qi = A[i] * (b + mean[i]);
+        if (target < cum + qi) { ci = i; break; }
+        cum += qi;
+    }
+    const double qsel = A[ci] * (b + mean[ci]);
+    const double uci = fmin((target - cum) / qsel, 1.0);
+    philox_words(seed, id, step, 1u, r1);
+    const int thermal = uci * (b + mean[ci]) < b;
+    const double c3 = cos(2.0 * M_PI * u16_to_unit(r1[1] >> 16));
+    const double sfac = thermal ? c3 * c3 : 1.0;
+    const double r2 = -2.0 * (log(u32_to_unit(r0[3])) + log(u32_to_unit(r1[0])) * sfac);
+    const double rad = sig[ci] * sqrt(r2);
+    const double ct = 2.0 * u16_to_unit(r1[1] & 0xffffu) - 1.0;
+    const double st = sqrt(fmax(0.0, 1.0 - ct * ct));
+    const double ph = 2.0 * M_PI * u16_to_unit(r1[2] >> 16);
+    double vn[3] = {ug[0] + rad * (st * cos(ph)), ug[1] + rad * (st * sin(ph)), ug[2] + rad * ct};
+    double gv[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
+    const double g = sqrt(gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2]);
+    double K = A[ci] * g;
+    for (int j = 0; j < n; ++j) {
+        if (j == ci) continue;
+        uint32_t rj[4];
+        philox_words(seed, id, step, 4u + (uint32_t)j, rj);
+        const double ra = sqrt(-2.0 * log(u32_to_unit(rj[0])));
+        const double rb = sqrt(-2.0 * log(u32_to_unit(rj[1])));
+        const double pa = 2.0 * M_PI * u16_to_unit(rj[2] >> 16);
+        const double pb = 2.0 * M_PI * u16_to_unit(rj[2] & 0xffffu);
+        const double hx = v[0] - (ug[0] + sig[j] * ra * cos(pa));
+        const double hy = v[1] - (ug[1] + sig[j] * ra * sin(pa));
+        const double hz = v[2] - (ug[2] + sig[j] * rb * cos(pb));
+        K += A[j] * sqrt(hx * hx + hy * hy + hz * hz);
+    }
+    const double pc = -expm1(-K);
+    if (!(u32_to_unit(r0[2]) * K * (b + rad) < g * pc)) return 1;
+    const double mn = d->gas_mix_mass_kg[ci];
+    const double inv = 1.0 / (mi + mn);
+    const double fac = mn * inv;
+    const double ct2 = 2.0 * u16_to_unit(r1[2] & 0xffffu) - 1.0;
+    const double st2 = sqrt(fmax(0.0, 1.0 - ct2 * ct2));
+    const double ph2 = 2.0 * M_PI * u16_to_unit(r1[3] >> 16);
+    double dir[3] = {st2 * cos(ph2), st2 * sin(ph2), ct2};
+    for (int c = 0; c < 3; ++c) {
+        double vcom = (v[c] * mi + vn[c] * mn) * inv;
+        v[c] = vcom + (dir[c] * g) * fac;
+    }
+    return 2;
+}
+
 /* Per-step clock (RK4). */
 static int hss_nullcoll(const orc_domain* d, double v[3], double mi, uint64_t seed, uint32_t id,
                         uint32_t step, double* S, double* U, uint64_t* overflow) {
@@ -634,10 +717,11 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
             uint32_t* clk_next, uint32_t* clk_start,
             uint64_t first_id, uint64_t step0, double t0, int64_t n_steps,
             int64_t snap_every, int64_t ref_step, double* moments, uint64_t* counters, int n_threads) {
-    const int clocked = (collision == 2 || collision == 3 || collision == 4);
+    const int clocked = (collision == 2 || collision == 3 || collision == 4 || collision == 5);
     if (clocked && (!clk_S || !clk_U)) return 1;
     if (clocked && integrator == 0 && (!clk_next || !clk_start)) return 1;
-    if ((collision == 3 || collision == 4) && integrator != 0) return 1;
+    if ((collision == 3 || collision == 4 || collision == 5) && integrator != 0) return 1;
+    if (collision == 5 && (d->n_gas < 2 || d->n_gas > 4)) return 1;
     if (collision == 4 && !g_ipm_tab) return 1;
     const gas_consts G = gas_of(d);
     const int64_t n_snap = (snap_every > 0) ? n_steps / snap_every : 0;
@@ -672,6 +756,16 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                 Gi.Amean = -expm1(-langevin_lambda(d, q, m));   /* per-step probability */
             } else if (collision == 4) {
                 Gi.A = d->gas_density_m3 * (M_PI * d->ipm_bmax_m * d->ipm_bmax_m) * d->dt_s;
+                Gi.Amean = Gi.A * Gi.mean_th;
+            } else if (collision == 5) {
+                double A = 0.0, Am = 0.0;
+                for (int g = 0; g < d->n_gas; ++g) {
+                    const double Ag = d->gas_mix_density_m3[g] * d->gas_mix_sigma_m2[g] * d->dt_s;
+                    A += Ag;
+                    Am += Ag * (sqrt(ORC_KB * d->temperature_K / d->gas_mix_mass_kg[g]) * 1.5957691216057308);
+                }
+                Gi.A = A;
+                Gi.mean_th = A > 0.0 ? Am / A : 0.0;
                 Gi.Amean = Gi.A * Gi.mean_th;
             }
             if (skip) {
@@ -708,8 +802,10 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                             if (sk.next & ORC_REFRESH) {
                                 sk.tau = sk.tau - (double)(gs + 1u - sk.start) * sk.lam;
                             } else {
-                                int r = nullcoll_candidate(&Gi, v, m, seed, id, gs, 1, &sk.tau, sk.qstar, 0.0,
-                                                           collision == 3 ? 1 : (collision == 4 ? 2 : 0));
+                                int r = (collision == 5)
+                                    ? mix_candidate(d, &Gi, v, m, seed, id, gs, &sk.tau, sk.qstar)
+                                    : nullcoll_candidate(&Gi, v, m, seed, id, gs, 1, &sk.tau, sk.qstar, 0.0,
+                                                         collision == 3 ? 1 : (collision == 4 ? 2 : 0));
                                 if (r >= 1) ++cand_tot;
                                 if (r == 2) ++coll_tot;
                             }

@@ -39,6 +39,8 @@ class Domain(C.Structure):
         ("temperature_K", C.c_double), ("gas_density_m3", C.c_double), ("gas_mass_kg", C.c_double),
         ("gas_velocity_m_s", D3), ("gas_polarizability_m3", C.c_double), ("sigma_m2", C.c_double),
         ("ipm_bmax_m", C.c_double), ("dt_s", C.c_double), ("detector_z_m", C.c_double),
+        ("n_gas", C.c_int32), ("reserved_", C.c_int32), ("gas_mix_density_m3", C.c_double * 4),
+        ("gas_mix_mass_kg", C.c_double * 4), ("gas_mix_sigma_m2", C.c_double * 4),
     ]
 
 
@@ -143,14 +145,14 @@ def run(domain: dict, state: dict, n_steps: int, *, integrator: int = 0, collisi
     call, or None to initialise; Boris uses the skip clock, RK4 the per-step
     clock), 3 Langevin capture with Philox (Boris, skip clock), 4
     interaction-potential table collisions (Boris, skip clock; table from
-    set_ipm_table)."""
+    set_ipm_table), 5 HSS gas mixture (Boris, skip clock)."""
     d = domain_struct(domain)
     n = state["x"].shape[0]
     for k in ("t_death", "t_arrival"):
         if state.get(k) is None:
             state[k] = np.full(n, -1.0)
     S = U = nxt = start = None
-    if collision in (2, 3, 4):
+    if collision in (2, 3, 4, 5):
         if clock is None:
             S, U = np.zeros(n), np.zeros(n)
             nxt, start = np.zeros(n, dtype=np.uint32), np.zeros(n, dtype=np.uint32)

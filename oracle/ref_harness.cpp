@@ -113,6 +113,21 @@ config::DomainConfig make_domain(const Args& a) {
     d.environment.temperature_K = num(a, "T", 300.0);
     d.environment.pressure_Pa = num(a, "P", 1000.0);
     d.environment.gas_species = str(a, "gas", "N2");
+    // gas mixture "species:fraction:sigma_m2,..." (EnvironmentConfig::gas_mixture)
+    const std::string mix = str(a, "mix", "");
+    size_t pos = 0;
+    while (pos < mix.size()) {
+        size_t end = mix.find(',', pos);
+        if (end == std::string::npos) end = mix.size();
+        const std::string item = mix.substr(pos, end - pos);
+        const size_t c1 = item.find(':'), c2 = item.find(':', c1 + 1);
+        config::GasMixtureComponent comp;
+        comp.species = item.substr(0, c1);
+        comp.mole_fraction = std::stod(item.substr(c1 + 1, c2 - c1 - 1));
+        comp.cross_section_m2 = std::stod(item.substr(c2 + 1));
+        d.environment.gas_mixture.push_back(comp);
+        pos = end + 1;
+    }
     d.environment.compute_derived_properties();
     if (a.count("EN_Td")) {
         const double EN_Td = num(a, "EN_Td", 0.0);

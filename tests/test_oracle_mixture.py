@@ -1,0 +1,53 @@
+"""HSS gas mixtures (CPU): the oracle's exact null-collision restatement of
+the reference's mixture law (HSSCollisionHandler.cpp:105-249) against the
+reference's own handler (compiled harness) on the same cloud: collision
+fraction within 1.5 %, drift and mean energy within 4 combined standard
+errors."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as orc
+from helpers import CONFIG0_DOMAIN, config0_ions, domain_json, oracle_state
+from icarion_b200 import config as cfg
+
+MIX = [("N2", 0.79, 150e-20), ("He", 0.21, 60e-20)]
+
+
+def _mix_ensemble():
+    dom = domain_json(CONFIG0_DOMAIN)
+    dom["env"]["gas_mixture"] = [{"species": s, "mole_fraction": f, "cross_section_m2": c} for s, f, c in MIX]
+    return cfg.ensemble_params(dom, 150e-20, 5e-10)
+
+
+def test_mixture_constants_follow_the_loader():
+    e = _mix_ensemble()
+    n = cfg.gas_density(1000.0, 300.0)
+    assert e["n_gas"] == 2
+    np.testing.assert_allclose(e["gas_mix_density_m3"][:2], [0.79 * n, 0.21 * n], rtol=1e-15)
+    assert e["gas_mix_mass_kg"][1] == cfg.GAS_MASS_KG["He"]
+    assert e["gas_mix_sigma_m2"][:2] == [150e-20, 60e-20]
+
+
+@pytest.mark.skipif(not orc.HARNESS.exists(), reason="compiled reference harness not built")
+def test_mixture_oracle_matches_reference_handler():
+    n, steps = 2048, 6000
+    st0 = config0_ions(n)
+    ref_state = oracle_state(st0)
+    ref_state["ccs"] = np.full(n, 150e-20)
+    mix = ",".join(f"{s}:{f}:{c!r}" for s, f, c in MIX)
+    rst, rstats, _ = orc.harness_run(ref_state, steps, dict(CONFIG0_DOMAIN, mix=mix), integrator="boris",
+                                     collision="hss", dt=5e-10, seed=11, threads=8)
+    ost = oracle_state(st0)
+    r = orc.run(_mix_ensemble(), ost, steps, integrator=0, collision=5, seed=11, threads=8)
+    f_ref = rstats["collisions"] / (n * steps)
+    f_me = r["collisions"] / (n * steps)
+    assert abs(f_me / f_ref - 1.0) < 0.015, (f_me, f_ref)
+    dz_ref, dz_me = rst["z"] - st0.z, ost["z"] - st0.z
+    se = np.hypot(dz_ref.std(), dz_me.std()) / np.sqrt(n)
+    assert abs(dz_me.mean() - dz_ref.mean()) <= 4 * se
+    ke_ref = (rst["vx"] ** 2 + rst["vy"] ** 2 + rst["vz"] ** 2)
+    ke_me = (ost["vx"] ** 2 + ost["vy"] ** 2 + ost["vz"] ** 2)
+    se_ke = np.hypot(ke_ref.std(), ke_me.std()) / np.sqrt(n)
+    assert abs(ke_me.mean() - ke_ref.mean()) <= 4 * se_ke
