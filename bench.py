@@ -251,8 +251,8 @@ def run_ours(args) -> None:
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def make_sim(prec, K=args.steps_per_launch):
-        s = Simulation(ensembles, precision=prec, integrator=capi.INTEGRATOR_BORIS, collision=capi.COLLISION_HSS,
+    def make_sim(prec, K=args.steps_per_launch, collision=capi.COLLISION_HSS):
+        s = Simulation(ensembles, precision=prec, integrator=capi.INTEGRATOR_BORIS, collision=collision,
                        rng_seed=123, device=dev, steps_per_launch=K, block_size=args.block,
                        pending_threshold=args.pending, steps_per_vote=args.spv, use_graphs=int(args.graphs))
         s.set_stream(stream.cuda_stream)
@@ -329,8 +329,23 @@ def run_ours(args) -> None:
         ms64, _, _, _, _ = timed_loop(s64, args.fp64_steps, STEPS_PER_BENCH_STEP, allreduce=False)
         ms64 = parallel.max_over_ranks(ms64)
         v64 = n_ions * STEPS_PER_BENCH_STEP * args.fp64_steps * world / (ms64 * 1e-3)
-        fp64_line = {"value": v64, "unit": "ion-steps/s", "steps": args.fp64_steps, "speedup_mixed_over_fp64": value / v64}
+        fp64_line = {"value": v64, "unit": "ion-steps/s", "steps": args.fp64_steps, "speedup_mixed_over_fp64": value / v64,
+                     "form": "the same null-collision algorithm in FP64 (skip clock, deferred collisions)"}
         s64.close()
+        # the plain FP64 form: the reference's per-step algorithm (a
+        # Maxwell-Boltzmann neutral and an exp test for every ion every step)
+        sp = make_sim(capi.PREC_FP64, collision=capi.COLLISION_HSS_PLAIN)
+        sp.advance(STEPS_PER_BENCH_STEP)
+        sp.upload(st0, ens_offsets=offsets, first_id=first_id)
+        torch.cuda.synchronize()
+        n_plain = max(1, min(args.fp64_steps, 3))
+        msp, _, _, _, _ = timed_loop(sp, n_plain, STEPS_PER_BENCH_STEP, allreduce=False)
+        msp = parallel.max_over_ranks(msp)
+        vp = n_ions * STEPS_PER_BENCH_STEP * n_plain * world / (msp * 1e-3)
+        fp64_line["plain_fp64_form"] = {"value": vp, "unit": "ion-steps/s", "steps": n_plain,
+                                        "speedup_mixed_over_plain_fp64": value / vp,
+                                        "form": "reference per-step HSS (MB neutral + exp test every step), FP64"}
+        sp.close()
 
     # end to end through the C ABI with host buffers: H2D state from pinned
     # memory, advance one snapshot interval, D2H state, every step

@@ -26,6 +26,7 @@ ICB_ERR_TIMEOUT = 7
 PREC_FP64, PREC_MIXED, PREC_MIXED_HILO = 0, 1, 2
 INTEGRATOR_BORIS, INTEGRATOR_RK4 = 0, 1
 COLLISION_NONE, COLLISION_HSS, COLLISION_IPM_TABLE, COLLISION_IPM_MLP, COLLISION_LANGEVIN = 0, 1, 2, 3, 4
+COLLISION_HSS_PLAIN = 5
 INSTRUMENT_IMS, INSTRUMENT_FTICR, INSTRUMENT_QUADRUPOLE_RF = 0, 1, 2
 SC_OFF, SC_P3M_ISOLATED, SC_PM_PERIODIC_REF = 0, 1, 2
 MLP_HIDDEN, MLP_N_PARAMS = 64, 4417

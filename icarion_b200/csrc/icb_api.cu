@@ -678,6 +678,11 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
                 return fail(ICB_ERR_UNSUPPORTED, "HSS gas mixtures are built for the Boris pusher");
             break;
         }
+        case ICB_COLLISION_HSS_PLAIN:
+            if (cfg->integrator != ICB_INTEGRATOR_BORIS || cfg->precision != ICB_PREC_FP64)
+                return fail(ICB_ERR_UNSUPPORTED, "the plain per-step HSS form is built for FP64 Boris");
+            coll = kCollHSSPlain;
+            break;
         case ICB_COLLISION_IPM_TABLE:
         case ICB_COLLISION_IPM_MLP:
             if (cfg->integrator != ICB_INTEGRATOR_BORIS)
@@ -1058,7 +1063,8 @@ int icb_spacecharge_configure(icb_handle* h, const icb_spacecharge_config* cfg) 
     if (h->hilo()) return fail(ICB_ERR_UNSUPPORTED, "space charge is built for the FP64 and mixed position forms");
     std::string err;
     SpaceChargeSolver* sc = nullptr;
-    int r = sc_create(*cfg, h->n, h->stream, &sc, err);
+    // the float forms run the particle-particle sums in float
+    int r = sc_create(*cfg, h->n, !h->fp64(), h->stream, &sc, err);
     if (r != ICB_OK) return fail(r, "space charge: %s", err.c_str());
     h->sc = sc;
     h->sc_emax_base = h->ens_const[0].Emax;

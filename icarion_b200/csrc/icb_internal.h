@@ -22,8 +22,8 @@ cudaError_t launch_step_hilo(int integ, int coll, int field, bool mag, const Ste
 // Space-charge solver (icb_p3m.cu).  Functions return ICB_* status codes
 // and put a message into `err` on failure.
 struct SpaceChargeSolver;
-int sc_create(const icb_spacecharge_config& cfg, uint64_t n_ions, cudaStream_t s, SpaceChargeSolver** out,
-              std::string& err);
+int sc_create(const icb_spacecharge_config& cfg, uint64_t n_ions, bool pp_float, cudaStream_t s,
+              SpaceChargeSolver** out, std::string& err);
 void sc_destroy(SpaceChargeSolver* sc);
 int sc_solve(SpaceChargeSolver* sc, const double* x, const double* y, const double* z, const double* q,
              const uint8_t* flags, uint64_t n, cudaStream_t s, std::string& err);

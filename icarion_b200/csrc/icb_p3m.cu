@@ -99,7 +99,7 @@ __global__ void k_sc_permute(MeshGeom g, const double* __restrict__ x, const dou
     const double4 v = make_double4(x[j], y[j], z[j], q[j]);
     ps[s] = v;
     pf[s] = make_float4(static_cast<float>(v.x - g.lo0), static_cast<float>(v.y - g.lo1),
-                        static_cast<float>(v.z - g.lo2), 0.f);
+                        static_cast<float>(v.z - g.lo2), static_cast<float>(v.w));
 }
 
 // CIC weight of corner (ox, oy, oz) of a cell for fractions fr (taken left
@@ -268,6 +268,9 @@ struct PPParams {
     float rc2_pre;           // float prefilter bound, slightly above rc^2
     double inv_dr;           // table intervals per metre
     const double* table;     // L(r) at r = k / inv_dr, k = 0..kPPTable
+    // float particle-particle arithmetic (the float forms): bounds in float
+    int use_float;
+    float rc2f, eps2f, min_d2f, inv_drf;
 };
 
 // Particle-particle table: L(r) = r^2 E_long(r) / k = erf(a r) - (2 a r /
@@ -285,8 +288,13 @@ __global__ void __launch_bounds__(256) k_sc_gather(MeshGeom g, PPParams pp, cons
                             const double* __restrict__ gy, const double* __restrict__ gz, double* __restrict__ ex,
                             double* __restrict__ ey, double* __restrict__ ez) {
     __shared__ double tab[REF_WEIGHTS ? 1 : kPPTable + 1];
+    float* tabf = reinterpret_cast<float*>(tab);
     if (!REF_WEIGHTS && pp.on) {
-        for (int k = threadIdx.x; k <= kPPTable; k += blockDim.x) tab[k] = pp.table[k];
+        if (pp.use_float) {
+            for (int k = threadIdx.x; k <= kPPTable; k += blockDim.x) tabf[k] = static_cast<float>(pp.table[k]);
+        } else {
+            for (int k = threadIdx.x; k <= kPPTable; k += blockDim.x) tab[k] = pp.table[k];
+        }
         __syncthreads();
     }
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -336,6 +344,35 @@ __global__ void __launch_bounds__(256) k_sc_gather(MeshGeom g, PPParams pp, cons
         const int x0 = max(ci - pp.r0, 0), x1 = min(ci + pp.r0, g.n0 - 2);
         const int y0 = max(cj - pp.r1, 0), y1 = min(cj + pp.r1, g.n1 - 2);
         const int z0 = max(ck - pp.r2, 0), z1 = min(ck + pp.r2, g.n2 - 2);
+        if (pp.use_float) {
+            // float arithmetic on positions relative to the mesh origin
+            float Ef[3] = {0.f, 0.f, 0.f};
+            const float kc = static_cast<float>(kCoulomb);
+            for (int cx = x0; cx <= x1; ++cx) {
+                for (int cy = y0; cy <= y1; ++cy) {
+                    const uint32_t row = (static_cast<uint32_t>(cx) * g.n1 + static_cast<uint32_t>(cy)) * g.n2;
+                    const uint32_t sa = start[row + static_cast<uint32_t>(z0)];
+                    const uint32_t sb = start[row + static_cast<uint32_t>(z1) + 1u];
+                    for (uint32_t s2 = sa; s2 < sb; ++s2) {
+                        const float4 qf = pf[s2];
+                        const float dx = fxi - qf.x, dy = fyi - qf.y, dz = fzi - qf.z;
+                        const float r2 = dx * dx + dy * dy + dz * dz;
+                        if (s2 == s || r2 >= pp.rc2f || r2 < pp.min_d2f) continue;
+                        const float r = sqrtf(r2);
+                        const float u = r * pp.inv_drf;
+                        const int kt = min(static_cast<int>(u), kPPTable - 1);
+                        const float fr = u - static_cast<float>(kt);
+                        const float L = fmaf(fr, tabf[kt + 1] - tabf[kt], tabf[kt]);
+                        const float sc = kc * (1.f / (r2 + pp.eps2f) - L / r2) / r * qf.w;
+                        Ef[0] += dx * sc;
+                        Ef[1] += dy * sc;
+                        Ef[2] += dz * sc;
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) E[c] += static_cast<double>(Ef[c]);
+        } else
         for (int cx = x0; cx <= x1; ++cx) {
             for (int cy = y0; cy <= y1; ++cy) {
                 const uint32_t row = (static_cast<uint32_t>(cx) * g.n1 + static_cast<uint32_t>(cy)) * g.n2;
@@ -440,8 +477,8 @@ struct SpaceChargeSolver {
         }                                                                                      \
     } while (0)
 
-int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, cudaStream_t s, SpaceChargeSolver** out,
-              std::string& err) {
+int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, bool pp_float, cudaStream_t s,
+              SpaceChargeSolver** out, std::string& err) {
     *out = nullptr;
     if (c.mode != ICB_SC_P3M_ISOLATED && c.mode != ICB_SC_PM_PERIODIC_REF) {
         err = "unknown space-charge mode";
@@ -501,6 +538,11 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, cudaStream_t s, 
         S.pp.eps2 = soft * soft;
         S.pp.min_d2 = std::max(soft * soft * 1e-4, 1e-30);
         S.pp.inv_dr = kPPTable / rc;
+        S.pp.use_float = pp_float ? 1 : 0;
+        S.pp.rc2f = static_cast<float>(rc * rc);
+        S.pp.eps2f = static_cast<float>(S.pp.eps2);
+        S.pp.min_d2f = static_cast<float>(S.pp.min_d2);
+        S.pp.inv_drf = static_cast<float>(S.pp.inv_dr);
         // float positions relative to the mesh origin carry an absolute error
         // below 1e-7 of the box; the margin keeps every pair under r_c
         S.pp.rc2_pre = static_cast<float>(rc * rc * 1.001 + 1e-6 * 3.0 * (c.box_max_m[0] - c.box_min_m[0]) * rc);

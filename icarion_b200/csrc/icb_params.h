@@ -16,7 +16,7 @@ constexpr int kMaxLaunchEns = 64;   // ensembles per launch chunk (param space b
 constexpr uint32_t kMaxStepsPerLaunch = 16384;
 
 enum FieldKind : int { kFieldUniform = 0, kFieldLinear = 1, kFieldLinearRF = 2 };
-enum CollKind : int { kCollNone = 0, kCollHSS = 1, kCollLangevin = 2, kCollIPMTable = 3, kCollIPMMLP = 4, kCollHSSMix = 5 };
+enum CollKind : int { kCollNone = 0, kCollHSS = 1, kCollLangevin = 2, kCollIPMTable = 3, kCollIPMMLP = 4, kCollHSSMix = 5, kCollHSSPlain = 6 };
 enum PrecKind : int { kPrecFP64 = 0, kPrecMixed = 1, kPrecHiLo = 2 };
 enum IntegKind : int { kBoris = 0, kRK4 = 1 };
 

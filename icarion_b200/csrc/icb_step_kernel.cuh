@@ -540,7 +540,7 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
     if (!LANG && !(u32(r0.z, R(0)) * q < pc)) return 1;
     if constexpr (COLL == kCollIPMMLP) {
         // deflection after the warp's network evaluation
-        const R mu = mi * mn * inv_mt;
+        const R mu = mi * fac;   // m_i m_n / (m_i + m_n); the product m_i m_n underflows in float
         ip->E = R(0.5) * mu * (g * g);
         ip->bn = m_sqrt(u16(r1.z & 0xffffu, R(0)));
         angle_cs(u16(r1.w >> 16, R(0)), ip->cp, ip->sp);
@@ -551,7 +551,7 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
     }
     if constexpr (COLL == kCollIPMTable) {
         // elastic deflection by chi(E, b): b uniform in area below b_max
-        const R mu = mi * mn * inv_mt;
+        const R mu = mi * fac;   // m_i m_n / (m_i + m_n); the product m_i m_n underflows in float
         const R E = R(0.5) * mu * (g * g);
         const R bn = m_sqrt(u16(r1.z & 0xffffu, R(0)));
         const R cx = ipm_table_cos<R>(p, E, bn);
@@ -683,6 +683,48 @@ __device__ __forceinline__ int candidate_mix(const EnsConst& C, const MixConst& 
     return 2;
 }
 
+// The reference's per-step HSS form (HSSCollisionHandler.cpp:331-376 with
+// VelocitySampling.cpp:9-66 and CollisionKernels.cpp:139-169), with Philox
+// in place of the per-ion mt19937_64: every step draws a Maxwell-Boltzmann
+// neutral (three Box-Muller cosine normals), collides with probability
+// 1 - exp(-n sigma |v - v_n| dt) and scatters isotropically in the centre of
+// mass.  This is the plain form the optimised null-collision kernels are
+// measured against; returns true on a collision.
+template <class R>
+__device__ __forceinline__ bool plain_hss(const EnsConst& C, R v[3], double mi_d, const uint32_t* rk, uint32_t id,
+                                          uint32_t step) {
+    const U4 a = philox4x32_10_rk(id, step, 0u, 0u, rk);
+    const U4 b = philox4x32_10_rk(id, step, 1u, 0u, rk);
+    const R sn = static_cast<R>(C.sig_n);
+    R vn[3];
+    const uint32_t w1[3] = {a.x, a.z, b.x}, w2[3] = {a.y, a.w, b.y};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        R cs, ss;
+        angle_cs(u32(w2[c], R(0)), cs, ss);
+        vn[c] = static_cast<R>(C.ug[c]) + sn * (m_sqrt(R(-2.0) * m_log(u32(w1[c], R(0)))) * cs);
+    }
+    const R gx = v[0] - vn[0], gy = v[1] - vn[1], gz = v[2] - vn[2];
+    const R g = m_sqrt(gx * gx + gy * gy + gz * gz);
+    const R P = -m_expm1(-static_cast<R>(C.A) * g);
+    if (!(u32(b.z, R(0)) < P)) return false;
+    const U4 c4 = philox4x32_10_rk(id, step, 2u, 0u, rk);
+    const R mi = static_cast<R>(mi_d), mn = static_cast<R>(C.m_gas);
+    const R inv = R(1) / (mi + mn);
+    const R fac = mn * inv;
+    const R ct = R(2.0) * u32(b.w, R(0)) - R(1.0);
+    const R st = m_sqrt(m_fmax(R(0), R(1.0) - ct * ct));
+    R cp, sp;
+    angle_cs(u32(c4.x, R(0)), cp, sp);
+    const R dir[3] = {st * cp, st * sp, ct};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const R vcom = (v[c] * mi + vn[c] * mn) * inv;
+        v[c] = vcom + (dir[c] * g) * fac;
+    }
+    return true;
+}
+
 // ---- finalize ------------------------------------------------------------------
 // CylindricalGeometry::contains (CylindricalGeometry.h:35-40) on the global
 // position; false for positions outside or non-finite.
@@ -708,13 +750,17 @@ __device__ __forceinline__ unsigned long long warp_sum_u32(uint32_t v) {
 // crossed) detector plane (lim).  The L1 length bounds the true path, so no
 // exit or crossing is missed; NaN or Inf makes acc non-finite and forces the
 // check.  Float accumulation error over <= kMaxStepsPerLaunch steps is < 0.1%.
-template <int PREC>
-struct KernelShape { static constexpr int kMinBlocks = 6; };
-template <>
-struct KernelShape<kPrecFP64> { static constexpr int kMinBlocks = 4; };
+// Resident blocks of 128 threads per SM the register budget is set for:
+// 6 for the float forms (80 registers), 4 for FP64 (128).  The learned
+// deflection measured fastest at 6 too (4 and 5 remove its spills but lose
+// more to occupancy).
+template <int PREC, int COLL>
+struct KernelShape {
+    static constexpr int kMinBlocks = PREC == kPrecFP64 ? 4 : 6;
+};
 
 template <int PREC, int INTEG, int COLL, int FIELD, bool MAG, bool FUSED>
-__global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(const __grid_constant__ StepParams p) {
+__global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_step(const __grid_constant__ StepParams p) {
     using R = typename PrecT<PREC>::R;
     using Pos = typename PosOf<PREC>::T;
     using Snap = typename Pos::Snap;
@@ -751,7 +797,7 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
         v[0] = static_cast<const R*>(p.vx)[i];
         v[1] = static_cast<const R*>(p.vy)[i];
         v[2] = static_cast<const R*>(p.vz)[i];
-        if (COLL != kCollNone) {
+        if (COLL != kCollNone && COLL != kCollHSSPlain) {
             S = static_cast<const R*>(p.clkS)[i];
             U = static_cast<const R*>(p.clkU)[i];
         }
@@ -804,7 +850,7 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
     // event) or, if that lies beyond the horizon of H steps, a refresh at the
     // horizon's last step; restarts happen at global step indices fixed by
     // the lane's own history, so results do not depend on launch shape.
-    constexpr bool kSkip = (INTEG == kBoris) && (COLL != kCollNone);
+    constexpr bool kSkip = (INTEG == kBoris) && (COLL != kCollNone) && (COLL != kCollHSSPlain);
     constexpr uint32_t kRefresh = 0x80000000u, kNeedRestart = 0xFFFFFFFFu;
     uint32_t g_next = kNeedRestart, g_start = 0u, nk = 0xFFFFFFFFu, H = 1u;
     R lam = R(0), dvmax = R(0), absu = R(0);
@@ -929,6 +975,11 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
         }
         if constexpr (kSkip) {
             if (do_coll) cand = (kk == nk);
+        } else if constexpr (COLL == kCollHSSPlain) {
+            if (do_coll) {
+                ++n_cand;
+                if (plain_hss<R>(C, v, m, p.rk, id, step0 + kk)) ++n_coll;
+            }
         } else if constexpr (COLL != kCollNone) {
             if (do_coll) cand = clock_tick<R>(k, v, S, U, b, cb, n_ovf);
         }
@@ -1063,7 +1114,7 @@ __global__ void __launch_bounds__(128, KernelShape<PREC>::kMinBlocks) k_step(con
         static_cast<R*>(p.vx)[i] = v[0];
         static_cast<R*>(p.vy)[i] = v[1];
         static_cast<R*>(p.vz)[i] = v[2];
-        if (COLL != kCollNone) {
+        if (COLL != kCollNone && COLL != kCollHSSPlain) {
             static_cast<R*>(p.clkS)[i] = S;
             static_cast<R*>(p.clkU)[i] = U;
         }

@@ -51,7 +51,11 @@ enum {
     ICB_COLLISION_HSS = 1,
     ICB_COLLISION_IPM_TABLE = 2,
     ICB_COLLISION_IPM_MLP = 3,
-    ICB_COLLISION_LANGEVIN = 4
+    ICB_COLLISION_LANGEVIN = 4,
+    /* the reference's per-step HSS form (a Maxwell-Boltzmann neutral and an
+     * exp test every step), FP64 + Boris only: the plain baseline the
+     * null-collision kernels are measured against */
+    ICB_COLLISION_HSS_PLAIN = 5
 };
 enum {
     ICB_INSTRUMENT_IMS = 0,          /* AnalyticalFieldModel.cpp:136-161 */

@@ -459,7 +459,7 @@ static int nullcoll_candidate(const gas_consts* G, double v[3], double mi, uint6
         const double mn = G->mn;
         const double inv = 1.0 / (mi + mn);
         const double fac = mn * inv;
-        const double mu = mi * mn * inv;
+        const double mu = mi * fac;
         const double E = 0.5 * mu * (g * g);
         const double bn = sqrt(u16_to_unit(r1[2] & 0xffffu));
         const double cx = ipm_table_cos(E, bn);
@@ -563,6 +563,38 @@ static int mix_candidate(const orc_domain* d, const gas_consts* G, double v[3], 
         v[c] = vcom + (dir[c] * g) * fac;
     }
     return 2;
+}
+
+/* The reference's per-step HSS form with Philox words (collision 6): three
+ * Box-Muller cosine normals for the neutral (VelocitySampling.cpp:9-66),
+ * P = 1 - exp(-n sigma g dt), isotropic COM scatter (CollisionKernels.cpp:
+ * 139-169).  Words: a = (u1, u2, u1', u2'), b = (u1'', u2'', accept, cos),
+ * c = (phi, -, -, -). */
+static int plain_hss(const gas_consts* G, double v[3], double mi, uint64_t seed, uint32_t id, uint32_t step) {
+    uint32_t a[4], b[4], c[4];
+    philox_words(seed, id, step, 0u, a);
+    philox_words(seed, id, step, 1u, b);
+    const uint32_t w1[3] = {a[0], a[2], b[0]}, w2[3] = {a[1], a[3], b[1]};
+    double vn[3];
+    for (int k = 0; k < 3; ++k)
+        vn[k] = G->ug[k] + G->sig_n * (sqrt(-2.0 * log(u32_to_unit(w1[k]))) * cos(2.0 * M_PI * u32_to_unit(w2[k])));
+    double gv[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
+    const double g = sqrt(gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2]);
+    const double P = -expm1(-G->A * g);
+    if (!(u32_to_unit(b[2]) < P)) return 0;
+    philox_words(seed, id, step, 2u, c);
+    const double mn = G->mn;
+    const double inv = 1.0 / (mi + mn);
+    const double fac = mn * inv;
+    const double ct = 2.0 * u32_to_unit(b[3]) - 1.0;
+    const double st = sqrt(fmax(0.0, 1.0 - ct * ct));
+    const double ph = 2.0 * M_PI * u32_to_unit(c[0]);
+    double dir[3] = {st * cos(ph), st * sin(ph), ct};
+    for (int k = 0; k < 3; ++k) {
+        double vcom = (v[k] * mi + vn[k] * mn) * inv;
+        v[k] = vcom + (dir[k] * g) * fac;
+    }
+    return 1;
 }
 
 /* Per-step clock (RK4). */
@@ -793,7 +825,10 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                     double zold = p[2];
                     if (integrator == 0) boris_step(d, p, v, m, q, t, dt);
                     else rk4_step(d, p, v, m, q, t, dt);
-                    if (collision == 1) {
+                    if (collision == 6) {
+                        ++cand_tot;
+                        coll_tot += (uint64_t)plain_hss(&G, v, m, seed, id, (uint32_t)(step0 + (uint64_t)k));
+                    } else if (collision == 1) {
                         coll_tot += (uint64_t)hss_reference(d, v, m, rng);
                     } else if (skip) {
                         const uint32_t gs = (uint32_t)(step0 + (uint64_t)k);

@@ -145,7 +145,8 @@ def run(domain: dict, state: dict, n_steps: int, *, integrator: int = 0, collisi
     call, or None to initialise; Boris uses the skip clock, RK4 the per-step
     clock), 3 Langevin capture with Philox (Boris, skip clock), 4
     interaction-potential table collisions (Boris, skip clock; table from
-    set_ipm_table), 5 HSS gas mixture (Boris, skip clock)."""
+    set_ipm_table), 5 HSS gas mixture (Boris, skip clock), 6 the reference's
+    per-step HSS form with Philox words (no clock)."""
     d = domain_struct(domain)
     n = state["x"].shape[0]
     for k in ("t_death", "t_arrival"):

@@ -132,7 +132,7 @@ def test_learned_deflection_drift_close_to_table():
     p, _ = ipm.train(x, y, epochs=20, batch=1024, lr=3e-3, seed=5)
     e = _ensemble(s)
     st0 = config0_ions(20000)
-    dz = {}
+    dz, finals = {}, {}
     for model in (capi.COLLISION_IPM_TABLE, capi.COLLISION_IPM_MLP):
         with Simulation([e], precision=capi.PREC_MIXED, collision=model, rng_seed=9) as sim:
             sim.upload(st0)
@@ -143,4 +143,27 @@ def test_learned_deflection_drift_close_to_table():
             out = sim.download()
             assert rs["collisions"] > 0
         dz[model] = float(np.mean(out.z - st0.z))
+        finals[model] = out
     assert abs(dz[capi.COLLISION_IPM_MLP] / dz[capi.COLLISION_IPM_TABLE] - 1.0) < 0.03, dz
+    # the network, not the table fallback, deflected the collisions
+    assert not np.array_equal(finals[capi.COLLISION_IPM_MLP].vz, finals[capi.COLLISION_IPM_TABLE].vz)
+
+
+def test_mixed_precision_table_collisions_track_fp64():
+    """Energies in the float path (E = mu g^2 / 2 with mu = m_i m_n / (m_i +
+    m_n) formed without underflow): drift and collision count of the mixed
+    form within 4 standard errors / 1 % of FP64."""
+    s = ipm.IpmSetup()
+    e = _ensemble(s)
+    st0 = config0_ions(20000)
+    res = {}
+    for prec in (capi.PREC_FP64, capi.PREC_MIXED):
+        with Simulation([e], precision=prec, collision=capi.COLLISION_IPM_TABLE, rng_seed=9) as sim:
+            sim.upload(st0)
+            sim.configure_ipm(s)
+            rs = sim.advance(3000)
+            res[prec] = (sim.download(), rs["collisions"])
+    dz64 = res[capi.PREC_FP64][0].z - st0.z
+    dzm = res[capi.PREC_MIXED][0].z - st0.z
+    assert abs(dzm.mean() - dz64.mean()) <= 4 * dz64.std() / np.sqrt(dz64.size)
+    assert abs(res[capi.PREC_MIXED][1] / res[capi.PREC_FP64][1] - 1.0) < 0.01
