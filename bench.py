@@ -471,8 +471,9 @@ def run_fticr(args) -> None:
     # (16 B x (M/2+1)/M) grids, plus per ion position/charge reads, keys and
     # the 8-node x 3-component gather
     M = 2 * cell.sc_grid[0]
-    real_b = 8.0 * M ** 3
-    cplx_b = 16.0 * M * M * (M // 2 + 1)
+    esz = 4.0 if prec_id == capi.PREC_MIXED else 8.0   # the float forms use a single-precision mesh
+    real_b = esz * M ** 3
+    cplx_b = 2 * esz * M * M * (M // 2 + 1)
     grid_bytes = real_b + (real_b + cplx_b) + 3 * (3 * cplx_b) + 3 * (cplx_b + real_b)
     ion_bytes = n * (33 + 32 + 24 + 192 + 24)
     p3m_bytes = grid_bytes + ion_bytes

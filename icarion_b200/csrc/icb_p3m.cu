@@ -112,9 +112,9 @@ __device__ __forceinline__ W cic_w(int ox, int oy, int oz, W fx, W fy, W fz) {
 
 // Charge per mesh node (C), written into the FFT grid (whose nodes outside
 // the mesh were zeroed before).  One thread per mesh node.
-template <bool REF_WEIGHTS>
+template <bool REF_WEIGHTS, class T>
 __global__ void k_sc_deposit(MeshGeom g, const double4* __restrict__ ps, const uint32_t* __restrict__ start,
-                             double* __restrict__ rho) {
+                             T* __restrict__ rho) {
     const size_t total = static_cast<size_t>(g.n0) * g.n1 * g.n2;
     const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= total) return;
@@ -149,22 +149,32 @@ __global__ void k_sc_deposit(MeshGeom g, const double4* __restrict__ ps, const u
             }
         }
     }
-    rho[(static_cast<size_t>(a) * g.m1 + static_cast<size_t>(b)) * g.m2 + static_cast<size_t>(c)] = acc;
+    rho[(static_cast<size_t>(a) * g.m1 + static_cast<size_t>(b)) * g.m2 + static_cast<size_t>(c)] = static_cast<T>(acc);
 }
 
 // out_c = a * b_c (complex) for the three field components, n entries each
-__global__ void k_sc_cmul3(const cufftDoubleComplex* __restrict__ a, const cufftDoubleComplex* __restrict__ b0,
-                           const cufftDoubleComplex* __restrict__ b1, const cufftDoubleComplex* __restrict__ b2,
-                           cufftDoubleComplex* __restrict__ out, size_t n) {
+template <class CT>
+__global__ void k_sc_cmul3(const CT* __restrict__ a, const CT* __restrict__ b0, const CT* __restrict__ b1,
+                           const CT* __restrict__ b2, CT* __restrict__ out, size_t n) {
     const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const cufftDoubleComplex u = a[i];
-    const cufftDoubleComplex* bs[3] = {b0, b1, b2};
+    const CT u = a[i];
+    const CT* bs[3] = {b0, b1, b2};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const cufftDoubleComplex v = bs[c][i];
-        out[c * n + i] = make_cuDoubleComplex(u.x * v.x - u.y * v.y, u.x * v.y + u.y * v.x);
+        const CT v = bs[c][i];
+        CT r;
+        r.x = u.x * v.x - u.y * v.y;
+        r.y = u.x * v.y + u.y * v.x;
+        out[c * n + i] = r;
     }
+}
+
+// Transformed kernel to single precision (the float forms' mesh).
+__global__ void k_sc_to_c32(const cufftDoubleComplex* __restrict__ in, cufftComplex* __restrict__ out, size_t n) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = make_cuComplex(static_cast<float>(in[i].x), static_cast<float>(in[i].y));
 }
 
 __device__ __forceinline__ double e_long(double r, double alpha) {
@@ -280,12 +290,12 @@ constexpr int kPPTable = 4096;
 
 // Field of every ion: CIC interpolation of the mesh field (+ particle-
 // particle correction).  Thread s handles the ion in sorted slot s.
-template <bool REF_WEIGHTS>
+template <bool REF_WEIGHTS, class GT>
 __global__ void __launch_bounds__(256) k_sc_gather(MeshGeom g, PPParams pp, const double4* __restrict__ ps,
                             const float4* __restrict__ pf,
                             const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                            const uint32_t* __restrict__ start, uint32_t n, const double* __restrict__ gx,
-                            const double* __restrict__ gy, const double* __restrict__ gz, double* __restrict__ ex,
+                            const uint32_t* __restrict__ start, uint32_t n, const GT* __restrict__ gx,
+                            const GT* __restrict__ gy, const GT* __restrict__ gz, double* __restrict__ ex,
                             double* __restrict__ ey, double* __restrict__ ez) {
     __shared__ double tab[REF_WEIGHTS ? 1 : kPPTable + 1];
     float* tabf = reinterpret_cast<float*>(tab);
@@ -315,7 +325,7 @@ __global__ void __launch_bounds__(256) k_sc_gather(MeshGeom g, PPParams pp, cons
     const double fy = (yi - g.lo1) * g.ih1 - cj;
     const double fz = (zi - g.lo2) * g.ih2 - ck;
     double E[3] = {0.0, 0.0, 0.0};
-    const double* grid[3] = {gx, gy, gz};
+    const GT* grid[3] = {gx, gy, gz};
     // corners in the reference's order w000, w100, w010, w110, w001, ... (x fastest)
     for (int oz = 0; oz < 2; ++oz) {
         for (int oy = 0; oy < 2; ++oy) {
@@ -330,7 +340,7 @@ __global__ void __launch_bounds__(256) k_sc_gather(MeshGeom g, PPParams pp, cons
                 const size_t node = (static_cast<size_t>(ci + ox) * g.m1 + static_cast<size_t>(cj + oy)) * g.m2 +
                                     static_cast<size_t>(ck + oz);
 #pragma unroll
-                for (int c = 0; c < 3; ++c) E[c] += w * grid[c][node];
+                for (int c = 0; c < 3; ++c) E[c] += w * static_cast<double>(grid[c][node]);
             }
         }
     }
@@ -439,6 +449,13 @@ struct SpaceChargeSolver {
     double* esc[3] = {nullptr, nullptr, nullptr};
     cufftHandle fwd = 0, inv = 0, inv3 = 0;
     bool have_fwd = false, have_inv = false, have_inv3 = false;
+    // single-precision mesh (isolated solver in the float forms)
+    bool f32 = false;
+    float* rho_f = nullptr;
+    cufftComplex* rho_hat_f = nullptr;
+    cufftComplex* tmp_hat_f = nullptr;
+    float* egrid_f = nullptr;             // three grids, one block
+    cufftComplex* ghat_f[3] = {nullptr, nullptr, nullptr};
     double max_field = 0.0;
 
     ~SpaceChargeSolver() {
@@ -451,6 +468,10 @@ struct SpaceChargeSolver {
                         static_cast<void*>(rho), static_cast<void*>(rho_hat), static_cast<void*>(tmp_hat)})
             if (p) cudaFree(p);
         if (egrid[0]) cudaFree(egrid[0]);   // one block holds the three grids
+        for (void* q : {static_cast<void*>(rho_f), static_cast<void*>(rho_hat_f), static_cast<void*>(tmp_hat_f),
+                        static_cast<void*>(egrid_f), static_cast<void*>(ghat_f[0]), static_cast<void*>(ghat_f[1]),
+                        static_cast<void*>(ghat_f[2])})
+            if (q) cudaFree(q);
         for (int c = 0; c < 3; ++c) {
             if (ghat[c]) cudaFree(ghat[c]);
             if (esc[c]) cudaFree(esc[c]);
@@ -569,33 +590,70 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, bool pp_float, c
     SC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, S.cub_bytes, S.keys, S.keys_sorted, S.vals, S.vals_sorted,
                                             static_cast<int>(S.cap), 0, S.key_bits, s));
     SC_CUDA(cudaMalloc(&S.cub_tmp, std::max<size_t>(S.cub_bytes, 16)));
+    const bool f32 = iso && pp_float;
+    S.f32 = f32;
+    for (int a = 0; a < 3; ++a) SC_CUDA(dev_alloc(&S.esc[a], S.cap));
+    // the double grid and forward plan serve the transformed field kernels
+    // (always built in FP64) and the FP64 per-step path
     SC_CUDA(dev_alloc(&S.rho, S.real_size()));
-    SC_CUDA(dev_alloc(&S.rho_hat, S.cplx_size()));
-    SC_CUDA(dev_alloc(&S.egrid[0], 3 * S.real_size()));
-    for (int a = 0; a < 3; ++a) {
-        S.egrid[a] = S.egrid[0] + a * S.real_size();
-        SC_CUDA(dev_alloc(&S.esc[a], S.cap));
-    }
     SC_FFT(cufftPlan3d(&S.fwd, g.m0, g.m1, g.m2, CUFFT_D2Z));
     S.have_fwd = true;
-    SC_FFT(cufftPlan3d(&S.inv, g.m0, g.m1, g.m2, CUFFT_Z2D));
-    S.have_inv = true;
     SC_FFT(cufftSetStream(S.fwd, s));
-    SC_FFT(cufftSetStream(S.inv, s));
+    if (!f32) {
+        SC_CUDA(dev_alloc(&S.rho_hat, S.cplx_size()));
+        SC_CUDA(dev_alloc(&S.egrid[0], 3 * S.real_size()));
+        for (int a = 0; a < 3; ++a) S.egrid[a] = S.egrid[0] + a * S.real_size();
+        SC_FFT(cufftPlan3d(&S.inv, g.m0, g.m1, g.m2, CUFFT_Z2D));
+        S.have_inv = true;
+        SC_FFT(cufftSetStream(S.inv, s));
+    }
     if (iso) {
-        // the three field components go through one batched inverse transform
         int dims[3] = {g.m0, g.m1, g.m2};
-        SC_FFT(cufftPlanMany(&S.inv3, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 3));
-        S.have_inv3 = true;
-        SC_FFT(cufftSetStream(S.inv3, s));
-        SC_CUDA(dev_alloc(&S.tmp_hat, 3 * S.cplx_size()));
+        cufftDoubleComplex* tmp = nullptr;
+        if (!f32) {
+            // the three field components go through one batched inverse transform
+            SC_FFT(cufftPlanMany(&S.inv3, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 3));
+            S.have_inv3 = true;
+            SC_FFT(cufftSetStream(S.inv3, s));
+            SC_CUDA(dev_alloc(&S.tmp_hat, 3 * S.cplx_size()));
+        } else {
+            SC_CUDA(dev_alloc(&tmp, S.cplx_size()));
+        }
         for (int a = 0; a < 3; ++a) {
-            SC_CUDA(dev_alloc(&S.ghat[a], S.cplx_size()));
+            cufftDoubleComplex* gh = tmp;
+            if (!f32) {
+                SC_CUDA(dev_alloc(&S.ghat[a], S.cplx_size()));
+                gh = S.ghat[a];
+            }
             k_sc_green<<<blocks_for(S.real_size(), 256), 256, 0, s>>>(g, S.h[0], S.h[1], S.h[2], S.pp.alpha, a, S.rho);
             SC_CUDA(cudaGetLastError());
-            SC_FFT(cufftExecD2Z(S.fwd, S.rho, S.ghat[a]));
-            k_sc_normalize<<<blocks_for(S.cplx_size(), 256), 256, 0, s>>>(g, S.ghat[a]);
+            SC_FFT(cufftExecD2Z(S.fwd, S.rho, gh));
+            k_sc_normalize<<<blocks_for(S.cplx_size(), 256), 256, 0, s>>>(g, gh);
             SC_CUDA(cudaGetLastError());
+            if (f32) {
+                SC_CUDA(dev_alloc(&S.ghat_f[a], S.cplx_size()));
+                k_sc_to_c32<<<blocks_for(S.cplx_size(), 256), 256, 0, s>>>(gh, S.ghat_f[a], S.cplx_size());
+                SC_CUDA(cudaGetLastError());
+            }
+        }
+        if (f32) {
+            // single-precision per-step mesh: R2C, products, batched C2R
+            SC_CUDA(cudaStreamSynchronize(s));
+            cudaFree(tmp);
+            cudaFree(S.rho);
+            S.rho = nullptr;
+            cufftDestroy(S.fwd);
+            S.have_fwd = false;
+            SC_CUDA(dev_alloc(&S.rho_f, S.real_size()));
+            SC_CUDA(dev_alloc(&S.rho_hat_f, S.cplx_size()));
+            SC_CUDA(dev_alloc(&S.tmp_hat_f, 3 * S.cplx_size()));
+            SC_CUDA(dev_alloc(&S.egrid_f, 3 * S.real_size()));
+            SC_FFT(cufftPlan3d(&S.fwd, g.m0, g.m1, g.m2, CUFFT_R2C));
+            S.have_fwd = true;
+            SC_FFT(cufftSetStream(S.fwd, s));
+            SC_FFT(cufftPlanMany(&S.inv3, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, 3));
+            S.have_inv3 = true;
+            SC_FFT(cufftSetStream(S.inv3, s));
         }
     }
     SC_CUDA(cudaStreamSynchronize(s));
@@ -615,7 +673,7 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
     const bool iso = S->mode == ICB_SC_P3M_ISOLATED;
     const uint32_t nn = static_cast<uint32_t>(n);
     SC_FFT(cufftSetStream(S->fwd, s));
-    SC_FFT(cufftSetStream(S->inv, s));
+    if (S->have_inv) SC_FFT(cufftSetStream(S->inv, s));
     if (S->have_inv3) SC_FFT(cufftSetStream(S->inv3, s));
     k_sc_bin<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, flags, nn, iso ? 0 : 1, S->keys, S->vals);
     SC_CUDA(cudaGetLastError());
@@ -628,21 +686,35 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
     k_sc_permute<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, q, S->vals_sorted, nn, S->ps, S->pf);
     SC_CUDA(cudaGetLastError());
     const size_t mesh_nodes = static_cast<size_t>(g.n0) * g.n1 * g.n2;
-    if (iso) {
+    if (iso && S->f32) {
+        SC_CUDA(cudaMemsetAsync(S->rho_f, 0, S->real_size() * sizeof(float), s));
+        k_sc_deposit<false, float><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho_f);
+        SC_CUDA(cudaGetLastError());
+        SC_FFT(cufftExecR2C(S->fwd, S->rho_f, S->rho_hat_f));
+        k_sc_cmul3<cufftComplex><<<blocks_for(S->cplx_size(), 256), 256, 0, s>>>(
+            S->rho_hat_f, S->ghat_f[0], S->ghat_f[1], S->ghat_f[2], S->tmp_hat_f, S->cplx_size());
+        SC_CUDA(cudaGetLastError());
+        SC_FFT(cufftExecC2R(S->inv3, S->tmp_hat_f, S->egrid_f));
+        const size_t rs = S->real_size();
+        k_sc_gather<false, float><<<blocks_for(nn, 256), 256, 0, s>>>(
+            g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted, S->start, nn, S->egrid_f, S->egrid_f + rs,
+            S->egrid_f + 2 * rs, S->esc[0], S->esc[1], S->esc[2]);
+        SC_CUDA(cudaGetLastError());
+    } else if (iso) {
         SC_CUDA(cudaMemsetAsync(S->rho, 0, S->real_size() * sizeof(double), s));
-        k_sc_deposit<false><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho);
+        k_sc_deposit<false, double><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho);
         SC_CUDA(cudaGetLastError());
         SC_FFT(cufftExecD2Z(S->fwd, S->rho, S->rho_hat));
-        k_sc_cmul3<<<blocks_for(S->cplx_size(), 256), 256, 0, s>>>(S->rho_hat, S->ghat[0], S->ghat[1], S->ghat[2],
+        k_sc_cmul3<cufftDoubleComplex><<<blocks_for(S->cplx_size(), 256), 256, 0, s>>>(S->rho_hat, S->ghat[0], S->ghat[1], S->ghat[2],
                                                                     S->tmp_hat, S->cplx_size());
         SC_CUDA(cudaGetLastError());
         SC_FFT(cufftExecZ2D(S->inv3, S->tmp_hat, S->egrid[0]));
-        k_sc_gather<false><<<blocks_for(nn, 256), 256, 0, s>>>(g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted,
+        k_sc_gather<false, double><<<blocks_for(nn, 256), 256, 0, s>>>(g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted,
                                                                 S->start, nn, S->egrid[0], S->egrid[1], S->egrid[2],
                                                                 S->esc[0], S->esc[1], S->esc[2]);
         SC_CUDA(cudaGetLastError());
     } else {
-        k_sc_deposit<true><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho);
+        k_sc_deposit<true, double><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho);
         SC_CUDA(cudaGetLastError());
         SC_FFT(cufftExecD2Z(S->fwd, S->rho, S->rho_hat));
         k_sc_poisson_ref<<<blocks_for(S->cplx_size(), 256), 256, 0, s>>>(g, S->h[0], S->h[1], S->h[2], S->rho_hat);
@@ -653,7 +725,7 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
         k_sc_efield_ref<<<blocks_for(S->real_size(), 256), 256, 0, s>>>(g, S->h[0], S->h[1], S->h[2], scale, S->rho,
                                                                          S->egrid[0], S->egrid[1], S->egrid[2]);
         SC_CUDA(cudaGetLastError());
-        k_sc_gather<true><<<blocks_for(nn, 256), 256, 0, s>>>(g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted,
+        k_sc_gather<true, double><<<blocks_for(nn, 256), 256, 0, s>>>(g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted,
                                                                S->start, nn, S->egrid[0], S->egrid[1], S->egrid[2],
                                                                S->esc[0], S->esc[1], S->esc[2]);
         SC_CUDA(cudaGetLastError());

@@ -15,6 +15,8 @@ numpy restatements of the space-charge field on the batch step:
   (one-sided at the grid edges), CIC interpolation with float weights.
   Every ion deposits (the reference passes all ions, active or not); ions
   with a grid coordinate outside [0, n-1) are skipped and get E = 0.
+  Pinned against the reference's own GPU code
+  (``periodic_pm_field_reference_gpu``, run on a GPU).
 * ``p3m_field`` — the isolated-boundary P3M solver of this library:
   CIC charges on the mesh, convolved (zero-padded FFT, Hockney-Eastwood)
   with the sampled long-range Coulomb field of a Gaussian-screened charge,
@@ -82,6 +84,29 @@ def direct_field_reference(x, y, z, q, active, softening: float = DIRECT_SOFTENI
         write_state(ip, st)
         harness("direct", **{"in": ip, "out": op, "softening": repr(softening)})
         return np.fromfile(op, dtype=np.float64).reshape(3, n)
+
+
+REF_P3M = Path(__file__).resolve().parent / "_ref" / "ref_p3m"
+
+
+def periodic_pm_field_reference_gpu(x, y, z, q, lo, hi, n) -> np.ndarray:
+    """The reference's own GPU solver (GPUSpaceChargeP3M, compiled from its
+    sources into _ref/ref_p3m by oracle/Makefile): [3, N] field."""
+    import subprocess
+    m = x.shape[0]
+    with tempfile.TemporaryDirectory() as td:
+        ip, op = Path(td) / "ions.bin", Path(td) / "field.bin"
+        with open(ip, "wb") as f:
+            f.write(np.int64(m).tobytes())
+            for a in (x, y, z, q):
+                f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+        args = [str(REF_P3M), f"in={ip}", f"out={op}", f"nx={n[0]}", f"ny={n[1]}", f"nz={n[2]}",
+                f"xmin={lo[0]!r}", f"ymin={lo[1]!r}", f"zmin={lo[2]!r}",
+                f"xmax={hi[0]!r}", f"ymax={hi[1]!r}", f"zmax={hi[2]!r}"]
+        r = subprocess.run(args, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_p3m failed ({r.returncode}): {r.stderr[-500:]}")
+        return np.fromfile(op, dtype=np.float64).reshape(3, m)
 
 
 # ---------------------------------------------------------------------------

@@ -96,6 +96,25 @@ def test_reference_periodic_solver_matches_oracle():
     assert np.max(np.abs(got - want)) <= 1e-6 * np.max(np.abs(want))
 
 
+@pytest.mark.skipif(not p3m.REF_P3M.exists(), reason="reference GPU solver not built (oracle/Makefile)")
+def test_periodic_solver_matches_reference_gpu_code():
+    """The library's ICB_SC_PM_PERIODIC_REF and the numpy restatement against
+    the reference's own GPUSpaceChargeP3M run on the same ions: within 1e-5
+    of the largest field (float weights and outputs on both sides; the
+    reference deposits with atomics, in no fixed order)."""
+    x, y, z, q = _cloud(2000, seed=2)
+    n = (32, 24, 20)
+    lo, hi = [-5e-3, -4e-3, -3.5e-3], [5e-3, 4e-3, 3.5e-3]
+    ref = p3m.periodic_pm_field_reference_gpu(x, y, z, q, lo, hi, n)
+    want = p3m.periodic_pm_field(x, y, z, q, lo, hi, n)
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(want - ref)) <= 1e-5 * scale
+    with _sim(_state(x, y, z, q, np.zeros(2000, dtype=np.uint8))) as sim:
+        sim.configure_space_charge(capi.SC_PM_PERIODIC_REF, n, lo, hi, field_bound=1.0)
+        got = sim.space_charge_field()
+    assert np.max(np.abs(got - ref)) <= 1e-5 * scale
+
+
 @pytest.mark.parametrize("mode,tol", [(capi.SC_PM_PERIODIC_REF, 0.25), (capi.SC_P3M_ISOLATED, 2e-3)])
 def test_two_ion_coulomb_case(mode, tol):
     """tests/gpu/test_gpu_space_charge.cpp:76-139 (the reference's bound is 25 %)."""
