@@ -151,6 +151,7 @@ SIGNATURES = {
     "icb_update_state": (C.c_int, [_H, _DP, _DP, _DP, _DP, _DP, _DP, _U8P]),
     "icb_ion_count": (C.c_uint64, [_H]),
     "icb_advance": (C.c_int, [_H, C.c_uint64, _P(RunStats)]),
+    "icb_advance_host": (C.c_int, [_H, C.c_uint64, C.c_int, _DP, _DP, _DP, _DP, _DP, _DP, _U8P, _P(RunStats)]),
     "icb_push": (C.c_int, [_H]),
     "icb_collide": (C.c_int, [_H, _P(RunStats)]),
     "icb_finalize": (C.c_int, [_H, _P(RunStats)]),

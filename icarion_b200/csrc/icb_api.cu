@@ -301,6 +301,10 @@ struct icb_handle {
     DevBuf<float> mlp_f;
     DevBuf<MixConst> mix;              // HSS gas mixtures, per ensemble
     bool mlp_ready = false;
+    // host fast path: copy stream, per-chunk events, velocity staging (3n)
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> hev;
+    DevBuf<double> hstage;
     // space charge (solved before every step when configured)
     SpaceChargeSolver* sc = nullptr;
     double sc_emax_base = 0.0;         // ensemble 0's field bound without space charge
@@ -316,6 +320,8 @@ struct icb_handle {
         drop_graph();
         if (sc) sc_destroy(sc);
         for (cudaEvent_t e : sc_ev) cudaEventDestroy(e);
+        for (cudaEvent_t e : hev) cudaEventDestroy(e);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
         for (cudaEvent_t e : kev) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -472,7 +478,9 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
 
 inline unsigned grid_for(uint64_t n, int block) { return static_cast<unsigned>((n + block - 1) / block); }
 
-int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_finalize) {
+// Step kernels for ions [lo, hi) (all ions by default).
+int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_finalize, uint64_t lo = 0,
+                uint64_t hi = ~0ull) {
     const int n_ens = static_cast<int>(h->ens.size());
     if ((h->coll == kCollIPMTable || h->coll == kCollIPMMLP) && h->ipm_nE == 0)
         return fail(ICB_ERR_STATE, "interaction-potential collisions need icb_ipm_configure first");
@@ -480,8 +488,9 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         return fail(ICB_ERR_STATE, "the learned deflection needs icb_ipm_set_mlp first");
     for (int e0 = 0; e0 < n_ens; e0 += kMaxLaunchEns) {
         const int ne = std::min(kMaxLaunchEns, n_ens - e0);
-        const uint64_t b = h->ens_off[static_cast<size_t>(e0)];
-        const uint64_t en = h->ens_off[static_cast<size_t>(e0 + ne)];
+        auto clip = [&](uint64_t v) { return std::min(std::max(v, lo), hi); };
+        const uint64_t b = clip(h->ens_off[static_cast<size_t>(e0)]);
+        const uint64_t en = clip(h->ens_off[static_cast<size_t>(e0 + ne)]);
         if (en <= b) continue;
         StepParams p;
         std::memset(&p, 0, sizeof(p));
@@ -519,7 +528,7 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.ens_base = static_cast<uint32_t>(e0);
         p.n_ens = static_cast<uint32_t>(ne);
         p.do_push = do_push; p.do_collide = do_collide; p.do_finalize = do_finalize;
-        for (int e = 0; e <= ne; ++e) p.ens_off[e] = h->ens_off[static_cast<size_t>(e0 + e)];
+        for (int e = 0; e <= ne; ++e) p.ens_off[e] = clip(h->ens_off[static_cast<size_t>(e0 + e)]);
         for (int e = 0; e < ne; ++e) p.ens[e] = h->ens_const[static_cast<size_t>(e0 + e)];
         const dim3 grid(grid_for(en - b, h->block)), block(static_cast<unsigned>(h->block));
         cudaError_t err;
@@ -1241,6 +1250,97 @@ int icb_autotune(icb_handle* h, uint64_t trial_steps, icb_tuning* out) {
         out->trials = trials;
         out->ion_steps_per_s = static_cast<double>(h->n) * static_cast<double>(trial_steps) / (best_ms * 1e-3);
     }
+    return ICB_OK;
+}
+
+int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, double* y, double* z, double* vx,
+                     double* vy, double* vz, uint8_t* active, icb_run_stats* stats) {
+    if (int r = check_handle(h)) return r;
+    if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
+    if (!x || !y || !z || !vx || !vy || !vz || !active) return fail(ICB_ERR_INVALID_ARGUMENT, "null state array");
+    if (n_chunks < 1 || n_chunks > 64) return fail(ICB_ERR_INVALID_ARGUMENT, "n_chunks must be in [1, 64]");
+    if (n_steps == 0) return fail(ICB_ERR_INVALID_ARGUMENT, "n_steps must be > 0");
+    // the overlapped form needs one launch per chunk and independent ions
+    if (n_chunks == 1 || n_steps > h->K || h->sc || h->hilo() || h->cfg.use_graphs) {
+        if (int r = icb_update_state(h, x, y, z, vx, vy, vz, active)) return r;
+        if (int r = icb_advance(h, n_steps, stats)) return r;
+        return icb_download_ions(h, x, y, z, vx, vy, vz, active, nullptr, nullptr);
+    }
+    if (h->host_step + n_steps >= (1ull << 31))
+        return fail(ICB_ERR_INVALID_ARGUMENT, "runs are limited to 2^31 engine steps");
+    const uint64_t n = h->n;
+    const bool f64 = h->fp64();
+    if (!h->copy_stream) ICB_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    while (h->hev.size() < static_cast<size_t>(2 * n_chunks + 1)) {
+        cudaEvent_t e;
+        ICB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        h->hev.push_back(e);
+    }
+    if (!f64 && h->hstage.n < 3 * n) ICB_CUDA(h->hstage.alloc(3 * n));
+    cudaStream_t s = h->stream, cs = h->copy_stream;
+    double* pos[3] = {x, y, z};
+    double* vel[3] = {vx, vy, vz};
+    double* pd[3] = {h->x.p, h->y.p, h->z.p};
+    double* vd[3] = {h->vxd.p, h->vyd.p, h->vzd.p};
+    float* vf[3] = {h->vxf.p, h->vyf.p, h->vzf.p};
+    // chunk c = ions [lim[c], lim[c+1]), boundaries on 256-ion multiples
+    std::vector<uint64_t> lim(static_cast<size_t>(n_chunks) + 1);
+    for (int c = 0; c <= n_chunks; ++c)
+        lim[static_cast<size_t>(c)] = c == n_chunks ? n : std::min<uint64_t>(n, ((n * c / n_chunks) + 255) & ~255ull);
+    h->host_step += n_steps;
+    h->launches = 0;
+    h->sc_timed = 0;
+    ICB_CUDA(cudaMemsetAsync(h->counters.p, 0, kNumCounters * sizeof(unsigned long long), s));
+    ICB_CUDA(cudaEventRecord(h->ev0, s));
+    ICB_CUDA(cudaEventRecord(h->hev[2 * n_chunks], s));
+    ICB_CUDA(cudaStreamWaitEvent(cs, h->hev[2 * n_chunks], 0));   // earlier work on the state is done
+    // inputs of every chunk on the copy stream
+    for (int c = 0; c < n_chunks; ++c) {
+        const uint64_t a = lim[static_cast<size_t>(c)], cnt = lim[static_cast<size_t>(c) + 1] - a;
+        if (cnt == 0) continue;
+        for (int k = 0; k < 3; ++k) {
+            ICB_CUDA(cudaMemcpyAsync(pd[k] + a, pos[k] + a, cnt * sizeof(double), cudaMemcpyHostToDevice, cs));
+            double* dst = f64 ? vd[k] + a : h->hstage.p + k * n + a;
+            ICB_CUDA(cudaMemcpyAsync(dst, vel[k] + a, cnt * sizeof(double), cudaMemcpyHostToDevice, cs));
+        }
+        ICB_CUDA(cudaMemcpyAsync(h->active_stage.p + a, active + a, cnt, cudaMemcpyHostToDevice, cs));
+        ICB_CUDA(cudaEventRecord(h->hev[2 * c], cs));
+    }
+    // steps of chunk c overlap the copies of the others
+    for (int c = 0; c < n_chunks; ++c) {
+        const uint64_t a = lim[static_cast<size_t>(c)], b = lim[static_cast<size_t>(c) + 1], cnt = b - a;
+        if (cnt == 0) continue;
+        const unsigned g = grid_for(cnt, 256);
+        ICB_CUDA(cudaStreamWaitEvent(s, h->hev[2 * c], 0));
+        if (!f64)
+            for (int k = 0; k < 3; ++k) k_to_float<<<g, 256, 0, s>>>(h->hstage.p + k * n + a, vf[k] + a, cnt);
+        k_flags_update<<<g, 256, 0, s>>>(h->active_stage.p + a, h->flags.p + a, cnt);
+        ICB_CUDA(cudaGetLastError());
+        if (int r = launch_step(h, static_cast<uint32_t>(n_steps), 1, 1, 1, a, b)) return r;
+        if (!f64)
+            for (int k = 0; k < 3; ++k) k_from_float<<<g, 256, 0, s>>>(vf[k] + a, h->hstage.p + k * n + a, cnt);
+        k_flags_out<<<g, 256, 0, s>>>(h->flags.p + a, h->active_stage.p + a, cnt);
+        ICB_CUDA(cudaGetLastError());
+        h->launches += f64 ? 2 : 8;
+        ICB_CUDA(cudaEventRecord(h->hev[2 * c + 1], s));
+        ICB_CUDA(cudaStreamWaitEvent(cs, h->hev[2 * c + 1], 0));
+        for (int k = 0; k < 3; ++k) {
+            ICB_CUDA(cudaMemcpyAsync(pos[k] + a, pd[k] + a, cnt * sizeof(double), cudaMemcpyDeviceToHost, cs));
+            const double* src = f64 ? vd[k] + a : h->hstage.p + k * n + a;
+            ICB_CUDA(cudaMemcpyAsync(vel[k] + a, src, cnt * sizeof(double), cudaMemcpyDeviceToHost, cs));
+        }
+        ICB_CUDA(cudaMemcpyAsync(active + a, h->active_stage.p + a, cnt, cudaMemcpyDeviceToHost, cs));
+    }
+    const int ne = static_cast<int>(h->ens.size());
+    k_clock_advance<<<(ne + 127) / 128, 128, 0, s>>>(h->step_dev.p, h->t_dev.p, h->dt_dev.p, ne,
+                                                      static_cast<uint32_t>(n_steps));
+    ICB_CUDA(cudaGetLastError());
+    ++h->launches;
+    ICB_CUDA(cudaEventRecord(h->hev[2 * n_chunks], cs));
+    ICB_CUDA(cudaStreamWaitEvent(s, h->hev[2 * n_chunks], 0));    // the stream sees the copies done
+    ICB_CUDA(cudaEventRecord(h->ev1, s));
+    if (stats) return read_stats(h, stats, n_steps, 0);
+    ICB_CUDA(cudaStreamSynchronize(s));
     return ICB_OK;
 }
 

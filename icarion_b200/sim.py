@@ -158,6 +158,16 @@ class Simulation:
         capi.check(self._lib.icb_advance(self._h, int(n_steps), C.byref(rs)))
         return rs.as_dict()
 
+    def advance_host(self, st: IonState, n_steps: int, n_chunks: int = 4) -> dict:
+        """Host state in, n_steps, host state out (positions, velocities and
+        active flags of ``st`` are read and overwritten), copies overlapped
+        with the steps of other ion chunks (icb_advance_host)."""
+        rs = capi.RunStats()
+        capi.check(self._lib.icb_advance_host(
+            self._h, int(n_steps), int(n_chunks), capi.dptr(st.x), capi.dptr(st.y), capi.dptr(st.z),
+            capi.dptr(st.vx), capi.dptr(st.vy), capi.dptr(st.vz), capi.u8ptr(st.active), C.byref(rs)))
+        return rs.as_dict()
+
     def advance_async(self, n_steps: int) -> None:
         capi.check(self._lib.icb_advance(self._h, int(n_steps), None))
 

@@ -217,6 +217,17 @@ uint64_t icb_ion_count(struct icb_handle* h);
 /* Fused uniform-dt batch step, n_steps times: push (Boris/RK4) -> collision
  * -> domain/NaN finalize -> t += dt (SimulationEngine.cpp:374-428). */
 int icb_advance(struct icb_handle* h, uint64_t n_steps, icb_run_stats* stats);
+/* The engine fast path with host state in one call: icb_update_state (the
+ * given positions, velocities and active flags) + icb_advance(n_steps) +
+ * icb_download_ions (same arrays), with the ions split into n_chunks whose
+ * host<->device copies overlap the steps of the other chunks (copy stream +
+ * events; host arrays should be pinned for the overlap).  The overlapped
+ * form needs n_steps <= steps_per_launch, no space charge, no CUDA graphs
+ * and the double-position forms; otherwise (and for n_chunks = 1) the three
+ * calls run in order.  Results equal the three separate calls bit for bit. */
+int icb_advance_host(struct icb_handle* h, uint64_t n_steps, int n_chunks,
+                     double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                     uint8_t* active, icb_run_stats* stats);
 /* Unfused parts of one step, for the per-step plug points:
  * icb_push   = IIntegrationStrategy::step_batch (push only, no finalize)
  * icb_collide = ICollisionHandler::handle_batch (collision only)

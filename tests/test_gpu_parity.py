@@ -257,6 +257,27 @@ def test_autotune_restores_state_and_keeps_fp64_results():
     assert c0[0] == c1[0] and np.array_equal(c0[1], c1[1])
 
 
+@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_MIXED])
+def test_advance_host_equals_separate_calls(precision):
+    """icb_advance_host with 4 overlapped ion chunks gives the state of
+    icb_update_state + icb_advance + icb_download_ions bit for bit."""
+    e = config0_ensemble()
+    st0 = config0_ions(5000)
+    outs = []
+    for chunks in (1, 4):
+        with Simulation([e], precision=precision, collision=capi.COLLISION_HSS, rng_seed=3,
+                        steps_per_launch=400) as sim:
+            sim.upload(st0)
+            host = st0.copy()
+            host.t_death = host.t_arrival = None
+            for _ in range(3):
+                rs = sim.advance_host(host, 400, n_chunks=chunks)
+            outs.append((host, sim.clock(), rs["collisions"]))
+    for k in KEYS + ("active",):
+        assert np.array_equal(getattr(outs[0][0], k), getattr(outs[1][0], k)), k
+    assert outs[0][1][0] == outs[1][1][0] == 1200 and outs[0][2] == outs[1][2]
+
+
 def test_unfused_plug_points_equal_fused_step():
     """push (step_batch) -> collide (handle_batch) -> finalize, one call each
     per step, gives the fused icb_advance result bit for bit (FP64)."""
