@@ -26,7 +26,7 @@ ICB_ERR_TIMEOUT = 7
 PREC_FP64, PREC_MIXED, PREC_MIXED_HILO = 0, 1, 2
 INTEGRATOR_BORIS, INTEGRATOR_RK4 = 0, 1
 COLLISION_NONE, COLLISION_HSS, COLLISION_IPM_TABLE, COLLISION_IPM_MLP, COLLISION_LANGEVIN = 0, 1, 2, 3, 4
-COLLISION_HSS_PLAIN = 5
+COLLISION_HSS_PLAIN, COLLISION_EHSS = 5, 6
 INSTRUMENT_IMS, INSTRUMENT_FTICR, INSTRUMENT_QUADRUPOLE_RF = 0, 1, 2
 SC_OFF, SC_P3M_ISOLATED, SC_PM_PERIODIC_REF = 0, 1, 2
 MLP_HIDDEN, MLP_N_PARAMS = 64, 4417
@@ -166,6 +166,7 @@ SIGNATURES = {
     "icb_ipm_configure": (C.c_int, [_H, _P(IpmConfig)]),
     "icb_ipm_table": (C.c_int, [_H, _FP]),
     "icb_ipm_set_mlp": (C.c_int, [_H, _FP]),
+    "icb_ehss_set_geometry": (C.c_int, [_H, C.c_int32, C.c_int32, _DP, _DP, C.c_double]),
     "icb_mlp_init": (C.c_int, [C.c_uint64, _FP]),
     "icb_mlp_train": (C.c_int, [C.c_int, _P(MlpTrainConfig), C.c_uint64, _FP, _FP, _FP, _DP]),
     "icb_mlp_forward": (C.c_int, [C.c_int, _FP, C.c_uint64, _FP, _FP, C.c_int]),

@@ -300,6 +300,12 @@ struct icb_handle {
     DevBuf<uint32_t> mlp_w2;
     DevBuf<float> mlp_f;
     DevBuf<MixConst> mix;              // HSS gas mixtures, per ensemble
+    // EHSS geometry: host copies per ensemble and the device arrays
+    std::vector<std::vector<double4>> ehss_host;
+    std::vector<double> ehss_rgas_host;
+    DevBuf<double4> ehss_atoms;
+    DevBuf<int32_t> ehss_off;
+    DevBuf<double> ehss_rgas;
     bool mlp_ready = false;
     // host fast path: copy stream, per-chunk events, velocity staging (3n)
     cudaStream_t copy_stream = nullptr;
@@ -486,6 +492,11 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         return fail(ICB_ERR_STATE, "interaction-potential collisions need icb_ipm_configure first");
     if (h->coll == kCollIPMMLP && !h->mlp_ready)
         return fail(ICB_ERR_STATE, "the learned deflection needs icb_ipm_set_mlp first");
+    if (h->coll == kCollEHSS) {
+        for (size_t e = 0; e < h->ens.size(); ++e)
+            if (e >= h->ehss_host.size() || h->ehss_host[e].empty())
+                return fail(ICB_ERR_STATE, "EHSS needs icb_ehss_set_geometry for ensemble %zu", e);
+    }
     for (int e0 = 0; e0 < n_ens; e0 += kMaxLaunchEns) {
         const int ne = std::min(kMaxLaunchEns, n_ens - e0);
         auto clip = [&](uint64_t v) { return std::min(std::max(v, lo), hi); };
@@ -516,6 +527,9 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.mlp_w2 = h->mlp_w2.p;
         p.mlp_f = h->mlp_f.p;
         p.mix = h->mix.p;
+        p.ehss_atoms = h->ehss_atoms.p;
+        p.ehss_off = h->ehss_off.p;
+        p.ehss_rgas = h->ehss_rgas.p;
         p.counters = h->counters.p;
         p.step_dev = h->step_dev.p;
         p.t_dev = h->t_dev.p;
@@ -687,6 +701,11 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
                 return fail(ICB_ERR_UNSUPPORTED, "HSS gas mixtures are built for the Boris pusher");
             break;
         }
+        case ICB_COLLISION_EHSS:
+            if (cfg->integrator != ICB_INTEGRATOR_BORIS)
+                return fail(ICB_ERR_UNSUPPORTED, "EHSS collisions are built for the Boris pusher");
+            coll = kCollEHSS;
+            break;
         case ICB_COLLISION_HSS_PLAIN:
             if (cfg->integrator != ICB_INTEGRATOR_BORIS || cfg->precision != ICB_PREC_FP64)
                 return fail(ICB_ERR_UNSUPPORTED, "the plain per-step HSS form is built for FP64 Boris");
@@ -1126,6 +1145,42 @@ int icb_ipm_configure(icb_handle* h, const icb_ipm_config* cfg) {
     h->ipm_bmax = cfg->b_max_m;
     h->ipm_Emin = cfg->E_min_J;
     h->ipm_Emax = cfg->E_max_J;
+    ++h->gen;
+    return ICB_OK;
+}
+
+int icb_ehss_set_geometry(icb_handle* h, int32_t ensemble, int32_t n_atoms, const double* centers_m,
+                          const double* radii_m, double gas_radius_m) {
+    if (int r = check_handle(h)) return r;
+    if (ensemble < 0 || static_cast<size_t>(ensemble) >= h->ens.size())
+        return fail(ICB_ERR_INVALID_ARGUMENT, "ensemble %d out of range", ensemble);
+    if (n_atoms < 1 || n_atoms > 100000 || !centers_m || !radii_m)
+        return fail(ICB_ERR_INVALID_ARGUMENT, "EHSS geometry needs 1..100000 atoms with centres and radii");
+    if (!(gas_radius_m >= 0.0)) return fail(ICB_ERR_INVALID_ARGUMENT, "gas_radius_m must be >= 0");
+    for (int32_t j = 0; j < n_atoms; ++j)
+        if (!(radii_m[j] > 0.0)) return fail(ICB_ERR_INVALID_ARGUMENT, "atom %d: radius must be > 0", j);
+    h->ehss_host.resize(h->ens.size());
+    h->ehss_rgas_host.resize(h->ens.size(), 0.0);
+    auto& atoms = h->ehss_host[static_cast<size_t>(ensemble)];
+    atoms.resize(static_cast<size_t>(n_atoms));
+    for (int32_t j = 0; j < n_atoms; ++j)
+        atoms[static_cast<size_t>(j)] = make_double4(centers_m[3 * j], centers_m[3 * j + 1], centers_m[3 * j + 2],
+                                                     radii_m[j]);
+    h->ehss_rgas_host[static_cast<size_t>(ensemble)] = gas_radius_m;
+    std::vector<double4> all;
+    std::vector<int32_t> off(1, 0);
+    for (const auto& v : h->ehss_host) {
+        all.insert(all.end(), v.begin(), v.end());
+        off.push_back(static_cast<int32_t>(all.size()));
+    }
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
+    ICB_CUDA(h->ehss_atoms.alloc(all.size()));
+    ICB_CUDA(h->ehss_off.alloc(off.size()));
+    ICB_CUDA(h->ehss_rgas.alloc(h->ehss_rgas_host.size()));
+    ICB_CUDA(cudaMemcpy(h->ehss_atoms.p, all.data(), all.size() * sizeof(double4), cudaMemcpyHostToDevice));
+    ICB_CUDA(cudaMemcpy(h->ehss_off.p, off.data(), off.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    ICB_CUDA(cudaMemcpy(h->ehss_rgas.p, h->ehss_rgas_host.data(), h->ehss_rgas_host.size() * sizeof(double),
+                        cudaMemcpyHostToDevice));
     ++h->gen;
     return ICB_OK;
 }

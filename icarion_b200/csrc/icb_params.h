@@ -16,7 +16,7 @@ constexpr int kMaxLaunchEns = 64;   // ensembles per launch chunk (param space b
 constexpr uint32_t kMaxStepsPerLaunch = 16384;
 
 enum FieldKind : int { kFieldUniform = 0, kFieldLinear = 1, kFieldLinearRF = 2 };
-enum CollKind : int { kCollNone = 0, kCollHSS = 1, kCollLangevin = 2, kCollIPMTable = 3, kCollIPMMLP = 4, kCollHSSMix = 5, kCollHSSPlain = 6 };
+enum CollKind : int { kCollNone = 0, kCollHSS = 1, kCollLangevin = 2, kCollIPMTable = 3, kCollIPMMLP = 4, kCollHSSMix = 5, kCollHSSPlain = 6, kCollEHSS = 7 };
 enum PrecKind : int { kPrecFP64 = 0, kPrecMixed = 1, kPrecHiLo = 2 };
 enum IntegKind : int { kBoris = 0, kRK4 = 1 };
 
@@ -112,6 +112,11 @@ struct StepParams {
     const uint32_t* mlp_w2;            // W2 as mma B fragments
     const float* mlp_f;                // W1 (128), b1 (64), b2 (64), W3 (64), b3 (1)
     const MixConst* mix;               // per ensemble (global index), HSS mixtures
+    // EHSS molecule geometry: atoms (x, y, z, radius) of ensemble e in
+    // [ehss_off[e], ehss_off[e+1]), gas (contact) radius per ensemble
+    const double4* ehss_atoms;
+    const int32_t* ehss_off;
+    const double* ehss_rgas;
     unsigned long long* counters;      // kNumCounters
     const unsigned long long* step_dev;// engine step index at launch start
     const double* t_dev;               // engine time per ensemble at launch start

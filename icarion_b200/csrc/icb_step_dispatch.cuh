@@ -42,6 +42,7 @@ cudaError_t dispatch_step(int integ, int coll, int field, bool mag, const StepPa
         if (coll == kCollIPMTable) return dispatch_field<PREC, kBoris, kCollIPMTable>(field, mag, p, g, b, s);
         if (coll == kCollIPMMLP) return dispatch_field<PREC, kBoris, kCollIPMMLP>(field, mag, p, g, b, s);
         if (coll == kCollHSSMix) return dispatch_field<PREC, kBoris, kCollHSSMix>(field, mag, p, g, b, s);
+        if (coll == kCollEHSS) return dispatch_field<PREC, kBoris, kCollEHSS>(field, mag, p, g, b, s);
         if constexpr (PREC == kPrecFP64) {
             if (coll == kCollHSSPlain) return dispatch_field<PREC, kBoris, kCollHSSPlain>(field, mag, p, g, b, s);
         }

@@ -51,6 +51,8 @@ __device__ __forceinline__ float m_expm1(float x) { return expm1f(x); }
 __device__ __forceinline__ double m_fmax(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ float m_fmax(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double m_fmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ double m_fabs(double a) { return fabs(a); }
+__device__ __forceinline__ float m_fabs(float a) { return fabsf(a); }
 __device__ __forceinline__ float m_fmin(float a, float b) { return fminf(a, b); }
 
 // Uniforms from Philox words.  FP64: (w + 1) 2^-32 in (0, 1] and, for a
@@ -489,10 +491,122 @@ __device__ __forceinline__ void ipm_apply(const EnsConst& C, R v[3], const IpmPe
     }
 }
 
+// EHSS scattering (CollisionKernels::ehss_collision, CollisionKernels.cpp:
+// 13-137, 220-381): a uniformly random orientation of the molecule
+// (Shoemake quaternion from three uniforms, CollisionGeometry.cpp:30-59) in
+// the frame of the collision axis g/|g|, the maximal impact parameter of the
+// rotated atoms plus the gas radius, impact points uniform in that disk
+// until the straight trajectory meets an atom (at most 256 draws; the disk
+// grows by 1.5 after 64), the earliest contact's normal, specular
+// reflection of g and the centre-of-mass transform.  No hit in 256 draws
+// leaves v unchanged, as in the reference.  Philox substreams: 2 for the
+// orientation, 8 + a/2 for draw a.
+template <class R>
+__device__ void ehss_scatter(const StepParams& p, uint32_t eg, R v[3], const R vn[3], const R g3[3], R g, R mi,
+                             R mn, R inv_mt, R fac, const uint32_t* rk, uint32_t id, uint32_t step) {
+    const int a0 = p.ehss_off[eg], a1 = p.ehss_off[eg + 1];
+    if (a1 <= a0 || !(g > R(0))) return;
+    const R rg = static_cast<R>(p.ehss_rgas[eg]);
+    const R ax[3] = {g3[0] / g, g3[1] / g, g3[2] / g};
+    // orthonormal basis of the impact plane (CollisionGeometry.cpp:11-28)
+    const R ea[3] = {m_fabs(ax[0]) < R(0.9) ? R(1) : R(0), m_fabs(ax[0]) < R(0.9) ? R(0) : R(1), R(0)};
+    R t1[3] = {ax[1] * ea[2] - ax[2] * ea[1], ax[2] * ea[0] - ax[0] * ea[2], ax[0] * ea[1] - ax[1] * ea[0]};
+    R nt = R(1) / m_sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+    t1[0] *= nt; t1[1] *= nt; t1[2] *= nt;
+    R t2[3] = {ax[1] * t1[2] - ax[2] * t1[1], ax[2] * t1[0] - ax[0] * t1[2], ax[0] * t1[1] - ax[1] * t1[0]};
+    nt = R(1) / m_sqrt(t2[0] * t2[0] + t2[1] * t2[1] + t2[2] * t2[2]);
+    t2[0] *= nt; t2[1] *= nt; t2[2] *= nt;
+    // random orientation, expressed in the collision-axis frame: Rm = B Q
+    const U4 ro = philox4x32_10_rk(id, step, 2u, 0u, rk);
+    const R u1 = u32(ro.x, R(0));
+    R s2, c2, s3, c3;
+    angle_cs(u32(ro.y, R(0)), c2, s2);
+    angle_cs(u32(ro.z, R(0)), c3, s3);
+    const R qa = m_sqrt(R(1) - u1), qb = m_sqrt(u1);
+    const R qx = qa * s2, qy = qa * c2, qz = qb * s3, qw = qb * c3;
+    const R Q[3][3] = {{R(1) - R(2) * (qy * qy + qz * qz), R(2) * (qx * qy - qz * qw), R(2) * (qx * qz + qy * qw)},
+                       {R(2) * (qx * qy + qz * qw), R(1) - R(2) * (qx * qx + qz * qz), R(2) * (qy * qz - qx * qw)},
+                       {R(2) * (qx * qz - qy * qw), R(2) * (qy * qz + qx * qw), R(1) - R(2) * (qx * qx + qy * qy)}};
+    const R B[3][3] = {{t1[0], t2[0], ax[0]}, {t1[1], t2[1], ax[1]}, {t1[2], t2[2], ax[2]}};
+    R Rm[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Rm[i][j] = B[i][0] * Q[0][j] + B[i][1] * Q[1][j] + B[i][2] * Q[2][j];
+    auto rot = [&](const double4& c, R out[3]) {
+        const R cx = static_cast<R>(c.x), cy = static_cast<R>(c.y), cz = static_cast<R>(c.z);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) out[i] = Rm[i][0] * cx + Rm[i][1] * cy + Rm[i][2] * cz;
+    };
+    R bmax = R(0);
+    for (int j = a0; j < a1; ++j) {
+        const double4 c = p.ehss_atoms[j];
+        R ra[3];
+        rot(c, ra);
+        const R sra = ax[0] * ra[0] + ax[1] * ra[1] + ax[2] * ra[2];
+        const R px = ra[0] - ax[0] * sra, py = ra[1] - ax[1] * sra, pz = ra[2] - ax[2] * sra;
+        const R cur = m_sqrt(px * px + py * py + pz * pz) + static_cast<R>(c.w);
+        if (cur > bmax) bmax = cur;
+    }
+    bmax += rg;
+    U4 w{};
+    for (int at = 0; at < 256; ++at) {
+        if ((at & 1) == 0) w = philox4x32_10_rk(id, step, 8u + static_cast<uint32_t>(at >> 1), 0u, rk);
+        const uint32_t wa = (at & 1) ? w.z : w.x, wb = (at & 1) ? w.w : w.y;
+        const R bb = bmax * m_sqrt(u32(wa, R(0)));
+        R cph, sph;
+        angle_cs(u32(wb, R(0)), cph, sph);
+        const R off[3] = {t1[0] * (bb * cph) + t2[0] * (bb * sph), t1[1] * (bb * cph) + t2[1] * (bb * sph),
+                          t1[2] * (bb * cph) + t2[2] * (bb * sph)};
+        bool hit = false;
+        R best = R(0), nrm[3] = {R(0), R(0), R(0)};
+        for (int j = a0; j < a1; ++j) {
+            const double4 c = p.ehss_atoms[j];
+            R ra[3];
+            rot(c, ra);
+            const R rs = static_cast<R>(c.w) + rg;
+            const R rel[3] = {off[0] - ra[0], off[1] - ra[1], off[2] - ra[2]};
+            const R ss = ax[0] * rel[0] + ax[1] * rel[1] + ax[2] * rel[2];
+            const R dv[3] = {rel[0] - ax[0] * ss, rel[1] - ax[1] * ss, rel[2] - ax[2] * ss};
+            const R d2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+            if (d2 <= rs * rs) {
+                const R hgt = m_sqrt(m_fmax(R(0), rs * rs - d2));
+                const R sh = ss - hgt;
+                if (!hit || sh < best) {
+                    const R ph[3] = {rel[0] - ax[0] * sh, rel[1] - ax[1] * sh, rel[2] - ax[2] * sh};
+                    const R pr2 = ph[0] * ph[0] + ph[1] * ph[1] + ph[2] * ph[2];
+                    if (pr2 <= R(1e-24)) {
+                        nrm[0] = -ax[0]; nrm[1] = -ax[1]; nrm[2] = -ax[2];
+                    } else {
+                        const R ip = R(1) / m_sqrt(pr2);
+                        nrm[0] = ph[0] * ip; nrm[1] = ph[1] * ip; nrm[2] = ph[2] * ip;
+                        if (ax[0] * nrm[0] + ax[1] * nrm[1] + ax[2] * nrm[2] > R(0)) {
+                            nrm[0] = -nrm[0]; nrm[1] = -nrm[1]; nrm[2] = -nrm[2];
+                        }
+                    }
+                    hit = true;
+                    best = sh;
+                }
+            }
+        }
+        if (hit) {
+            const R vd = g3[0] * nrm[0] + g3[1] * nrm[1] + g3[2] * nrm[2];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const R gr = g3[c] - nrm[c] * (R(2) * vd);
+                const R vcom = (v[c] * mi + vn[c] * mn) * inv_mt;
+                v[c] = vcom + gr * fac;
+            }
+            return;
+        }
+        if (at == 64) bmax *= R(1.5);
+    }
+}
+
 template <class R, bool SKIP, int COLL>
 __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qstar, R Amean, R b, double mi_d,
                                          const uint32_t* rk, uint32_t id, uint32_t step, const StepParams& p,
-                                         IpmPend<R>* ip) {
+                                         IpmPend<R>* ip, uint32_t eg) {
     constexpr bool LANG = COLL == kCollLangevin;
     R A, mean_th, sig_n, ug[3], mi, mn, inv_mt, fac;
     if constexpr (sizeof(R) == 8) {
@@ -538,6 +652,11 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
     const R q = A * (b + rad);
     const R pc = -m_expm1(-A * g);
     if (!LANG && !(u32(r0.z, R(0)) * q < pc)) return 1;
+    if constexpr (COLL == kCollEHSS) {
+        const R g3[3] = {gx, gy, gz};
+        ehss_scatter<R>(p, eg, v, vn, g3, g, mi, mn, inv_mt, fac, rk, id, step);
+        return 2;
+    }
     if constexpr (COLL == kCollIPMMLP) {
         // deflection after the warp's network evaluation
         const R mu = mi * fac;   // m_i m_n / (m_i + m_n); the product m_i m_n underflows in float
@@ -1048,7 +1167,7 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
                             if constexpr (COLL == kCollHSSMix)
                                 st = candidate_mix<R, true>(C, p.mix[p.ens_base + e], v, S, U, k.Amean, b, m, p.rk, id, gs);
                             else
-                                st = candidate<R, true, COLL>(C, v, S, U, k.Amean, b, m, p.rk, id, gs, p, &ip);
+                                st = candidate<R, true, COLL>(C, v, S, U, k.Amean, b, m, p.rk, id, gs, p, &ip, p.ens_base + e);
                             if (st >= 1) ++n_cand;
                             if (st >= 2) ++n_coll;
                             need_net = st == 3;
@@ -1059,7 +1178,7 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
                         if constexpr (COLL == kCollHSSMix)
                             st = candidate_mix<R, false>(C, p.mix[p.ens_base + e], v, U, R(0), k.Amean, b, m, p.rk, id, gs);
                         else
-                            st = candidate<R, false, COLL>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs, p, &ip);
+                            st = candidate<R, false, COLL>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs, p, &ip, p.ens_base + e);
                         if (st >= 2) ++n_coll;
                         need_net = st == 3;
                     }

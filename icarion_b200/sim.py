@@ -244,6 +244,13 @@ class Simulation:
         capi.check(self._lib.icb_ipm_table(self._h, capi.fptr(out.reshape(-1))))
         return out
 
+    def set_ehss_geometry(self, ensemble: int, centers_m: np.ndarray, radii_m: np.ndarray,
+                          gas_radius_m: float) -> None:
+        c = np.ascontiguousarray(centers_m, dtype=np.float64).reshape(-1, 3)
+        r = np.ascontiguousarray(radii_m, dtype=np.float64)
+        capi.check(self._lib.icb_ehss_set_geometry(self._h, ensemble, c.shape[0], capi.dptr(c.ravel()),
+                                                   capi.dptr(r), gas_radius_m))
+
     def set_mlp(self, params: np.ndarray) -> None:
         p = np.ascontiguousarray(params, dtype=np.float32)
         capi.check(self._lib.icb_ipm_set_mlp(self._h, capi.fptr(p)))

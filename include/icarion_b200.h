@@ -55,7 +55,11 @@ enum {
     /* the reference's per-step HSS form (a Maxwell-Boltzmann neutral and an
      * exp test every step), FP64 + Boris only: the plain baseline the
      * null-collision kernels are measured against */
-    ICB_COLLISION_HSS_PLAIN = 5
+    ICB_COLLISION_HSS_PLAIN = 5,
+    /* exact hard-sphere scattering on a molecule of atoms (EHSS,
+     * CollisionKernels.cpp:13-137, 220-381), rate n sigma_m2 |v - v_n|;
+     * geometry from icb_ehss_set_geometry */
+    ICB_COLLISION_EHSS = 6
 };
 enum {
     ICB_INSTRUMENT_IMS = 0,          /* AnalyticalFieldModel.cpp:136-161 */
@@ -354,6 +358,14 @@ int icb_mlp_gradients(int device, const float* params, uint64_t n, const float* 
                       float* grad, double* loss);
 /* Load network parameters into the handle (ICB_COLLISION_IPM_MLP). */
 int icb_ipm_set_mlp(struct icb_handle* h, const float* params);
+
+/* ---- EHSS molecule geometry ------------------------------------------- */
+/* Atoms (centres relative to the ion's centre of mass, n_atoms x 3 doubles,
+ * and radii) of the ions of one ensemble, and the gas (contact) radius
+ * (EHSSCollisionHandler.cpp:278-297, geometry_map_ of the handler).  Every
+ * ensemble needs one before stepping with ICB_COLLISION_EHSS. */
+int icb_ehss_set_geometry(struct icb_handle* h, int32_t ensemble, int32_t n_atoms, const double* centers_m,
+                          const double* radii_m, double gas_radius_m);
 
 /* ---- launch-shape tuning ----------------------------------------------- */
 typedef struct icb_tuning {

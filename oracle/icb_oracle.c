@@ -421,7 +421,114 @@ static void deflect(const double g3[3], double g, double cx, double sx, double c
     }
 }
 
-/* model: 0 hard sphere, 1 Langevin capture, 2 interaction-potential table */
+/* EHSS geometry of the oracle's ensemble (collision 7): atoms x, y, z, r. */
+static const double* g_ehss_atoms = NULL;
+static int g_ehss_n = 0;
+static double g_ehss_rgas = 0.0;
+
+void orc_set_ehss(const double* atoms4, int n, double gas_radius) {
+    g_ehss_atoms = atoms4;
+    g_ehss_n = n;
+    g_ehss_rgas = gas_radius;
+}
+
+/* EHSS scattering with Philox words (the product's restatement of
+ * CollisionKernels::ehss_collision, CollisionKernels.cpp:13-137, 220-381):
+ * orientation quaternion from substream 2 (Shoemake), impact points from
+ * substreams 8 + a/2 (words (0,1) for even a, (2,3) for odd a), earliest
+ * atom contact, specular reflection, COM transform; v unchanged when 256
+ * draws miss. */
+static void ehss_scatter_orc(double v[3], const double vn[3], const double g3[3], double g, double mi, double mn,
+                             uint64_t seed, uint32_t id, uint32_t step) {
+    if (g_ehss_n <= 0 || !(g > 0.0)) return;
+    const double ax[3] = {g3[0] / g, g3[1] / g, g3[2] / g};
+    const double ea[3] = {fabs(ax[0]) < 0.9 ? 1.0 : 0.0, fabs(ax[0]) < 0.9 ? 0.0 : 1.0, 0.0};
+    double t1[3] = {ax[1] * ea[2] - ax[2] * ea[1], ax[2] * ea[0] - ax[0] * ea[2], ax[0] * ea[1] - ax[1] * ea[0]};
+    double nt = 1.0 / sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+    for (int c = 0; c < 3; ++c) t1[c] *= nt;
+    double t2[3] = {ax[1] * t1[2] - ax[2] * t1[1], ax[2] * t1[0] - ax[0] * t1[2], ax[0] * t1[1] - ax[1] * t1[0]};
+    nt = 1.0 / sqrt(t2[0] * t2[0] + t2[1] * t2[1] + t2[2] * t2[2]);
+    for (int c = 0; c < 3; ++c) t2[c] *= nt;
+    uint32_t ro[4];
+    philox_words(seed, id, step, 2u, ro);
+    const double u1 = u32_to_unit(ro[0]);
+    const double p2 = 2.0 * M_PI * u32_to_unit(ro[1]), p3 = 2.0 * M_PI * u32_to_unit(ro[2]);
+    const double qa = sqrt(1.0 - u1), qb = sqrt(u1);
+    const double qx = qa * sin(p2), qy = qa * cos(p2), qz = qb * sin(p3), qw = qb * cos(p3);
+    const double Q[3][3] = {{1.0 - 2.0 * (qy * qy + qz * qz), 2.0 * (qx * qy - qz * qw), 2.0 * (qx * qz + qy * qw)},
+                            {2.0 * (qx * qy + qz * qw), 1.0 - 2.0 * (qx * qx + qz * qz), 2.0 * (qy * qz - qx * qw)},
+                            {2.0 * (qx * qz - qy * qw), 2.0 * (qy * qz + qx * qw), 1.0 - 2.0 * (qx * qx + qy * qy)}};
+    const double B[3][3] = {{t1[0], t2[0], ax[0]}, {t1[1], t2[1], ax[1]}, {t1[2], t2[2], ax[2]}};
+    double Rm[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Rm[i][j] = B[i][0] * Q[0][j] + B[i][1] * Q[1][j] + B[i][2] * Q[2][j];
+    double bmax = 0.0;
+    for (int j = 0; j < g_ehss_n; ++j) {
+        const double* c = g_ehss_atoms + 4 * j;
+        double ra[3];
+        for (int i = 0; i < 3; ++i) ra[i] = Rm[i][0] * c[0] + Rm[i][1] * c[1] + Rm[i][2] * c[2];
+        const double sra = ax[0] * ra[0] + ax[1] * ra[1] + ax[2] * ra[2];
+        const double px = ra[0] - ax[0] * sra, py = ra[1] - ax[1] * sra, pz = ra[2] - ax[2] * sra;
+        const double cur = sqrt(px * px + py * py + pz * pz) + c[3];
+        if (cur > bmax) bmax = cur;
+    }
+    bmax += g_ehss_rgas;
+    uint32_t w[4] = {0, 0, 0, 0};
+    for (int at = 0; at < 256; ++at) {
+        if ((at & 1) == 0) philox_words(seed, id, step, 8u + (uint32_t)(at >> 1), w);
+        const uint32_t wa = (at & 1) ? w[2] : w[0], wb = (at & 1) ? w[3] : w[1];
+        const double bb = bmax * sqrt(u32_to_unit(wa));
+        const double ph = 2.0 * M_PI * u32_to_unit(wb);
+        const double cph = cos(ph), sph = sin(ph);
+        const double off[3] = {t1[0] * (bb * cph) + t2[0] * (bb * sph), t1[1] * (bb * cph) + t2[1] * (bb * sph),
+                               t1[2] * (bb * cph) + t2[2] * (bb * sph)};
+        int hit = 0;
+        double best = 0.0, nrm[3] = {0.0, 0.0, 0.0};
+        for (int j = 0; j < g_ehss_n; ++j) {
+            const double* c = g_ehss_atoms + 4 * j;
+            double ra[3];
+            for (int i = 0; i < 3; ++i) ra[i] = Rm[i][0] * c[0] + Rm[i][1] * c[1] + Rm[i][2] * c[2];
+            const double rs = c[3] + g_ehss_rgas;
+            const double rel[3] = {off[0] - ra[0], off[1] - ra[1], off[2] - ra[2]};
+            const double ss = ax[0] * rel[0] + ax[1] * rel[1] + ax[2] * rel[2];
+            const double dv[3] = {rel[0] - ax[0] * ss, rel[1] - ax[1] * ss, rel[2] - ax[2] * ss};
+            const double d2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+            if (d2 <= rs * rs) {
+                const double hgt = sqrt(fmax(0.0, rs * rs - d2));
+                const double sh = ss - hgt;
+                if (!hit || sh < best) {
+                    const double phr[3] = {rel[0] - ax[0] * sh, rel[1] - ax[1] * sh, rel[2] - ax[2] * sh};
+                    const double pr2 = phr[0] * phr[0] + phr[1] * phr[1] + phr[2] * phr[2];
+                    if (pr2 <= 1e-24) {
+                        nrm[0] = -ax[0]; nrm[1] = -ax[1]; nrm[2] = -ax[2];
+                    } else {
+                        const double ip = 1.0 / sqrt(pr2);
+                        nrm[0] = phr[0] * ip; nrm[1] = phr[1] * ip; nrm[2] = phr[2] * ip;
+                        if (ax[0] * nrm[0] + ax[1] * nrm[1] + ax[2] * nrm[2] > 0.0) {
+                            nrm[0] = -nrm[0]; nrm[1] = -nrm[1]; nrm[2] = -nrm[2];
+                        }
+                    }
+                    hit = 1;
+                    best = sh;
+                }
+            }
+        }
+        if (hit) {
+            const double vd = g3[0] * nrm[0] + g3[1] * nrm[1] + g3[2] * nrm[2];
+            const double inv = 1.0 / (mi + mn);
+            const double fac = mn * inv;
+            for (int c = 0; c < 3; ++c) {
+                const double gr = g3[c] - nrm[c] * (2.0 * vd);
+                const double vcom = (v[c] * mi + vn[c] * mn) * inv;
+                v[c] = vcom + gr * fac;
+            }
+            return;
+        }
+        if (at == 64) bmax *= 1.5;
+    }
+}
+
+/* model: 0 hard sphere, 1 Langevin capture, 2 interaction-potential table, 3 EHSS */
 static int nullcoll_candidate(const gas_consts* G, double v[3], double mi, uint64_t seed, uint32_t id,
                               uint32_t step, int skip, double* clk, double qstar, double b, int model) {
     const int langevin = model == 1;
@@ -455,6 +562,10 @@ static int nullcoll_candidate(const gas_consts* G, double v[3], double mi, uint6
     double q = G->A * (b + rad);
     double p = -expm1(-G->A * g);
     if (!langevin && !(u32_to_unit(r0[2]) * q < p)) return 1;
+    if (model == 3) {
+        ehss_scatter_orc(v, vn, gv, g, mi, G->mn, seed, id, step);
+        return 2;
+    }
     if (model == 2) {
         const double mn = G->mn;
         const double inv = 1.0 / (mi + mn);
@@ -749,10 +860,11 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
             uint32_t* clk_next, uint32_t* clk_start,
             uint64_t first_id, uint64_t step0, double t0, int64_t n_steps,
             int64_t snap_every, int64_t ref_step, double* moments, uint64_t* counters, int n_threads) {
-    const int clocked = (collision == 2 || collision == 3 || collision == 4 || collision == 5);
+    const int clocked = (collision == 2 || collision == 3 || collision == 4 || collision == 5 || collision == 7);
     if (clocked && (!clk_S || !clk_U)) return 1;
     if (clocked && integrator == 0 && (!clk_next || !clk_start)) return 1;
-    if ((collision == 3 || collision == 4 || collision == 5) && integrator != 0) return 1;
+    if ((collision == 3 || collision == 4 || collision == 5 || collision == 7) && integrator != 0) return 1;
+    if (collision == 7 && !g_ehss_atoms) return 1;
     if (collision == 5 && (d->n_gas < 2 || d->n_gas > 4)) return 1;
     if (collision == 4 && !g_ipm_tab) return 1;
     const gas_consts G = gas_of(d);
@@ -840,7 +952,7 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                                 int r = (collision == 5)
                                     ? mix_candidate(d, &Gi, v, m, seed, id, gs, &sk.tau, sk.qstar)
                                     : nullcoll_candidate(&Gi, v, m, seed, id, gs, 1, &sk.tau, sk.qstar, 0.0,
-                                                         collision == 3 ? 1 : (collision == 4 ? 2 : 0));
+                                                         collision == 3 ? 1 : (collision == 4 ? 2 : (collision == 7 ? 3 : 0)));
                                 if (r >= 1) ++cand_tot;
                                 if (r == 2) ++coll_tot;
                             }
@@ -993,4 +1105,20 @@ double orc_ipm_cos_chi_trajectory(double c12, double c6, double c4, double m_red
         }
     }
     return NAN;
+}
+
+/* EHSS scattering alone (for the law check against the reference kernel):
+ * ion i collides with its neutral using Philox(seed, id = i, step = 0). */
+void orc_ehss_scatter_many(int64_t n, const double* v_ion, const double* v_n, double mi, double mn, uint64_t seed,
+                           double* out) {
+    for (int64_t i = 0; i < n; ++i) {
+        double v[3] = {v_ion[3 * i], v_ion[3 * i + 1], v_ion[3 * i + 2]};
+        const double vn[3] = {v_n[3 * i], v_n[3 * i + 1], v_n[3 * i + 2]};
+        const double g3[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
+        const double g = sqrt(g3[0] * g3[0] + g3[1] * g3[1] + g3[2] * g3[2]);
+        ehss_scatter_orc(v, vn, g3, g, mi, mn, seed, (uint32_t)i, 0u);
+        out[3 * i] = v[0];
+        out[3 * i + 1] = v[1];
+        out[3 * i + 2] = v[2];
+    }
 }

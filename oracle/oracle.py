@@ -89,6 +89,8 @@ def lib() -> C.CDLL:
                               C.c_uint64, C.c_uint64, C.c_double, C.c_int64, C.c_int64, C.c_int64,
                               DP, U64P, C.c_int]
         L.orc_run.restype = C.c_int
+        L.orc_set_ehss.argtypes = [DP, C.c_int, C.c_double]
+        L.orc_ehss_scatter_many.argtypes = [C.c_int64, DP, DP, C.c_double, C.c_double, C.c_uint64, DP]
         L.orc_set_ipm_table.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_double, C.c_double]
         L.orc_ipm_cos_chi_trajectory.argtypes = [C.c_double] * 7
         L.orc_ipm_cos_chi_trajectory.restype = C.c_double
@@ -112,6 +114,44 @@ def set_ipm_table(tab: np.ndarray, n_E: int, n_b: int, ln_E_min: float, inv_dlnE
     global _ipm_table_ref
     _ipm_table_ref = np.ascontiguousarray(tab, dtype=np.float32)
     lib().orc_set_ipm_table(_ipm_table_ref.ctypes.data_as(C.POINTER(C.c_float)), n_E, n_b, ln_E_min, inv_dlnE)
+
+
+_ehss_ref = None
+
+
+def set_ehss(atoms: np.ndarray, gas_radius: float) -> None:
+    """EHSS geometry (n x 4: x, y, z, r) for collision model 7 (kept alive here)."""
+    global _ehss_ref
+    _ehss_ref = np.ascontiguousarray(atoms, dtype=np.float64).reshape(-1, 4)
+    lib().orc_set_ehss(_dp(_ehss_ref.ravel()), _ehss_ref.shape[0], gas_radius)
+
+
+def ehss_scatter_many(v_ion: np.ndarray, v_n: np.ndarray, mi: float, mn: float, seed: int) -> np.ndarray:
+    """The restated EHSS scattering of n ions (geometry from set_ehss)."""
+    vi = np.ascontiguousarray(v_ion, dtype=np.float64).reshape(-1, 3)
+    vn = np.ascontiguousarray(v_n, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros_like(vi)
+    lib().orc_ehss_scatter_many(vi.shape[0], _dp(vi.ravel()), _dp(vn.ravel()), mi, mn, seed, _dp(out.ravel()))
+    return out
+
+
+def harness_ehss(atoms: np.ndarray, gas_radius: float, v_ion: np.ndarray, v_n: np.ndarray, mi: float, mn: float,
+                 seed: int = 1) -> np.ndarray:
+    """The reference's own CollisionKernels::ehss_collision on the same inputs."""
+    at = np.ascontiguousarray(atoms, dtype=np.float64).reshape(-1, 4)
+    vi = np.ascontiguousarray(v_ion, dtype=np.float64).reshape(-1, 3)
+    vn = np.ascontiguousarray(v_n, dtype=np.float64).reshape(-1, 3)
+    with tempfile.TemporaryDirectory() as td:
+        ip, op = Path(td) / "in.bin", Path(td) / "out.bin"
+        with open(ip, "wb") as f:
+            f.write(np.int64(at.shape[0]).tobytes())
+            f.write(at.tobytes())
+            f.write(np.int64(vi.shape[0]).tobytes())
+            f.write(vi.tobytes())
+            f.write(vn.tobytes())
+        harness("ehss", **{"in": ip, "out": op, "mi": repr(mi), "mn": repr(mn), "rgas": repr(gas_radius),
+                           "seed": seed})
+        return np.fromfile(op, dtype=np.float64).reshape(-1, 3)
 
 
 def ipm_cos_chi_trajectory(c12: float, c6: float, c4: float, m_red: float, E: float, b: float,
@@ -146,14 +186,15 @@ def run(domain: dict, state: dict, n_steps: int, *, integrator: int = 0, collisi
     clock), 3 Langevin capture with Philox (Boris, skip clock), 4
     interaction-potential table collisions (Boris, skip clock; table from
     set_ipm_table), 5 HSS gas mixture (Boris, skip clock), 6 the reference's
-    per-step HSS form with Philox words (no clock)."""
+    per-step HSS form with Philox words (no clock), 7 EHSS on the geometry
+    of set_ehss (Boris, skip clock)."""
     d = domain_struct(domain)
     n = state["x"].shape[0]
     for k in ("t_death", "t_arrival"):
         if state.get(k) is None:
             state[k] = np.full(n, -1.0)
     S = U = nxt = start = None
-    if collision in (2, 3, 4, 5):
+    if collision in (2, 3, 4, 5, 7):
         if clock is None:
             S, U = np.zeros(n), np.zeros(n)
             nxt, start = np.zeros(n, dtype=np.uint32), np.zeros(n, dtype=np.uint32)

@@ -36,6 +36,7 @@
 #include "core/config/types/CylindricalGeometry.h"
 #include "core/types/IonEnsemble.h"
 #include "core/physics/spacecharge/SpaceChargeDirectModel.h"
+#include "core/physics/collisions/core/CollisionKernels.h"
 #include "core/types/CollisionTypes.h"
 #include "utils/constants.h"
 
@@ -233,6 +234,43 @@ int mode_direct(const Args& a) {
         }
     }
     std::fclose(f);
+    return 0;
+}
+
+// EHSS scattering law of the reference kernel
+// (CollisionKernels::ehss_collision, CollisionKernels.cpp:13-137, 220-381).
+// in: int64 n_atoms, then x,y,z,r per atom; int64 n, then v_ion (3n) and
+// v_neutral (3n).  out: v_post (3n).  PhysicsRng(seed) drives all draws.
+int mode_ehss(const Args& a) {
+    FILE* f = std::fopen(str(a, "in", "ehss.bin").c_str(), "rb");
+    if (!f) throw std::runtime_error("cannot open ehss input");
+    int64_t na = 0, n = 0;
+    if (std::fread(&na, sizeof(na), 1, f) != 1) throw std::runtime_error("bad ehss input");
+    std::vector<double> atoms(static_cast<size_t>(4 * na));
+    if (std::fread(atoms.data(), sizeof(double), atoms.size(), f) != atoms.size()) throw std::runtime_error("short");
+    if (std::fread(&n, sizeof(n), 1, f) != 1) throw std::runtime_error("bad ehss input");
+    std::vector<double> vi(static_cast<size_t>(3 * n)), vn(static_cast<size_t>(3 * n));
+    if (std::fread(vi.data(), sizeof(double), vi.size(), f) != vi.size()) throw std::runtime_error("short");
+    if (std::fread(vn.data(), sizeof(double), vn.size(), f) != vn.size()) throw std::runtime_error("short");
+    std::fclose(f);
+    std::vector<Vec3> centers(static_cast<size_t>(na));
+    std::vector<double> radii(static_cast<size_t>(na));
+    for (int64_t j = 0; j < na; ++j) {
+        centers[static_cast<size_t>(j)] = Vec3{atoms[4 * j], atoms[4 * j + 1], atoms[4 * j + 2]};
+        radii[static_cast<size_t>(j)] = atoms[4 * j + 3];
+    }
+    const double mi = num(a, "mi", 1e-25), mn = num(a, "mn", 4.65e-26), rg = num(a, "rgas", 1.8e-10);
+    physics::PhysicsRng rng(static_cast<uint64_t>(std::strtoull(str(a, "seed", "1").c_str(), nullptr, 10)));
+    FILE* o = std::fopen(str(a, "out", "ehss_out.bin").c_str(), "wb");
+    for (int64_t i = 0; i < n; ++i) {
+        const Vec3 v{vi[3 * i], vi[3 * i + 1], vi[3 * i + 2]};
+        const Vec3 w{vn[3 * i], vn[3 * i + 1], vn[3 * i + 2]};
+        const Vec3 p = physics::collision_core::CollisionKernels::ehss_collision(v, w, mi, mn, rg, centers, radii,
+                                                                                   rng);
+        const double q[3] = {p.x, p.y, p.z};
+        std::fwrite(q, sizeof(double), 3, o);
+    }
+    std::fclose(o);
     return 0;
 }
 
@@ -436,6 +474,7 @@ int main(int argc, char** argv) {
         if (mode == "derive") return mode_derive(a);
         if (mode == "run") return mode_run(a);
         if (mode == "direct") return mode_direct(a);
+        if (mode == "ehss") return mode_ehss(a);
         std::fprintf(stderr, "unknown mode %s\n", argv[1]);
         return 2;
     } catch (const std::exception& e) {

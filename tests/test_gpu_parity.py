@@ -194,6 +194,41 @@ def test_fp64_plain_form_matches_oracle():
     assert rs["candidates"] == n * steps
 
 
+def test_fp64_ehss_trajectories_match_oracle():
+    """EHSS collisions on a 7-atom molecule against the oracle's
+    restatement (itself checked against the reference kernel on CPU): >= 99 %
+    of FP64 ions to 1e-9 after 2000 steps, collision counts within 1 %; the
+    mixed form's collision count within 1 % of FP64."""
+    from test_oracle_ehss import molecule
+    at = molecule()
+    e = config0_ensemble()
+    n, steps = 512, 2000
+    st0 = config0_ions(n)
+    ost = oracle_state(st0)
+    orc.set_ehss(at, 1.8e-10)
+    r = orc.run(e, ost, steps, integrator=0, collision=7, seed=123)
+
+    def run(prec, st):
+        with Simulation([e], precision=prec, collision=capi.COLLISION_EHSS, rng_seed=123) as sim:
+            sim.upload(st)
+            sim.set_ehss_geometry(0, at[:, :3], at[:, 3], 1.8e-10)
+            rs = sim.advance(steps)
+            return sim.download(), rs
+    out, rs = run(capi.PREC_FP64, st0)
+    pos = np.stack([out.x, out.y, out.z])
+    opos = np.stack([ost["x"], ost["y"], ost["z"]])
+    vel = np.stack([out.vx, out.vy, out.vz])
+    ovel = np.stack([ost["vx"], ost["vy"], ost["vz"]])
+    rel = np.maximum(np.linalg.norm(pos - opos, axis=0) / np.linalg.norm(opos, axis=0),
+                     np.linalg.norm(vel - ovel, axis=0) / np.linalg.norm(ovel, axis=0))
+    assert float(np.mean(rel < 1e-9)) >= 0.99, np.sort(rel)[-5:]
+    assert abs(rs["collisions"] - r["collisions"]) <= 0.01 * r["collisions"]
+    st1 = config0_ions(8192)
+    _, r64 = run(capi.PREC_FP64, st1)
+    _, rmx = run(capi.PREC_MIXED, st1)
+    assert abs(rmx["collisions"] / r64["collisions"] - 1.0) < 0.01
+
+
 def test_results_independent_of_launch_shape():
     """Same Philox counters and per-lane step order: block size, steps per
     launch and the deferred-collision threshold do not change results."""
