@@ -584,6 +584,7 @@ def run_ipm(args) -> None:
         sim.configure_ipm(setup)
         if model == capi.COLLISION_IPM_MLP:
             sim.set_mlp(params)
+        tuned = sim.autotune(300) if args.autotune else None
         for _ in range(args.warmup):
             sim.advance(STEPS_PER_BENCH_STEP)
         sim.upload(st0, ens_offsets=offsets, first_id=rank * n_total)
@@ -611,7 +612,8 @@ def run_ipm(args) -> None:
             n_gas = ensembles[e]["gas_density_m3"]
             E = en[e] * 1e-21 * n_gas
             k0.append(v_d / E * (n_gas / cfg.n0_loschmidt()) * 1e4)
-        results[name] = {"ion_steps_per_s": n_total * STEPS_PER_BENCH_STEP * args.steps / (ms * 1e-3),
+        results[name] = {"autotuned": tuned,
+                         "ion_steps_per_s": n_total * STEPS_PER_BENCH_STEP * args.steps / (ms * 1e-3),
                          "ms_per_step": ms / args.steps, "K0_cm2_Vs": k0,
                          "collision_fraction": coll / (n_total * STEPS_PER_BENCH_STEP * args.steps)}
         sim.close()
