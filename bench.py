@@ -54,6 +54,7 @@ BYTES_PER_ION_LAUNCH = {"mixed": 130, "hilo": 130, "fp64": 170}
 # DRAM bytes of one fused mixed launch at 1,048,576 ions from an ncu capture
 # of that launch (dram__bytes_read.sum + dram__bytes_write.sum; writes still
 # in L2 at kernel end are not counted).
+STEPPING = {"events": 0, "per-step": 1}
 NCU_TRAFFIC_PER_LAUNCH = {"mixed": 81.245952e6 + 8.287232e6}
 
 
@@ -254,7 +255,8 @@ def run_ours(args) -> None:
     def make_sim(prec, K=args.steps_per_launch, collision=capi.COLLISION_HSS):
         s = Simulation(ensembles, precision=prec, integrator=capi.INTEGRATOR_BORIS, collision=collision,
                        rng_seed=123, device=dev, steps_per_launch=K, block_size=args.block,
-                       pending_threshold=args.pending, steps_per_vote=args.spv, use_graphs=int(args.graphs))
+                       pending_threshold=args.pending, steps_per_vote=args.spv, use_graphs=int(args.graphs),
+                       stepping=STEPPING[args.stepping])
         s.set_stream(stream.cuda_stream)
         s.upload(st0, ens_offsets=offsets, first_id=first_id)
         return s
@@ -397,7 +399,7 @@ def run_ours(args) -> None:
                    "steps_per_launch": sim_K(None), "collisions": "HSS null-collision, Philox4x32-10",
                    "parallelism": f"ions sharded, {world} GPU(s)", "l2": "flushed between timed steps (256 MB write)",
                    "collision_fraction": stt["collisions"] / max(ion_steps / world, 1),
-                   "cuda_graphs": bool(args.graphs), "autotuned": tuning},
+                   "cuda_graphs": bool(args.graphs), "autotuned": tuning, "stepping": args.stepping},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"],
@@ -578,7 +580,8 @@ def run_ipm(args) -> None:
     clocks = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)).split(",")[0]) if world == 1 else dev)
     clocks.start()
     for name, model in (("table", capi.COLLISION_IPM_TABLE), ("mlp", capi.COLLISION_IPM_MLP)):
-        sim = Simulation(ensembles, precision=capi.PREC_MIXED, collision=model, rng_seed=123, device=dev)
+        sim = Simulation(ensembles, precision=capi.PREC_MIXED, collision=model, rng_seed=123, device=dev,
+                         stepping=STEPPING[args.stepping])
         sim.set_stream(stream.cuda_stream)
         sim.upload(st0, ens_offsets=offsets, first_id=rank * n_total)
         sim.configure_ipm(setup)
@@ -663,6 +666,8 @@ def main():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--pending", type=int, default=0)
     ap.add_argument("--spv", type=int, default=0, help="collision-free steps between warp votes")
+    ap.add_argument("--stepping", choices=["events", "per-step"], default="events",
+                    help="float forms: event-to-event closed-form drift, or the step-by-step loop")
     ap.add_argument("--workload", choices=["ims-1M", "en-sweep", "fticr-sc", "ipm"], default="ims-1M",
                     help="ims-1M: the 1,048,576-ion IMS run (default); en-sweep: the batched 64-ensemble E/N "
                          "sweep; fticr-sc: the 262,144-ion FT-ICR cell with P3M space charge; ipm: learned "

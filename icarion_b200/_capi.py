@@ -29,6 +29,7 @@ COLLISION_NONE, COLLISION_HSS, COLLISION_IPM_TABLE, COLLISION_IPM_MLP, COLLISION
 COLLISION_HSS_PLAIN, COLLISION_EHSS = 5, 6
 INSTRUMENT_IMS, INSTRUMENT_FTICR, INSTRUMENT_QUADRUPOLE_RF = 0, 1, 2
 SC_OFF, SC_P3M_ISOLATED, SC_PM_PERIODIC_REF = 0, 1, 2
+STEPPING_EVENTS, STEPPING_PER_STEP = 0, 1
 MLP_HIDDEN, MLP_N_PARAMS = 64, 4417
 POS_POINT, POS_GAUSSIAN, POS_UNIFORM_SPHERE, POS_UNIFORM_CYLINDER, POS_UNIFORM_BOX = 0, 1, 2, 3, 4
 VEL_FIXED, VEL_THERMAL = 0, 1
@@ -70,7 +71,7 @@ class Config(C.Structure):
         ("n_ensembles", C.c_int32), ("ensembles", C.POINTER(EnsembleParams)), ("rng_seed", C.c_uint64),
         ("device", C.c_int32), ("block_size", C.c_int32), ("steps_per_launch", C.c_int32),
         ("pending_threshold", C.c_int32), ("use_graphs", C.c_int32), ("steps_per_vote", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("stepping", C.c_int32), ("reserved", C.c_int32 * 5),
     ]
 
 

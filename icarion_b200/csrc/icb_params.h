@@ -128,6 +128,7 @@ struct StepParams {
     uint32_t ens_base;                 // global index of this chunk's ensemble 0
     uint32_t n_ens;
     uint32_t do_push, do_collide, do_finalize, steps_per_vote;
+    uint32_t jumps;                    // event-to-event drift where the kernel supports it
     uint64_t ens_off[kMaxLaunchEns + 1];  // absolute ion offsets of the chunk's ensembles
     EnsConst ens[kMaxLaunchEns];
 };

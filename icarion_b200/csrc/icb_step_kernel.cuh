@@ -100,6 +100,7 @@ struct PosD {
     __device__ void drift(double vx, double vy, double vz, double dt, double) {
         x += vx * dt; y += vy * dt; z += vz * dt;
     }
+    __device__ void jump(double Dx, double Dy, double Dz) { x += Dx; y += Dy; z += Dz; }
     __device__ bool finite() const { return isfinite(x) && isfinite(y) && isfinite(z); }
 };
 
@@ -132,6 +133,11 @@ struct PosA {
     }
     __device__ void drift(float vx, float vy, float vz, double, float d) {
         dx = fmaf(vx, d, dx); dy = fmaf(vy, d, dy); dz = fmaf(vz, d, dz);
+    }
+    // A multi-step displacement goes straight into the anchor (the jump loop
+    // never leaves an offset).
+    __device__ void jump(float Dx, float Dy, float Dz) {
+        ax += static_cast<double>(Dx); ay += static_cast<double>(Dy); az += static_cast<double>(Dz);
     }
     __device__ bool finite() const {
         return isfinite(ax) && isfinite(ay) && isfinite(az) && isfinite(dx) && isfinite(dy) && isfinite(dz);
@@ -177,6 +183,11 @@ struct PosHL {
         two_sum_acc(xh, xl, vx * d);
         two_sum_acc(yh, yl, vy * d);
         two_sum_acc(zh, zl, vz * d);
+    }
+    __device__ void jump(float Dx, float Dy, float Dz) {
+        two_sum_acc(xh, xl, Dx);
+        two_sum_acc(yh, yl, Dy);
+        two_sum_acc(zh, zl, Dz);
     }
     __device__ bool finite() const {
         return isfinite(xh) && isfinite(yh) && isfinite(zh) && isfinite(xl) && isfinite(yl) && isfinite(zl);
@@ -970,6 +981,9 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
     // horizon's last step; restarts happen at global step indices fixed by
     // the lane's own history, so results do not depend on launch shape.
     constexpr bool kSkip = (INTEG == kBoris) && (COLL != kCollNone) && (COLL != kCollHSSPlain);
+    // closed-form event-to-event drift (run_jumps below)
+    constexpr bool kJump = FUSED && (INTEG == kBoris) && (FIELD == kFieldUniform) && !MAG &&
+                           (PREC != kPrecFP64) && (COLL != kCollHSSPlain);
     constexpr uint32_t kRefresh = 0x80000000u, kNeedRestart = 0xFFFFFFFFu;
     uint32_t g_next = kNeedRestart, g_start = 0u, nk = 0xFFFFFFFFu, H = 1u;
     R lam = R(0), dvmax = R(0), absu = R(0);
@@ -1052,32 +1066,102 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
         if (live && (do_coll || do_push) && g_next == kNeedRestart) clock_restart(step0);
     }
 
-    // exact finalize of the current step (SimulationEngineLifecycle.cpp:123-195)
+    // exact finalize of a step that started at time ts with z = zo
+    // (SimulationEngineLifecycle.cpp:123-195)
+    auto check_exact = [&](double zo, double ts) {
+        const double znew = x.gz();
+        if (!had_arrival && zo < zdet && znew >= zdet) {
+            tarr = ts + dt * ((zdet - zo) / (znew - zo));
+            had_arrival = true;
+            arr_now = true;
+            ++n_arr;
+        }
+        bool ok = inside(C, x);
+        if (ok) ok = x.finite() && isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]);
+        if (!ok) {
+            live = false;
+            kill(ts);
+        } else {
+            new_limit();
+        }
+    };
     auto finalize_step = [&]() {
         // the unfused finalize call has no drift history: always exact
         if (do_fin && (!FUSED || !(acc <= lim))) {
             double zo = x.z_of(zold);
             if (!FUSED && !do_push) zo = p.zprev[i];
             x.fold();
-            const double ts = t_step();
-            const double znew = x.gz();
-            if (!had_arrival && zo < zdet && znew >= zdet) {
-                tarr = ts + dt * ((zdet - zo) / (znew - zo));
-                had_arrival = true;
-                arr_now = true;
-                ++n_arr;
-            }
-            bool ok = inside(C, x);
-            if (ok) ok = x.finite() && isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]);
-            if (!ok) {
-                live = false;
-                kill(ts);
-            } else {
-                new_limit();
-            }
+            check_exact(zo, t_step());
         }
         ++kk;
         if (kAccumT) t = t + dt;
+    };
+
+    // The clock event of step gs (a lane with has_ev): candidate (or horizon
+    // refresh), the warp's shared network evaluation for the learned
+    // deflection, and the clock restart from the step after.  Every lane of
+    // the warp calls this together.
+    auto collide_at = [&](bool has_ev, uint32_t gs) {
+        IpmPend<R> ip;
+        bool need_net = false;
+        if (has_ev) {
+            if constexpr (kSkip) {
+                if (g_next & kRefresh) {
+                    // horizon end without an event: consume its steps
+                    S = S - static_cast<R>(gs + 1u - g_start) * lam;
+                } else {
+                    int st;
+                    if constexpr (COLL == kCollHSSMix)
+                        st = candidate_mix<R, true>(C, p.mix[p.ens_base + e], v, S, U, k.Amean, b, m, p.rk, id, gs);
+                    else
+                        st = candidate<R, true, COLL>(C, v, S, U, k.Amean, b, m, p.rk, id, gs, p, &ip, p.ens_base + e);
+                    if (st >= 1) ++n_cand;
+                    if (st >= 2) ++n_coll;
+                    need_net = st == 3;
+                }
+            } else {
+                ++n_cand;
+                int st;
+                if constexpr (COLL == kCollHSSMix)
+                    st = candidate_mix<R, false>(C, p.mix[p.ens_base + e], v, U, R(0), k.Amean, b, m, p.rk, id, gs);
+                else
+                    st = candidate<R, false, COLL>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs, p, &ip, p.ens_base + e);
+                if (st >= 2) ++n_coll;
+                need_net = st == 3;
+            }
+        }
+        if constexpr (COLL == kCollIPMMLP) {
+            // the warp's accepted collisions share one tensor-core
+            // evaluation of the deflection network; energies outside
+            // the trained range use the table
+            if (__any_sync(0xffffffffu, need_net)) {
+                R tt = R(0);
+                bool in_dom = false;
+                if (need_net) {
+                    tt = (m_log(ip.E) - static_cast<R>(p.ipm_lnEmin)) * static_cast<R>(p.ipm_inv_dlnE);
+                    in_dom = tt >= R(0) && tt <= static_cast<R>(p.ipm_nE - 1);
+                }
+                const float x0 = static_cast<float>(R(2) * tt / static_cast<R>(p.ipm_nE - 1) - R(1));
+                const float x1 = static_cast<float>(R(2) * ip.bn - R(1));
+                const float y = mlp_warp_eval(p.mlp_w2, p.mlp_f, x0, x1, need_net && in_dom);
+                if (need_net) {
+                    R cx = in_dom ? m_fmin(m_fmax(static_cast<R>(y), R(-1)), R(1))
+                                  : ipm_table_cos<R>(p, ip.E, ip.bn);
+                    ipm_apply<R>(C, v, ip, cx, m);
+                }
+            }
+        }
+        if (has_ev) {
+            if constexpr (kSkip) {
+                clock_restart(gs + 1u);
+            } else {
+                S = R(1);
+                if constexpr (sizeof(R) == 4) {
+                    const R wx = v[0] - k.ug[0], wy = v[1] - k.ug[1], wz = v[2] - k.ug[2];
+                    cb.set(wx * wx + wy * wy + wz * wz);
+                }
+            }
+        }
     };
 
     // one collision-free step (or a step that leaves the lane pending)
@@ -1154,69 +1238,9 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
             const unsigned run_mask = __ballot_sync(0xffffffffu, can_step);
             if (pend_mask != 0u &&
                 (run_mask == 0u || static_cast<uint32_t>(__popc(pend_mask)) >= p.pend_threshold)) {
-                IpmPend<R> ip;
-                bool need_net = false;
-                const uint32_t gs = step0 + kk;
-                if (pending && cand) {
-                    if constexpr (kSkip) {
-                        if (g_next & kRefresh) {
-                            // horizon end without an event: consume its steps
-                            S = S - static_cast<R>(gs + 1u - g_start) * lam;
-                        } else {
-                            int st;
-                            if constexpr (COLL == kCollHSSMix)
-                                st = candidate_mix<R, true>(C, p.mix[p.ens_base + e], v, S, U, k.Amean, b, m, p.rk, id, gs);
-                            else
-                                st = candidate<R, true, COLL>(C, v, S, U, k.Amean, b, m, p.rk, id, gs, p, &ip, p.ens_base + e);
-                            if (st >= 1) ++n_cand;
-                            if (st >= 2) ++n_coll;
-                            need_net = st == 3;
-                        }
-                    } else {
-                        ++n_cand;
-                        int st;
-                        if constexpr (COLL == kCollHSSMix)
-                            st = candidate_mix<R, false>(C, p.mix[p.ens_base + e], v, U, R(0), k.Amean, b, m, p.rk, id, gs);
-                        else
-                            st = candidate<R, false, COLL>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs, p, &ip, p.ens_base + e);
-                        if (st >= 2) ++n_coll;
-                        need_net = st == 3;
-                    }
-                }
-                if constexpr (COLL == kCollIPMMLP) {
-                    // the warp's accepted collisions share one tensor-core
-                    // evaluation of the deflection network; energies outside
-                    // the trained range use the table
-                    if (__any_sync(0xffffffffu, need_net)) {
-                        R t = R(0);
-                        bool in_dom = false;
-                        if (need_net) {
-                            t = (m_log(ip.E) - static_cast<R>(p.ipm_lnEmin)) * static_cast<R>(p.ipm_inv_dlnE);
-                            in_dom = t >= R(0) && t <= static_cast<R>(p.ipm_nE - 1);
-                        }
-                        const float x0 = static_cast<float>(R(2) * t / static_cast<R>(p.ipm_nE - 1) - R(1));
-                        const float x1 = static_cast<float>(R(2) * ip.bn - R(1));
-                        const float y = mlp_warp_eval(p.mlp_w2, p.mlp_f, x0, x1, need_net && in_dom);
-                        if (need_net) {
-                            R cx = in_dom ? m_fmin(m_fmax(static_cast<R>(y), R(-1)), R(1))
-                                          : ipm_table_cos<R>(p, ip.E, ip.bn);
-                            ipm_apply<R>(C, v, ip, cx, m);
-                        }
-                    }
-                }
+                collide_at(pending && cand, step0 + kk);
                 if (pending) {
-                    if (cand) {
-                        if constexpr (kSkip) {
-                            clock_restart(gs + 1u);
-                        } else {
-                            S = R(1);
-                            if constexpr (sizeof(R) == 4) {
-                                const R wx = v[0] - k.ug[0], wy = v[1] - k.ug[1], wz = v[2] - k.ug[2];
-                                cb.set(wx * wx + wy * wy + wz * wz);
-                            }
-                        }
-                        cand = false;
-                    }
+                    cand = false;
                     pending = false;
                     finalize_step();
                 }
@@ -1225,8 +1249,87 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
             if (run_mask == 0u) break;
         }
     };
-    if (__any_sync(0xffffffffu, waiting)) run(std::true_type{});
-    else run(std::false_type{});
+    // Event-to-event drift (float forms, Boris in a uniform field without a
+    // magnetic field, fused launches).  With a constant acceleration a the
+    // Boris steps have a closed form: n steps from velocity v end at
+    // v + a n dt after the displacement n dt v + a (n dt)^2 / 2 (the sum of
+    // the per-step drifts (v + a dt/2 + (j-1) a dt) dt, j = 1..n).  Each lane
+    // moves in one update to the first of: its clock event, the step at
+    // which its displacement budget may run out, the end of the launch; the
+    // warp then handles the events of all its lanes together, so candidate
+    // work runs with most lanes active and no per-step work remains.
+    // Events fall on the same steps and draw the same Philox counters as the
+    // step-by-step loop; the drift differs from it by float rounding only.
+    // Budget: the L1 path of j steps is at most
+    //   B(j) = j dt s0 + ca j (j-1) / 2,  s0 = |v + a dt/2|_1,  ca = |a|_1 dt^2,
+    // so a jump of n steps with B(n-1) <= lim - acc passes no step at which
+    // the exact check could fire; it checks its last step exactly when
+    // acc + B(n) exceeds lim.
+    auto run_jumps = [&]() {
+        const R a0 = k.a_uni[0], a1 = k.a_uni[1], a2 = k.a_uni[2];
+        const R ca = (m_fabs(a0) + m_fabs(a1) + m_fabs(a2)) * dt_r * dt_r;
+        const R ah0 = a0 * k.h, ah1 = a1 * k.h, ah2 = a2 * k.h;
+        while (true) {
+            const bool act = live && kk < K;
+            if (__ballot_sync(0xffffffffu, act) == 0u) break;
+            bool ev = false, exact = false;
+            double zo = 0.0;
+            if (act) {
+                uint32_t n = K - kk;
+                uint32_t ne = 0xFFFFFFFFu;
+                if constexpr (kSkip) {
+                    ne = nk + 1u - kk;    // steps up to and including the clock event
+                    if (ne < n) n = ne;
+                }
+                const R s0 = m_fabs(v[0] + ah0) + m_fabs(v[1] + ah1) + m_fabs(v[2] + ah2);
+                const R sd = s0 * dt_r;
+                auto bound = [&](uint32_t j) {
+                    const R rj = static_cast<R>(j);
+                    return rj * (sd + R(0.5) * ca * (rj - R(1)));
+                };
+                if (budget) {
+                    const R rem = lim - acc;
+                    uint32_t nb = 0;
+                    if (rem >= R(0)) {     // false for a non-finite state
+                        const R B = sd - R(0.5) * ca;
+                        const R den = B + m_sqrt(m_fmax(B * B + R(2) * ca * rem, R(0)));
+                        R nbf = R(0);
+                        if (den > R(0)) nbf = (R(2) * rem) / den;
+                        else if (den == R(0)) nbf = static_cast<R>(n);
+                        nb = nbf >= static_cast<R>(n) ? n : static_cast<uint32_t>(nbf);
+                        if (nb > 0u && !(bound(nb) <= rem)) --nb;
+                    }
+                    if (nb + 1u < n) n = nb + 1u;
+                } else {
+                    n = 1u;               // short launches check every step
+                }
+                ev = n == ne;
+                acc += bound(n);
+                exact = !budget || !(acc <= lim);
+                const R nd = static_cast<R>(n) * dt_r;
+                const R hn = R(0.5) * nd;
+                x.jump(nd * (v[0] + a0 * hn), nd * (v[1] + a1 * hn), nd * (v[2] + a2 * hn));
+                v[0] = v[0] + a0 * nd;
+                v[1] = v[1] + a1 * nd;
+                v[2] = v[2] + a2 * nd;
+                kk += n;
+                // z before the last step: minus that step's drift (v - a dt/2) dt
+                if (exact) zo = x.gz() - static_cast<double>(dt_r * (v[2] - ah2));
+            }
+            collide_at(ev, step0 + kk - 1u);
+            if (exact) check_exact(zo, fma(static_cast<double>(kk - 1u), dt, t0));
+        }
+    };
+    if (__any_sync(0xffffffffu, waiting)) {
+        run(std::true_type{});
+    } else {
+        if constexpr (kJump) {
+            if (p.jumps) run_jumps();
+            else run(std::false_type{});
+        } else {
+            run(std::false_type{});
+        }
+    }
 
     if (in_range) {
         x.store(p, i);

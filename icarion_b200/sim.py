@@ -85,7 +85,8 @@ class Simulation:
     def __init__(self, ensembles: list[dict], precision: int = capi.PREC_MIXED,
                  integrator: int = capi.INTEGRATOR_BORIS, collision: int = capi.COLLISION_HSS,
                  rng_seed: int = 123, device: int = 0, block_size: int = 0, steps_per_launch: int = 0,
-                 pending_threshold: int = 0, use_graphs: int = 0, steps_per_vote: int = 0):
+                 pending_threshold: int = 0, use_graphs: int = 0, steps_per_vote: int = 0,
+                 stepping: int = capi.STEPPING_EVENTS):
         self._lib = capi.lib()
         self.n_ens = len(ensembles)
         self._ens = (capi.EnsembleParams * self.n_ens)(*[cfgmod.to_struct(e) for e in ensembles])
@@ -102,6 +103,7 @@ class Simulation:
         cfg.pending_threshold = pending_threshold
         cfg.use_graphs = use_graphs
         cfg.steps_per_vote = steps_per_vote
+        cfg.stepping = stepping
         self._h = C.c_void_p()
         capi.check(self._lib.icb_create(C.byref(cfg), C.byref(self._h)))
         self.ensembles = ensembles

@@ -128,8 +128,18 @@ typedef struct icb_config {
     int32_t pending_threshold; /* deferred-collision batch size per warp, 0 = default */
     int32_t use_graphs;        /* capture launch sequences in CUDA graphs */
     int32_t steps_per_vote;    /* collision-free steps between warp votes, 0 = default */
-    int32_t reserved[6];
+    int32_t stepping;          /* ICB_STEPPING_* (0 = event-to-event drift where supported) */
+    int32_t reserved[5];
 } icb_config;
+
+/* Stepping of the fused float forms (MIXED, MIXED_HILO) with Boris in a
+ * uniform field and no magnetic field: EVENTS moves each ion in one
+ * closed-form update from one event (collision-clock event, exact domain
+ * check, end of launch) to the next; PER_STEP applies the steps one by one.
+ * Both draw the same random numbers at the same steps; their drifts differ
+ * by float rounding.  FP64, RK4, non-uniform fields and the per-step plug
+ * points always step one by one. */
+enum { ICB_STEPPING_EVENTS = 0, ICB_STEPPING_PER_STEP = 1 };
 
 #define ICB_MAX_ENSEMBLES 256
 
