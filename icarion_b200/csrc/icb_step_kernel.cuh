@@ -1289,17 +1289,21 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
                 };
                 if (budget) {
                     const R rem = lim - acc;
-                    uint32_t nb = 0;
-                    if (rem >= R(0)) {     // false for a non-finite state
-                        const R B = sd - R(0.5) * ca;
-                        const R den = B + m_sqrt(m_fmax(B * B + R(2) * ca * rem, R(0)));
-                        R nbf = R(0);
-                        if (den > R(0)) nbf = (R(2) * rem) / den;
-                        else if (den == R(0)) nbf = static_cast<R>(n);
-                        nb = nbf >= static_cast<R>(n) ? n : static_cast<uint32_t>(nbf);
-                        if (nb > 0u && !(bound(nb) <= rem)) --nb;
+                    // the largest nb with B(nb) <= rem, solved only when the
+                    // whole jump does not fit (near a wall or the detector)
+                    if (!(bound(n) <= rem)) {
+                        uint32_t nb = 0;
+                        if (rem >= R(0)) {     // false for a non-finite state
+                            const R B = sd - R(0.5) * ca;
+                            const R den = B + m_sqrt(m_fmax(B * B + R(2) * ca * rem, R(0)));
+                            R nbf = R(0);
+                            if (den > R(0)) nbf = (R(2) * rem) / den;
+                            else if (den == R(0)) nbf = static_cast<R>(n);
+                            nb = nbf >= static_cast<R>(n) ? n : static_cast<uint32_t>(nbf);
+                            if (nb > 0u && !(bound(nb) <= rem)) --nb;
+                        }
+                        if (nb + 1u < n) n = nb + 1u;
                     }
-                    if (nb + 1u < n) n = nb + 1u;
                 } else {
                     n = 1u;               // short launches check every step
                 }

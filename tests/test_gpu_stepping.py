@@ -134,6 +134,49 @@ def test_short_launches_check_every_step():
     assert np.mean(_rel_err(ev, ref) <= 1e-5) >= 0.99
 
 
+def test_every_ion_of_a_large_cloud_is_advanced():
+    """300,000 ions: more than the resident grid's threads, so threads move
+    on to further ions.  Every ion moves, and the states follow the
+    step-by-step loop (one thread per ion)."""
+    e = config0_ensemble()
+    st0 = config0_ions(300_000)
+    ev, rs_ev = _run(e, st0, 400, capi.PREC_MIXED, capi.STEPPING_EVENTS)
+    ps, rs_ps = _run(e, st0, 400, capi.PREC_MIXED, capi.STEPPING_PER_STEP)
+    assert np.all(ev.z != st0.z) and np.all(ev.vz != st0.vz)
+    assert np.mean(_rel_err(ev, ps) <= 1e-4) >= 0.98
+    assert abs(rs_ev["collisions"] - rs_ps["collisions"]) <= 0.005 * rs_ps["collisions"]
+    assert int(ev.active.sum()) == int(ps.active.sum())
+
+
+def test_births_follow_step_by_step():
+    """Unborn ions wait unmoved until the first step whose start time reaches
+    their birth time, then step; the event form jumps to that step."""
+    e = config0_ensemble()
+    n = 4096
+    st = config0_ions(n)
+    rng = np.random.default_rng(5)
+    st.birth = rng.uniform(0.0, 1100 * DT, n)
+    st.birth[:64] = 1.0                     # never born within the run
+    st.birth[64:128] = 0.0
+    st.birth[128:192] = 700 * DT            # exactly on a step start
+    outs = []
+    for stepping in (capi.STEPPING_EVENTS, capi.STEPPING_PER_STEP):
+        with Simulation([e], precision=capi.PREC_MIXED, collision=capi.COLLISION_HSS, rng_seed=77,
+                        stepping=stepping, steps_per_launch=400) as sim:
+            sim.upload(st)
+            sim.advance(500)
+            mid = sim.download()
+            sim.advance(700)
+            outs.append((mid, sim.download()))
+    (mid_ev, ev), (mid_ps, ps) = outs
+    for a, b in ((mid_ev, mid_ps), (ev, ps)):
+        assert np.array_equal(a.active, b.active)
+        unborn = b.active == 0
+        assert np.array_equal(a.z[unborn], st.z[unborn]) and np.array_equal(b.z[unborn], st.z[unborn])
+        assert np.mean(_rel_err(a, b) <= 1e-4) >= 0.98
+    assert not ev.active[:64].any() and ev.active[64:].all()
+
+
 def test_stepping_mode_is_validated():
     with pytest.raises(capi.IcbError):
         Simulation([config0_ensemble()], stepping=7)
