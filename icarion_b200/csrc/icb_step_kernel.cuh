@@ -633,14 +633,23 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
         inv_mt = __frcp_rn(mi + mn);
         fac = mn * inv_mt;
     }
+    // The hard-sphere kinds run without branches: every event lane draws
+    // both Philox blocks and forms the scattered velocity, and the outcome
+    // (thinned, rejected, collided) selects what is kept.  The values are
+    // those of the early-exit form.
+    constexpr bool kFlat = COLL == kCollHSS || COLL == kCollLangevin;
     const U4 r0 = philox4x32_10_rk(id, step, 0u, 0u, rk);
     R uc = u32(r0.y, R(0));
+    bool kept = true;                 // not thinned away
     if constexpr (SKIP) {
         clk = -m_log(u32(r0.x, R(0)));
         const R wx = v[0] - ug[0], wy = v[1] - ug[1], wz = v[2] - ug[2];
         b = m_sqrt(wx * wx + wy * wy + wz * wz);
         const R Q = A * b + Amean;
-        if (!(uc * qstar < Q)) return 0;
+        kept = uc * qstar < Q;
+        if constexpr (!kFlat) {
+            if (!kept) return 0;
+        }
         uc = uc * qstar / Q;          // uniform on (0, 1) given the acceptance
     } else {
         clk = u32(r0.x, R(0));
@@ -662,7 +671,10 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
     const R g = m_sqrt(gx * gx + gy * gy + gz * gz);
     const R q = A * (b + rad);
     const R pc = -m_expm1(-A * g);
-    if (!LANG && !(u32(r0.z, R(0)) * q < pc)) return 1;
+    const bool hit = kept && (LANG || u32(r0.z, R(0)) * q < pc);
+    if constexpr (!kFlat) {
+        if (!hit) return 1;
+    }
     if constexpr (COLL == kCollEHSS) {
         const R g3[3] = {gx, gy, gz};
         ehss_scatter<R>(p, eg, v, vn, g3, g, mi, mn, inv_mt, fac, rk, id, step);
@@ -706,9 +718,10 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const R vcom = (v[c] * mi + vn[c] * mn) * inv_mt;
-        v[c] = vcom + (dir[c] * g) * fac;
+        const R vs = vcom + (dir[c] * g) * fac;
+        v[c] = hit ? vs : v[c];
     }
-    return 2;
+    return hit ? 2 : (kept ? 1 : 0);
 }
 
 // Candidate of an HSS gas mixture (HSSCollisionHandler.cpp:105-249): the
