@@ -55,7 +55,7 @@ BYTES_PER_ION_LAUNCH = {"mixed": 130, "hilo": 130, "fp64": 170}
 # of that launch (dram__bytes_read.sum + dram__bytes_write.sum; writes still
 # in L2 at kernel end are not counted).
 STEPPING = {"events": 0, "per-step": 1}
-NCU_TRAFFIC_PER_LAUNCH = {"mixed": 81.245952e6 + 8.287232e6}
+NCU_TRAFFIC_PER_LAUNCH = {"mixed": 80.829696e6 + 6.218752e6}
 
 
 def _env_rank():
