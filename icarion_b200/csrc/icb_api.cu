@@ -307,8 +307,10 @@ struct icb_handle {
     DevBuf<int32_t> ehss_off;
     DevBuf<double> ehss_rgas;
     bool mlp_ready = false;
-    // host fast path: copy stream, per-chunk events, velocity staging (3n)
+    // host fast path: copy stream, per-chunk compute streams and events,
+    // velocity staging (3n)
     cudaStream_t copy_stream = nullptr;
+    std::vector<cudaStream_t> chunk_streams;
     std::vector<cudaEvent_t> hev;
     DevBuf<double> hstage;
     // space charge (solved before every step when configured)
@@ -328,6 +330,7 @@ struct icb_handle {
         for (cudaEvent_t e : sc_ev) cudaEventDestroy(e);
         for (cudaEvent_t e : hev) cudaEventDestroy(e);
         if (copy_stream) cudaStreamDestroy(copy_stream);
+        for (cudaStream_t cst : chunk_streams) cudaStreamDestroy(cst);
         for (cudaEvent_t e : kev) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -486,7 +489,8 @@ inline unsigned grid_for(uint64_t n, int block) { return static_cast<unsigned>((
 
 // Step kernels for ions [lo, hi) (all ions by default).
 int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_finalize, uint64_t lo = 0,
-                uint64_t hi = ~0ull) {
+                uint64_t hi = ~0ull, cudaStream_t stream = nullptr) {
+    cudaStream_t st = stream ? stream : h->stream;
     const int n_ens = static_cast<int>(h->ens.size());
     if ((h->coll == kCollIPMTable || h->coll == kCollIPMMLP) && h->ipm_nE == 0)
         return fail(ICB_ERR_STATE, "interaction-potential collisions need icb_ipm_configure first");
@@ -548,9 +552,9 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         const dim3 grid(grid_for(en - b, h->block)), block(static_cast<unsigned>(h->block));
         cudaError_t err;
         switch (h->cfg.precision) {
-            case ICB_PREC_FP64: err = launch_step_fp64(h->cfg.integrator, h->coll, h->field_kind, h->magnetic, p, grid, block, h->stream); break;
-            case ICB_PREC_MIXED: err = launch_step_mixed(h->cfg.integrator, h->coll, h->field_kind, h->magnetic, p, grid, block, h->stream); break;
-            default: err = launch_step_hilo(h->cfg.integrator, h->coll, h->field_kind, h->magnetic, p, grid, block, h->stream); break;
+            case ICB_PREC_FP64: err = launch_step_fp64(h->cfg.integrator, h->coll, h->field_kind, h->magnetic, p, grid, block, st); break;
+            case ICB_PREC_MIXED: err = launch_step_mixed(h->cfg.integrator, h->coll, h->field_kind, h->magnetic, p, grid, block, st); break;
+            default: err = launch_step_hilo(h->cfg.integrator, h->coll, h->field_kind, h->magnetic, p, grid, block, st); break;
         }
         ++h->launches;
         if (err == cudaErrorNotSupported)
@@ -1329,6 +1333,11 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
     const uint64_t n = h->n;
     const bool f64 = h->fp64();
     if (!h->copy_stream) ICB_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    while (h->chunk_streams.size() < static_cast<size_t>(n_chunks)) {
+        cudaStream_t cst;
+        ICB_CUDA(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking));
+        h->chunk_streams.push_back(cst);
+    }
     while (h->hev.size() < static_cast<size_t>(2 * n_chunks + 1)) {
         cudaEvent_t e;
         ICB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -1364,24 +1373,28 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
         ICB_CUDA(cudaMemcpyAsync(h->active_stage.p + a, active + a, cnt, cudaMemcpyHostToDevice, cs));
         ICB_CUDA(cudaEventRecord(h->hev[2 * c], cs));
     }
-    // steps of chunk c overlap the copies of the others
+    // steps of chunk c overlap the copies of the others; each chunk runs on
+    // its own stream, so a chunk's blocks fill the SMs while the previous
+    // chunk's last blocks finish
     for (int c = 0; c < n_chunks; ++c) {
         const uint64_t a = lim[static_cast<size_t>(c)], b = lim[static_cast<size_t>(c) + 1], cnt = b - a;
         if (cnt == 0) continue;
         const unsigned g = grid_for(cnt, 256);
-        ICB_CUDA(cudaStreamWaitEvent(s, h->hev[2 * c], 0));
+        cudaStream_t ks = h->chunk_streams[static_cast<size_t>(c)];
+        ICB_CUDA(cudaStreamWaitEvent(ks, h->hev[2 * c], 0));
         if (!f64)
-            for (int k = 0; k < 3; ++k) k_to_float<<<g, 256, 0, s>>>(h->hstage.p + k * n + a, vf[k] + a, cnt);
-        k_flags_update<<<g, 256, 0, s>>>(h->active_stage.p + a, h->flags.p + a, cnt);
+            for (int k = 0; k < 3; ++k) k_to_float<<<g, 256, 0, ks>>>(h->hstage.p + k * n + a, vf[k] + a, cnt);
+        k_flags_update<<<g, 256, 0, ks>>>(h->active_stage.p + a, h->flags.p + a, cnt);
         ICB_CUDA(cudaGetLastError());
-        if (int r = launch_step(h, static_cast<uint32_t>(n_steps), 1, 1, 1, a, b)) return r;
+        if (int r = launch_step(h, static_cast<uint32_t>(n_steps), 1, 1, 1, a, b, ks)) return r;
         if (!f64)
-            for (int k = 0; k < 3; ++k) k_from_float<<<g, 256, 0, s>>>(vf[k] + a, h->hstage.p + k * n + a, cnt);
-        k_flags_out<<<g, 256, 0, s>>>(h->flags.p + a, h->active_stage.p + a, cnt);
+            for (int k = 0; k < 3; ++k) k_from_float<<<g, 256, 0, ks>>>(vf[k] + a, h->hstage.p + k * n + a, cnt);
+        k_flags_out<<<g, 256, 0, ks>>>(h->flags.p + a, h->active_stage.p + a, cnt);
         ICB_CUDA(cudaGetLastError());
         h->launches += f64 ? 2 : 8;
-        ICB_CUDA(cudaEventRecord(h->hev[2 * c + 1], s));
+        ICB_CUDA(cudaEventRecord(h->hev[2 * c + 1], ks));
         ICB_CUDA(cudaStreamWaitEvent(cs, h->hev[2 * c + 1], 0));
+        ICB_CUDA(cudaStreamWaitEvent(s, h->hev[2 * c + 1], 0));   // the clock advance follows every chunk
         for (int k = 0; k < 3; ++k) {
             ICB_CUDA(cudaMemcpyAsync(pos[k] + a, pd[k] + a, cnt * sizeof(double), cudaMemcpyDeviceToHost, cs));
             const double* src = f64 ? vd[k] + a : h->hstage.p + k * n + a;
