@@ -125,9 +125,9 @@ def ensemble_params(domain: dict, sigma_m2: float, dt_s: float, detector_z_m: fl
     L = float(geom.get("length_m", 0.1))
     mix = env.get("gas_mixture", []) or []
     n_mix = len(mix) if len(mix) >= 2 else 0
-    if n_mix > 4:
-        raise ValueError("at most 4 gas mixture components")
-    dens, mass, sig = [0.0] * 4, [0.0] * 4, [0.0] * 4
+    if n_mix > 8:
+        raise ValueError("at most 8 gas mixture components")
+    dens, mass, sig = [0.0] * 8, [0.0] * 8, [0.0] * 8
     if n_mix:
         fsum = sum(float(c.get("mole_fraction", 0.0)) for c in mix)
         norm = fsum if fsum > 0.0 else 1.0

@@ -64,7 +64,7 @@ struct EnsConst {
 // A_i = n_i sigma_i dt, thermal widths and masses per component.  The
 // ensemble's EnsConst carries the totals (A = sum A_i, A mean_th =
 // sum A_i mean_th_i) for the collision clock.
-constexpr int kMaxGas = 4;
+constexpr int kMaxGas = 8;
 struct MixConst {
     int32_t n;
     int32_t pad_;

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define ICB_ABI_VERSION 3
+#define ICB_ABI_VERSION 4
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -109,11 +109,11 @@ typedef struct icb_ensemble_params {
      * (HSSCollisionHandler.cpp:105-249); 0 or 1 = the single gas above. */
     int32_t n_gas;
     int32_t reserved_;
-    double gas_mix_density_m3[4];
-    double gas_mix_mass_kg[4];
-    double gas_mix_sigma_m2[4];
+    double gas_mix_density_m3[8];
+    double gas_mix_mass_kg[8];
+    double gas_mix_sigma_m2[8];
 } icb_ensemble_params;
-#define ICB_MAX_GAS 4
+#define ICB_MAX_GAS 8
 
 typedef struct icb_config {
     int32_t precision;         /* ICB_PREC_* */

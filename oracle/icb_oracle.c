@@ -76,9 +76,9 @@ typedef struct orc_domain {
     double detector_z_m;
     int32_t n_gas;
     int32_t reserved_;
-    double gas_mix_density_m3[4];
-    double gas_mix_mass_kg[4];
-    double gas_mix_sigma_m2[4];
+    double gas_mix_density_m3[8];
+    double gas_mix_mass_kg[8];
+    double gas_mix_sigma_m2[8];
 } orc_domain;
 
 /* ======================================================================
@@ -606,7 +606,7 @@ static int nullcoll_candidate(const gas_consts* G, double v[3], double mi, uint6
 static int mix_candidate(const orc_domain* d, const gas_consts* G, double v[3], double mi, uint64_t seed,
                          uint32_t id, uint32_t step, double* clk, double qstar) {
     const int n = d->n_gas;
-    double A[4], mean[4], sig[4];
+    double A[8], mean[8], sig[8];
     for (int i = 0; i < n; ++i) {
         A[i] = d->gas_mix_density_m3[i] * d->gas_mix_sigma_m2[i] * d->dt_s;
         sig[i] = sqrt(ORC_KB * d->temperature_K / d->gas_mix_mass_kg[i]);
@@ -865,7 +865,7 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
     if (clocked && integrator == 0 && (!clk_next || !clk_start)) return 1;
     if ((collision == 3 || collision == 4 || collision == 5 || collision == 7) && integrator != 0) return 1;
     if (collision == 7 && !g_ehss_atoms) return 1;
-    if (collision == 5 && (d->n_gas < 2 || d->n_gas > 4)) return 1;
+    if (collision == 5 && (d->n_gas < 2 || d->n_gas > 8)) return 1;
     if (collision == 4 && !g_ipm_tab) return 1;
     const gas_consts G = gas_of(d);
     const int64_t n_snap = (snap_every > 0) ? n_steps / snap_every : 0;

@@ -140,8 +140,14 @@ def test_fp64_langevin_trajectories_match_oracle():
     assert r["collisions"] == r["candidates"] > 0.02 * n * steps
 
 
-def test_fp64_gas_mixture_trajectories_match_oracle():
-    """HSS in an N2/He mixture (HSSCollisionHandler.cpp:105-249) against the
+MIX2 = [("N2", 0.79, 150e-20), ("He", 0.21, 60e-20)]
+MIX7 = [("N2", 0.50, 150e-20), ("He", 0.14, 60e-20), ("Ar", 0.10, 130e-20), ("O2", 0.09, 140e-20),
+        ("CO2", 0.07, 190e-20), ("Ne", 0.06, 80e-20), ("H2O", 0.04, 120e-20)]
+
+
+@pytest.mark.parametrize("mix_def", [MIX2, MIX7], ids=["2 gases", "7 gases"])
+def test_fp64_gas_mixture_trajectories_match_oracle(mix_def):
+    """HSS in a gas mixture (HSSCollisionHandler.cpp:105-249) against the
     oracle's restatement with the same Philox streams (the oracle itself is
     checked against the reference handler on CPU): >= 99 % of ions to 1e-9
     after 3000 steps, collision counts within 1 %; mixed precision keeps the
@@ -149,8 +155,7 @@ def test_fp64_gas_mixture_trajectories_match_oracle():
     from icarion_b200 import config as cfg
     from helpers import CONFIG0_DOMAIN, domain_json
     dom = domain_json(CONFIG0_DOMAIN)
-    dom["env"]["gas_mixture"] = [{"species": "N2", "mole_fraction": 0.79, "cross_section_m2": 150e-20},
-                                 {"species": "He", "mole_fraction": 0.21, "cross_section_m2": 60e-20}]
+    dom["env"]["gas_mixture"] = [{"species": g, "mole_fraction": f, "cross_section_m2": c} for g, f, c in mix_def]
     e = cfg.ensemble_params(dom, 150e-20, 5e-10)
     n, steps = 512, 3000
     st0 = config0_ions(n)

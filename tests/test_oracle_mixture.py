@@ -1,8 +1,8 @@
 """HSS gas mixtures (CPU): the oracle's exact null-collision restatement of
 the reference's mixture law (HSSCollisionHandler.cpp:105-249) against the
-reference's own handler (compiled harness) on the same cloud: collision
-fraction within 1.5 %, drift and mean energy within 4 combined standard
-errors."""
+reference's own handler (compiled harness) on the same cloud, with two and
+five components: collision fraction within 1.5 %, drift and mean energy
+within 4 combined standard errors."""
 from __future__ import annotations
 
 import numpy as np
@@ -13,11 +13,14 @@ from helpers import CONFIG0_DOMAIN, config0_ions, domain_json, oracle_state
 from icarion_b200 import config as cfg
 
 MIX = [("N2", 0.79, 150e-20), ("He", 0.21, 60e-20)]
+# five components: the kernel takes up to eight
+MIX5 = [("N2", 0.55, 150e-20), ("He", 0.15, 60e-20), ("Ar", 0.12, 130e-20), ("O2", 0.10, 140e-20),
+        ("CO2", 0.08, 190e-20)]
 
 
-def _mix_ensemble():
+def _mix_ensemble(mix=MIX):
     dom = domain_json(CONFIG0_DOMAIN)
-    dom["env"]["gas_mixture"] = [{"species": s, "mole_fraction": f, "cross_section_m2": c} for s, f, c in MIX]
+    dom["env"]["gas_mixture"] = [{"species": s, "mole_fraction": f, "cross_section_m2": c} for s, f, c in mix]
     return cfg.ensemble_params(dom, 150e-20, 5e-10)
 
 
@@ -30,17 +33,28 @@ def test_mixture_constants_follow_the_loader():
     assert e["gas_mix_sigma_m2"][:2] == [150e-20, 60e-20]
 
 
+def test_eight_components_accepted_nine_rejected():
+    gases = ["N2", "He", "Ar", "O2", "CO2", "Ne", "H2O", "N2", "He"]
+    dom = domain_json(CONFIG0_DOMAIN)
+    dom["env"]["gas_mixture"] = [{"species": g, "mole_fraction": 1.0} for g in gases[:8]]
+    assert cfg.ensemble_params(dom, 150e-20, 5e-10)["n_gas"] == 8
+    dom["env"]["gas_mixture"] = [{"species": g, "mole_fraction": 1.0} for g in gases]
+    with pytest.raises(ValueError):
+        cfg.ensemble_params(dom, 150e-20, 5e-10)
+
+
 @pytest.mark.skipif(not orc.HARNESS.exists(), reason="compiled reference harness not built")
-def test_mixture_oracle_matches_reference_handler():
+@pytest.mark.parametrize("mix_def", [MIX, MIX5], ids=["2 gases", "5 gases"])
+def test_mixture_oracle_matches_reference_handler(mix_def):
     n, steps = 2048, 6000
     st0 = config0_ions(n)
     ref_state = oracle_state(st0)
     ref_state["ccs"] = np.full(n, 150e-20)
-    mix = ",".join(f"{s}:{f}:{c!r}" for s, f, c in MIX)
+    mix = ",".join(f"{s}:{f}:{c!r}" for s, f, c in mix_def)
     rst, rstats, _ = orc.harness_run(ref_state, steps, dict(CONFIG0_DOMAIN, mix=mix), integrator="boris",
                                      collision="hss", dt=5e-10, seed=11, threads=8)
     ost = oracle_state(st0)
-    r = orc.run(_mix_ensemble(), ost, steps, integrator=0, collision=5, seed=11, threads=8)
+    r = orc.run(_mix_ensemble(mix_def), ost, steps, integrator=0, collision=5, seed=11, threads=8)
     f_ref = rstats["collisions"] / (n * steps)
     f_me = r["collisions"] / (n * steps)
     assert abs(f_me / f_ref - 1.0) < 0.015, (f_me, f_ref)
