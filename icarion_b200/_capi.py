@@ -30,6 +30,7 @@ COLLISION_HSS_PLAIN, COLLISION_EHSS = 5, 6
 INSTRUMENT_IMS, INSTRUMENT_FTICR, INSTRUMENT_QUADRUPOLE_RF = 0, 1, 2
 SC_OFF, SC_P3M_ISOLATED, SC_PM_PERIODIC_REF = 0, 1, 2
 STEPPING_EVENTS, STEPPING_PER_STEP = 0, 1
+FLOW_CONSTANT, FLOW_AXIAL_UNIFORM, FLOW_AXIAL_PARABOLIC = 0, 1, 2
 MLP_HIDDEN, MLP_N_PARAMS = 64, 4417
 POS_POINT, POS_GAUSSIAN, POS_UNIFORM_SPHERE, POS_UNIFORM_CYLINDER, POS_UNIFORM_BOX = 0, 1, 2, 3, 4
 VEL_FIXED, VEL_THERMAL = 0, 1
@@ -60,8 +61,9 @@ class EnsembleParams(C.Structure):
         ("temperature_K", C.c_double), ("gas_density_m3", C.c_double), ("gas_mass_kg", C.c_double),
         ("gas_velocity_m_s", D3), ("gas_polarizability_m3", C.c_double), ("sigma_m2", C.c_double),
         ("ipm_bmax_m", C.c_double), ("dt_s", C.c_double), ("detector_z_m", C.c_double),
-        ("n_gas", C.c_int32), ("reserved_", C.c_int32), ("gas_mix_density_m3", C.c_double * 8),
+        ("n_gas", C.c_int32), ("flow_model", C.c_int32), ("gas_mix_density_m3", C.c_double * 8),
         ("gas_mix_mass_kg", C.c_double * 8), ("gas_mix_sigma_m2", C.c_double * 8),
+        ("axial_flow_velocity_m_s", C.c_double), ("axial_flow_max_velocity_m_s", C.c_double),
     ]
 
 

@@ -164,11 +164,26 @@ def ensemble_params(domain: dict, sigma_m2: float, dt_s: float, detector_z_m: fl
         "dt_s": float(dt_s),
         "detector_z_m": float(detector_z_m),
         "n_gas": n_mix,
-        "reserved_": 0,
+        "flow_model": flow_model(env.get("flow_model", "constant")),
         "gas_mix_density_m3": dens,
         "gas_mix_mass_kg": mass,
         "gas_mix_sigma_m2": sig,
+        "axial_flow_velocity_m_s": float(env.get("axial_flow_velocity_m_s", 0.0)),
+        "axial_flow_max_velocity_m_s": float(env.get("axial_flow_max_velocity_m_s", 0.0)),
     }
+
+
+def flow_model(name: str) -> int:
+    """env.flow_model names (EnvironmentConfig::parse_flow_model,
+    EnvironmentConfig.h:81-94) -> ICB_FLOW_*."""
+    key = str(name).lower()
+    if key in ("constant", "legacy"):
+        return capi.FLOW_CONSTANT
+    if key in ("axial_uniform", "uniform", "axial_const"):
+        return capi.FLOW_AXIAL_UNIFORM
+    if key in ("axial_parabolic", "parabolic", "poiseuille"):
+        return capi.FLOW_AXIAL_PARABOLIC
+    raise ValueError(f"unknown flow_model '{name}'")
 
 
 def to_struct(p: dict) -> capi.EnsembleParams:

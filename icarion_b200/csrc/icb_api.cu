@@ -459,7 +459,25 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
         C.sig_n = std::sqrt(kBoltzmann * P.temperature_K / P.gas_mass_kg);
         C.mean_th = C.sig_n * kMeanChi3;
         C.m_gas = P.gas_mass_kg;
+        // gas flow (EnvironmentConfig::gas_velocity_at): constant vectors here,
+        // the parabolic profile per ion in the kernel
+        if (P.flow_model != ICB_FLOW_CONSTANT && P.flow_model != ICB_FLOW_AXIAL_UNIFORM &&
+            P.flow_model != ICB_FLOW_AXIAL_PARABOLIC)
+            return fail(ICB_ERR_INVALID_ARGUMENT, "unknown flow_model %d", P.flow_model);
+        if (P.flow_model == ICB_FLOW_AXIAL_UNIFORM && !(P.axial_flow_velocity_m_s >= 0.0))
+            return fail(ICB_ERR_INVALID_ARGUMENT, "axial_flow_velocity_m_s must be >= 0 for axial_uniform flow");
+        if (P.flow_model == ICB_FLOW_AXIAL_PARABOLIC && !(P.axial_flow_max_velocity_m_s >= 0.0))
+            return fail(ICB_ERR_INVALID_ARGUMENT,
+                        "axial_flow_max_velocity_m_s must be >= 0 for axial_parabolic flow");
         for (int a = 0; a < 3; ++a) C.ug[a] = P.gas_velocity_m_s[a];
+        if (P.flow_model == ICB_FLOW_AXIAL_UNIFORM) {
+            C.ug[0] = 0.0; C.ug[1] = 0.0; C.ug[2] = P.axial_flow_velocity_m_s;
+        } else if (P.flow_model == ICB_FLOW_AXIAL_PARABOLIC) {
+            C.ug[0] = 0.0; C.ug[1] = 0.0; C.ug[2] = 0.0;
+            C.flow = 1;
+            C.flow_umax = P.axial_flow_max_velocity_m_s;
+            C.flow_r2 = P.radius_m * P.radius_m;
+        }
         C.fA = static_cast<float>(C.A);
         C.fmean_th = static_cast<float>(C.mean_th);
         C.fsig_n = static_cast<float>(C.sig_n);
@@ -548,7 +566,10 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.n_ens = static_cast<uint32_t>(ne);
         p.do_push = do_push; p.do_collide = do_collide; p.do_finalize = do_finalize;
         for (int e = 0; e <= ne; ++e) p.ens_off[e] = clip(h->ens_off[static_cast<size_t>(e0 + e)]);
-        for (int e = 0; e < ne; ++e) p.ens[e] = h->ens_const[static_cast<size_t>(e0 + e)];
+        for (int e = 0; e < ne; ++e) {
+            p.ens[e] = h->ens_const[static_cast<size_t>(e0 + e)];
+            if (p.ens[e].flow) p.flows = 1u;
+        }
         const dim3 grid(grid_for(en - b, h->block)), block(static_cast<unsigned>(h->block));
         cudaError_t err;
         switch (h->cfg.precision) {

@@ -52,12 +52,15 @@ struct EnsConst {
     // Langevin capture: per-step event probability parameter
     // lambda_i = lang_c |q_i| / sqrt(mu_i)
     double lang_c;
+    // parabolic axial gas flow (flow != 0): u_z = flow_umax max(0, 1 - r^2 /
+    // flow_r2) at the ion; ug is then zero and refreshed at each collision
+    double flow_umax, flow_r2;
     int32_t magnetic;
     int32_t rf;
     // float copies for the float collision path
     float fA, fmean_th, fsig_n, fm_gas;
     float fug[3];
-    float pad_;
+    int32_t flow;
 };
 
 // HSS gas mixture of one ensemble (read by the candidate step only):
@@ -129,6 +132,7 @@ struct StepParams {
     uint32_t n_ens;
     uint32_t do_push, do_collide, do_finalize, steps_per_vote;
     uint32_t jumps;                    // event-to-event drift where the kernel supports it
+    uint32_t flows;                    // some ensemble of the launch has a parabolic gas flow
     uint64_t ens_off[kMaxLaunchEns + 1];  // absolute ion offsets of the chunk's ensembles
     EnsConst ens[kMaxLaunchEns];
 };

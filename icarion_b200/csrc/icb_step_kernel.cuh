@@ -614,6 +614,8 @@ __device__ void ehss_scatter(const StepParams& p, uint32_t eg, R v[3], const R v
     }
 }
 
+// A parabolic-flow ensemble (C.flow) calls this with v in the local gas
+// frame (v_z - u_z at the ion) and C.ug = 0.
 template <class R, bool SKIP, int COLL>
 __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qstar, R Amean, R b, double mi_d,
                                          const uint32_t* rk, uint32_t id, uint32_t step, const StepParams& p,
@@ -835,7 +837,7 @@ __device__ __forceinline__ int candidate_mix(const EnsConst& C, const MixConst& 
 // measured against; returns true on a collision.
 template <class R>
 __device__ __forceinline__ bool plain_hss(const EnsConst& C, R v[3], double mi_d, const uint32_t* rk, uint32_t id,
-                                          uint32_t step) {
+                                          uint32_t step, R ugz) {
     const U4 a = philox4x32_10_rk(id, step, 0u, 0u, rk);
     const U4 b = philox4x32_10_rk(id, step, 1u, 0u, rk);
     const R sn = static_cast<R>(C.sig_n);
@@ -845,7 +847,8 @@ __device__ __forceinline__ bool plain_hss(const EnsConst& C, R v[3], double mi_d
     for (int c = 0; c < 3; ++c) {
         R cs, ss;
         angle_cs(u32(w2[c], R(0)), cs, ss);
-        vn[c] = static_cast<R>(C.ug[c]) + sn * (m_sqrt(R(-2.0) * m_log(u32(w1[c], R(0)))) * cs);
+        const R u = (C.flow && c == 2) ? ugz : static_cast<R>(C.ug[c]);
+        vn[c] = u + sn * (m_sqrt(R(-2.0) * m_log(u32(w1[c], R(0)))) * cs);
     }
     const R gx = v[0] - vn[0], gy = v[1] - vn[1], gz = v[2] - vn[2];
     const R g = m_sqrt(gx * gx + gy * gy + gz * gz);
@@ -1004,6 +1007,7 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
         if (in_range) { g_next = p.clk_next[i]; g_start = p.clk_start[i]; }
         dvmax = static_cast<R>(fabs(k.qm) * static_cast<R>(C.Emax) * static_cast<R>(C.dt));
         absu = m_sqrt(k.ug[0] * k.ug[0] + k.ug[1] * k.ug[1] + k.ug[2] * k.ug[2]);
+        if (C.flow) absu = static_cast<R>(C.flow_umax);   // |u(x)| <= u_max
         // horizon minimising the majorant's excess plus refreshes: 1/sqrt(A dv)
         R hz = R(1) / m_sqrt(k.A * dvmax);
         if (!(hz < R(4096))) hz = R(4096);
@@ -1041,6 +1045,15 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
     R acc = R(0), lim = R(0);
 
     auto t_step = [&]() -> double { return kAccumT ? t : fma(static_cast<double>(kk), dt, t0); };
+    // z component of the parabolic gas flow at the ion
+    // (EnvironmentConfig::gas_velocity_at, EnvironmentConfig.h:115-125)
+    auto flow_z = [&]() -> R {
+        if (!C.flow) return R(0);
+        const double lx = x.gx() - C.ox, ly = x.gy() - C.oy;
+        const double r2 = lx * lx + ly * ly;
+        const double rr = (C.flow_r2 > 0.0) ? r2 / C.flow_r2 : 0.0;
+        return static_cast<R>(C.flow_umax * fmax(0.0, 1.0 - rr));
+    };
     auto kill = [&](double when) {
         flags &= static_cast<uint8_t>(~kFlagActive);
         tdeath = when;
@@ -1117,12 +1130,16 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
     auto collide_at = [&](bool has_ev, uint32_t gs) {
         IpmPend<R> ip;
         bool need_net = false;
+        // a parabolic flow is handled in the local gas frame: v_z - u_z(x)
+        // during the candidate, u_z added back afterwards (x is unchanged)
+        bool shifted = false;
         if (has_ev) {
             if constexpr (kSkip) {
                 if (g_next & kRefresh) {
                     // horizon end without an event: consume its steps
                     S = S - static_cast<R>(gs + 1u - g_start) * lam;
                 } else {
+                    if (p.flows && C.flow) { v[2] = v[2] - flow_z(); shifted = true; }
                     int st;
                     if constexpr (COLL == kCollHSSMix)
                         st = candidate_mix<R, true>(C, p.mix[p.ens_base + e], v, S, U, k.Amean, b, m, p.rk, id, gs);
@@ -1133,6 +1150,7 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
                     need_net = st == 3;
                 }
             } else {
+                if (p.flows && C.flow) { v[2] = v[2] - flow_z(); shifted = true; }
                 ++n_cand;
                 int st;
                 if constexpr (COLL == kCollHSSMix)
@@ -1164,6 +1182,7 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
                 }
             }
         }
+        if (shifted) v[2] = v[2] + flow_z();
         if (has_ev) {
             if constexpr (kSkip) {
                 clock_restart(gs + 1u);
@@ -1194,10 +1213,13 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
         } else if constexpr (COLL == kCollHSSPlain) {
             if (do_coll) {
                 ++n_cand;
-                if (plain_hss<R>(C, v, m, p.rk, id, step0 + kk)) ++n_coll;
+                if (plain_hss<R>(C, v, m, p.rk, id, step0 + kk, flow_z())) ++n_coll;
             }
         } else if constexpr (COLL != kCollNone) {
-            if (do_coll) cand = clock_tick<R>(k, v, S, U, b, cb, n_ovf);
+            if (do_coll) {
+                if (p.flows && C.flow) k.ug[2] = flow_z();
+                cand = clock_tick<R>(k, v, S, U, b, cb, n_ovf);
+            }
         }
         // A collision candidate or an exhausted displacement budget stops the
         // lane at this step; both are handled in the warp's deferred phase,

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define ICB_ABI_VERSION 4
+#define ICB_ABI_VERSION 5
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -108,11 +108,19 @@ typedef struct icb_ensemble_params {
      * gas_mass_kg / sigma_m2 above for HSS collisions
      * (HSSCollisionHandler.cpp:105-249); 0 or 1 = the single gas above. */
     int32_t n_gas;
-    int32_t reserved_;
+    int32_t flow_model;        /* ICB_FLOW_* (env.flow_model, EnvironmentConfig.h:81-128) */
     double gas_mix_density_m3[8];
     double gas_mix_mass_kg[8];
     double gas_mix_sigma_m2[8];
+    /* Gas flow profile: CONSTANT uses gas_velocity_m_s; AXIAL_UNIFORM
+     * (0, 0, axial_flow_velocity_m_s); AXIAL_PARABOLIC u_z =
+     * axial_flow_max_velocity_m_s * max(0, 1 - r^2/R^2), r the distance
+     * from the cylinder axis, R = radius_m, at the ion's position when it
+     * collides (SimulationEngineCollisionRuntime.cpp:124-131). */
+    double axial_flow_velocity_m_s;
+    double axial_flow_max_velocity_m_s;
 } icb_ensemble_params;
+enum { ICB_FLOW_CONSTANT = 0, ICB_FLOW_AXIAL_UNIFORM = 1, ICB_FLOW_AXIAL_PARABOLIC = 2 };
 #define ICB_MAX_GAS 8
 
 typedef struct icb_config {

@@ -75,11 +75,31 @@ typedef struct orc_domain {
     double dt_s;
     double detector_z_m;
     int32_t n_gas;
-    int32_t reserved_;
+    int32_t flow_model;        /* 0 constant, 1 axial uniform, 2 axial parabolic */
     double gas_mix_density_m3[8];
     double gas_mix_mass_kg[8];
     double gas_mix_sigma_m2[8];
+    double axial_flow_velocity_m_s;
+    double axial_flow_max_velocity_m_s;
 } orc_domain;
+
+/* Gas flow velocity at global position p (EnvironmentConfig::gas_velocity_at,
+ * EnvironmentConfig.h:96-128, for an unrotated cylinder): the constant
+ * vector, (0, 0, u) for the axial uniform profile, and u_z = u_max
+ * max(0, 1 - r^2/R^2) for the parabolic one, r measured from the axis. */
+static void gas_flow_at(const orc_domain* d, const double p[3], double ug[3]) {
+    if (d->flow_model == 1) {
+        ug[0] = 0.0; ug[1] = 0.0; ug[2] = d->axial_flow_velocity_m_s;
+    } else if (d->flow_model == 2) {
+        const double lx = p[0] - d->origin_m[0], ly = p[1] - d->origin_m[1];
+        const double r2 = lx * lx + ly * ly;
+        const double R2 = d->radius_m * d->radius_m;
+        const double rr = (R2 > 0.0) ? r2 / R2 : 0.0;
+        ug[0] = 0.0; ug[1] = 0.0; ug[2] = d->axial_flow_max_velocity_m_s * fmax(0.0, 1.0 - rr);
+    } else {
+        ug[0] = d->gas_velocity_m_s[0]; ug[1] = d->gas_velocity_m_s[1]; ug[2] = d->gas_velocity_m_s[2];
+    }
+}
 
 /* ======================================================================
  * mt19937_64 (Matsumoto & Nishimura, ACM TOMACS 2000; 64-bit variant of
@@ -294,14 +314,16 @@ static void rk4_step(const orc_domain* d, double x[3], double v[3], double m, do
  * Collisions
  * ==================================================================== */
 /* Reference HSS, single gas (HSSCollisionHandler.cpp:257-376). */
-static int hss_reference(const orc_domain* d, double v[3], double mi, orc_mt64* rng) {
+static int hss_reference(const orc_domain* d, const double p[3], double v[3], double mi, orc_mt64* rng) {
     double sig_n = sqrt(ORC_KB * d->temperature_K / d->gas_mass_kg);
     double vn[3];
     for (int c = 0; c < 3; ++c) {
         double u1 = mt64_uniform01(rng), u2 = mt64_uniform01(rng);
         vn[c] = sig_n * sqrt(-2.0 * log(u1)) * cos(2.0 * M_PI * u2);
     }
-    for (int c = 0; c < 3; ++c) vn[c] = vn[c] + d->gas_velocity_m_s[c];
+    double ug[3];
+    gas_flow_at(d, p, ug);
+    for (int c = 0; c < 3; ++c) vn[c] = vn[c] + ug[c];
     double vr[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
     double g = sqrt(vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]);
     if (g < ORC_MIN_REL_VEL) return 0;
@@ -367,7 +389,10 @@ static gas_consts gas_of(const orc_domain* d) {
     g.mean_th = g.sig_n * 1.5957691216057308;   /* E|th| = sigma*2*sqrt(2/pi) */
     g.A = d->gas_density_m3 * d->sigma_m2 * d->dt_s;
     g.Amean = g.A * g.mean_th;
-    for (int c = 0; c < 3; ++c) g.ug[c] = d->gas_velocity_m_s[c];
+    /* position-independent flows; the parabolic profile is set per collision */
+    const double p0[3] = {0.0, 0.0, 0.0};
+    gas_flow_at(d, p0, g.ug);
+    if (d->flow_model == 2) g.ug[2] = 0.0;
     return g;
 }
 
@@ -709,16 +734,21 @@ static int plain_hss(const gas_consts* G, double v[3], double mi, uint64_t seed,
 }
 
 /* Per-step clock (RK4). */
-static int hss_nullcoll(const orc_domain* d, double v[3], double mi, uint64_t seed, uint32_t id,
+static int hss_nullcoll(const orc_domain* d, const double p[3], double v[3], double mi, uint64_t seed, uint32_t id,
                         uint32_t step, double* S, double* U, uint64_t* overflow) {
     const gas_consts G = gas_of(d);
-    double w[3] = {v[0] - G.ug[0], v[1] - G.ug[1], v[2] - G.ug[2]};
+    double ul[3];
+    gas_flow_at(d, p, ul);
+    double w[3] = {v[0] - ul[0], v[1] - ul[1], v[2] - ul[2]};
     double gu = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
     double Q = G.A * gu + G.Amean;
     if (Q > 1.0) { Q = 1.0; ++*overflow; }
     *S = *S - *S * Q;
     if (!(*S < *U)) return -1;
+    /* a parabolic flow: the candidate runs in the local gas frame */
+    if (d->flow_model == 2) v[2] = v[2] - ul[2];
     const int r = nullcoll_candidate(&G, v, mi, seed, id, step, 0, U, 0.0, gu, 0);
+    if (d->flow_model == 2) v[2] = v[2] + ul[2];
     *S = 1.0;
     return r;
 }
@@ -781,6 +811,7 @@ static void skip_setup(skip_clock* k, const orc_domain* d, const gas_consts* G, 
     const double qm = q / m;
     k->dvmax = fabs(qm) * orc_field_bound(d) * d->dt_s;
     k->absu = sqrt(G->ug[0] * G->ug[0] + G->ug[1] * G->ug[1] + G->ug[2] * G->ug[2]);
+    if (d->flow_model == 2) k->absu = d->axial_flow_max_velocity_m_s;   /* |u(x)| <= u_max */
     double hz = 1.0 / sqrt(G->A * k->dvmax);
     if (!(hz < 4096.0)) hz = 4096.0;
     if (hz < 16.0) hz = 16.0;
@@ -938,10 +969,12 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                     if (integrator == 0) boris_step(d, p, v, m, q, t, dt);
                     else rk4_step(d, p, v, m, q, t, dt);
                     if (collision == 6) {
+                        gas_consts Gp = Gi;
+                        gas_flow_at(d, p, Gp.ug);            /* flow at the ion after the push */
                         ++cand_tot;
-                        coll_tot += (uint64_t)plain_hss(&G, v, m, seed, id, (uint32_t)(step0 + (uint64_t)k));
+                        coll_tot += (uint64_t)plain_hss(&Gp, v, m, seed, id, (uint32_t)(step0 + (uint64_t)k));
                     } else if (collision == 1) {
-                        coll_tot += (uint64_t)hss_reference(d, v, m, rng);
+                        coll_tot += (uint64_t)hss_reference(d, p, v, m, rng);
                     } else if (skip) {
                         const uint32_t gs = (uint32_t)(step0 + (uint64_t)k);
                         if (sk.next != ORC_NEED_RESTART && gs == (sk.next & ~ORC_REFRESH)) {
@@ -949,10 +982,20 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                             if (sk.next & ORC_REFRESH) {
                                 sk.tau = sk.tau - (double)(gs + 1u - sk.start) * sk.lam;
                             } else {
+                                /* a parabolic flow: the candidate runs in the local gas frame */
+                                double ul[3];
+                                if (d->flow_model == 2) {
+                                    gas_flow_at(d, p, ul);
+                                    v[2] = v[2] - ul[2];
+                                }
                                 int r = (collision == 5)
                                     ? mix_candidate(d, &Gi, v, m, seed, id, gs, &sk.tau, sk.qstar)
                                     : nullcoll_candidate(&Gi, v, m, seed, id, gs, 1, &sk.tau, sk.qstar, 0.0,
                                                          collision == 3 ? 1 : (collision == 4 ? 2 : (collision == 7 ? 3 : 0)));
+                                if (d->flow_model == 2) {
+                                    gas_flow_at(d, p, ul);
+                                    v[2] = v[2] + ul[2];
+                                }
                                 if (r >= 1) ++cand_tot;
                                 if (r == 2) ++coll_tot;
                             }
@@ -961,7 +1004,7 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                         }
                     } else if (collision == 2) {
                         uint64_t ov = 0;
-                        int r = hss_nullcoll(d, v, m, seed, id, (uint32_t)(step0 + (uint64_t)k), &S, &U, &ov);
+                        int r = hss_nullcoll(d, p, v, m, seed, id, (uint32_t)(step0 + (uint64_t)k), &S, &U, &ov);
                         ovf_tot += ov;
                         if (r >= 1) ++cand_tot;
                         if (r == 2) ++coll_tot;

@@ -129,6 +129,10 @@ config::DomainConfig make_domain(const Args& a) {
         d.environment.gas_mixture.push_back(comp);
         pos = end + 1;
     }
+    // gas flow profile (EnvironmentConfig::flow_model; DomainConfigLoader.cpp:204-212)
+    if (a.count("flow_model")) d.environment.flow_model = config::EnvironmentConfig::parse_flow_model(str(a, "flow_model", ""));
+    d.environment.axial_flow_velocity_m_s = num(a, "axial_flow_velocity", 0.0);
+    d.environment.axial_flow_max_velocity_m_s = num(a, "axial_flow_max_velocity", 0.0);
     d.environment.compute_derived_properties();
     if (a.count("EN_Td")) {
         const double EN_Td = num(a, "EN_Td", 0.0);
@@ -338,6 +342,17 @@ int mode_run(const Args& a) {
     std::vector<double> mom(static_cast<size_t>(n_snap * 20), 0.0);
     std::vector<double> rx(px, px + n), ry(py, py + n), rz(pz, pz + n);
     uint64_t collisions = 0;
+    // the collision environment of ion i: the reference engine evaluates a
+    // non-constant gas flow at the ion's position before each collision
+    // (SimulationEngineCollisionRuntime.cpp:124-131; unrotated cylinder)
+    const bool flow_var = d.environment.flow_model != config::FlowModelKind::Constant;
+    auto env_at = [&](int64_t i) -> const config::EnvironmentConfig& {
+        if (!flow_var) return d.environment;
+        thread_local config::EnvironmentConfig local_env;
+        local_env = d.environment;
+        local_env.gas_velocity_m_s = d.environment.gas_velocity_at(Vec3{px[i], py[i], pz[i]}, &d.geometry);
+        return local_env;
+    };
 
     double t = num(a, "t0", 0.0);
     const auto wall0 = std::chrono::steady_clock::now();
@@ -361,7 +376,7 @@ int mode_run(const Args& a) {
                 for (int64_t i = 0; i < n; ++i) {
                     if (!active[i]) continue;
                     auto cv = ens.collision_data(static_cast<size_t>(i));
-                    collisions += hss.handle_collision(cv, dt, rng[static_cast<size_t>(i)], d.environment) ? 1 : 0;
+                    collisions += hss.handle_collision(cv, dt, rng[static_cast<size_t>(i)], env_at(i)) ? 1 : 0;
                 }
             }
         } else if (faithful) {
@@ -373,7 +388,7 @@ int mode_run(const Args& a) {
                 for (int64_t i = 0; i < n; ++i) {
                     if (!active[i]) continue;
                     auto cv = ens.collision_data(static_cast<size_t>(i));
-                    collisions += hss.handle_collision(cv, dt, rng[static_cast<size_t>(i)], d.environment) ? 1 : 0;
+                    collisions += hss.handle_collision(cv, dt, rng[static_cast<size_t>(i)], env_at(i)) ? 1 : 0;
                 }
             }
         } else {
@@ -384,7 +399,7 @@ int mode_run(const Args& a) {
                 boris.step(ens, static_cast<size_t>(i), t, dt, *reg);
                 if (coll == "hss") {
                     auto cv = ens.collision_data(static_cast<size_t>(i));
-                    collisions += hss.handle_collision(cv, dt, rng[static_cast<size_t>(i)], d.environment) ? 1 : 0;
+                    collisions += hss.handle_collision(cv, dt, rng[static_cast<size_t>(i)], env_at(i)) ? 1 : 0;
                 }
             }
         }

@@ -178,6 +178,40 @@ def test_fp64_gas_mixture_trajectories_match_oracle(mix_def):
     assert abs(dzm.mean() - dz64.mean()) <= 4 * dz64.std() / np.sqrt(8192)
 
 
+@pytest.mark.parametrize("model", ["axial_parabolic", "axial_uniform"])
+def test_fp64_gas_flow_trajectories_match_oracle(model):
+    """Gas flow evaluated at the colliding ion (EnvironmentConfig.h:96-128;
+    the oracle itself is checked against the reference's flow and handler on
+    CPU): FP64 device vs oracle >= 99 % of ions to 1e-9 after 3000 steps,
+    collision counts within 1 %; the float forms keep the collision
+    fraction within 1 % and the mean drift within 4 standard errors."""
+    from test_oracle_flow import CASES, flow_ensemble
+    e = flow_ensemble(model, CASES[model][0])
+    n, steps = 512, 3000
+    st0 = config0_ions(n)
+    ost = oracle_state(st0)
+    r = orc.run(e, ost, steps, integrator=0, collision=2, seed=123)
+    out, rs = _hss_gpu(st0, e, steps)
+    live = (ost["active"] != 0) & (out.active != 0)
+    assert live.sum() > 0.8 * n and np.array_equal(ost["active"] != 0, out.active != 0)
+    pos = np.stack([out.x, out.y, out.z])[:, live]
+    opos = np.stack([ost["x"], ost["y"], ost["z"]])[:, live]
+    vel = np.stack([out.vx, out.vy, out.vz])[:, live]
+    ovel = np.stack([ost["vx"], ost["vy"], ost["vz"]])[:, live]
+    rel = np.maximum(np.linalg.norm(pos - opos, axis=0) / np.linalg.norm(opos, axis=0),
+                     np.linalg.norm(vel - ovel, axis=0) / np.linalg.norm(ovel, axis=0))
+    assert float(np.mean(rel < 1e-9)) >= 0.99, np.sort(rel)[-5:]
+    assert abs(rs["collisions"] - r["collisions"]) <= 0.01 * r["collisions"]
+    st1 = config0_ions(8192)
+    f64, r64 = _hss_gpu(st1, e, steps)
+    for prec in (capi.PREC_MIXED, capi.PREC_MIXED_HILO):
+        mix, rmx = _hss_gpu(st1, e, steps, precision=prec)
+        assert abs(rmx["collisions"] / r64["collisions"] - 1.0) < 0.01
+        a64, am = f64.active != 0, mix.active != 0
+        dz64, dzm = (f64.z - st1.z)[a64], (mix.z - st1.z)[am]
+        assert abs(dzm.mean() - dz64.mean()) <= 4 * dz64.std() / np.sqrt(dz64.size)
+
+
 def test_fp64_plain_form_matches_oracle():
     """The plain per-step HSS form (the bench's plain FP64 baseline) against
     the oracle with the same Philox words: >= 99 % of ions to 1e-9 after
