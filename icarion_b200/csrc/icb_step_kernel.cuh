@@ -1008,8 +1008,11 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
         dvmax = static_cast<R>(fabs(k.qm) * static_cast<R>(C.Emax) * static_cast<R>(C.dt));
         absu = m_sqrt(k.ug[0] * k.ug[0] + k.ug[1] * k.ug[1] + k.ug[2] * k.ug[2]);
         if (C.flow) absu = static_cast<R>(C.flow_umax);   // |u(x)| <= u_max
-        // horizon minimising the majorant's excess plus refreshes: 1/sqrt(A dv)
-        R hz = R(1) / m_sqrt(k.A * dvmax);
+        // Horizon: a longer one thins more events (the majorant's excess
+        // A H dv), a shorter one refreshes more often.  With a thinned event
+        // costing about four refreshes, H = 1 / (2 sqrt(A dv)) balances them
+        // (4 % faster than 1 / sqrt(A dv) at 20 Td, measured).
+        R hz = R(0.5) / m_sqrt(k.A * dvmax);
         if (!(hz < R(4096))) hz = R(4096);
         if (hz < R(16)) hz = R(16);
         H = static_cast<uint32_t>(hz);

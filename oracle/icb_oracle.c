@@ -812,7 +812,7 @@ static void skip_setup(skip_clock* k, const orc_domain* d, const gas_consts* G, 
     k->dvmax = fabs(qm) * orc_field_bound(d) * d->dt_s;
     k->absu = sqrt(G->ug[0] * G->ug[0] + G->ug[1] * G->ug[1] + G->ug[2] * G->ug[2]);
     if (d->flow_model == 2) k->absu = d->axial_flow_max_velocity_m_s;   /* |u(x)| <= u_max */
-    double hz = 1.0 / sqrt(G->A * k->dvmax);
+    double hz = 0.5 / sqrt(G->A * k->dvmax);   /* the product's horizon */
     if (!(hz < 4096.0)) hz = 4096.0;
     if (hz < 16.0) hz = 16.0;
     k->H = (uint32_t)hz;

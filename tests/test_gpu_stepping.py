@@ -135,9 +135,8 @@ def test_short_launches_check_every_step():
 
 
 def test_every_ion_of_a_large_cloud_is_advanced():
-    """300,000 ions: more than the resident grid's threads, so threads move
-    on to further ions.  Every ion moves, and the states follow the
-    step-by-step loop (one thread per ion)."""
+    """300,000 ions (about 2.6 waves of resident blocks): every ion moves, and
+    the event form follows the step-by-step loop."""
     e = config0_ensemble()
     st0 = config0_ions(300_000)
     ev, rs_ev = _run(e, st0, 400, capi.PREC_MIXED, capi.STEPPING_EVENTS)
@@ -150,7 +149,8 @@ def test_every_ion_of_a_large_cloud_is_advanced():
 
 def test_births_follow_step_by_step():
     """Unborn ions wait unmoved until the first step whose start time reaches
-    their birth time, then step; the event form jumps to that step."""
+    their birth time, then step (a warp with an unborn ion takes the
+    step-by-step loop in both stepping modes)."""
     e = config0_ensemble()
     n = 4096
     st = config0_ions(n)
