@@ -676,7 +676,7 @@ def main():
     ap.add_argument("--graphs", action="store_true", help="replay icb_advance through CUDA graphs")
     ap.add_argument("--fp64-steps", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=20)
-    ap.add_argument("--e2e-chunks", type=int, default=16, help="ion chunks of the overlapped host path")
+    ap.add_argument("--e2e-chunks", type=int, default=24, help="ion chunks of the overlapped host path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

@@ -307,9 +307,9 @@ struct icb_handle {
     DevBuf<int32_t> ehss_off;
     DevBuf<double> ehss_rgas;
     bool mlp_ready = false;
-    // host fast path: copy stream, per-chunk compute streams and events,
-    // velocity staging (3n)
-    cudaStream_t copy_stream = nullptr;
+    // host fast path: copy and copy-back streams, per-chunk compute streams
+    // and events, velocity staging (3n)
+    cudaStream_t copy_stream = nullptr, copy_back_stream = nullptr;
     std::vector<cudaStream_t> chunk_streams;
     std::vector<cudaEvent_t> hev;
     DevBuf<double> hstage;
@@ -330,6 +330,7 @@ struct icb_handle {
         for (cudaEvent_t e : sc_ev) cudaEventDestroy(e);
         for (cudaEvent_t e : hev) cudaEventDestroy(e);
         if (copy_stream) cudaStreamDestroy(copy_stream);
+        if (copy_back_stream) cudaStreamDestroy(copy_back_stream);
         for (cudaStream_t cst : chunk_streams) cudaStreamDestroy(cst);
         for (cudaEvent_t e : kev) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
@@ -1354,6 +1355,7 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
     const uint64_t n = h->n;
     const bool f64 = h->fp64();
     if (!h->copy_stream) ICB_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    if (!h->copy_back_stream) ICB_CUDA(cudaStreamCreateWithFlags(&h->copy_back_stream, cudaStreamNonBlocking));
     while (h->chunk_streams.size() < static_cast<size_t>(n_chunks)) {
         cudaStream_t cst;
         ICB_CUDA(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking));
@@ -1365,7 +1367,7 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
         h->hev.push_back(e);
     }
     if (!f64 && h->hstage.n < 3 * n) ICB_CUDA(h->hstage.alloc(3 * n));
-    cudaStream_t s = h->stream, cs = h->copy_stream;
+    cudaStream_t s = h->stream, cs = h->copy_stream, bs = h->copy_back_stream;
     double* pos[3] = {x, y, z};
     double* vel[3] = {vx, vy, vz};
     double* pd[3] = {h->x.p, h->y.p, h->z.p};
@@ -1382,9 +1384,12 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
     ICB_CUDA(cudaEventRecord(h->ev0, s));
     ICB_CUDA(cudaEventRecord(h->hev[2 * n_chunks], s));
     ICB_CUDA(cudaStreamWaitEvent(cs, h->hev[2 * n_chunks], 0));   // earlier work on the state is done
-    // inputs of every chunk on the copy stream
+    // Chunk by chunk: inputs on the copy stream, steps on the chunk's own
+    // stream (so a chunk's blocks fill the SMs while the previous chunk's
+    // last blocks finish), results on the copy-back stream.  Queued in chunk
+    // order, the first chunk's steps start as soon as its inputs are in.
     for (int c = 0; c < n_chunks; ++c) {
-        const uint64_t a = lim[static_cast<size_t>(c)], cnt = lim[static_cast<size_t>(c) + 1] - a;
+        const uint64_t a = lim[static_cast<size_t>(c)], b = lim[static_cast<size_t>(c) + 1], cnt = b - a;
         if (cnt == 0) continue;
         for (int k = 0; k < 3; ++k) {
             ICB_CUDA(cudaMemcpyAsync(pd[k] + a, pos[k] + a, cnt * sizeof(double), cudaMemcpyHostToDevice, cs));
@@ -1393,13 +1398,6 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
         }
         ICB_CUDA(cudaMemcpyAsync(h->active_stage.p + a, active + a, cnt, cudaMemcpyHostToDevice, cs));
         ICB_CUDA(cudaEventRecord(h->hev[2 * c], cs));
-    }
-    // steps of chunk c overlap the copies of the others; each chunk runs on
-    // its own stream, so a chunk's blocks fill the SMs while the previous
-    // chunk's last blocks finish
-    for (int c = 0; c < n_chunks; ++c) {
-        const uint64_t a = lim[static_cast<size_t>(c)], b = lim[static_cast<size_t>(c) + 1], cnt = b - a;
-        if (cnt == 0) continue;
         const unsigned g = grid_for(cnt, 256);
         cudaStream_t ks = h->chunk_streams[static_cast<size_t>(c)];
         ICB_CUDA(cudaStreamWaitEvent(ks, h->hev[2 * c], 0));
@@ -1414,21 +1412,21 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
         ICB_CUDA(cudaGetLastError());
         h->launches += f64 ? 2 : 8;
         ICB_CUDA(cudaEventRecord(h->hev[2 * c + 1], ks));
-        ICB_CUDA(cudaStreamWaitEvent(cs, h->hev[2 * c + 1], 0));
+        ICB_CUDA(cudaStreamWaitEvent(bs, h->hev[2 * c + 1], 0));
         ICB_CUDA(cudaStreamWaitEvent(s, h->hev[2 * c + 1], 0));   // the clock advance follows every chunk
         for (int k = 0; k < 3; ++k) {
-            ICB_CUDA(cudaMemcpyAsync(pos[k] + a, pd[k] + a, cnt * sizeof(double), cudaMemcpyDeviceToHost, cs));
+            ICB_CUDA(cudaMemcpyAsync(pos[k] + a, pd[k] + a, cnt * sizeof(double), cudaMemcpyDeviceToHost, bs));
             const double* src = f64 ? vd[k] + a : h->hstage.p + k * n + a;
-            ICB_CUDA(cudaMemcpyAsync(vel[k] + a, src, cnt * sizeof(double), cudaMemcpyDeviceToHost, cs));
+            ICB_CUDA(cudaMemcpyAsync(vel[k] + a, src, cnt * sizeof(double), cudaMemcpyDeviceToHost, bs));
         }
-        ICB_CUDA(cudaMemcpyAsync(active + a, h->active_stage.p + a, cnt, cudaMemcpyDeviceToHost, cs));
+        ICB_CUDA(cudaMemcpyAsync(active + a, h->active_stage.p + a, cnt, cudaMemcpyDeviceToHost, bs));
     }
     const int ne = static_cast<int>(h->ens.size());
     k_clock_advance<<<(ne + 127) / 128, 128, 0, s>>>(h->step_dev.p, h->t_dev.p, h->dt_dev.p, ne,
                                                       static_cast<uint32_t>(n_steps));
     ICB_CUDA(cudaGetLastError());
     ++h->launches;
-    ICB_CUDA(cudaEventRecord(h->hev[2 * n_chunks], cs));
+    ICB_CUDA(cudaEventRecord(h->hev[2 * n_chunks], bs));
     ICB_CUDA(cudaStreamWaitEvent(s, h->hev[2 * n_chunks], 0));    // the stream sees the copies done
     ICB_CUDA(cudaEventRecord(h->ev1, s));
     if (stats) return read_stats(h, stats, n_steps, 0);

@@ -160,7 +160,7 @@ class Simulation:
         capi.check(self._lib.icb_advance(self._h, int(n_steps), C.byref(rs)))
         return rs.as_dict()
 
-    def advance_host(self, st: IonState, n_steps: int, n_chunks: int = 16) -> dict:
+    def advance_host(self, st: IonState, n_steps: int, n_chunks: int = 24) -> dict:
         """Host state in, n_steps, host state out (positions, velocities and
         active flags of ``st`` are read and overwritten), copies overlapped
         with the steps of other ion chunks (icb_advance_host)."""

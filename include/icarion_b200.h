@@ -242,9 +242,10 @@ int icb_advance(struct icb_handle* h, uint64_t n_steps, icb_run_stats* stats);
 /* The engine fast path with host state in one call: icb_update_state (the
  * given positions, velocities and active flags) + icb_advance(n_steps) +
  * icb_download_ions (same arrays), with the ions split into n_chunks whose
- * host<->device copies overlap the steps of the other chunks (copy stream,
- * one compute stream per chunk, events; host arrays should be pinned for the
- * overlap; 16 chunks measured best for 1M ions on a B200).  The overlapped
+ * host<->device copies overlap the steps of the other chunks (copy and
+ * copy-back streams, one compute stream per chunk, events, queued chunk by
+ * chunk; host arrays should be pinned for the overlap; 24 chunks measured
+ * best for 1M ions on a B200).  The overlapped
  * form needs n_steps <= steps_per_launch, no space charge, no CUDA graphs
  * and the double-position forms; otherwise (and for n_chunks = 1) the three
  * calls run in order.  Results equal the three separate calls bit for bit. */
