@@ -55,7 +55,30 @@ BYTES_PER_ION_LAUNCH = {"mixed": 130, "hilo": 130, "fp64": 170}
 # of that launch (dram__bytes_read.sum + dram__bytes_write.sum; writes still
 # in L2 at kernel end are not counted).
 STEPPING = {"events": 0, "per-step": 1}
-NCU_TRAFFIC_PER_LAUNCH = {"mixed": 80.829696e6 + 6.218752e6}
+NCU_TRAFFIC_PER_LAUNCH = {"mixed": 80.850176e6 + 6.612992e6}
+# Warp instructions of one fused mixed launch (1,048,576 ions x 1000 steps,
+# event-to-event form) from the same capture (smsp__inst_executed.sum): the
+# kernel is bound by instruction issue, so its second roofline is the issue
+# peak of 4 warp instructions per SM per cycle.
+NCU_INST_PER_LAUNCH = {"mixed": 2.100741539e9}
+
+
+def issue_roofline(args, avg_launch_ms: float, clk: dict) -> dict | None:
+    """Instruction-issue roofline of the fused mixed kernel: warp
+    instructions per launch (ncu, same workload) / live launch time, against
+    4 schedulers x SMs x the SM clock sampled during the run."""
+    if args.precision != "mixed" or args.steps_per_launch != 1000 or args.workload != "ims-1M" \
+            or args.stepping != "events":
+        return None
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+    inst = NCU_INST_PER_LAUNCH["mixed"]
+    achieved = inst / (avg_launch_ms * 1e-3)
+    peak = 4.0 * sms * mhz * 1e6
+    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp instructions/s",
+            "frac": achieved / peak, "inst_per_launch": inst, "sms": sms, "sm_mhz": mhz,
+            "source": "smsp__inst_executed.sum of one launch (ncu); peak = 4 x SMs x sampled SM clock"}
 
 
 def _env_rank():
@@ -409,6 +432,7 @@ def run_ours(args) -> None:
                      "bytes_per_launch": bpl, "avg_launch_ms": avg_launch_ms,
                      "note": "fused K-step kernel: state crosses HBM once per launch, so it is instruction-issue "
                              "bound, not HBM bound; see roofline_per_step and profiles/"},
+        "roofline_issue": issue_roofline(args, avg_launch_ms, clk),
         "roofline_per_step": {"bound": "hbm", "achieved": ach1, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                               "frac": ach1 / peaks["hbm_gbs"], "avg_launch_ms": avg1,
                               "kernel": f"k_step<{args.precision},boris,hss,uniform> 1 step/launch",
