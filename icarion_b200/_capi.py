@@ -30,6 +30,7 @@ COLLISION_HSS_PLAIN, COLLISION_EHSS = 5, 6
 INSTRUMENT_IMS, INSTRUMENT_FTICR, INSTRUMENT_QUADRUPOLE_RF = 0, 1, 2
 SC_OFF, SC_P3M_ISOLATED, SC_PM_PERIODIC_REF = 0, 1, 2
 STEPPING_EVENTS, STEPPING_PER_STEP = 0, 1
+MATH_NEG_LOG1M, MATH_NEG_LOG1M_CUDA, MATH_ONE_MINUS_EXP, MATH_ONE_MINUS_EXP_CUDA = 0, 1, 2, 3
 FLOW_CONSTANT, FLOW_AXIAL_UNIFORM, FLOW_AXIAL_PARABOLIC = 0, 1, 2
 MLP_HIDDEN, MLP_N_PARAMS = 64, 4417
 POS_POINT, POS_GAUSSIAN, POS_UNIFORM_SPHERE, POS_UNIFORM_CYLINDER, POS_UNIFORM_BOX = 0, 1, 2, 3, 4
@@ -176,6 +177,7 @@ SIGNATURES = {
     "icb_mlp_gradients": (C.c_int, [C.c_int, _FP, C.c_uint64, _FP, _FP, _FP, _DP]),
     "icb_generate_ions": (C.c_int, [C.c_uint32, C.c_int32, _P(SpeciesSpec), _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]),
     "icb_philox_eval": (C.c_int, [C.c_int, C.c_uint64, _U32P, C.c_uint64, C.c_int, _U32P]),
+    "icb_clock_math_eval": (C.c_int, [C.c_int, C.c_uint64, _FP, C.c_int, _FP]),
     "icb_moments_noalloc": (C.c_int, [C.c_int, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

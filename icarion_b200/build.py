@@ -7,7 +7,7 @@ Compiles every ``csrc/*.cu`` translation unit with nvcc
 ``icarion_b200/_lib/libicarion_b200.so``.  Per-unit flags:
 
 * ``icb_step_fp64.cu``   ``--fmad=false`` (bit-faithful IEEE double push)
-* ``icb_step_mixed.cu``, ``icb_step_hilo.cu``, ``icb_mlp*.cu``  ``-use_fast_math``
+* ``icb_step_mixed.cu``, ``icb_step_hilo.cu``, ``icb_mathcheck.cu``, ``icb_mlp*.cu``  ``-use_fast_math``
 
 Objects are rebuilt only when a source or header is newer than the object.
 """
@@ -35,6 +35,7 @@ PER_UNIT = {
     "icb_step_fp64.cu": ["--fmad=false"],
     "icb_step_mixed.cu": ["-use_fast_math"],
     "icb_step_hilo.cu": ["-use_fast_math"],
+    "icb_mathcheck.cu": ["-use_fast_math"],
 }
 LINK_LIBS = ["-lcufft"]
 

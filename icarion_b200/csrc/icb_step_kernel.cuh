@@ -48,6 +48,39 @@ __device__ __forceinline__ double m_log1p(double x) { return log1p(x); }
 __device__ __forceinline__ float m_log1p(float x) { return log1pf(x); }
 __device__ __forceinline__ double m_expm1(double x) { return expm1(x); }
 __device__ __forceinline__ float m_expm1(float x) { return expm1f(x); }
+
+// -ln(1 - q), 0 <= q < 1 (a per-step probability -> hazard).  FP64: log1p.
+// Float: the Taylor series sum_{k>=1} q^k / k to k = 12 below q = 1/4
+// (truncation < q^12 / (13 (1 - q)) < 5e-9 relative), above it -ln(1 - q)
+// with the hardware log (1 - q is exact for q >= 1/2; absolute error
+// < 4e-7 on a value >= 0.28).
+__device__ __forceinline__ double m_neg_log1m(double q) { return -log1p(-q); }
+__device__ __forceinline__ float m_neg_log1m(float q) {
+    if (q < 0.25f) {
+        float s = 1.0f / 12.0f;
+        s = fmaf(q, s, 1.0f / 11.0f); s = fmaf(q, s, 1.0f / 10.0f); s = fmaf(q, s, 1.0f / 9.0f);
+        s = fmaf(q, s, 1.0f / 8.0f);  s = fmaf(q, s, 1.0f / 7.0f);  s = fmaf(q, s, 1.0f / 6.0f);
+        s = fmaf(q, s, 0.2f);         s = fmaf(q, s, 0.25f);        s = fmaf(q, s, 1.0f / 3.0f);
+        s = fmaf(q, s, 0.5f);         s = fmaf(q, s, 1.0f);
+        return q * s;
+    }
+    return -__logf(1.0f - q);
+}
+// 1 - e^-x, x >= 0 (a hazard -> probability).  FP64: -expm1(-x).  Float:
+// the series x sum_{k>=0} (-x)^k / (k+1)! to k = 8 below x = 1/4
+// (truncation < x^9 / 10! < 1e-11), above it 1 - e^-x with the hardware exp
+// (relative error < 2e-6 on a value >= 0.22).
+__device__ __forceinline__ double m_one_minus_exp(double x) { return -expm1(-x); }
+__device__ __forceinline__ float m_one_minus_exp(float x) {
+    if (x < 0.25f) {
+        float s = 1.0f / 362880.0f;
+        s = fmaf(-x, s, 1.0f / 40320.0f); s = fmaf(-x, s, 1.0f / 5040.0f); s = fmaf(-x, s, 1.0f / 720.0f);
+        s = fmaf(-x, s, 1.0f / 120.0f);   s = fmaf(-x, s, 1.0f / 24.0f);   s = fmaf(-x, s, 1.0f / 6.0f);
+        s = fmaf(-x, s, 0.5f);            s = fmaf(-x, s, 1.0f);
+        return x * s;
+    }
+    return 1.0f - __expf(-x);
+}
 __device__ __forceinline__ double m_fmax(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ float m_fmax(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double m_fmin(double a, double b) { return fmin(a, b); }
@@ -672,7 +705,7 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
     const R gx = v[0] - vn[0], gy = v[1] - vn[1], gz = v[2] - vn[2];
     const R g = m_sqrt(gx * gx + gy * gy + gz * gz);
     const R q = A * (b + rad);
-    const R pc = -m_expm1(-A * g);
+    const R pc = m_one_minus_exp(A * g);
     const bool hit = kept && (LANG || u32(r0.z, R(0)) * q < pc);
     if constexpr (!kFlat) {
         if (!hit) return 1;
@@ -808,7 +841,7 @@ __device__ __forceinline__ int candidate_mix(const EnsConst& C, const MixConst& 
         const R hz = v[2] - (ug[2] + s * rb * cb2);
         K += Ai(j) * m_sqrt(hx * hx + hy * hy + hz * hz);
     }
-    const R pc = -m_expm1(-K);
+    const R pc = m_one_minus_exp(K);
     if (!(u32(r0.z, R(0)) * K * (b + rad) < g * pc)) return 1;
     const R mn = Gm(ci);
     R inv_mt;
@@ -1016,7 +1049,7 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
         if (!(hz < R(4096))) hz = R(4096);
         if (hz < R(16)) hz = R(16);
         H = static_cast<uint32_t>(hz);
-        if (U > R(0)) lam = -m_log1p(-U);
+        if (U > R(0)) lam = m_neg_log1m(U);
         if (g_next != kNeedRestart) nk = (g_next & ~kRefresh) - step0;
     }
     auto clock_restart = [&](uint32_t gs) {
@@ -1025,7 +1058,7 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
         R qs = k.A * bstar + k.Amean;
         if (qs > R(0.99999904632568359375)) { qs = R(0.99999904632568359375); ++n_ovf; }
         U = qs;
-        lam = -m_log1p(-qs);
+        lam = m_neg_log1m(qs);
         const R nf = ceil(S / lam);
         g_start = gs;
         if (nf <= static_cast<R>(H)) g_next = gs + (nf < R(1) ? 1u : static_cast<uint32_t>(nf)) - 1u;

@@ -435,6 +435,15 @@ int icb_moments_noalloc(int device, uint64_t n, const double* x, const double* y
 int icb_philox_eval(int device, uint64_t n, const uint32_t* counters, uint64_t seed,
                     int use_curand, uint32_t* out);
 
+/* Evaluate on `device` the float clock functions of the step kernel next to
+ * CUDA's: NEG_LOG1M = -ln(1 - q) (series / hardware log), NEG_LOG1M_CUDA =
+ * -log1pf(-q), ONE_MINUS_EXP = 1 - e^-x (series / hardware exp),
+ * ONE_MINUS_EXP_CUDA = -expm1f(-x); n inputs x, results to out.  Replaces
+ * nothing in the reference: it bounds the kernel's float forms. */
+enum { ICB_MATH_NEG_LOG1M = 0, ICB_MATH_NEG_LOG1M_CUDA = 1, ICB_MATH_ONE_MINUS_EXP = 2,
+       ICB_MATH_ONE_MINUS_EXP_CUDA = 3 };
+int icb_clock_math_eval(int device, uint64_t n, const float* x, int which, float* out);
+
 #ifdef __cplusplus
 }
 #endif

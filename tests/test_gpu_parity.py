@@ -99,6 +99,39 @@ def _hss_gpu(st0: IonState, e: dict, steps: int, **kw) -> tuple[IonState, dict]:
         return sim.download(), rs
 
 
+def _clock_math(x, which):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty_like(x)
+    capi.check(capi.lib().icb_clock_math_eval(0, x.size, capi.fptr(x), which, capi.fptr(out)))
+    return out.astype(np.float64)
+
+
+def test_float_clock_functions_match_cuda():
+    """The float kernels' -ln(1 - q) and 1 - e^-x (Taylor series below 1/4,
+    hardware log/exp above) against CUDA's log1pf / expm1f on the device and
+    against FP64: relative error <= 3e-7 on the series range, <= 2e-6 on
+    the rest (q up to the kernel's cap 1 - 2^-20, x up to 30)."""
+    q = np.concatenate([np.logspace(-12, np.log10(0.2499), 4000), np.linspace(0.25, 0.99999904632568359375, 4000)])
+    q = q.astype(np.float32).astype(np.float64)
+    exact = -np.log1p(-q)
+    ours, cuda = _clock_math(q, capi.MATH_NEG_LOG1M), _clock_math(q, capi.MATH_NEG_LOG1M_CUDA)
+    lo = q < 0.25
+    for got in (ours, cuda):
+        rel = np.abs(got - exact) / exact
+        assert rel[lo].max() <= 3e-7 and rel[~lo].max() <= 2e-6, (rel[lo].max(), rel[~lo].max())
+    assert np.max(np.abs(ours - cuda) / exact) <= 2e-6
+    x = np.concatenate([np.logspace(-12, np.log10(0.2499), 4000), np.linspace(0.25, 30.0, 4000)])
+    x = x.astype(np.float32).astype(np.float64)
+    exact = -np.expm1(-x)
+    ours, cuda = _clock_math(x, capi.MATH_ONE_MINUS_EXP), _clock_math(x, capi.MATH_ONE_MINUS_EXP_CUDA)
+    lo = x < 0.25
+    for got in (ours, cuda):
+        rel = np.abs(got - exact) / exact
+        assert rel[lo].max() <= 3e-7 and rel[~lo].max() <= 2e-6, (rel[lo].max(), rel[~lo].max())
+    with pytest.raises(capi.IcbError):
+        _clock_math(x[:4], 9)
+
+
 def test_fp64_hss_trajectories_match_oracle():
     n, steps = 512, 3000
     e = config0_ensemble()
