@@ -124,19 +124,33 @@ def ensemble_params(domain: dict, sigma_m2: float, dt_s: float, detector_z_m: fl
     gas = env.get("gas_species", "He")
     L = float(geom.get("length_m", 0.1))
     mix = env.get("gas_mixture", []) or []
-    n_mix = len(mix) if len(mix) >= 2 else 0
-    if n_mix > 8:
+    # densities from the normalised mole fractions of all components
+    # (EnvironmentConfig.h:155-175); only those that take part in collisions
+    # enter the collision law (HSSCollisionHandler.cpp:127-133)
+    fsum = sum(float(c.get("mole_fraction", 0.0)) for c in mix)
+    norm = fsum if fsum > 0.0 else 1.0
+    n_tot = gas_density(P, T)
+    comps = []
+    for c in mix:
+        n_i = float(c.get("mole_fraction", 0.0)) / norm * n_tot
+        if not c.get("participates_in_collisions", True) or n_i <= 0.0:
+            continue
+        override = float(c.get("cross_section_m2", -1.0))
+        comps.append((n_i, GAS_MASS_KG.get(c["species"], GAS_MASS_KG["He"]),
+                      override if override > 0.0 else float((sigma_by_gas or {}).get(c["species"], sigma_m2))))
+    if len(comps) > 8:
         raise ValueError("at most 8 gas mixture components")
+    n_mix = len(comps) if len(comps) >= 2 else 0
     dens, mass, sig = [0.0] * 8, [0.0] * 8, [0.0] * 8
-    if n_mix:
-        fsum = sum(float(c.get("mole_fraction", 0.0)) for c in mix)
-        norm = fsum if fsum > 0.0 else 1.0
-        n_tot = gas_density(P, T)
-        for i, c in enumerate(mix):
-            dens[i] = float(c.get("mole_fraction", 0.0)) / norm * n_tot
-            mass[i] = GAS_MASS_KG.get(c["species"], GAS_MASS_KG["He"])
-            override = float(c.get("cross_section_m2", -1.0))
-            sig[i] = override if override > 0.0 else float((sigma_by_gas or {}).get(c["species"], sigma_m2))
+    for i, (n_i, m_i, s_i) in enumerate(comps if n_mix else []):
+        dens[i], mass[i], sig[i] = n_i, m_i, s_i
+    # a mixture with one colliding component is that component alone; with
+    # none, no collisions
+    single_gas = (gas_density(P, T), GAS_MASS_KG[gas], float(sigma_m2))
+    if mix and len(comps) == 1:
+        single_gas = comps[0]
+    elif mix and not comps:
+        single_gas = (0.0, GAS_MASS_KG[gas], float(sigma_m2))
     axial = 0.0
     if "EN_Td" in dc:
         axial = axial_voltage_from_en(float(dc["EN_Td"]), P, T, L)
@@ -155,11 +169,11 @@ def ensemble_params(domain: dict, sigma_m2: float, dt_s: float, detector_z_m: fl
         "rf_frequency_Hz": float(rf.get("frequency_Hz", 0.0)),
         "B_T": [float(v) for v in mag.get("field_strength_T", [0.0, 0.0, 0.0])],
         "temperature_K": T,
-        "gas_density_m3": gas_density(P, T),
-        "gas_mass_kg": GAS_MASS_KG[gas],
+        "gas_density_m3": single_gas[0],
+        "gas_mass_kg": single_gas[1],
         "gas_velocity_m_s": [float(v) for v in env.get("gas_velocity_m_s", [0.0, 0.0, 0.0])],
         "gas_polarizability_m3": GAS_POLARIZABILITY_M3.get(gas, 0.0),
-        "sigma_m2": float(sigma_m2),
+        "sigma_m2": single_gas[2],
         "ipm_bmax_m": float(ipm_bmax_m),
         "dt_s": float(dt_s),
         "detector_z_m": float(detector_z_m),

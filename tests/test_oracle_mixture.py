@@ -33,6 +33,24 @@ def test_mixture_constants_follow_the_loader():
     assert e["gas_mix_sigma_m2"][:2] == [150e-20, 60e-20]
 
 
+def test_components_outside_collisions_are_left_out():
+    """participates_in_collisions = false drops a component from the
+    collision law; its mole fraction still dilutes the others
+    (EnvironmentConfig.h:155-175, HSSCollisionHandler.cpp:127-133)."""
+    dom = domain_json(CONFIG0_DOMAIN)
+    n = cfg.gas_density(1000.0, 300.0)
+    dom["env"]["gas_mixture"] = [{"species": "N2", "mole_fraction": 0.5, "cross_section_m2": 150e-20},
+                                 {"species": "He", "mole_fraction": 0.25, "cross_section_m2": 60e-20},
+                                 {"species": "Ar", "mole_fraction": 0.25, "participates_in_collisions": False}]
+    e = cfg.ensemble_params(dom, 150e-20, 5e-10)
+    assert e["n_gas"] == 2
+    np.testing.assert_allclose(e["gas_mix_density_m3"][:2], [0.5 * n, 0.25 * n], rtol=1e-15)
+    dom["env"]["gas_mixture"][1]["participates_in_collisions"] = False
+    e = cfg.ensemble_params(dom, 150e-20, 5e-10)
+    assert e["n_gas"] == 0 and e["gas_density_m3"] == 0.5 * n and e["gas_mass_kg"] == cfg.GAS_MASS_KG["N2"]
+    assert e["sigma_m2"] == 150e-20
+
+
 def test_eight_components_accepted_nine_rejected():
     gases = ["N2", "He", "Ar", "O2", "CO2", "Ne", "H2O", "N2", "He"]
     dom = domain_json(CONFIG0_DOMAIN)
