@@ -27,7 +27,7 @@ PREC_FP64, PREC_MIXED, PREC_MIXED_HILO = 0, 1, 2
 INTEGRATOR_BORIS, INTEGRATOR_RK4 = 0, 1
 COLLISION_NONE, COLLISION_HSS, COLLISION_IPM_TABLE, COLLISION_IPM_MLP, COLLISION_LANGEVIN = 0, 1, 2, 3, 4
 COLLISION_HSS_PLAIN, COLLISION_EHSS = 5, 6
-INSTRUMENT_IMS, INSTRUMENT_FTICR, INSTRUMENT_QUADRUPOLE_RF = 0, 1, 2
+INSTRUMENT_IMS, INSTRUMENT_FTICR, INSTRUMENT_QUADRUPOLE_RF, INSTRUMENT_LQIT = 0, 1, 2, 3
 SC_OFF, SC_P3M_ISOLATED, SC_PM_PERIODIC_REF = 0, 1, 2
 STEPPING_EVENTS, STEPPING_PER_STEP = 0, 1
 MATH_NEG_LOG1M, MATH_NEG_LOG1M_CUDA, MATH_ONE_MINUS_EXP, MATH_ONE_MINUS_EXP_CUDA = 0, 1, 2, 3
@@ -65,6 +65,8 @@ class EnsembleParams(C.Structure):
         ("n_gas", C.c_int32), ("flow_model", C.c_int32), ("gas_mix_density_m3", C.c_double * 8),
         ("gas_mix_mass_kg", C.c_double * 8), ("gas_mix_sigma_m2", C.c_double * 8),
         ("axial_flow_velocity_m_s", C.c_double), ("axial_flow_max_velocity_m_s", C.c_double),
+        ("ac_amplitude_V", C.c_double * 2), ("ac_frequency_Hz", C.c_double * 2), ("ac_phase_rad", C.c_double * 2),
+        ("ac_ramp", C.c_double * 2), ("ac_dipolar", C.c_int32), ("reserved2_", C.c_int32),
     ]
 
 

@@ -51,8 +51,39 @@ GAS_POLARIZABILITY_M3 = {
     "N2": 1.74e-30, "O2": 1.567e-30, "H2O": 1.45e-30,
 }
 
-INSTRUMENTS = {"IMS": capi.INSTRUMENT_IMS, "FTICR": capi.INSTRUMENT_FTICR,
-               "QuadrupoleRF": capi.INSTRUMENT_QUADRUPOLE_RF}
+# TIMS uses the IMS field (AnalyticalFieldModel.cpp:72)
+INSTRUMENTS = {"IMS": capi.INSTRUMENT_IMS, "TIMS": capi.INSTRUMENT_IMS, "FTICR": capi.INSTRUMENT_FTICR,
+               "QuadrupoleRF": capi.INSTRUMENT_QUADRUPOLE_RF, "LQIT": capi.INSTRUMENT_LQIT}
+
+
+def ac_drives(fields: dict) -> tuple[list[float], list[float], list[float], list[float], int]:
+    """fields.AC of an LQIT (DomainConfigLoader.cpp:262-275, 505-545;
+    FieldsConfig.h:93-168) -> per-axis (amplitude V, frequency Hz, phase rad)
+    and ramp for x and y, and whether the drive is the two-axis dipolar one
+    (AC.dipolar_excitation, the AC.x / AC.y shorthand or
+    fields.dipolar_excitation; a disabled axis gets amplitude 0); otherwise
+    the single-axis AC.voltage_V drives x.  Constant values only."""
+    ac = fields.get("AC", fields.get("ac", {})) or {}
+    dip = fields.get("dipolar_excitation")
+    if dip is None:
+        dip = ac.get("dipolar_excitation")
+    if dip is None and ("x" in ac or "y" in ac):
+        dip = {k: ac[k] for k in ("x", "y") if k in ac}
+    amp, freq, phase, ramp = [0.0, 0.0], [0.0, 0.0], [0.0, 0.0], [1.0, 1.0]
+    if dip is not None:
+        for a, key in enumerate(("x", "y")):
+            axis = dip.get(key)
+            if not axis or not axis.get("enabled", True):
+                continue
+            amp[a] = float(axis.get("amplitude_V", axis.get("voltage_V", 0.0)))
+            ramp[a] = float(axis.get("ramp", 1.0))
+            freq[a] = float(axis.get("frequency_Hz", 0.0))
+            phase[a] = float(axis.get("phase_rad", 0.0))
+    else:
+        amp[0] = float(ac.get("voltage_V", 0.0))
+        freq[0] = float(ac.get("frequency_Hz", 0.0))
+        phase[0] = float(ac.get("phase_rad", 0.0))
+    return amp, freq, phase, ramp, int(dip is not None)
 INTEGRATORS = {"Boris": capi.INTEGRATOR_BORIS, "RK4": capi.INTEGRATOR_RK4}
 COLLISIONS = {"None": capi.COLLISION_NONE, "none": capi.COLLISION_NONE, "HSS": capi.COLLISION_HSS,
               "IPM": capi.COLLISION_IPM_TABLE}
@@ -151,6 +182,7 @@ def ensemble_params(domain: dict, sigma_m2: float, dt_s: float, detector_z_m: fl
         single_gas = comps[0]
     elif mix and not comps:
         single_gas = (0.0, GAS_MASS_KG[gas], float(sigma_m2))
+    ac_amp, ac_freq, ac_phase, ac_ramp, ac_dipolar = ac_drives(fields)
     axial = 0.0
     if "EN_Td" in dc:
         axial = axial_voltage_from_en(float(dc["EN_Td"]), P, T, L)
@@ -184,6 +216,12 @@ def ensemble_params(domain: dict, sigma_m2: float, dt_s: float, detector_z_m: fl
         "gas_mix_sigma_m2": sig,
         "axial_flow_velocity_m_s": float(env.get("axial_flow_velocity_m_s", 0.0)),
         "axial_flow_max_velocity_m_s": float(env.get("axial_flow_max_velocity_m_s", 0.0)),
+        "ac_amplitude_V": ac_amp,
+        "ac_frequency_Hz": ac_freq,
+        "ac_phase_rad": ac_phase,
+        "ac_ramp": ac_ramp,
+        "ac_dipolar": ac_dipolar,
+        "reserved2_": 0,
     }
 
 

@@ -360,9 +360,11 @@ double field_bound(const EnsConst& C, const icb_ensemble_params& P) {
     const double gx = C.G[0] * ex, gy = C.G[1] * ey, gz = C.G[2] * ez;
     e = e + std::sqrt(gx * gx + gy * gy + gz * gz);
     if (C.rf) {
-        const double raxis = std::sqrt(C.ox * C.ox + C.oy * C.oy) + Rp;
+        const double dx = C.ox - C.c[0], dy = C.oy - C.c[1];
+        const double raxis = std::sqrt(dx * dx + dy * dy) + Rp;
         e = e + 2.0 * (std::fabs(C.rf_U0) + std::fabs(C.rf_V)) * raxis / C.r0sq;
     }
+    if (C.ac) e = e + (std::fabs(C.ac_amp[0]) + std::fabs(C.ac_amp[1]));
     return e;
 }
 
@@ -413,6 +415,33 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
             C.G[0] = factor; C.G[1] = factor; C.G[2] = -2.0 * factor;
             C.c[2] = 0.5 * L;
             kind = kFieldLinear;
+            break;
+        }
+        case ICB_INSTRUMENT_LQIT: {         // AnalyticalFieldModel.cpp:81-134 (unrotated cylinder)
+            // RF quadrupole about the cylinder axis, axial well about L/2
+            C.c[0] = P.origin_m[0];
+            C.c[1] = P.origin_m[1];
+            if (std::fabs(P.axial_V) > kMinVoltage) {
+                const double L = P.length_m;
+                const double alpha = P.axial_V / (L * L);
+                C.G[2] = -2.0 * alpha;
+                C.c[2] = P.origin_m[2] + 0.5 * L;
+                kind = kFieldLinear;
+            }
+            // the single-axis drive is x alone, without a ramp
+            for (int a = 0; a < (P.ac_dipolar ? 2 : 1); ++a) {
+                const double A = P.ac_amplitude_V[a] * (P.ac_dipolar ? P.ac_ramp[a] : 1.0);
+                if (!(P.ac_frequency_Hz[a] >= 0.0) || !std::isfinite(A))
+                    return fail(ICB_ERR_INVALID_ARGUMENT, "LQIT AC drive %d needs a finite amplitude and frequency >= 0",
+                                a);
+                if (std::fabs(A) > kMinVoltage) {
+                    C.ac = 1;
+                    C.ac_amp[a] = -A / P.radius_m;
+                    C.ac_omega[a] = 2.0 * M_PI * P.ac_frequency_Hz[a];
+                    C.ac_phase[a] = P.ac_phase_rad[a];
+                }
+            }
+            if (rf || C.ac) kind = kFieldLinearRF;
             break;
         }
         default:

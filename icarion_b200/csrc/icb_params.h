@@ -55,8 +55,13 @@ struct EnsConst {
     // parabolic axial gas flow (flow != 0): u_z = flow_umax max(0, 1 - r^2 /
     // flow_r2) at the ion; ug is then zero and refreshed at each collision
     double flow_umax, flow_r2;
+    // AC drives (ac != 0): E_a += ac_amp[a] cos(ac_omega[a] t + ac_phase[a]),
+    // a = x, y, ac_amp = -amplitude * ramp / r0; the RF quadrupole is
+    // centred on (c[0], c[1])
+    double ac_amp[2], ac_omega[2], ac_phase[2];
     int32_t magnetic;
     int32_t rf;
+    int32_t ac;
     // float copies for the float collision path
     float fA, fmean_th, fsig_n, fm_gas;
     float fug[3];

@@ -239,6 +239,8 @@ struct Consts {
     double c[3];
     R rfU0, rfV, r0sq;
     double rfw;
+    double acA[2], acw[2], acp[2];   // AC drives (time-dependent field only)
+    bool ac;
     R tv[3], sv[3];          // Boris rotation vectors (RK4: B itself in tv)
     R a_uni[3];              // acceleration of a uniform field for this ion
     R q, qm, inv_m;
@@ -263,6 +265,9 @@ __device__ void load_consts(Consts<R>& k, const EnsConst& C, double q, double m)
     k.rfV = static_cast<R>(C.rf_V);
     k.r0sq = static_cast<R>(C.r0sq);
     k.rfw = C.rf_omega;
+    k.ac = C.ac != 0;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) { k.acA[a] = C.ac_amp[a]; k.acw[a] = C.ac_omega[a]; k.acp[a] = C.ac_phase[a]; }
     k.dt = C.dt;
     k.hd = C.dt * 0.5;
     k.dt6 = C.dt / 6.0;
@@ -313,11 +318,21 @@ __device__ __forceinline__ void efield(const Consts<R>& k, const Pos& x, double 
     }
     if constexpr (FIELD == kFieldLinearRF) {
         // AnalyticalFieldModel.cpp:152-158: U = dc_quad + V cos(w t);
-        // E_x = -2 x U / r0^2, E_y = 2 y U / r0^2.
-        const R U = k.rfU0 + k.rfV * static_cast<R>(cos(k.rfw * t));
-        const R px = x.template rel<R>(0, 0.0), py = x.template rel<R>(1, 0.0);
-        E[0] = R(-2.0) * px * U / k.r0sq;
-        E[1] = R(2.0) * py * U / k.r0sq;
+        // E_x = -2 x U / r0^2, E_y = 2 y U / r0^2, x and y from the
+        // quadrupole axis (c[0], c[1]: 0 for IMS / QuadrupoleRF, the
+        // cylinder axis for the LQIT, AnalyticalFieldModel.cpp:90-103).
+        // Without an RF voltage the LQIT's x, y come from G = 0.
+        if (k.rfV != R(0)) {
+            const R U = k.rfU0 + k.rfV * static_cast<R>(cos(k.rfw * t));
+            const R px = x.template rel<R>(0, k.c[0]), py = x.template rel<R>(1, k.c[1]);
+            E[0] = R(-2.0) * px * U / k.r0sq;
+            E[1] = R(2.0) * py * U / k.r0sq;
+        }
+        // LQIT AC drives (AnalyticalFieldModel.cpp:104-121)
+        if (k.ac) {
+            E[0] += static_cast<R>(k.acA[0] * cos(k.acw[0] * t + k.acp[0]));
+            E[1] += static_cast<R>(k.acA[1] * cos(k.acw[1] * t + k.acp[1]));
+        }
     }
 }
 

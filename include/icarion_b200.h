@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define ICB_ABI_VERSION 5
+#define ICB_ABI_VERSION 6
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -64,7 +64,11 @@ enum {
 enum {
     ICB_INSTRUMENT_IMS = 0,          /* AnalyticalFieldModel.cpp:136-161 */
     ICB_INSTRUMENT_FTICR = 1,        /* AnalyticalFieldModel.cpp:174-186 */
-    ICB_INSTRUMENT_QUADRUPOLE_RF = 2 /* AnalyticalFieldModel.cpp:219-248 */
+    ICB_INSTRUMENT_QUADRUPOLE_RF = 2,/* AnalyticalFieldModel.cpp:219-248 */
+    /* linear quadrupole ion trap, AnalyticalFieldModel.cpp:81-134: RF
+     * quadrupole about the cylinder axis, AC drives (ac_* below) and the
+     * axial DC well E_z = -2 axial_V / L^2 (z_local - L/2) */
+    ICB_INSTRUMENT_LQIT = 3
 };
 
 /* Number of doubles per ensemble returned by icb_moments:
@@ -119,6 +123,20 @@ typedef struct icb_ensemble_params {
      * collides (SimulationEngineCollisionRuntime.cpp:124-131). */
     double axial_flow_velocity_m_s;
     double axial_flow_max_velocity_m_s;
+    /* AC drives of the LQIT (fields.ac): E_x += -ac_amplitude_V[0] *
+     * ac_ramp[0] / radius_m * cos(2 pi ac_frequency_Hz[0] t + ac_phase_rad[0]),
+     * E_y the same with [1].  ac_dipolar = 0: the single-axis drive
+     * (ac.voltage_V, frequency_Hz, phase_rad) on axis 0 alone, ac_ramp and
+     * axis 1 unused; 1: the
+     * two-axis dipolar drive (ac.dipolar_x / dipolar_y: amplitude_V, ramp,
+     * frequency_Hz, phase_rad; a disabled axis has amplitude 0).  Drives
+     * with |amplitude * ramp| <= 1e-12 V are off. */
+    double ac_amplitude_V[2];
+    double ac_frequency_Hz[2];
+    double ac_phase_rad[2];
+    double ac_ramp[2];
+    int32_t ac_dipolar;
+    int32_t reserved2_;
 } icb_ensemble_params;
 enum { ICB_FLOW_CONSTANT = 0, ICB_FLOW_AXIAL_UNIFORM = 1, ICB_FLOW_AXIAL_PARABOLIC = 2 };
 #define ICB_MAX_GAS 8

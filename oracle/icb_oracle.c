@@ -81,6 +81,12 @@ typedef struct orc_domain {
     double gas_mix_sigma_m2[8];
     double axial_flow_velocity_m_s;
     double axial_flow_max_velocity_m_s;
+    double ac_amplitude_V[2];  /* LQIT AC drives: x (single-axis or dipolar x), y (dipolar y) */
+    double ac_frequency_Hz[2];
+    double ac_phase_rad[2];
+    double ac_ramp[2];
+    int32_t ac_dipolar;
+    int32_t reserved2_;
 } orc_domain;
 
 /* Gas flow velocity at global position p (EnvironmentConfig::gas_velocity_at,
@@ -231,6 +237,34 @@ static void field_E(const orc_domain* d, const double p[3], double t, double E[3
             E[1] = 2.0 * p[1] * U / r0_sq;
         }
         if (fabs(d->axial_V) > ORC_MIN_VOLTAGE) E[2] = d->axial_V / d->length_m;
+    } else if (d->instrument == 3) {        /* LQIT: AnalyticalFieldModel.cpp:81-134, unrotated */
+        const double q[3] = {p[0] - d->origin_m[0], p[1] - d->origin_m[1], p[2] - d->origin_m[2]};
+        if (fabs(d->rf_voltage_V) > ORC_MIN_VOLTAGE) {
+            double r0_sq = d->radius_m * d->radius_m;
+            double omega = 2.0 * M_PI * d->rf_frequency_Hz;
+            double U = d->dc_quad_V + d->rf_voltage_V * cos(omega * t);
+            E[0] = -2.0 * q[0] * U / r0_sq;
+            E[1] = 2.0 * q[1] * U / r0_sq;
+        }
+        if (d->ac_dipolar) {
+            /* two-axis dipolar drive: amplitude * ramp * cos(w t + phase), skipped
+             * where |drive| <= threshold (eval_dipolar_axis_voltage) */
+            for (int a = 0; a < 2; ++a) {
+                if (fabs(d->ac_amplitude_V[a]) <= ORC_MIN_VOLTAGE) continue;
+                const double omega = 2.0 * M_PI * d->ac_frequency_Hz[a];
+                const double drive = d->ac_amplitude_V[a] * d->ac_ramp[a] * cos(omega * t + d->ac_phase_rad[a]);
+                if (fabs(drive) > ORC_MIN_VOLTAGE) E[a] += -drive / d->radius_m;
+            }
+        } else if (fabs(d->ac_amplitude_V[0]) > ORC_MIN_VOLTAGE) {
+            /* single-axis drive on x */
+            const double omega_ac = 2.0 * M_PI * d->ac_frequency_Hz[0];
+            E[0] += -d->ac_amplitude_V[0] / d->radius_m * cos(omega_ac * t + d->ac_phase_rad[0]);
+        }
+        if (fabs(d->axial_V) > ORC_MIN_VOLTAGE) {
+            const double L = d->length_m;
+            const double alpha = d->axial_V / (L * L);
+            E[2] = -2.0 * alpha * (q[2] - 0.5 * L);
+        }
     }
 }
 
@@ -780,6 +814,14 @@ double orc_field_bound(const orc_domain* d) {
         double factor = d->radial_V / (dd * dd);
         Gv[0] = factor; Gv[1] = factor; Gv[2] = -2.0 * factor;
         c[2] = 0.5 * L;
+    } else if (d->instrument == 3) {
+        c[0] = d->origin_m[0];
+        c[1] = d->origin_m[1];
+        if (fabs(d->axial_V) > ORC_MIN_VOLTAGE) {
+            const double L = d->length_m;
+            Gv[2] = -2.0 * (d->axial_V / (L * L));
+            c[2] = d->origin_m[2] + 0.5 * L;
+        }
     }
     const double Rp = d->radius_m + ORC_GEOM_EPS;
     const double ox = d->origin_m[0], oy = d->origin_m[1], oz = d->origin_m[2];
@@ -791,8 +833,17 @@ double orc_field_bound(const orc_domain* d) {
     const double gx = Gv[0] * ex, gy = Gv[1] * ey, gz = Gv[2] * ez;
     e = e + sqrt(gx * gx + gy * gy + gz * gz);
     if (rf) {
-        const double raxis = sqrt(ox * ox + oy * oy) + Rp;
+        const double dx = ox - c[0], dy = oy - c[1];
+        const double raxis = sqrt(dx * dx + dy * dy) + Rp;
         e = e + 2.0 * (fabs(d->dc_quad_V) + fabs(d->rf_voltage_V)) * raxis / (d->radius_m * d->radius_m);
+    }
+    if (d->instrument == 3) {
+        double ac = 0.0;
+        for (int a = 0; a < (d->ac_dipolar ? 2 : 1); ++a) {
+            const double A = d->ac_amplitude_V[a] * (d->ac_dipolar ? d->ac_ramp[a] : 1.0);
+            if (fabs(A) > ORC_MIN_VOLTAGE) ac += fabs(-A / d->radius_m);
+        }
+        if (ac > 0.0) e = e + ac;
     }
     return e;
 }

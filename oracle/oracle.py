@@ -42,6 +42,8 @@ class Domain(C.Structure):
         ("n_gas", C.c_int32), ("flow_model", C.c_int32), ("gas_mix_density_m3", C.c_double * 8),
         ("gas_mix_mass_kg", C.c_double * 8), ("gas_mix_sigma_m2", C.c_double * 8),
         ("axial_flow_velocity_m_s", C.c_double), ("axial_flow_max_velocity_m_s", C.c_double),
+        ("ac_amplitude_V", C.c_double * 2), ("ac_frequency_Hz", C.c_double * 2), ("ac_phase_rad", C.c_double * 2),
+        ("ac_ramp", C.c_double * 2), ("ac_dipolar", C.c_int32), ("reserved2_", C.c_int32),
     ]
 
 

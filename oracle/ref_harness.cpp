@@ -107,6 +107,7 @@ config::DomainConfig make_domain(const Args& a) {
     if (inst == "IMS") d.instrument = config::Instrument::IMS;
     else if (inst == "FTICR") d.instrument = config::Instrument::FTICR;
     else if (inst == "QuadrupoleRF") d.instrument = config::Instrument::QuadrupoleRF;
+    else if (inst == "LQIT") d.instrument = config::Instrument::LQIT;
     else throw std::runtime_error("unsupported instrument " + inst);
     d.geometry.origin_m = Vec3{num(a, "origin_x", 0.0), num(a, "origin_y", 0.0), num(a, "origin_z", 0.0)};
     d.geometry.length_m = num(a, "length", 0.1);
@@ -148,6 +149,23 @@ config::DomainConfig make_domain(const Args& a) {
     d.fields.rf.frequency_Hz.constant_value = num(a, "rf_f", 0.0);
     d.fields.magnetic.enabled = num(a, "magnetic", 0.0) != 0.0;
     d.fields.magnetic.field_strength_T = Vec3{num(a, "B_x", 0.0), num(a, "B_y", 0.0), num(a, "B_z", 0.0)};
+    // LQIT AC excitation (FieldsConfig.h:93-168): single-axis ac_V/ac_f/ac_phase,
+    // or the two-axis dipolar drive dip_{x,y}_{A,f,phase,ramp}
+    d.fields.ac.voltage_V.constant_value = num(a, "ac_V", 0.0);
+    d.fields.ac.frequency_Hz.constant_value = num(a, "ac_f", 0.0);
+    d.fields.ac.phase_rad = num(a, "ac_phase", 0.0);
+    for (const char* axis : {"x", "y"}) {
+        const std::string pre = std::string("dip_") + axis + "_";
+        if (!a.count(pre + "A")) continue;
+        d.fields.ac.dipolar_excitation_defined = true;
+        config::ACDipolarAxisConfig& ax = axis[0] == 'x' ? d.fields.ac.dipolar_x : d.fields.ac.dipolar_y;
+        ax.enabled = true;
+        ax.amplitude_V.constant_value = num(a, (pre + "A").c_str(), 0.0);
+        ax.frequency_Hz.constant_value = num(a, (pre + "f").c_str(), 0.0);
+        ax.phase_rad = num(a, (pre + "phase").c_str(), 0.0);
+        ax.ramp.constant_value = num(a, (pre + "ramp").c_str(), 1.0);
+    }
+    d.fields.ac.compute_derived();
     return d;
 }
 

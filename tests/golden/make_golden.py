@@ -13,7 +13,7 @@ Fixtures
   rng_mt64.npz          PhysicsRng(seed).uniform01() streams (seeds 123, 4219)
   ions_init.npz         IonLoader gaussian/thermal cloud from std::mt19937(123)
   derived.json          loader-derived n, gas mass, axial_V, E_z (config 0)
-  push_<case>.npz       collision-free Boris / RK4 runs (IMS, FTICR, QuadrupoleRF)
+  push_<case>.npz       collision-free Boris / RK4 runs (IMS, FTICR, QuadrupoleRF, LQIT)
   hss_ref.npz           Boris + reference HSS, 64 ions x 2000 steps
   ims_config0.npz       config 0: 4096 ions x 100k steps, moments every 1000
                         steps, displacement reference after 20k steps,
@@ -42,6 +42,13 @@ FTICR_DOMAIN = dict(instrument="FTICR", origin_z=0.0, length=0.05, radius=0.025,
                     radial_V=1.0, magnetic=1, B_z=7.0)
 QUAD_DOMAIN = dict(instrument="QuadrupoleRF", origin_z=-0.05, length=0.1, radius=0.005, T=300, P=1.0, gas="He",
                    rf_V=200.0, rf_f=1.0e6, dc_quad_V=5.0, axial_V=1.0)
+# linear ion trap: RF 200 V at 1 MHz (q ~ 0.6 at 200 Da), 2 V axial well,
+# two-axis dipolar drive (single-axis drive in LQIT1_DOMAIN)
+LQIT_DOMAIN = dict(instrument="LQIT", origin_z=-0.025, length=0.05, radius=0.004, T=300, P=0.1, gas="He",
+                   rf_V=200.0, rf_f=1.0e6, dc_quad_V=1.0, axial_V=2.0,
+                   dip_x_A=0.5, dip_x_f=1.0e5, dip_x_phase=0.3, dip_x_ramp=0.8, dip_y_A=0.2, dip_y_f=1.2e5)
+LQIT1_DOMAIN = dict(instrument="LQIT", origin_z=-0.025, length=0.05, radius=0.004, T=300, P=0.1, gas="He",
+                    rf_V=200.0, rf_f=1.0e6, axial_V=2.0, ac_V=0.4, ac_f=9.0e4, ac_phase=1.1)
 
 
 def init_state(n: int, seed: int = 123, mass_amu: float = 200.0, sigma_pos: float = 5e-4) -> dict:
@@ -75,10 +82,13 @@ def save(name: str, **arrays) -> None:
     print("wrote", name, flush=True)
 
 
-def main(quick: bool) -> None:
+def main(quick: bool, only: set[str] | None = None) -> None:
     if not orc.have_harness():
         raise SystemExit("oracle/_ref/ref_harness missing: run `make -C oracle` with the reference tree present")
 
+    if only:
+        push_only(only)
+        return
     # 1. PhysicsRng streams
     streams = {}
     for seed in (123, 4219):
@@ -98,18 +108,7 @@ def main(quick: bool) -> None:
     (OUT / "derived.json").write_text(json.dumps(d, indent=1) + "\n")
 
     # 4. collision-free pushes
-    cases = {
-        "boris_ims": (IMS_DOMAIN, "boris", init_state(64), 5000, 5e-10),
-        "rk4_ims": (IMS_DOMAIN, "rk4", init_state(64), 5000, 5e-10),
-        "boris_fticr": (FTICR_DOMAIN, "boris", fticr_state(64), 20000, 1e-9),
-        "rk4_fticr": (FTICR_DOMAIN, "rk4", fticr_state(64), 5000, 1e-9),
-        "boris_quadrf": (QUAD_DOMAIN, "boris", init_state(64, mass_amu=100.0, sigma_pos=2e-4), 4000, 1e-9),
-    }
-    for name, (dom, integ, s0, steps, dt) in cases.items():
-        fin, stats, _ = orc.harness_run(s0, steps, dom, integrator=integ, collision="none", dt=dt)
-        save(f"push_{name}.npz", **{f"in_{k}": s0[k] for k in orc.STATE_KEYS},
-             **{f"out_{k}": fin[k] for k in orc.STATE_KEYS}, steps=steps, dt=dt,
-             domain=json.dumps(dom), integrator=integ)
+    push_only(None)
 
     # 5. Boris + reference HSS, bit-level fixture for the restatement
     s0 = init_state(64)
@@ -129,7 +128,34 @@ def main(quick: bool) -> None:
          collisions=stats["collisions"], domain=json.dumps(IMS_DOMAIN))
 
 
+def push_cases() -> dict:
+    return {
+        "boris_ims": (IMS_DOMAIN, "boris", lambda: init_state(64), 5000, 5e-10),
+        "rk4_ims": (IMS_DOMAIN, "rk4", lambda: init_state(64), 5000, 5e-10),
+        "boris_fticr": (FTICR_DOMAIN, "boris", lambda: fticr_state(64), 20000, 1e-9),
+        "rk4_fticr": (FTICR_DOMAIN, "rk4", lambda: fticr_state(64), 5000, 1e-9),
+        "boris_quadrf": (QUAD_DOMAIN, "boris", lambda: init_state(64, mass_amu=100.0, sigma_pos=2e-4), 4000, 1e-9),
+        "boris_lqit": (LQIT_DOMAIN, "boris", lambda: init_state(64, sigma_pos=2e-4), 8000, 1e-9),
+        "rk4_lqit1": (LQIT1_DOMAIN, "rk4", lambda: init_state(64, sigma_pos=2e-4), 4000, 1e-9),
+    }
+
+
+def push_only(only: set[str] | None) -> None:
+    """Collision-free Boris / RK4 runs of the reference code (all, or the
+    named ones)."""
+    for name, (dom, integ, make_state, steps, dt) in push_cases().items():
+        if only is not None and name not in only:
+            continue
+        s0 = make_state()
+        fin, stats, _ = orc.harness_run(s0, steps, dom, integrator=integ, collision="none", dt=dt)
+        save(f"push_{name}.npz", **{f"in_{k}": s0[k] for k in orc.STATE_KEYS},
+             **{f"out_{k}": fin[k] for k in orc.STATE_KEYS}, steps=steps, dt=dt,
+             domain=json.dumps(dom), integrator=integ)
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--quick", action="store_true")
-    main(ap.parse_args().quick)
+    ap.add_argument("--only", nargs="*", default=None, help="regenerate only these push fixtures (e.g. boris_lqit)")
+    a = ap.parse_args()
+    main(a.quick, set(a.only) if a.only else None)

@@ -19,11 +19,17 @@ def domain_json(kw: dict) -> dict:
     for k1, k2 in (("EN_Td", "EN_Td"), ("axial_V", "axial_V"), ("radial_V", "radial_V"), ("dc_quad_V", "quad_V")):
         if k1 in kw:
             dc[k2] = kw[k1]
+    ac = {"voltage_V": kw.get("ac_V", 0.0), "frequency_Hz": kw.get("ac_f", 0.0), "phase_rad": kw.get("ac_phase", 0.0)}
+    dip = {a: {"amplitude_V": kw[f"dip_{a}_A"], "frequency_Hz": kw.get(f"dip_{a}_f", 0.0),
+               "phase_rad": kw.get(f"dip_{a}_phase", 0.0), "ramp": kw.get(f"dip_{a}_ramp", 1.0)}
+           for a in ("x", "y") if f"dip_{a}_A" in kw}
+    if dip:
+        ac["dipolar_excitation"] = dip
     return {
         "instrument": kw["instrument"],
         "geometry": {"origin_m": [0.0, 0.0, kw.get("origin_z", 0.0)], "length_m": kw["length"], "radius_m": kw["radius"]},
         "env": {"temperature_K": kw["T"], "pressure_Pa": kw["P"], "gas_species": kw["gas"]},
-        "fields": {"DC": dc, "RF": {"voltage_V": kw.get("rf_V", 0.0), "frequency_Hz": kw.get("rf_f", 0.0)},
+        "fields": {"DC": dc, "RF": {"voltage_V": kw.get("rf_V", 0.0), "frequency_Hz": kw.get("rf_f", 0.0)}, "AC": ac,
                    "magnetic": {"enabled": bool(kw.get("magnetic", 0)), "field_strength_T": [0.0, 0.0, kw.get("B_z", 0.0)]}},
     }
 

@@ -24,7 +24,7 @@ from icarion_b200.sim import IonState, Simulation, device_count
 
 pytestmark = pytest.mark.gpu
 
-PUSH_CASES = ["boris_ims", "rk4_ims", "boris_fticr", "rk4_fticr", "boris_quadrf"]
+PUSH_CASES = ["boris_ims", "rk4_ims", "boris_fticr", "rk4_fticr", "boris_quadrf", "boris_lqit", "rk4_lqit1"]
 BIT_EXACT = {"boris_ims", "rk4_ims", "boris_fticr", "rk4_fticr"}
 KEYS = ("x", "y", "z", "vx", "vy", "vz")
 
@@ -243,6 +243,39 @@ def test_fp64_gas_flow_trajectories_match_oracle(model):
         a64, am = f64.active != 0, mix.active != 0
         dz64, dzm = (f64.z - st1.z)[a64], (mix.z - st1.z)[am]
         assert abs(dzm.mean() - dz64.mean()) <= 4 * dz64.std() / np.sqrt(dz64.size)
+
+
+def test_fp64_lqit_collisions_match_oracle():
+    """Linear ion trap (RF quadrupole about the axis, axial DC well, two-axis
+    dipolar drive; AnalyticalFieldModel.cpp:81-134) with HSS in He at 50 Pa:
+    FP64 device vs oracle >= 99 % of ions to 1e-9 after 3000 steps, collision
+    counts within 1 %; the mixed form's collision count within 1 % of FP64."""
+    from helpers import domain_json
+    from icarion_b200 import config as cfg
+    kw = dict(instrument="LQIT", origin_z=-0.025, length=0.05, radius=0.004, T=300, P=50.0, gas="He",
+              rf_V=200.0, rf_f=1.0e6, dc_quad_V=1.0, axial_V=2.0,
+              dip_x_A=0.5, dip_x_f=1.0e5, dip_x_phase=0.3, dip_x_ramp=0.8, dip_y_A=0.2, dip_y_f=1.2e5)
+    e = cfg.ensemble_params(domain_json(kw), 150e-20, 1e-9)
+    assert e["instrument"] == capi.INSTRUMENT_LQIT and e["ac_dipolar"] == 1
+    n, steps = 512, 3000
+    st0 = config0_ions(n)
+    st0.x *= 0.2; st0.y *= 0.2; st0.z *= 0.2
+    ost = oracle_state(st0)
+    r = orc.run(e, ost, steps, integrator=0, collision=2, seed=123)
+    out, rs = _hss_gpu(st0, e, steps)
+    assert r["collisions"] > 50 * n
+    live = (ost["active"] != 0) & (out.active != 0)
+    assert live.sum() > 0.9 * n
+    pos = np.stack([out.x, out.y, out.z])[:, live]
+    opos = np.stack([ost["x"], ost["y"], ost["z"]])[:, live]
+    vel = np.stack([out.vx, out.vy, out.vz])[:, live]
+    ovel = np.stack([ost["vx"], ost["vy"], ost["vz"]])[:, live]
+    rel = np.maximum(np.linalg.norm(pos - opos, axis=0) / np.linalg.norm(opos, axis=0),
+                     np.linalg.norm(vel - ovel, axis=0) / np.linalg.norm(ovel, axis=0))
+    assert float(np.mean(rel < 1e-9)) >= 0.99, np.sort(rel)[-5:]
+    assert abs(rs["collisions"] - r["collisions"]) <= 0.01 * r["collisions"]
+    _, rmx = _hss_gpu(st0, e, steps, precision=capi.PREC_MIXED)
+    assert abs(rmx["collisions"] / rs["collisions"] - 1.0) < 0.01
 
 
 def test_fp64_plain_form_matches_oracle():

@@ -14,7 +14,7 @@ import oracle as orc
 from helpers import config0_ions, domain_json, ensemble_from_golden, golden_state, oracle_state
 from icarion_b200 import config as cfg
 
-PUSH_CASES = ["boris_ims", "rk4_ims", "boris_fticr", "rk4_fticr", "boris_quadrf"]
+PUSH_CASES = ["boris_ims", "rk4_ims", "boris_fticr", "rk4_fticr", "boris_quadrf", "boris_lqit", "rk4_lqit1"]
 KEYS = ("x", "y", "z", "vx", "vy", "vz")
 
 
