@@ -76,7 +76,7 @@ class Config(C.Structure):
         ("n_ensembles", C.c_int32), ("ensembles", C.POINTER(EnsembleParams)), ("rng_seed", C.c_uint64),
         ("device", C.c_int32), ("block_size", C.c_int32), ("steps_per_launch", C.c_int32),
         ("pending_threshold", C.c_int32), ("use_graphs", C.c_int32), ("steps_per_vote", C.c_int32),
-        ("stepping", C.c_int32), ("reserved", C.c_int32 * 5),
+        ("stepping", C.c_int32), ("collision_subcycles", C.c_int32), ("reserved", C.c_int32 * 4),
     ]
 
 

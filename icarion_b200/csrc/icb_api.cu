@@ -592,6 +592,7 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.pend_threshold = h->pend;
         p.steps_per_vote = h->spv;
         p.jumps = h->cfg.stepping == ICB_STEPPING_EVENTS ? 1u : 0u;
+        p.subcycles = h->cfg.collision_subcycles > 1 ? static_cast<uint32_t>(h->cfg.collision_subcycles) : 1u;
         p.ens_base = static_cast<uint32_t>(e0);
         p.n_ens = static_cast<uint32_t>(ne);
         p.do_push = do_push; p.do_collide = do_collide; p.do_finalize = do_finalize;
@@ -780,6 +781,10 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
             break;
         default: return fail(ICB_ERR_UNSUPPORTED, "collision model %d not available", cfg->collision_model);
     }
+    if (cfg->collision_subcycles < 0 || cfg->collision_subcycles > 1024)
+        return fail(ICB_ERR_INVALID_ARGUMENT, "collision_subcycles must be in [0, 1024]");
+    if (cfg->collision_subcycles > 1 && cfg->collision_model != ICB_COLLISION_HSS_PLAIN)
+        return fail(ICB_ERR_UNSUPPORTED, "collision sub-steps need ICB_COLLISION_HSS_PLAIN");
     int ndev = 0;
     cudaError_t ce = cudaGetDeviceCount(&ndev);
     if (ce != cudaSuccess || ndev == 0) return fail(ICB_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(ce));

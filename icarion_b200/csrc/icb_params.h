@@ -137,6 +137,7 @@ struct StepParams {
     uint32_t n_ens;
     uint32_t do_push, do_collide, do_finalize, steps_per_vote;
     uint32_t jumps;                    // event-to-event drift where the kernel supports it
+    uint32_t subcycles;                // collision sub-steps per step (plain form), >= 1
     uint32_t flows;                    // some ensemble of the launch has a parabolic gas flow
     uint64_t ens_off[kMaxLaunchEns + 1];  // absolute ion offsets of the chunk's ensembles
     EnsConst ens[kMaxLaunchEns];

@@ -885,9 +885,9 @@ __device__ __forceinline__ int candidate_mix(const EnsConst& C, const MixConst& 
 // measured against; returns true on a collision.
 template <class R>
 __device__ __forceinline__ bool plain_hss(const EnsConst& C, R v[3], double mi_d, const uint32_t* rk, uint32_t id,
-                                          uint32_t step, R ugz) {
-    const U4 a = philox4x32_10_rk(id, step, 0u, 0u, rk);
-    const U4 b = philox4x32_10_rk(id, step, 1u, 0u, rk);
+                                          uint32_t step, R ugz, R A, uint32_t sub0) {
+    const U4 a = philox4x32_10_rk(id, step, sub0 + 0u, 0u, rk);
+    const U4 b = philox4x32_10_rk(id, step, sub0 + 1u, 0u, rk);
     const R sn = static_cast<R>(C.sig_n);
     R vn[3];
     const uint32_t w1[3] = {a.x, a.z, b.x}, w2[3] = {a.y, a.w, b.y};
@@ -900,9 +900,9 @@ __device__ __forceinline__ bool plain_hss(const EnsConst& C, R v[3], double mi_d
     }
     const R gx = v[0] - vn[0], gy = v[1] - vn[1], gz = v[2] - vn[2];
     const R g = m_sqrt(gx * gx + gy * gy + gz * gz);
-    const R P = -m_expm1(-static_cast<R>(C.A) * g);
+    const R P = -m_expm1(-A * g);
     if (!(u32(b.z, R(0)) < P)) return false;
-    const U4 c4 = philox4x32_10_rk(id, step, 2u, 0u, rk);
+    const U4 c4 = philox4x32_10_rk(id, step, sub0 + 2u, 0u, rk);
     const R mi = static_cast<R>(mi_d), mn = static_cast<R>(C.m_gas);
     const R inv = R(1) / (mi + mn);
     const R fac = mn * inv;
@@ -1263,8 +1263,14 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
             if (do_coll) cand = (kk == nk);
         } else if constexpr (COLL == kCollHSSPlain) {
             if (do_coll) {
-                ++n_cand;
-                if (plain_hss<R>(C, v, m, p.rk, id, step0 + kk, flow_z())) ++n_coll;
+                // m collision sub-steps of dt/m at this position; sub-step j
+                // draws from Philox substreams 4j, 4j + 1, 4j + 2
+                const uint32_t ms = p.subcycles;
+                const R A = ms > 1u ? static_cast<R>(C.A / static_cast<double>(ms)) : static_cast<R>(C.A);
+                for (uint32_t j = 0; j < ms; ++j) {
+                    ++n_cand;
+                    if (plain_hss<R>(C, v, m, p.rk, id, step0 + kk, flow_z(), A, 4u * j)) ++n_coll;
+                }
             }
         } else if constexpr (COLL != kCollNone) {
             if (do_coll) {

@@ -86,7 +86,7 @@ class Simulation:
                  integrator: int = capi.INTEGRATOR_BORIS, collision: int = capi.COLLISION_HSS,
                  rng_seed: int = 123, device: int = 0, block_size: int = 0, steps_per_launch: int = 0,
                  pending_threshold: int = 0, use_graphs: int = 0, steps_per_vote: int = 0,
-                 stepping: int = capi.STEPPING_EVENTS):
+                 stepping: int = capi.STEPPING_EVENTS, collision_subcycles: int = 0):
         self._lib = capi.lib()
         self.n_ens = len(ensembles)
         self._ens = (capi.EnsembleParams * self.n_ens)(*[cfgmod.to_struct(e) for e in ensembles])
@@ -104,6 +104,7 @@ class Simulation:
         cfg.use_graphs = use_graphs
         cfg.steps_per_vote = steps_per_vote
         cfg.stepping = stepping
+        cfg.collision_subcycles = collision_subcycles
         self._h = C.c_void_p()
         capi.check(self._lib.icb_create(C.byref(cfg), C.byref(self._h)))
         self.ensembles = ensembles

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define ICB_ABI_VERSION 6
+#define ICB_ABI_VERSION 7
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -155,7 +155,13 @@ typedef struct icb_config {
     int32_t use_graphs;        /* capture launch sequences in CUDA graphs */
     int32_t steps_per_vote;    /* collision-free steps between warp votes, 0 = default */
     int32_t stepping;          /* ICB_STEPPING_* (0 = event-to-event drift where supported) */
-    int32_t reserved[5];
+    /* Collision sub-steps per step (physics.collision_subcycles_per_step, or
+     * collision_max_events_per_step in multi-event mode;
+     * SimulationEngineCollisionRuntime.cpp:79-190): m > 1 repeats the
+     * collision test m times per step with dt/m at the pushed position.
+     * Needs ICB_COLLISION_HSS_PLAIN; 0 or 1 = one test per step. */
+    int32_t collision_subcycles;
+    int32_t reserved[4];
 } icb_config;
 
 /* Stepping of the fused float forms (MIXED, MIXED_HILO) with Boris in a

@@ -740,10 +740,17 @@ static int mix_candidate(const orc_domain* d, const gas_consts* G, double v[3], 
  * P = 1 - exp(-n sigma g dt), isotropic COM scatter (CollisionKernels.cpp:
  * 139-169).  Words: a = (u1, u2, u1', u2'), b = (u1'', u2'', accept, cos),
  * c = (phi, -, -, -). */
-static int plain_hss(const gas_consts* G, double v[3], double mi, uint64_t seed, uint32_t id, uint32_t step) {
+/* Collision sub-steps per step for the plain form (collision 6): m tests of
+ * dt/m at the pushed position (SimulationEngineCollisionRuntime.cpp:79-190),
+ * sub-step j from Philox substreams 4j, 4j + 1, 4j + 2. */
+static int g_subcycles = 1;
+void orc_set_subcycles(int m) { g_subcycles = m > 1 ? m : 1; }
+
+static int plain_hss(const gas_consts* G, double v[3], double mi, uint64_t seed, uint32_t id, uint32_t step,
+                     uint32_t sub0) {
     uint32_t a[4], b[4], c[4];
-    philox_words(seed, id, step, 0u, a);
-    philox_words(seed, id, step, 1u, b);
+    philox_words(seed, id, step, sub0 + 0u, a);
+    philox_words(seed, id, step, sub0 + 1u, b);
     const uint32_t w1[3] = {a[0], a[2], b[0]}, w2[3] = {a[1], a[3], b[1]};
     double vn[3];
     for (int k = 0; k < 3; ++k)
@@ -752,7 +759,7 @@ static int plain_hss(const gas_consts* G, double v[3], double mi, uint64_t seed,
     const double g = sqrt(gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2]);
     const double P = -expm1(-G->A * g);
     if (!(u32_to_unit(b[2]) < P)) return 0;
-    philox_words(seed, id, step, 2u, c);
+    philox_words(seed, id, step, sub0 + 2u, c);
     const double mn = G->mn;
     const double inv = 1.0 / (mi + mn);
     const double fac = mn * inv;
@@ -1022,8 +1029,12 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                     if (collision == 6) {
                         gas_consts Gp = Gi;
                         gas_flow_at(d, p, Gp.ug);            /* flow at the ion after the push */
-                        ++cand_tot;
-                        coll_tot += (uint64_t)plain_hss(&Gp, v, m, seed, id, (uint32_t)(step0 + (uint64_t)k));
+                        if (g_subcycles > 1) Gp.A = Gi.A / (double)g_subcycles;
+                        for (int j = 0; j < g_subcycles; ++j) {
+                            ++cand_tot;
+                            coll_tot += (uint64_t)plain_hss(&Gp, v, m, seed, id, (uint32_t)(step0 + (uint64_t)k),
+                                                            4u * (uint32_t)j);
+                        }
                     } else if (collision == 1) {
                         coll_tot += (uint64_t)hss_reference(d, p, v, m, rng);
                     } else if (skip) {

@@ -93,6 +93,7 @@ def lib() -> C.CDLL:
                               DP, U64P, C.c_int]
         L.orc_run.restype = C.c_int
         L.orc_set_ehss.argtypes = [DP, C.c_int, C.c_double]
+        L.orc_set_subcycles.argtypes = [C.c_int]
         L.orc_ehss_scatter_many.argtypes = [C.c_int64, DP, DP, C.c_double, C.c_double, C.c_uint64, DP]
         L.orc_set_ipm_table.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_double, C.c_double]
         L.orc_ipm_cos_chi_trajectory.argtypes = [C.c_double] * 7
@@ -180,7 +181,7 @@ def philox(ctr: np.ndarray, seed: int) -> np.ndarray:
 
 def run(domain: dict, state: dict, n_steps: int, *, integrator: int = 0, collision: int = 0, seed: int = 123,
         first_id: int = 0, step0: int = 0, t0: float = 0.0, snap_every: int = 0, ref_step: int = 0,
-        clock: tuple | None = None, threads: int = 1) -> dict:
+        clock: tuple | None = None, threads: int = 1, subcycles: int = 1) -> dict:
     """Run the restatement.  ``state`` holds float64 arrays x..vz, mass, charge,
     uint8 active and optional t_death / t_arrival; it is updated in place.
     collision: 0 none, 1 reference HSS (mt19937_64 per ion), 2 null-collision
@@ -189,9 +190,11 @@ def run(domain: dict, state: dict, n_steps: int, *, integrator: int = 0, collisi
     clock), 3 Langevin capture with Philox (Boris, skip clock), 4
     interaction-potential table collisions (Boris, skip clock; table from
     set_ipm_table), 5 HSS gas mixture (Boris, skip clock), 6 the reference's
-    per-step HSS form with Philox words (no clock), 7 EHSS on the geometry
-    of set_ehss (Boris, skip clock)."""
+    per-step HSS form with Philox words (no clock; ``subcycles`` collision
+    sub-steps of dt/m per step), 7 EHSS on the geometry of set_ehss (Boris,
+    skip clock)."""
     d = domain_struct(domain)
+    lib().orc_set_subcycles(int(subcycles))
     n = state["x"].shape[0]
     for k in ("t_death", "t_arrival"):
         if state.get(k) is None:

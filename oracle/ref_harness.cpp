@@ -363,6 +363,9 @@ int mode_run(const Args& a) {
     // the collision environment of ion i: the reference engine evaluates a
     // non-constant gas flow at the ion's position before each collision
     // (SimulationEngineCollisionRuntime.cpp:124-131; unrotated cylinder)
+    // collision sub-steps: handle_collision m times with dt / m at the pushed
+    // position (SimulationEngineCollisionRuntime.cpp:79-190)
+    const int subcycles = std::max(1, static_cast<int>(num(a, "subcycles", 1.0)));
     const bool flow_var = d.environment.flow_model != config::FlowModelKind::Constant;
     auto env_at = [&](int64_t i) -> const config::EnvironmentConfig& {
         if (!flow_var) return d.environment;
@@ -394,7 +397,8 @@ int mode_run(const Args& a) {
                 for (int64_t i = 0; i < n; ++i) {
                     if (!active[i]) continue;
                     auto cv = ens.collision_data(static_cast<size_t>(i));
-                    collisions += hss.handle_collision(cv, dt, rng[static_cast<size_t>(i)], env_at(i)) ? 1 : 0;
+                    for (int sc = 0; sc < subcycles; ++sc)
+                        collisions += hss.handle_collision(cv, dt / subcycles, rng[static_cast<size_t>(i)], env_at(i)) ? 1 : 0;
                 }
             }
         } else if (faithful) {
@@ -406,7 +410,8 @@ int mode_run(const Args& a) {
                 for (int64_t i = 0; i < n; ++i) {
                     if (!active[i]) continue;
                     auto cv = ens.collision_data(static_cast<size_t>(i));
-                    collisions += hss.handle_collision(cv, dt, rng[static_cast<size_t>(i)], env_at(i)) ? 1 : 0;
+                    for (int sc = 0; sc < subcycles; ++sc)
+                        collisions += hss.handle_collision(cv, dt / subcycles, rng[static_cast<size_t>(i)], env_at(i)) ? 1 : 0;
                 }
             }
         } else {
@@ -417,7 +422,8 @@ int mode_run(const Args& a) {
                 boris.step(ens, static_cast<size_t>(i), t, dt, *reg);
                 if (coll == "hss") {
                     auto cv = ens.collision_data(static_cast<size_t>(i));
-                    collisions += hss.handle_collision(cv, dt, rng[static_cast<size_t>(i)], env_at(i)) ? 1 : 0;
+                    for (int sc = 0; sc < subcycles; ++sc)
+                        collisions += hss.handle_collision(cv, dt / subcycles, rng[static_cast<size_t>(i)], env_at(i)) ? 1 : 0;
                 }
             }
         }

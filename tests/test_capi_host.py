@@ -60,7 +60,7 @@ def test_struct_sizes_match_c_layout():
 
 def test_abi_version_and_error_reporting_without_compute():
     lib = capi.lib()
-    assert lib.icb_abi_version() == 6
+    assert lib.icb_abi_version() == 7
     # invalid configuration is rejected before any device work
     h = C.c_void_p()
     c = capi.Config()
@@ -105,3 +105,26 @@ def test_shard_ranges_cover_all_ions():
             assert max(e - b for b, e in spans) - min(e - b for b, e in spans) <= 1
     off = np.array([0, 10, 25, 40], dtype=np.uint64)
     assert parallel.shard_offsets(off, 12, 30).tolist() == [0, 0, 13, 18]
+
+
+def test_collision_substeps_need_the_plain_form():
+    """Collision sub-steps run in the plain per-step form only; the
+    null-collision forms reject them before any device work, and so does a
+    count outside [0, 1024]."""
+    import sys
+    sys.path.insert(0, str(ROOT / "tests"))
+    from helpers import config0_ensemble
+    ens = (capi.EnsembleParams * 1)(cfg.to_struct(config0_ensemble()))
+    for coll, sub, rc in ((capi.COLLISION_HSS, 4, capi.ICB_ERR_UNSUPPORTED),
+                          (capi.COLLISION_HSS_PLAIN, 2000, capi.ICB_ERR_INVALID_ARGUMENT),
+                          (capi.COLLISION_HSS_PLAIN, -1, capi.ICB_ERR_INVALID_ARGUMENT)):
+        c = capi.Config()
+        c.precision = capi.PREC_FP64
+        c.integrator = capi.INTEGRATOR_BORIS
+        c.collision_model = coll
+        c.n_ensembles = 1
+        c.ensembles = C.cast(ens, C.POINTER(capi.EnsembleParams))
+        c.collision_subcycles = sub
+        h = C.c_void_p()
+        assert capi.lib().icb_create(C.byref(c), C.byref(h)) == rc
+        assert "collision" in capi.lib().icb_last_error().decode()

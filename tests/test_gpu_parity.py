@@ -278,16 +278,18 @@ def test_fp64_lqit_collisions_match_oracle():
     assert abs(rmx["collisions"] / rs["collisions"] - 1.0) < 0.01
 
 
-def test_fp64_plain_form_matches_oracle():
-    """The plain per-step HSS form (the bench's plain FP64 baseline) against
-    the oracle with the same Philox words: >= 99 % of ions to 1e-9 after
-    3000 steps, collision counts within 1 %."""
+@pytest.mark.parametrize("subcycles", [1, 4])
+def test_fp64_plain_form_matches_oracle(subcycles):
+    """The plain per-step HSS form (the bench's plain FP64 baseline; with 4
+    collision sub-steps per step) against the oracle with the same Philox
+    words: >= 99 % of ions to 1e-9 after 3000 steps, collision counts within
+    1 %."""
     n, steps = 512, 3000
     e = config0_ensemble()
     st0 = config0_ions(n)
     ost = oracle_state(st0)
-    r = orc.run(e, ost, steps, integrator=0, collision=6, seed=123)
-    out, rs = _hss_gpu(st0, e, steps, collision=capi.COLLISION_HSS_PLAIN)
+    r = orc.run(e, ost, steps, integrator=0, collision=6, seed=123, subcycles=subcycles)
+    out, rs = _hss_gpu(st0, e, steps, collision=capi.COLLISION_HSS_PLAIN, collision_subcycles=subcycles)
     pos = np.stack([out.x, out.y, out.z])
     opos = np.stack([ost["x"], ost["y"], ost["z"]])
     vel = np.stack([out.vx, out.vy, out.vz])
@@ -296,7 +298,7 @@ def test_fp64_plain_form_matches_oracle():
                      np.linalg.norm(vel - ovel, axis=0) / np.linalg.norm(ovel, axis=0))
     assert float(np.mean(rel < 1e-9)) >= 0.99, np.sort(rel)[-5:]
     assert abs(rs["collisions"] - r["collisions"]) <= 0.01 * r["collisions"]
-    assert rs["candidates"] == n * steps
+    assert rs["candidates"] == n * steps * subcycles
 
 
 def test_fp64_ehss_trajectories_match_oracle():
