@@ -364,19 +364,22 @@ __global__ void __launch_bounds__(256) k_sc_gather(MeshGeom g, PPParams pp, cons
                     const uint32_t sa = start[row + static_cast<uint32_t>(z0)];
                     const uint32_t sb = start[row + static_cast<uint32_t>(z1) + 1u];
                     for (uint32_t s2 = sa; s2 < sb; ++s2) {
+                        // every pair takes the same instructions; pairs outside
+                        // (min_d, r_c) or the ion itself add nothing (select)
                         const float4 qf = pf[s2];
                         const float dx = fxi - qf.x, dy = fyi - qf.y, dz = fzi - qf.z;
                         const float r2 = dx * dx + dy * dy + dz * dz;
-                        if (s2 == s || r2 >= pp.rc2f || r2 < pp.min_d2f) continue;
-                        const float r = sqrtf(r2);
-                        const float u = r * pp.inv_drf;
-                        const int kt = min(static_cast<int>(u), kPPTable - 1);
+                        const bool near = s2 != s && r2 < pp.rc2f && r2 >= pp.min_d2f;
+                        const float rinv = rsqrtf(r2);
+                        const float u = r2 * rinv * pp.inv_drf;
+                        const int kt = max(min(static_cast<int>(u), kPPTable - 1), 0);
                         const float fr = u - static_cast<float>(kt);
                         const float L = fmaf(fr, tabf[kt + 1] - tabf[kt], tabf[kt]);
-                        const float sc = kc * (1.f / (r2 + pp.eps2f) - L / r2) / r * qf.w;
-                        Ef[0] += dx * sc;
-                        Ef[1] += dy * sc;
-                        Ef[2] += dz * sc;
+                        // kc (1 / (r^2 + eps^2) - L / r^2) / r q_j
+                        const float sc = kc * (__fdividef(1.f, r2 + pp.eps2f) - L * rinv * rinv) * rinv * qf.w;
+                        Ef[0] += near ? dx * sc : 0.f;
+                        Ef[1] += near ? dy * sc : 0.f;
+                        Ef[2] += near ? dz * sc : 0.f;
                     }
                 }
             }
