@@ -70,6 +70,51 @@ ICB_HD U4 philox4x32_10_rk(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, c
     return U4{c0, c1, c2, c3};
 }
 
+// The candidate draws of one ion: counter (id, step, s, 0) for s = 0, 1.
+// The first round depends on the step only through c1, and the second
+// round's multiply of c2 only on the ion, so both are formed once per ion:
+// after round 0 the state is (w_s ^ step, lo(M1 s), hi(M0 id) ^ rk1,
+// lo(M0 id)) with w_s = hi(M1 s) ^ rk0; round 1 then needs one multiply.
+// philox_ion(pre, step, s) equals philox4x32_10_rk(id, step, s, 0, rk).
+struct PhiloxIon {
+    uint32_t x1[2];   // round-1 outputs c0 = hi(M1 c2_1) ^ lo(M1 s) ^ rk2, s = 0, 1
+    uint32_t y1;      // c1 = lo(M1 c2_1)
+    uint32_t z1;      // lo(M0 id) ^ rk3 (folds into c2 of round 1)
+};
+
+ICB_HD PhiloxIon philox_ion_setup(uint32_t id, const uint32_t* rk) {
+    PhiloxIon q;
+    const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * id;
+    const uint32_t c2_1 = static_cast<uint32_t>(p0 >> 32) ^ rk[1];
+    const uint64_t p1 = static_cast<uint64_t>(0xCD9E8D57u) * c2_1;
+    for (uint32_t s = 0; s < 2; ++s) {
+        const uint32_t lo_s = static_cast<uint32_t>(static_cast<uint64_t>(0xCD9E8D57u) * s);
+        q.x1[s] = static_cast<uint32_t>(p1 >> 32) ^ lo_s ^ rk[2];
+    }
+    q.y1 = static_cast<uint32_t>(p1);
+    q.z1 = static_cast<uint32_t>(p0) ^ rk[3];
+    return q;
+}
+
+ICB_HD U4 philox_ion(const PhiloxIon& q, uint32_t step, uint32_t s, const uint32_t* rk) {
+    // round 0: c0 = hi(M1 s) ^ step ^ rk0 (the only step-dependent word)
+    const uint32_t hi_s = static_cast<uint32_t>((static_cast<uint64_t>(0xCD9E8D57u) * s) >> 32);
+    const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * (hi_s ^ step ^ rk[0]);
+    // round 1
+    uint32_t c0 = q.x1[s], c1 = q.y1;
+    uint32_t c2 = static_cast<uint32_t>(p0 >> 32) ^ q.z1, c3 = static_cast<uint32_t>(p0);
+#pragma unroll
+    for (int r = 2; r < 10; ++r) {
+        const uint64_t a = static_cast<uint64_t>(0xD2511F53u) * c0;
+        const uint64_t b = static_cast<uint64_t>(0xCD9E8D57u) * c2;
+        c0 = static_cast<uint32_t>(b >> 32) ^ c1 ^ rk[2 * r];
+        c1 = static_cast<uint32_t>(b);
+        c2 = static_cast<uint32_t>(a >> 32) ^ c3 ^ rk[2 * r + 1];
+        c3 = static_cast<uint32_t>(a);
+    }
+    return U4{c0, c1, c2, c3};
+}
+
 // 32-bit word -> double in (0, 1]: (w + 1) * 2^-32, exact.
 ICB_HD double unit_d(uint32_t w) { return (static_cast<double>(w) + 1.0) * 2.3283064365386963e-10; }
 // 32-bit word -> float in (0, 1]: (top 24 bits + 1) * 2^-24, exact.

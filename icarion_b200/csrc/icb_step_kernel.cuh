@@ -667,7 +667,7 @@ __device__ void ehss_scatter(const StepParams& p, uint32_t eg, R v[3], const R v
 template <class R, bool SKIP, int COLL>
 __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qstar, R Amean, R b, double mi_d,
                                          const uint32_t* rk, uint32_t id, uint32_t step, const StepParams& p,
-                                         IpmPend<R>* ip, uint32_t eg) {
+                                         IpmPend<R>* ip, uint32_t eg, const PhiloxIon& pq) {
     constexpr bool LANG = COLL == kCollLangevin;
     R A, mean_th, sig_n, ug[3], mi, mn, inv_mt, fac;
     if constexpr (sizeof(R) == 8) {
@@ -688,7 +688,7 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
     // (thinned, rejected, collided) selects what is kept.  The values are
     // those of the early-exit form.
     constexpr bool kFlat = COLL == kCollHSS || COLL == kCollLangevin;
-    const U4 r0 = philox4x32_10_rk(id, step, 0u, 0u, rk);
+    const U4 r0 = philox_ion(pq, step, 0u, rk);   // = philox4x32_10_rk(id, step, 0, 0, rk)
     R uc = u32(r0.y, R(0));
     bool kept = true;                 // not thinned away
     if constexpr (SKIP) {
@@ -704,7 +704,7 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
     } else {
         clk = u32(r0.x, R(0));
     }
-    const U4 r1 = philox4x32_10_rk(id, step, 1u, 0u, rk);
+    const U4 r1 = philox_ion(pq, step, 1u, rk);
     // Langevin capture: Maxwellian neutral (the thermal branch), every event collides
     const bool thermal = LANG || (uc * (b + mean_th) < b);
     R c3, s3;
@@ -786,7 +786,7 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
 template <class R, bool SKIP>
 __device__ __forceinline__ int candidate_mix(const EnsConst& C, const MixConst& M, R v[3], R& clk, R qstar,
                                              R Amean, R b, double mi_d, const uint32_t* rk, uint32_t id,
-                                             uint32_t step) {
+                                             uint32_t step, const PhiloxIon& pq) {
     constexpr bool D = sizeof(R) == 8;
     R ug[3], mi;
     if constexpr (D) {
@@ -801,7 +801,7 @@ __device__ __forceinline__ int candidate_mix(const EnsConst& C, const MixConst& 
     auto Mi = [&](int i) -> R { if constexpr (D) return M.mean_th[i]; else return M.fmean_th[i]; };
     auto Si = [&](int i) -> R { if constexpr (D) return M.sig_n[i]; else return M.fsig_n[i]; };
     auto Gm = [&](int i) -> R { if constexpr (D) return M.m[i]; else return M.fm[i]; };
-    const U4 r0 = philox4x32_10_rk(id, step, 0u, 0u, rk);
+    const U4 r0 = philox_ion(pq, step, 0u, rk);
     R uc = u32(r0.y, R(0));
     if constexpr (SKIP) {
         clk = -m_log(u32(r0.x, R(0)));
@@ -827,7 +827,7 @@ __device__ __forceinline__ int candidate_mix(const EnsConst& C, const MixConst& 
     }
     const R qsel = Ai(ci) * (b + Mi(ci));
     const R uci = m_fmin((target - cum) / qsel, R(1));
-    const U4 r1 = philox4x32_10_rk(id, step, 1u, 0u, rk);
+    const U4 r1 = philox_ion(pq, step, 1u, rk);
     const bool thermal = uci * (b + Mi(ci)) < b;
     R c3, s3;
     angle_cs(u16(r1.y >> 16, R(0)), c3, s3);
@@ -1033,6 +1033,8 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
     }
 
     const uint32_t id = static_cast<uint32_t>(p.first_id + i);
+    // the ion's share of the candidate draws' first two Philox rounds
+    const PhiloxIon pq = philox_ion_setup(id, p.rk);
     const uint32_t step0 = static_cast<uint32_t>(*p.step_dev);
     uint32_t n_cand = 0, n_coll = 0, n_ovf = 0, n_dead = 0, n_arr = 0;
 
@@ -1193,9 +1195,9 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
                     if (p.flows && C.flow) { v[2] = v[2] - flow_z(); shifted = true; }
                     int st;
                     if constexpr (COLL == kCollHSSMix)
-                        st = candidate_mix<R, true>(C, p.mix[p.ens_base + e], v, S, U, k.Amean, b, m, p.rk, id, gs);
+                        st = candidate_mix<R, true>(C, p.mix[p.ens_base + e], v, S, U, k.Amean, b, m, p.rk, id, gs, pq);
                     else
-                        st = candidate<R, true, COLL>(C, v, S, U, k.Amean, b, m, p.rk, id, gs, p, &ip, p.ens_base + e);
+                        st = candidate<R, true, COLL>(C, v, S, U, k.Amean, b, m, p.rk, id, gs, p, &ip, p.ens_base + e, pq);
                     if (st >= 1) ++n_cand;
                     if (st >= 2) ++n_coll;
                     need_net = st == 3;
@@ -1205,9 +1207,9 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
                 ++n_cand;
                 int st;
                 if constexpr (COLL == kCollHSSMix)
-                    st = candidate_mix<R, false>(C, p.mix[p.ens_base + e], v, U, R(0), k.Amean, b, m, p.rk, id, gs);
+                    st = candidate_mix<R, false>(C, p.mix[p.ens_base + e], v, U, R(0), k.Amean, b, m, p.rk, id, gs, pq);
                 else
-                    st = candidate<R, false, COLL>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs, p, &ip, p.ens_base + e);
+                    st = candidate<R, false, COLL>(C, v, U, R(0), k.Amean, b, m, p.rk, id, gs, p, &ip, p.ens_base + e, pq);
                 if (st >= 2) ++n_coll;
                 need_net = st == 3;
             }

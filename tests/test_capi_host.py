@@ -128,3 +128,49 @@ def test_collision_substeps_need_the_plain_form():
         h = C.c_void_p()
         assert capi.lib().icb_create(C.byref(c), C.byref(h)) == rc
         assert "collision" in capi.lib().icb_last_error().decode()
+
+
+def test_per_ion_philox_rounds_equal_the_generator():
+    """The kernel forms the candidate draws' first two Philox rounds once per
+    ion (icb_rng.cuh: philox_ion_setup / philox_ion); on random keys, ions,
+    steps and both candidate substreams the words equal Philox4x32-10's
+    (compiled on the host from the same header), and those equal the
+    oracle's generator."""
+    import sys
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    src = r'''
+    #include <cstdio>
+    #include <cstdint>
+    #include "icb_rng.cuh"
+    using namespace icb;
+    int main() {
+        uint64_t x = 0x9E3779B97F4A7C15ull;
+        auto next = [&]() { x ^= x << 13; x ^= x >> 7; x ^= x << 17; return x; };
+        for (int t = 0; t < 4000; ++t) {
+            const uint64_t seed = next();
+            uint32_t rk[20];
+            philox_round_keys(seed, rk);
+            const uint32_t id = static_cast<uint32_t>(next()), step = static_cast<uint32_t>(next());
+            const PhiloxIon q = philox_ion_setup(id, rk);
+            for (uint32_t s = 0; s < 2; ++s) {
+                const U4 a = philox4x32_10_rk(id, step, s, 0u, rk), b = philox_ion(q, step, s, rk);
+                if (a.x != b.x || a.y != b.y || a.z != b.z || a.w != b.w) return 1;
+                if (t < 16) std::printf("%llu %u %u %u %u %u %u %u\n", (unsigned long long)seed, id, step, s,
+                                        a.x, a.y, a.z, a.w);
+            }
+        }
+        return 0;
+    }'''
+    tmp = Path(subprocess.run(["mktemp", "-d"], capture_output=True, text=True).stdout.strip())
+    (tmp / "p.cpp").write_text(src)
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", str(ROOT / "icarion_b200" / "csrc"), str(tmp / "p.cpp"),
+                    "-o", str(tmp / "p")], check=True)
+    out = subprocess.run([str(tmp / "p")], capture_output=True, text=True)
+    assert out.returncode == 0, "per-ion rounds differ from Philox4x32-10"
+    lines = out.stdout.splitlines()
+    assert len(lines) == 32
+    for line in lines:
+        seed, idv, step, s, *words = (int(v) for v in line.split())
+        ctr = np.array([[idv, step, s, 0]], dtype=np.uint32)
+        assert np.array_equal(orc.philox(ctr, seed)[0], np.array(words, dtype=np.uint32))
