@@ -80,7 +80,17 @@ def device_count() -> int:
 
 
 class Simulation:
-    """One device-resident population of ions in one or more ensembles."""
+    """One device-resident population of ions in one or more ensembles.
+
+    The keyword arguments are the fields of ``icb_config``: ``precision``
+    (PREC_FP64 / PREC_MIXED / PREC_MIXED_HILO), ``integrator``, ``collision``
+    (COLLISION_*), ``rng_seed``, ``device``; launch shape ``block_size``,
+    ``steps_per_launch``, ``pending_threshold``, ``steps_per_vote`` (0 =
+    defaults), ``use_graphs``; ``stepping`` (STEPPING_EVENTS: the float forms
+    move each ion from event to event in closed form; STEPPING_PER_STEP: the
+    step-by-step loop); ``collision_subcycles`` (collision tests per step,
+    plain FP64 form only).
+    """
 
     def __init__(self, ensembles: list[dict], precision: int = capi.PREC_MIXED,
                  integrator: int = capi.INTEGRATOR_BORIS, collision: int = capi.COLLISION_HSS,
