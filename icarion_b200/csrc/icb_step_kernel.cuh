@@ -16,14 +16,19 @@
 //              float offset (folded into the anchor at every warp vote).
 //   HILO       float velocity; position as a compensated float hi/lo pair.
 //
-// Deferred collisions.  A collision candidate fires in ~10% of ion-steps;
-// executed in place it would make almost every warp-step run the expensive
-// candidate branch with a few lanes active.  Instead a lane whose clock
-// fires stops ("pending") while the other lanes keep stepping; once
-// `pend_threshold` lanes of the warp are pending (or no lane can step) the
-// warp processes all pending collisions together, converged.  Every lane
-// still applies its own steps in order, so results do not depend on the
-// threshold or the launch shape.
+// Two loops run the steps.  The event-to-event form (float precisions, Boris
+// in a uniform field without B; run_jumps below) moves each lane in one
+// closed-form update to its next clock event, exact domain check or the
+// launch end, and the warp then handles the events of all its lanes
+// together.  The step-by-step loop (FP64, RK4, other fields, births,
+// ICB_STEPPING_PER_STEP) defers collisions instead: a collision candidate
+// fires in ~10% of ion-steps; executed in place it would make almost every
+// warp-step run the expensive candidate branch with a few lanes active, so
+// a lane whose clock fires stops ("pending") while the other lanes keep
+// stepping; once `pend_threshold` lanes of the warp are pending (or no lane
+// can step) the warp processes all pending collisions together, converged.
+// Every lane still applies its own steps in order, so results do not depend
+// on the threshold or the launch shape.
 #pragma once
 #include <cstdint>
 #include <cmath>
