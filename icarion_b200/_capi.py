@@ -27,7 +27,14 @@ PREC_FP64, PREC_MIXED, PREC_MIXED_HILO = 0, 1, 2
 INTEGRATOR_BORIS, INTEGRATOR_RK4 = 0, 1
 COLLISION_NONE, COLLISION_HSS, COLLISION_IPM_TABLE, COLLISION_IPM_MLP, COLLISION_LANGEVIN = 0, 1, 2, 3, 4
 COLLISION_HSS_PLAIN, COLLISION_EHSS = 5, 6
-INSTRUMENT_IMS, INSTRUMENT_FTICR, INSTRUMENT_QUADRUPOLE_RF, INSTRUMENT_LQIT = 0, 1, 2, 3
+INSTRUMENT_IMS, INSTRUMENT_FTICR, INSTRUMENT_QUADRUPOLE_RF, INSTRUMENT_LQIT, INSTRUMENT_TIMS = 0, 1, 2, 3, 4
+MAX_WAVE_POINTS = 64
+(WAVE_CONSTANT, WAVE_LINEAR, WAVE_QUADRATIC, WAVE_EXPONENTIAL, WAVE_SINUSOIDAL, WAVE_PWM, WAVE_PULSED,
+ WAVE_ARBITRARY) = range(8)
+INTERP_LINEAR, INTERP_STEP, INTERP_CUBIC = 0, 1, 2
+(CHANNEL_DC_AXIAL_V, CHANNEL_DC_QUAD_V, CHANNEL_RF_VOLTAGE_V, CHANNEL_RF_FREQUENCY_HZ,
+ CHANNEL_TIMS_RAMP_FRACTION, N_CHANNELS) = range(6)
+TIMS_RAMP_LINEAR, TIMS_RAMP_EXPONENTIAL = 0, 1
 SC_OFF, SC_P3M_ISOLATED, SC_PM_PERIODIC_REF = 0, 1, 2
 STEPPING_EVENTS, STEPPING_PER_STEP = 0, 1
 MATH_NEG_LOG1M, MATH_NEG_LOG1M_CUDA, MATH_ONE_MINUS_EXP, MATH_ONE_MINUS_EXP_CUDA = 0, 1, 2, 3
@@ -90,6 +97,23 @@ class RunStats(C.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Waveform(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32), ("clamp", C.c_int32), ("interp", C.c_int32), ("n_points", C.c_int32),
+        ("p", C.c_double * 8), ("times_s", C.c_double * 64), ("values", C.c_double * 64),
+    ]
+
+
+class TimsField(C.Structure):
+    _fields_ = [
+        ("ramp_mode", C.c_int32), ("n_nodes", C.c_int32), ("has_final_profile", C.c_int32),
+        ("reserved_", C.c_int32), ("initial_uniform_V_m", C.c_double), ("final_uniform_V_m", C.c_double),
+        ("ramp_start_s", C.c_double), ("ramp_end_s", C.c_double), ("ramp_tau_s", C.c_double),
+        ("z_positions_m", C.c_double * 64), ("initial_profile_V_m", C.c_double * 64),
+        ("final_profile_V_m", C.c_double * 64),
+    ]
 
 
 class SpaceChargeConfig(C.Structure):
@@ -173,6 +197,8 @@ SIGNATURES = {
     "icb_ipm_table": (C.c_int, [_H, _FP]),
     "icb_ipm_set_mlp": (C.c_int, [_H, _FP]),
     "icb_ehss_set_geometry": (C.c_int, [_H, C.c_int32, C.c_int32, _DP, _DP, C.c_double]),
+    "icb_set_waveform": (C.c_int, [_H, C.c_int32, C.c_int32, _P(Waveform)]),
+    "icb_set_tims_field": (C.c_int, [_H, C.c_int32, _P(TimsField)]),
     "icb_mlp_init": (C.c_int, [C.c_uint64, _FP]),
     "icb_mlp_train": (C.c_int, [C.c_int, _P(MlpTrainConfig), C.c_uint64, _FP, _FP, _FP, _DP]),
     "icb_mlp_forward": (C.c_int, [C.c_int, _FP, C.c_uint64, _FP, _FP, C.c_int]),

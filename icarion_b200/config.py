@@ -51,9 +51,214 @@ GAS_POLARIZABILITY_M3 = {
     "N2": 1.74e-30, "O2": 1.567e-30, "H2O": 1.45e-30,
 }
 
-# TIMS uses the IMS field (AnalyticalFieldModel.cpp:72)
-INSTRUMENTS = {"IMS": capi.INSTRUMENT_IMS, "TIMS": capi.INSTRUMENT_IMS, "FTICR": capi.INSTRUMENT_FTICR,
+# Every TIMS domain (and every domain with an enabled fields.TIMS block) is
+# stepped in TIMSAxialFieldModel (PhysicsSetup.cpp:190-196)
+INSTRUMENTS = {"IMS": capi.INSTRUMENT_IMS, "TIMS": capi.INSTRUMENT_TIMS, "FTICR": capi.INSTRUMENT_FTICR,
                "QuadrupoleRF": capi.INSTRUMENT_QUADRUPOLE_RF, "LQIT": capi.INSTRUMENT_LQIT}
+
+WAVE_TYPES = {"constant": capi.WAVE_CONSTANT, "linear": capi.WAVE_LINEAR, "quadratic": capi.WAVE_QUADRATIC,
+              "exponential": capi.WAVE_EXPONENTIAL, "sinusoidal": capi.WAVE_SINUSOIDAL, "pwm": capi.WAVE_PWM,
+              "pulsed": capi.WAVE_PULSED, "arbitrary": capi.WAVE_ARBITRARY}
+
+
+def waveform(obj: dict) -> capi.Waveform:
+    """A waveform JSON object -> icb_waveform, with WaveformLoader's
+    required fields, defaults and checks (WaveformLoader.cpp:60-262)."""
+    kind = obj.get("type")
+    if kind not in WAVE_TYPES:
+        raise ValueError(f"unknown waveform type {kind!r}")
+    w = capi.Waveform()
+    w.type = WAVE_TYPES[kind]
+    if kind in ("linear", "exponential", "pwm"):
+        w.clamp = int(bool(obj.get("clamp", True)))
+    req = lambda k: float(obj[k])
+    opt = lambda k, d: float(obj.get(k, d))
+    if kind == "constant":
+        p = [req("value")]
+    elif kind == "linear":
+        p = [req("start"), req("end"), opt("start_time_s", 0.0), req("end_time_s")]
+        if p[3] <= p[2]:
+            raise ValueError("LinearWaveform: end_time_s must be > start_time_s")
+    elif kind == "quadratic":
+        p = [req("a"), req("b"), req("c"), opt("start_time_s", 0.0), opt("end_time_s", 1e9)]
+    elif kind == "exponential":
+        p = [opt("offset", 0.0), req("amplitude"), req("rate_per_s"), opt("start_time_s", 0.0), opt("end_time_s", 1e9)]
+        if p[4] <= p[3]:
+            raise ValueError("ExponentialWaveform: end_time_s must be > start_time_s")
+    elif kind == "sinusoidal":
+        p = [opt("offset", 0.0), req("amplitude"), req("frequency_Hz"), opt("phase_rad", 0.0)]
+        if p[2] <= 0.0:
+            raise ValueError("SinusoidalWaveform: frequency_Hz must be positive")
+    elif kind == "pwm":
+        p = [req("low"), req("high"), req("frequency_Hz"), req("duty_cycle"), opt("phase_rad", 0.0),
+             opt("start_time_s", 0.0), opt("end_time_s", 1e9)]
+        if p[2] <= 0.0 or not 0.0 <= p[3] <= 1.0 or p[6] <= p[5]:
+            raise ValueError("PWMWaveform: needs frequency > 0, duty_cycle in [0, 1], end_time_s > start_time_s")
+    elif kind == "pulsed":
+        p = [req("low"), req("high"), req("pulse_start_s"), req("pulse_width_s")]
+        if p[3] <= 0.0 or p[2] < 0.0:
+            raise ValueError("PulsedWaveform: needs pulse_width_s > 0 and pulse_start_s >= 0")
+    else:
+        times = [float(v) for v in obj["times"]]
+        values = [float(v) for v in obj["values"]]
+        if len(times) != len(values) or len(times) < 2:
+            raise ValueError("ArbitraryWaveform: 'times' and 'values' need the same length >= 2")
+        if any(b <= a for a, b in zip(times, times[1:])):
+            raise ValueError("ArbitraryWaveform: times must be strictly increasing")
+        if len(times) > capi.MAX_WAVE_POINTS:
+            raise ValueError(f"ArbitraryWaveform: at most {capi.MAX_WAVE_POINTS} points")
+        w.interp = {"linear": capi.INTERP_LINEAR, "step": capi.INTERP_STEP,
+                    "cubic": capi.INTERP_CUBIC}[obj.get("interpolation", "linear")]
+        w.n_points = len(times)
+        w.times_s[:len(times)] = times
+        w.values[:len(values)] = values
+        p = []
+    w.p[:] = (p + [0.0] * 8)[:8]
+    return w
+
+
+def value_or_waveform(v: Any, library: dict) -> float | capi.Waveform:
+    """ValueOrWaveform JSON (number, "@id" or inline object) -> a constant or
+    a waveform (WaveformLoader::load_value_or_waveform; "@id" resolves to an
+    inline copy, local library first)."""
+    if isinstance(v, (int, float)):
+        return float(v)
+    if isinstance(v, str):
+        if not v.startswith("@"):
+            raise ValueError(f"waveform reference must start with '@' (got {v!r})")
+        if v[1:] not in library:
+            raise ValueError(f"waveform reference not found: {v[1:]}")
+        return waveform(library[v[1:]])
+    return waveform(v)
+
+
+def wave_value(w: capi.Waveform, t: float) -> float:
+    """A waveform's value at one time t (host; the FTICR radial voltage is
+    read once at t = 0, AnalyticalFieldModel.cpp:174-176)."""
+    p = list(w.p)
+    if w.type == capi.WAVE_CONSTANT:
+        return p[0]
+    if w.type == capi.WAVE_LINEAR:
+        if t < p[2]:
+            return p[0]
+        if t >= p[3]:
+            return p[1] if w.clamp else p[0]
+        return p[0] + (p[1] - p[0]) * ((t - p[2]) / (p[3] - p[2]))
+    if w.type == capi.WAVE_QUADRATIC:
+        return p[0] if (t < p[3] or t > p[4]) else p[0] + p[1] * t + p[2] * t * t
+    if w.type == capi.WAVE_EXPONENTIAL:
+        rel = 0.0 if t < p[3] else ((p[4] - p[3]) if w.clamp else 0.0) if t >= p[4] else t - p[3]
+        return p[0] + p[1] * math.exp(p[2] * rel)
+    if w.type == capi.WAVE_SINUSOIDAL:
+        return p[0] + p[1] * math.sin(2.0 * math.pi * p[2] * t + p[3])
+    if w.type == capi.WAVE_PWM:
+        if p[2] <= 0.0 or t < p[5] or (t >= p[6] and not w.clamp):
+            return p[0]
+        tr = (p[6] - p[5]) if t >= p[6] else t - p[5]
+        period = 1.0 / p[2]
+        ph = math.fmod(tr + p[4] / (2.0 * math.pi * p[2]), period)
+        ph = ph + period if ph < 0.0 else ph
+        return p[1] if ph < p[3] * period else p[0]
+    if w.type == capi.WAVE_PULSED:
+        return p[1] if p[2] <= t < p[2] + p[3] else p[0]
+    n = w.n_points
+    ts, vs = list(w.times_s[:n]), list(w.values[:n])
+    if t <= ts[0]:
+        return vs[0]
+    if t >= ts[-1]:
+        return vs[-1]
+    i1 = next(i for i, x in enumerate(ts) if x >= t)
+    i0 = i1 - 1
+    if w.interp == capi.INTERP_STEP:
+        return vs[i0]
+    a = (t - ts[i0]) / (ts[i1] - ts[i0])
+    if w.interp == capi.INTERP_LINEAR:
+        return vs[i0] + a * (vs[i1] - vs[i0])
+    raise ValueError("cubic interpolation is evaluated on the device only")
+
+
+def _scalar(v: Any) -> float:
+    """The constant of a ValueOrWaveform slot; 0 for a waveform (carried by
+    time_fields)."""
+    return float(v) if isinstance(v, (int, float)) else 0.0
+
+
+def _tims_block(fields: dict) -> dict | None:
+    t = fields.get("TIMS", fields.get("tims"))
+    if t is None or not t.get("enabled", True):
+        return None
+    return t
+
+
+def uses_tims_model(domain: dict) -> bool:
+    """PhysicsSetup.cpp:190-196: instrument TIMS or fields.TIMS.enabled."""
+    return domain.get("instrument", "IMS") == "TIMS" or _tims_block(domain.get("fields", {})) is not None
+
+
+def time_fields(domain: dict, global_waveforms: dict | None = None) -> tuple[dict, capi.TimsField | None]:
+    """Waveform channels and TIMS axial field of one domain, as the
+    reference's field model evaluates them: {ICB_CHANNEL_*: icb_waveform}
+    and an icb_tims_field (or None).
+
+    IMS and QuadrupoleRF read a voltage only when it is a constant or a
+    waveform_ref (AnalyticalFieldModel.cpp:140-147, 226-233), and the loader
+    turns every waveform, "@id" included, into an inline copy
+    (WaveformLoader.cpp:290-320): their waveforms read as 0 V.  The LQIT
+    and TIMS models evaluate inline waveforms (:41-45, TIMSAxialFieldModel.h
+    :60-64)."""
+    fields = domain.get("fields", {})
+    lib = dict(global_waveforms or {})
+    lib.update(fields.get("waveforms", {}) or {})
+    dc = fields.get("DC", fields.get("dc", {})) or {}
+    rf = fields.get("RF", fields.get("rf", {})) or {}
+    tims_on = uses_tims_model(domain)
+    inst = domain.get("instrument", "IMS")
+    evaluates_inline = tims_on or inst == "LQIT"
+    waves = {}
+    slots = ((capi.CHANNEL_DC_AXIAL_V, dc, "axial_V"), (capi.CHANNEL_DC_QUAD_V, dc, "quad_V"),
+             (capi.CHANNEL_RF_VOLTAGE_V, rf, "voltage_V"), (capi.CHANNEL_RF_FREQUENCY_HZ, rf, "frequency_Hz"))
+    for ch, blk, key in slots:
+        if key not in blk or not evaluates_inline:
+            continue
+        v = value_or_waveform(blk[key], lib)
+        if isinstance(v, capi.Waveform):
+            waves[ch] = v
+    tims = None
+    # the TIMS model reads the block's values whether or not it is enabled
+    tb = fields.get("TIMS", fields.get("tims"))
+    if tims_on and tb is not None:
+        tims = capi.TimsField()
+        mode = tb.get("ramp_mode", "linear")
+        if mode not in ("linear", "exponential"):
+            raise ValueError("TIMS ramp_mode must be 'linear' or 'exponential'")
+        tims.ramp_mode = capi.TIMS_RAMP_EXPONENTIAL if mode == "exponential" else capi.TIMS_RAMP_LINEAR
+        tims.initial_uniform_V_m = float(tb.get("axial_field_initial_uniform_V_m", 0.0))
+        tims.final_uniform_V_m = float(tb.get("axial_field_final_uniform_V_m", 0.0))
+        tims.ramp_start_s = float(tb.get("ramp_start_s", 0.0))
+        tims.ramp_end_s = float(tb.get("ramp_end_s", 0.0))
+        tims.ramp_tau_s = float(tb.get("ramp_tau_s", 1e-3))
+        z = [float(v) for v in tb.get("z_positions_m", [])]
+        pi = [float(v) for v in tb.get("axial_field_initial_profile_V_m", [])]
+        pf = [float(v) for v in tb.get("axial_field_final_profile_V_m", [])]
+        if z:
+            if len(z) < 2 or len(pi) != len(z) or (pf and len(pf) != len(z)):
+                raise ValueError("TIMS profiles need >= 2 z positions and matching profile sizes")
+            if len(z) > capi.MAX_WAVE_POINTS:
+                raise ValueError(f"TIMS profiles take at most {capi.MAX_WAVE_POINTS} nodes")
+            tims.n_nodes = len(z)
+            tims.has_final_profile = int(bool(pf))
+            tims.z_positions_m[:len(z)] = z
+            tims.initial_profile_V_m[:len(pi)] = pi
+            tims.final_profile_V_m[:len(pf)] = pf
+        if "ramp_fraction" in tb:
+            v = value_or_waveform(tb["ramp_fraction"], lib)
+            if not isinstance(v, capi.Waveform):
+                c = capi.Waveform()
+                c.type = capi.WAVE_CONSTANT
+                c.p[0] = v
+                v = c
+            waves[capi.CHANNEL_TIMS_RAMP_FRACTION] = v
+    return waves, tims
 
 
 def ac_drives(fields: dict) -> tuple[list[float], list[float], list[float], list[float], int]:
@@ -184,21 +389,28 @@ def ensemble_params(domain: dict, sigma_m2: float, dt_s: float, detector_z_m: fl
         single_gas = (0.0, GAS_MASS_KG[gas], float(sigma_m2))
     ac_amp, ac_freq, ac_phase, ac_ramp, ac_dipolar = ac_drives(fields)
     axial = 0.0
-    if "EN_Td" in dc:
+    if isinstance(dc.get("EN_Td"), (int, float)):
         axial = axial_voltage_from_en(float(dc["EN_Td"]), P, T, L)
     if "axial_V" in dc:
-        axial = float(dc["axial_V"])
+        axial = _scalar(dc["axial_V"])
+    radial = dc.get("radial_V", 0.0)
+    if not isinstance(radial, (int, float)):
+        lib = fields.get("waveforms", {}) or {}
+        radial = wave_value(value_or_waveform(radial, lib), 0.0)
+    instrument = INSTRUMENTS[domain.get("instrument", "IMS")]
+    if uses_tims_model(domain):
+        instrument = capi.INSTRUMENT_TIMS
     return {
-        "instrument": INSTRUMENTS[domain.get("instrument", "IMS")],
+        "instrument": instrument,
         "magnetic_enabled": int(bool(mag.get("enabled", False))),
         "origin_m": [float(v) for v in geom.get("origin_m", [0.0, 0.0, 0.0])],
         "length_m": L,
         "radius_m": float(geom.get("radius_m", 0.05)),
         "axial_V": axial,
-        "radial_V": float(dc.get("radial_V", 0.0)),
-        "dc_quad_V": float(dc.get("quad_V", 0.0)),
-        "rf_voltage_V": float(rf.get("voltage_V", 0.0)),
-        "rf_frequency_Hz": float(rf.get("frequency_Hz", 0.0)),
+        "radial_V": float(radial),
+        "dc_quad_V": _scalar(dc.get("quad_V", 0.0)),
+        "rf_voltage_V": _scalar(rf.get("voltage_V", 0.0)),
+        "rf_frequency_Hz": _scalar(rf.get("frequency_Hz", 0.0)),
         "B_T": [float(v) for v in mag.get("field_strength_T", [0.0, 0.0, 0.0])],
         "temperature_K": T,
         "gas_density_m3": single_gas[0],

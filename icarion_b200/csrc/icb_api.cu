@@ -300,6 +300,14 @@ struct icb_handle {
     DevBuf<uint32_t> mlp_w2;
     DevBuf<float> mlp_f;
     DevBuf<MixConst> mix;              // HSS gas mixtures, per ensemble
+    // time-dependent fields: waveforms per (ensemble, channel), TIMS axial
+    // fields, and the device table built from them
+    std::vector<icb_waveform> waves;   // n_ens * ICB_N_CHANNELS
+    std::vector<uint8_t> wave_set;
+    std::vector<icb_tims_field> tims;
+    std::vector<uint8_t> tims_set;
+    DevBuf<TimeField> tfield;
+    int base_field_kind = kFieldUniform;
     // EHSS geometry: host copies per ensemble and the device arrays
     std::vector<std::vector<double4>> ehss_host;
     std::vector<double> ehss_rgas_host;
@@ -368,6 +376,100 @@ double field_bound(const EnsConst& C, const icb_ensemble_params& P) {
     return e;
 }
 
+// Largest |value| a waveform takes at any time (infinite when unbounded).
+double wave_bound(const icb_waveform& w) {
+    const double* p = w.p;
+    switch (w.type) {
+        case ICB_WAVE_CONSTANT: return std::fabs(p[0]);
+        case ICB_WAVE_LINEAR: return std::fmax(std::fabs(p[0]), std::fabs(p[1]));
+        case ICB_WAVE_QUADRATIC: {
+            auto q = [&](double t) { return std::fabs(p[0] + p[1] * t + p[2] * t * t); };
+            double b = std::fmax(std::fabs(p[0]), std::fmax(q(p[3]), q(p[4])));
+            if (p[2] != 0.0) {
+                const double tv = -p[1] / (2.0 * p[2]);
+                if (tv > p[3] && tv < p[4]) b = std::fmax(b, q(tv));
+            }
+            return b;
+        }
+        case ICB_WAVE_EXPONENTIAL: {   // monotone in t between the start and end values
+            const double v0 = std::fabs(p[0] + p[1]);
+            const double v1 = std::fabs(p[0] + p[1] * std::exp(p[2] * (p[4] - p[3])));
+            return std::fmax(v0, v1);
+        }
+        case ICB_WAVE_SINUSOIDAL: return std::fabs(p[0]) + std::fabs(p[1]);
+        case ICB_WAVE_PWM:
+        case ICB_WAVE_PULSED: return std::fmax(std::fabs(p[0]), std::fabs(p[1]));
+        default: {
+            double m = 0.0;
+            for (int i = 0; i < w.n_points; ++i) m = std::fmax(m, std::fabs(w.values[i]));
+            // Catmull-Rom: |h10|, |h11| <= 4/27 and |dt m| <= 2 max|v| keep the
+            // spline within 1.6 max|v|
+            return w.interp == ICB_INTERP_CUBIC ? 2.0 * m : m;
+        }
+    }
+}
+
+int check_waveform(const icb_waveform& w) {
+    if (w.type < ICB_WAVE_CONSTANT || w.type > ICB_WAVE_ARBITRARY)
+        return fail(ICB_ERR_INVALID_ARGUMENT, "unknown waveform type %d", w.type);
+    for (int i = 0; i < 8; ++i)
+        if (!std::isfinite(w.p[i])) return fail(ICB_ERR_INVALID_ARGUMENT, "waveform parameter %d is not finite", i);
+    if (w.type == ICB_WAVE_ARBITRARY) {
+        if (w.n_points < 1 || w.n_points > ICB_MAX_WAVE_POINTS)
+            return fail(ICB_ERR_INVALID_ARGUMENT, "arbitrary waveform needs 1..%d points", ICB_MAX_WAVE_POINTS);
+        if (w.interp < ICB_INTERP_LINEAR || w.interp > ICB_INTERP_CUBIC)
+            return fail(ICB_ERR_INVALID_ARGUMENT, "unknown interpolation %d", w.interp);
+        for (int i = 0; i < w.n_points; ++i) {
+            if (!std::isfinite(w.times_s[i]) || !std::isfinite(w.values[i]))
+                return fail(ICB_ERR_INVALID_ARGUMENT, "arbitrary waveform point %d is not finite", i);
+            if (i > 0 && w.times_s[i] < w.times_s[i - 1])
+                return fail(ICB_ERR_INVALID_ARGUMENT, "arbitrary waveform times must be ascending");
+        }
+    }
+    if (!std::isfinite(wave_bound(w)))
+        return fail(ICB_ERR_INVALID_ARGUMENT, "waveform is unbounded over its time range (give a finite end time)");
+    return ICB_OK;
+}
+
+WaveConst wave_const(const icb_waveform& w) {
+    WaveConst c;
+    std::memset(&c, 0, sizeof(c));
+    c.type = w.type;
+    c.clamp = w.clamp;
+    c.interp = w.interp;
+    c.n = w.type == ICB_WAVE_ARBITRARY ? w.n_points : 0;
+    for (int i = 0; i < 8; ++i) c.p[i] = w.p[i];
+    for (int i = 0; i < c.n; ++i) { c.tt[i] = w.times_s[i]; c.vv[i] = w.values[i]; }
+    return c;
+}
+
+// Field bound of an ensemble on the time-dependent table (triangle
+// inequality over the axial, radial and AC terms; every waveform at its
+// largest |value|).
+double tf_bound(const EnsConst& C, const icb_ensemble_params& P, const TimeField& F, const double wb[ICB_N_CHANNELS]) {
+    const double Rp = P.radius_m + kGeomEps;
+    const double L = P.length_m;
+    double ez = 0.0;
+    double raxis = Rp;
+    if (F.inst == ICB_INSTRUMENT_TIMS) {
+        double m = std::fmax(std::fabs(F.tims_ei), std::fabs(F.tims_ef));
+        for (int i = 0; i < F.tims_nodes; ++i) {
+            m = std::fmax(m, std::fabs(F.tims_pi[i]));
+            if (F.tims_final_profile) m = std::fmax(m, std::fabs(F.tims_pf[i]));
+        }
+        ez = m;
+    } else if (F.inst == ICB_INSTRUMENT_LQIT) {
+        ez = 2.0 * (wb[kChAxial] / (L * L)) * (0.5 * L + kGeomEps);
+    } else {
+        ez = wb[kChAxial] / L;
+        raxis = std::sqrt(P.origin_m[0] * P.origin_m[0] + P.origin_m[1] * P.origin_m[1]) + Rp;
+    }
+    const double exy = 2.0 * (wb[kChQuad] + wb[kChRfV]) * raxis / (P.radius_m * P.radius_m);
+    double e = ez + exy;
+    if (C.ac) e = e + (std::fabs(C.ac_amp[0]) + std::fabs(C.ac_amp[1]));
+    return e;
+}
+
 // Per-ensemble constants exactly as the reference derives them.
 // HSS mixture constants of one ensemble (a single gas becomes n = 1).
 int build_mix(const icb_ensemble_params& P, MixConst& M) {
@@ -417,6 +519,11 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
             kind = kFieldLinear;
             break;
         }
+        case ICB_INSTRUMENT_TIMS:           // TIMSAxialFieldModel.h (time-dependent field table)
+            C.tf = 1;
+            C.r0sq = P.radius_m * P.radius_m;
+            kind = kFieldLinearRF;
+            break;
         case ICB_INSTRUMENT_LQIT: {         // AnalyticalFieldModel.cpp:81-134 (unrotated cylinder)
             // RF quadrupole about the cylinder axis, axial well about L/2
             C.c[0] = P.origin_m[0];
@@ -533,6 +640,80 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
     return ICB_OK;
 }
 
+// Rebuild the time-dependent field table, the ensembles' tf flags and
+// field bounds, and the handle's field kind from the waveforms and TIMS
+// fields set so far; uploads the table when any ensemble uses it.
+int rebuild_time_fields(icb_handle* h) {
+    const size_t ne = h->ens.size();
+    std::vector<TimeField> tfs(ne);
+    bool any = false;
+    for (size_t e = 0; e < ne; ++e) {
+        const icb_ensemble_params& P = h->ens[e];
+        EnsConst& C = h->ens_const[e];
+        bool set = false;
+        for (int c = 0; c < ICB_N_CHANNELS; ++c) set = set || h->wave_set[e * ICB_N_CHANNELS + c];
+        const bool tims = P.instrument == ICB_INSTRUMENT_TIMS;
+        C.tf = (set || tims) ? 1 : 0;
+        double base;
+        if (C.tf) {
+            any = true;
+            TimeField& F = tfs[e];
+            std::memset(&F, 0, sizeof(F));
+            F.inst = P.instrument;
+            F.L = P.length_m;
+            F.r0sq = P.radius_m * P.radius_m;
+            F.ox = P.origin_m[0]; F.oy = P.origin_m[1]; F.oz = P.origin_m[2];
+            const double constants[4] = {P.axial_V, P.dc_quad_V, P.rf_voltage_V, P.rf_frequency_Hz};
+            double wb[ICB_N_CHANNELS] = {0.0, 0.0, 0.0, 0.0, 1.0};
+            for (int c = 0; c < ICB_N_CHANNELS; ++c) {
+                if (h->wave_set[e * ICB_N_CHANNELS + c]) {
+                    const icb_waveform& w = h->waves[e * ICB_N_CHANNELS + c];
+                    F.ch[c] = wave_const(w);
+                    if (c < 4) wb[c] = wave_bound(w);
+                } else if (c < 4) {
+                    F.ch[c].type = kWaveConstant;
+                    F.ch[c].p[0] = constants[c];
+                    wb[c] = std::fabs(constants[c]);
+                }
+            }
+            F.ramp_wave = h->wave_set[e * ICB_N_CHANNELS + ICB_CHANNEL_TIMS_RAMP_FRACTION];
+            if (tims && h->tims_set[e]) {
+                const icb_tims_field& T = h->tims[e];
+                F.tims_mode = T.ramp_mode;
+                F.tims_nodes = T.n_nodes;
+                F.tims_final_profile = T.n_nodes > 0 && T.has_final_profile;
+                F.tims_t0 = T.ramp_start_s;
+                F.tims_t1 = T.ramp_end_s;
+                F.tims_tau = T.ramp_tau_s;
+                F.tims_ei = T.initial_uniform_V_m;
+                F.tims_ef = T.final_uniform_V_m;
+                for (int i = 0; i < T.n_nodes; ++i) {
+                    F.tims_z[i] = T.z_positions_m[i];
+                    F.tims_pi[i] = T.initial_profile_V_m[i];
+                    F.tims_pf[i] = T.final_profile_V_m[i];
+                }
+            }
+            base = tf_bound(C, P, F, wb);
+        } else {
+            base = field_bound(C, P);
+        }
+        if (e == 0 && h->sc) {
+            C.Emax = base + (C.Emax - h->sc_emax_base);
+            h->sc_emax_base = base;
+        } else {
+            C.Emax = base;
+        }
+    }
+    h->field_kind = any ? std::max(h->base_field_kind, static_cast<int>(kFieldLinearRF)) : h->base_field_kind;
+    if (any) {
+        ICB_CUDA(cudaStreamSynchronize(h->stream));
+        if (h->tfield.n < ne) ICB_CUDA(h->tfield.alloc(ne));
+        ICB_CUDA(cudaMemcpy(h->tfield.p, tfs.data(), ne * sizeof(TimeField), cudaMemcpyHostToDevice));
+    }
+    ++h->gen;
+    return ICB_OK;
+}
+
 inline unsigned grid_for(uint64_t n, int block) { return static_cast<unsigned>((n + block - 1) / block); }
 
 // Step kernels for ions [lo, hi) (all ions by default).
@@ -579,6 +760,7 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.mlp_w2 = h->mlp_w2.p;
         p.mlp_f = h->mlp_f.p;
         p.mix = h->mix.p;
+        p.tfield = h->tfield.p;
         p.ehss_atoms = h->ehss_atoms.p;
         p.ehss_off = h->ehss_off.p;
         p.ehss_rgas = h->ehss_rgas.p;
@@ -842,6 +1024,12 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
         ICB_CUDA(h->mix.alloc(mixes.size()));
         ICB_CUDA(cudaMemcpy(h->mix.p, mixes.data(), mixes.size() * sizeof(MixConst), cudaMemcpyHostToDevice));
     }
+    h->base_field_kind = h->field_kind;
+    h->waves.assign(h->ens.size() * ICB_N_CHANNELS, icb_waveform{});
+    h->wave_set.assign(h->ens.size() * ICB_N_CHANNELS, 0);
+    h->tims.assign(h->ens.size(), icb_tims_field{});
+    h->tims_set.assign(h->ens.size(), 0);
+    if (int r = rebuild_time_fields(h.get())) return r;
     *out = h.release();
     return ICB_OK;
 }
@@ -1246,6 +1434,57 @@ int icb_ehss_set_geometry(icb_handle* h, int32_t ensemble, int32_t n_atoms, cons
                         cudaMemcpyHostToDevice));
     ++h->gen;
     return ICB_OK;
+}
+
+int icb_set_waveform(icb_handle* h, int32_t ensemble, int32_t channel, const icb_waveform* w) {
+    if (int r = check_handle(h)) return r;
+    if (ensemble < 0 || static_cast<size_t>(ensemble) >= h->ens.size())
+        return fail(ICB_ERR_INVALID_ARGUMENT, "ensemble %d out of range", ensemble);
+    if (channel < 0 || channel >= ICB_N_CHANNELS) return fail(ICB_ERR_INVALID_ARGUMENT, "unknown channel %d", channel);
+    const int inst = h->ens[static_cast<size_t>(ensemble)].instrument;
+    if (inst == ICB_INSTRUMENT_FTICR)
+        return fail(ICB_ERR_UNSUPPORTED, "the FTICR field evaluates its voltages once (t = 0): no waveforms");
+    if (channel == ICB_CHANNEL_TIMS_RAMP_FRACTION && inst != ICB_INSTRUMENT_TIMS)
+        return fail(ICB_ERR_INVALID_ARGUMENT, "the TIMS ramp channel needs instrument TIMS");
+    if (w) {
+        if (int r = check_waveform(*w)) return r;
+    }
+    const size_t slot = static_cast<size_t>(ensemble) * ICB_N_CHANNELS + static_cast<size_t>(channel);
+    if (w) h->waves[slot] = *w;
+    h->wave_set[slot] = w ? 1 : 0;
+    return rebuild_time_fields(h);
+}
+
+int icb_set_tims_field(icb_handle* h, int32_t ensemble, const icb_tims_field* f) {
+    if (int r = check_handle(h)) return r;
+    if (ensemble < 0 || static_cast<size_t>(ensemble) >= h->ens.size())
+        return fail(ICB_ERR_INVALID_ARGUMENT, "ensemble %d out of range", ensemble);
+    if (h->ens[static_cast<size_t>(ensemble)].instrument != ICB_INSTRUMENT_TIMS)
+        return fail(ICB_ERR_INVALID_ARGUMENT, "ensemble %d is not a TIMS domain", ensemble);
+    if (f) {
+        // TIMSFieldConfig::validate (FieldsConfig.h:262-300)
+        if (f->ramp_mode != ICB_TIMS_RAMP_LINEAR && f->ramp_mode != ICB_TIMS_RAMP_EXPONENTIAL)
+            return fail(ICB_ERR_INVALID_ARGUMENT, "TIMS ramp_mode must be linear or exponential");
+        const double sc[5] = {f->initial_uniform_V_m, f->final_uniform_V_m, f->ramp_start_s, f->ramp_end_s,
+                              f->ramp_tau_s};
+        for (double v : sc)
+            if (!std::isfinite(v)) return fail(ICB_ERR_INVALID_ARGUMENT, "TIMS parameters must be finite");
+        if (f->ramp_end_s < f->ramp_start_s) return fail(ICB_ERR_INVALID_ARGUMENT, "TIMS ramp_end_s must be >= ramp_start_s");
+        if (f->ramp_mode == ICB_TIMS_RAMP_EXPONENTIAL && !(f->ramp_tau_s > 0.0))
+            return fail(ICB_ERR_INVALID_ARGUMENT, "TIMS ramp_tau_s must be > 0 for exponential mode");
+        if (f->n_nodes != 0 && (f->n_nodes < 2 || f->n_nodes > ICB_MAX_WAVE_POINTS))
+            return fail(ICB_ERR_INVALID_ARGUMENT, "TIMS profiles need 2..%d nodes", ICB_MAX_WAVE_POINTS);
+        for (int i = 0; i < f->n_nodes; ++i) {
+            if (!std::isfinite(f->z_positions_m[i]) || !std::isfinite(f->initial_profile_V_m[i]) ||
+                (f->has_final_profile && !std::isfinite(f->final_profile_V_m[i])))
+                return fail(ICB_ERR_INVALID_ARGUMENT, "TIMS profile node %d is not finite", i);
+            if (i > 0 && f->z_positions_m[i] < f->z_positions_m[i - 1])
+                return fail(ICB_ERR_INVALID_ARGUMENT, "TIMS z_positions_m must be ascending");
+        }
+        h->tims[static_cast<size_t>(ensemble)] = *f;
+    }
+    h->tims_set[static_cast<size_t>(ensemble)] = f ? 1 : 0;
+    return rebuild_time_fields(h);
 }
 
 int icb_ipm_set_mlp(icb_handle* h, const float* params) {

@@ -66,6 +66,7 @@ struct EnsConst {
     float fA, fmean_th, fsig_n, fm_gas;
     float fug[3];
     int32_t flow;
+    int32_t tf;        // time-dependent field of TimeField (waveforms, TIMS)
 };
 
 // HSS gas mixture of one ensemble (read by the candidate step only):
@@ -78,6 +79,33 @@ struct MixConst {
     int32_t pad_;
     double A[kMaxGas], mean_th[kMaxGas], sig_n[kMaxGas], m[kMaxGas];
     float fA[kMaxGas], fmean_th[kMaxGas], fsig_n[kMaxGas], fm[kMaxGas];
+};
+
+// Time-dependent field of one ensemble: voltages given as waveforms
+// (ValueOrWaveform) and the TIMS axial ramp, evaluated in FP64 at every
+// field evaluation.  Lives in device memory, one per ensemble (global index).
+constexpr int kMaxWavePoints = 64;
+enum WaveKind : int32_t {
+    kWaveConstant = 0, kWaveLinear = 1, kWaveQuadratic = 2, kWaveExponential = 3,
+    kWaveSinusoidal = 4, kWavePWM = 5, kWavePulsed = 6, kWaveArbitrary = 7
+};
+enum WaveChannel : int { kChAxial = 0, kChQuad = 1, kChRfV = 2, kChRfF = 3, kChTimsRamp = 4, kNumChannels = 5 };
+struct WaveConst {
+    int32_t type, clamp, interp, n;
+    double p[8];
+    double tt[kMaxWavePoints], vv[kMaxWavePoints];
+};
+struct TimeField {
+    int32_t inst;            // ICB_INSTRUMENT_* (IMS, QuadrupoleRF, LQIT, TIMS)
+    int32_t tims_mode;       // 0 linear, 1 exponential ramp
+    int32_t tims_nodes;      // 0 = uniform initial / final fields
+    int32_t tims_final_profile;
+    int32_t ramp_wave;       // ch[kChTimsRamp] replaces the built-in ramp
+    int32_t pad_;
+    double L, r0sq, ox, oy, oz;
+    double tims_t0, tims_t1, tims_tau, tims_ei, tims_ef;
+    double tims_z[kMaxWavePoints], tims_pi[kMaxWavePoints], tims_pf[kMaxWavePoints];
+    WaveConst ch[kNumChannels];
 };
 
 // Ion-neutral interaction potential V = c12/r^12 - c6/r^6 - c4/r^4 (SI).
@@ -120,6 +148,7 @@ struct StepParams {
     const uint32_t* mlp_w2;            // W2 as mma B fragments
     const float* mlp_f;                // W1 (128), b1 (64), b2 (64), W3 (64), b3 (1)
     const MixConst* mix;               // per ensemble (global index), HSS mixtures
+    const TimeField* tfield;           // per ensemble (global index), nullable
     // EHSS molecule geometry: atoms (x, y, z, radius) of ensemble e in
     // [ehss_off[e], ehss_off[e+1]), gas (contact) radius per ensemble
     const double4* ehss_atoms;

@@ -255,6 +255,7 @@ struct Consts {
     R A, Amean, ug[3];       // collision clock: Q = A |v - u| + A <|th|>
     R escq[3];               // space-charge force E_sc q of this step
     bool sc;                 // space charge on (one step per launch)
+    const TimeField* tf;     // time-dependent field (waveforms, TIMS) or null
 };
 
 template <class R, int FIELD, bool MAG>
@@ -311,27 +312,193 @@ __device__ void load_consts(Consts<R>& k, const EnsConst& C, double q, double m)
     k.Amean = static_cast<R>(C.A * C.mean_th);
 }
 
+// ---- time-dependent fields ------------------------------------------------------
+constexpr double kPiD = 3.141592653589793;   // M_PI
+constexpr double kMinVoltageD = 1e-12;       // MIN_VOLTAGE_THRESHOLD of the field models
+
+// std::clamp(v, 0, 1) (NaN passes through)
+__device__ __forceinline__ double clamp01(double v) { return v < 0.0 ? 0.0 : (1.0 < v ? 1.0 : v); }
+
+// One waveform at time t, each type as WaveformConfig.h:33-188 and
+// ArbitraryWaveform::evaluate (WaveformConfig.cpp:10-91) compute it.
+static __device__ __noinline__ double wave_eval(const WaveConst& w, double t) {
+    const double* p = w.p;
+    switch (w.type) {
+        case kWaveConstant: return p[0];
+        case kWaveLinear: {          // start, end, t_start, t_end
+            if (t < p[2]) return p[0];
+            if (t >= p[3]) return w.clamp ? p[1] : p[0];
+            const double duration = p[3] - p[2];
+            const double t_norm = (t - p[2]) / duration;
+            return p[0] + (p[1] - p[0]) * t_norm;
+        }
+        case kWaveQuadratic:         // a, b, c, t_start, t_end
+            if (t < p[3] || t > p[4]) return p[0];
+            return p[0] + p[1] * t + p[2] * t * t;
+        case kWaveExponential: {     // offset, amplitude, rate, t_start, t_end
+            double rel = t - p[3];
+            if (t < p[3]) rel = 0.0;
+            else if (t >= p[4]) rel = w.clamp ? p[4] - p[3] : 0.0;
+            return p[0] + p[1] * exp(p[2] * rel);
+        }
+        case kWaveSinusoidal: {      // offset, amplitude, frequency, phase
+            const double omega = 2.0 * kPiD * p[2];
+            return p[0] + p[1] * sin(omega * t + p[3]);
+        }
+        case kWavePWM: {             // low, high, frequency, duty, phase, t_start, t_end
+            if (p[2] <= 0.0) return p[0];
+            if (t < p[5]) return p[0];
+            double t_rel = t - p[5];
+            if (t >= p[6]) {
+                if (!w.clamp) return p[0];
+                t_rel = p[6] - p[5];
+            }
+            const double period = 1.0 / p[2];
+            const double phase_shift = p[4] / (2.0 * kPiD * p[2]);
+            double phase = fmod(t_rel + phase_shift, period);
+            if (phase < 0.0) phase += period;
+            return (phase < p[3] * period) ? p[1] : p[0];
+        }
+        case kWavePulsed:            // low, high, pulse_start, pulse_width
+            return (t >= p[2] && t < p[2] + p[3]) ? p[1] : p[0];
+        default: {                   // arbitrary table
+            const int n = w.n;
+            if (!(t > w.tt[0])) return w.vv[0];          // also a NaN time
+            if (t >= w.tt[n - 1]) return w.vv[n - 1];
+            int lo = 0, hi = n;      // lower_bound: first tt[i] >= t, 1 <= i <= n - 1 here
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (w.tt[mid] < t) lo = mid + 1; else hi = mid;
+            }
+            const int i1 = lo, i0 = lo - 1;
+            const double t0 = w.tt[i0], t1 = w.tt[i1], v0 = w.vv[i0], v1 = w.vv[i1];
+            if (w.interp == 1) return v0;
+            const double alpha = (t - t0) / (t1 - t0);
+            if (w.interp == 0) return v0 + alpha * (v1 - v0);
+            double m0, m1;
+            if (i0 == 0) m0 = (v1 - v0) / (t1 - t0);
+            else m0 = (v1 - w.vv[i0 - 1]) / (t1 - w.tt[i0 - 1]);
+            if (i1 == n - 1) m1 = (v1 - v0) / (t1 - t0);
+            else m1 = (w.vv[i1 + 1] - v0) / (w.tt[i1 + 1] - t0);
+            const double h00 = 2 * alpha * alpha * alpha - 3 * alpha * alpha + 1;
+            const double h10 = alpha * alpha * alpha - 2 * alpha * alpha + alpha;
+            const double h01 = -2 * alpha * alpha * alpha + 3 * alpha * alpha;
+            const double h11 = alpha * alpha * alpha - alpha * alpha;
+            const double dt = t1 - t0;
+            return h00 * v0 + h10 * dt * m0 + h01 * v1 + h11 * dt * m1;
+        }
+    }
+}
+
+// TIMS ramp fraction f(t) (TIMSAxialFieldModel.h:66-96).
+__device__ __forceinline__ double tims_ramp(const TimeField& F, double t) {
+    if (F.ramp_wave) return clamp01(wave_eval(F.ch[kChTimsRamp], t));
+    const double t0 = F.tims_t0, t1 = F.tims_t1;
+    if (t <= t0) return 0.0;
+    if (t >= t1) return 1.0;
+    const double duration = t1 - t0;
+    if (duration <= 0.0) return 1.0;
+    const double rel = t - t0;
+    if (F.tims_mode == 1) {
+        const double tau = F.tims_tau < 1e-30 ? 1e-30 : F.tims_tau;
+        const double denom = 1.0 - exp(-duration / tau);
+        if (fabs(denom) < 1e-15) return clamp01(rel / duration);
+        return clamp01((1.0 - exp(-rel / tau)) / denom);
+    }
+    return clamp01(rel / duration);
+}
+
+// Piecewise-linear axial profile at local z (TIMSAxialFieldModel.h:98-124);
+// n == 0: the uniform value.
+__device__ __forceinline__ double tims_sample(const double* zn, const double* val, int n, double z, double uni) {
+    if (n == 0) return uni;
+    if (!(z > zn[0])) return val[0];                 // also a NaN position
+    if (z >= zn[n - 1]) return val[n - 1];
+    int lo = 0, hi = n;          // lower_bound, 1 <= result <= n - 1 here
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (zn[mid] < z) lo = mid + 1; else hi = mid;
+    }
+    const int i1 = lo, i0 = lo - 1;
+    const double z0 = zn[i0], z1 = zn[i1];
+    const double dz = z1 - z0;
+    if (dz <= 0.0) return val[i0];
+    const double alpha = (z - z0) / dz;
+    return val[i0] + alpha * (val[i1] - val[i0]);
+}
+
+// Field of an ensemble with waveforms or the TIMS model, in FP64 with the
+// reference's operation order: IMS AnalyticalFieldModel.cpp:136-161,
+// QuadrupoleRF :219-248, LQIT :81-134 (RF and axial well; the AC drives are
+// added by the caller), TIMS TIMSAxialFieldModel.h:30-44, 126-148.
+template <class R, class Pos>
+__device__ __noinline__ void tf_field(const TimeField& F, const Pos& x, double t, R E[3]) {
+    const double rfv = wave_eval(F.ch[kChRfV], t);
+    double ex = 0.0, ey = 0.0, ez = 0.0;
+    if (F.inst == 4) {           // TIMS
+        const double zl = x.template rel<double>(2, F.oz);
+        const double f = tims_ramp(F, t);
+        const double ei = tims_sample(F.tims_z, F.tims_pi, F.tims_nodes, zl, F.tims_ei);
+        const double ef = tims_sample(F.tims_z, F.tims_pf, F.tims_final_profile ? F.tims_nodes : 0, zl, F.tims_ef);
+        ez = (1.0 - f) * ei + f * ef;
+        const double rff = wave_eval(F.ch[kChRfF], t);
+        const double quad = wave_eval(F.ch[kChQuad], t);
+        const double omega = 2.0 * kPiD * rff;
+        const double u = quad + rfv * cos(omega * t);
+        ex = -2.0 * x.template rel<double>(0, F.ox) * u / F.r0sq;
+        ey = 2.0 * x.template rel<double>(1, F.oy) * u / F.r0sq;
+    } else {
+        const double axial = wave_eval(F.ch[kChAxial], t);
+        const bool lqit = F.inst == 3;
+        if (fabs(rfv) > kMinVoltageD) {
+            const double rff = wave_eval(F.ch[kChRfF], t);
+            const double quad = wave_eval(F.ch[kChQuad], t);
+            const double omega = 2.0 * kPiD * rff;
+            const double u = quad + rfv * cos(omega * t);
+            ex = -2.0 * x.template rel<double>(0, lqit ? F.ox : 0.0) * u / F.r0sq;
+            ey = 2.0 * x.template rel<double>(1, lqit ? F.oy : 0.0) * u / F.r0sq;
+        }
+        if (F.inst == 0) {
+            ez = axial / F.L;
+        } else if (fabs(axial) > kMinVoltageD) {
+            if (lqit) {
+                const double alpha = axial / (F.L * F.L);
+                ez = -2.0 * alpha * (x.template rel<double>(2, F.oz) - 0.5 * F.L);
+            } else {
+                ez = axial / F.L;
+            }
+        }
+    }
+    E[0] = static_cast<R>(ex); E[1] = static_cast<R>(ey); E[2] = static_cast<R>(ez);
+}
+
 // ---- fields -----------------------------------------------------------------
 template <class R, int FIELD, class Pos>
 __device__ __forceinline__ void efield(const Consts<R>& k, const Pos& x, double t, R E[3]) {
     if constexpr (FIELD == kFieldUniform) {
         E[0] = k.E0[0]; E[1] = k.E0[1]; E[2] = k.E0[2];
         return;
-    } else {
+    } else if constexpr (FIELD == kFieldLinear) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) E[a] = k.E0[a] + k.G[a] * x.template rel<R>(a, k.c[a]);
-    }
-    if constexpr (FIELD == kFieldLinearRF) {
-        // AnalyticalFieldModel.cpp:152-158: U = dc_quad + V cos(w t);
-        // E_x = -2 x U / r0^2, E_y = 2 y U / r0^2, x and y from the
-        // quadrupole axis (c[0], c[1]: 0 for IMS / QuadrupoleRF, the
-        // cylinder axis for the LQIT, AnalyticalFieldModel.cpp:90-103).
-        // Without an RF voltage the LQIT's x, y come from G = 0.
-        if (k.rfV != R(0)) {
-            const R U = k.rfU0 + k.rfV * static_cast<R>(cos(k.rfw * t));
-            const R px = x.template rel<R>(0, k.c[0]), py = x.template rel<R>(1, k.c[1]);
-            E[0] = R(-2.0) * px * U / k.r0sq;
-            E[1] = R(2.0) * py * U / k.r0sq;
+        return;
+    } else {
+        if (k.tf != nullptr) {
+            tf_field<R>(*k.tf, x, t, E);
+        } else {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) E[a] = k.E0[a] + k.G[a] * x.template rel<R>(a, k.c[a]);
+            // AnalyticalFieldModel.cpp:152-158: U = dc_quad + V cos(w t);
+            // E_x = -2 x U / r0^2, E_y = 2 y U / r0^2, x and y from the
+            // quadrupole axis (c[0], c[1]: 0 for IMS / QuadrupoleRF, the
+            // cylinder axis for the LQIT, AnalyticalFieldModel.cpp:90-103).
+            // Without an RF voltage the LQIT's x, y come from G = 0.
+            if (k.rfV != R(0)) {
+                const R U = k.rfU0 + k.rfV * static_cast<R>(cos(k.rfw * t));
+                const R px = x.template rel<R>(0, k.c[0]), py = x.template rel<R>(1, k.c[1]);
+                E[0] = R(-2.0) * px * U / k.r0sq;
+                E[1] = R(2.0) * py * U / k.r0sq;
+            }
         }
         // LQIT AC drives (AnalyticalFieldModel.cpp:104-121)
         if (k.ac) {
@@ -1007,6 +1174,10 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
     }
     Consts<R> k;
     load_consts<R, FIELD, MAG>(k, C, q, m);
+    k.tf = nullptr;
+    if constexpr (FIELD == kFieldLinearRF) {
+        if (C.tf && p.tfield != nullptr) k.tf = p.tfield + (p.ens_base + static_cast<uint32_t>(e));
+    }
     if constexpr (COLL == kCollLangevin) {
         // speed-independent capture rate nu_i: event probability per step
         // Q = 1 - exp(-nu_i dt) (A = 0)

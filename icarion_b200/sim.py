@@ -264,6 +264,24 @@ class Simulation:
         capi.check(self._lib.icb_ehss_set_geometry(self._h, ensemble, c.shape[0], capi.dptr(c.ravel()),
                                                    capi.dptr(r), gas_radius_m))
 
+    def set_waveform(self, ensemble: int, channel: int, w: capi.Waveform | None) -> None:
+        """Drive one field channel (capi.CHANNEL_*) of an ensemble by a
+        waveform, or back to its constant (None)."""
+        capi.check(self._lib.icb_set_waveform(self._h, ensemble, channel, C.byref(w) if w is not None else None))
+
+    def set_tims_field(self, ensemble: int, f: capi.TimsField | None) -> None:
+        """TIMS axial field of a TIMS ensemble (None: zero axial field)."""
+        capi.check(self._lib.icb_set_tims_field(self._h, ensemble, C.byref(f) if f is not None else None))
+
+    def apply_time_fields(self, ensemble: int, domain: dict, global_waveforms: dict | None = None) -> None:
+        """Waveforms and TIMS field of a reference JSON domain
+        (config.time_fields) on one ensemble."""
+        waves, tims = cfgmod.time_fields(domain, global_waveforms)
+        if tims is not None:
+            self.set_tims_field(ensemble, tims)
+        for ch, w in waves.items():
+            self.set_waveform(ensemble, ch, w)
+
     def set_mlp(self, params: np.ndarray) -> None:
         p = np.ascontiguousarray(params, dtype=np.float32)
         capi.check(self._lib.icb_ipm_set_mlp(self._h, capi.fptr(p)))

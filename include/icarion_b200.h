@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define ICB_ABI_VERSION 7
+#define ICB_ABI_VERSION 8
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -68,7 +68,14 @@ enum {
     /* linear quadrupole ion trap, AnalyticalFieldModel.cpp:81-134: RF
      * quadrupole about the cylinder axis, AC drives (ac_* below) and the
      * axial DC well E_z = -2 axial_V / L^2 (z_local - L/2) */
-    ICB_INSTRUMENT_LQIT = 3
+    ICB_INSTRUMENT_LQIT = 3,
+    /* trapped IMS, TIMSAxialFieldModel.h:18-193 (the model of every domain
+     * with instrument TIMS or fields.TIMS.enabled, PhysicsSetup.cpp:190-196):
+     * E_z(z, t) = (1 - f(t)) E_initial(z) + f(t) E_final(z) in local z from
+     * icb_set_tims_field (zero without it), plus the radial quadrupole
+     * E_x = -2 x U / r0^2, E_y = 2 y U / r0^2, U = dc_quad + V cos(w t),
+     * x, y from the cylinder axis; no dc.axial_V term */
+    ICB_INSTRUMENT_TIMS = 4
 };
 
 /* Number of doubles per ensemble returned by icb_moments:
@@ -410,6 +417,74 @@ int icb_ipm_set_mlp(struct icb_handle* h, const float* params);
  * ensemble needs one before stepping with ICB_COLLISION_EHSS. */
 int icb_ehss_set_geometry(struct icb_handle* h, int32_t ensemble, int32_t n_atoms, const double* centers_m,
                           const double* radii_m, double gas_radius_m);
+
+/* ---- time-dependent fields ---------------------------------------------- */
+/* A voltage given as a waveform instead of a constant (ValueOrWaveform,
+ * WaveformConfig.h:19-276, WaveformConfig.cpp:10-107), evaluated at the
+ * field's time at every field evaluation, as the reference does.  p[] holds
+ * the type's parameters in this order:
+ *   CONSTANT     value
+ *   LINEAR       start_value, end_value, start_time_s, end_time_s (clamp)
+ *   QUADRATIC    a, b, c, start_time_s, end_time_s
+ *   EXPONENTIAL  offset, amplitude, rate_per_s, start_time_s, end_time_s (clamp)
+ *   SINUSOIDAL   offset, amplitude, frequency_Hz, phase_rad
+ *   PWM          low_value, high_value, frequency_Hz, duty_cycle, phase_rad,
+ *                start_time_s, end_time_s (clamp)
+ *   PULSED       low_value, high_value, pulse_start_s, pulse_width_s
+ *   ARBITRARY    n_points (1..ICB_MAX_WAVE_POINTS) ascending times_s and
+ *                values, interp LINEAR / STEP / CUBIC (Catmull-Rom) */
+#define ICB_MAX_WAVE_POINTS 64
+enum { ICB_WAVE_CONSTANT = 0, ICB_WAVE_LINEAR = 1, ICB_WAVE_QUADRATIC = 2, ICB_WAVE_EXPONENTIAL = 3,
+       ICB_WAVE_SINUSOIDAL = 4, ICB_WAVE_PWM = 5, ICB_WAVE_PULSED = 6, ICB_WAVE_ARBITRARY = 7 };
+enum { ICB_INTERP_LINEAR = 0, ICB_INTERP_STEP = 1, ICB_INTERP_CUBIC = 2 };
+typedef struct icb_waveform {
+    int32_t type;              /* ICB_WAVE_* */
+    int32_t clamp;             /* LINEAR / EXPONENTIAL / PWM: hold the end value after end_time_s */
+    int32_t interp;            /* ARBITRARY: ICB_INTERP_* */
+    int32_t n_points;          /* ARBITRARY */
+    double p[8];
+    double times_s[ICB_MAX_WAVE_POINTS];
+    double values[ICB_MAX_WAVE_POINTS];
+} icb_waveform;
+
+/* Field channels that may carry a waveform (fields.DC.axial_V, DC.quad_V,
+ * RF.voltage_V, RF.frequency_Hz, TIMS.ramp_fraction).  A channel without a
+ * waveform uses the constant of icb_ensemble_params (the TIMS ramp its
+ * built-in linear / exponential ramp). */
+enum { ICB_CHANNEL_DC_AXIAL_V = 0, ICB_CHANNEL_DC_QUAD_V = 1, ICB_CHANNEL_RF_VOLTAGE_V = 2,
+       ICB_CHANNEL_RF_FREQUENCY_HZ = 3, ICB_CHANNEL_TIMS_RAMP_FRACTION = 4, ICB_N_CHANNELS = 5 };
+
+/* Set (w != NULL) or clear (w == NULL) the waveform of one field channel of
+ * one ensemble (IMS, QuadrupoleRF, LQIT or TIMS).  An ensemble with a
+ * waveform, like every TIMS ensemble, is stepped through the time-dependent
+ * field path (one field evaluation per step or RK4 stage). */
+int icb_set_waveform(struct icb_handle* h, int32_t ensemble, int32_t channel, const icb_waveform* w);
+
+/* TIMS axial field (fields.TIMS, FieldsConfig.h:244-300): uniform initial /
+ * final fields, or profiles over n_nodes local z positions (2..64,
+ * ascending; the final profile may be absent, then the final uniform field
+ * applies), ramped by f(t) = clamp((t - start) / (end - start)) (linear) or
+ * (1 - e^{-(t - start)/tau}) / (1 - e^{-(end - start)/tau}) (exponential),
+ * f = 0 before start and 1 after end; a TIMS.ramp_fraction waveform
+ * (channel ICB_CHANNEL_TIMS_RAMP_FRACTION, clamped to [0, 1]) replaces the
+ * built-in ramp.  Needs instrument ICB_INSTRUMENT_TIMS; f == NULL clears
+ * (zero axial field). */
+enum { ICB_TIMS_RAMP_LINEAR = 0, ICB_TIMS_RAMP_EXPONENTIAL = 1 };
+typedef struct icb_tims_field {
+    int32_t ramp_mode;         /* ICB_TIMS_RAMP_* */
+    int32_t n_nodes;           /* 0 = uniform fields */
+    int32_t has_final_profile; /* final_profile_V_m given */
+    int32_t reserved_;
+    double initial_uniform_V_m;
+    double final_uniform_V_m;
+    double ramp_start_s;
+    double ramp_end_s;
+    double ramp_tau_s;
+    double z_positions_m[ICB_MAX_WAVE_POINTS];
+    double initial_profile_V_m[ICB_MAX_WAVE_POINTS];
+    double final_profile_V_m[ICB_MAX_WAVE_POINTS];
+} icb_tims_field;
+int icb_set_tims_field(struct icb_handle* h, int32_t ensemble, const icb_tims_field* f);
 
 /* ---- launch-shape tuning ----------------------------------------------- */
 typedef struct icb_tuning {

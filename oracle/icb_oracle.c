@@ -207,16 +207,167 @@ void orc_unit_uniforms(uint64_t seed, uint32_t ion_id, uint32_t step, uint32_t s
 }
 
 /* ======================================================================
+ * Time-dependent voltages and the TIMS axial field
+ * ==================================================================== */
+/* Same layouts as icb_waveform / icb_tims_field of the C ABI (own copies). */
+#define ORC_MAX_WAVE 64
+typedef struct {
+    int32_t type, clamp, interp, n_points;
+    double p[8];
+    double times_s[ORC_MAX_WAVE];
+    double values[ORC_MAX_WAVE];
+} orc_wave;
+typedef struct {
+    int32_t ramp_mode, n_nodes, has_final_profile, reserved_;
+    double ei, ef, t0, t1, tau;
+    double z[ORC_MAX_WAVE], pi[ORC_MAX_WAVE], pf[ORC_MAX_WAVE];
+} orc_tims;
+
+/* channels: 0 DC.axial_V, 1 DC.quad_V, 2 RF.voltage_V, 3 RF.frequency_Hz,
+ * 4 TIMS.ramp_fraction */
+static orc_wave g_wave[5];
+static int g_wave_set[5];
+static orc_tims g_tims;
+static int g_tims_set;
+
+void orc_set_time_field(const orc_tims* tims, const orc_wave* waves, const int32_t* set) {
+    g_tims_set = tims != NULL;
+    if (tims) g_tims = *tims;
+    for (int c = 0; c < 5; ++c) {
+        g_wave_set[c] = (waves && set && set[c]) ? 1 : 0;
+        if (g_wave_set[c]) g_wave[c] = waves[c];
+    }
+}
+
+/* Waveform value at t: WaveformConfig.h:33-188 (constant, linear,
+ * quadratic, exponential, sinusoidal, PWM, pulsed) and
+ * ArbitraryWaveform::evaluate, WaveformConfig.cpp:10-91. */
+static double wave_eval(const orc_wave* w, double t) {
+    const double* p = w->p;
+    switch (w->type) {
+    case 0: return p[0];
+    case 1:
+        if (t < p[2]) return p[0];
+        if (t >= p[3]) return w->clamp ? p[1] : p[0];
+        return p[0] + (p[1] - p[0]) * ((t - p[2]) / (p[3] - p[2]));
+    case 2:
+        if (t < p[3] || t > p[4]) return p[0];
+        return p[0] + p[1] * t + p[2] * t * t;
+    case 3: {
+        double rel;
+        if (t < p[3]) rel = 0.0;
+        else if (t >= p[4]) rel = w->clamp ? (p[4] - p[3]) : 0.0;
+        else rel = t - p[3];
+        return p[0] + p[1] * exp(p[2] * rel);
+    }
+    case 4: return p[0] + p[1] * sin(2.0 * M_PI * p[2] * t + p[3]);
+    case 5: {
+        double tr, period, phase;
+        if (p[2] <= 0.0 || t < p[5]) return p[0];
+        if (t >= p[6]) {
+            if (!w->clamp) return p[0];
+            tr = p[6] - p[5];
+        } else {
+            tr = t - p[5];
+        }
+        period = 1.0 / p[2];
+        phase = fmod(tr + p[4] / (2.0 * M_PI * p[2]), period);
+        if (phase < 0.0) phase += period;
+        return phase < p[3] * period ? p[1] : p[0];
+    }
+    case 6: return (t >= p[2] && t < p[2] + p[3]) ? p[1] : p[0];
+    default: {
+        const int n = w->n_points;
+        const double* T = w->times_s;
+        const double* V = w->values;
+        int i1 = 0;
+        if (!(t > T[0])) return V[0];
+        if (t >= T[n - 1]) return V[n - 1];
+        while (T[i1] < t) ++i1;             /* first T[i] >= t */
+        {
+            const int i0 = i1 - 1;
+            const double t0 = T[i0], t1 = T[i1], v0 = V[i0], v1 = V[i1];
+            double a, m0, m1, h00, h10, h01, h11, dt;
+            if (w->interp == 1) return v0;
+            a = (t - t0) / (t1 - t0);
+            if (w->interp == 0) return v0 + a * (v1 - v0);
+            m0 = i0 == 0 ? (v1 - v0) / (t1 - t0) : (v1 - V[i0 - 1]) / (t1 - T[i0 - 1]);
+            m1 = i1 == n - 1 ? (v1 - v0) / (t1 - t0) : (V[i1 + 1] - v0) / (T[i1 + 1] - t0);
+            h00 = 2 * a * a * a - 3 * a * a + 1;
+            h10 = a * a * a - 2 * a * a + a;
+            h01 = -2 * a * a * a + 3 * a * a;
+            h11 = a * a * a - a * a;
+            dt = t1 - t0;
+            return h00 * v0 + h10 * dt * m0 + h01 * v1 + h11 * dt * m1;
+        }
+    }
+    }
+}
+
+double orc_wave_value(const orc_wave* w, double t) { return wave_eval(w, t); }
+
+/* Value of a field channel at t: its waveform, else the constant. */
+static double chan(const orc_domain* d, int c, double t) {
+    if (g_wave_set[c]) return wave_eval(&g_wave[c], t);
+    switch (c) {
+    case 0: return d->axial_V;
+    case 1: return d->dc_quad_V;
+    case 2: return d->rf_voltage_V;
+    case 3: return d->rf_frequency_Hz;
+    default: return 0.0;
+    }
+}
+
+static double clamp01(double v) { return v < 0.0 ? 0.0 : (1.0 < v ? 1.0 : v); }
+
+/* TIMS ramp fraction (TIMSAxialFieldModel.h:66-96). */
+static double tims_ramp(double t) {
+    const orc_tims* T = &g_tims;
+    double t0, t1, duration, rel;
+    if (g_wave_set[4]) return clamp01(wave_eval(&g_wave[4], t));
+    t0 = g_tims_set ? T->t0 : 0.0;
+    t1 = g_tims_set ? T->t1 : 0.0;
+    if (t <= t0) return 0.0;
+    if (t >= t1) return 1.0;
+    duration = t1 - t0;
+    if (duration <= 0.0) return 1.0;
+    rel = t - t0;
+    if (T->ramp_mode == 1) {
+        const double tau = T->tau < 1e-30 ? 1e-30 : T->tau;
+        const double denom = 1.0 - exp(-duration / tau);
+        if (fabs(denom) < 1e-15) return clamp01(rel / duration);
+        return clamp01((1.0 - exp(-rel / tau)) / denom);
+    }
+    return clamp01(rel / duration);
+}
+
+/* Axial profile at local z (TIMSAxialFieldModel.h:98-124). */
+static double tims_sample(const double* zn, const double* v, int n, double z, double uni) {
+    int i1 = 0;
+    if (n == 0) return uni;
+    if (!(z > zn[0])) return v[0];
+    if (z >= zn[n - 1]) return v[n - 1];
+    while (zn[i1] < z) ++i1;
+    {
+        const int i0 = i1 - 1;
+        const double dz = zn[i1] - zn[i0];
+        if (dz <= 0.0) return v[i0];
+        return v[i0] + ((z - zn[i0]) / dz) * (v[i1] - v[i0]);
+    }
+}
+
+/* ======================================================================
  * Fields and geometry
  * ==================================================================== */
 static void field_E(const orc_domain* d, const double p[3], double t, double E[3]) {
     E[0] = E[1] = E[2] = 0.0;
     if (d->instrument == 0) {               /* IMS: AnalyticalFieldModel.cpp:136-161 */
-        E[2] = d->axial_V / d->length_m;
-        if (fabs(d->rf_voltage_V) > ORC_MIN_VOLTAGE) {
+        const double rfv = chan(d, 2, t);
+        E[2] = chan(d, 0, t) / d->length_m;
+        if (fabs(rfv) > ORC_MIN_VOLTAGE) {
             double r0_sq = d->radius_m * d->radius_m;
-            double omega = 2.0 * M_PI * d->rf_frequency_Hz;
-            double U = d->dc_quad_V + d->rf_voltage_V * cos(omega * t);
+            double omega = 2.0 * M_PI * chan(d, 3, t);
+            double U = chan(d, 1, t) + rfv * cos(omega * t);
             E[0] = -2.0 * p[0] * U / r0_sq;
             E[1] = 2.0 * p[1] * U / r0_sq;
         }
@@ -229,20 +380,37 @@ static void field_E(const orc_domain* d, const double p[3], double t, double E[3
         E[1] = factor * p[1];
         E[2] = -2.0 * factor * zc;
     } else if (d->instrument == 2) {        /* QuadrupoleRF: AnalyticalFieldModel.cpp:219-248 */
-        if (fabs(d->rf_voltage_V) > ORC_MIN_VOLTAGE) {
+        const double rfv = chan(d, 2, t), axial = chan(d, 0, t);
+        if (fabs(rfv) > ORC_MIN_VOLTAGE) {
             double r0_sq = d->radius_m * d->radius_m;
-            double omega = 2.0 * M_PI * d->rf_frequency_Hz;
-            double U = d->dc_quad_V + d->rf_voltage_V * cos(omega * t);
+            double omega = 2.0 * M_PI * chan(d, 3, t);
+            double U = chan(d, 1, t) + rfv * cos(omega * t);
             E[0] = -2.0 * p[0] * U / r0_sq;
             E[1] = 2.0 * p[1] * U / r0_sq;
         }
-        if (fabs(d->axial_V) > ORC_MIN_VOLTAGE) E[2] = d->axial_V / d->length_m;
+        if (fabs(axial) > ORC_MIN_VOLTAGE) E[2] = axial / d->length_m;
+    } else if (d->instrument == 4) {        /* TIMS: TIMSAxialFieldModel.h:30-44, 126-148, unrotated */
+        const double q[3] = {p[0] - d->origin_m[0], p[1] - d->origin_m[1], p[2] - d->origin_m[2]};
+        const orc_tims* T = &g_tims;
+        const int n = g_tims_set ? T->n_nodes : 0;
+        const double f = tims_ramp(t);
+        const double ei = tims_sample(T->z, T->pi, n, q[2], g_tims_set ? T->ei : 0.0);
+        const double ef = tims_sample(T->z, T->pf, T->has_final_profile ? n : 0, q[2], g_tims_set ? T->ef : 0.0);
+        const double r0_sq = d->radius_m * d->radius_m;
+        E[2] = (1.0 - f) * ei + f * ef;
+        if (r0_sq > 0.0) {
+            const double omega = 2.0 * M_PI * chan(d, 3, t);
+            const double u = chan(d, 1, t) + chan(d, 2, t) * cos(omega * t);
+            E[0] = -2.0 * q[0] * u / r0_sq;
+            E[1] = 2.0 * q[1] * u / r0_sq;
+        }
     } else if (d->instrument == 3) {        /* LQIT: AnalyticalFieldModel.cpp:81-134, unrotated */
         const double q[3] = {p[0] - d->origin_m[0], p[1] - d->origin_m[1], p[2] - d->origin_m[2]};
-        if (fabs(d->rf_voltage_V) > ORC_MIN_VOLTAGE) {
+        const double rfv = chan(d, 2, t), axial = chan(d, 0, t);
+        if (fabs(rfv) > ORC_MIN_VOLTAGE) {
             double r0_sq = d->radius_m * d->radius_m;
-            double omega = 2.0 * M_PI * d->rf_frequency_Hz;
-            double U = d->dc_quad_V + d->rf_voltage_V * cos(omega * t);
+            double omega = 2.0 * M_PI * chan(d, 3, t);
+            double U = chan(d, 1, t) + rfv * cos(omega * t);
             E[0] = -2.0 * q[0] * U / r0_sq;
             E[1] = 2.0 * q[1] * U / r0_sq;
         }
@@ -260,9 +428,9 @@ static void field_E(const orc_domain* d, const double p[3], double t, double E[3
             const double omega_ac = 2.0 * M_PI * d->ac_frequency_Hz[0];
             E[0] += -d->ac_amplitude_V[0] / d->radius_m * cos(omega_ac * t + d->ac_phase_rad[0]);
         }
-        if (fabs(d->axial_V) > ORC_MIN_VOLTAGE) {
+        if (fabs(axial) > ORC_MIN_VOLTAGE) {
             const double L = d->length_m;
-            const double alpha = d->axial_V / (L * L);
+            const double alpha = axial / (L * L);
             E[2] = -2.0 * alpha * (q[2] - 0.5 * L);
         }
     }
@@ -806,11 +974,83 @@ static double langevin_lambda(const orc_domain* d, double q, double m) {
     return c * fabs(q) / sqrt(mu);
 }
 
+/* Largest |value| of a waveform over all t (same expression as the
+ * product's bound). */
+static double wave_bound(const orc_wave* w) {
+    const double* p = w->p;
+    switch (w->type) {
+    case 0: return fabs(p[0]);
+    case 1: return fmax(fabs(p[0]), fabs(p[1]));
+    case 2: {
+        const double q3 = fabs(p[0] + p[1] * p[3] + p[2] * p[3] * p[3]);
+        const double q4 = fabs(p[0] + p[1] * p[4] + p[2] * p[4] * p[4]);
+        double b = fmax(fabs(p[0]), fmax(q3, q4));
+        if (p[2] != 0.0) {
+            const double tv = -p[1] / (2.0 * p[2]);
+            if (tv > p[3] && tv < p[4]) b = fmax(b, fabs(p[0] + p[1] * tv + p[2] * tv * tv));
+        }
+        return b;
+    }
+    case 3: return fmax(fabs(p[0] + p[1]), fabs(p[0] + p[1] * exp(p[2] * (p[4] - p[3]))));
+    case 4: return fabs(p[0]) + fabs(p[1]);
+    case 5: case 6: return fmax(fabs(p[0]), fabs(p[1]));
+    default: {
+        double m = 0.0;
+        for (int i = 0; i < w->n_points; ++i) m = fmax(m, fabs(w->values[i]));
+        return w->interp == 2 ? 2.0 * m : m;
+    }
+    }
+}
+
+/* Field bound of a domain on the time-dependent path (instrument TIMS or a
+ * waveform on any channel; same expression as the product's tf_bound). */
+static double tf_field_bound(const orc_domain* d) {
+    const double Rp = d->radius_m + ORC_GEOM_EPS;
+    const double L = d->length_m;
+    const double cst[4] = {d->axial_V, d->dc_quad_V, d->rf_voltage_V, d->rf_frequency_Hz};
+    double wb[4], ez, raxis = Rp, e;
+    for (int c = 0; c < 4; ++c) wb[c] = g_wave_set[c] ? wave_bound(&g_wave[c]) : fabs(cst[c]);
+    if (d->instrument == 4) {
+        const orc_tims* T = &g_tims;
+        const int n = g_tims_set ? T->n_nodes : 0;
+        double m = g_tims_set ? fmax(fabs(T->ei), fabs(T->ef)) : fmax(0.0, 0.0);
+        for (int i = 0; i < n; ++i) {
+            m = fmax(m, fabs(T->pi[i]));
+            if (T->has_final_profile) m = fmax(m, fabs(T->pf[i]));
+        }
+        ez = m;
+    } else if (d->instrument == 3) {
+        ez = 2.0 * (wb[0] / (L * L)) * (0.5 * L + ORC_GEOM_EPS);
+    } else {
+        ez = wb[0] / L;
+        raxis = sqrt(d->origin_m[0] * d->origin_m[0] + d->origin_m[1] * d->origin_m[1]) + Rp;
+    }
+    e = ez + 2.0 * (wb[1] + wb[2]) * raxis / (d->radius_m * d->radius_m);
+    if (d->instrument == 3) {
+        double ac = 0.0;
+        for (int a = 0; a < (d->ac_dipolar ? 2 : 1); ++a) {
+            const double A = d->ac_amplitude_V[a] * (d->ac_dipolar ? d->ac_ramp[a] : 1.0);
+            if (fabs(A) > ORC_MIN_VOLTAGE) ac += fabs(-A / d->radius_m);
+        }
+        if (ac > 0.0) e = e + ac;
+    }
+    return e;
+}
+
+static int time_field_on(const orc_domain* d) {
+    int c;
+    if (d->instrument == 4) return 1;
+    for (c = 0; c < 5; ++c)
+        if (g_wave_set[c]) return 1;
+    return 0;
+}
+
 /* Upper bound of |E| over the cylinder (same expression as the product's
  * field_bound): |E0| + |G .* max|x - c|| + 2 (|U0| + |V|) r_axis / r0^2. */
 double orc_field_bound(const orc_domain* d) {
     double E0[3] = {0.0, 0.0, 0.0}, Gv[3] = {0.0, 0.0, 0.0}, c[3] = {0.0, 0.0, 0.0};
     int rf = fabs(d->rf_voltage_V) > ORC_MIN_VOLTAGE;
+    if (time_field_on(d)) return tf_field_bound(d);
     if (d->instrument == 0) {
         E0[2] = d->axial_V / d->length_m;
     } else if (d->instrument == 2) {

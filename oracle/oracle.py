@@ -47,6 +47,98 @@ class Domain(C.Structure):
     ]
 
 
+class OWave(C.Structure):
+    """orc_wave (same layout as icb_waveform)."""
+    _fields_ = [("type", C.c_int32), ("clamp", C.c_int32), ("interp", C.c_int32), ("n_points", C.c_int32),
+                ("p", C.c_double * 8), ("times_s", C.c_double * 64), ("values", C.c_double * 64)]
+
+
+class OTims(C.Structure):
+    """orc_tims (same layout as icb_tims_field)."""
+    _fields_ = [("ramp_mode", C.c_int32), ("n_nodes", C.c_int32), ("has_final_profile", C.c_int32),
+                ("reserved_", C.c_int32), ("ei", C.c_double), ("ef", C.c_double), ("t0", C.c_double),
+                ("t1", C.c_double), ("tau", C.c_double), ("z", C.c_double * 64), ("pi", C.c_double * 64),
+                ("pf", C.c_double * 64)]
+
+
+WAVE_KEYS = ("wave_axial", "wave_quad", "wave_rfv", "wave_rff", "wave_ramp")
+
+
+def parse_wave(spec: str) -> dict:
+    """Harness waveform spec "type|clamp|interp|p0,..|t0,..|v0,.." -> fields."""
+    f = (str(spec).split("|") + [""] * 6)[:6]
+    num = lambda x: [float(v) for v in x.split(",") if v != ""]
+    p = (num(f[3]) + [0.0] * 8)[:8]
+    return {"type": int(f[0]), "clamp": int(f[1] or 0), "interp": int(f[2] or 0), "p": p,
+            "times": num(f[4]), "values": num(f[5])}
+
+
+def wave_struct(spec: str, cls=OWave):
+    d = parse_wave(spec)
+    w = cls()
+    w.type, w.clamp, w.interp = d["type"], d["clamp"], d["interp"]
+    w.n_points = len(d["times"]) if d["type"] == 7 else 0
+    w.p[:] = d["p"]
+    w.times_s[:len(d["times"])] = d["times"]
+    w.values[:len(d["values"])] = d["values"]
+    return w
+
+
+def tims_struct(kw: dict, cls=OTims, names=("ei", "ef", "t0", "t1", "tau", "z", "pi", "pf")):
+    """Harness TIMS keys -> orc_tims (or the ABI struct with its field names)."""
+    if not kw.get("tims"):
+        return None
+    num = lambda x: [float(v) for v in str(x).split(",") if v != ""]
+    t = cls()
+    t.ramp_mode = int(kw.get("tims_mode", 0))
+    z, pi, pf = num(kw.get("tims_z", "")), num(kw.get("tims_pi", "")), num(kw.get("tims_pf", ""))
+    t.n_nodes = len(z)
+    t.has_final_profile = int(len(pf) == len(z) and len(z) > 0)
+    ei, ef, t0, t1, tau, zf, pif, pff = names
+    setattr(t, ei, float(kw.get("tims_ei", 0.0)))
+    setattr(t, ef, float(kw.get("tims_ef", 0.0)))
+    setattr(t, t0, float(kw.get("tims_t0", 0.0)))
+    setattr(t, t1, float(kw.get("tims_t1", 0.0)))
+    setattr(t, tau, float(kw.get("tims_tau", 1e-3)))
+    getattr(t, zf)[:len(z)] = z
+    getattr(t, pif)[:len(pi)] = pi
+    getattr(t, pff)[:len(pf)] = pf
+    return t
+
+
+def wave_value(spec: str, t: float) -> float:
+    """The restated waveform evaluation at one time."""
+    w = wave_struct(spec)
+    return lib().orc_wave_value(C.byref(w), float(t))
+
+
+def set_time_field(kw: dict | None) -> None:
+    """Waveforms and TIMS field of the harness domain keys (None clears)."""
+    kw = kw or {}
+    waves = (OWave * 5)()
+    on = (C.c_int32 * 5)()
+    for c, key in enumerate(WAVE_KEYS):
+        if key in kw:
+            waves[c] = wave_struct(kw[key])
+            on[c] = 1
+    t = tims_struct(kw)
+    lib().orc_set_time_field(C.byref(t) if t is not None else None, waves, on)
+
+
+def field(domain: dict, pts: np.ndarray, time_field: dict | None = None) -> np.ndarray:
+    """E of the restated field model at rows (x, y, z, t)."""
+    d = domain_struct(domain)
+    set_time_field(time_field)
+    pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 4)
+    out = np.zeros((pts.shape[0], 3))
+    for i in range(pts.shape[0]):
+        p = np.ascontiguousarray(pts[i, :3])
+        e = np.zeros(3)
+        lib().orc_field(C.byref(d), _dp(p), float(pts[i, 3]), _dp(e))
+        out[i] = e
+    return out
+
+
 def domain_struct(p: dict) -> Domain:
     d = Domain()
     for k, _ in Domain._fields_:
@@ -94,6 +186,9 @@ def lib() -> C.CDLL:
         L.orc_run.restype = C.c_int
         L.orc_set_ehss.argtypes = [DP, C.c_int, C.c_double]
         L.orc_set_subcycles.argtypes = [C.c_int]
+        L.orc_set_time_field.argtypes = [C.POINTER(OTims), C.POINTER(OWave), C.POINTER(C.c_int32)]
+        L.orc_wave_value.argtypes = [C.POINTER(OWave), C.c_double]
+        L.orc_wave_value.restype = C.c_double
         L.orc_ehss_scatter_many.argtypes = [C.c_int64, DP, DP, C.c_double, C.c_double, C.c_uint64, DP]
         L.orc_set_ipm_table.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_double, C.c_double]
         L.orc_ipm_cos_chi_trajectory.argtypes = [C.c_double] * 7
@@ -181,7 +276,8 @@ def philox(ctr: np.ndarray, seed: int) -> np.ndarray:
 
 def run(domain: dict, state: dict, n_steps: int, *, integrator: int = 0, collision: int = 0, seed: int = 123,
         first_id: int = 0, step0: int = 0, t0: float = 0.0, snap_every: int = 0, ref_step: int = 0,
-        clock: tuple | None = None, threads: int = 1, subcycles: int = 1) -> dict:
+        clock: tuple | None = None, threads: int = 1, subcycles: int = 1,
+        time_field: dict | None = None) -> dict:
     """Run the restatement.  ``state`` holds float64 arrays x..vz, mass, charge,
     uint8 active and optional t_death / t_arrival; it is updated in place.
     collision: 0 none, 1 reference HSS (mt19937_64 per ion), 2 null-collision
@@ -192,9 +288,11 @@ def run(domain: dict, state: dict, n_steps: int, *, integrator: int = 0, collisi
     set_ipm_table), 5 HSS gas mixture (Boris, skip clock), 6 the reference's
     per-step HSS form with Philox words (no clock; ``subcycles`` collision
     sub-steps of dt/m per step), 7 EHSS on the geometry of set_ehss (Boris,
-    skip clock)."""
+    skip clock).  ``time_field`` holds the harness's waveform / TIMS keys
+    (wave_*, tims*) of the domain; the default clears them."""
     d = domain_struct(domain)
     lib().orc_set_subcycles(int(subcycles))
+    set_time_field(time_field)
     n = state["x"].shape[0]
     for k in ("t_death", "t_arrival"):
         if state.get(k) is None:
@@ -263,6 +361,17 @@ def harness(mode: str, **kw) -> str:
     if r.returncode != 0:
         raise RuntimeError(f"ref_harness {mode} failed: {r.stderr}")
     return r.stdout
+
+
+def harness_field(domain_kw: dict, pts: np.ndarray) -> np.ndarray:
+    """E of the reference's own field model (the one PhysicsSetup builds for
+    the domain) at rows (x, y, z, t)."""
+    pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 4)
+    with tempfile.TemporaryDirectory() as td:
+        ip, op = Path(td) / "pts.bin", Path(td) / "E.bin"
+        ip.write_bytes(pts.tobytes())
+        harness("field", **{"in": ip, "out": op}, **domain_kw)
+        return np.fromfile(op, dtype=np.float64).reshape(-1, 3)
 
 
 def harness_run(state: dict, n_steps: int, domain_kw: dict, **kw) -> tuple[dict, dict, np.ndarray | None]:

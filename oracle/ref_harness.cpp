@@ -22,6 +22,14 @@
 //            ion cloud as IonLoader::sample_position/sample_velocity
 //            (gaussian at the origin, thermal), std::mt19937(seed)
 //   derive   <domain keys>             print the loader-derived constants
+//   field    <domain keys> in= out=    E of the domain's field model at the
+//            (x, y, z, t) rows of in (4 doubles each) into out (3 each)
+//
+// Time-dependent domain keys: wave_<axial|quad|rfv|rff|ramp>=
+// "type|clamp|interp|p0,p1,..|t0,t1,..|v0,v1,.." (type 0..7 in the order of
+// WaveformType), attached inline as the loader does, or through the
+// waveform library (waveform_ref) with wave_ref=1; TIMS: tims=1 tims_mode=
+// tims_ei= tims_ef= tims_t0= tims_t1= tims_tau= tims_z= tims_pi= tims_pf=.
 //   run      in= out= <domain keys> integrator= collision= steps= snap=
 //            ref_step= threads= seed= schedule=static|faithful mom=
 //            moments (20 per snapshot, layout of ICB_N_MOMENTS) of the
@@ -33,6 +41,8 @@
 #include "core/physics/forces/ElectricFieldForce.h"
 #include "core/physics/forces/MagneticFieldForce.h"
 #include "core/config/types/AnalyticalFieldModel.h"
+#include "core/config/types/TIMSAxialFieldModel.h"
+#include "core/config/types/WaveformConfig.h"
 #include "core/config/types/CylindricalGeometry.h"
 #include "core/types/IonEnsemble.h"
 #include "core/physics/spacecharge/SpaceChargeDirectModel.h"
@@ -98,6 +108,63 @@ void write_state(const std::string& path, const State& s) {
     std::fclose(f);
 }
 
+std::vector<double> list(const std::string& v) {
+    std::vector<double> out;
+    size_t pos = 0;
+    while (pos < v.size()) {
+        size_t end = v.find(',', pos);
+        if (end == std::string::npos) end = v.size();
+        if (end > pos) out.push_back(std::strtod(v.substr(pos, end - pos).c_str(), nullptr));
+        pos = end + 1;
+    }
+    return out;
+}
+
+// "type|clamp|interp|params|times|values" -> the reference's Waveform variant
+config::Waveform parse_wave(const std::string& spec) {
+    std::vector<std::string> f;
+    size_t pos = 0;
+    while (true) {
+        size_t end = spec.find('|', pos);
+        f.push_back(spec.substr(pos, end == std::string::npos ? std::string::npos : end - pos));
+        if (end == std::string::npos) break;
+        pos = end + 1;
+    }
+    while (f.size() < 6) f.push_back("");
+    const int type = std::atoi(f[0].c_str());
+    const bool clamp = std::atoi(f[1].c_str()) != 0;
+    const int interp = std::atoi(f[2].c_str());
+    std::vector<double> p = list(f[3]);
+    p.resize(8, 0.0);
+    config::Waveform w;
+    switch (type) {
+        case 0: { config::ConstantWaveform c; c.value = p[0]; w.data = c; break; }
+        case 1: { config::LinearWaveform c; c.start_value = p[0]; c.end_value = p[1]; c.start_time_s = p[2];
+                  c.end_time_s = p[3]; c.clamp = clamp; w.data = c; break; }
+        case 2: { config::QuadraticWaveform c; c.a = p[0]; c.b = p[1]; c.c = p[2]; c.start_time_s = p[3];
+                  c.end_time_s = p[4]; w.data = c; break; }
+        case 3: { config::ExponentialWaveform c; c.offset = p[0]; c.amplitude = p[1]; c.rate_per_s = p[2];
+                  c.start_time_s = p[3]; c.end_time_s = p[4]; c.clamp = clamp; w.data = c; break; }
+        case 4: { config::SinusoidalWaveform c; c.offset = p[0]; c.amplitude = p[1]; c.frequency_Hz = p[2];
+                  c.phase_rad = p[3]; w.data = c; break; }
+        case 5: { config::PWMWaveform c; c.low_value = p[0]; c.high_value = p[1]; c.frequency_Hz = p[2];
+                  c.duty_cycle = p[3]; c.phase_rad = p[4]; c.start_time_s = p[5]; c.end_time_s = p[6];
+                  c.clamp = clamp; w.data = c; break; }
+        case 6: { config::PulsedWaveform c; c.low_value = p[0]; c.high_value = p[1]; c.pulse_start_s = p[2];
+                  c.pulse_width_s = p[3]; w.data = c; break; }
+        default: {
+            config::ArbitraryWaveform c;
+            c.times_s = list(f[4]);
+            c.values = list(f[5]);
+            c.interp = interp == 1 ? config::ArbitraryWaveform::Interpolation::Step
+                     : interp == 2 ? config::ArbitraryWaveform::Interpolation::Cubic
+                                   : config::ArbitraryWaveform::Interpolation::Linear;
+            w.data = c;
+        }
+    }
+    return w;
+}
+
 // Domain exactly as the loader builds it: E/N -> axial_V via N = P/(kB T)
 // (DomainConfigLoader.cpp:417-431), density and gas mass from
 // EnvironmentConfig::compute_derived_properties.
@@ -108,6 +175,7 @@ config::DomainConfig make_domain(const Args& a) {
     else if (inst == "FTICR") d.instrument = config::Instrument::FTICR;
     else if (inst == "QuadrupoleRF") d.instrument = config::Instrument::QuadrupoleRF;
     else if (inst == "LQIT") d.instrument = config::Instrument::LQIT;
+    else if (inst == "TIMS") d.instrument = config::Instrument::TIMS;
     else throw std::runtime_error("unsupported instrument " + inst);
     d.geometry.origin_m = Vec3{num(a, "origin_x", 0.0), num(a, "origin_y", 0.0), num(a, "origin_z", 0.0)};
     d.geometry.length_m = num(a, "length", 0.1);
@@ -166,7 +234,67 @@ config::DomainConfig make_domain(const Args& a) {
         ax.ramp.constant_value = num(a, (pre + "ramp").c_str(), 1.0);
     }
     d.fields.ac.compute_derived();
+    // waveforms: inline (the loader resolves "@id" into an inline copy,
+    // WaveformLoader.cpp:290-320) or through the library (wave_ref=1)
+    const bool by_ref = num(a, "wave_ref", 0.0) != 0.0;
+    const std::pair<const char*, config::ValueOrWaveform*> chans[] = {
+        {"wave_axial", &d.fields.dc.axial_V}, {"wave_quad", &d.fields.dc.quad_V},
+        {"wave_rfv", &d.fields.rf.voltage_V}, {"wave_rff", &d.fields.rf.frequency_Hz},
+        {"wave_ramp", &d.fields.tims.ramp_fraction}};
+    for (const auto& [key, slot] : chans) {
+        if (!a.count(key)) continue;
+        config::Waveform w = parse_wave(str(a, key, ""));
+        *slot = config::ValueOrWaveform{};
+        if (by_ref) {
+            w.id = key;
+            d.fields.waveform_library[key] = w;
+            slot->waveform_ref = key;
+        } else {
+            slot->waveform = w;
+        }
+        if (std::string(key) == "wave_ramp") d.fields.tims.ramp_fraction_defined = true;
+    }
+    if (num(a, "tims", 0.0) != 0.0) {
+        auto& t = d.fields.tims;
+        t.enabled = true;
+        t.axial_field_initial_uniform_V_m = num(a, "tims_ei", 0.0);
+        t.axial_field_final_uniform_V_m = num(a, "tims_ef", 0.0);
+        t.ramp_start_s = num(a, "tims_t0", 0.0);
+        t.ramp_end_s = num(a, "tims_t1", 0.0);
+        t.ramp_mode = num(a, "tims_mode", 0.0) != 0.0 ? "exponential" : "linear";
+        t.ramp_tau_s = num(a, "tims_tau", 1e-3);
+        t.z_positions_m = list(str(a, "tims_z", ""));
+        t.axial_field_initial_profile_V_m = list(str(a, "tims_pi", ""));
+        t.axial_field_final_profile_V_m = list(str(a, "tims_pf", ""));
+    }
     return d;
+}
+
+// The field model PhysicsSetup builds for the domain (PhysicsSetup.cpp:190-196).
+std::unique_ptr<config::IFieldModel> make_field_model(const config::DomainConfig& d) {
+    if (d.instrument == config::Instrument::TIMS || d.fields.tims.enabled)
+        return std::make_unique<config::TIMSAxialFieldModel>(d);
+    return std::make_unique<config::AnalyticalFieldModel>(d);
+}
+
+int mode_field(const Args& a) {
+    config::DomainConfig d = make_domain(a);
+    auto model = make_field_model(d);
+    FILE* f = std::fopen(str(a, "in", "pts.bin").c_str(), "rb");
+    if (!f) throw std::runtime_error("cannot open points");
+    std::vector<double> pts;
+    double buf[4];
+    while (std::fread(buf, sizeof(double), 4, f) == 4) pts.insert(pts.end(), buf, buf + 4);
+    std::fclose(f);
+    std::vector<double> out;
+    for (size_t i = 0; i + 3 < pts.size(); i += 4) {
+        const Vec3 E = model->E(Vec3{pts[i], pts[i + 1], pts[i + 2]}, pts[i + 3]);
+        out.push_back(E.x); out.push_back(E.y); out.push_back(E.z);
+    }
+    FILE* g = std::fopen(str(a, "out", "E.bin").c_str(), "wb");
+    std::fwrite(out.data(), sizeof(double), out.size(), g);
+    std::fclose(g);
+    return 0;
 }
 
 int mode_uniforms(const Args& a) {
@@ -332,12 +460,12 @@ int mode_run(const Args& a) {
     }
     core::IonEnsemble ens = core::IonEnsemble::from_legacy(ions);
 
-    config::AnalyticalFieldModel field_model(d);
+    auto field_model = make_field_model(d);
     auto reg = std::make_shared<physics::ForceRegistry>(d);
     reg->add_force(std::make_unique<physics::ElectricFieldForce>(d));
     if (d.fields.magnetic.enabled && integ != "boris")
         reg->add_force(std::make_unique<physics::MagneticFieldForce>(d.fields.magnetic));
-    reg->set_field_model(&field_model);
+    reg->set_field_model(field_model.get());
     std::vector<std::shared_ptr<physics::ForceRegistry>> regs{reg};
     config::CylindricalGeometry geom(d);
 
@@ -511,6 +639,7 @@ int main(int argc, char** argv) {
         if (mode == "uniforms") return mode_uniforms(a);
         if (mode == "init") return mode_init(a);
         if (mode == "derive") return mode_derive(a);
+        if (mode == "field") return mode_field(a);
         if (mode == "run") return mode_run(a);
         if (mode == "direct") return mode_direct(a);
         if (mode == "ehss") return mode_ehss(a);

@@ -51,6 +51,88 @@ LQIT1_DOMAIN = dict(instrument="LQIT", origin_z=-0.025, length=0.05, radius=0.00
                     rf_V=200.0, rf_f=1.0e6, axial_V=2.0, ac_V=0.4, ac_f=9.0e4, ac_phase=1.1)
 
 
+# Time-dependent fields.  Waveform specs are "type|clamp|interp|params|times|values"
+# with the types in WaveformType order (constant, linear, quadratic,
+# exponential, sinusoidal, pwm, pulsed, arbitrary).
+# TIMS (TIMSAxialFieldModel): profile ramp over 1..4 us, RF confinement
+TIMS_DOMAIN = dict(instrument="TIMS", origin_z=-0.01, length=0.02, radius=0.005, T=300, P=310.0, gas="N2",
+                   rf_V=180.0, rf_f=2.0e6, dc_quad_V=0.0, tims=1, tims_z="0,0.02", tims_pi="0,-449.5",
+                   tims_pf="0,0", tims_t0=1e-6, tims_t1=4e-6)
+# exponential ramp between uniform fields, DC quadrupole offset
+TIMS_EXP_DOMAIN = dict(instrument="TIMS", origin_z=-0.01, length=0.02, radius=0.005, T=300, P=310.0, gas="N2",
+                       rf_V=150.0, rf_f=1.5e6, dc_quad_V=2.0, tims=1, tims_mode=1, tims_ei=-300.0, tims_ef=-100.0,
+                       tims_t0=5e-7, tims_t1=3.5e-6, tims_tau=1e-6)
+# an enabled TIMS block on an IMS domain: ramp fraction from a cubic
+# arbitrary waveform (clamped above 1), three-node initial profile, final
+# uniform field, RF frequency ramp
+TIMS_WAVE_DOMAIN = dict(instrument="IMS", origin_z=-0.01, length=0.02, radius=0.005, T=300, P=310.0, gas="N2",
+                        rf_V=180.0, rf_f=2.0e6, tims=1, tims_z="0,0.008,0.02", tims_pi="-100,-400,-250",
+                        tims_ef=-50.0, wave_ramp="7|0|2||0,1e-6,2e-6,3e-6,4e-6|0,0.1,0.5,0.9,1.2",
+                        wave_rff="1|1|0|2e6,2.2e6,0,4e-6")
+# LQIT with an axial ramp, modulated RF amplitude, chirped RF frequency and
+# a gated PWM DC quadrupole
+LQIT_WAVE_DOMAIN = dict(LQIT_DOMAIN, wave_axial="1|1|0|2,5,0,4e-6", wave_rfv="4|0|0|200,20,2e5,0.3",
+                        wave_rff="2|0|0|1e6,1e10,0,0,1e-5", wave_quad="5|0|0|0.5,1.5,5e5,0.3,0.2,1e-6,4e-6")
+# IMS / QuadrupoleRF read waveforms given as waveform_ref
+IMS_REF_DOMAIN = dict(IMS_DOMAIN, wave_ref=1, wave_axial="3|1|0|1000,500,-3e5,1e-6,6e-6",
+                      wave_rfv="6|0|0|0,50,1e-6,2e-6", wave_rff="0|0|0|1e6", wave_quad="7|0|1||0,2e-6,4e-6|0,1,-1")
+QUAD_REF_DOMAIN = dict(QUAD_DOMAIN, wave_ref=1, wave_rfv="1|1|0|200,250,0,3e-6", wave_axial="4|0|0|1,0.5,3e5,0")
+# ... and read inline waveforms (what the loader makes of "@id" and objects) as 0 V
+IMS_INLINE_DOMAIN = dict(IMS_DOMAIN, wave_axial="1|1|0|0,2000,0,2e-6")
+# every waveform type, clamp and interpolation on the RF voltage of a
+# QuadrupoleRF domain (waveform_ref)
+WAVE_TYPE_SPECS = {
+    "constant": "0|0|0|190",
+    "linear_clamp": "1|1|0|150,250,1e-6,3e-6",
+    "linear_hold_start": "1|0|0|150,250,1e-6,3e-6",
+    "quadratic": "2|0|0|100,3e7,4e12,5e-7,4e-6",
+    "exponential_clamp": "3|1|0|120,80,-6e5,1e-6,4e-6",
+    "exponential_noclamp": "3|0|0|120,80,4e5,1e-6,4e-6",
+    "sinusoidal": "4|0|0|200,30,7e5,0.4",
+    "pwm_clamp": "5|1|0|100,220,8e5,0.35,0.7,5e-7,4.1e-6",
+    "pwm_noclamp": "5|0|0|100,220,8e5,0.35,-0.5,5e-7,4.1e-6",
+    "pulsed": "6|0|0|80,240,1.5e-6,1e-6",
+    "arbitrary_linear": "7|0|0||0,1e-6,2.5e-6,4e-6|100,260,180,220",
+    "arbitrary_step": "7|0|1||0,1e-6,2.5e-6,4e-6|100,260,180,220",
+    "arbitrary_cubic": "7|0|2||0,1e-6,2.5e-6,4e-6,5e-6|100,260,180,220,150",
+}
+
+
+def field_cases() -> dict:
+    cases = {"tims": TIMS_DOMAIN, "tims_exp": TIMS_EXP_DOMAIN, "tims_wave": TIMS_WAVE_DOMAIN,
+             "lqit_wave": LQIT_WAVE_DOMAIN, "ims_ref": IMS_REF_DOMAIN, "quadrf_ref": QUAD_REF_DOMAIN,
+             "ims_inline": IMS_INLINE_DOMAIN}
+    for name, spec in WAVE_TYPE_SPECS.items():
+        cases[f"wave_{name}"] = dict(QUAD_DOMAIN, wave_ref=1, wave_rfv=spec)
+    return cases
+
+
+def field_points(kw: dict, n: int = 40, seed: int = 7) -> np.ndarray:
+    """(x, y, z, t) rows inside and just outside the cylinder, at times on a
+    grid over -1..8 us plus every boundary time the cases use."""
+    rng = np.random.default_rng(seed)
+    L, R, oz = float(kw["length"]), float(kw["radius"]), float(kw.get("origin_z", 0.0))
+    t_edges = [0.0, 5e-7, 1e-6, 1.5e-6, 2e-6, 2.5e-6, 3e-6, 3.5e-6, 4e-6, 4.1e-6, 5e-6, 6e-6]
+    t = np.concatenate([np.linspace(-1e-6, 8e-6, n), t_edges])
+    m = t.size
+    r = R * np.sqrt(rng.random(m))
+    ph = 2 * np.pi * rng.random(m)
+    z = oz + L * (1.2 * rng.random(m) - 0.1)
+    return np.stack([r * np.cos(ph), r * np.sin(ph), z, t], axis=1)
+
+
+def field_only() -> None:
+    """E of the reference's own field models on the time-dependent cases."""
+    arrays, names = {}, []
+    for name, kw in field_cases().items():
+        pts = field_points(kw)
+        arrays[f"{name}_pts"] = pts
+        arrays[f"{name}_E"] = orc.harness_field(kw, pts)
+        arrays[f"{name}_domain"] = json.dumps(kw)
+        names.append(name)
+    save("field_timed.npz", names=json.dumps(names), **arrays)
+
+
 def init_state(n: int, seed: int = 123, mass_amu: float = 200.0, sigma_pos: float = 5e-4) -> dict:
     st_path = OUT / "_tmp_init.bin"
     orc.harness("init", seed=seed, n=n, sigma_pos=sigma_pos, T=300, mass=repr(mass_amu * AMU), out=st_path)
@@ -87,7 +169,9 @@ def main(quick: bool, only: set[str] | None = None) -> None:
         raise SystemExit("oracle/_ref/ref_harness missing: run `make -C oracle` with the reference tree present")
 
     if only:
-        push_only(only)
+        if "field_timed" in only:
+            field_only()
+        push_only(only - {"field_timed"})
         return
     # 1. PhysicsRng streams
     streams = {}
@@ -109,6 +193,7 @@ def main(quick: bool, only: set[str] | None = None) -> None:
 
     # 4. collision-free pushes
     push_only(None)
+    field_only()
 
     # 5. Boris + reference HSS, bit-level fixture for the restatement
     s0 = init_state(64)
@@ -137,6 +222,14 @@ def push_cases() -> dict:
         "boris_quadrf": (QUAD_DOMAIN, "boris", lambda: init_state(64, mass_amu=100.0, sigma_pos=2e-4), 4000, 1e-9),
         "boris_lqit": (LQIT_DOMAIN, "boris", lambda: init_state(64, sigma_pos=2e-4), 8000, 1e-9),
         "rk4_lqit1": (LQIT1_DOMAIN, "rk4", lambda: init_state(64, sigma_pos=2e-4), 4000, 1e-9),
+        "boris_tims": (TIMS_DOMAIN, "boris", lambda: init_state(64, sigma_pos=2e-4), 5000, 1e-9),
+        "rk4_tims_exp": (TIMS_EXP_DOMAIN, "rk4", lambda: init_state(64, sigma_pos=2e-4), 4000, 1e-9),
+        "boris_tims_wave": (TIMS_WAVE_DOMAIN, "boris", lambda: init_state(64, sigma_pos=2e-4), 5000, 1e-9),
+        "boris_lqit_wave": (LQIT_WAVE_DOMAIN, "boris", lambda: init_state(64, sigma_pos=2e-4), 5000, 1e-9),
+        "rk4_ims_waveref": (IMS_REF_DOMAIN, "rk4", lambda: init_state(64), 5000, 1e-9),
+        "boris_quadrf_waveref": (QUAD_REF_DOMAIN, "boris", lambda: init_state(64, mass_amu=100.0, sigma_pos=2e-4),
+                                 4000, 1e-9),
+        "boris_ims_inline": (IMS_INLINE_DOMAIN, "boris", lambda: init_state(64), 3000, 5e-10),
     }
 
 

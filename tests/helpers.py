@@ -6,11 +6,75 @@ import json
 
 import numpy as np
 
+from icarion_b200 import _capi as capi
 from icarion_b200 import config as cfg
 from icarion_b200.sim import IonState
 
 AMU = cfg.AMU_TO_KG
 E_CHARGE = cfg.ELEM_CHARGE_C
+
+
+WAVE_JSON_KEYS = {
+    0: ("constant", ["value"]),
+    1: ("linear", ["start", "end", "start_time_s", "end_time_s"]),
+    2: ("quadratic", ["a", "b", "c", "start_time_s", "end_time_s"]),
+    3: ("exponential", ["offset", "amplitude", "rate_per_s", "start_time_s", "end_time_s"]),
+    4: ("sinusoidal", ["offset", "amplitude", "frequency_Hz", "phase_rad"]),
+    5: ("pwm", ["low", "high", "frequency_Hz", "duty_cycle", "phase_rad", "start_time_s", "end_time_s"]),
+    6: ("pulsed", ["low", "high", "pulse_start_s", "pulse_width_s"]),
+}
+
+
+def wave_json(spec: str) -> dict:
+    """Harness waveform spec -> the reference's waveform JSON object
+    (WaveformLoader.cpp:60-262 field names)."""
+    import oracle as orc
+    d = orc.parse_wave(spec)
+    if d["type"] == 7:
+        return {"type": "arbitrary", "times": d["times"], "values": d["values"],
+                "interpolation": ("linear", "step", "cubic")[d["interp"]]}
+    name, keys = WAVE_JSON_KEYS[d["type"]]
+    obj = {"type": name, **{k: d["p"][i] for i, k in enumerate(keys)}}
+    if d["type"] in (1, 3, 5):
+        obj["clamp"] = bool(d["clamp"])
+    return obj
+
+
+def time_field_structs(kw: dict) -> tuple[dict, object]:
+    """Waveform channels and TIMS field of the harness keys as ABI structs,
+    every channel evaluated (the reference's waveform_ref semantics)."""
+    import oracle as orc
+    chans = (capi.CHANNEL_DC_AXIAL_V, capi.CHANNEL_DC_QUAD_V, capi.CHANNEL_RF_VOLTAGE_V,
+             capi.CHANNEL_RF_FREQUENCY_HZ, capi.CHANNEL_TIMS_RAMP_FRACTION)
+    waves = {ch: orc.wave_struct(kw[key], cls=capi.Waveform) for ch, key in zip(chans, orc.WAVE_KEYS) if key in kw}
+    tims = orc.tims_struct(kw, cls=capi.TimsField,
+                           names=("initial_uniform_V_m", "final_uniform_V_m", "ramp_start_s", "ramp_end_s",
+                                  "ramp_tau_s", "z_positions_m", "initial_profile_V_m", "final_profile_V_m"))
+    return waves, tims
+
+
+def oracle_time_field(kw: dict) -> dict:
+    """The harness keys the reference's field model reads: inline waveforms
+    of IMS / QuadrupoleRF domains read as 0 V (AnalyticalFieldModel.cpp
+    :140-147, 226-233), so those channels are dropped."""
+    import oracle as orc
+    if kw.get("wave_ref") or kw.get("tims") or kw["instrument"] in ("LQIT", "TIMS"):
+        return dict(kw)
+    return {k: v for k, v in kw.items() if k not in orc.WAVE_KEYS}
+
+
+def apply_time_field(sim, kw: dict, ensemble: int = 0) -> None:
+    """Waveforms / TIMS field of the harness keys on a Simulation: through
+    the JSON adapter (config.time_fields), or as direct structs for
+    waveform_ref domains (wave_ref=1), which JSON cannot express."""
+    if kw.get("wave_ref"):
+        waves, tims = time_field_structs(kw)
+    else:
+        waves, tims = cfg.time_fields(domain_json(kw))
+    if tims is not None:
+        sim.set_tims_field(ensemble, tims)
+    for ch, w in waves.items():
+        sim.set_waveform(ensemble, ch, w)
 
 
 def domain_json(kw: dict) -> dict:
@@ -19,6 +83,11 @@ def domain_json(kw: dict) -> dict:
     for k1, k2 in (("EN_Td", "EN_Td"), ("axial_V", "axial_V"), ("radial_V", "radial_V"), ("dc_quad_V", "quad_V")):
         if k1 in kw:
             dc[k2] = kw[k1]
+    rf = {"voltage_V": kw.get("rf_V", 0.0), "frequency_Hz": kw.get("rf_f", 0.0)}
+    for key, blk, name in (("wave_axial", dc, "axial_V"), ("wave_quad", dc, "quad_V"),
+                           ("wave_rfv", rf, "voltage_V"), ("wave_rff", rf, "frequency_Hz")):
+        if key in kw:
+            blk[name] = wave_json(kw[key])
     ac = {"voltage_V": kw.get("ac_V", 0.0), "frequency_Hz": kw.get("ac_f", 0.0), "phase_rad": kw.get("ac_phase", 0.0)}
     dip = {a: {"amplitude_V": kw[f"dip_{a}_A"], "frequency_Hz": kw.get(f"dip_{a}_f", 0.0),
                "phase_rad": kw.get(f"dip_{a}_phase", 0.0), "ramp": kw.get(f"dip_{a}_ramp", 1.0)}
@@ -29,9 +98,28 @@ def domain_json(kw: dict) -> dict:
         "instrument": kw["instrument"],
         "geometry": {"origin_m": [0.0, 0.0, kw.get("origin_z", 0.0)], "length_m": kw["length"], "radius_m": kw["radius"]},
         "env": {"temperature_K": kw["T"], "pressure_Pa": kw["P"], "gas_species": kw["gas"]},
-        "fields": {"DC": dc, "RF": {"voltage_V": kw.get("rf_V", 0.0), "frequency_Hz": kw.get("rf_f", 0.0)}, "AC": ac,
-                   "magnetic": {"enabled": bool(kw.get("magnetic", 0)), "field_strength_T": [0.0, 0.0, kw.get("B_z", 0.0)]}},
+        "fields": {"DC": dc, "RF": rf, "AC": ac,
+                   "magnetic": {"enabled": bool(kw.get("magnetic", 0)), "field_strength_T": [0.0, 0.0, kw.get("B_z", 0.0)]},
+                   **({"TIMS": tims_json(kw)} if kw.get("tims") else {})},
     }
+
+
+def tims_json(kw: dict) -> dict:
+    """Harness TIMS keys -> the reference's fields.TIMS block."""
+    num = lambda x: [float(v) for v in str(x).split(",") if v != ""]
+    t = {"enabled": True, "axial_field_initial_uniform_V_m": float(kw.get("tims_ei", 0.0)),
+         "axial_field_final_uniform_V_m": float(kw.get("tims_ef", 0.0)),
+         "ramp_start_s": float(kw.get("tims_t0", 0.0)), "ramp_end_s": float(kw.get("tims_t1", 0.0)),
+         "ramp_mode": "exponential" if int(kw.get("tims_mode", 0)) else "linear",
+         "ramp_tau_s": float(kw.get("tims_tau", 1e-3))}
+    if kw.get("tims_z"):
+        t["z_positions_m"] = num(kw["tims_z"])
+        t["axial_field_initial_profile_V_m"] = num(kw["tims_pi"])
+        if kw.get("tims_pf"):
+            t["axial_field_final_profile_V_m"] = num(kw["tims_pf"])
+    if "wave_ramp" in kw:
+        t["ramp_fraction"] = wave_json(kw["wave_ramp"])
+    return t
 
 
 def ensemble_from_golden(z, sigma_m2: float = 150e-20, detector_z_m: float = 1e30) -> dict:
