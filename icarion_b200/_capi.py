@@ -33,7 +33,8 @@ MAX_WAVE_POINTS = 64
  WAVE_ARBITRARY) = range(8)
 INTERP_LINEAR, INTERP_STEP, INTERP_CUBIC = 0, 1, 2
 (CHANNEL_DC_AXIAL_V, CHANNEL_DC_QUAD_V, CHANNEL_RF_VOLTAGE_V, CHANNEL_RF_FREQUENCY_HZ,
- CHANNEL_TIMS_RAMP_FRACTION, N_CHANNELS) = range(6)
+ CHANNEL_TIMS_RAMP_FRACTION, CHANNEL_AC_X_AMPLITUDE_V, CHANNEL_AC_X_FREQUENCY_HZ, CHANNEL_AC_X_RAMP,
+ CHANNEL_AC_Y_AMPLITUDE_V, CHANNEL_AC_Y_FREQUENCY_HZ, CHANNEL_AC_Y_RAMP, N_CHANNELS) = range(12)
 TIMS_RAMP_LINEAR, TIMS_RAMP_EXPONENTIAL = 0, 1
 SC_OFF, SC_P3M_ISOLATED, SC_PM_PERIODIC_REF = 0, 1, 2
 STEPPING_EVENTS, STEPPING_PER_STEP = 0, 1

@@ -223,6 +223,16 @@ def time_fields(domain: dict, global_waveforms: dict | None = None) -> tuple[dic
         v = value_or_waveform(blk[key], lib)
         if isinstance(v, capi.Waveform):
             waves[ch] = v
+    if inst == "LQIT" and not tims_on:
+        dip, ac_slots = _ac_slots(fields)
+        for a, sl in enumerate(ac_slots):
+            if sl is None:
+                continue
+            base = capi.CHANNEL_AC_X_AMPLITUDE_V + 3 * a
+            for j, v in enumerate(sl[:3] if dip else sl[:2]):
+                v = value_or_waveform(v, lib)
+                if isinstance(v, capi.Waveform):
+                    waves[base + j] = v
     tims = None
     # the TIMS model reads the block's values whether or not it is enabled
     tb = fields.get("TIMS", fields.get("tims"))
@@ -268,27 +278,37 @@ def ac_drives(fields: dict) -> tuple[list[float], list[float], list[float], list
     (AC.dipolar_excitation, the AC.x / AC.y shorthand or
     fields.dipolar_excitation; a disabled axis gets amplitude 0); otherwise
     the single-axis AC.voltage_V drives x.  Constant values only."""
+    dip, slots = _ac_slots(fields)
+    amp, freq, phase, ramp = [0.0, 0.0], [0.0, 0.0], [0.0, 0.0], [1.0, 1.0]
+    for a, sl in enumerate(slots):
+        if sl is None:
+            continue
+        amp[a], freq[a], phase[a] = _scalar(sl[0]), _scalar(sl[1]), float(sl[3])
+        ramp[a] = _scalar(sl[2]) if dip else 1.0
+    return amp, freq, phase, ramp, int(dip)
+
+
+def _ac_slots(fields: dict) -> tuple[bool, list]:
+    """The AC drive's (amplitude, frequency, ramp, phase) JSON values per
+    axis (None for an absent or disabled axis) and whether the drive is the
+    two-axis dipolar one."""
     ac = fields.get("AC", fields.get("ac", {})) or {}
     dip = fields.get("dipolar_excitation")
     if dip is None:
         dip = ac.get("dipolar_excitation")
     if dip is None and ("x" in ac or "y" in ac):
         dip = {k: ac[k] for k in ("x", "y") if k in ac}
-    amp, freq, phase, ramp = [0.0, 0.0], [0.0, 0.0], [0.0, 0.0], [1.0, 1.0]
-    if dip is not None:
-        for a, key in enumerate(("x", "y")):
-            axis = dip.get(key)
-            if not axis or not axis.get("enabled", True):
-                continue
-            amp[a] = float(axis.get("amplitude_V", axis.get("voltage_V", 0.0)))
-            ramp[a] = float(axis.get("ramp", 1.0))
-            freq[a] = float(axis.get("frequency_Hz", 0.0))
-            phase[a] = float(axis.get("phase_rad", 0.0))
-    else:
-        amp[0] = float(ac.get("voltage_V", 0.0))
-        freq[0] = float(ac.get("frequency_Hz", 0.0))
-        phase[0] = float(ac.get("phase_rad", 0.0))
-    return amp, freq, phase, ramp, int(dip is not None)
+    if dip is None:
+        return False, [(ac.get("voltage_V", 0.0), ac.get("frequency_Hz", 0.0), 1.0, ac.get("phase_rad", 0.0)), None]
+    slots = []
+    for key in ("x", "y"):
+        axis = dip.get(key)
+        if not axis or not axis.get("enabled", True):
+            slots.append(None)
+            continue
+        slots.append((axis.get("amplitude_V", axis.get("voltage_V", 0.0)), axis.get("frequency_Hz", 0.0),
+                      axis.get("ramp", 1.0), axis.get("phase_rad", 0.0)))
+    return True, slots
 INTEGRATORS = {"Boris": capi.INTEGRATOR_BORIS, "RK4": capi.INTEGRATOR_RK4}
 COLLISIONS = {"None": capi.COLLISION_NONE, "none": capi.COLLISION_NONE, "HSS": capi.COLLISION_HSS,
               "IPM": capi.COLLISION_IPM_TABLE}

@@ -466,7 +466,15 @@ double tf_bound(const EnsConst& C, const icb_ensemble_params& P, const TimeField
     }
     const double exy = 2.0 * (wb[kChQuad] + wb[kChRfV]) * raxis / (P.radius_m * P.radius_m);
     double e = ez + exy;
-    if (C.ac) e = e + (std::fabs(C.ac_amp[0]) + std::fabs(C.ac_amp[1]));
+    if (F.inst == ICB_INSTRUMENT_LQIT) {
+        double ac = 0.0;
+        for (int a = 0; a < (F.ac_dipolar ? 2 : 1); ++a) {
+            const double A = wb[kChAcA + 3 * a] * (F.ac_dipolar ? wb[kChAcR + 3 * a] : 1.0);
+            if (A > kMinVoltage) ac += A / P.radius_m;
+        }
+        if (ac > 0.0) e = e + ac;
+    }
+    (void)C;
     return e;
 }
 
@@ -661,16 +669,24 @@ int rebuild_time_fields(icb_handle* h) {
             std::memset(&F, 0, sizeof(F));
             F.inst = P.instrument;
             F.L = P.length_m;
+            F.R = P.radius_m;
             F.r0sq = P.radius_m * P.radius_m;
             F.ox = P.origin_m[0]; F.oy = P.origin_m[1]; F.oz = P.origin_m[2];
-            const double constants[4] = {P.axial_V, P.dc_quad_V, P.rf_voltage_V, P.rf_frequency_Hz};
-            double wb[ICB_N_CHANNELS] = {0.0, 0.0, 0.0, 0.0, 1.0};
+            F.ac_dipolar = P.ac_dipolar ? 1 : 0;
+            F.ac_phase[0] = P.ac_phase_rad[0];
+            F.ac_phase[1] = P.ac_phase_rad[1];
+            // channel constants (the TIMS ramp has none: built-in ramp)
+            const double constants[ICB_N_CHANNELS] = {
+                P.axial_V, P.dc_quad_V, P.rf_voltage_V, P.rf_frequency_Hz, 0.0,
+                P.ac_amplitude_V[0], P.ac_frequency_Hz[0], P.ac_ramp[0],
+                P.ac_amplitude_V[1], P.ac_frequency_Hz[1], P.ac_ramp[1]};
+            double wb[ICB_N_CHANNELS];
             for (int c = 0; c < ICB_N_CHANNELS; ++c) {
                 if (h->wave_set[e * ICB_N_CHANNELS + c]) {
                     const icb_waveform& w = h->waves[e * ICB_N_CHANNELS + c];
                     F.ch[c] = wave_const(w);
-                    if (c < 4) wb[c] = wave_bound(w);
-                } else if (c < 4) {
+                    wb[c] = wave_bound(w);
+                } else {
                     F.ch[c].type = kWaveConstant;
                     F.ch[c].p[0] = constants[c];
                     wb[c] = std::fabs(constants[c]);
@@ -1446,6 +1462,12 @@ int icb_set_waveform(icb_handle* h, int32_t ensemble, int32_t channel, const icb
         return fail(ICB_ERR_UNSUPPORTED, "the FTICR field evaluates its voltages once (t = 0): no waveforms");
     if (channel == ICB_CHANNEL_TIMS_RAMP_FRACTION && inst != ICB_INSTRUMENT_TIMS)
         return fail(ICB_ERR_INVALID_ARGUMENT, "the TIMS ramp channel needs instrument TIMS");
+    if (channel >= ICB_CHANNEL_AC_X_AMPLITUDE_V) {
+        if (inst != ICB_INSTRUMENT_LQIT) return fail(ICB_ERR_INVALID_ARGUMENT, "the AC channels need an LQIT");
+        const bool dip = h->ens[static_cast<size_t>(ensemble)].ac_dipolar != 0;
+        if (!dip && (channel == ICB_CHANNEL_AC_X_RAMP || channel >= ICB_CHANNEL_AC_Y_AMPLITUDE_V))
+            return fail(ICB_ERR_INVALID_ARGUMENT, "ramp and y-axis AC channels need the two-axis dipolar drive");
+    }
     if (w) {
         if (int r = check_waveform(*w)) return r;
     }

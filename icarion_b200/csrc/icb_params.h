@@ -89,7 +89,11 @@ enum WaveKind : int32_t {
     kWaveConstant = 0, kWaveLinear = 1, kWaveQuadratic = 2, kWaveExponential = 3,
     kWaveSinusoidal = 4, kWavePWM = 5, kWavePulsed = 6, kWaveArbitrary = 7
 };
-enum WaveChannel : int { kChAxial = 0, kChQuad = 1, kChRfV = 2, kChRfF = 3, kChTimsRamp = 4, kNumChannels = 5 };
+enum WaveChannel : int {
+    kChAxial = 0, kChQuad = 1, kChRfV = 2, kChRfF = 3, kChTimsRamp = 4,
+    kChAcA = 5, kChAcF = 6, kChAcR = 7,      // AC axis a: kChAc* + 3 a
+    kNumChannels = 11
+};
 struct WaveConst {
     int32_t type, clamp, interp, n;
     double p[8];
@@ -101,8 +105,9 @@ struct TimeField {
     int32_t tims_nodes;      // 0 = uniform initial / final fields
     int32_t tims_final_profile;
     int32_t ramp_wave;       // ch[kChTimsRamp] replaces the built-in ramp
-    int32_t pad_;
-    double L, r0sq, ox, oy, oz;
+    int32_t ac_dipolar;      // LQIT AC: two-axis dipolar drive (else x alone, no ramp)
+    double L, R, r0sq, ox, oy, oz;
+    double ac_phase[2];
     double tims_t0, tims_t1, tims_tau, tims_ei, tims_ef;
     double tims_z[kMaxWavePoints], tims_pi[kMaxWavePoints], tims_pf[kMaxWavePoints];
     WaveConst ch[kNumChannels];

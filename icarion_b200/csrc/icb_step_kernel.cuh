@@ -429,8 +429,8 @@ __device__ __forceinline__ double tims_sample(const double* zn, const double* va
 
 // Field of an ensemble with waveforms or the TIMS model, in FP64 with the
 // reference's operation order: IMS AnalyticalFieldModel.cpp:136-161,
-// QuadrupoleRF :219-248, LQIT :81-134 (RF and axial well; the AC drives are
-// added by the caller), TIMS TIMSAxialFieldModel.h:30-44, 126-148.
+// QuadrupoleRF :219-248, LQIT :81-134 (RF, AC drives, axial well), TIMS
+// TIMSAxialFieldModel.h:30-44, 126-148.
 template <class R, class Pos>
 __device__ __noinline__ void tf_field(const TimeField& F, const Pos& x, double t, R E[3]) {
     const double rfv = wave_eval(F.ch[kChRfV], t);
@@ -457,6 +457,27 @@ __device__ __noinline__ void tf_field(const TimeField& F, const Pos& x, double t
             const double u = quad + rfv * cos(omega * t);
             ex = -2.0 * x.template rel<double>(0, lqit ? F.ox : 0.0) * u / F.r0sq;
             ey = 2.0 * x.template rel<double>(1, lqit ? F.oy : 0.0) * u / F.r0sq;
+        }
+        if (lqit) {                  // AC drives, AnalyticalFieldModel.cpp:47-61, 104-121
+            if (F.ac_dipolar) {
+                for (int a = 0; a < 2; ++a) {
+                    const double amp = wave_eval(F.ch[kChAcA + 3 * a], t);
+                    if (fabs(amp) <= kMinVoltageD) continue;
+                    const double f = wave_eval(F.ch[kChAcF + 3 * a], t);
+                    const double ramp = wave_eval(F.ch[kChAcR + 3 * a], t);
+                    const double drive = amp * ramp * cos(2.0 * kPiD * f * t + F.ac_phase[a]);
+                    if (fabs(drive) > kMinVoltageD) {
+                        if (a == 0) ex += -drive / F.R;
+                        else ey += -drive / F.R;
+                    }
+                }
+            } else {
+                const double v = wave_eval(F.ch[kChAcA], t);
+                if (fabs(v) > kMinVoltageD) {
+                    const double f = wave_eval(F.ch[kChAcF], t);
+                    ex += -v / F.R * cos(2.0 * kPiD * f * t + F.ac_phase[0]);
+                }
+            }
         }
         if (F.inst == 0) {
             ez = axial / F.L;
@@ -485,6 +506,7 @@ __device__ __forceinline__ void efield(const Consts<R>& k, const Pos& x, double 
     } else {
         if (k.tf != nullptr) {
             tf_field<R>(*k.tf, x, t, E);
+            return;
         } else {
 #pragma unroll
             for (int a = 0; a < 3; ++a) E[a] = k.E0[a] + k.G[a] * x.template rel<R>(a, k.c[a]);

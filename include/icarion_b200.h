@@ -448,14 +448,20 @@ typedef struct icb_waveform {
 } icb_waveform;
 
 /* Field channels that may carry a waveform (fields.DC.axial_V, DC.quad_V,
- * RF.voltage_V, RF.frequency_Hz, TIMS.ramp_fraction).  A channel without a
- * waveform uses the constant of icb_ensemble_params (the TIMS ramp its
- * built-in linear / exponential ramp). */
+ * RF.voltage_V, RF.frequency_Hz, TIMS.ramp_fraction, and the LQIT AC
+ * drives: axis x = AC.voltage_V / frequency_Hz of the single-axis drive or
+ * dipolar_x.amplitude_V / frequency_Hz / ramp, axis y = dipolar_y's).  A
+ * channel without a waveform uses the constant of icb_ensemble_params (the
+ * TIMS ramp its built-in linear / exponential ramp). */
 enum { ICB_CHANNEL_DC_AXIAL_V = 0, ICB_CHANNEL_DC_QUAD_V = 1, ICB_CHANNEL_RF_VOLTAGE_V = 2,
-       ICB_CHANNEL_RF_FREQUENCY_HZ = 3, ICB_CHANNEL_TIMS_RAMP_FRACTION = 4, ICB_N_CHANNELS = 5 };
+       ICB_CHANNEL_RF_FREQUENCY_HZ = 3, ICB_CHANNEL_TIMS_RAMP_FRACTION = 4,
+       ICB_CHANNEL_AC_X_AMPLITUDE_V = 5, ICB_CHANNEL_AC_X_FREQUENCY_HZ = 6, ICB_CHANNEL_AC_X_RAMP = 7,
+       ICB_CHANNEL_AC_Y_AMPLITUDE_V = 8, ICB_CHANNEL_AC_Y_FREQUENCY_HZ = 9, ICB_CHANNEL_AC_Y_RAMP = 10,
+       ICB_N_CHANNELS = 11 };
 
 /* Set (w != NULL) or clear (w == NULL) the waveform of one field channel of
- * one ensemble (IMS, QuadrupoleRF, LQIT or TIMS).  An ensemble with a
+ * one ensemble (IMS, QuadrupoleRF, LQIT or TIMS; the AC channels on an LQIT
+ * only, the ramp channels with the two-axis dipolar drive).  An ensemble with a
  * waveform, like every TIMS ensemble, is stepped through the time-dependent
  * field path (one field evaluation per step or RK4 stage). */
 int icb_set_waveform(struct icb_handle* h, int32_t ensemble, int32_t channel, const icb_waveform* w);

@@ -224,16 +224,18 @@ typedef struct {
 } orc_tims;
 
 /* channels: 0 DC.axial_V, 1 DC.quad_V, 2 RF.voltage_V, 3 RF.frequency_Hz,
- * 4 TIMS.ramp_fraction */
-static orc_wave g_wave[5];
-static int g_wave_set[5];
+ * 4 TIMS.ramp_fraction, 5-7 AC x amplitude / frequency / ramp (the
+ * single-axis drive or dipolar_x), 8-10 the same for dipolar_y */
+#define ORC_N_CH 11
+static orc_wave g_wave[ORC_N_CH];
+static int g_wave_set[ORC_N_CH];
 static orc_tims g_tims;
 static int g_tims_set;
 
 void orc_set_time_field(const orc_tims* tims, const orc_wave* waves, const int32_t* set) {
     g_tims_set = tims != NULL;
     if (tims) g_tims = *tims;
-    for (int c = 0; c < 5; ++c) {
+    for (int c = 0; c < ORC_N_CH; ++c) {
         g_wave_set[c] = (waves && set && set[c]) ? 1 : 0;
         if (g_wave_set[c]) g_wave[c] = waves[c];
     }
@@ -314,6 +316,12 @@ static double chan(const orc_domain* d, int c, double t) {
     case 1: return d->dc_quad_V;
     case 2: return d->rf_voltage_V;
     case 3: return d->rf_frequency_Hz;
+    case 5: return d->ac_amplitude_V[0];
+    case 6: return d->ac_frequency_Hz[0];
+    case 7: return d->ac_ramp[0];
+    case 8: return d->ac_amplitude_V[1];
+    case 9: return d->ac_frequency_Hz[1];
+    case 10: return d->ac_ramp[1];
     default: return 0.0;
     }
 }
@@ -418,15 +426,19 @@ static void field_E(const orc_domain* d, const double p[3], double t, double E[3
             /* two-axis dipolar drive: amplitude * ramp * cos(w t + phase), skipped
              * where |drive| <= threshold (eval_dipolar_axis_voltage) */
             for (int a = 0; a < 2; ++a) {
-                if (fabs(d->ac_amplitude_V[a]) <= ORC_MIN_VOLTAGE) continue;
-                const double omega = 2.0 * M_PI * d->ac_frequency_Hz[a];
-                const double drive = d->ac_amplitude_V[a] * d->ac_ramp[a] * cos(omega * t + d->ac_phase_rad[a]);
+                const double amp = chan(d, 5 + 3 * a, t);
+                if (fabs(amp) <= ORC_MIN_VOLTAGE) continue;
+                const double omega = 2.0 * M_PI * chan(d, 6 + 3 * a, t);
+                const double drive = amp * chan(d, 7 + 3 * a, t) * cos(omega * t + d->ac_phase_rad[a]);
                 if (fabs(drive) > ORC_MIN_VOLTAGE) E[a] += -drive / d->radius_m;
             }
-        } else if (fabs(d->ac_amplitude_V[0]) > ORC_MIN_VOLTAGE) {
+        } else {
             /* single-axis drive on x */
-            const double omega_ac = 2.0 * M_PI * d->ac_frequency_Hz[0];
-            E[0] += -d->ac_amplitude_V[0] / d->radius_m * cos(omega_ac * t + d->ac_phase_rad[0]);
+            const double v = chan(d, 5, t);
+            if (fabs(v) > ORC_MIN_VOLTAGE) {
+                const double omega_ac = 2.0 * M_PI * chan(d, 6, t);
+                E[0] += -v / d->radius_m * cos(omega_ac * t + d->ac_phase_rad[0]);
+            }
         }
         if (fabs(axial) > ORC_MIN_VOLTAGE) {
             const double L = d->length_m;
@@ -1007,9 +1019,8 @@ static double wave_bound(const orc_wave* w) {
 static double tf_field_bound(const orc_domain* d) {
     const double Rp = d->radius_m + ORC_GEOM_EPS;
     const double L = d->length_m;
-    const double cst[4] = {d->axial_V, d->dc_quad_V, d->rf_voltage_V, d->rf_frequency_Hz};
-    double wb[4], ez, raxis = Rp, e;
-    for (int c = 0; c < 4; ++c) wb[c] = g_wave_set[c] ? wave_bound(&g_wave[c]) : fabs(cst[c]);
+    double wb[ORC_N_CH], ez, raxis = Rp, e;
+    for (int c = 0; c < ORC_N_CH; ++c) wb[c] = g_wave_set[c] ? wave_bound(&g_wave[c]) : fabs(chan(d, c, 0.0));
     if (d->instrument == 4) {
         const orc_tims* T = &g_tims;
         const int n = g_tims_set ? T->n_nodes : 0;
@@ -1029,8 +1040,8 @@ static double tf_field_bound(const orc_domain* d) {
     if (d->instrument == 3) {
         double ac = 0.0;
         for (int a = 0; a < (d->ac_dipolar ? 2 : 1); ++a) {
-            const double A = d->ac_amplitude_V[a] * (d->ac_dipolar ? d->ac_ramp[a] : 1.0);
-            if (fabs(A) > ORC_MIN_VOLTAGE) ac += fabs(-A / d->radius_m);
+            const double A = wb[5 + 3 * a] * (d->ac_dipolar ? wb[7 + 3 * a] : 1.0);
+            if (A > ORC_MIN_VOLTAGE) ac += A / d->radius_m;
         }
         if (ac > 0.0) e = e + ac;
     }
@@ -1040,7 +1051,7 @@ static double tf_field_bound(const orc_domain* d) {
 static int time_field_on(const orc_domain* d) {
     int c;
     if (d->instrument == 4) return 1;
-    for (c = 0; c < 5; ++c)
+    for (c = 0; c < ORC_N_CH; ++c)
         if (g_wave_set[c]) return 1;
     return 0;
 }

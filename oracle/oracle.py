@@ -61,7 +61,8 @@ class OTims(C.Structure):
                 ("pf", C.c_double * 64)]
 
 
-WAVE_KEYS = ("wave_axial", "wave_quad", "wave_rfv", "wave_rff", "wave_ramp")
+WAVE_KEYS = ("wave_axial", "wave_quad", "wave_rfv", "wave_rff", "wave_ramp",
+             "wave_acxA", "wave_acxf", "wave_acxr", "wave_acyA", "wave_acyf", "wave_acyr")
 
 
 def parse_wave(spec: str) -> dict:
@@ -115,8 +116,8 @@ def wave_value(spec: str, t: float) -> float:
 def set_time_field(kw: dict | None) -> None:
     """Waveforms and TIMS field of the harness domain keys (None clears)."""
     kw = kw or {}
-    waves = (OWave * 5)()
-    on = (C.c_int32 * 5)()
+    waves = (OWave * len(WAVE_KEYS))()
+    on = (C.c_int32 * len(WAVE_KEYS))()
     for c, key in enumerate(WAVE_KEYS):
         if key in kw:
             waves[c] = wave_struct(kw[key])

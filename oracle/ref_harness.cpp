@@ -25,9 +25,11 @@
 //   field    <domain keys> in= out=    E of the domain's field model at the
 //            (x, y, z, t) rows of in (4 doubles each) into out (3 each)
 //
-// Time-dependent domain keys: wave_<axial|quad|rfv|rff|ramp>=
+// Time-dependent domain keys: wave_<axial|quad|rfv|rff|ramp|acxA|acxf|acxr|acyA|acyf|acyr>=
 // "type|clamp|interp|p0,p1,..|t0,t1,..|v0,v1,.." (type 0..7 in the order of
-// WaveformType), attached inline as the loader does, or through the
+// WaveformType; acx / acy: AC drive amplitude A, frequency f, ramp r of the
+// single-axis drive or dipolar x, and dipolar y), attached inline as the
+// loader does, or through the
 // waveform library (waveform_ref) with wave_ref=1; TIMS: tims=1 tims_mode=
 // tims_ei= tims_ef= tims_t0= tims_t1= tims_tau= tims_z= tims_pi= tims_pf=.
 //   run      in= out= <domain keys> integrator= collision= steps= snap=
@@ -240,7 +242,12 @@ config::DomainConfig make_domain(const Args& a) {
     const std::pair<const char*, config::ValueOrWaveform*> chans[] = {
         {"wave_axial", &d.fields.dc.axial_V}, {"wave_quad", &d.fields.dc.quad_V},
         {"wave_rfv", &d.fields.rf.voltage_V}, {"wave_rff", &d.fields.rf.frequency_Hz},
-        {"wave_ramp", &d.fields.tims.ramp_fraction}};
+        {"wave_ramp", &d.fields.tims.ramp_fraction},
+        {"wave_acxA", d.fields.ac.dipolar_excitation_defined ? &d.fields.ac.dipolar_x.amplitude_V : &d.fields.ac.voltage_V},
+        {"wave_acxf", d.fields.ac.dipolar_excitation_defined ? &d.fields.ac.dipolar_x.frequency_Hz : &d.fields.ac.frequency_Hz},
+        {"wave_acxr", &d.fields.ac.dipolar_x.ramp},
+        {"wave_acyA", &d.fields.ac.dipolar_y.amplitude_V}, {"wave_acyf", &d.fields.ac.dipolar_y.frequency_Hz},
+        {"wave_acyr", &d.fields.ac.dipolar_y.ramp}};
     for (const auto& [key, slot] : chans) {
         if (!a.count(key)) continue;
         config::Waveform w = parse_wave(str(a, key, ""));

@@ -73,6 +73,12 @@ TIMS_WAVE_DOMAIN = dict(instrument="IMS", origin_z=-0.01, length=0.02, radius=0.
 # a gated PWM DC quadrupole
 LQIT_WAVE_DOMAIN = dict(LQIT_DOMAIN, wave_axial="1|1|0|2,5,0,4e-6", wave_rfv="4|0|0|200,20,2e5,0.3",
                         wave_rff="2|0|0|1e6,1e10,0,0,1e-5", wave_quad="5|0|0|0.5,1.5,5e5,0.3,0.2,1e-6,4e-6")
+# LQIT AC drives as waveforms: a resonance scan (chirped x drive faded in,
+# pulsed y drive) on the dipolar trap, and a modulated single-axis drive
+# with a quadratic chirp
+LQIT_AC_DOMAIN = dict(LQIT_DOMAIN, wave_acxf="1|1|0|1e5,2e5,0,4e-6", wave_acxr="1|1|0|0,1,0,2e-6",
+                      wave_acyA="6|0|0|0,0.4,1e-6,2e-6")
+LQIT1_AC_DOMAIN = dict(LQIT1_DOMAIN, wave_acxA="4|0|0|0.4,0.2,3e5,0", wave_acxf="2|0|0|9e4,2e10,0,0,1e-5")
 # IMS / QuadrupoleRF read waveforms given as waveform_ref
 IMS_REF_DOMAIN = dict(IMS_DOMAIN, wave_ref=1, wave_axial="3|1|0|1000,500,-3e5,1e-6,6e-6",
                       wave_rfv="6|0|0|0,50,1e-6,2e-6", wave_rff="0|0|0|1e6", wave_quad="7|0|1||0,2e-6,4e-6|0,1,-1")
@@ -101,7 +107,7 @@ WAVE_TYPE_SPECS = {
 def field_cases() -> dict:
     cases = {"tims": TIMS_DOMAIN, "tims_exp": TIMS_EXP_DOMAIN, "tims_wave": TIMS_WAVE_DOMAIN,
              "lqit_wave": LQIT_WAVE_DOMAIN, "ims_ref": IMS_REF_DOMAIN, "quadrf_ref": QUAD_REF_DOMAIN,
-             "ims_inline": IMS_INLINE_DOMAIN}
+             "ims_inline": IMS_INLINE_DOMAIN, "lqit_ac": LQIT_AC_DOMAIN, "lqit1_ac": LQIT1_AC_DOMAIN}
     for name, spec in WAVE_TYPE_SPECS.items():
         cases[f"wave_{name}"] = dict(QUAD_DOMAIN, wave_ref=1, wave_rfv=spec)
     return cases
@@ -230,6 +236,8 @@ def push_cases() -> dict:
         "boris_quadrf_waveref": (QUAD_REF_DOMAIN, "boris", lambda: init_state(64, mass_amu=100.0, sigma_pos=2e-4),
                                  4000, 1e-9),
         "boris_ims_inline": (IMS_INLINE_DOMAIN, "boris", lambda: init_state(64), 3000, 5e-10),
+        "boris_lqit_ac": (LQIT_AC_DOMAIN, "boris", lambda: init_state(64, sigma_pos=2e-4), 5000, 1e-9),
+        "rk4_lqit1_ac": (LQIT1_AC_DOMAIN, "rk4", lambda: init_state(64, sigma_pos=2e-4), 4000, 1e-9),
     }
 
 

@@ -44,8 +44,7 @@ def time_field_structs(kw: dict) -> tuple[dict, object]:
     """Waveform channels and TIMS field of the harness keys as ABI structs,
     every channel evaluated (the reference's waveform_ref semantics)."""
     import oracle as orc
-    chans = (capi.CHANNEL_DC_AXIAL_V, capi.CHANNEL_DC_QUAD_V, capi.CHANNEL_RF_VOLTAGE_V,
-             capi.CHANNEL_RF_FREQUENCY_HZ, capi.CHANNEL_TIMS_RAMP_FRACTION)
+    chans = range(capi.N_CHANNELS)          # the order of orc.WAVE_KEYS
     waves = {ch: orc.wave_struct(kw[key], cls=capi.Waveform) for ch, key in zip(chans, orc.WAVE_KEYS) if key in kw}
     tims = orc.tims_struct(kw, cls=capi.TimsField,
                            names=("initial_uniform_V_m", "final_uniform_V_m", "ramp_start_s", "ramp_end_s",
@@ -94,6 +93,15 @@ def domain_json(kw: dict) -> dict:
            for a in ("x", "y") if f"dip_{a}_A" in kw}
     if dip:
         ac["dipolar_excitation"] = dip
+        for a in ("x", "y"):
+            for key, name in ((f"wave_ac{a}A", "amplitude_V"), (f"wave_ac{a}f", "frequency_Hz"),
+                              (f"wave_ac{a}r", "ramp")):
+                if key in kw and a in dip:
+                    dip[a][name] = wave_json(kw[key])
+    else:
+        for key, name in (("wave_acxA", "voltage_V"), ("wave_acxf", "frequency_Hz")):
+            if key in kw:
+                ac[name] = wave_json(kw[key])
     return {
         "instrument": kw["instrument"],
         "geometry": {"origin_m": [0.0, 0.0, kw.get("origin_z", 0.0)], "length_m": kw["length"], "radius_m": kw["radius"]},

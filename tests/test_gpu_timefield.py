@@ -20,7 +20,7 @@ from icarion_b200.sim import Simulation, device_count
 pytestmark = pytest.mark.gpu
 
 TIMED_PUSHES = ["boris_tims", "rk4_tims_exp", "boris_tims_wave", "boris_lqit_wave", "rk4_ims_waveref",
-                "boris_quadrf_waveref", "boris_ims_inline"]
+                "boris_quadrf_waveref", "boris_ims_inline", "boris_lqit_ac", "rk4_lqit1_ac"]
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -154,9 +154,20 @@ def test_time_field_argument_checks(golden):
             assert ei.value.code == capi.ICB_ERR_INVALID_ARGUMENT, ch
         with pytest.raises(IcbError):
             sim.set_tims_field(0, capi.TimsField())
+    z1 = golden("push_rk4_lqit1.npz")              # single-axis AC drive
+    with Simulation([ensemble_from_golden(z1)], precision=capi.PREC_FP64, integrator=capi.INTEGRATOR_RK4,
+                    collision=capi.COLLISION_NONE) as sim:
+        w = capi.Waveform()
+        for ch in (capi.CHANNEL_AC_X_RAMP, capi.CHANNEL_AC_Y_AMPLITUDE_V):
+            with pytest.raises(IcbError) as ei:
+                sim.set_waveform(0, ch, w)
+            assert ei.value.code == capi.ICB_ERR_INVALID_ARGUMENT
+        sim.set_waveform(0, capi.CHANNEL_AC_X_FREQUENCY_HZ, w)
     zt = golden("push_boris_tims.npz")
     with Simulation([ensemble_from_golden(zt)], precision=capi.PREC_FP64, integrator=capi.INTEGRATOR_BORIS,
                     collision=capi.COLLISION_NONE) as sim:
+        with pytest.raises(IcbError):
+            sim.set_waveform(0, capi.CHANNEL_AC_X_AMPLITUDE_V, capi.Waveform())
         f = capi.TimsField(); f.n_nodes = 1
         with pytest.raises(IcbError):
             sim.set_tims_field(0, f)

@@ -18,7 +18,7 @@ from icarion_b200 import _capi as capi
 from icarion_b200 import config as cfg
 
 TIMED_PUSHES = ["boris_tims", "rk4_tims_exp", "boris_tims_wave", "boris_lqit_wave", "rk4_ims_waveref",
-                "boris_quadrf_waveref", "boris_ims_inline"]
+                "boris_quadrf_waveref", "boris_ims_inline", "boris_lqit_ac", "rk4_lqit1_ac"]
 KEYS = ("x", "y", "z", "vx", "vy", "vz")
 
 
@@ -143,6 +143,27 @@ def test_time_fields_follow_the_field_models():
              "fields": {"DC": {"radial_V": {"type": "sinusoidal", "offset": 1.0, "amplitude": 0.5,
                                             "frequency_Hz": 1e3, "phase_rad": 0.5}}}}
     assert cfg.ensemble_params(fticr, 1e-18, 1e-9)["radial_V"] == 1.0 + 0.5 * math.sin(0.5)
+
+
+def test_ac_drive_channels_from_json():
+    """LQIT AC drives as waveforms: dipolar axes carry amplitude, frequency
+    and ramp channels, a disabled axis none; the single-axis drive carries
+    amplitude and frequency (AnalyticalFieldModel.cpp:47-61, 104-121)."""
+    chirp = {"type": "linear", "start": 1e5, "end": 2e5, "end_time_s": 1e-3}
+    fade = {"type": "linear", "start": 0.0, "end": 1.0, "end_time_s": 1e-4}
+    base = {"instrument": "LQIT", "geometry": {"length_m": 0.05, "radius_m": 0.004},
+            "env": {"temperature_K": 300.0, "pressure_Pa": 0.1, "gas_species": "He"}}
+    dom = dict(base, fields={"AC": {"dipolar_excitation": {
+        "x": {"amplitude_V": 0.5, "frequency_Hz": chirp, "ramp": fade},
+        "y": {"enabled": False, "amplitude_V": chirp}}}})
+    e = cfg.ensemble_params(dom, 1e-18, 1e-9)
+    assert e["ac_dipolar"] == 1 and e["ac_amplitude_V"] == [0.5, 0.0] and e["ac_frequency_Hz"][0] == 0.0
+    waves, _ = cfg.time_fields(dom)
+    assert set(waves) == {capi.CHANNEL_AC_X_FREQUENCY_HZ, capi.CHANNEL_AC_X_RAMP}
+    dom = dict(base, fields={"AC": {"voltage_V": chirp, "frequency_Hz": 9e4}})
+    waves, _ = cfg.time_fields(dom)
+    assert set(waves) == {capi.CHANNEL_AC_X_AMPLITUDE_V}
+    assert cfg.ensemble_params(dom, 1e-18, 1e-9)["ac_dipolar"] == 0
 
 
 def test_time_field_structs_layout():
