@@ -147,7 +147,7 @@ def test_time_field_argument_checks(golden):
         bad.append((capi.CHANNEL_RF_FREQUENCY_HZ, w))         # not finite
         w = capi.Waveform()
         bad.append((capi.CHANNEL_TIMS_RAMP_FRACTION, w))      # not a TIMS domain
-        bad.append((7, w))                                    # unknown channel
+        bad.append((capi.N_CHANNELS, w))                      # unknown channel
         for ch, w in bad:
             with pytest.raises(IcbError) as ei:
                 sim.set_waveform(0, ch, w)
