@@ -46,6 +46,18 @@ SWEEP_WORKLOAD = ("E/N sweep, 64 ensembles (2-100 Td log-spaced, N2 300 K 1000 P
                   "(100/250/600 A^2) round-robin, {n:,} ions (log-uniform 1k-256k per ensemble, seed 123), "
                   "dt = 0.1/nu_max per ensemble, Boris + HSS")
 WORKLOAD = "IMS drift, 1,048,576 ions (200 Da, +1, 150 A^2 HSS) in N2 300 K 1000 Pa, 20 Td, Boris + HSS, dt 5e-10 s"
+# trapped IMS on the time-dependent field path (TIMSAxialFieldModel): 20 mm
+# tube, axial profile 0 -> -4495 V/m ramped to zero over 10..40 us, RF
+# 180 V at 2 MHz (r0 5 mm), axial gas flow 134 m/s, N2 300 K 310 Pa
+TIMS_DOMAIN = {"instrument": "TIMS", "geometry": {"origin_m": [0.0, 0.0, -0.01], "length_m": 0.02, "radius_m": 0.005},
+               "env": {"temperature_K": 300.0, "pressure_Pa": 310.0, "gas_species": "N2",
+                       "flow_model": "axial_uniform", "axial_flow_velocity_m_s": 134.0},
+               "fields": {"RF": {"voltage_V": 180.0, "frequency_Hz": 2.0e6}, "DC": {"quad_V": 0.0},
+                          "TIMS": {"z_positions_m": [0.0, 0.02], "axial_field_initial_profile_V_m": [0.0, -4495.0],
+                                   "axial_field_final_profile_V_m": [0.0, 0.0], "ramp_start_s": 1.0e-5,
+                                   "ramp_end_s": 4.0e-5, "ramp_mode": "linear"}}}
+TIMS_WORKLOAD = ("TIMS ramp, 1,048,576 ions (200 Da, +1, 150 A^2 HSS) in N2 300 K 310 Pa against 134 m/s flow, "
+                 "profile 0..-4495 V/m ramped over 10-40 us, RF 180 V 2 MHz, Boris + HSS, dt 5e-10 s")
 # Algorithmic bytes each ion moves per launch of the fused kernel:
 # read  x,y,z(24) v(12) tau,Q*(8) next,start(8) mass,charge(16) flags(1) t_arr(8) = 77
 # write x,y,z(24) v(12) tau,Q*(8) next,start(8) flags(1)                          = 53
@@ -251,6 +263,7 @@ def run_ours(args) -> None:
     dev = torch.cuda.current_device()
     prec_id = {"mixed": capi.PREC_MIXED, "fp64": capi.PREC_FP64, "hilo": capi.PREC_MIXED_HILO}[args.precision]
 
+    tf_domain = None
     if args.workload == "en-sweep":
         # batched E/N sweep: 64 ensembles in one launch sequence (CUDA graphs, autotuned shape)
         from icarion_b200 import sweep
@@ -258,6 +271,15 @@ def run_ours(args) -> None:
         ensembles, st0, offsets, n_ions = sw.ensembles, sw.ions, sw.offsets, sw.n_ions
         workload = SWEEP_WORKLOAD.format(n=n_ions)
         args.graphs, args.autotune = True, True
+    elif args.workload == "tims-1M":
+        # trapped IMS: axial profile ramped over 10..40 us against a 134 m/s
+        # axial gas flow, RF radial confinement (the time-dependent field path)
+        tf_domain = TIMS_DOMAIN
+        ensembles = [cfg.ensemble_params(tf_domain, 150e-20, DT, detector_z_m=1e30)]
+        spec = cfg.species_spec(N_IONS, 200.0 * cfg.AMU_TO_KG, cfg.ELEM_CHARGE_C,
+                                {"type": "gaussian", "center": [0, 0, 0], "std": [5e-4] * 3},
+                                {"type": "thermal", "temperature_K": 300.0})
+        st0, offsets, n_ions, workload = generate_ions(123, [spec]), None, N_IONS, TIMS_WORKLOAD
     else:
         domain = {"instrument": "IMS", "geometry": {"origin_m": [0.0, 0.0, -0.01], "length_m": 0.1, "radius_m": 0.05},
                   "env": {"temperature_K": 300.0, "pressure_Pa": 1000.0, "gas_species": "N2"},
@@ -281,6 +303,8 @@ def run_ours(args) -> None:
                        pending_threshold=args.pending, steps_per_vote=args.spv, use_graphs=int(args.graphs),
                        stepping=STEPPING[args.stepping])
         s.set_stream(stream.cuda_stream)
+        if tf_domain is not None:
+            s.apply_time_fields(0, tf_domain)
         s.upload(st0, ens_offsets=offsets, first_id=first_id)
         return s
 
@@ -692,7 +716,7 @@ def main():
     ap.add_argument("--spv", type=int, default=0, help="collision-free steps between warp votes")
     ap.add_argument("--stepping", choices=["events", "per-step"], default="events",
                     help="float forms: event-to-event closed-form drift, or the step-by-step loop")
-    ap.add_argument("--workload", choices=["ims-1M", "en-sweep", "fticr-sc", "ipm"], default="ims-1M",
+    ap.add_argument("--workload", choices=["ims-1M", "en-sweep", "fticr-sc", "ipm", "tims-1M"], default="ims-1M",
                     help="ims-1M: the 1,048,576-ion IMS run (default); en-sweep: the batched 64-ensemble E/N "
                          "sweep; fticr-sc: the 262,144-ion FT-ICR cell with P3M space charge; ipm: learned "
                          "interaction-potential collisions vs the table")
