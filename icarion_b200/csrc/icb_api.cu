@@ -307,6 +307,8 @@ struct icb_handle {
     std::vector<icb_tims_field> tims;
     std::vector<uint8_t> tims_set;
     DevBuf<TimeField> tfield;
+    DevBuf<double> tf_tab;             // per-step field scalars, one launch chunk at a time
+    bool any_tf = false;
     int base_field_kind = kFieldUniform;
     // EHSS geometry: host copies per ensemble and the device arrays
     std::vector<std::vector<double4>> ehss_host;
@@ -720,6 +722,7 @@ int rebuild_time_fields(icb_handle* h) {
             C.Emax = base;
         }
     }
+    h->any_tf = any;
     h->field_kind = any ? std::max(h->base_field_kind, static_cast<int>(kFieldLinearRF)) : h->base_field_kind;
     if (any) {
         ICB_CUDA(cudaStreamSynchronize(h->stream));
@@ -732,10 +735,59 @@ int rebuild_time_fields(icb_handle* h) {
 
 inline unsigned grid_for(uint64_t n, int block) { return static_cast<unsigned>((n + block - 1) / block); }
 
-// Step kernels for ions [lo, hi) (all ions by default).
+uint32_t tf_stride(const icb_handle* h) { return h->cfg.integrator == ICB_INTEGRATOR_RK4 ? 12u : 6u; }
+
+// Room for the per-step field tables of launches of up to K steps (all
+// ensembles, plus the time sequences); allocates outside stream capture only.
+int ensure_tf_tab(icb_handle* h, uint32_t K, cudaStream_t st) {
+    const size_t rows = static_cast<size_t>(K) + 1u;
+    const size_t need = h->ens.size() * rows * (tf_stride(h) + 1u);
+    if (h->tf_tab.n >= need) return ICB_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    ICB_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+        return fail(ICB_ERR_STATE, "field table too small inside a stream capture");
+    ICB_CUDA(cudaDeviceSynchronize());
+    ICB_CUDA(h->tf_tab.alloc(need));
+    h->drop_graph();
+    return ICB_OK;
+}
+
+// The time-only field scalars of every step of a K-step launch for the
+// ensembles with a time-dependent field, built on `st` before the step
+// kernels read them (stage 0 at t_k; RK4 adds the half step).
+int enqueue_tf_tables(icb_handle* h, uint32_t K, cudaStream_t st) {
+    if (!h->any_tf) return ICB_OK;
+    if (int r = ensure_tf_tab(h, K, st)) return r;
+    const uint32_t stride = tf_stride(h);
+    const int n_ens = static_cast<int>(h->ens.size());
+    double* tseq = h->tf_tab.p + h->ens.size() * (static_cast<size_t>(K) + 1u) * stride;
+    for (int e0 = 0; e0 < n_ens; e0 += kMaxLaunchEns) {
+        const int ne = std::min(kMaxLaunchEns, n_ens - e0);
+        StepParams p;
+        std::memset(&p, 0, sizeof(p));
+        p.tfield = h->tfield.p;
+        p.t_dev = h->t_dev.p;
+        p.n_steps = K;
+        p.ens_base = static_cast<uint32_t>(e0);
+        p.n_ens = static_cast<uint32_t>(ne);
+        for (int e = 0; e < ne; ++e) p.ens[e] = h->ens_const[static_cast<size_t>(e0 + e)];
+        const cudaError_t te = launch_tf_table(p, h->tf_tab.p, tseq, stride, st);
+        ++h->launches;
+        if (te != cudaSuccess) return fail(ICB_ERR_CUDA, "field table launch: %s", cudaGetErrorString(te));
+    }
+    return ICB_OK;
+}
+
+// Step kernels for ions [lo, hi) (all ions by default); the field tables of
+// a time-dependent field are built first unless the caller built them
+// (build_tf = false).
 int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_finalize, uint64_t lo = 0,
-                uint64_t hi = ~0ull, cudaStream_t stream = nullptr) {
+                uint64_t hi = ~0ull, cudaStream_t stream = nullptr, bool build_tf = true) {
     cudaStream_t st = stream ? stream : h->stream;
+    if (build_tf) {
+        if (int r = enqueue_tf_tables(h, K, st)) return r;
+    }
     const int n_ens = static_cast<int>(h->ens.size());
     if ((h->coll == kCollIPMTable || h->coll == kCollIPMMLP) && h->ipm_nE == 0)
         return fail(ICB_ERR_STATE, "interaction-potential collisions need icb_ipm_configure first");
@@ -798,6 +850,10 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         for (int e = 0; e < ne; ++e) {
             p.ens[e] = h->ens_const[static_cast<size_t>(e0 + e)];
             if (p.ens[e].flow) p.flows = 1u;
+        }
+        if (h->any_tf) {
+            p.tf_tab = h->tf_tab.p;
+            p.tf_stride = tf_stride(h);
         }
         const dim3 grid(grid_for(en - b, h->block)), block(static_cast<unsigned>(h->block));
         cudaError_t err;
@@ -1298,6 +1354,9 @@ int icb_advance(icb_handle* h, uint64_t n_steps, icb_run_stats* stats) {
             // Captured on the handle's own non-blocking stream (capture is
             // not allowed on the legacy default stream); replayed on h->stream.
             cudaGraph_t g = nullptr;
+            if (h->any_tf) {
+                if (int r = ensure_tf_tab(h, static_cast<uint32_t>(std::min<uint64_t>(n_steps, h->K)), s)) return r;
+            }
             ICB_CUDA(cudaStreamBeginCapture(h->own_stream, cudaStreamCaptureModeThreadLocal));
             h->stream = h->own_stream;
             int r = enqueue_advance(h, n_steps, 0);
@@ -1683,6 +1742,8 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
     // stream (so a chunk's blocks fill the SMs while the previous chunk's
     // last blocks finish), results on the copy-back stream.  Queued in chunk
     // order, the first chunk's steps start as soon as its inputs are in.
+    // one field table for all chunks, ahead of every chunk's steps
+    if (int r = enqueue_tf_tables(h, static_cast<uint32_t>(n_steps), cs)) return r;
     for (int c = 0; c < n_chunks; ++c) {
         const uint64_t a = lim[static_cast<size_t>(c)], b = lim[static_cast<size_t>(c) + 1], cnt = b - a;
         if (cnt == 0) continue;
@@ -1700,7 +1761,7 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
             for (int k = 0; k < 3; ++k) k_to_float<<<g, 256, 0, ks>>>(h->hstage.p + k * n + a, vf[k] + a, cnt);
         k_flags_update<<<g, 256, 0, ks>>>(h->active_stage.p + a, h->flags.p + a, cnt);
         ICB_CUDA(cudaGetLastError());
-        if (int r = launch_step(h, static_cast<uint32_t>(n_steps), 1, 1, 1, a, b, ks)) return r;
+        if (int r = launch_step(h, static_cast<uint32_t>(n_steps), 1, 1, 1, a, b, ks, false)) return r;
         if (!f64)
             for (int k = 0; k < 3; ++k) k_from_float<<<g, 256, 0, ks>>>(vf[k] + a, h->hstage.p + k * n + a, cnt);
         k_flags_out<<<g, 256, 0, ks>>>(h->flags.p + a, h->active_stage.p + a, cnt);

@@ -12,6 +12,8 @@ namespace icb {
 
 // Kernel launchers, one per precision translation unit.  Each returns the
 // launch's cudaError_t (cudaErrorNotSupported for an absent combination).
+// Per-step time-only field scalars of one launch (tf_tab of StepParams).
+cudaError_t launch_tf_table(const StepParams& p, double* tab, double* tseq, uint32_t stride, cudaStream_t s);
 cudaError_t launch_step_fp64(int integ, int coll, int field, bool mag, const StepParams& p,
                              dim3 grid, dim3 block, cudaStream_t s);
 cudaError_t launch_step_mixed(int integ, int coll, int field, bool mag, const StepParams& p,

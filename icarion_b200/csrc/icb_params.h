@@ -154,6 +154,10 @@ struct StepParams {
     const float* mlp_f;                // W1 (128), b1 (64), b2 (64), W3 (64), b3 (1)
     const MixConst* mix;               // per ensemble (global index), HSS mixtures
     const TimeField* tfield;           // per ensemble (global index), nullable
+    // per-step time-only field scalars of this launch (k_tf_table), rows
+    // k = 0..n_steps of tf_stride doubles per chunk ensemble; nullable
+    const double* tf_tab;
+    uint32_t tf_stride;
     // EHSS molecule geometry: atoms (x, y, z, radius) of ensemble e in
     // [ehss_off[e], ehss_off[e+1]), gas (contact) radius per ensemble
     const double4* ehss_atoms;

@@ -256,6 +256,9 @@ struct Consts {
     R escq[3];               // space-charge force E_sc q of this step
     bool sc;                 // space charge on (one step per launch)
     const TimeField* tf;     // time-dependent field (waveforms, TIMS) or null
+    const double* tftab;     // its per-step scalars for this launch (k_tf_table)
+    const double* tfrow;     // ... of the current step
+    uint32_t tfstride;       // doubles per row
 };
 
 template <class R, int FIELD, bool MAG>
@@ -427,75 +430,124 @@ __device__ __forceinline__ double tims_sample(const double* zn, const double* va
     return val[i0] + alpha * (val[i1] - val[i0]);
 }
 
-// Field of an ensemble with waveforms or the TIMS model, in FP64 with the
-// reference's operation order: IMS AnalyticalFieldModel.cpp:136-161,
-// QuadrupoleRF :219-248, LQIT :81-134 (RF, AC drives, axial well), TIMS
-// TIMSAxialFieldModel.h:30-44, 126-148.
-template <class R, class Pos>
-__device__ __noinline__ void tf_field(const TimeField& F, const Pos& x, double t, R E[3]) {
+// Time-only part of the field of an ensemble with waveforms or the TIMS
+// model at time t, in FP64 with the reference's operation order (IMS
+// AnalyticalFieldModel.cpp:136-161, QuadrupoleRF :219-248, LQIT :81-134,
+// TIMS TIMSAxialFieldModel.h:30-44, 126-148).  Every ion of the ensemble
+// shares it at a step, so k_tf_table evaluates it once per step (and RK4
+// half step) of a launch:
+//   s[0] U = dc_quad + V cos(2 pi f t)      s[1] 1 if the RF term applies
+//   s[2] IMS / QuadrupoleRF axial / L, LQIT axial / L^2, TIMS ramp f(t)
+//   s[3] 1 if the axial term applies        s[4], s[5] AC drive E_x, E_y
+constexpr int kTfScalars = 6;
+static __device__ __noinline__ void tf_scalars(const TimeField& F, double t, double s[kTfScalars]) {
     const double rfv = wave_eval(F.ch[kChRfV], t);
-    double ex = 0.0, ey = 0.0, ez = 0.0;
-    if (F.inst == 4) {           // TIMS
-        const double zl = x.template rel<double>(2, F.oz);
-        const double f = tims_ramp(F, t);
-        const double ei = tims_sample(F.tims_z, F.tims_pi, F.tims_nodes, zl, F.tims_ei);
-        const double ef = tims_sample(F.tims_z, F.tims_pf, F.tims_final_profile ? F.tims_nodes : 0, zl, F.tims_ef);
-        ez = (1.0 - f) * ei + f * ef;
+    s[0] = 0.0; s[1] = 0.0; s[2] = 0.0; s[3] = 0.0; s[4] = 0.0; s[5] = 0.0;
+    if (F.inst == 4 || fabs(rfv) > kMinVoltageD) {
         const double rff = wave_eval(F.ch[kChRfF], t);
         const double quad = wave_eval(F.ch[kChQuad], t);
         const double omega = 2.0 * kPiD * rff;
-        const double u = quad + rfv * cos(omega * t);
-        ex = -2.0 * x.template rel<double>(0, F.ox) * u / F.r0sq;
-        ey = 2.0 * x.template rel<double>(1, F.oy) * u / F.r0sq;
-    } else {
-        const double axial = wave_eval(F.ch[kChAxial], t);
-        const bool lqit = F.inst == 3;
-        if (fabs(rfv) > kMinVoltageD) {
-            const double rff = wave_eval(F.ch[kChRfF], t);
-            const double quad = wave_eval(F.ch[kChQuad], t);
-            const double omega = 2.0 * kPiD * rff;
-            const double u = quad + rfv * cos(omega * t);
-            ex = -2.0 * x.template rel<double>(0, lqit ? F.ox : 0.0) * u / F.r0sq;
-            ey = 2.0 * x.template rel<double>(1, lqit ? F.oy : 0.0) * u / F.r0sq;
-        }
-        if (lqit) {                  // AC drives, AnalyticalFieldModel.cpp:47-61, 104-121
-            if (F.ac_dipolar) {
-                for (int a = 0; a < 2; ++a) {
-                    const double amp = wave_eval(F.ch[kChAcA + 3 * a], t);
-                    if (fabs(amp) <= kMinVoltageD) continue;
-                    const double f = wave_eval(F.ch[kChAcF + 3 * a], t);
-                    const double ramp = wave_eval(F.ch[kChAcR + 3 * a], t);
-                    const double drive = amp * ramp * cos(2.0 * kPiD * f * t + F.ac_phase[a]);
-                    if (fabs(drive) > kMinVoltageD) {
-                        if (a == 0) ex += -drive / F.R;
-                        else ey += -drive / F.R;
-                    }
-                }
-            } else {
-                const double v = wave_eval(F.ch[kChAcA], t);
-                if (fabs(v) > kMinVoltageD) {
-                    const double f = wave_eval(F.ch[kChAcF], t);
-                    ex += -v / F.R * cos(2.0 * kPiD * f * t + F.ac_phase[0]);
-                }
+        s[0] = quad + rfv * cos(omega * t);
+        s[1] = 1.0;
+    }
+    if (F.inst == 4) {               // TIMS
+        s[2] = tims_ramp(F, t);
+        s[3] = 1.0;
+        return;
+    }
+    const double axial = wave_eval(F.ch[kChAxial], t);
+    if (F.inst == 0 || fabs(axial) > kMinVoltageD) {
+        s[2] = F.inst == 3 ? axial / (F.L * F.L) : axial / F.L;
+        s[3] = 1.0;
+    }
+    if (F.inst == 3) {               // LQIT AC drives, AnalyticalFieldModel.cpp:47-61, 104-121
+        if (F.ac_dipolar) {
+            for (int a = 0; a < 2; ++a) {
+                const double amp = wave_eval(F.ch[kChAcA + 3 * a], t);
+                if (fabs(amp) <= kMinVoltageD) continue;
+                const double f = wave_eval(F.ch[kChAcF + 3 * a], t);
+                const double ramp = wave_eval(F.ch[kChAcR + 3 * a], t);
+                const double drive = amp * ramp * cos(2.0 * kPiD * f * t + F.ac_phase[a]);
+                if (fabs(drive) > kMinVoltageD) s[4 + a] = -drive / F.R;
+            }
+        } else {
+            const double v = wave_eval(F.ch[kChAcA], t);
+            if (fabs(v) > kMinVoltageD) {
+                const double f = wave_eval(F.ch[kChAcF], t);
+                s[4] = -v / F.R * cos(2.0 * kPiD * f * t + F.ac_phase[0]);
             }
         }
-        if (F.inst == 0) {
-            ez = axial / F.L;
-        } else if (fabs(axial) > kMinVoltageD) {
-            if (lqit) {
-                const double alpha = axial / (F.L * F.L);
-                ez = -2.0 * alpha * (x.template rel<double>(2, F.oz) - 0.5 * F.L);
-            } else {
-                ez = axial / F.L;
-            }
-        }
+    }
+}
+
+// The field at one ion from the step's scalars s (tf_scalars).
+template <class R, class Pos>
+__device__ __forceinline__ void tf_apply(const TimeField& F, const Pos& x, const double* s, R E[3]) {
+    double ex = 0.0, ey = 0.0, ez = 0.0;
+    const bool local = F.inst >= 3;  // LQIT, TIMS: x, y from the cylinder axis
+    if (s[1] != 0.0) {
+        const double u = s[0];
+        ex = -2.0 * x.template rel<double>(0, local ? F.ox : 0.0) * u / F.r0sq;
+        ey = 2.0 * x.template rel<double>(1, local ? F.oy : 0.0) * u / F.r0sq;
+    }
+    if (F.inst == 4) {
+        const double zl = x.template rel<double>(2, F.oz);
+        const double f = s[2];
+        const double ei = tims_sample(F.tims_z, F.tims_pi, F.tims_nodes, zl, F.tims_ei);
+        const double ef = tims_sample(F.tims_z, F.tims_pf, F.tims_final_profile ? F.tims_nodes : 0, zl, F.tims_ef);
+        ez = (1.0 - f) * ei + f * ef;
+    } else if (F.inst == 3) {
+        ex += s[4];
+        ey += s[5];
+        if (s[3] != 0.0) ez = -2.0 * s[2] * (x.template rel<double>(2, F.oz) - 0.5 * F.L);
+    } else if (s[3] != 0.0) {
+        ez = s[2];
     }
     E[0] = static_cast<R>(ex); E[1] = static_cast<R>(ey); E[2] = static_cast<R>(ez);
 }
 
+#ifdef ICB_TF_TABLE_UNIT
+// Per-step scalars of the launch for the ensembles with a time-dependent
+// field (built in the FP64 unit only, without FMA contraction, for every
+// precision): block e fills rows k = 0..K of the table of chunk ensemble e
+// (global index ens_base + e; stage 0 at t_k, stage 1 at t_k + dt/2 for
+// RK4), t_k accumulated as the step kernel does (t_{k+1} = t_k + dt) into
+// tseq first, so each lane reads the values it would compute.
+__global__ void k_tf_table(const StepParams p, double* tab, double* tseq, uint32_t stride) {
+    const uint32_t e = blockIdx.x;
+    const EnsConst& C = p.ens[e];
+    if (!C.tf) return;
+    const uint32_t g = p.ens_base + e;
+    const TimeField& F = p.tfield[g];
+    const uint32_t rows = p.n_steps + 1u;
+    double* T = tab + static_cast<size_t>(g) * rows * stride;
+    double* ts = tseq + static_cast<size_t>(g) * rows;
+    if (threadIdx.x == 0) {
+        double t = p.t_dev[g];
+        for (uint32_t k = 0; k < rows; ++k) {
+            ts[k] = t;
+            t = t + C.dt;
+        }
+    }
+    __syncthreads();
+    const double hd = C.dt * 0.5;
+    for (uint32_t k = threadIdx.x; k < rows; k += blockDim.x) {
+        double* row = T + static_cast<size_t>(k) * stride;
+        const double t = ts[k];
+        double sc[kTfScalars];
+        tf_scalars(F, t, sc);
+        for (int j = 0; j < kTfScalars; ++j) row[j] = sc[j];
+        if (stride > static_cast<uint32_t>(kTfScalars)) {
+            tf_scalars(F, t + hd, sc);
+            for (int j = 0; j < kTfScalars; ++j) row[kTfScalars + j] = sc[j];
+        }
+    }
+}
+#endif
+
 // ---- fields -----------------------------------------------------------------
 template <class R, int FIELD, class Pos>
-__device__ __forceinline__ void efield(const Consts<R>& k, const Pos& x, double t, R E[3]) {
+__device__ __forceinline__ void efield(const Consts<R>& k, const Pos& x, double t, R E[3], int stage = 0) {
     if constexpr (FIELD == kFieldUniform) {
         E[0] = k.E0[0]; E[1] = k.E0[1]; E[2] = k.E0[2];
         return;
@@ -505,7 +557,9 @@ __device__ __forceinline__ void efield(const Consts<R>& k, const Pos& x, double 
         return;
     } else {
         if (k.tf != nullptr) {
-            tf_field<R>(*k.tf, x, t, E);
+            // stage 0 at t_k, 1 at t_k + dt/2 (RK4), 2 at t_k + dt = the next row
+            const double* row = k.tfrow + (stage == 0 ? 0 : stage == 1 ? kTfScalars : static_cast<int>(k.tfstride));
+            tf_apply<R>(*k.tf, x, row, E);
             return;
         } else {
 #pragma unroll
@@ -586,9 +640,10 @@ __device__ __forceinline__ R boris(const Consts<R>& k, Pos& x, R v[3], double t)
 // MagneticFieldForce.cpp:61-88; magnetic force is registered for non-Boris
 // integrators, PhysicsSetup.cpp:206).
 template <class R, int FIELD, bool MAG, class Pos>
-__device__ __forceinline__ void rk4_acc(const Consts<R>& k, const Pos& x, const R v[3], double t, R acc[3]) {
+__device__ __forceinline__ void rk4_acc(const Consts<R>& k, const Pos& x, const R v[3], double t, R acc[3],
+                                        int stage) {
     R E[3];
-    efield<R, FIELD>(k, x, t, E);
+    efield<R, FIELD>(k, x, t, E, stage);
     R F[3] = {E[0] * k.q, E[1] * k.q, E[2] * k.q};
     if constexpr (MAG) {
         const R B0 = k.tv[0], B1 = k.tv[1], B2 = k.tv[2];
@@ -612,19 +667,19 @@ __device__ __forceinline__ R rk4(const Consts<R>& k, Pos& x, R v[3], double t) {
     const Pos x0 = x;
     const R v0[3] = {v[0], v[1], v[2]};
     R k1a[3], k2a[3], k3a[3], k4a[3], v2[3], v3[3], v4[3];
-    rk4_acc<R, FIELD, MAG>(k, x0, v0, t, k1a);
+    rk4_acc<R, FIELD, MAG>(k, x0, v0, t, k1a, 0);
     Pos p2 = x0; p2.drift(v0[0], v0[1], v0[2], hd, h);
 #pragma unroll
     for (int c = 0; c < 3; ++c) v2[c] = v0[c] + k1a[c] * h;
-    rk4_acc<R, FIELD, MAG>(k, p2, v2, t + hd, k2a);
+    rk4_acc<R, FIELD, MAG>(k, p2, v2, t + hd, k2a, 1);
     Pos p3 = x0; p3.drift(v2[0], v2[1], v2[2], hd, h);
 #pragma unroll
     for (int c = 0; c < 3; ++c) v3[c] = v0[c] + k2a[c] * h;
-    rk4_acc<R, FIELD, MAG>(k, p3, v3, t + hd, k3a);
+    rk4_acc<R, FIELD, MAG>(k, p3, v3, t + hd, k3a, 1);
     Pos p4 = x0; p4.drift(v3[0], v3[1], v3[2], dt, dtr);
 #pragma unroll
     for (int c = 0; c < 3; ++c) v4[c] = v0[c] + k3a[c] * dtr;
-    rk4_acc<R, FIELD, MAG>(k, p4, v4, t + dt, k4a);
+    rk4_acc<R, FIELD, MAG>(k, p4, v4, t + dt, k4a, 2);
     R dv[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) dv[c] = v0[c] + v2[c] * R(2.0) + v3[c] * R(2.0) + v4[c];
@@ -1197,8 +1252,16 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
     Consts<R> k;
     load_consts<R, FIELD, MAG>(k, C, q, m);
     k.tf = nullptr;
+    k.tftab = nullptr;
+    k.tfrow = nullptr;
+    k.tfstride = p.tf_stride;
     if constexpr (FIELD == kFieldLinearRF) {
-        if (C.tf && p.tfield != nullptr) k.tf = p.tfield + (p.ens_base + static_cast<uint32_t>(e));
+        if (C.tf && p.tfield != nullptr && p.tf_tab != nullptr) {
+            k.tf = p.tfield + (p.ens_base + static_cast<uint32_t>(e));
+            k.tftab = p.tf_tab + static_cast<size_t>(p.ens_base + static_cast<uint32_t>(e)) * (p.n_steps + 1u) *
+                                     p.tf_stride;
+            k.tfrow = k.tftab;
+        }
     }
     if constexpr (COLL == kCollLangevin) {
         // speed-independent capture rate nu_i: event probability per step
@@ -1454,7 +1517,10 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
         if (do_push) {
             R l1;
             double tn = 0.0;   // only a time-dependent field reads the clock
-            if constexpr (FIELD == kFieldLinearRF) tn = t_step();
+            if constexpr (FIELD == kFieldLinearRF) {
+                tn = t_step();
+                if (k.tf != nullptr) k.tfrow = k.tftab + static_cast<size_t>(kk) * k.tfstride;
+            }
             if (INTEG == kBoris) l1 = boris<R, FIELD, MAG>(k, x, v, tn);
             else l1 = rk4<R, FIELD, MAG>(k, x, v, tn);
             acc += l1 * dt_r;
