@@ -709,6 +709,11 @@ int rebuild_time_fields(icb_handle* h) {
                     F.tims_z[i] = T.z_positions_m[i];
                     F.tims_pi[i] = T.initial_profile_V_m[i];
                     F.tims_pf[i] = T.final_profile_V_m[i];
+                    F.tims_zf[i] = static_cast<float>(T.z_positions_m[i]);
+                    F.tims_pif[i] = static_cast<float>(T.initial_profile_V_m[i]);
+                    F.tims_pff[i] = static_cast<float>(T.final_profile_V_m[i]);
+                    const double dz = i + 1 < T.n_nodes ? T.z_positions_m[i + 1] - T.z_positions_m[i] : 0.0;
+                    F.tims_idz[i] = dz > 0.0 ? static_cast<float>(1.0 / dz) : 0.0f;
                 }
             }
             base = tf_bound(C, P, F, wb);
@@ -735,7 +740,9 @@ int rebuild_time_fields(icb_handle* h) {
 
 inline unsigned grid_for(uint64_t n, int block) { return static_cast<unsigned>((n + block - 1) / block); }
 
-uint32_t tf_stride(const icb_handle* h) { return h->cfg.integrator == ICB_INTEGRATOR_RK4 ? 12u : 6u; }
+uint32_t tf_stride(const icb_handle* h) {
+    return static_cast<uint32_t>(kTfRowScalars * (h->cfg.integrator == ICB_INTEGRATOR_RK4 ? 2 : 1));
+}
 
 // Room for the per-step field tables of launches of up to K steps (all
 // ensembles, plus the time sequences); allocates outside stream capture only.

@@ -85,6 +85,7 @@ struct MixConst {
 // (ValueOrWaveform) and the TIMS axial ramp, evaluated in FP64 at every
 // field evaluation.  Lives in device memory, one per ensemble (global index).
 constexpr int kMaxWavePoints = 64;
+constexpr int kTfRowScalars = 8;     // doubles per step and stage of the per-step field table
 enum WaveKind : int32_t {
     kWaveConstant = 0, kWaveLinear = 1, kWaveQuadratic = 2, kWaveExponential = 3,
     kWaveSinusoidal = 4, kWavePWM = 5, kWavePulsed = 6, kWaveArbitrary = 7
@@ -110,6 +111,8 @@ struct TimeField {
     double ac_phase[2];
     double tims_t0, tims_t1, tims_tau, tims_ei, tims_ef;
     double tims_z[kMaxWavePoints], tims_pi[kMaxWavePoints], tims_pf[kMaxWavePoints];
+    // float copies for the float forms: nodes, profiles, 1 / (z[i+1] - z[i])
+    float tims_zf[kMaxWavePoints], tims_pif[kMaxWavePoints], tims_pff[kMaxWavePoints], tims_idz[kMaxWavePoints];
     WaveConst ch[kNumChannels];
 };
 

@@ -439,16 +439,19 @@ __device__ __forceinline__ double tims_sample(const double* zn, const double* va
 //   s[0] U = dc_quad + V cos(2 pi f t)      s[1] 1 if the RF term applies
 //   s[2] IMS / QuadrupoleRF axial / L, LQIT axial / L^2, TIMS ramp f(t)
 //   s[3] 1 if the axial term applies        s[4], s[5] AC drive E_x, E_y
-constexpr int kTfScalars = 6;
+//   s[6], s[7] -2 U / r0^2, 2 U / r0^2 (the float forms' coefficients)
+constexpr int kTfScalars = kTfRowScalars;
 static __device__ __noinline__ void tf_scalars(const TimeField& F, double t, double s[kTfScalars]) {
     const double rfv = wave_eval(F.ch[kChRfV], t);
-    s[0] = 0.0; s[1] = 0.0; s[2] = 0.0; s[3] = 0.0; s[4] = 0.0; s[5] = 0.0;
+    for (int j = 0; j < kTfScalars; ++j) s[j] = 0.0;
     if (F.inst == 4 || fabs(rfv) > kMinVoltageD) {
         const double rff = wave_eval(F.ch[kChRfF], t);
         const double quad = wave_eval(F.ch[kChQuad], t);
         const double omega = 2.0 * kPiD * rff;
         s[0] = quad + rfv * cos(omega * t);
         s[1] = 1.0;
+        s[6] = -2.0 * s[0] / F.r0sq;
+        s[7] = 2.0 * s[0] / F.r0sq;
     }
     if (F.inst == 4) {               // TIMS
         s[2] = tims_ramp(F, t);
@@ -480,9 +483,53 @@ static __device__ __noinline__ void tf_scalars(const TimeField& F, double t, dou
     }
 }
 
-// The field at one ion from the step's scalars s (tf_scalars).
+// Float piecewise-linear profile (the float forms): reciprocal interval
+// widths instead of the division.
+__device__ __forceinline__ float tims_sample_f(const float* zn, const float* val, const float* idz, int n, float z,
+                                               float uni) {
+    if (n == 0) return uni;
+    if (!(z > zn[0])) return val[0];
+    if (z >= zn[n - 1]) return val[n - 1];
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (zn[mid] < z) lo = mid + 1; else hi = mid;
+    }
+    const int i0 = lo - 1;
+    const float alpha = (z - zn[i0]) * idz[i0];
+    return fmaf(alpha, val[lo] - val[i0], val[i0]);
+}
+
+// The field at one ion from the step's scalars s (tf_scalars): FP64 in the
+// reference's operation order; the float forms in float from the per-step
+// coefficients.
 template <class R, class Pos>
 __device__ __forceinline__ void tf_apply(const TimeField& F, const Pos& x, const double* s, R E[3]) {
+    if constexpr (sizeof(R) == 4) {
+        const bool local = F.inst >= 3;
+        float ex = 0.0f, ey = 0.0f, ez = 0.0f;
+        if (s[1] != 0.0) {
+            ex = x.template rel<float>(0, local ? F.ox : 0.0) * static_cast<float>(s[6]);
+            ey = x.template rel<float>(1, local ? F.oy : 0.0) * static_cast<float>(s[7]);
+        }
+        if (F.inst == 4) {
+            const float zl = x.template rel<float>(2, F.oz);
+            const float f = static_cast<float>(s[2]);
+            const float ei = tims_sample_f(F.tims_zf, F.tims_pif, F.tims_idz, F.tims_nodes, zl,
+                                           static_cast<float>(F.tims_ei));
+            const float ef = tims_sample_f(F.tims_zf, F.tims_pff, F.tims_idz, F.tims_final_profile ? F.tims_nodes : 0,
+                                           zl, static_cast<float>(F.tims_ef));
+            ez = fmaf(f, ef - ei, ei);
+        } else if (F.inst == 3) {
+            ex += static_cast<float>(s[4]);
+            ey += static_cast<float>(s[5]);
+            if (s[3] != 0.0) ez = static_cast<float>(-2.0 * s[2]) * x.template rel<float>(2, F.oz + 0.5 * F.L);
+        } else if (s[3] != 0.0) {
+            ez = static_cast<float>(s[2]);
+        }
+        E[0] = ex; E[1] = ey; E[2] = ez;
+        return;
+    }
     double ex = 0.0, ey = 0.0, ez = 0.0;
     const bool local = F.inst >= 3;  // LQIT, TIMS: x, y from the cylinder axis
     if (s[1] != 0.0) {
