@@ -12,8 +12,12 @@
  *                                 SimulationEngineLifecycle.cpp:72-195
  *   - Boris push with x += v_plus*dt     BorisStrategy.cpp:18-98
  *   - RK4 batch                          RK4Strategy.cpp:181-361
- *   - analytic E of IMS / FTICR / QuadrupoleRF
- *                                        AnalyticalFieldModel.cpp:136-248
+ *   - analytic E of IMS / FTICR / QuadrupoleRF / LQIT
+ *                                        AnalyticalFieldModel.cpp:81-248
+ *   - voltages given as waveforms (all eight types), evaluated per field
+ *     call                               WaveformConfig.h:33-188,
+ *                                        WaveformConfig.cpp:10-91
+ *   - the TIMS axial field model         TIMSAxialFieldModel.h:30-148
  *   - magnetic force for RK4             MagneticFieldForce.cpp:61-118
  *   - cylinder containment (eps 1e-12)   CylindricalGeometry.h:35-40
  *   - reference HSS: full Maxwell-Boltzmann neutral every step, P=1-exp,
