@@ -250,6 +250,7 @@ struct icb_handle {
     uint32_t K = 1000;
     uint32_t pend = 0;      // 0 = precision default (set at create)
     uint32_t spv = 8;       // collision-free steps between warp votes
+    bool shape_tuned = false;  // block / pend / spv chosen by icb_autotune
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -727,9 +728,10 @@ int rebuild_time_fields(icb_handle* h) {
             C.Emax = base;
         }
     }
-    if (any != h->any_tf) {
-        // launch shape of the time-dependent instance where the caller gave
-        // none (autotuner optimum on the TIMS workload: +10 %)
+    if (any != h->any_tf && !h->shape_tuned) {
+        // launch shape of the time-dependent instance where neither the
+        // caller nor icb_autotune chose one (autotuner optimum on the TIMS
+        // workload: +10 %)
         if (h->cfg.block_size <= 0) h->block = any ? 64 : 128;
         if (h->cfg.pending_threshold <= 0) h->pend = any ? 6u : 10u;
         if (h->cfg.steps_per_vote <= 0) h->spv = any ? 4u : 8u;
@@ -761,7 +763,13 @@ int ensure_tf_tab(icb_handle* h, uint32_t K, cudaStream_t st) {
     ICB_CUDA(cudaStreamIsCapturing(st, &cs));
     if (cs != cudaStreamCaptureStatusNone)
         return fail(ICB_ERR_STATE, "field table too small inside a stream capture");
-    ICB_CUDA(cudaDeviceSynchronize());
+    // the old table may still be read by this handle's queued work: wait
+    // for the handle's own streams only (not the whole device)
+    ICB_CUDA(cudaStreamSynchronize(st));
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->copy_stream) ICB_CUDA(cudaStreamSynchronize(h->copy_stream));
+    if (h->copy_back_stream) ICB_CUDA(cudaStreamSynchronize(h->copy_back_stream));
+    for (cudaStream_t cs2 : h->chunk_streams) ICB_CUDA(cudaStreamSynchronize(cs2));
     ICB_CUDA(h->tf_tab.alloc(need));
     h->drop_graph();
     return ICB_OK;
@@ -1687,7 +1695,7 @@ int icb_autotune(icb_handle* h, uint64_t trial_steps, icb_tuning* out) {
         }
     }
     // Back to the saved state with the chosen shape (or the old one on error).
-    if (rc == ICB_OK) { h->block = best_blk; h->spv = best_spv; h->pend = best_pend; }
+    if (rc == ICB_OK) { h->block = best_blk; h->spv = best_spv; h->pend = best_pend; h->shape_tuned = true; }
     else { h->block = blk0; h->spv = spv0; h->pend = pend0; }
     ICB_CUDA(copy_all(false));
     ICB_CUDA(cudaStreamSynchronize(s));

@@ -18,6 +18,12 @@
 //    serialised by the caller;
 //  * the scratch keeps the last call's contents.  Nothing in it has to
 //    start at zero: each call writes every partial-sum slot it later reads.
+//
+// The caller's current device is the same after the call as before it.  The
+// scratch array's device address is looked up once per device context (the
+// first call on a device, and the first call after that device has been
+// reset, since a reset reloads this library's device code at a new
+// address); make that first call before any stream capture.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -33,9 +39,61 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxItems * ICB_N_MOMENTS];
 
-// Device address of the scratch per device, looked up once per device.
+// Device address of the scratch per device, with the unique id of the
+// context it was looked up in (0 = not yet looked up).
 double* g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
 std::mutex g_scratch_mutex;
+
+// The driver's context queries, reached through the runtime so that the
+// library does not link the driver library itself.
+using CtxGetCurrentFn = int (*)(void** ctx);
+using CtxGetIdFn = int (*)(void* ctx, unsigned long long* id);
+
+// Unique id of the calling thread's current context, or 0 when it cannot be
+// had (the caller then looks the address up on every call).
+unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+    });
+    if (!get_current || !get_id) return 0;
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Makes `device` current for the lifetime of the guard and gives the
+// caller's current device back on every return path.
+class DeviceGuard {
+  public:
+    explicit DeviceGuard(int device) {
+        ok_ = cudaGetDevice(&saved_) == cudaSuccess;
+        if (ok_ && saved_ != device) ok_ = cudaSetDevice(device) == cudaSuccess;
+        else if (!ok_) saved_ = -1;
+        if (!ok_) cudaGetLastError();
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (saved_ >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != saved_) cudaSetDevice(saved_);
+    }
+    bool ok() const { return ok_; }
+
+  private:
+    int saved_ = -1;
+    bool ok_ = false;
+};
 
 // One block per work item: a fixed-order block reduction of the item's ions
 // into partials[item] (slots as ICB_N_MOMENTS).
@@ -115,18 +173,22 @@ extern "C" int icb_moments_noalloc(int device, uint64_t n, const double* x, cons
     if (items > static_cast<uint64_t>(kNoAllocMaxItems))
         return set_error(ICB_ERR_INVALID_ARGUMENT,
                          "icb_moments_noalloc: at most 33554432 ions (the fixed 640 KB scratch holds 4096 partial sums)");
-    if (cudaSetDevice(device) != cudaSuccess) return set_error(ICB_ERR_NO_DEVICE, "cudaSetDevice failed");
+    DeviceGuard guard(device);
+    if (!guard.ok()) return set_error(ICB_ERR_NO_DEVICE, "cudaSetDevice failed");
     double* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_scratch_mutex);
-        if (!g_scratch_addr[device]) {
-            // First call on this device: resolve the scratch array's device
-            // address with the device current.  Make this first call before
-            // any stream capture.
+        const unsigned long long ctx = current_context_id();
+        if (!g_scratch_addr[device] || ctx == 0 || ctx != g_scratch_ctx[device]) {
+            // First call in this device's context: resolve the scratch
+            // array's device address with the device current.
             void* ptr = nullptr;
-            if (cudaGetSymbolAddress(&ptr, g_noalloc_partials) != cudaSuccess || !ptr)
+            if (cudaGetSymbolAddress(&ptr, g_noalloc_partials) != cudaSuccess || !ptr) {
+                g_scratch_addr[device] = nullptr;
                 return set_error(ICB_ERR_CUDA, "cudaGetSymbolAddress of the moments scratch failed");
+            }
             g_scratch_addr[device] = static_cast<double*>(ptr);
+            g_scratch_ctx[device] = ctx;
         }
         scratch = g_scratch_addr[device];
     }

@@ -521,10 +521,11 @@ int icb_autotune(struct icb_handle* h, uint64_t trial_steps, icb_tuning* out);
  * slots 11/12 are 0) into `out` (device, ICB_N_MOMENTS doubles), launched on
  * `cuda_stream` (NULL = default stream).  Allocates nothing: partial sums go
  * to a 640 KB file-scope device array, so n <= 33,554,432 ions (larger n is
- * rejected with ICB_ERR_INVALID_ARGUMENT).  The first call on a device
- * resolves that array's address and should come before any stream capture.
- * All calls on a device share the array: calls that overlap on the GPU race
- * and must be serialised by the caller. */
+ * rejected with ICB_ERR_INVALID_ARGUMENT).  The first call on a device (and
+ * the first after that device is reset) resolves that array's address and
+ * should come before any stream capture.  The caller's current device is
+ * unchanged on return.  All calls on a device share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
 int icb_moments_noalloc(int device, uint64_t n, const double* x, const double* y, const double* z,
                         const double* vx, const double* vy, const double* vz,
                         const double* x_ref, const double* y_ref, const double* z_ref,

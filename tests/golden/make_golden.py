@@ -1,6 +1,6 @@
 """Generate the golden fixtures of tests/golden/ from the reference's own code.
 
-    make -C oracle && python tests/golden/make_golden.py [--quick]
+    make -C oracle REF=<reference tree> && python tests/golden/make_golden.py [--quick]
 
 Every fixture is produced by ``oracle/_ref/ref_harness`` — the reference's
 hot-path sources (BorisStrategy, RK4Strategy, HSSCollisionHandler,
@@ -172,7 +172,7 @@ def save(name: str, **arrays) -> None:
 
 def main(quick: bool, only: set[str] | None = None) -> None:
     if not orc.have_harness():
-        raise SystemExit("oracle/_ref/ref_harness missing: run `make -C oracle` with the reference tree present")
+        raise SystemExit("oracle/_ref/ref_harness missing: run `make -C oracle REF=<reference tree>`")
 
     if only:
         if "field_timed" in only:

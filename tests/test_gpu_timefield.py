@@ -181,3 +181,76 @@ def test_time_field_argument_checks(golden):
         with pytest.raises(IcbError):
             sim.set_tims_field(0, f)
         sim.set_tims_field(0, None)
+
+
+TIMS_HSS = dict(instrument="TIMS", origin_z=-0.01, length=0.02, radius=0.005, T=300, P=300.0, gas="N2",
+                rf_V=180.0, rf_f=2.0e6, tims=1, tims_z="0,0.008,0.02", tims_pi="0,-800,-1500",
+                tims_pf="0,-200,-300", tims_t0=5e-7, tims_t1=2.5e-6, wave_rff="4|0|0|2e6,1e5,3e5,0")
+
+
+def _time_field_case(case: str, golden):
+    """(ensemble, harness keys, initial state, integrator, collision model)
+    of a time-dependent field case: the TIMS ramp with HSS collisions
+    (Boris), or a golden LQIT push with a waveform-scanned AC drive (RK4,
+    which reads the per-step field table at half steps too)."""
+    if case == "tims_hss":
+        e = cfg.ensemble_params(domain_json(TIMS_HSS), 150e-20, 1e-9)
+        st0 = config0_ions(2000)
+        st0.x *= 0.2; st0.y *= 0.2; st0.z *= 0.2
+        return e, TIMS_HSS, st0, capi.INTEGRATOR_BORIS, capi.COLLISION_HSS
+    z = golden(f"push_{case}.npz")
+    integ = capi.INTEGRATOR_BORIS if str(z["integrator"]) == "boris" else capi.INTEGRATOR_RK4
+    return ensemble_from_golden(z), json.loads(str(z["domain"])), golden_state(z), integ, capi.COLLISION_NONE
+
+
+def _same_state(a, b) -> None:
+    for k in ("x", "y", "z", "vx", "vy", "vz", "active"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+
+
+@pytest.mark.parametrize("case", ["tims_hss", "rk4_lqit1_ac", "boris_lqit_ac"])
+def test_fp64_time_field_host_path_equals_separate_calls(golden, case):
+    """icb_advance_host (4 overlapped ion chunks; the per-step field table
+    built once on the copy stream for every chunk) gives the state of
+    icb_update_state + icb_advance + icb_download_ions bit for bit, call
+    after call."""
+    e, kw, st0, integ, coll = _time_field_case(case, golden)
+    args = dict(precision=capi.PREC_FP64, integrator=integ, collision=coll, rng_seed=123, steps_per_launch=128)
+    with Simulation([e], **args) as sim:
+        apply_time_field(sim, kw)
+        sim.upload(st0)
+        host = st0.copy()
+        host.t_death = host.t_arrival = None
+        for _ in range(3):
+            sim.advance_host(host, 300, n_chunks=4)
+        c_host = sim.clock()
+    with Simulation([e], **args) as sim:
+        apply_time_field(sim, kw)
+        sim.upload(st0)
+        sep = st0.copy()
+        for _ in range(3):
+            sim.update_state(sep)
+            sim.advance(300)
+            sep = sim.download(sep)
+        c_sep = sim.clock()
+    _same_state(host, sep)
+    assert c_host[0] == c_sep[0] == 900 and np.array_equal(c_host[1], c_sep[1])
+
+
+@pytest.mark.parametrize("case", ["tims_hss", "rk4_lqit1_ac"])
+def test_fp64_time_field_graph_replay_equals_direct_launches(golden, case):
+    """use_graphs = 1 (the field table rebuilt inside each captured launch
+    sequence, replayed for repeated step counts, recaptured when the count
+    changes) gives the direct-launch result bit for bit."""
+    e, kw, st0, integ, coll = _time_field_case(case, golden)
+    outs = []
+    for graphs in (0, 1):
+        with Simulation([e], precision=capi.PREC_FP64, integrator=integ, collision=coll, rng_seed=123,
+                        steps_per_launch=128, use_graphs=graphs) as sim:
+            apply_time_field(sim, kw)
+            sim.upload(st0)
+            stats = [sim.advance(k) for k in (300, 300, 125, 300)]
+            outs.append((sim.download(), sim.clock(), [s["collisions"] for s in stats]))
+    _same_state(outs[0][0], outs[1][0])
+    assert outs[0][1][0] == outs[1][1][0] == 1025 and np.array_equal(outs[0][1][1], outs[1][1][1])
+    assert outs[0][2] == outs[1][2]
