@@ -132,7 +132,8 @@ class IpmPotential(C.Structure):
 
 class IpmConfig(C.Structure):
     _fields_ = [("potential", IpmPotential), ("b_max_m", C.c_double), ("E_min_J", C.c_double),
-                ("E_max_J", C.c_double), ("n_E", C.c_int32), ("n_b", C.c_int32), ("reserved", C.c_int32 * 6)]
+                ("E_max_J", C.c_double), ("n_E", C.c_int32), ("n_b", C.c_int32), ("net_E_min_J", C.c_double),
+                ("net_E_max_J", C.c_double), ("reserved", C.c_int32 * 2)]
 
 
 class MlpTrainConfig(C.Structure):

@@ -298,6 +298,7 @@ struct icb_handle {
     DevBuf<float> ipm_tab;
     int ipm_nE = 0, ipm_nb = 0;
     double ipm_lnEmin = 0.0, ipm_inv_dlnE = 0.0, ipm_bmax = 0.0, ipm_Emin = 0.0, ipm_Emax = 0.0;
+    double ipm_net_lnEmin = 0.0, ipm_net_scale = 0.0;   // x0 = (ln E - lnEmin) scale - 1
     DevBuf<uint32_t> mlp_w2;
     DevBuf<float> mlp_f;
     DevBuf<MixConst> mix;              // HSS gas mixtures, per ensemble
@@ -847,6 +848,8 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.ipm_nb = h->ipm_nb;
         p.ipm_lnEmin = h->ipm_lnEmin;
         p.ipm_inv_dlnE = h->ipm_inv_dlnE;
+        p.ipm_net_lnEmin = h->ipm_net_lnEmin;
+        p.ipm_net_scale = h->ipm_net_scale;
         p.mlp_w2 = h->mlp_w2.p;
         p.mlp_f = h->mlp_f.p;
         p.mix = h->mix.p;
@@ -1472,6 +1475,11 @@ int icb_ipm_configure(icb_handle* h, const icb_ipm_config* cfg) {
         return fail(ICB_ERR_INVALID_ARGUMENT, "IPM table needs 2 <= n_E, n_b <= 16384");
     if (!(cfg->E_min_J > 0.0) || !(cfg->E_max_J > cfg->E_min_J) || !(cfg->b_max_m > 0.0))
         return fail(ICB_ERR_INVALID_ARGUMENT, "IPM table needs 0 < E_min < E_max and b_max > 0");
+    const bool net_default = cfg->net_E_min_J == 0.0 && cfg->net_E_max_J == 0.0;
+    const double net_lo = net_default ? cfg->E_min_J : cfg->net_E_min_J;
+    const double net_hi = net_default ? cfg->E_max_J : cfg->net_E_max_J;
+    if (!(net_lo > 0.0) || !(net_hi > net_lo))
+        return fail(ICB_ERR_INVALID_ARGUMENT, "IPM network range needs 0 < net_E_min < net_E_max");
     for (const auto& e : h->ens)
         if (std::fabs(e.ipm_bmax_m - cfg->b_max_m) > 1e-12 * cfg->b_max_m)
             return fail(ICB_ERR_INVALID_ARGUMENT, "b_max_m must equal every ensemble's ipm_bmax_m");
@@ -1493,6 +1501,8 @@ int icb_ipm_configure(icb_handle* h, const icb_ipm_config* cfg) {
     h->ipm_bmax = cfg->b_max_m;
     h->ipm_Emin = cfg->E_min_J;
     h->ipm_Emax = cfg->E_max_J;
+    h->ipm_net_lnEmin = std::log(net_lo);
+    h->ipm_net_scale = 2.0 / (std::log(net_hi) - h->ipm_net_lnEmin);
     ++h->gen;
     return ICB_OK;
 }

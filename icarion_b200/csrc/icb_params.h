@@ -151,6 +151,9 @@ struct StepParams {
     const float* ipm_tab;
     int32_t ipm_nE, ipm_nb;
     double ipm_lnEmin, ipm_inv_dlnE;
+    // learned deflection input: x0 = (ln E - net_lnEmin) net_scale - 1,
+    // inside the trained range when |x0| <= 1
+    double ipm_net_lnEmin, ipm_net_scale;
     // learned deflection (MLP 2-64-64-1): packed BF16 weights and FP32
     // biases (nullable unless the MLP model is selected)
     const uint32_t* mlp_w2;            // W2 as mma B fragments

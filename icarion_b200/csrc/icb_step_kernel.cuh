@@ -1527,13 +1527,13 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
             // evaluation of the deflection network; energies outside
             // the trained range use the table
             if (__any_sync(0xffffffffu, need_net)) {
-                R tt = R(0);
+                R xr = R(0);
                 bool in_dom = false;
                 if (need_net) {
-                    tt = (m_log(ip.E) - static_cast<R>(p.ipm_lnEmin)) * static_cast<R>(p.ipm_inv_dlnE);
-                    in_dom = tt >= R(0) && tt <= static_cast<R>(p.ipm_nE - 1);
+                    xr = (m_log(ip.E) - static_cast<R>(p.ipm_net_lnEmin)) * static_cast<R>(p.ipm_net_scale) - R(1);
+                    in_dom = xr >= R(-1) && xr <= R(1);
                 }
-                const float x0 = static_cast<float>(R(2) * tt / static_cast<R>(p.ipm_nE - 1) - R(1));
+                const float x0 = static_cast<float>(xr);
                 const float x1 = static_cast<float>(R(2) * ip.bn - R(1));
                 const float y = mlp_warp_eval(p.mlp_w2, p.mlp_f, x0, x1, need_net && in_dom);
                 if (need_net) {

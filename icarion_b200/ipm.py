@@ -6,8 +6,12 @@ Default potential: the reference's LJ1264 form (interaction_potential_
 precompute.cpp:1386-1508) for an ion in N2 with a 12-6 well of 5 meV at
 r_m = 4 A plus the induced-dipole term of the N2 polarisability 1.74 A^3
 (utils/constants.h:54) for a singly charged ion; ion mass 300 Da.  The
-collision event cross-section is pi b_max^2 with b_max = 12 A; the table
-and the network cover centre-of-mass energies 1 meV - 10 eV.
+collision event cross-section is pi b_max^2 with b_max = 12 A.  The network
+is trained on centre-of-mass energies 1 meV - 10 eV (E_min_J .. E_max_J);
+the table covers 0.01 meV - 10 eV (table_E_min_J .. E_max_J), so that the
+slowest thermal encounters (about 0.6 % of collisions at 300 K fall below
+1 meV) are deflected at their own energy, and serves the network outside
+its range.
 """
 from __future__ import annotations
 
@@ -30,9 +34,10 @@ class IpmSetup:
     polarizability_m3: float = 1.74e-30
     charge_C: float = cfg.ELEM_CHARGE_C
     b_max_m: float = 12e-10
-    E_min_J: float = 1e-3 * EV_J
+    E_min_J: float = 1e-3 * EV_J          # trained range of the network
     E_max_J: float = 10.0 * EV_J
-    n_E: int = 512
+    table_E_min_J: float = 1e-5 * EV_J    # table range: table_E_min_J .. E_max_J
+    n_E: int = 640
     n_b: int = 256
 
     def potential(self) -> capi.IpmPotential:
@@ -47,11 +52,23 @@ class IpmSetup:
         c = capi.IpmConfig()
         c.potential = self.potential()
         c.b_max_m = self.b_max_m
-        c.E_min_J = self.E_min_J
+        c.E_min_J = self.table_E_min_J
         c.E_max_J = self.E_max_J
         c.n_E = self.n_E
         c.n_b = self.n_b
+        c.net_E_min_J = self.E_min_J
+        c.net_E_max_J = self.E_max_J
         return c
+
+    def table_grid(self) -> tuple[np.ndarray, np.ndarray]:
+        """(E [n_E], b [n_b]) nodes of the handle's cos(chi) table."""
+        lnE = np.linspace(math.log(self.table_E_min_J), math.log(self.E_max_J), self.n_E)
+        return np.exp(lnE), np.linspace(0.0, self.b_max_m, self.n_b)
+
+    def table_scale(self) -> tuple[float, float]:
+        """(ln E_min, (n_E - 1) / ln(E_max / E_min)) of the table."""
+        lo = math.log(self.table_E_min_J)
+        return lo, (self.n_E - 1) / (math.log(self.E_max_J) - lo)
 
     def coefficients(self) -> tuple[float, float, float]:
         """(c12, c6, c4) of V = c12/r^12 - c6/r^6 - c4/r^4."""

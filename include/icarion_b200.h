@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define ICB_ABI_VERSION 8
+#define ICB_ABI_VERSION 9
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -366,11 +366,14 @@ typedef struct icb_ipm_config {
     double b_max_m;            /* must equal every ensemble's ipm_bmax_m */
     double E_min_J, E_max_J;   /* table range (log-spaced); energies outside are clamped */
     int32_t n_E, n_b;          /* table size (>= 2 each) */
-    int32_t reserved[6];
+    /* trained range of the learned deflection (its input normalisation);
+     * 0, 0 = the table range */
+    double net_E_min_J, net_E_max_J;
+    int32_t reserved[2];
 } icb_ipm_config;
 /* Build the cos(chi) table of the handle on its device (collision models
  * ICB_COLLISION_IPM_TABLE and ICB_COLLISION_IPM_MLP need it; the learned
- * model falls back to it outside [E_min, E_max]). */
+ * model falls back to it outside [net_E_min, net_E_max]). */
 int icb_ipm_configure(struct icb_handle* h, const icb_ipm_config* cfg);
 /* Copy the table (n_E * n_b floats, row-major [E][b]) to the host. */
 int icb_ipm_table(struct icb_handle* h, float* out);
@@ -378,7 +381,8 @@ int icb_ipm_table(struct icb_handle* h, float* out);
 /* ---- learned deflection (MLP 2 -> 64 -> 64 -> 1, tanh) ------------------
  * No counterpart in the reference: a network trained on the quadrature's
  * cos(chi) replaces the table lookup in the collision path.  Inputs
- * x0 = 2 (ln E - ln E_min) / (ln E_max - ln E_min) - 1, x1 = 2 b / b_max - 1;
+ * x0 = 2 (ln E - ln net_E_min) / (ln net_E_max - ln net_E_min) - 1,
+ * x1 = 2 b / b_max - 1;
  * output cos(chi).  Parameters (ICB_MLP_N_PARAMS floats, in order):
  * W1[64][2], b1[64], W2[64][64], b2[64], W3[64], b3.  In the collision path
  * the weights are BF16 and the 64x64 layer runs on the tensor cores

@@ -1482,3 +1482,122 @@ void orc_ehss_scatter_many(int64_t n, const double* v_ion, const double* v_n, do
         out[3 * i + 2] = v[2];
     }
 }
+
+/* ---- interaction potential: classical deflection by quadrature ---------
+ * CPU restatement of the library's device quadrature (the same steps):
+ *   chi = pi - 2 (b / r0) int_0^1 2 s ds / sqrt(F(r0 / (1 - s^2))),
+ *   F(r) = 1 - b^2/r^2 - V(r)/E,  V = c12/r^12 - c6/r^6 - c4/r^4,
+ * r0 the outermost zero of F: stepped inwards by 2 % from 4 (b + sigma),
+ * then bisected; 64-point Gauss-Legendre on [0, 1].  Used to build cos(chi)
+ * tables and the reference-format momentum-transfer sample sets on the CPU.
+ * Returns cos(chi); chi itself through chi_out when non-NULL. */
+#define ORC_GL 64
+static double g_gl_s[ORC_GL], g_gl_w[ORC_GL];
+static int g_gl_ready = 0;
+
+static void orc_gl_init(void) {
+    if (g_gl_ready) return;
+#pragma omp critical(orc_gl)
+    {
+        if (!g_gl_ready) {
+            const int n = ORC_GL;
+            for (int i = 0; i < n; ++i) {
+                double x = cos(M_PI * (i + 0.75) / (n + 0.5));
+                double dp = 0.0;
+                for (int it = 0; it < 100; ++it) {
+                    double p0 = 1.0, p1 = x;
+                    for (int k = 2; k <= n; ++k) {
+                        const double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+                        p0 = p1;
+                        p1 = p2;
+                    }
+                    dp = n * (x * p1 - p0) / (x * x - 1.0);
+                    const double dx = p1 / dp;
+                    x -= dx;
+                    if (fabs(dx) < 1e-16) break;
+                }
+                g_gl_s[i] = 0.5 * (x + 1.0);
+                g_gl_w[i] = 0.5 * (2.0 / ((1.0 - x * x) * dp * dp));
+            }
+            g_gl_ready = 1;
+        }
+    }
+}
+
+static double ipm_F(double c12, double c6, double c4, double E, double b, double r) {
+    const double ir2 = 1.0 / (r * r);
+    const double ir4 = ir2 * ir2, ir6 = ir4 * ir2, ir12 = ir6 * ir6;
+    const double V = c12 * ir12 - c6 * ir6 - c4 * ir4;
+    return 1.0 - b * b * ir2 - V / E;
+}
+
+double orc_ipm_chi_quad(double c12, double c6, double c4, double sigma, double E, double b) {
+    orc_gl_init();
+    if (!(E > 0.0)) return 0.0;
+    double r = 4.0 * (b + sigma);
+    int it = 0;
+    while (ipm_F(c12, c6, c4, E, b, r * 0.98) > 0.0 && it < 4000) {
+        r *= 0.98;
+        ++it;
+    }
+    double lo = r * 0.98, hi = r;
+    for (int k = 0; k < 200 && hi - lo > 1e-15 * hi; ++k) {
+        const double mid = 0.5 * (lo + hi);
+        if (ipm_F(c12, c6, c4, E, b, mid) > 0.0) hi = mid; else lo = mid;
+    }
+    const double r0 = hi;
+    double I = 0.0;
+    for (int k = 0; k < ORC_GL; ++k) {
+        const double s = g_gl_s[k];
+        const double u = 1.0 - s * s;
+        const double F = fmax(ipm_F(c12, c6, c4, E, b, r0 / u), 1e-300);
+        I += g_gl_w[k] * 2.0 * s / sqrt(F);
+    }
+    return M_PI - 2.0 * (b / r0) * I;
+}
+
+/* cos(chi) of n (E, b) pairs (OpenMP over pairs). */
+void orc_ipm_cos_chi_many(int64_t n, double c12, double c6, double c4, double sigma, const double* E,
+                          const double* b, double* out) {
+    orc_gl_init();
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < n; ++i) out[i] = cos(orc_ipm_chi_quad(c12, c6, c4, sigma, E[i], b[i]));
+}
+
+/* The reference's per-cell momentum-transfer samples
+ * (interaction_potential_precompute.cpp:2692-2880, store_full_cdf) for one
+ * isotropic site and a fixed b_max, n_cells relative speeds g[c]: per cell
+ * n_trials impact points uniform over the disk of radius b_max (b = b_max
+ * sqrt(w), phi = 2 pi u), the deflection chi(E = mu g^2 / 2, b) by the
+ * quadrature above, and the centre-of-mass momentum change dp = mu (v_out -
+ * v0) in the frame with v0 along +z: v_out = g (sin chi cos phi,
+ * sin chi sin phi, cos chi) (chi > 0 deflects away from the scattering
+ * centre, i.e. along the impact offset).  The tool draws w and u as
+ * independent uniforms (mt19937_64 per cell); stratified = 1 takes w from
+ * the t-th of n_trials equal-area annuli instead (w = (t + u') / n_trials),
+ * the same uniform-area law without the Monte Carlo noise of the cell's
+ * momentum-transfer mean.  dp: 3 n_trials doubles per cell, cells in order
+ * (OpenMP over cells). */
+void orc_ipm_sample_cells(int64_t n_cells, const double* g, double c12, double c6, double c4, double sigma,
+                          double mu, double b_max, int64_t n_trials, uint64_t seed, int stratified, double* dp) {
+    orc_gl_init();
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t c = 0; c < n_cells; ++c) {
+        orc_mt64 rng;
+        mt64_seed(&rng, seed * 1000003ull + (uint64_t)c);
+        const double E = 0.5 * mu * g[c] * g[c];
+        double* out = dp + 3 * n_trials * c;
+        for (int64_t t = 0; t < n_trials; ++t) {
+            const double u1 = mt64_uniform01(&rng);
+            const double u2 = mt64_uniform01(&rng);
+            const double w = stratified ? ((double)t + u1) / (double)n_trials : u1;
+            const double b = b_max * sqrt(w);
+            const double phi = 2.0 * M_PI * u2;
+            const double chi = orc_ipm_chi_quad(c12, c6, c4, sigma, E, b);
+            const double sn = sin(chi), cs = cos(chi);
+            out[3 * t] = mu * (g[c] * sn * cos(phi));
+            out[3 * t + 1] = mu * (g[c] * sn * sin(phi));
+            out[3 * t + 2] = mu * (g[c] * cs - g[c]);
+        }
+    }
+}

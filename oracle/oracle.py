@@ -194,6 +194,10 @@ def lib() -> C.CDLL:
         L.orc_set_ipm_table.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_double, C.c_double]
         L.orc_ipm_cos_chi_trajectory.argtypes = [C.c_double] * 7
         L.orc_ipm_cos_chi_trajectory.restype = C.c_double
+        L.orc_ipm_chi_quad.argtypes = [C.c_double] * 6
+        L.orc_ipm_chi_quad.restype = C.c_double
+        L.orc_ipm_cos_chi_many.argtypes = [C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double, DP, DP, DP]
+        L.orc_ipm_sample_cells.argtypes = [C.c_int64, DP] + [C.c_double] * 6 + [C.c_int64, C.c_uint64, C.c_int, DP]
         _lib = L
     return _lib
 
@@ -258,6 +262,75 @@ def ipm_cos_chi_trajectory(c12: float, c6: float, c4: float, m_red: float, E: fl
                            max_step_m: float = 0.05e-10) -> float:
     """cos(chi) from the restated reference trajectory integrator."""
     return lib().orc_ipm_cos_chi_trajectory(c12, c6, c4, m_red, E, b, max_step_m)
+
+
+def ipm_cos_chi_quad(c12: float, c6: float, c4: float, sigma: float, E: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """cos(chi) of the restated deflection quadrature at (E, b) pairs."""
+    E = np.ascontiguousarray(E, dtype=np.float64).ravel()
+    b = np.ascontiguousarray(np.broadcast_to(b, E.shape), dtype=np.float64)
+    out = np.zeros_like(E)
+    lib().orc_ipm_cos_chi_many(E.size, c12, c6, c4, sigma, _dp(E), _dp(b), _dp(out))
+    return out
+
+
+def ipm_table(c12: float, c6: float, c4: float, sigma: float, n_E: int, n_b: int, E_min: float, E_max: float,
+              b_max: float) -> np.ndarray:
+    """The handle's cos(chi) table on the CPU: float32 [n_E, n_b] at
+    E_k = E_min (E_max / E_min)^(k / (n_E - 1)), b_j = b_max j / (n_b - 1)."""
+    import math
+    dlnE = (math.log(E_max) - math.log(E_min)) / (n_E - 1)
+    E = np.repeat(np.exp(math.log(E_min) + np.arange(n_E) * dlnE), n_b)
+    b = np.tile(np.arange(n_b) * (b_max / (n_b - 1)), n_E)
+    return ipm_cos_chi_quad(c12, c6, c4, sigma, E, b).astype(np.float32).reshape(n_E, n_b)
+
+
+def ipm_sample_cells(c12: float, c6: float, c4: float, sigma: float, mu: float, g: np.ndarray, b_max: float,
+                     n_trials: int, seed: int, stratified: bool = True) -> np.ndarray:
+    """Momentum-transfer samples of sample-set cells at relative speeds g
+    ((len(g), n_trials, 3)): the reference tool's per-cell rule with the
+    restated quadrature; stratified = True takes the impact points from
+    equal-area annuli (same law, no Monte Carlo noise in the cell means)."""
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    dp = np.zeros(3 * n_trials * g.size)
+    lib().orc_ipm_sample_cells(g.size, _dp(g), c12, c6, c4, sigma, mu, b_max, n_trials, seed, int(stratified),
+                               _dp(dp))
+    return dp.reshape(g.size, n_trials, 3)
+
+
+def write_ipm_sample_set(path: Path, c12: float, c6: float, c4: float, sigma: float, mu: float, g_min: float,
+                         g_max: float, n_bins: int, b_max: float, n_trials: int, seed: int, stratified: bool = True,
+                         gas: str = "N2") -> dict:
+    """The reference's offline sample set (InteractionPotentialOfflineSampleSet
+    .h:16-98: one orientation, n_bins log-spaced relative speeds, a fixed
+    event disk of radius b_max, full momentum-transfer CDFs with equal
+    weights, interaction_potential_precompute.cpp:2692-2880) in the flat file
+    layout read by oracle/ref_ipm_loader.cpp.  Returns the per-bin summary."""
+    logv = np.linspace(np.log(g_min), np.log(g_max), n_bins)
+    g = np.exp(logv)
+    dps = ipm_sample_cells(c12, c6, c4, sigma, mu, g, b_max, n_trials, seed, stratified)
+    one_minus_cos = -dps[:, :, 2] / (mu * g[:, None])
+    smt = np.pi * b_max ** 2 * one_minus_cos.mean(axis=1)
+    perp = np.hypot(dps[:, :, 0], dps[:, :, 1])
+    stats = np.stack([dps[:, :, 2].mean(axis=1), perp.mean(axis=1), dps[:, :, 2].var(axis=1), perp.var(axis=1)],
+                     axis=1)
+    cells = n_bins
+    sev = np.full(cells, np.pi * b_max ** 2)
+    offsets = np.arange(cells, dtype=np.int64) * n_trials
+    counts = np.full(cells, n_trials, dtype=np.int64)
+    cdf = np.tile((np.arange(n_trials) + 1.0) / n_trials, cells)
+    gb = gas.encode()
+    with open(path, "wb") as f:
+        f.write(b"ICBIPMS1")
+        f.write(np.array([1, n_bins, cells * n_trials, len(gb)], dtype=np.int64).tobytes())
+        f.write(gb)
+        for arr in (logv, smt, sev, np.full(cells, b_max)):
+            f.write(np.ascontiguousarray(arr, dtype=np.float64).tobytes())
+        f.write(offsets.tobytes())
+        f.write(counts.tobytes())
+        f.write(cdf.astype(np.float64).tobytes())
+        f.write(np.ascontiguousarray(dps, dtype=np.float64).tobytes())
+        f.write(np.ascontiguousarray(stats, dtype=np.float64).tobytes())
+    return {"logv_bins": logv, "sigma_mt_m2": smt, "sigma_event_m2": sev}
 
 
 def mt64_uniforms(seed: int, n: int) -> np.ndarray:

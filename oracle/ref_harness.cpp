@@ -37,9 +37,15 @@
 //            moments (20 per snapshot, layout of ICB_N_MOMENTS) of the
 //            active ions; slots 14..19 are displacement moments from the
 //            positions after ref_step steps.
+//            collision=ipm ipm_samples=<file>: the reference's
+//            InteractionPotentialCollisionHandler (random orientation mode)
+//            with the offline sample set of <file> for species "ion"
+//            (read by oracle/ref_ipm_loader.cpp).
 #include "core/integrator/strategies/BorisStrategy.h"
 #include "core/integrator/strategies/RK4Strategy.h"
 #include "core/physics/collisions/HSSCollisionHandler.h"
+#include "core/physics/collisions/InteractionPotentialCollisionHandler.h"
+#include "core/config/types/SpeciesConfig.h"
 #include "core/physics/forces/ElectricFieldForce.h"
 #include "core/physics/forces/MagneticFieldForce.h"
 #include "core/config/types/AnalyticalFieldModel.h"
@@ -479,7 +485,22 @@ int mode_run(const Args& a) {
     integrator::BorisStrategy boris;
     integrator::RK4Strategy rk4;
     rk4.set_parallel_enabled(threads > 1);
-    physics::HSSCollisionHandler hss(false, nullptr);
+    physics::HSSCollisionHandler hss_handler(false, nullptr);
+    // interaction-potential collisions: the reference handler reads the
+    // sample set named in the species database (the engine's wiring,
+    // CollisionHandlerFactory.cpp:94-111, SpeciesConfig.h:39)
+    config::SpeciesDatabase species_db;
+    std::unique_ptr<physics::InteractionPotentialCollisionHandler> ipm_handler;
+    if (coll == "ipm") {
+        config::SpeciesProperties sp{};
+        sp.id = "ion";
+        sp.ipm_samples_file = str(a, "ipm_samples", "ipm_samples.bin");
+        species_db.species.emplace("ion", sp);
+        ipm_handler = std::make_unique<physics::InteractionPotentialCollisionHandler>(false, &species_db, "random");
+    }
+    physics::ICollisionHandler& hss = ipm_handler ? static_cast<physics::ICollisionHandler&>(*ipm_handler)
+                                                  : static_cast<physics::ICollisionHandler&>(hss_handler);
+    const bool colliding = coll == "hss" || coll == "ipm";
     std::vector<physics::PhysicsRng> rng;
     rng.reserve(static_cast<size_t>(n));
     for (int64_t i = 0; i < n; ++i) rng.emplace_back(seed + static_cast<uint64_t>(i));
@@ -527,7 +548,7 @@ int mode_run(const Args& a) {
         }
         if (integ == "rk4") {
             rk4.step_batch(ens, t, dt, regs, dom);
-            if (coll == "hss") {
+            if (colliding) {
 #pragma omp parallel for schedule(static) reduction(+ : collisions)
                 for (int64_t i = 0; i < n; ++i) {
                     if (!active[i]) continue;
@@ -540,7 +561,7 @@ int mode_run(const Args& a) {
             // Engine order as written: serial Boris loop, OpenMP collision loop.
             for (int64_t i = 0; i < n; ++i)
                 if (active[i]) boris.step(ens, static_cast<size_t>(i), t, dt, *reg);
-            if (coll == "hss") {
+            if (colliding) {
 #pragma omp parallel for schedule(guided, 128) reduction(+ : collisions)
                 for (int64_t i = 0; i < n; ++i) {
                     if (!active[i]) continue;
@@ -555,7 +576,7 @@ int mode_run(const Args& a) {
             for (int64_t i = 0; i < n; ++i) {
                 if (!active[i]) continue;
                 boris.step(ens, static_cast<size_t>(i), t, dt, *reg);
-                if (coll == "hss") {
+                if (colliding) {
                     auto cv = ens.collision_data(static_cast<size_t>(i));
                     for (int sc = 0; sc < subcycles; ++sc)
                         collisions += hss.handle_collision(cv, dt / subcycles, rng[static_cast<size_t>(i)], env_at(i)) ? 1 : 0;

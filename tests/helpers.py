@@ -164,3 +164,43 @@ def config0_ions(n: int, seed: int = 123):
     spec = cfg.species_spec(n, 200.0 * AMU, E_CHARGE, {"type": "gaussian", "center": [0, 0, 0], "std": [5e-4] * 3},
                             {"type": "thermal", "temperature_K": 300.0})
     return generate_ions(seed, [spec])
+
+
+def ion_cloud(n: int, mass_amu: float, seed: int = 123):
+    """Seed-123 IonLoader cloud of +1 ions: gaussian sigma 0.5 mm at the
+    origin, thermal at 300 K (the reference harness's init mode)."""
+    from icarion_b200.sim import generate_ions
+    spec = cfg.species_spec(n, mass_amu * AMU, E_CHARGE, {"type": "gaussian", "center": [0, 0, 0], "std": [5e-4] * 3},
+                            {"type": "thermal", "temperature_K": 300.0})
+    return generate_ions(seed, [spec])
+
+
+def ipm_reference_case(z):
+    """(ensemble, initial ions, fit) of the reference interaction-potential
+    fixture ipm_ref_40Td.npz; fit(moments) gives v_drift, K0, D_L, D_T with
+    standard errors (icarion_b200.observables)."""
+    from icarion_b200 import ipm
+    from icarion_b200 import observables as ob
+    setup = ipm.IpmSetup()
+    dt = float(z["dt"])
+    e = cfg.ensemble_params(domain_json(json.loads(str(z["domain"]))), 0.0, dt, detector_z_m=1e30,
+                            ipm_bmax_m=setup.b_max_m)
+    st0 = ion_cloud(int(z["n_ions"]), float(z["ion_mass_amu"]), int(z["seed"]))
+    snap, ref = int(z["snap_every"]), int(z["ref_step"])
+    e_z = e["axial_V"] / e["length_m"]
+
+    def fit(mom):
+        t = np.arange(1, mom.shape[0] + 1) * snap * dt
+        f = ob.fit_transport(t, mom, t_ref=ref * dt)
+        f["K0"] = ob.k0_from_drift(f["v_drift"], e_z, e["gas_density_m3"])
+        f["se_K0"] = f["K0"] * f["se_v_drift"] / f["v_drift"]
+        return f
+
+    return setup, e, st0, fit
+
+
+def assert_transport_close(got: dict, want: dict, n_sigma: float = 4.0) -> None:
+    """v_drift, K0, D_L, D_T within n_sigma combined standard errors."""
+    for key in ("v_drift", "K0", "D_L", "D_T"):
+        se = float(np.hypot(got["se_" + key], want["se_" + key]))
+        assert abs(got[key] - want[key]) <= n_sigma * se, (key, got[key], want[key], se)

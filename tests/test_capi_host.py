@@ -48,19 +48,21 @@ def test_struct_sizes_match_c_layout():
     src = r'''
     #include "icarion_b200.h"
     #include <stdio.h>
-    int main(void){printf("%zu %zu %zu %zu\n", sizeof(icb_ensemble_params), sizeof(icb_config),
-        sizeof(icb_run_stats), sizeof(icb_species_spec)); return 0;}'''
+    #include <stddef.h>
+    int main(void){printf("%zu %zu %zu %zu %zu %zu\n", sizeof(icb_ensemble_params), sizeof(icb_config),
+        sizeof(icb_run_stats), sizeof(icb_species_spec), sizeof(icb_ipm_config),
+        offsetof(icb_ipm_config, net_E_min_J)); return 0;}'''
     tmp = Path(subprocess.run(["mktemp", "-d"], capture_output=True, text=True).stdout.strip())
     (tmp / "s.c").write_text(src)
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(tmp / "s.c"), "-o", str(tmp / "s")], check=True)
     sizes = [int(v) for v in subprocess.run([str(tmp / "s")], capture_output=True, text=True).stdout.split()]
     assert sizes == [C.sizeof(capi.EnsembleParams), C.sizeof(capi.Config), C.sizeof(capi.RunStats),
-                     C.sizeof(capi.SpeciesSpec)]
+                     C.sizeof(capi.SpeciesSpec), C.sizeof(capi.IpmConfig), capi.IpmConfig.net_E_min_J.offset]
 
 
 def test_abi_version_and_error_reporting_without_compute():
     lib = capi.lib()
-    assert lib.icb_abi_version() == 8
+    assert lib.icb_abi_version() == 9
     # invalid configuration is rejected before any device work
     h = C.c_void_p()
     c = capi.Config()

@@ -10,7 +10,11 @@ Tolerances (stated per test):
     norm error <= 1e-4; forward FP32 <= 1e-5 absolute; the BF16 tensor-core
     forward within 2e-2 of FP32 (BF16 weights and activations);
   * training lowers the loss tenfold;
-  * learned vs table deflection: mean drift within 3 % at 40 Td.
+  * learned vs table deflection: mean drift within 3 % at 40 Td;
+  * device table collisions (FP64 and mixed) against the reference's own
+    InteractionPotentialCollisionHandler (fixture ipm_ref_40Td.npz, 65,536
+    ions x 30,000 steps at 40 Td): v_drift, K0, D_L, D_T within 4 combined
+    standard errors, collision fraction within 4 sqrt(2 / collisions).
 """
 from __future__ import annotations
 
@@ -21,7 +25,7 @@ import pytest
 
 import mlp as omlp
 import oracle as orc
-from helpers import config0_ions, oracle_state
+from helpers import assert_transport_close, config0_ions, ipm_reference_case, oracle_state
 from icarion_b200 import _capi as capi
 from icarion_b200 import config as cfg
 from icarion_b200 import ipm
@@ -61,9 +65,9 @@ def test_handle_table_equals_quadrature_at_nodes():
         sim.upload(config0_ions(64))
         sim.configure_ipm(s)
         tab = sim.ipm_table()
-    lnE = np.linspace(math.log(s.E_min_J), math.log(s.E_max_J), s.n_E)
-    E = np.repeat(np.exp(lnE), s.n_b)
-    b = np.tile(np.linspace(0.0, s.b_max_m, s.n_b), s.n_E)
+    En, bn = s.table_grid()
+    E = np.repeat(En, s.n_b)
+    b = np.tile(bn, s.n_E)
     want = ipm.deflection(s, E, b).reshape(s.n_E, s.n_b)
     np.testing.assert_allclose(tab, want.astype(np.float32), rtol=0, atol=2e-6)
 
@@ -79,8 +83,7 @@ def test_fp64_table_collisions_match_oracle():
         tab = sim.ipm_table()
         rs = sim.advance(steps)
         out = sim.download()
-    lnEmin = math.log(s.E_min_J)
-    orc.set_ipm_table(tab.ravel(), s.n_E, s.n_b, lnEmin, (s.n_E - 1) / (math.log(s.E_max_J) - lnEmin))
+    orc.set_ipm_table(tab.ravel(), s.n_E, s.n_b, *s.table_scale())
     ost = oracle_state(st0)
     r = orc.run(e, ost, steps, integrator=0, collision=4, seed=123)
     pos = np.stack([out.x, out.y, out.z])
@@ -167,3 +170,19 @@ def test_mixed_precision_table_collisions_track_fp64():
     dzm = res[capi.PREC_MIXED][0].z - st0.z
     assert abs(dzm.mean() - dz64.mean()) <= 4 * dz64.std() / np.sqrt(dz64.size)
     assert abs(res[capi.PREC_MIXED][1] / res[capi.PREC_FP64][1] - 1.0) < 0.01
+
+
+@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_MIXED])
+def test_table_collisions_match_reference_handler(golden, precision):
+    """The device table path against the reference's runtime sampler (the
+    same fixture pins the oracle on the CPU, tests/test_oracle_ipm_reference.py)."""
+    z = golden("ipm_ref_40Td.npz")
+    setup, e, st0, fit = ipm_reference_case(z)
+    n, steps = int(z["n_ions"]), int(z["steps"])
+    with Simulation([e], precision=precision, collision=capi.COLLISION_IPM_TABLE, rng_seed=int(z["seed"])) as sim:
+        sim.upload(st0)
+        sim.configure_ipm(setup)
+        _, mom, tot = sim.run(steps, int(z["snap_every"]), ref_step=int(z["ref_step"]))
+    assert_transport_close(fit(mom[:, 0, :]), fit(z["moments"]))
+    c_ref = float(z["collisions"])
+    assert abs(tot["collisions"] / c_ref - 1.0) <= 4.0 * math.sqrt(2.0 / c_ref), (tot["collisions"], c_ref)
