@@ -58,6 +58,12 @@
 #include "core/types/CollisionTypes.h"
 #include "utils/constants.h"
 
+#ifdef ICB_WITH_ADAPTERS
+// the reference-side adapters of this library (icarion_b200/adapters)
+#include "B200IntegrationStrategy.h"
+#include "B200CollisionHandler.h"
+#endif
+
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -649,6 +655,93 @@ int mode_run(const Args& a) {
     return 0;
 }
 
+#ifdef ICB_WITH_ADAPTERS
+// adapters: the reference engine's per-step order (as mode_run) with the
+// plug points served by this library's reference-side adapters:
+// B200IntegrationStrategy::step_batch (IIntegrationStrategy.h:119-132) and
+// B200CollisionHandler::handle_batch (ICollisionHandler.h:121-134) on the
+// reference's own IonEnsemble; prepare and finalize stay the engine's.
+//   adapters in= out= <domain keys> integrator=boris|rk4 collision=none|hss
+//            steps= dt= seed= precision=0|1|2
+int mode_adapters(const Args& a) {
+    State s = read_state(str(a, "in", "state.bin"));
+    const int64_t n = s.n;
+    config::DomainConfig d = make_domain(a);
+    const double dt = num(a, "dt", 5e-10);
+    const int64_t steps = static_cast<int64_t>(num(a, "steps", 100));
+    const uint64_t seed = std::strtoull(str(a, "seed", "123").c_str(), nullptr, 10);
+    const std::string integ = str(a, "integrator", "boris");
+    const std::string coll = str(a, "collision", "hss");
+    std::vector<IonState> ions(static_cast<size_t>(n));
+    for (int64_t i = 0; i < n; ++i) {
+        auto& ion = ions[static_cast<size_t>(i)];
+        const size_t k = static_cast<size_t>(i);
+        ion.pos = Vec3{s.a[0][k], s.a[1][k], s.a[2][k]};
+        ion.vel = Vec3{s.a[3][k], s.a[4][k], s.a[5][k]};
+        ion.mass_kg = s.a[6][k];
+        ion.ion_charge_C = s.a[7][k];
+        ion.CCS_m2 = s.a[8][k];
+        ion.active = s.a[9][k] != 0.0;
+        ion.born = true;
+        ion.species_id = "ion";
+    }
+    core::IonEnsemble ens = core::IonEnsemble::from_legacy(ions);
+    integrator::B200IntegrationStrategy strategy(d, integ == "rk4" ? "RK4" : "Boris", coll == "hss" ? "HSS" : "none",
+                                                 seed, dt, n > 0 ? s.a[8][0] : 0.0,
+                                                 static_cast<int>(num(a, "precision", 0)));
+    physics::B200CollisionHandler collisions(strategy);
+    auto reg = std::make_shared<physics::ForceRegistry>(d);
+    std::vector<std::shared_ptr<physics::ForceRegistry>> regs{reg};
+    std::vector<physics::PhysicsRng> rng_pool;     // ignored by the B200 handler (ICollisionHandler.h:118)
+    config::CylindricalGeometry geom(d);
+    auto* px = ens.pos_x_data(); auto* py = ens.pos_y_data(); auto* pz = ens.pos_z_data();
+    auto* vx = ens.vel_x_data(); auto* vy = ens.vel_y_data(); auto* vz = ens.vel_z_data();
+    auto* active = ens.active_data();
+    std::vector<int> dom(static_cast<size_t>(n), 0);
+    std::vector<size_t> idx;
+    double t = 0.0;
+    for (int64_t k = 0; k < steps; ++k) {
+        idx.clear();
+        for (int64_t i = 0; i < n; ++i) {           // prepare_ions_for_integration
+            const size_t k2 = static_cast<size_t>(i);
+            if (!active[i]) { dom[k2] = -1; continue; }
+            if (!geom.contains(Vec3{px[i], py[i], pz[i]})) {
+                active[i] = 0;
+                s.a[10][k2] = t;
+                dom[k2] = -1;
+                continue;
+            }
+            dom[k2] = 0;
+            idx.push_back(k2);
+        }
+        if (!strategy.step_batch(ens, t, dt, regs, dom)) throw std::runtime_error("step_batch refused");
+        if (coll == "hss" && !collisions.handle_batch(ens, idx, dt, d.environment, rng_pool))
+            throw std::runtime_error("handle_batch refused");
+        for (int64_t i = 0; i < n; ++i) {           // finalize_ions_after_integration
+            const size_t k2 = static_cast<size_t>(i);
+            if (dom[k2] < 0) continue;
+            const Vec3 p{px[i], py[i], pz[i]};
+            if (!geom.contains(p) || !(std::isfinite(p.x) && std::isfinite(p.y) && std::isfinite(p.z) &&
+                                       std::isfinite(vx[i]) && std::isfinite(vy[i]) && std::isfinite(vz[i]))) {
+                active[i] = 0;
+                s.a[10][k2] = t;
+            }
+        }
+        t = t + dt;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        const size_t k = static_cast<size_t>(i);
+        s.a[0][k] = px[i]; s.a[1][k] = py[i]; s.a[2][k] = pz[i];
+        s.a[3][k] = vx[i]; s.a[4][k] = vy[i]; s.a[5][k] = vz[i];
+        s.a[9][k] = active[i] ? 1.0 : 0.0;
+    }
+    write_state(str(a, "out", "state_out.bin"), s);
+    std::printf("{\"ion_steps\": %lld, \"strategy\": \"%s\", \"handler\": \"%s\", \"t_end\": %.17g}\n",
+                static_cast<long long>(n * steps), strategy.name().c_str(), collisions.name().c_str(), t);
+    return 0;
+}
+#endif
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -671,6 +764,9 @@ int main(int argc, char** argv) {
         if (mode == "run") return mode_run(a);
         if (mode == "direct") return mode_direct(a);
         if (mode == "ehss") return mode_ehss(a);
+#ifdef ICB_WITH_ADAPTERS
+        if (mode == "adapters") return mode_adapters(a);
+#endif
         std::fprintf(stderr, "unknown mode %s\n", argv[1]);
         return 2;
     } catch (const std::exception& e) {
