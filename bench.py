@@ -587,8 +587,8 @@ def run_ipm(args) -> None:
     sys.path.insert(0, str(ROOT))
     from icarion_b200 import _capi as capi
     from icarion_b200 import config as cfg
-    from icarion_b200 import ipm, sweep
-    from icarion_b200.sim import Simulation, generate_ions
+    from icarion_b200 import ipm
+    from icarion_b200.sim import Simulation
 
     rank, world, local = _env_rank()
     torch.cuda.set_device(local if world > 1 else 0)
@@ -605,21 +605,7 @@ def run_ipm(args) -> None:
 
     en = (10.0, 40.0, 80.0)
     n_total = N_IONS
-    counts = [n_total // 3 + (1 if k < n_total % 3 else 0) for k in range(3)]
-    m_ion = 300.0 * cfg.AMU_TO_KG
-    sigma_ev = math.pi * setup.b_max_m ** 2
-    ensembles, specs = [], []
-    for e_td, c in zip(en, counts):
-        nu = sweep.collision_frequency_max(e_td, m_ion, sigma_ev, cfg.GAS_MASS_KG["N2"], 300.0, 1000.0)
-        domain = {"instrument": "IMS", "geometry": {"origin_m": [0.0, 0.0, -0.01], "length_m": 0.1, "radius_m": 0.05},
-                  "env": {"temperature_K": 300.0, "pressure_Pa": 1000.0, "gas_species": "N2"},
-                  "fields": {"DC": {"EN_Td": e_td}}}
-        ensembles.append(cfg.ensemble_params(domain, 0.0, 0.1 / nu, ipm_bmax_m=setup.b_max_m))
-        specs.append(cfg.species_spec(c, m_ion, cfg.ELEM_CHARGE_C,
-                                      {"type": "gaussian", "center": [0, 0, 0], "std": [5e-4] * 3},
-                                      {"type": "thermal", "temperature_K": 300.0}))
-    st0 = generate_ions(123, specs)
-    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
+    ensembles, st0, offsets = ipm.drift_ensembles(setup, en, n_total)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -627,7 +613,11 @@ def run_ipm(args) -> None:
     launches = 0
     clocks = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)).split(",")[0]) if world == 1 else dev)
     clocks.start()
-    for name, model in (("table", capi.COLLISION_IPM_TABLE), ("mlp", capi.COLLISION_IPM_MLP)):
+    # the table, the learned network, and the FP64 quadrature at every
+    # collision (the method without the network; timed on fewer steps)
+    for name, model in (("table", capi.COLLISION_IPM_TABLE), ("mlp", capi.COLLISION_IPM_MLP),
+                        ("quadrature", capi.COLLISION_IPM_QUAD)):
+        n_timed = args.steps if model != capi.COLLISION_IPM_QUAD else min(args.steps, 2)
         sim = Simulation(ensembles, precision=capi.PREC_MIXED, collision=model, rng_seed=123, device=dev,
                          stepping=STEPPING[args.stepping])
         sim.set_stream(stream.cuda_stream)
@@ -635,14 +625,14 @@ def run_ipm(args) -> None:
         sim.configure_ipm(setup)
         if model == capi.COLLISION_IPM_MLP:
             sim.set_mlp(params)
-        tuned = sim.autotune(300) if args.autotune else None
-        for _ in range(args.warmup):
+        tuned = sim.autotune(300) if args.autotune and model != capi.COLLISION_IPM_QUAD else None
+        for _ in range(args.warmup if model != capi.COLLISION_IPM_QUAD else 1):
             sim.advance(STEPS_PER_BENCH_STEP)
         sim.upload(st0, ens_offsets=offsets, first_id=rank * n_total)
         sim.set_clock(0, np.zeros(3))
         torch.cuda.synchronize()
         ms, kms, nl, coll = 0.0, 0.0, 0, 0
-        for _ in range(args.steps):
+        for _ in range(n_timed):
             flush.zero_()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
@@ -664,9 +654,9 @@ def run_ipm(args) -> None:
             E = en[e] * 1e-21 * n_gas
             k0.append(v_d / E * (n_gas / cfg.n0_loschmidt()) * 1e4)
         results[name] = {"autotuned": tuned,
-                         "ion_steps_per_s": n_total * STEPS_PER_BENCH_STEP * args.steps / (ms * 1e-3),
-                         "ms_per_step": ms / args.steps, "K0_cm2_Vs": k0,
-                         "collision_fraction": coll / (n_total * STEPS_PER_BENCH_STEP * args.steps)}
+                         "ion_steps_per_s": n_total * STEPS_PER_BENCH_STEP * n_timed / (ms * 1e-3),
+                         "ms_per_step": ms / n_timed, "K0_cm2_Vs": k0, "timed_steps": n_timed,
+                         "collision_fraction": coll / (n_total * STEPS_PER_BENCH_STEP * n_timed)}
         sim.close()
     clk = clocks.stop()
     if rank != 0:
@@ -684,8 +674,12 @@ def run_ipm(args) -> None:
                                "(N2 1.74 A^3) ion-N2 potential, 300 Da, 1,048,576 ions in three ensembles at "
                                "10/40/80 Td, N2 300 K 1000 Pa, b_max 12 A, dt = 0.1/nu_max",
                    "ions_per_gpu": n_total, "engine_steps_per_bench_step": STEPS_PER_BENCH_STEP,
-                   "table": results["table"], "mlp": mlp,
+                   "table": results["table"], "mlp": mlp, "quadrature": results["quadrature"],
                    "K0_shift_mlp_vs_table": [m / t - 1.0 for m, t in zip(mlp["K0_cm2_Vs"], results["table"]["K0_cm2_Vs"])],
+                   "speedup_mlp_over_quadrature": mlp["ion_steps_per_s"] / results["quadrature"]["ion_steps_per_s"],
+                   "speedup_mlp_over_table": mlp["ion_steps_per_s"] / results["table"]["ion_steps_per_s"],
+                   "K0_note": "K0 here is <dz>/t over the timed steps (transient included); the K0 gates are "
+                              "fitted in tests/test_gpu_ipm_config3.py",
                    "training": {"samples": 1 << 20, "epochs": 20, "batch": 1024, "data_s": t_data,
                                 "train_s": t_train, "final_loss": float(losses[-1]),
                                 "validation_rms_cos_chi": val_rms},

@@ -26,7 +26,7 @@ ICB_ERR_TIMEOUT = 7
 PREC_FP64, PREC_MIXED, PREC_MIXED_HILO = 0, 1, 2
 INTEGRATOR_BORIS, INTEGRATOR_RK4 = 0, 1
 COLLISION_NONE, COLLISION_HSS, COLLISION_IPM_TABLE, COLLISION_IPM_MLP, COLLISION_LANGEVIN = 0, 1, 2, 3, 4
-COLLISION_HSS_PLAIN, COLLISION_EHSS = 5, 6
+COLLISION_HSS_PLAIN, COLLISION_EHSS, COLLISION_IPM_QUAD = 5, 6, 7
 INSTRUMENT_IMS, INSTRUMENT_FTICR, INSTRUMENT_QUADRUPOLE_RF, INSTRUMENT_LQIT, INSTRUMENT_TIMS = 0, 1, 2, 3, 4
 MAX_WAVE_POINTS = 64
 (WAVE_CONSTANT, WAVE_LINEAR, WAVE_QUADRATIC, WAVE_EXPONENTIAL, WAVE_SINUSOIDAL, WAVE_PWM, WAVE_PULSED,

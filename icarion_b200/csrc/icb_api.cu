@@ -299,6 +299,8 @@ struct icb_handle {
     int ipm_nE = 0, ipm_nb = 0;
     double ipm_lnEmin = 0.0, ipm_inv_dlnE = 0.0, ipm_bmax = 0.0, ipm_Emin = 0.0, ipm_Emax = 0.0;
     double ipm_net_lnEmin = 0.0, ipm_net_scale = 0.0;   // x0 = (ln E - lnEmin) scale - 1
+    IpmPotential ipm_pot{};
+    const GLNodes* ipm_gl = nullptr;
     DevBuf<uint32_t> mlp_w2;
     DevBuf<float> mlp_f;
     DevBuf<MixConst> mix;              // HSS gas mixtures, per ensemble
@@ -594,7 +596,7 @@ int build_ens_const(const icb_ensemble_params& P, EnsConst& C, int& field_kind, 
                 return fail(ICB_ERR_INVALID_ARGUMENT, "Langevin collisions need gas_polarizability_m3 > 0");
             C.A = 0.0;
             C.lang_c = P.gas_density_m3 * P.dt_s * M_PI * std::sqrt(P.gas_polarizability_m3 / (4.0 * M_PI * kEps0));
-        } else if (coll == kCollIPMTable || coll == kCollIPMMLP) {
+        } else if (coll == kCollIPMTable || coll == kCollIPMMLP || coll == kCollIPMQuad) {
             // event cross-section pi b_max^2 (InteractionPotentialCollisionHandler.cpp:443-447)
             if (!(P.ipm_bmax_m > 0.0))
                 return fail(ICB_ERR_INVALID_ARGUMENT, "interaction-potential collisions need ipm_bmax_m > 0");
@@ -812,7 +814,7 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         if (int r = enqueue_tf_tables(h, K, st)) return r;
     }
     const int n_ens = static_cast<int>(h->ens.size());
-    if ((h->coll == kCollIPMTable || h->coll == kCollIPMMLP) && h->ipm_nE == 0)
+    if ((h->coll == kCollIPMTable || h->coll == kCollIPMMLP || h->coll == kCollIPMQuad) && h->ipm_nE == 0)
         return fail(ICB_ERR_STATE, "interaction-potential collisions need icb_ipm_configure first");
     if (h->coll == kCollIPMMLP && !h->mlp_ready)
         return fail(ICB_ERR_STATE, "the learned deflection needs icb_ipm_set_mlp first");
@@ -848,6 +850,9 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.ipm_nb = h->ipm_nb;
         p.ipm_lnEmin = h->ipm_lnEmin;
         p.ipm_inv_dlnE = h->ipm_inv_dlnE;
+        p.ipm_pot = h->ipm_pot;
+        p.ipm_bmax = h->ipm_bmax;
+        p.ipm_gl = h->ipm_gl;
         p.ipm_net_lnEmin = h->ipm_net_lnEmin;
         p.ipm_net_scale = h->ipm_net_scale;
         p.mlp_w2 = h->mlp_w2.p;
@@ -1049,9 +1054,12 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
             break;
         case ICB_COLLISION_IPM_TABLE:
         case ICB_COLLISION_IPM_MLP:
+        case ICB_COLLISION_IPM_QUAD:
             if (cfg->integrator != ICB_INTEGRATOR_BORIS)
                 return fail(ICB_ERR_UNSUPPORTED, "interaction-potential collisions are built for the Boris pusher");
-            coll = cfg->collision_model == ICB_COLLISION_IPM_TABLE ? kCollIPMTable : kCollIPMMLP;
+            coll = cfg->collision_model == ICB_COLLISION_IPM_TABLE ? kCollIPMTable
+                 : cfg->collision_model == ICB_COLLISION_IPM_MLP   ? kCollIPMMLP
+                                                                   : kCollIPMQuad;
             break;
         case ICB_COLLISION_LANGEVIN:
             if (cfg->integrator != ICB_INTEGRATOR_BORIS)
@@ -1501,6 +1509,8 @@ int icb_ipm_configure(icb_handle* h, const icb_ipm_config* cfg) {
     h->ipm_bmax = cfg->b_max_m;
     h->ipm_Emin = cfg->E_min_J;
     h->ipm_Emax = cfg->E_max_J;
+    if (int r2 = ipm_gl_nodes(h->cfg.device, &h->ipm_gl, err)) return fail(r2, "%s", err.c_str());
+    h->ipm_pot = P;
     h->ipm_net_lnEmin = std::log(net_lo);
     h->ipm_net_scale = 2.0 / (std::log(net_hi) - h->ipm_net_lnEmin);
     ++h->gen;

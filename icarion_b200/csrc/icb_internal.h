@@ -34,6 +34,10 @@ int sc_kernel_count(const SpaceChargeSolver* sc);
 
 // Interaction-potential physics (icb_ipm.cu).
 int ipm_potential_from(const icb_ipm_potential& p, IpmPotential& P, std::string& err);
+// Device Gauss-Legendre nodes of the deflection quadrature (one copy per
+// device, made on first use).
+struct GLNodes;
+int ipm_gl_nodes(int device, const GLNodes** out, std::string& err);
 int ipm_build_table(int device, const IpmPotential& P, int nE, int nb, double Emin, double Emax, double bmax,
                     float* dev_table, cudaStream_t s, std::string& err);
 

@@ -26,19 +26,13 @@
 
 #include "../../include/icarion_b200.h"
 #include "icb_internal.h"
+#include "icb_ipm.cuh"
 
 namespace icb {
 
 namespace {
 
 constexpr double kCoulomb = 8.987551787e9;   // utils/constants.h:20
-constexpr int kGL = 64;
-
-struct GLNodes {
-    double s[kGL];   // nodes on [0, 1]
-    double w[kGL];   // weights on [0, 1]
-};
-
 // Gauss-Legendre nodes and weights on [-1, 1] by Newton iteration on P_n
 // (Golub-Welsch-free textbook recurrence), mapped to [0, 1].
 GLNodes make_gl() {
@@ -64,38 +58,6 @@ GLNodes make_gl() {
         g.w[i] = 0.5 * w;
     }
     return g;
-}
-
-__device__ __forceinline__ double ipm_F(const IpmPotential& P, double E, double b, double r) {
-    const double ir2 = 1.0 / (r * r);
-    const double ir4 = ir2 * ir2, ir6 = ir4 * ir2, ir12 = ir6 * ir6;
-    const double V = P.c12 * ir12 - P.c6 * ir6 - P.c4 * ir4;
-    return 1.0 - b * b * ir2 - V / E;
-}
-
-__device__ double ipm_cos_chi(const IpmPotential& P, const GLNodes& gl, double E, double b) {
-    if (!(E > 0.0)) return 1.0;
-    double r = 4.0 * (b + P.sigma);
-    int it = 0;
-    while (ipm_F(P, E, b, r * 0.98) > 0.0 && it < 4000) {
-        r *= 0.98;
-        ++it;
-    }
-    double lo = r * 0.98, hi = r;
-    for (int k = 0; k < 200 && hi - lo > 1e-15 * hi; ++k) {
-        const double mid = 0.5 * (lo + hi);
-        if (ipm_F(P, E, b, mid) > 0.0) hi = mid; else lo = mid;
-    }
-    const double r0 = hi;
-    double I = 0.0;
-    for (int k = 0; k < kGL; ++k) {
-        const double s = gl.s[k];
-        const double u = 1.0 - s * s;
-        const double F = fmax(ipm_F(P, E, b, r0 / u), 1e-300);
-        I += gl.w[k] * 2.0 * s / sqrt(F);
-    }
-    const double chi = M_PI - 2.0 * (b / r0) * I;
-    return cos(chi);
 }
 
 __global__ void k_ipm_deflection(IpmPotential P, const GLNodes* __restrict__ gl, uint64_t n,
@@ -154,6 +116,8 @@ int gl_nodes(int device, const GLNodes** out, std::string& err) {
 }
 
 }  // namespace
+
+int ipm_gl_nodes(int device, const GLNodes** out, std::string& err) { return gl_nodes(device, out, err); }
 
 int ipm_potential_from(const icb_ipm_potential& p, IpmPotential& P, std::string& err) {
     if (!(p.epsilon_J >= 0.0) || !(p.r_m_m > 0.0) || !(p.polarizability_m3 >= 0.0)) {

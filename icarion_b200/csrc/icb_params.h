@@ -16,7 +16,7 @@ constexpr int kMaxLaunchEns = 64;   // ensembles per launch chunk (param space b
 constexpr uint32_t kMaxStepsPerLaunch = 16384;
 
 enum FieldKind : int { kFieldUniform = 0, kFieldLinear = 1, kFieldLinearRF = 2 };
-enum CollKind : int { kCollNone = 0, kCollHSS = 1, kCollLangevin = 2, kCollIPMTable = 3, kCollIPMMLP = 4, kCollHSSMix = 5, kCollHSSPlain = 6, kCollEHSS = 7 };
+enum CollKind : int { kCollNone = 0, kCollHSS = 1, kCollLangevin = 2, kCollIPMTable = 3, kCollIPMMLP = 4, kCollHSSMix = 5, kCollHSSPlain = 6, kCollEHSS = 7, kCollIPMQuad = 8 };
 enum PrecKind : int { kPrecFP64 = 0, kPrecMixed = 1, kPrecHiLo = 2 };
 enum IntegKind : int { kBoris = 0, kRK4 = 1 };
 
@@ -151,6 +151,11 @@ struct StepParams {
     const float* ipm_tab;
     int32_t ipm_nE, ipm_nb;
     double ipm_lnEmin, ipm_inv_dlnE;
+    // per-collision quadrature (kCollIPMQuad): the potential, b_max and the
+    // Gauss-Legendre nodes (struct GLNodes of icb_ipm.cuh)
+    IpmPotential ipm_pot;
+    double ipm_bmax;
+    const void* ipm_gl;
     // learned deflection input: x0 = (ln E - net_lnEmin) net_scale - 1,
     // inside the trained range when |x0| <= 1
     double ipm_net_lnEmin, ipm_net_scale;

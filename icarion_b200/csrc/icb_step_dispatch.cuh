@@ -41,6 +41,11 @@ cudaError_t dispatch_step(int integ, int coll, int field, bool mag, const StepPa
         if (coll == kCollLangevin) return dispatch_field<PREC, kBoris, kCollLangevin>(field, mag, p, g, b, s);
         if (coll == kCollIPMTable) return dispatch_field<PREC, kBoris, kCollIPMTable>(field, mag, p, g, b, s);
         if (coll == kCollIPMMLP) return dispatch_field<PREC, kBoris, kCollIPMMLP>(field, mag, p, g, b, s);
+        if (coll == kCollIPMQuad) {
+            // the per-collision quadrature: built for the uniform drift field
+            if (field != kFieldUniform || mag) return cudaErrorNotSupported;
+            return launch_one<PREC, kBoris, kCollIPMQuad, kFieldUniform, false>(p, g, b, s);
+        }
         if (coll == kCollHSSMix) return dispatch_field<PREC, kBoris, kCollHSSMix>(field, mag, p, g, b, s);
         if (coll == kCollEHSS) return dispatch_field<PREC, kBoris, kCollEHSS>(field, mag, p, g, b, s);
         if constexpr (PREC == kPrecFP64) {

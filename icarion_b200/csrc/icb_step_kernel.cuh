@@ -36,6 +36,7 @@
 #include "icb_params.h"
 #include "icb_rng.cuh"
 #include "icb_mlp.cuh"
+#include "icb_ipm.cuh"
 
 namespace icb {
 
@@ -1037,12 +1038,19 @@ __device__ __forceinline__ int candidate(const EnsConst& C, R v[3], R& clk, R qs
         ip->vn[0] = vn[0]; ip->vn[1] = vn[1]; ip->vn[2] = vn[2];
         return 3;
     }
-    if constexpr (COLL == kCollIPMTable) {
-        // elastic deflection by chi(E, b): b uniform in area below b_max
+    if constexpr (COLL == kCollIPMTable || COLL == kCollIPMQuad) {
+        // elastic deflection by chi(E, b): b uniform in area below b_max;
+        // chi from the table, or (kCollIPMQuad) by the FP64 quadrature of
+        // this collision's own (E, b)
         const R mu = mi * fac;   // m_i m_n / (m_i + m_n); the product m_i m_n underflows in float
         const R E = R(0.5) * mu * (g * g);
         const R bn = m_sqrt(u16(r1.z & 0xffffu, R(0)));
-        const R cx = ipm_table_cos<R>(p, E, bn);
+        R cx;
+        if constexpr (COLL == kCollIPMQuad)
+            cx = static_cast<R>(ipm_cos_chi(p.ipm_pot, *static_cast<const GLNodes*>(p.ipm_gl),
+                                            static_cast<double>(E), static_cast<double>(bn) * p.ipm_bmax));
+        else
+            cx = ipm_table_cos<R>(p, E, bn);
         const R sx = m_sqrt(m_fmax(R(0), R(1) - cx * cx));
         R cp2, sp2;
         angle_cs(u16(r1.w >> 16, R(0)), cp2, sp2);

@@ -23,6 +23,7 @@ import numpy as np
 
 from . import _capi as capi
 from . import config as cfg
+from . import sweep
 
 EV_J = 1.602176634e-19
 
@@ -151,3 +152,27 @@ def gradients(params: np.ndarray, x: np.ndarray, y: np.ndarray, device: int = 0)
     capi.check(capi.lib().icb_mlp_gradients(device, capi.fptr(np.ascontiguousarray(params, dtype=np.float32)),
                                             y.size, capi.fptr(x), capi.fptr(y), capi.fptr(g), C.byref(loss)))
     return g, loss.value
+
+
+def drift_ensembles(setup: IpmSetup, en_td=(10.0, 40.0, 80.0), n_total: int = 1 << 20, ion_mass_amu: float = 300.0,
+                    seed: int = 123):
+    """The learned-IPM evaluation workload: n_total ions of ion_mass_amu, +1,
+    split evenly over one IMS drift ensemble per E/N (N2, 300 K, 1000 Pa,
+    event radius b_max, dt = 0.1 / nu_max at that E/N).  Returns
+    (ensembles, initial IonState, ensemble offsets)."""
+    from .sim import generate_ions
+    counts = [n_total // len(en_td) + (1 if k < n_total % len(en_td) else 0) for k in range(len(en_td))]
+    m_ion = ion_mass_amu * cfg.AMU_TO_KG
+    sigma_ev = math.pi * setup.b_max_m ** 2
+    ensembles, specs = [], []
+    for e_td, c in zip(en_td, counts):
+        nu = sweep.collision_frequency_max(e_td, m_ion, sigma_ev, cfg.GAS_MASS_KG["N2"], 300.0, 1000.0)
+        domain = {"instrument": "IMS", "geometry": {"origin_m": [0.0, 0.0, -0.01], "length_m": 0.1, "radius_m": 0.05},
+                  "env": {"temperature_K": 300.0, "pressure_Pa": 1000.0, "gas_species": "N2"},
+                  "fields": {"DC": {"EN_Td": e_td}}}
+        ensembles.append(cfg.ensemble_params(domain, 0.0, 0.1 / nu, ipm_bmax_m=setup.b_max_m))
+        specs.append(cfg.species_spec(c, m_ion, cfg.ELEM_CHARGE_C,
+                                      {"type": "gaussian", "center": [0, 0, 0], "std": [5e-4] * 3},
+                                      {"type": "thermal", "temperature_K": 300.0}))
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
+    return ensembles, generate_ions(seed, specs), offsets

@@ -59,7 +59,12 @@ enum {
     /* exact hard-sphere scattering on a molecule of atoms (EHSS,
      * CollisionKernels.cpp:13-137, 220-381), rate n sigma_m2 |v - v_n|;
      * geometry from icb_ehss_set_geometry */
-    ICB_COLLISION_EHSS = 6
+    ICB_COLLISION_EHSS = 6,
+    /* interaction-potential collisions with the deflection computed by the
+     * FP64 quadrature at every collision (no table, no network): the plain
+     * method the learned deflection is measured against; Boris in a uniform
+     * field without B */
+    ICB_COLLISION_IPM_QUAD = 7
 };
 enum {
     ICB_INSTRUMENT_IMS = 0,          /* AnalyticalFieldModel.cpp:136-161 */

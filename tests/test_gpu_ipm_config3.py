@@ -1,0 +1,78 @@
+"""The learned deflection at its own evaluation settings, and what it gains.
+
+Workload (learned-IPM evaluation): 1,048,576 ions of 300 Da in N2 at 300 K
+and 1000 Pa, one ensemble per E/N of 10, 40 and 80 Td, the LJ 12-6 + C4
+potential, b_max = 12 A, dt = 0.1 / nu_max, 50,000 steps; moments every
+1,000 steps, displacement reference after 10,000.  The network is trained
+on the device on 2^20 (E, b) pairs from the quadrature (E log-uniform over
+1 meV - 10 eV, b uniform over [0, 12 A]).
+
+1. K0 of the learned deflection within 0.3 % of the table's at every E/N
+   (standard error of each K0 ~0.05-0.08 %, stated by the fit).
+2. The gain: the same run with the deflection computed by the FP64
+   quadrature at every collision (the method without the network).  The
+   learned path's K0 is within 0.3 % of the quadrature's at every E/N, and
+   it advances at least 5x as many ion-steps per second (device time of
+   the step kernels).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from icarion_b200 import _capi as capi
+from icarion_b200 import ipm
+from icarion_b200 import observables as ob
+from icarion_b200.sim import Simulation, device_count
+
+pytestmark = pytest.mark.gpu
+
+EN = (10.0, 40.0, 80.0)
+N_IONS = 1 << 20
+STEPS, SNAP, REF = 50_000, 1_000, 10_000
+
+
+@pytest.fixture(scope="module")
+def workload():
+    assert device_count() > 0, "these tests need a CUDA device"
+    setup = ipm.IpmSetup()
+    x, y, _, _ = ipm.training_set(setup, n=1 << 20, seed=2024)
+    params, losses = ipm.train(x, y, epochs=20, batch=1024, lr=3e-3, seed=7)
+    assert losses[-1] < 0.1 * losses[0]
+    ens, st0, off = ipm.drift_ensembles(setup, EN, N_IONS)
+    return setup, params, ens, st0, off
+
+
+def run(workload, model: int, steps: int = STEPS):
+    setup, params, ens, st0, off = workload
+    with Simulation(ens, precision=capi.PREC_MIXED, collision=model, rng_seed=123) as sim:
+        sim.upload(st0, ens_offsets=off)
+        sim.configure_ipm(setup)
+        if model == capi.COLLISION_IPM_MLP:
+            sim.set_mlp(params)
+        steps_idx, mom, tot = sim.run(steps, SNAP, ref_step=REF)
+    fits = []
+    for e, E in enumerate(ens):
+        t = steps_idx * E["dt_s"]
+        f = ob.fit_transport(t, mom[:, e, :], t_ref=REF * E["dt_s"])
+        f["K0"] = ob.k0_from_drift(f["v_drift"], E["axial_V"] / E["length_m"], E["gas_density_m3"])
+        f["se_K0"] = f["K0"] * f["se_v_drift"] / f["v_drift"]
+        fits.append(f)
+    return fits, N_IONS * steps / (tot["device_ms"] * 1e-3), tot
+
+
+def test_learned_k0_within_0p3_percent_of_table(workload):
+    table, rate_t, _ = run(workload, capi.COLLISION_IPM_TABLE)
+    learned, rate_l, tot = run(workload, capi.COLLISION_IPM_MLP)
+    assert tot["collisions"] > 0.04 * N_IONS * STEPS
+    for e_td, t, m in zip(EN, table, learned):
+        assert t["se_K0"] / t["K0"] < 1.2e-3, (e_td, t["se_K0"] / t["K0"])
+        assert abs(m["K0"] / t["K0"] - 1.0) <= 3e-3, (e_td, m["K0"], t["K0"])
+
+
+def test_learned_deflection_gain_over_per_collision_quadrature(workload):
+    quad, rate_q, _ = run(workload, capi.COLLISION_IPM_QUAD)
+    learned, rate_l, _ = run(workload, capi.COLLISION_IPM_MLP)
+    for e_td, q, m in zip(EN, quad, learned):
+        assert abs(m["K0"] / q["K0"] - 1.0) <= 3e-3, (e_td, m["K0"], q["K0"])
+    assert rate_l >= 5.0 * rate_q, (rate_l, rate_q)
