@@ -63,34 +63,58 @@ TIMS_WORKLOAD = ("TIMS ramp, 1,048,576 ions (200 Da, +1, 150 A^2 HSS) in N2 300 
 # write x,y,z(24) v(12) tau,Q*(8) next,start(8) flags(1)                          = 53
 # (hi/lo: positions 6 floats = 24 B as well; FP64: v and the clock are doubles: 97 + 73)
 BYTES_PER_ION_LAUNCH = {"mixed": 130, "hilo": 130, "fp64": 170}
-# DRAM bytes of one fused mixed launch at 1,048,576 ions from an ncu capture
-# of that launch (dram__bytes_read.sum + dram__bytes_write.sum; writes still
-# in L2 at kernel end are not counted).
-STEPPING = {"events": 0, "per-step": 1}
-NCU_TRAFFIC_PER_LAUNCH = {"mixed": 80.850176e6 + 6.612992e6}
-# Warp instructions of one fused mixed launch (1,048,576 ions x 1000 steps,
-# event-to-event form) from the same capture (smsp__inst_executed.sum): the
-# kernel is bound by instruction issue, so its second roofline is the issue
-# peak of 4 warp instructions per SM per cycle.
-NCU_INST_PER_LAUNCH = {"mixed": 2.100741539e9}
+STEPPING = {"events": 0, "per-step": 1, "events-all": 2}
+# ncu summary of the fused mixed launch (1,048,576 ions x 1000 steps, event
+# form).  Its "bench figures" block holds the warp instructions
+# (smsp__inst_executed.sum) and DRAM bytes (dram__bytes_read.sum +
+# dram__bytes_write.sum) of one launch, and the kernel_source_hash of the
+# sources the capture ran; the figures are used only while that hash matches
+# the current sources.
+PROFILE_FUSED = "profiles/k_step_mixed_fused_ims_1M.md"
 
 
-def issue_roofline(args, avg_launch_ms: float, clk: dict) -> dict | None:
+def profile_figures(rel: str, unit: str = "icb_step_mixed.cu") -> dict:
+    """Figures of a committed ncu summary and whether they belong to the
+    kernel as built now."""
+    import re
+    sys.path.insert(0, str(ROOT))
+    from icarion_b200.build import kernel_source_hash
+    path = ROOT / rel
+    txt = path.read_text() if path.exists() else ""
+    m = re.search(r"<!-- bench figures\n(.*?)-->", txt, re.S)
+    figs = {}
+    for line in (m.group(1).splitlines() if m else []):
+        if ":" in line:
+            k, v = line.split(":", 1)
+            figs[k.strip()] = v.strip()
+    fresh = bool(figs) and figs.get("source_sha256") == kernel_source_hash(unit)
+    out = {"file": rel, "fresh": fresh}
+    if fresh:
+        out["inst_per_launch"] = float(figs["inst_per_launch"])
+        out["dram_bytes_per_launch"] = float(figs["dram_bytes_per_launch"])
+    else:
+        out["note"] = ("no figures block" if not figs else
+                       "stale: the summary was taken of other kernel sources; its figures are not used")
+    return out
+
+
+def issue_roofline(args, avg_launch_ms: float, clk: dict, prof: dict) -> dict | None:
     """Instruction-issue roofline of the fused mixed kernel: warp
-    instructions per launch (ncu, same workload) / live launch time, against
-    4 schedulers x SMs x the SM clock sampled during the run."""
+    instructions per launch (ncu summary of the same workload, current
+    sources only) / live launch time, against 4 schedulers x SMs x the SM
+    clock sampled during the run."""
     if args.precision != "mixed" or args.steps_per_launch != 1000 or args.workload != "ims-1M" \
-            or args.stepping != "events":
+            or args.stepping != "events" or not prof.get("fresh"):
         return None
     import torch
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
-    inst = NCU_INST_PER_LAUNCH["mixed"]
+    inst = prof["inst_per_launch"]
     achieved = inst / (avg_launch_ms * 1e-3)
     peak = 4.0 * sms * mhz * 1e6
     return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp instructions/s",
             "frac": achieved / peak, "inst_per_launch": inst, "sms": sms, "sm_mhz": mhz,
-            "source": "smsp__inst_executed.sum of one launch (ncu); peak = 4 x SMs x sampled SM clock"}
+            "source": f"smsp__inst_executed.sum of one launch ({prof['file']}); peak = 4 x SMs x sampled SM clock"}
 
 
 def _env_rank():
@@ -176,33 +200,57 @@ def _harness():
     return orc
 
 
-def reference_sample(n_ions: int, n_steps: int, threads: int, state_path: Path | None = None) -> dict:
-    """Run the reference's Boris + HSS code (best CPU form: one OpenMP loop per
-    step) on n_ions for n_steps; returns the harness's own loop timing."""
+def reference_sample(n_ions: int, n_steps: int, threads: int, schedule: str = "static") -> dict:
+    """Run the reference's Boris + HSS code on n_ions for n_steps; returns the
+    harness's own loop timing.  schedule "static": the best CPU form (one
+    OpenMP loop per step, push then collide per ion); "faithful": the engine's
+    order as written (serial Boris loop, SimulationEngineIntegration.cpp:
+    114-146, then the OpenMP collision loop, SimulationEngineCollisionRuntime
+    .cpp:103-105)."""
     orc = _harness()
     with tempfile.TemporaryDirectory() as td:
         sp = Path(td) / "s.bin"
         orc.harness("init", seed=123, n=n_ions, sigma_pos=5e-4, T=300, mass=repr(200.0 * 1.66053906660e-27), out=sp)
         out = orc.harness("run", **{"in": sp, "out": Path(td) / "o.bin"}, **REF_DOMAIN, integrator="boris",
-                          collision="hss", dt=DT, steps=n_steps, threads=threads, seed=123)
+                          collision="hss", dt=DT, steps=n_steps, threads=threads, seed=123, schedule=schedule)
     return json.loads(out.strip().splitlines()[-1])
 
 
-def cpu_baseline(budget_s: float = 15.0) -> dict:
-    """Bounded sample of the same workload on the host cores (rank 0, N=1)."""
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline(budget_s: float = 12.0) -> dict:
+    """Bounded samples of the same workload on the host cores (rank 0, N=1):
+    the reference code in its best CPU form (the reported value) and in the
+    engine's own order."""
     orc = _harness()
     threads = cpu_threads()
     n = 65536
     if not orc.have_harness():
         return {"value": None, "unit": "ion-steps/s", "cores": threads, "kind": "reference",
                 "sample": "unavailable: oracle/_ref/ref_harness was not built"}
-    probe = reference_sample(n, 20, threads)
-    rate = max(probe["ion_steps_per_s"], 1.0)
-    steps = int(min(max(budget_s * rate / n, 20), 100000))
-    r = reference_sample(n, steps, threads)
+    out = {}
+    for schedule in ("static", "faithful"):
+        probe = reference_sample(n, 20, threads, schedule)
+        rate = max(probe["ion_steps_per_s"], 1.0)
+        steps = int(min(max(budget_s * rate / n, 20), 100000))
+        out[schedule] = (reference_sample(n, steps, threads, schedule), steps)
+    (r, steps), (rf, steps_f) = out["static"], out["faithful"]
     return {"value": r["ion_steps_per_s"], "unit": "ion-steps/s", "cores": threads, "kind": "reference",
+            "cpu_model": cpu_model(),
             "sample": f"{n} ions x {steps} steps of the same physics (reference BorisStrategy + HSSCollisionHandler, "
-                      f"OpenMP over ions, {threads} threads, {r['wall_s']:.1f} s)"}
+                      f"best CPU form: one OpenMP loop over ions per step, {threads} threads, {r['wall_s']:.1f} s)",
+            "faithful_engine_order": {"value": rf["ion_steps_per_s"], "unit": "ion-steps/s",
+                                      "sample": f"{n} ions x {steps_f} steps, serial Boris loop then the OpenMP "
+                                                f"collision loop (the engine's order), {threads} threads, "
+                                                f"{rf['wall_s']:.1f} s"}}
 
 
 def run_reference_arm(args) -> None:
@@ -235,7 +283,9 @@ def run_reference_arm(args) -> None:
                  "config": {"workload": WORKLOAD, "ions": n, "engine_steps_per_bench_step": sub,
                             "sample": f"{n} of {N_IONS} ions per step (bounded CPU sample)"},
                  "cpu_baseline": {"value": value, "unit": "ion-steps/s", "cores": threads, "kind": "reference",
-                                  "sample": f"{n} ions x {sub} engine steps per bench step"},
+                                  "cpu_model": cpu_model(),
+                                  "sample": f"{n} ions x {sub} engine steps per bench step (best CPU form: one "
+                                            f"OpenMP loop over ions per step)"},
                  "e2e": {"value": value, "unit": "ion-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
     print(json.dumps(line))
 
@@ -297,11 +347,11 @@ def run_ours(args) -> None:
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def make_sim(prec, K=args.steps_per_launch, collision=capi.COLLISION_HSS):
+    def make_sim(prec, K=args.steps_per_launch, collision=capi.COLLISION_HSS, stepping=None):
         s = Simulation(ensembles, precision=prec, integrator=capi.INTEGRATOR_BORIS, collision=collision,
                        rng_seed=123, device=dev, steps_per_launch=K, block_size=args.block,
                        pending_threshold=args.pending, steps_per_vote=args.spv, use_graphs=int(args.graphs),
-                       stepping=STEPPING[args.stepping])
+                       stepping=STEPPING[args.stepping] if stepping is None else stepping)
         s.set_stream(stream.cuda_stream)
         if tf_domain is not None:
             s.apply_time_fields(0, tf_domain)
@@ -358,6 +408,24 @@ def run_ours(args) -> None:
     bpl = BYTES_PER_ION_LAUNCH[args.precision] * n_ions
     achieved = bpl / (avg_launch_ms * 1e-3) / 1e9
 
+    # The fused kernel moves the state through HBM once per 1000 steps, so
+    # it is bound by instruction issue; its roofline leads with the issue
+    # bound (from the ncu summary of the current kernel) and keeps the HBM
+    # fraction beside it.
+    prof = profile_figures(PROFILE_FUSED) if args.workload == "ims-1M" else {"fresh": False, "note": "not profiled"}
+    kname = f"k_step<{args.precision},boris,hss,uniform> fused {sim_K(None)} steps/launch"
+    hbm = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+           "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"], "bytes_per_launch": bpl,
+           "traffic": prof.get("dram_bytes_per_launch") if args.steps_per_launch == 1000 else None}
+    issue = issue_roofline(args, avg_launch_ms, clk, prof)
+    if issue is not None:
+        roofline = {**issue, "traffic": hbm["traffic"], "traffic_unit": "DRAM bytes per launch (ncu)",
+                    "kernel": kname, "avg_launch_ms": avg_launch_ms, "hbm": hbm, "profile": prof}
+    else:
+        roofline = {**hbm, "traffic_unit": "DRAM bytes per launch (ncu)", "kernel": kname,
+                    "avg_launch_ms": avg_launch_ms, "profile": prof,
+                    "note": "issue roofline needs a current ncu summary of this kernel"}
+
     # the same kernel in per-step form (one engine step per launch; state round-trips HBM every step)
     sim1 = make_sim(prec_id, K=1)
     for _ in range(3):
@@ -368,33 +436,48 @@ def run_ours(args) -> None:
     ach1 = bpl / (avg1 * 1e-3) / 1e9
     sim1.close()
 
-    # plain FP64 form of the same kernel (same algorithm), a shorter timed run
-    fp64_line = None
-    if args.precision != "fp64" and args.fp64_steps > 0:
-        s64 = make_sim(capi.PREC_FP64)
-        s64.advance(STEPS_PER_BENCH_STEP)
-        s64.upload(st0, ens_offsets=offsets, first_id=first_id)
-        torch.cuda.synchronize()
-        ms64, _, _, _, _ = timed_loop(s64, args.fp64_steps, STEPS_PER_BENCH_STEP, allreduce=False)
-        ms64 = parallel.max_over_ranks(ms64)
-        v64 = n_ions * STEPS_PER_BENCH_STEP * args.fp64_steps * world / (ms64 * 1e-3)
-        fp64_line = {"value": v64, "unit": "ion-steps/s", "steps": args.fp64_steps, "speedup_mixed_over_fp64": value / v64,
-                     "form": "the same null-collision algorithm in FP64 (skip clock, deferred collisions)"}
-        s64.close()
-        # the plain FP64 form: the reference's per-step algorithm (a
-        # Maxwell-Boltzmann neutral and an exp test for every ion every step)
-        sp = make_sim(capi.PREC_FP64, collision=capi.COLLISION_HSS_PLAIN)
-        sp.advance(STEPS_PER_BENCH_STEP)
-        sp.upload(st0, ens_offsets=offsets, first_id=first_id)
-        torch.cuda.synchronize()
-        n_plain = max(1, min(args.fp64_steps, 3))
-        msp, _, _, _, _ = timed_loop(sp, n_plain, STEPS_PER_BENCH_STEP, allreduce=False)
-        msp = parallel.max_over_ranks(msp)
-        vp = n_ions * STEPS_PER_BENCH_STEP * n_plain * world / (msp * 1e-3)
-        fp64_line["plain_fp64_form"] = {"value": vp, "unit": "ion-steps/s", "steps": n_plain,
-                                        "speedup_mixed_over_plain_fp64": value / vp,
-                                        "form": "reference per-step HSS (MB neutral + exp test every step), FP64"}
-        sp.close()
+    # The same workload in the other precision forms, each on a shorter
+    # timed run, labelled by algorithm: the event-to-event drift (the
+    # headline's algorithm) and the step-by-step loop in every precision, and
+    # the reference's per-step algorithm (a Maxwell-Boltzmann neutral and an
+    # exp test for every ion every step) in FP64.
+    forms = None
+    if args.precision == "mixed" and args.stepping == "events" and args.fp64_steps > 0:
+        def time_form(prec, stepping, n_timed, collision=capi.COLLISION_HSS):
+            sf = make_sim(prec, collision=collision, stepping=stepping)
+            sf.advance(STEPS_PER_BENCH_STEP)
+            sf.upload(st0, ens_offsets=offsets, first_id=first_id)
+            torch.cuda.synchronize()
+            msf, _, _, _, _ = timed_loop(sf, n_timed, STEPS_PER_BENCH_STEP, allreduce=False)
+            sf.close()
+            msf = parallel.max_over_ranks(msf)
+            return {"value": n_ions * STEPS_PER_BENCH_STEP * n_timed * world / (msf * 1e-3), "unit": "ion-steps/s",
+                    "steps": n_timed}
+        nf = args.fp64_steps
+        forms = {
+            "mixed_events": {"value": value, "unit": "ion-steps/s", "steps": args.steps,
+                             "form": "f32 v / f64 x, event-to-event drift (the headline)"},
+            "hilo_events": {**time_form(capi.PREC_MIXED_HILO, capi.STEPPING_EVENTS, nf),
+                            "form": "f32 v / compensated f32 hi-lo x, event-to-event drift"},
+            "fp64_events": {**time_form(capi.PREC_FP64, capi.STEPPING_EVENTS_ALL, nf),
+                            "form": "f64, event-to-event drift (same algorithm as the headline)"},
+            "mixed_per_step": {**time_form(capi.PREC_MIXED, capi.STEPPING_PER_STEP, nf),
+                               "form": "f32 v / f64 x, step-by-step loop with deferred collisions"},
+            "fp64_per_step": {**time_form(capi.PREC_FP64, capi.STEPPING_PER_STEP, nf),
+                              "form": "f64, step-by-step loop (same algorithm as mixed_per_step; the "
+                                      "bit-faithful FP64 form of the parity tests)"},
+            "plain_fp64": {**time_form(capi.PREC_FP64, capi.STEPPING_PER_STEP, max(1, min(nf, 3)),
+                                       collision=capi.COLLISION_HSS_PLAIN),
+                           "form": "f64, the reference's per-step HSS algorithm (MB neutral + exp test "
+                                   "every ion every step) with Philox: the plain FP64 GPU form"},
+        }
+        forms["speedups"] = {
+            "precision_only_events": value / forms["fp64_events"]["value"],
+            "precision_only_per_step": forms["mixed_per_step"]["value"] / forms["fp64_per_step"]["value"],
+            "hilo_over_fp64_events": forms["hilo_events"]["value"] / forms["fp64_events"]["value"],
+            "algorithm_and_precision_vs_plain_fp64": value / forms["plain_fp64"]["value"],
+            "algorithm_only_fp64_events_vs_plain": forms["fp64_events"]["value"] / forms["plain_fp64"]["value"],
+        }
 
     # end to end through the C ABI with host buffers: H2D state from pinned
     # memory, advance one snapshot interval, D2H state, every step
@@ -448,20 +531,12 @@ def run_ours(args) -> None:
                    "collision_fraction": stt["collisions"] / max(ion_steps / world, 1),
                    "cuda_graphs": bool(args.graphs), "autotuned": tuning, "stepping": args.stepping},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"],
-                     "traffic": NCU_TRAFFIC_PER_LAUNCH.get(args.precision) if args.steps_per_launch == 1000 else None,
-                     "traffic_unit": "bytes per launch (ncu)", "peak_source": peaks["source"],
-                     "kernel": f"k_step<{args.precision},boris,hss,uniform> fused {sim_K(None)} steps/launch",
-                     "bytes_per_launch": bpl, "avg_launch_ms": avg_launch_ms,
-                     "note": "fused K-step kernel: state crosses HBM once per launch, so it is instruction-issue "
-                             "bound, not HBM bound; see roofline_per_step and profiles/"},
-        "roofline_issue": issue_roofline(args, avg_launch_ms, clk),
+        "roofline": roofline,
         "roofline_per_step": {"bound": "hbm", "achieved": ach1, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                               "frac": ach1 / peaks["hbm_gbs"], "avg_launch_ms": avg1,
                               "kernel": f"k_step<{args.precision},boris,hss,uniform> 1 step/launch",
                               "ion_steps_per_s": n_ions / (avg1 * 1e-3)},
-        "fp64_form": fp64_line,
+        "precision_forms": forms,
         "e2e": {"value": e2e_value, "unit": "ion-steps/s", "h2d_bytes_per_step": 6 * 8 * n_ions,
                 "d2h_bytes_per_step": 6 * 8 * n_ions + n_ions, "steps": e2e_steps,
                 "path": f"icb_advance_host(1000 steps, {args.e2e_chunks} ion chunks): pinned host state in and out, "
@@ -708,7 +783,7 @@ def main():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--pending", type=int, default=0)
     ap.add_argument("--spv", type=int, default=0, help="collision-free steps between warp votes")
-    ap.add_argument("--stepping", choices=["events", "per-step"], default="events",
+    ap.add_argument("--stepping", choices=["events", "per-step", "events-all"], default="events",
                     help="float forms: event-to-event closed-form drift, or the step-by-step loop")
     ap.add_argument("--workload", choices=["ims-1M", "en-sweep", "fticr-sc", "ipm", "tims-1M"], default="ims-1M",
                     help="ims-1M: the 1,048,576-ion IMS run (default); en-sweep: the batched 64-ensemble E/N "

@@ -37,7 +37,7 @@ INTERP_LINEAR, INTERP_STEP, INTERP_CUBIC = 0, 1, 2
  CHANNEL_AC_Y_AMPLITUDE_V, CHANNEL_AC_Y_FREQUENCY_HZ, CHANNEL_AC_Y_RAMP, N_CHANNELS) = range(12)
 TIMS_RAMP_LINEAR, TIMS_RAMP_EXPONENTIAL = 0, 1
 SC_OFF, SC_P3M_ISOLATED, SC_PM_PERIODIC_REF = 0, 1, 2
-STEPPING_EVENTS, STEPPING_PER_STEP = 0, 1
+STEPPING_EVENTS, STEPPING_PER_STEP, STEPPING_EVENTS_ALL = 0, 1, 2
 MATH_NEG_LOG1M, MATH_NEG_LOG1M_CUDA, MATH_ONE_MINUS_EXP, MATH_ONE_MINUS_EXP_CUDA = 0, 1, 2, 3
 FLOW_CONSTANT, FLOW_AXIAL_UNIFORM, FLOW_AXIAL_PARABOLIC = 0, 1, 2
 MLP_HIDDEN, MLP_N_PARAMS = 64, 4417

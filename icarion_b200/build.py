@@ -92,6 +92,19 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     return LIB
 
 
+def kernel_source_hash(unit: str = "icb_step_mixed.cu") -> str:
+    """sha256 over one translation unit, every kernel header and its nvcc
+    flags: a profile taken of a kernel records this, and readers of the
+    profile's figures compare it with the current sources."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in [CSRC / unit] + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")):
+        h.update(f.name.encode())
+        h.update(f.read_bytes())
+    h.update(" ".join(ARCH + COMMON[:4] + PER_UNIT.get(unit, [])).encode())
+    return h.hexdigest()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--force", action="store_true")

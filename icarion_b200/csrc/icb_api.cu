@@ -871,7 +871,8 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
         p.n_steps = K;
         p.pend_threshold = h->pend;
         p.steps_per_vote = h->spv;
-        p.jumps = h->cfg.stepping == ICB_STEPPING_EVENTS ? 1u : 0u;
+        p.jumps = (h->cfg.stepping == ICB_STEPPING_EVENTS && !h->fp64()) || h->cfg.stepping == ICB_STEPPING_EVENTS_ALL
+                      ? 1u : 0u;
         p.subcycles = h->cfg.collision_subcycles > 1 ? static_cast<uint32_t>(h->cfg.collision_subcycles) : 1u;
         p.ens_base = static_cast<uint32_t>(e0);
         p.n_ens = static_cast<uint32_t>(ne);
@@ -1107,8 +1108,9 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
     h->pend = 10u;
     if (cfg->pending_threshold > 0) h->pend = static_cast<uint32_t>(std::min(cfg->pending_threshold, 32));
     if (cfg->steps_per_vote > 0) h->spv = static_cast<uint32_t>(std::min(cfg->steps_per_vote, 64));
-    if (cfg->stepping != ICB_STEPPING_EVENTS && cfg->stepping != ICB_STEPPING_PER_STEP)
-        return fail(ICB_ERR_INVALID_ARGUMENT, "stepping must be ICB_STEPPING_EVENTS or ICB_STEPPING_PER_STEP");
+    if (cfg->stepping != ICB_STEPPING_EVENTS && cfg->stepping != ICB_STEPPING_PER_STEP &&
+        cfg->stepping != ICB_STEPPING_EVENTS_ALL)
+        return fail(ICB_ERR_INVALID_ARGUMENT, "stepping must be ICB_STEPPING_EVENTS, _PER_STEP or _EVENTS_ALL");
     ICB_CUDA(cudaSetDevice(cfg->device));
     ICB_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     h->stream = h->own_stream;

@@ -16,12 +16,13 @@
 //              float offset (folded into the anchor at every warp vote).
 //   HILO       float velocity; position as a compensated float hi/lo pair.
 //
-// Two loops run the steps.  The event-to-event form (float precisions, Boris
-// in a uniform field without B; run_jumps below) moves each lane in one
-// closed-form update to its next clock event, exact domain check or the
-// launch end, and the warp then handles the events of all its lanes
-// together.  The step-by-step loop (FP64, RK4, other fields, births,
-// ICB_STEPPING_PER_STEP) defers collisions instead: a collision candidate
+// Two loops run the steps.  The event-to-event form (float precisions, and
+// FP64 on request; Boris in a uniform field without B; run_jumps below)
+// moves each lane in one closed-form update to its next clock event, exact
+// domain check or the launch end, and the warp then handles the events of
+// all its lanes together.  The step-by-step loop (FP64 by default, RK4,
+// other fields, births, ICB_STEPPING_PER_STEP) defers collisions instead:
+// a collision candidate
 // fires in ~10% of ion-steps; executed in place it would make almost every
 // warp-step run the expensive candidate branch with a few lanes active, so
 // a lane whose clock fires stops ("pending") while the other lanes keep
@@ -1364,8 +1365,9 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
     // the lane's own history, so results do not depend on launch shape.
     constexpr bool kSkip = (INTEG == kBoris) && (COLL != kCollNone) && (COLL != kCollHSSPlain);
     // closed-form event-to-event drift (run_jumps below)
+    // (FP64 only when the host asks for it: ICB_STEPPING_EVENTS_ALL)
     constexpr bool kJump = FUSED && (INTEG == kBoris) && (FIELD == kFieldUniform) && !MAG &&
-                           (PREC != kPrecFP64) && (COLL != kCollHSSPlain);
+                           (COLL != kCollHSSPlain);
     constexpr uint32_t kRefresh = 0x80000000u, kNeedRestart = 0xFFFFFFFFu;
     uint32_t g_next = kNeedRestart, g_start = 0u, nk = 0xFFFFFFFFu, H = 1u;
     R lam = R(0), dvmax = R(0), absu = R(0);

@@ -181,9 +181,13 @@ typedef struct icb_config {
  * closed-form update from one event (collision-clock event, exact domain
  * check, end of launch) to the next; PER_STEP applies the steps one by one.
  * Both draw the same random numbers at the same steps; their drifts differ
- * by float rounding.  FP64, RK4, non-uniform fields and the per-step plug
- * points always step one by one. */
-enum { ICB_STEPPING_EVENTS = 0, ICB_STEPPING_PER_STEP = 1 };
+ * by float rounding.  FP64 steps one by one under EVENTS (so that its pushes
+ * keep the reference's operation order); EVENTS_ALL moves FP64 from event
+ * to event too (the same algorithm as the float forms, for measuring what
+ * precision alone costs; its drifts differ from the step loop's by double
+ * rounding).  RK4, non-uniform fields and the per-step plug points always
+ * step one by one. */
+enum { ICB_STEPPING_EVENTS = 0, ICB_STEPPING_PER_STEP = 1, ICB_STEPPING_EVENTS_ALL = 2 };
 
 #define ICB_MAX_ENSEMBLES 256
 
