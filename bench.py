@@ -426,15 +426,40 @@ def run_ours(args) -> None:
                     "avg_launch_ms": avg_launch_ms, "profile": prof,
                     "note": "issue roofline needs a current ncu summary of this kernel"}
 
-    # the same kernel in per-step form (one engine step per launch; state round-trips HBM every step)
-    sim1 = make_sim(prec_id, K=1)
-    for _ in range(3):
+    # The per-step kernel (collision_test = PER_STEP: one engine step per
+    # launch, the state through HBM every step) on the same physics with
+    # N_PER_STEP ions, so that the state (37 B per ion in the float forms)
+    # is 5x the L2 and every launch streams it from HBM.  Algorithmic bytes
+    # per ion-step: positions 24 + velocities 12 (24 in FP64) + flag 1 read,
+    # positions and velocities written.
+    per_step = None
+    if args.workload == "ims-1M" and args.per_step_ions > 0:
+        n1 = args.per_step_ions
+        spec1 = cfg.species_spec(n1, 200.0 * cfg.AMU_TO_KG, cfg.ELEM_CHARGE_C,
+                                 {"type": "gaussian", "center": [0, 0, 0], "std": [5e-4] * 3},
+                                 {"type": "thermal", "temperature_K": 300.0})
+        st1 = generate_ions(123, [spec1])
+        b1 = {"fp64": 97, "mixed": 73, "hilo": 73}[args.precision]
+        sim1 = Simulation(ensembles, precision=prec_id, integrator=capi.INTEGRATOR_BORIS,
+                          collision=capi.COLLISION_HSS, rng_seed=123, device=dev,
+                          collision_test=capi.TEST_PER_STEP)
+        sim1.set_stream(stream.cuda_stream)
+        sim1.upload(st1, first_id=first_id)
+        del st1
         sim1.advance(10)
-    torch.cuda.synchronize()
-    r1 = sim1.advance(50)
-    avg1 = r1["step_kernel_ms"] / 50
-    ach1 = bpl / (avg1 * 1e-3) / 1e9
-    sim1.close()
+        torch.cuda.synchronize()
+        n_launch = 40
+        r1 = sim1.advance(n_launch)
+        torch.cuda.synchronize()
+        avg1 = r1["step_kernel_ms"] / n_launch
+        ach1 = b1 * n1 / (avg1 * 1e-3) / 1e9
+        sim1.close()
+        per_step = {"bound": "hbm", "achieved": ach1, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": ach1 / peaks["hbm_gbs"], "peak_source": peaks["source"], "avg_launch_ms": avg1,
+                    "kernel": f"k_step1<{args.precision},hss> (collision_test = PER_STEP), 1 step/launch",
+                    "ions": n1, "bytes_per_ion_step": b1, "launches_timed": n_launch,
+                    "ion_steps_per_s": n1 / (avg1 * 1e-3),
+                    "collision_fraction": r1["collisions"] / (n1 * n_launch)}
 
     # The same workload in the other precision forms, each on a shorter
     # timed run, labelled by algorithm: the event-to-event drift (the
@@ -532,10 +557,7 @@ def run_ours(args) -> None:
                    "cuda_graphs": bool(args.graphs), "autotuned": tuning, "stepping": args.stepping},
         "gpu_launches": launches,
         "roofline": roofline,
-        "roofline_per_step": {"bound": "hbm", "achieved": ach1, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                              "frac": ach1 / peaks["hbm_gbs"], "avg_launch_ms": avg1,
-                              "kernel": f"k_step<{args.precision},boris,hss,uniform> 1 step/launch",
-                              "ion_steps_per_s": n_ions / (avg1 * 1e-3)},
+        "roofline_per_step": per_step,
         "precision_forms": forms,
         "e2e": {"value": e2e_value, "unit": "ion-steps/s", "h2d_bytes_per_step": 6 * 8 * n_ions,
                 "d2h_bytes_per_step": 6 * 8 * n_ions + n_ions, "steps": e2e_steps,
@@ -792,6 +814,8 @@ def main():
     ap.add_argument("--autotune", action="store_true", help="pick the launch shape with icb_autotune first")
     ap.add_argument("--graphs", action="store_true", help="replay icb_advance through CUDA graphs")
     ap.add_argument("--fp64-steps", type=int, default=10)
+    ap.add_argument("--per-step-ions", type=int, default=16 * 1048576,
+                    help="ions of the per-step kernel's HBM roofline run (0 = skip)")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--e2e-chunks", type=int, default=24, help="ion chunks of the overlapped host path")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -38,6 +38,7 @@ INTERP_LINEAR, INTERP_STEP, INTERP_CUBIC = 0, 1, 2
 TIMS_RAMP_LINEAR, TIMS_RAMP_EXPONENTIAL = 0, 1
 SC_OFF, SC_P3M_ISOLATED, SC_PM_PERIODIC_REF = 0, 1, 2
 STEPPING_EVENTS, STEPPING_PER_STEP, STEPPING_EVENTS_ALL = 0, 1, 2
+TEST_CLOCK, TEST_PER_STEP = 0, 1
 MATH_NEG_LOG1M, MATH_NEG_LOG1M_CUDA, MATH_ONE_MINUS_EXP, MATH_ONE_MINUS_EXP_CUDA = 0, 1, 2, 3
 FLOW_CONSTANT, FLOW_AXIAL_UNIFORM, FLOW_AXIAL_PARABOLIC = 0, 1, 2
 MLP_HIDDEN, MLP_N_PARAMS = 64, 4417
@@ -84,7 +85,8 @@ class Config(C.Structure):
         ("n_ensembles", C.c_int32), ("ensembles", C.POINTER(EnsembleParams)), ("rng_seed", C.c_uint64),
         ("device", C.c_int32), ("block_size", C.c_int32), ("steps_per_launch", C.c_int32),
         ("pending_threshold", C.c_int32), ("use_graphs", C.c_int32), ("steps_per_vote", C.c_int32),
-        ("stepping", C.c_int32), ("collision_subcycles", C.c_int32), ("reserved", C.c_int32 * 4),
+        ("stepping", C.c_int32), ("collision_subcycles", C.c_int32), ("collision_test", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 

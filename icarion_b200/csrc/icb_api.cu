@@ -251,6 +251,7 @@ struct icb_handle {
     uint32_t pend = 0;      // 0 = precision default (set at create)
     uint32_t spv = 8;       // collision-free steps between warp votes
     bool shape_tuned = false;  // block / pend / spv chosen by icb_autotune
+    std::vector<double> sp_m, sp_q;   // per ensemble: shared ion mass / charge (0 = per ion)
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -886,6 +887,27 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
             p.tf_tab = h->tf_tab.p;
             p.tf_stride = tf_stride(h);
         }
+        if (h->cfg.collision_test == ICB_TEST_PER_STEP) {
+            // the per-step kernel: fused steps only, none of the per-launch extras
+            if (!(do_push && do_collide && do_finalize))
+                return fail(ICB_ERR_UNSUPPORTED, "the per-step collision test runs fused steps only (icb_advance)");
+            if (h->any_tf || h->sc)
+                return fail(ICB_ERR_UNSUPPORTED, "the per-step collision test has no time-dependent field or space charge");
+            for (int e = 0; e < ne; ++e) {
+                p.ens[e].sp_m = h->sp_m[static_cast<size_t>(e0 + e)];
+                p.ens[e].sp_q = h->sp_q[static_cast<size_t>(e0 + e)];
+            }
+            const dim3 grid1(grid_for(en - b, kStep1BlockHost));
+            cudaError_t err1;
+            switch (h->cfg.precision) {
+                case ICB_PREC_FP64: err1 = launch_step1_fp64(h->coll, p, grid1, st); break;
+                case ICB_PREC_MIXED: err1 = launch_step1_mixed(h->coll, p, grid1, st); break;
+                default: err1 = launch_step1_hilo(h->coll, p, grid1, st); break;
+            }
+            ++h->launches;
+            if (err1 != cudaSuccess) return fail(ICB_ERR_CUDA, "per-step kernel launch: %s", cudaGetErrorString(err1));
+            continue;
+        }
         const dim3 grid(grid_for(en - b, h->block)), block(static_cast<unsigned>(h->block));
         cudaError_t err;
         switch (h->cfg.precision) {
@@ -1111,6 +1133,18 @@ int icb_create(const icb_config* cfg, icb_handle** out) {
     if (cfg->stepping != ICB_STEPPING_EVENTS && cfg->stepping != ICB_STEPPING_PER_STEP &&
         cfg->stepping != ICB_STEPPING_EVENTS_ALL)
         return fail(ICB_ERR_INVALID_ARGUMENT, "stepping must be ICB_STEPPING_EVENTS, _PER_STEP or _EVENTS_ALL");
+    if (cfg->collision_test != ICB_TEST_CLOCK && cfg->collision_test != ICB_TEST_PER_STEP)
+        return fail(ICB_ERR_INVALID_ARGUMENT, "collision_test must be ICB_TEST_CLOCK or ICB_TEST_PER_STEP");
+    if (cfg->collision_test == ICB_TEST_PER_STEP) {
+        // the per-step kernel's physics (icb_step1.cuh)
+        if (cfg->integrator != ICB_INTEGRATOR_BORIS || (coll != kCollNone && coll != kCollHSS))
+            return fail(ICB_ERR_UNSUPPORTED, "the per-step collision test runs Boris with hard-sphere or no collisions");
+        if (h->field_kind != kFieldUniform || h->magnetic)
+            return fail(ICB_ERR_UNSUPPORTED, "the per-step collision test runs uniform electric fields without B");
+        for (const auto& c : h->ens_const)
+            if (c.flow) return fail(ICB_ERR_UNSUPPORTED, "the per-step collision test needs a constant or axial-uniform gas flow");
+        if (cfg->steps_per_launch <= 0) h->K = 1u;   // the state goes back to HBM after every step
+    }
     ICB_CUDA(cudaSetDevice(cfg->device));
     ICB_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     h->stream = h->own_stream;
@@ -1188,6 +1222,19 @@ int icb_upload_ions(icb_handle* h, uint64_t n,
     }
     for (uint64_t i = 0; i < n; ++i) {
         if (!(mass_kg[i] > 0.0)) return fail(ICB_ERR_INVALID_ARGUMENT, "ion %llu: mass must be > 0", static_cast<unsigned long long>(i));
+    }
+    if (h->cfg.collision_test == ICB_TEST_PER_STEP && birth_time_s)
+        return fail(ICB_ERR_UNSUPPORTED, "the per-step collision test has no births (birth_time_s must be NULL)");
+    // the species of each ensemble when all its ions share mass and charge
+    // (the per-step kernel then reads neither per-ion array)
+    h->sp_m.assign(ne, 0.0);
+    h->sp_q.assign(ne, 0.0);
+    for (size_t e = 0; e < ne; ++e) {
+        if (off[e + 1] == off[e]) continue;
+        const double m0 = mass_kg[off[e]], q0 = charge_C[off[e]];
+        bool same = true;
+        for (uint64_t i = off[e]; same && i < off[e + 1]; ++i) same = mass_kg[i] == m0 && charge_C[i] == q0;
+        if (same) { h->sp_m[e] = m0; h->sp_q[e] = q0; }
     }
     ICB_CUDA(cudaStreamSynchronize(h->stream));
     if (h->n != n) {
@@ -1654,6 +1701,8 @@ int icb_spacecharge_field(icb_handle* h, double* ex, double* ey, double* ez) {
 int icb_autotune(icb_handle* h, uint64_t trial_steps, icb_tuning* out) {
     if (int r = check_handle(h)) return r;
     if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
+    if (h->cfg.collision_test == ICB_TEST_PER_STEP)
+        return fail(ICB_ERR_UNSUPPORTED, "the per-step kernel has a fixed launch shape");
     if (trial_steps == 0) trial_steps = 500;
     if (trial_steps > 100000) return fail(ICB_ERR_INVALID_ARGUMENT, "trial_steps must be <= 100000");
     if (h->host_step + trial_steps >= (1ull << 31))

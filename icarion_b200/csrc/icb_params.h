@@ -28,6 +28,7 @@ enum CounterSlot : int {
 // Flags byte per ion.
 constexpr uint8_t kFlagActive = 1u;
 constexpr uint8_t kFlagBorn = 2u;
+constexpr uint8_t kFlagArrived = 4u;   // per-step kernel: arrival time recorded
 
 struct EnsConst {
     // Electric field E = E0 + G .* (x - c); with rf: E_x, E_y from the
@@ -67,6 +68,9 @@ struct EnsConst {
     float fug[3];
     int32_t flow;
     int32_t tf;        // time-dependent field of TimeField (waveforms, TIMS)
+    // the species of every ion of the ensemble (per-step kernel): mass and
+    // charge when all its ions share them, sp_m = 0 otherwise
+    double sp_m, sp_q;
 };
 
 // HSS gas mixture of one ensemble (read by the candidate step only):

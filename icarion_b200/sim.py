@@ -89,14 +89,17 @@ class Simulation:
     defaults), ``use_graphs``; ``stepping`` (STEPPING_EVENTS: the float forms
     move each ion from event to event in closed form; STEPPING_PER_STEP: the
     step-by-step loop); ``collision_subcycles`` (collision tests per step,
-    plain FP64 form only).
+    plain FP64 form only); ``collision_test`` (TEST_CLOCK: the collision clock
+    of the fused kernels; TEST_PER_STEP: the stateless per-step test of the
+    per-step kernel).
     """
 
     def __init__(self, ensembles: list[dict], precision: int = capi.PREC_MIXED,
                  integrator: int = capi.INTEGRATOR_BORIS, collision: int = capi.COLLISION_HSS,
                  rng_seed: int = 123, device: int = 0, block_size: int = 0, steps_per_launch: int = 0,
                  pending_threshold: int = 0, use_graphs: int = 0, steps_per_vote: int = 0,
-                 stepping: int = capi.STEPPING_EVENTS, collision_subcycles: int = 0):
+                 stepping: int = capi.STEPPING_EVENTS, collision_subcycles: int = 0,
+                 collision_test: int = capi.TEST_CLOCK):
         self._lib = capi.lib()
         self.n_ens = len(ensembles)
         self._ens = (capi.EnsembleParams * self.n_ens)(*[cfgmod.to_struct(e) for e in ensembles])
@@ -115,6 +118,7 @@ class Simulation:
         cfg.steps_per_vote = steps_per_vote
         cfg.stepping = stepping
         cfg.collision_subcycles = collision_subcycles
+        cfg.collision_test = collision_test
         self._h = C.c_void_p()
         capi.check(self._lib.icb_create(C.byref(cfg), C.byref(self._h)))
         self.ensembles = ensembles

@@ -173,8 +173,23 @@ typedef struct icb_config {
      * collision test m times per step with dt/m at the pushed position.
      * Needs ICB_COLLISION_HSS_PLAIN; 0 or 1 = one test per step. */
     int32_t collision_subcycles;
-    int32_t reserved[4];
+    int32_t collision_test;    /* ICB_TEST_* (0 = the collision clock) */
+    int32_t reserved[3];
 } icb_config;
+
+/* How the null-collision candidates of hard-sphere collisions are found.
+ * CLOCK: a collision clock carried per ion between launches (the skip clock
+ * for Boris, a survival product for RK4); the fused kernels.  PER_STEP: a
+ * stateless test every step (Philox(id, step) against Q = A (|v - u| +
+ * <|th|>) of the current velocity), run by the per-step kernel, which moves
+ * only positions, velocities and the flag byte through HBM each step:
+ * the form for an engine that hands the state back every step.  Same
+ * per-step collision law; the two draw different random numbers.  PER_STEP
+ * runs Boris in a uniform electric field without B, hard-sphere or no
+ * collisions, a single gas with constant or axial-uniform flow, no births,
+ * no space charge and no time-dependent field; its steps_per_launch
+ * defaults to 1. */
+enum { ICB_TEST_CLOCK = 0, ICB_TEST_PER_STEP = 1 };
 
 /* Stepping of the fused float forms (MIXED, MIXED_HILO) with Boris in a
  * uniform field and no magnetic field: EVENTS moves each ion in one

@@ -1207,7 +1207,8 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
     const int clocked = (collision == 2 || collision == 3 || collision == 4 || collision == 5 || collision == 7);
     if (clocked && (!clk_S || !clk_U)) return 1;
     if (clocked && integrator == 0 && (!clk_next || !clk_start)) return 1;
-    if ((collision == 3 || collision == 4 || collision == 5 || collision == 7) && integrator != 0) return 1;
+    if ((collision == 3 || collision == 4 || collision == 5 || collision == 7 || collision == 8) && integrator != 0)
+        return 1;
     if (collision == 7 && !g_ehss_atoms) return 1;
     if (collision == 5 && (d->n_gas < 2 || d->n_gas > 8)) return 1;
     if (collision == 4 && !g_ipm_tab) return 1;
@@ -1318,6 +1319,22 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                             }
                             skip_restart(&sk, &Gi, v, gs + 1u, &ov);
                             ovf_tot += ov;
+                        }
+                    } else if (collision == 8) {
+                        /* the per-step kernel's stateless test: a candidate
+                         * when Philox(id, step, 0).x < Q = A |v - u| + A <|th|>,
+                         * then the per-step clock's candidate with b exact */
+                        const uint32_t gs = (uint32_t)(step0 + (uint64_t)k);
+                        uint32_t r0[4];
+                        philox_words(seed, id, gs, 0u, r0);
+                        const double w[3] = {v[0] - Gi.ug[0], v[1] - Gi.ug[1], v[2] - Gi.ug[2]};
+                        const double b = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+                        double Q = Gi.A * b + Gi.Amean;
+                        if (Q > 1.0) { Q = 1.0; ++ovf_tot; }
+                        if (u32_to_unit(r0[0]) < Q) {
+                            double clk = 0.0;
+                            ++cand_tot;
+                            if (nullcoll_candidate(&Gi, v, m, seed, id, gs, 0, &clk, 0.0, b, 0) == 2) ++coll_tot;
                         }
                     } else if (collision == 2) {
                         uint64_t ov = 0;

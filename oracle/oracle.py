@@ -362,7 +362,8 @@ def run(domain: dict, state: dict, n_steps: int, *, integrator: int = 0, collisi
     set_ipm_table), 5 HSS gas mixture (Boris, skip clock), 6 the reference's
     per-step HSS form with Philox words (no clock; ``subcycles`` collision
     sub-steps of dt/m per step), 7 EHSS on the geometry of set_ehss (Boris,
-    skip clock).  ``time_field`` holds the harness's waveform / TIMS keys
+    skip clock), 8 null-collision HSS with the per-step kernel's stateless
+    test (Boris; no clock state).  ``time_field`` holds the harness's waveform / TIMS keys
     (wave_*, tims*) of the domain; the default clears them."""
     d = domain_struct(domain)
     lib().orc_set_subcycles(int(subcycles))
