@@ -269,6 +269,23 @@ void mlp_pack(const float* params, std::vector<uint32_t>& frag, std::vector<floa
                 frag[base] = bf16_bits_host(row[k0]) | (bf16_bits_host(row[k0 + 1]) << 16);
                 frag[base + 1] = bf16_bits_host(row[k0 + 8]) | (bf16_bits_host(row[k0 + 9]) << 16);
             }
+    // layer 1 as B fragments: (W1[n][0], W1[n][0]), (W1[n][1], W1[n][1]),
+    // (b1[n] hi, b1[n] lo), 0 for t = 0..3
+    for (int nt = 0; nt < 8; ++nt)
+        for (int lane = 0; lane < 32; ++lane) {
+            const int g = lane >> 2, t = lane & 3;
+            const int n = 8 * nt + g;
+            uint32_t w = 0u;
+            if (t < 2) {
+                const uint32_t b = bf16_bits_host(params[kMlpOffW1 + 2 * n + t]);
+                w = b | (b << 16);
+            } else if (t == 2) {
+                const float b1 = params[kMlpOffB1 + n];
+                const float hi = bf16_round_host(b1);
+                w = bf16_bits_host(hi) | (bf16_bits_host(b1 - hi) << 16);
+            }
+            frag[static_cast<size_t>(kMlpFragW1Off) + static_cast<size_t>(nt) * 32 + lane] = w;
+        }
     fblock.assign(kMlpFSize, 0.f);
     for (int k = 0; k < 128; ++k) fblock[kMlpFW1 + k] = bf16_round_host(params[kMlpOffW1 + k]);
     for (int k = 0; k < kMlpH; ++k) {

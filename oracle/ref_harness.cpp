@@ -37,6 +37,7 @@
 //            moments (20 per snapshot, layout of ICB_N_MOMENTS) of the
 //            active ions; slots 14..19 are displacement moments from the
 //            positions after ref_step steps.
+//            sc=direct softening=: the reference's direct space charge.
 //            collision=ipm ipm_samples=<file>: the reference's
 //            InteractionPotentialCollisionHandler (random orientation mode)
 //            with the offline sample set of <file> for species "ion"
@@ -485,6 +486,15 @@ int mode_run(const Args& a) {
     if (d.fields.magnetic.enabled && integ != "boris")
         reg->add_force(std::make_unique<physics::MagneticFieldForce>(d.fields.magnetic));
     reg->set_field_model(field_model.get());
+    // sc=direct: the reference's O(N^2) space charge (SpaceChargeDirectModel,
+    // softening as SpaceChargeModelFactory.h:26), updated once per step
+    // before the ions are prepared (SimulationEngineLifecycle.cpp:16-32) and
+    // added as q E_sc by the force registry (ForceRegistry.cpp:76-87)
+    std::shared_ptr<physics::SpaceChargeDirectModel> sc_model;
+    if (str(a, "sc", "none") == "direct") {
+        sc_model = std::make_shared<physics::SpaceChargeDirectModel>(num(a, "softening", 1e-10));
+        reg->set_space_charge_model(sc_model);
+    }
     std::vector<std::shared_ptr<physics::ForceRegistry>> regs{reg};
     config::CylindricalGeometry geom(d);
 
@@ -540,6 +550,7 @@ int mode_run(const Args& a) {
     double t = num(a, "t0", 0.0);
     const auto wall0 = std::chrono::steady_clock::now();
     for (int64_t k = 0; k < steps; ++k) {
+        if (sc_model) sc_model->update_fields(ens, t);
         // prepare_ions_for_integration
         for (int64_t i = 0; i < n; ++i) {
             if (!active[i]) { dom[static_cast<size_t>(i)] = -1; continue; }
