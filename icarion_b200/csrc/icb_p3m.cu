@@ -23,6 +23,7 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <memory>
@@ -291,7 +292,7 @@ constexpr int kPPTable = 4096;
 // Field of every ion: CIC interpolation of the mesh field (+ particle-
 // particle correction).  Thread s handles the ion in sorted slot s.
 template <bool REF_WEIGHTS, class GT>
-__global__ void __launch_bounds__(256) k_sc_gather(MeshGeom g, PPParams pp, const double4* __restrict__ ps,
+__global__ void __launch_bounds__(256, 4) k_sc_gather(MeshGeom g, PPParams pp, const double4* __restrict__ ps,
                             const float4* __restrict__ pf,
                             const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                             const uint32_t* __restrict__ start, uint32_t n, const GT* __restrict__ gx,
@@ -307,79 +308,129 @@ __global__ void __launch_bounds__(256) k_sc_gather(MeshGeom g, PPParams pp, cons
         }
         __syncthreads();
     }
+    // Every lane of a warp reaches the particle-particle loops (they use
+    // warp-wide ranges); lanes without an ion inside the mesh take part with
+    // empty ranges.
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    const uint32_t i = vals[s];
-    const uint32_t key = keys[s];
-    if (key >= g.ncell) {
-        ex[i] = 0.0; ey[i] = 0.0; ez[i] = 0.0;
+    const bool in_range = s < n;
+    const uint32_t i = in_range ? vals[s] : 0u;
+    const uint32_t key = in_range ? keys[s] : g.ncell;
+    const bool act = key < g.ncell;
+    if (!REF_WEIGHTS && pp.on && pp.use_float && __all_sync(0xffffffffu, !act)) {
+        if (in_range) { ex[i] = 0.0; ey[i] = 0.0; ez[i] = 0.0; }
         return;
     }
-    const int ck = static_cast<int>(key % g.n2);
-    const uint32_t t = key / g.n2;
+    if (!act && (REF_WEIGHTS || !pp.on || !pp.use_float)) {
+        if (in_range) { ex[i] = 0.0; ey[i] = 0.0; ez[i] = 0.0; }
+        return;
+    }
+    const uint32_t keyc = act ? key : 0u;
+    const int ck = static_cast<int>(keyc % g.n2);
+    const uint32_t t = keyc / g.n2;
     const int cj = static_cast<int>(t % g.n1);
     const int ci = static_cast<int>(t / g.n1);
-    const double4 pi4 = ps[s];
-    const double xi = pi4.x, yi = pi4.y, zi = pi4.z;
-    const double fx = (xi - g.lo0) * g.ih0 - ci;
-    const double fy = (yi - g.lo1) * g.ih1 - cj;
-    const double fz = (zi - g.lo2) * g.ih2 - ck;
     double E[3] = {0.0, 0.0, 0.0};
-    const GT* grid[3] = {gx, gy, gz};
-    // corners in the reference's order w000, w100, w010, w110, w001, ... (x fastest)
-    for (int oz = 0; oz < 2; ++oz) {
-        for (int oy = 0; oy < 2; ++oy) {
-            for (int ox = 0; ox < 2; ++ox) {
-                double w;
-                if (REF_WEIGHTS) {
-                    w = static_cast<double>(cic_w<float>(ox, oy, oz, static_cast<float>(fx), static_cast<float>(fy),
-                                                         static_cast<float>(fz)));
-                } else {
-                    w = cic_w<double>(ox, oy, oz, fx, fy, fz);
-                }
-                const size_t node = (static_cast<size_t>(ci + ox) * g.m1 + static_cast<size_t>(cj + oy)) * g.m2 +
-                                    static_cast<size_t>(ck + oz);
+    const double4 pi4 = act ? ps[s] : make_double4(0.0, 0.0, 0.0, 0.0);
+    const double xi = pi4.x, yi = pi4.y, zi = pi4.z;
+    if (act) {
+        const double fx = (xi - g.lo0) * g.ih0 - ci;
+        const double fy = (yi - g.lo1) * g.ih1 - cj;
+        const double fz = (zi - g.lo2) * g.ih2 - ck;
+        const GT* grid[3] = {gx, gy, gz};
+        // corners in the reference's order w000, w100, w010, w110, w001, ... (x fastest)
+        for (int oz = 0; oz < 2; ++oz) {
+            for (int oy = 0; oy < 2; ++oy) {
+                for (int ox = 0; ox < 2; ++ox) {
+                    double w;
+                    if (REF_WEIGHTS) {
+                        w = static_cast<double>(cic_w<float>(ox, oy, oz, static_cast<float>(fx), static_cast<float>(fy),
+                                                             static_cast<float>(fz)));
+                    } else {
+                        w = cic_w<double>(ox, oy, oz, fx, fy, fz);
+                    }
+                    const size_t node = (static_cast<size_t>(ci + ox) * g.m1 + static_cast<size_t>(cj + oy)) * g.m2 +
+                                        static_cast<size_t>(ck + oz);
 #pragma unroll
-                for (int c = 0; c < 3; ++c) E[c] += w * static_cast<double>(grid[c][node]);
+                    for (int c = 0; c < 3; ++c) E[c] += w * static_cast<double>(grid[c][node]);
+                }
             }
         }
-    }
-    if (REF_WEIGHTS) {
+        if (REF_WEIGHTS) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) E[c] = static_cast<double>(static_cast<float>(E[c]));
+            for (int c = 0; c < 3; ++c) E[c] = static_cast<double>(static_cast<float>(E[c]));
+        }
     }
     if (!REF_WEIGHTS && pp.on) {
-        const float4 own = pf[s];
+        const float4 own = act ? pf[s] : make_float4(0.f, 0.f, 0.f, 0.f);
         const float fxi = own.x, fyi = own.y, fzi = own.z;
         const int x0 = max(ci - pp.r0, 0), x1 = min(ci + pp.r0, g.n0 - 2);
         const int y0 = max(cj - pp.r1, 0), y1 = min(cj + pp.r1, g.n1 - 2);
         const int z0 = max(ck - pp.r2, 0), z1 = min(ck + pp.r2, g.n2 - 2);
         if (pp.use_float) {
-            // float arithmetic on positions relative to the mesh origin
+            // float arithmetic on positions relative to the mesh origin.
+            // Each (cx, cy) column contributes the cells whose z interval
+            // reaches within r_c of the ion given the column's distance in x
+            // and y (lower bounds, padded for rounding), and the warp walks
+            // the union of its lanes' slot ranges together when they overlap
+            // (every lane reads the same pair: one broadcast load, no
+            // divergence), else each lane walks its own.  Pairs outside a
+            // lane's range or outside (min_d, r_c) add exactly nothing, so
+            // the sums equal a walk over every pair of the 5x5x5 cells.
+            const unsigned full = 0xffffffffu;
             float Ef[3] = {0.f, 0.f, 0.f};
             const float kc = static_cast<float>(kCoulomb);
-            for (int cx = x0; cx <= x1; ++cx) {
-                for (int cy = y0; cy <= y1; ++cy) {
-                    const uint32_t row = (static_cast<uint32_t>(cx) * g.n1 + static_cast<uint32_t>(cy)) * g.n2;
-                    const uint32_t sa = start[row + static_cast<uint32_t>(z0)];
-                    const uint32_t sb = start[row + static_cast<uint32_t>(z1) + 1u];
-                    for (uint32_t s2 = sa; s2 < sb; ++s2) {
-                        // every pair takes the same instructions; pairs outside
-                        // (min_d, r_c) or the ion itself add nothing (select)
-                        const float4 qf = pf[s2];
-                        const float dx = fxi - qf.x, dy = fyi - qf.y, dz = fzi - qf.z;
-                        const float r2 = dx * dx + dy * dy + dz * dz;
-                        const bool near = s2 != s && r2 < pp.rc2f && r2 >= pp.min_d2f;
-                        const float rinv = rsqrtf(r2);
-                        const float u = r2 * rinv * pp.inv_drf;
-                        const int kt = max(min(static_cast<int>(u), kPPTable - 1), 0);
-                        const float fr = u - static_cast<float>(kt);
-                        const float L = fmaf(fr, tabf[kt + 1] - tabf[kt], tabf[kt]);
-                        // kc (1 / (r^2 + eps^2) - L / r^2) / r q_j
-                        const float sc = kc * (__fdividef(1.f, r2 + pp.eps2f) - L * rinv * rinv) * rinv * qf.w;
-                        Ef[0] += near ? dx * sc : 0.f;
-                        Ef[1] += near ? dy * sc : 0.f;
-                        Ef[2] += near ? dz * sc : 0.f;
+            const float h0 = static_cast<float>(1.0 / g.ih0), h1 = static_cast<float>(1.0 / g.ih1);
+            const float ih2 = static_cast<float>(g.ih2);
+            const float rcpad = pp.rc2f * 1.0001f;
+            const float zpad = 1e-4f * static_cast<float>(1.0 / g.ih2);
+            auto pair = [&](const float4& qf, bool take) {
+                const float dx = fxi - qf.x, dy = fyi - qf.y, dz = fzi - qf.z;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                const bool near = take && r2 < pp.rc2f && r2 >= pp.min_d2f;
+                const float rinv = rsqrtf(r2);
+                const float u = r2 * rinv * pp.inv_drf;
+                const int kt = max(min(static_cast<int>(u), kPPTable - 1), 0);
+                const float fr = u - static_cast<float>(kt);
+                const float L = fmaf(fr, tabf[kt + 1] - tabf[kt], tabf[kt]);
+                // kc (1 / (r^2 + eps^2) - L / r^2) / r q_j
+                const float sc = kc * (__fdividef(1.f, r2 + pp.eps2f) - L * rinv * rinv) * rinv * qf.w;
+                Ef[0] += near ? dx * sc : 0.f;
+                Ef[1] += near ? dy * sc : 0.f;
+                Ef[2] += near ? dz * sc : 0.f;
+            };
+            const int wx0 = __reduce_min_sync(full, act ? x0 : INT_MAX);
+            const int wx1 = __reduce_max_sync(full, act ? x1 : INT_MIN);
+            const int wy0 = __reduce_min_sync(full, act ? y0 : INT_MAX);
+            const int wy1 = __reduce_max_sync(full, act ? y1 : INT_MIN);
+            for (int cx = wx0; cx <= wx1; ++cx) {
+                const float dxa = fmaxf(0.f, fmaxf(static_cast<float>(cx) * h0 - fxi,
+                                                   fxi - static_cast<float>(cx + 1) * h0));
+                for (int cy = wy0; cy <= wy1; ++cy) {
+                    uint32_t sa = 0u, sb = 0u;
+                    if (act && cx >= x0 && cx <= x1 && cy >= y0 && cy <= y1) {
+                        const float dya = fmaxf(0.f, fmaxf(static_cast<float>(cy) * h1 - fyi,
+                                                           fyi - static_cast<float>(cy + 1) * h1));
+                        const float rem = rcpad - dxa * dxa - dya * dya;
+                        if (rem > 0.f) {
+                            const float dzm = sqrtf(rem) + zpad;
+                            const int za = max(z0, static_cast<int>(floorf((fzi - dzm) * ih2)));
+                            const int zb = min(z1, static_cast<int>(floorf((fzi + dzm) * ih2)));
+                            if (za <= zb) {
+                                const uint32_t row = (static_cast<uint32_t>(cx) * g.n1 + static_cast<uint32_t>(cy)) * g.n2;
+                                sa = start[row + static_cast<uint32_t>(za)];
+                                sb = start[row + static_cast<uint32_t>(zb) + 1u];
+                            }
+                        }
+                    }
+                    const bool has = sb > sa;
+                    const uint32_t usa = __reduce_min_sync(full, has ? sa : 0xffffffffu);
+                    const uint32_t usb = __reduce_max_sync(full, has ? sb : 0u);
+                    if (usb <= usa) continue;                  // no lane has pairs in this column
+                    const uint32_t len = __reduce_max_sync(full, sb - sa);
+                    if (usb - usa <= 2u * len + 8u) {
+                        for (uint32_t s2 = usa; s2 < usb; ++s2) pair(pf[s2], s2 >= sa && s2 < sb && s2 != s);
+                    } else {
+                        for (uint32_t s2 = sa; s2 < sb; ++s2) pair(pf[s2], s2 != s);
                     }
                 }
             }
@@ -412,6 +463,10 @@ __global__ void __launch_bounds__(256) k_sc_gather(MeshGeom g, PPParams pp, cons
                 }
             }
         }
+    }
+    if (!act) {
+        if (in_range) { ex[i] = 0.0; ey[i] = 0.0; ez[i] = 0.0; }
+        return;
     }
     ex[i] = E[0]; ey[i] = E[1]; ez[i] = E[2];
 }
