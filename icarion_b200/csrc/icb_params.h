@@ -89,7 +89,12 @@ struct MixConst {
 // (ValueOrWaveform) and the TIMS axial ramp, evaluated in FP64 at every
 // field evaluation.  Lives in device memory, one per ensemble (global index).
 constexpr int kMaxWavePoints = 64;
-constexpr int kTfRowScalars = 8;     // doubles per step and stage of the per-step field table
+// Per-step field table: per step and stage, kTfScalars doubles (the FP64
+// scalars) then kTfFloatDoubles doubles holding 8 floats for the float
+// forms (the same values rounded once when the table is built).
+constexpr int kTfScalarsFP64 = 8;
+constexpr int kTfFloatDoubles = 4;
+constexpr int kTfRowScalars = kTfScalarsFP64 + kTfFloatDoubles;   // doubles per step and stage
 enum WaveKind : int32_t {
     kWaveConstant = 0, kWaveLinear = 1, kWaveQuadratic = 2, kWaveExponential = 3,
     kWaveSinusoidal = 4, kWavePWM = 5, kWavePulsed = 6, kWaveArbitrary = 7

@@ -261,6 +261,15 @@ struct Consts {
     const double* tftab;     // its per-step scalars for this launch (k_tf_table)
     const double* tfrow;     // ... of the current step
     uint32_t tfstride;       // doubles per row
+    // the time-dependent field's constants read by the float forms each
+    // step: instrument, uniform TIMS fields, final-profile flag
+    int tfc_inst;
+    float tfc_ei, tfc_ef;
+    bool tfc_final;
+    // the lane's current TIMS profile segment (z in (ts_lo, ts_hi]):
+    // mode 0 uniform, 1 constant (outside the nodes), 2 interpolated
+    mutable float ts_lo, ts_hi, ts_z0, ts_idz, ts_vi, ts_dvi, ts_vf, ts_dvf;
+    mutable int ts_mode;
 };
 
 template <class R, int FIELD, bool MAG>
@@ -442,7 +451,10 @@ __device__ __forceinline__ double tims_sample(const double* zn, const double* va
 //   s[2] IMS / QuadrupoleRF axial / L, LQIT axial / L^2, TIMS ramp f(t)
 //   s[3] 1 if the axial term applies        s[4], s[5] AC drive E_x, E_y
 //   s[6], s[7] -2 U / r0^2, 2 U / r0^2 (the float forms' coefficients)
-constexpr int kTfScalars = kTfRowScalars;
+// followed by the float block (8 floats): s[6], s[7], s[2], s[4], s[5] as
+// floats, 1.0f / 0.0f for s[1] != 0 and s[3] != 0, and 0.
+constexpr int kTfScalars = kTfScalarsFP64;
+constexpr int kTfFloats = 8;
 static __device__ __noinline__ void tf_scalars(const TimeField& F, double t, double s[kTfScalars]) {
     const double rfv = wave_eval(F.ch[kChRfV], t);
     for (int j = 0; j < kTfScalars; ++j) s[j] = 0.0;
@@ -503,31 +515,86 @@ __device__ __forceinline__ float tims_sample_f(const float* zn, const float* val
 }
 
 // The field at one ion from the step's scalars s (tf_scalars): FP64 in the
-// reference's operation order; the float forms in float from the per-step
-// coefficients.
-template <class R, class Pos>
-__device__ __forceinline__ void tf_apply(const TimeField& F, const Pos& x, const double* s, R E[3]) {
-    if constexpr (sizeof(R) == 4) {
-        const bool local = F.inst >= 3;
-        float ex = 0.0f, ey = 0.0f, ez = 0.0f;
-        if (s[1] != 0.0) {
-            ex = x.template rel<float>(0, local ? F.ox : 0.0) * static_cast<float>(s[6]);
-            ey = x.template rel<float>(1, local ? F.oy : 0.0) * static_cast<float>(s[7]);
+// reference's operation order; the float forms in float from the row's float
+// block, with the field's constants held by the lane (Consts: tfc_*) and the
+// TIMS profiles' current segment cached per lane (the same expression as
+// tims_sample_f over the cached nodes, so the same values).
+template <class R>
+__device__ __forceinline__ float tims_segment_sample(const Consts<R>& k, float z) {
+    if (!(z > k.ts_lo && z <= k.ts_hi)) {
+        const TimeField& F = *k.tf;
+        const int n = F.tims_nodes;
+        if (n == 0) {
+            k.ts_lo = -INFINITY; k.ts_hi = INFINITY; k.ts_mode = 0;
+        } else if (!(z > F.tims_zf[0])) {
+            k.ts_lo = -INFINITY; k.ts_hi = F.tims_zf[0]; k.ts_mode = 1;
+            k.ts_vi = F.tims_pif[0]; k.ts_vf = F.tims_final_profile ? F.tims_pff[0] : static_cast<float>(F.tims_ef);
+        } else if (z >= F.tims_zf[n - 1]) {
+            // z >= z[n-1] samples the last node; a z just below it lands in
+            // the last interval again, so the segment starts at z[n-1] itself
+            k.ts_lo = nextafterf(F.tims_zf[n - 1], -INFINITY); k.ts_hi = INFINITY; k.ts_mode = 1;
+            k.ts_vi = F.tims_pif[n - 1];
+            k.ts_vf = F.tims_final_profile ? F.tims_pff[n - 1] : static_cast<float>(F.tims_ef);
+        } else {
+            int lo = 0, hi = n;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (F.tims_zf[mid] < z) lo = mid + 1; else hi = mid;
+            }
+            const int i0 = lo - 1;
+            k.ts_lo = F.tims_zf[i0];
+            k.ts_hi = lo == n - 1 ? nextafterf(F.tims_zf[lo], -INFINITY) : F.tims_zf[lo];
+            k.ts_mode = 2;
+            k.ts_z0 = F.tims_zf[i0];
+            k.ts_idz = F.tims_idz[i0];
+            k.ts_vi = F.tims_pif[i0];
+            k.ts_dvi = F.tims_pif[lo] - F.tims_pif[i0];
+            if (F.tims_final_profile) {
+                k.ts_vf = F.tims_pff[i0];
+                k.ts_dvf = F.tims_pff[lo] - F.tims_pff[i0];
+            } else {
+                k.ts_vf = static_cast<float>(F.tims_ef);
+                k.ts_dvf = 0.0f;
+            }
         }
-        if (F.inst == 4) {
+    }
+    return z;
+}
+
+template <class R, class Pos>
+__device__ __forceinline__ void tf_apply(const Consts<R>& k, const TimeField& F, const Pos& x, const double* s,
+                                         R E[3]) {
+    if constexpr (sizeof(R) == 4) {
+        const float4 f0 = *reinterpret_cast<const float4*>(s + kTfScalars);
+        const float4 f1 = *reinterpret_cast<const float4*>(s + kTfScalars + 2);
+        float ex = 0.0f, ey = 0.0f, ez = 0.0f;
+        const bool local = k.tfc_inst >= 3;   // LQIT, TIMS: x, y from the cylinder axis
+        if (f1.y != 0.0f) {          // RF term
+            ex = x.template rel<float>(0, local ? F.ox : 0.0) * f0.x;
+            ey = x.template rel<float>(1, local ? F.oy : 0.0) * f0.y;
+        }
+        if (k.tfc_inst == 4) {
             const float zl = x.template rel<float>(2, F.oz);
-            const float f = static_cast<float>(s[2]);
-            const float ei = tims_sample_f(F.tims_zf, F.tims_pif, F.tims_idz, F.tims_nodes, zl,
-                                           static_cast<float>(F.tims_ei));
-            const float ef = tims_sample_f(F.tims_zf, F.tims_pff, F.tims_idz, F.tims_final_profile ? F.tims_nodes : 0,
-                                           zl, static_cast<float>(F.tims_ef));
-            ez = fmaf(f, ef - ei, ei);
-        } else if (F.inst == 3) {
-            ex += static_cast<float>(s[4]);
-            ey += static_cast<float>(s[5]);
-            if (s[3] != 0.0) ez = static_cast<float>(-2.0 * s[2]) * x.template rel<float>(2, F.oz + 0.5 * F.L);
-        } else if (s[3] != 0.0) {
-            ez = static_cast<float>(s[2]);
+            tims_segment_sample<R>(k, zl);
+            float ei, ef;
+            if (k.ts_mode == 2) {
+                const float alpha = (zl - k.ts_z0) * k.ts_idz;
+                ei = fmaf(alpha, k.ts_dvi, k.ts_vi);
+                ef = k.tfc_final ? fmaf(alpha, k.ts_dvf, k.ts_vf) : k.ts_vf;
+            } else if (k.ts_mode == 1) {
+                ei = k.ts_vi;
+                ef = k.ts_vf;
+            } else {
+                ei = k.tfc_ei;
+                ef = k.tfc_ef;
+            }
+            ez = fmaf(f0.z, ef - ei, ei);
+        } else if (k.tfc_inst == 3) {
+            ex += f0.w;
+            ey += f1.x;
+            if (f1.z != 0.0f) ez = (-2.0f * f0.z) * x.template rel<float>(2, F.oz + 0.5 * F.L);
+        } else if (f1.z != 0.0f) {
+            ez = f0.z;
         }
         E[0] = ex; E[1] = ey; E[2] = ez;
         return;
@@ -584,11 +651,23 @@ __global__ void k_tf_table(const StepParams p, double* tab, double* tseq, uint32
         double* row = T + static_cast<size_t>(k) * stride;
         const double t = ts[k];
         double sc[kTfScalars];
+        auto put = [&](double* r) {
+            for (int j = 0; j < kTfScalars; ++j) r[j] = sc[j];
+            float* f = reinterpret_cast<float*>(r + kTfScalars);
+            f[0] = static_cast<float>(sc[6]);
+            f[1] = static_cast<float>(sc[7]);
+            f[2] = static_cast<float>(sc[2]);
+            f[3] = static_cast<float>(sc[4]);
+            f[4] = static_cast<float>(sc[5]);
+            f[5] = sc[1] != 0.0 ? 1.0f : 0.0f;
+            f[6] = sc[3] != 0.0 ? 1.0f : 0.0f;
+            f[7] = 0.0f;
+        };
         tf_scalars(F, t, sc);
-        for (int j = 0; j < kTfScalars; ++j) row[j] = sc[j];
-        if (stride > static_cast<uint32_t>(kTfScalars)) {
+        put(row);
+        if (stride > static_cast<uint32_t>(kTfRowScalars)) {
             tf_scalars(F, t + hd, sc);
-            for (int j = 0; j < kTfScalars; ++j) row[kTfScalars + j] = sc[j];
+            put(row + kTfRowScalars);
         }
     }
 }
@@ -607,8 +686,8 @@ __device__ __forceinline__ void efield(const Consts<R>& k, const Pos& x, double 
     } else {
         if (k.tf != nullptr) {
             // stage 0 at t_k, 1 at t_k + dt/2 (RK4), 2 at t_k + dt = the next row
-            const double* row = k.tfrow + (stage == 0 ? 0 : stage == 1 ? kTfScalars : static_cast<int>(k.tfstride));
-            tf_apply<R>(*k.tf, x, row, E);
+            const double* row = k.tfrow + (stage == 0 ? 0 : stage == 1 ? kTfRowScalars : static_cast<int>(k.tfstride));
+            tf_apply<R>(k, *k.tf, x, row, E);
             return;
         } else {
 #pragma unroll
@@ -1252,14 +1331,15 @@ __device__ __forceinline__ unsigned long long warp_sum_u32(uint32_t v) {
 // Resident blocks of 128 threads per SM the register budget is set for:
 // 6 for the float forms (80 registers), 4 for FP64 (128).  The learned
 // deflection measured fastest at 6 too (4 and 5 remove its spills but lose
-// more to occupancy).
-template <int PREC, int COLL>
+// more to occupancy).  The float time-dependent instance holds the field's
+// constants and its TIMS profile segment per lane: 5 (102 registers).
+template <int PREC, int COLL, int FIELD>
 struct KernelShape {
-    static constexpr int kMinBlocks = PREC == kPrecFP64 ? 4 : 6;
+    static constexpr int kMinBlocks = PREC == kPrecFP64 ? 4 : (FIELD == kFieldLinearRF ? 5 : 6);
 };
 
 template <int PREC, int INTEG, int COLL, int FIELD, bool MAG, bool FUSED>
-__global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_step(const __grid_constant__ StepParams p) {
+__global__ void __launch_bounds__(128, KernelShape<PREC, COLL, FIELD>::kMinBlocks) k_step(const __grid_constant__ StepParams p) {
     using R = typename PrecT<PREC>::R;
     using Pos = typename PosOf<PREC>::T;
     using Snap = typename Pos::Snap;
@@ -1317,6 +1397,16 @@ __global__ void __launch_bounds__(128, KernelShape<PREC, COLL>::kMinBlocks) k_st
             k.tftab = p.tf_tab + static_cast<size_t>(p.ens_base + static_cast<uint32_t>(e)) * (p.n_steps + 1u) *
                                      p.tf_stride;
             k.tfrow = k.tftab;
+            if constexpr (sizeof(R) == 4) {
+                const TimeField& F = *k.tf;
+                k.tfc_inst = F.inst;
+                k.tfc_ei = static_cast<float>(F.tims_ei);
+                k.tfc_ef = static_cast<float>(F.tims_ef);
+                k.tfc_final = F.tims_final_profile != 0;
+                k.ts_lo = INFINITY;               // no segment yet
+                k.ts_hi = -INFINITY;
+                k.ts_mode = 0;
+            }
         }
     }
     if constexpr (COLL == kCollLangevin) {
