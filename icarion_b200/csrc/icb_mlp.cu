@@ -258,33 +258,43 @@ struct DevVec {
 // float block (W1, W3 rounded to BF16; biases FP32).
 void mlp_pack(const float* params, std::vector<uint32_t>& frag, std::vector<float>& fblock) {
     frag.assign(kMlpFragWords, 0u);
-    for (int nt = 0; nt < 8; ++nt)
+    // W2 as A fragments of m-tile mt (units 16mt..16mt+15) and k-step ks
+    auto pair = [&](int n, int k) {
+        const float* row = params + kMlpOffW2 + n * kMlpH;
+        return bf16_bits_host(row[k]) | (bf16_bits_host(row[k + 1]) << 16);
+    };
+    for (int mt = 0; mt < 4; ++mt)
         for (int ks = 0; ks < 4; ++ks)
             for (int lane = 0; lane < 32; ++lane) {
                 const int g = lane >> 2, t = lane & 3;
-                const int n = 8 * nt + g;
-                const int k0 = 16 * ks + 2 * t;
-                const float* row = params + kMlpOffW2 + n * kMlpH;
-                const size_t base = (static_cast<size_t>(nt * 4 + ks) * 32 + lane) * 2;
-                frag[base] = bf16_bits_host(row[k0]) | (bf16_bits_host(row[k0 + 1]) << 16);
-                frag[base + 1] = bf16_bits_host(row[k0 + 8]) | (bf16_bits_host(row[k0 + 9]) << 16);
+                const int n0 = 16 * mt + g, n1 = n0 + 8;
+                const int k0 = 16 * ks + 2 * t, k1 = k0 + 8;
+                const size_t base = (static_cast<size_t>(mt * 4 + ks) * 32 + lane) * 4;
+                frag[base] = pair(n0, k0);
+                frag[base + 1] = pair(n1, k0);
+                frag[base + 2] = pair(n0, k1);
+                frag[base + 3] = pair(n1, k1);
             }
-    // layer 1 as B fragments: (W1[n][0], W1[n][0]), (W1[n][1], W1[n][1]),
-    // (b1[n] hi, b1[n] lo), 0 for t = 0..3
-    for (int nt = 0; nt < 8; ++nt)
+    // layer 1 as A fragments: rows h of [W1[h][0] twice, W1[h][1] twice,
+    // b1[h] hi, b1[h] lo, 0 ...], words for rows 16mt+g and 16mt+g+8
+    auto l1 = [&](int h, int t) {
+        if (t < 2) {
+            const uint32_t b = bf16_bits_host(params[kMlpOffW1 + 2 * h + t]);
+            return b | (b << 16);
+        }
+        if (t == 2) {
+            const float b1 = params[kMlpOffB1 + h];
+            const float hi = bf16_round_host(b1);
+            return bf16_bits_host(hi) | (bf16_bits_host(b1 - hi) << 16);
+        }
+        return 0u;
+    };
+    for (int mt = 0; mt < 4; ++mt)
         for (int lane = 0; lane < 32; ++lane) {
             const int g = lane >> 2, t = lane & 3;
-            const int n = 8 * nt + g;
-            uint32_t w = 0u;
-            if (t < 2) {
-                const uint32_t b = bf16_bits_host(params[kMlpOffW1 + 2 * n + t]);
-                w = b | (b << 16);
-            } else if (t == 2) {
-                const float b1 = params[kMlpOffB1 + n];
-                const float hi = bf16_round_host(b1);
-                w = bf16_bits_host(hi) | (bf16_bits_host(b1 - hi) << 16);
-            }
-            frag[static_cast<size_t>(kMlpFragW1Off) + static_cast<size_t>(nt) * 32 + lane] = w;
+            const size_t base = static_cast<size_t>(kMlpFragW1Off) + (static_cast<size_t>(mt) * 32 + lane) * 2;
+            frag[base] = l1(16 * mt + g, t);
+            frag[base + 1] = l1(16 * mt + g + 8, t);
         }
     fblock.assign(kMlpFSize, 0.f);
     for (int k = 0; k < 128; ++k) fblock[kMlpFW1 + k] = bf16_round_host(params[kMlpOffW1 + k]);
