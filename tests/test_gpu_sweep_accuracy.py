@@ -7,11 +7,17 @@ nu_max per ensemble).
    v_drift, K0, D_L, D_T within 4 combined standard errors, collision
    fraction within 1 %, FP64 and mixed.
 2. The whole sweep (64 ensembles, 2-100 Td, the three species round-robin)
-   with 655,360 ions per ensemble: mixed against FP64 per ensemble, K0
-   within 0.3 % and D_L, D_T within 1 %.  Standard errors of one run at
-   this size: K0 <= 0.05 %, D_L and D_T ~0.17 % (sqrt(2/N)), so the
-   difference of two runs has ~0.25 % on D and the 1 % gate sits at 4 of
-   them.
+   with 655,360 ions per ensemble: mixed against FP64 per ensemble.  The
+   runs are statistically independent (float rounding decorrelates the
+   ions' collision sequences), so each difference carries the standard
+   error of both runs, stated by the fit: for D_L and D_T ~0.25 %
+   (sqrt(2/N) each), for K0 from 0.01 % at 100 Td to ~0.8 % at 2 Td (at
+   50,000 steps of dt = 0.1 / nu_max the low-field ensembles drift only a
+   few um against ~20 um of diffusion).  Gates: K0 within max(0.3 %, 4
+   standard errors of the difference), D_L and D_T within max(1 %, 4
+   standard errors), and no bias over the sweep: the mean squared
+   normalised difference of each observable below 2 (a shift of one
+   standard error in every ensemble would give 2).
 """
 from __future__ import annotations
 
@@ -76,11 +82,15 @@ def test_whole_sweep_mixed_matches_fp64_per_ensemble():
             steps_idx, mom, _ = sim.run(steps, snap, ref_step=ref)
         fits[prec] = fits_of(sw.ensembles, steps_idx, mom, ref)
     worst = {"K0": 0.0, "D_L": 0.0, "D_T": 0.0}
+    chi2 = {"K0": 0.0, "D_L": 0.0, "D_T": 0.0}
     for e in range(64):
         a, b = fits[capi.PREC_MIXED][e], fits[capi.PREC_FP64][e]
-        assert b["se_K0"] / b["K0"] < 1e-3 and b["se_D_L"] / b["D_L"] < 2.5e-3
         for key, tol in (("K0", 3e-3), ("D_L", 1e-2), ("D_T", 1e-2)):
             r = ob.rel_err(a[key], b[key])
+            se = float(np.hypot(a["se_" + key], b["se_" + key])) / abs(b[key])
             worst[key] = max(worst[key], r)
-            assert r <= tol, (e, key, a[key], b[key])
-    print("worst mixed-vs-FP64 relative error over the sweep:", worst)
+            chi2[key] += (r / se) ** 2 / 64.0
+            assert r <= max(tol, 4.0 * se), (e, key, a[key], b[key], se)
+    for key in chi2:
+        assert chi2[key] < 2.0, (key, chi2[key])
+    print("worst mixed-vs-FP64 relative difference over the sweep:", worst, "mean squared / se^2:", chi2)
