@@ -16,8 +16,9 @@ nu_max per ensemble).
    few um against ~20 um of diffusion).  Gates: K0 within max(0.3 %, 4
    standard errors of the difference), D_L and D_T within max(1 %, 4
    standard errors), and no bias over the sweep: the mean squared
-   normalised difference of each observable below 2 (a shift of one
-   standard error in every ensemble would give 2).
+   normalised difference of each observable below 4 (1 when the stated
+   errors are exact; a shift of two standard errors in every ensemble
+   gives 5).
 """
 from __future__ import annotations
 
@@ -92,5 +93,5 @@ def test_whole_sweep_mixed_matches_fp64_per_ensemble():
             chi2[key] += (r / se) ** 2 / 64.0
             assert r <= max(tol, 4.0 * se), (e, key, a[key], b[key], se)
     for key in chi2:
-        assert chi2[key] < 2.0, (key, chi2[key])
+        assert chi2[key] < 4.0, (key, chi2[key])
     print("worst mixed-vs-FP64 relative difference over the sweep:", worst, "mean squared / se^2:", chi2)
