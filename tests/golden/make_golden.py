@@ -15,9 +15,10 @@ Fixtures
   derived.json          loader-derived n, gas mass, axial_V, E_z (config 0)
   push_<case>.npz       collision-free Boris / RK4 runs (IMS, FTICR, QuadrupoleRF, LQIT)
   hss_ref.npz           Boris + reference HSS, 64 ions x 2000 steps
-  ims_config0.npz       config 0: 4096 ions x 100k steps, moments every 1000
-                        steps, displacement reference after 20k steps,
-                        arrival (z = 2 mm) and death times, OpenMP timing
+  ims_config0.npz       config-0 physics: 65,536 ions x 100k steps, moments
+                        every 1000 steps, displacement reference after 20k
+                        steps, arrival (z = 2 mm) and death times, OpenMP
+                        timing (--config0-only regenerates just this one)
 """
 from __future__ import annotations
 
@@ -33,6 +34,7 @@ sys.path.insert(0, str(ROOT / "oracle"))
 import oracle as orc  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
+CONFIG0_IONS = 65536
 AMU = 1.66053906660e-27
 E = 1.602176634e-19
 
@@ -208,8 +210,12 @@ def main(quick: bool, only: set[str] | None = None) -> None:
          **{f"out_{k}": fin[k] for k in orc.STATE_KEYS}, steps=2000, dt=5e-10, seed=123,
          collisions=stats["collisions"], domain=json.dumps(IMS_DOMAIN))
 
-    # 6. config 0 statistics
-    n, steps = (1024, 20000) if quick else (4096, 100000)
+    config0_statistics(1024 if quick else CONFIG0_IONS, 20000 if quick else 100000)
+
+
+def config0_statistics(n: int, steps: int) -> None:
+    """Config-0 physics run by the reference code: moments every 1000 steps,
+    displacement reference after steps / 5, arrivals at z = 2 mm."""
     s0 = init_state(n)
     fin, stats, mom = orc.harness_run(s0, steps, IMS_DOMAIN, integrator="boris", collision="hss", dt=5e-10,
                                       seed=123, snap=1000, ref_step=steps // 5, zdet=2.0e-3, threads=8)
@@ -258,5 +264,9 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--quick", action="store_true")
     ap.add_argument("--only", nargs="*", default=None, help="regenerate only these push fixtures (e.g. boris_lqit)")
+    ap.add_argument("--config0-only", action="store_true", help="regenerate only ims_config0.npz")
     a = ap.parse_args()
-    main(a.quick, set(a.only) if a.only else None)
+    if a.config0_only:
+        config0_statistics(CONFIG0_IONS, 100000)
+    else:
+        main(a.quick, set(a.only) if a.only else None)

@@ -1,10 +1,11 @@
 """Stochastic parity of the fused kernel.
 
-1. Config 0 (4,096 ions, 100,000 steps, Boris + HSS, 20 Td): FP64 and mixed
-   device runs against the reference's own CPU code (golden
-   ims_config0.npz, same initial cloud): drift velocity, K0, D_L, D_T within
-   4 combined standard errors; arrival-time distributions at z = 2 mm with a
-   two-sample KS p-value > 0.01.
+1. Config-0 physics (100,000 steps, Boris + HSS, 20 Td) on 65,536 ions:
+   FP64 and mixed device runs against the reference's own CPU code (golden
+   ims_config0.npz, same initial cloud): drift velocity, K0, D_L, D_T
+   within 4 combined standard errors (at this size ~0.04 % on K0, ~0.6 %
+   on D_L and D_T per run); collision fraction within 0.3 %; arrival-time
+   distributions at z = 2 mm with a two-sample KS p-value > 0.01.
 2. Config 1 physics at 1,048,576 ions: mixed and hi/lo mixed against the
    FP64 device form (the FP64 oracle run): K0 within 0.3 %, D_L and D_T
    within 1 %.
@@ -59,17 +60,18 @@ def reference_fit(golden):
 @pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_MIXED])
 def test_config0_observables_match_reference_cpu(golden, precision):
     ref, z = reference_fit(golden)
-    assert int(z["n_ions"]) == 4096 and int(z["steps"]) == 100000
-    fit, fin, tot = device_run(4096, 100000, precision)
+    n = int(z["n_ions"])
+    assert n >= 4096 and int(z["steps"]) == 100000
+    fit, fin, tot = device_run(n, 100000, precision)
     for key in ("v_drift", "K0", "D_L", "D_T"):
         se = np.hypot(ref["se_" + key], fit["se_" + key])
         assert abs(fit[key] - ref[key]) <= 4.0 * se, (key, fit[key], ref[key], se)
     # collision fraction of ion-steps (reference: collisions / (N * steps))
-    f_ref = float(z["collisions"]) / (4096 * 100000)
-    f_dev = tot["collisions"] / (4096 * 100000)
-    assert abs(f_dev - f_ref) / f_ref < 0.01, (f_dev, f_ref)
+    f_ref = float(z["collisions"]) / (n * 100000)
+    f_dev = tot["collisions"] / (n * 100000)
+    assert abs(f_dev - f_ref) / f_ref < 0.003, (f_dev, f_ref)
     a, b = fin.t_arrival[fin.t_arrival >= 0], z["t_arrival"][z["t_arrival"] >= 0]
-    assert abs(len(a) - len(b)) <= 0.02 * 4096
+    assert abs(len(a) - len(b)) <= 0.01 * n
     _, p = ob.ks_2samp(a, b)
     assert p > 0.01, p
 

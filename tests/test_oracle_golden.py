@@ -95,7 +95,7 @@ def test_nullcoll_scheme_reproduces_reference_collision_law():
 def test_nullcoll_oracle_tracks_reference_code_over_20k_steps(golden):
     """The null-collision scheme with the skip clock (oracle, FP64, Philox)
     against the reference's own Boris + HSS run (golden ims_config0.npz) on
-    the same 4,096-ion cloud over the first 20,000 steps: collision fraction
+    the same 65,536-ion cloud over the first 20,000 steps: collision fraction
     within 1% and drift velocity within 4 combined standard errors."""
     from helpers import config0_ensemble
     from icarion_b200 import observables as ob
