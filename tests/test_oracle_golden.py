@@ -139,3 +139,28 @@ def test_plain_per_step_form_tracks_reference_code(golden):
     f_ref = float(z["collisions"]) / (n * int(z["steps"]))
     f_me = r["collisions"] / (n * steps)
     assert abs(f_me - f_ref) / f_ref < 0.01, (f_me, f_ref)
+
+
+def test_stateless_per_step_test_tracks_reference_code(golden):
+    """The per-step kernel's stateless collision test (oracle collision 8:
+    Philox(id, step) against Q = A (|v - u| + <|th|>) every step, then the
+    per-step clock's candidate) against the reference's own Boris + HSS run
+    on the same cloud over 20,000 steps: collision fraction within 1 % and
+    drift within 4 combined standard errors."""
+    from helpers import config0_ensemble
+    from icarion_b200 import observables as ob
+    z = golden("ims_config0.npz")
+    n = int(z["n_ions"])
+    steps = 20000
+    e = config0_ensemble(detector_z_m=2.0e-3)
+    st = oracle_state(config0_ions(n))
+    r = orc.run(e, st, steps, integrator=0, collision=8, seed=123, snap_every=1000, ref_step=int(z["ref_step"]),
+                threads=8)
+    dt = float(z["dt"])
+    t = np.arange(1, steps // 1000 + 1) * 1000 * dt
+    mine = ob.fit_transport(t[3:], r["moments"][3:], t_ref=0.0)
+    ref = ob.fit_transport(t[3:], z["moments"][3:steps // 1000], t_ref=0.0)
+    assert abs(mine["v_drift"] - ref["v_drift"]) <= 4 * np.hypot(mine["se_v_drift"], ref["se_v_drift"]), (mine, ref)
+    f_ref = float(z["collisions"]) / (n * int(z["steps"]))
+    f_me = r["collisions"] / (n * steps)
+    assert abs(f_me - f_ref) / f_ref < 0.01, (f_me, f_ref)
