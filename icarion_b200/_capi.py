@@ -123,7 +123,7 @@ class SpaceChargeConfig(C.Structure):
     _fields_ = [
         ("mode", C.c_int32), ("grid_n", C.c_int32 * 3), ("box_min_m", D3), ("box_max_m", D3),
         ("alpha_h", C.c_double), ("pp_cutoff_cells", C.c_double), ("softening_m", C.c_double),
-        ("field_bound_V_m", C.c_double), ("reserved", C.c_int32 * 8),
+        ("field_bound_V_m", C.c_double), ("solver_fp32", C.c_int32), ("reserved", C.c_int32 * 7),
     ]
 
 

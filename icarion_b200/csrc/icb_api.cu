@@ -1499,8 +1499,9 @@ int icb_spacecharge_configure(icb_handle* h, const icb_spacecharge_config* cfg) 
     if (h->hilo()) return fail(ICB_ERR_UNSUPPORTED, "space charge is built for the FP64 and mixed position forms");
     std::string err;
     SpaceChargeSolver* sc = nullptr;
-    // the float forms run the particle-particle sums in float
-    int r = sc_create(*cfg, h->n, !h->fp64(), h->stream, &sc, err);
+    // the float forms (and an FP64 handle that asks for it) run the mesh and
+    // the particle-particle sums in single precision
+    int r = sc_create(*cfg, h->n, !h->fp64() || cfg->solver_fp32 != 0, h->stream, &sc, err);
     if (r != ICB_OK) return fail(r, "space charge: %s", err.c_str());
     h->sc = sc;
     h->sc_emax_base = h->ens_const[0].Emax;

@@ -71,5 +71,5 @@ def fticr_cell(n_ions: int = 262_144, seed: int = 123, mz_min: float = 500.0, mz
                      sc_box_max=(h, h, zc + h))
 
 
-def configure(sim, cell: FticrCell, mode: int = capi.SC_P3M_ISOLATED) -> None:
-    sim.configure_space_charge(mode, cell.sc_grid, cell.sc_box_min, cell.sc_box_max)
+def configure(sim, cell: FticrCell, mode: int = capi.SC_P3M_ISOLATED, solver_fp32: bool = False) -> None:
+    sim.configure_space_charge(mode, cell.sc_grid, cell.sc_box_min, cell.sc_box_max, solver_fp32=solver_fp32)

@@ -230,8 +230,10 @@ class Simulation:
 
     def configure_space_charge(self, mode: int, grid_n, box_min, box_max, alpha_h: float = 0.0,
                                pp_cutoff_cells: float = 0.0, softening_m: float = -1.0,
-                               field_bound: float = 0.0) -> None:
-        """Space charge solved before every step (see icb_spacecharge_configure)."""
+                               field_bound: float = 0.0, solver_fp32: bool = False) -> None:
+        """Space charge solved before every step (see icb_spacecharge_configure);
+        solver_fp32 runs the isolated solver in single precision under an
+        FP64 handle too."""
         c = capi.SpaceChargeConfig()
         c.mode = mode
         c.grid_n[:] = [int(v) for v in grid_n]
@@ -241,6 +243,7 @@ class Simulation:
         c.pp_cutoff_cells = pp_cutoff_cells
         c.softening_m = softening_m
         c.field_bound_V_m = field_bound
+        c.solver_fp32 = 1 if solver_fp32 else 0
         capi.check(self._lib.icb_spacecharge_configure(self._h, C.byref(c)))
 
     def space_charge_field(self) -> np.ndarray:

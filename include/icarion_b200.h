@@ -354,7 +354,10 @@ typedef struct icb_spacecharge_config {
     double softening_m;        /* isolated: direct-sum softening; < 0 = 1e-10 (SpaceChargeModelFactory.h:26) */
     double field_bound_V_m;    /* bound on |E_sc| added to the collision majorant's field bound;
                                   0 = 4 x the largest |E_sc| of the configured state */
-    int32_t reserved[8];
+    int32_t solver_fp32;       /* isolated: 1 = mesh and particle-particle sums in single
+                                  precision under an FP64 handle too (the float forms always
+                                  use them); E_sc stays FP64 per ion.  0 = the handle's form */
+    int32_t reserved[7];
 } icb_spacecharge_config;
 int icb_spacecharge_configure(struct icb_handle* h, const icb_spacecharge_config* cfg);
 /* Solve the field of the current state and copy E_sc (V/m) of every ion to

@@ -9,14 +9,21 @@ analytic motion.
    isolated P3M (128^3 mesh over a 14 mm cube, particle-particle correction
    within 2 cells).  The runs without space charge are bit-identical
    (FP64); the space-charge displacement of each ion (final position with
-   minus without) agrees within 5 % RMS of its own size in FP64 and 10 % in
+   minus without) agrees within 5 % RMS of its own size in FP64 (with the
+   FP64 or the single-precision solver, the workload's setting) and 10 % in
    the mixed form (the P3M field is resolution-limited at ~2 % RMS).
 2. Cyclotron frequency: ions started on a pure modified-cyclotron orbit
    (2 mm about the trap axis, m/z 500 / 1000 / 1500) turn at
    w+ = wc/2 + sqrt(wc^2/4 - q V / (m d^2)) (d^2 = L^2/8 + r^2/4, the
    field model's constant): the phase-fitted frequency is within 1e-6 of it
-   in FP64 and 2e-6 in mixed precision over 100,000 steps (Boris's own
-   rotation error (wc dt)^2/12 is below 5e-8).
+   in FP64 over 100,000 steps (Boris's own rotation error (wc dt)^2/12 is
+   below 5e-8).  The mixed form is held to 1e-5 only: on the orbit
+   (2.7 km/s at m/z 500) the trap field's kick per half step,
+   |q E / m| dt / 2 ~ 2e-4 m/s, is below one float ulp of the velocity
+   (2.4e-4 m/s), so the float velocity rounds the kick (to 0 or 1 ulp per
+   component) and the magnetron part of w+ (wc - w+ = 305 rad/s) comes out
+   ~1 % off: ~3e-6 of w+ at m/z 500 (measured 2.8e-6).  FT-ICR work
+   therefore pushes in FP64.
 """
 from __future__ import annotations
 
@@ -38,7 +45,7 @@ def _gpu():
     assert device_count() > 0, "these tests need a CUDA device"
 
 
-def _run(z, precision, space_charge: bool):
+def _run(z, precision, space_charge: bool, solver_fp32: bool = False):
     cell = fticr.fticr_cell(n_ions=int(z["n_ions"]), cloud_sigma_m=float(z["sigma_m"]))
     st = IonState(**{k: np.ascontiguousarray(z["in_" + k]) for k in ("x", "y", "z", "vx", "vy", "vz", "mass",
                                                                       "charge")},
@@ -46,16 +53,17 @@ def _run(z, precision, space_charge: bool):
     with Simulation([cell.ensemble], precision=precision, collision=capi.COLLISION_NONE, rng_seed=1) as sim:
         sim.upload(st)
         if space_charge:
-            fticr.configure(sim, cell)
+            fticr.configure(sim, cell, solver_fp32=solver_fp32)
         sim.advance(int(z["steps"]))
         return sim.download()
 
 
-@pytest.mark.parametrize("precision,tol", [(capi.PREC_FP64, 0.05), (capi.PREC_MIXED, 0.10)])
-def test_space_charge_displacement_matches_reference_direct_sum(golden, precision, tol):
+@pytest.mark.parametrize("precision,solver_fp32,tol", [(capi.PREC_FP64, False, 0.05), (capi.PREC_FP64, True, 0.05),
+                                                       (capi.PREC_MIXED, True, 0.10)])
+def test_space_charge_displacement_matches_reference_direct_sum(golden, precision, solver_fp32, tol):
     z = golden("fticr_sc_direct.npz")
     plain = _run(z, precision, False)
-    with_sc = _run(z, precision, True)
+    with_sc = _run(z, precision, True, solver_fp32)
     if precision == capi.PREC_FP64:
         for k in ("x", "y", "z", "vx", "vy", "vz"):
             assert np.array_equal(getattr(plain, k), z["nosc_" + k]), k
@@ -67,7 +75,7 @@ def test_space_charge_displacement_matches_reference_direct_sum(golden, precisio
     assert rms_err <= tol * rms_ref, (rms_err, rms_ref)
 
 
-@pytest.mark.parametrize("precision,tol", [(capi.PREC_FP64, 1e-6), (capi.PREC_MIXED, 2e-6)])
+@pytest.mark.parametrize("precision,tol", [(capi.PREC_FP64, 1e-6), (capi.PREC_MIXED, 1e-5)])
 def test_cyclotron_frequency_matches_the_trap(precision, tol):
     cell = fticr.fticr_cell(n_ions=3)
     e = cell.ensemble
@@ -95,7 +103,8 @@ def test_cyclotron_frequency_matches_the_trap(precision, tol):
             phases.append(np.arctan2(o.y, o.x))
     ph = np.unwrap(np.array(phases), axis=0)
     t = (np.arange(steps // every) + 1) * every * e["dt_s"]
+    errs = [abs(-np.polyfit(t, ph[:, j], 1)[0] / wp[j] - 1.0) for j in range(3)]
+    print("relative w+ error per m/z:", dict(zip(mz.tolist(), errs)))
     for j in range(3):
-        w_fit = -np.polyfit(t, ph[:, j], 1)[0]
-        assert abs(w_fit / wp[j] - 1.0) <= tol, (mz[j], w_fit, wp[j])
+        assert errs[j] <= tol, (mz[j], errs[j])
     assert math.isfinite(float(ph[-1, 0]))

