@@ -6,8 +6,9 @@ Compiles every ``csrc/*.cu`` translation unit with nvcc
 (``-gencode arch=compute_100a,code=sm_100a -lineinfo``) into
 ``icarion_b200/_lib/libicarion_b200.so``.  Per-unit flags:
 
-* ``icb_step_fp64.cu``   ``--fmad=false`` (bit-faithful IEEE double push)
-* ``icb_step_mixed.cu``, ``icb_step_hilo.cu``, ``icb_mathcheck.cu``, ``icb_mlp*.cu``  ``-use_fast_math``
+* ``icb_step_fp64.cu``, ``icb_step1_fp64.cu``   ``--fmad=false`` (bit-faithful IEEE double push)
+* ``icb_step_mixed.cu``, ``icb_step_hilo.cu``, ``icb_step1_mixed.cu``, ``icb_step1_hilo.cu``,
+  ``icb_mathcheck.cu``  ``-use_fast_math``
 
 Objects are rebuilt only when a source or header is newer than the object.
 """
@@ -35,6 +36,9 @@ PER_UNIT = {
     "icb_step_fp64.cu": ["--fmad=false"],
     "icb_step_mixed.cu": ["-use_fast_math"],
     "icb_step_hilo.cu": ["-use_fast_math"],
+    "icb_step1_fp64.cu": ["--fmad=false"],
+    "icb_step1_mixed.cu": ["-use_fast_math"],
+    "icb_step1_hilo.cu": ["-use_fast_math"],
     "icb_mathcheck.cu": ["-use_fast_math"],
 }
 LINK_LIBS = ["-lcufft"]
@@ -92,13 +96,31 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     return LIB
 
 
+def unit_headers(unit: str) -> list[Path]:
+    """The repository headers a translation unit includes, transitively
+    (quoted includes resolved in csrc/ and include/)."""
+    import re
+    seen: dict[str, Path] = {}
+    todo = [CSRC / unit]
+    while todo:
+        f = todo.pop()
+        for name in re.findall(r'^\s*#\s*include\s+"([^"]+)"', f.read_text(), re.M):
+            for d in (CSRC, INCLUDE):
+                p = d / name
+                if p.exists() and name not in seen:
+                    seen[name] = p
+                    todo.append(p)
+                    break
+    return [seen[k] for k in sorted(seen)]
+
+
 def kernel_source_hash(unit: str = "icb_step_mixed.cu") -> str:
-    """sha256 over one translation unit, every kernel header and its nvcc
-    flags: a profile taken of a kernel records this, and readers of the
+    """sha256 over one translation unit, the headers it includes and its
+    nvcc flags: a profile taken of a kernel records this, and readers of the
     profile's figures compare it with the current sources."""
     import hashlib
     h = hashlib.sha256()
-    for f in [CSRC / unit] + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")):
+    for f in [CSRC / unit] + unit_headers(unit):
         h.update(f.name.encode())
         h.update(f.read_bytes())
     h.update(" ".join(ARCH + COMMON[:4] + PER_UNIT.get(unit, [])).encode())

@@ -894,15 +894,23 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
             if (h->any_tf || h->sc)
                 return fail(ICB_ERR_UNSUPPORTED, "the per-step collision test has no time-dependent field or space charge");
             for (int e = 0; e < ne; ++e) {
-                p.ens[e].sp_m = h->sp_m[static_cast<size_t>(e0 + e)];
-                p.ens[e].sp_q = h->sp_q[static_cast<size_t>(e0 + e)];
+                EnsConst& E = p.ens[e];
+                E.sp_m = h->sp_m[static_cast<size_t>(e0 + e)];
+                E.sp_q = h->sp_q[static_cast<size_t>(e0 + e)];
+                if (E.sp_m > 0.0) {
+                    // the device's load_consts arithmetic, once per launch
+                    const double inv_m = 1.0 / E.sp_m;
+                    for (int a = 0; a < 3; ++a) {
+                        E.sp_a64[a] = (E.E0[a] * E.sp_q) / E.sp_m;
+                        E.sp_a32[a] = (E.E0[a] * E.sp_q) * inv_m;
+                    }
+                }
             }
-            const dim3 grid1(grid_for(en - b, kStep1BlockHost));
             cudaError_t err1;
             switch (h->cfg.precision) {
-                case ICB_PREC_FP64: err1 = launch_step1_fp64(h->coll, p, grid1, st); break;
-                case ICB_PREC_MIXED: err1 = launch_step1_mixed(h->coll, p, grid1, st); break;
-                default: err1 = launch_step1_hilo(h->coll, p, grid1, st); break;
+                case ICB_PREC_FP64: err1 = launch_step1_fp64(h->coll, p, st); break;
+                case ICB_PREC_MIXED: err1 = launch_step1_mixed(h->coll, p, st); break;
+                default: err1 = launch_step1_hilo(h->coll, p, st); break;
             }
             ++h->launches;
             if (err1 != cudaSuccess) return fail(ICB_ERR_CUDA, "per-step kernel launch: %s", cudaGetErrorString(err1));
@@ -996,6 +1004,9 @@ int read_stats(icb_handle* h, icb_run_stats* st, uint64_t steps, size_t n_timed_
     st->deaths = c[kCntDeaths];
     st->arrivals = c[kCntArrivals];
     st->device_ms = static_cast<double>(ms);
+    if (c[kCntStalls] != 0)
+        return fail(ICB_ERR_CUDA, "per-step kernel: %llu staged tile copies did not complete within a second",
+                    c[kCntStalls]);
     return ICB_OK;
 }
 

@@ -21,11 +21,10 @@ cudaError_t launch_step_mixed(int integ, int coll, int field, bool mag, const St
 cudaError_t launch_step_hilo(int integ, int coll, int field, bool mag, const StepParams& p,
                              dim3 grid, dim3 block, cudaStream_t s);
 // The per-step kernel (icb_step1.cuh) of each precision: coll kCollNone or
-// kCollHSS; grid over the launch's ions, its own block size.
-cudaError_t launch_step1_fp64(int coll, const StepParams& p, dim3 grid, cudaStream_t s);
-cudaError_t launch_step1_mixed(int coll, const StepParams& p, dim3 grid, cudaStream_t s);
-cudaError_t launch_step1_hilo(int coll, const StepParams& p, dim3 grid, cudaStream_t s);
-constexpr int kStep1BlockHost = 256;
+// kCollHSS; a persistent grid over the launch's tiles of its own shape.
+cudaError_t launch_step1_fp64(int coll, const StepParams& p, cudaStream_t s);
+cudaError_t launch_step1_mixed(int coll, const StepParams& p, cudaStream_t s);
+cudaError_t launch_step1_hilo(int coll, const StepParams& p, cudaStream_t s);
 
 // Space-charge solver (icb_p3m.cu).  Functions return ICB_* status codes
 // and put a message into `err` on failure.

@@ -22,7 +22,9 @@ enum IntegKind : int { kBoris = 0, kRK4 = 1 };
 
 // Counter slots (uint64 each) accumulated by the stepping kernels.
 enum CounterSlot : int {
-    kCntCandidates = 0, kCntCollisions = 1, kCntOverflow = 2, kCntDeaths = 3, kCntArrivals = 4, kNumCounters = 8
+    kCntCandidates = 0, kCntCollisions = 1, kCntOverflow = 2, kCntDeaths = 3, kCntArrivals = 4,
+    kCntStalls = 5,   // staged copies whose wait ran out (per-step kernel): an error
+    kNumCounters = 8
 };
 
 // Flags byte per ion.
@@ -69,8 +71,11 @@ struct EnsConst {
     int32_t flow;
     int32_t tf;        // time-dependent field of TimeField (waveforms, TIMS)
     // the species of every ion of the ensemble (per-step kernel): mass and
-    // charge when all its ions share them, sp_m = 0 otherwise
+    // charge when all its ions share them, sp_m = 0 otherwise; then also the
+    // uniform field's acceleration by the FP64 form's formula (E0 q) / m and
+    // by the float forms' (E0 q) (1 / m)
     double sp_m, sp_q;
+    double sp_a64[3], sp_a32[3];
 };
 
 // HSS gas mixture of one ensemble (read by the candidate step only):
@@ -200,5 +205,8 @@ struct StepParams {
     uint64_t ens_off[kMaxLaunchEns + 1];  // absolute ion offsets of the chunk's ensembles
     EnsConst ens[kMaxLaunchEns];
 };
+
+// The kernel parameter block holds at most 32,764 bytes.
+static_assert(sizeof(StepParams) <= 32764, "StepParams exceeds the kernel parameter space");
 
 }  // namespace icb

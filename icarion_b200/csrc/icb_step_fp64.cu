@@ -5,7 +5,6 @@
 #define ICB_TF_TABLE_UNIT
 #include "icb_step_kernel.cuh"
 #include "icb_step_dispatch.cuh"
-#include "icb_step1.cuh"
 
 namespace icb {
 cudaError_t launch_step_fp64(int integ, int coll, int field, bool mag, const StepParams& p,
@@ -16,9 +15,5 @@ cudaError_t launch_step_fp64(int integ, int coll, int field, bool mag, const Ste
 cudaError_t launch_tf_table(const StepParams& p, double* tab, double* tseq, uint32_t stride, cudaStream_t s) {
     k_tf_table<<<p.n_ens, 128, 0, s>>>(p, tab, tseq, stride);
     return cudaGetLastError();
-}
-
-cudaError_t launch_step1_fp64(int coll, const StepParams& p, dim3 grid, cudaStream_t s) {
-    return launch_step1<kPrecFP64>(coll, p, grid, s);
 }
 }  // namespace icb

@@ -4,15 +4,10 @@
 #include "icb_internal.h"
 #include "icb_step_kernel.cuh"
 #include "icb_step_dispatch.cuh"
-#include "icb_step1.cuh"
 
 namespace icb {
 cudaError_t launch_step_hilo(int integ, int coll, int field, bool mag, const StepParams& p,
                              dim3 grid, dim3 block, cudaStream_t s) {
     return dispatch_step<kPrecHiLo, false>(integ, coll, field, mag, p, grid, block, s);
-}
-
-cudaError_t launch_step1_hilo(int coll, const StepParams& p, dim3 grid, cudaStream_t s) {
-    return launch_step1<kPrecHiLo>(coll, p, grid, s);
 }
 }  // namespace icb
