@@ -23,7 +23,7 @@
 // the tiles k = first + blockIdx.x + it * gridDim.x of the launch's range,
 // with a grid of (resident CTAs per SM) x SMs.  A tile's state arrives in
 // shared memory by bulk copies (cp.async.bulk, one per array, completed on
-// the stage's mbarrier) issued kStep1Stages tiles ahead, so the loads of
+// the stage's mbarrier) issued two tiles ahead, so the loads of
 // later tiles are in flight while this one computes and the number of
 // bytes in flight does not depend on registers.  Tiles cut by the range's
 // ends load with ordinary per-thread loads.  Each step runs in three
@@ -48,7 +48,14 @@
 namespace icb {
 
 constexpr int kStep1Block = 256;    // ions per tile = threads per CTA
-constexpr int kStep1Stages = 2;     // tiles loaded ahead per CTA
+// Tiles loaded ahead per CTA (9.5 KB each in the float forms, 12.5 KB in
+// FP64).  Two keep the copies ahead of the push: four measured the same
+// (0.348 vs 0.342 ms per 16.8M-ion step), and five CTAs per SM with 40
+// registers measured 0.369 ms.
+template <int PREC>
+struct Step1Stages {
+    static constexpr int kN = 2;
+};
 
 // Resident CTAs per SM the register budget is built for.
 template <int PREC>
@@ -144,6 +151,7 @@ __global__ void __launch_bounds__(kStep1Block, Step1Shape<PREC>::kMinBlocks) k_s
     using S = Step1Stage<PREC>;
     constexpr bool kAccumT = PREC == kPrecFP64;   // FP64: the engine clock as the sum t += dt
     constexpr bool kColl = COLL == kCollHSS;
+    constexpr int kStep1Stages = Step1Stages<PREC>::kN;
 
     __shared__ __align__(128) unsigned char stage[kStep1Stages][S::kBytes];
     __shared__ __align__(8) uint64_t bar[kStep1Stages];
@@ -396,6 +404,7 @@ __global__ void __launch_bounds__(kStep1WsThreads, Step1WsShape<PREC>::kMinBlock
     using R = typename PrecT<PREC>::R;
     using Pos = typename PosOf<PREC>::T;
     using S = Step1Stage<PREC>;
+    constexpr int kStep1Stages = Step1Stages<PREC>::kN;
 
     __shared__ __align__(128) unsigned char stage[kStep1Stages][S::kBytes];
     __shared__ __align__(8) uint64_t bar[kStep1Stages];
@@ -509,6 +518,7 @@ __global__ void __launch_bounds__(kStep1WsThreads, Step1WsShape<PREC>::kMinBlock
     } else {
         // ---- the push warps ----
         const int j = tid;
+        const double t0_one = ONE ? p.t_dev[p.ens_base] : 0.0;   // the launch's clock (one ensemble)
         uint32_t uses[kStep1Stages];
 #pragma unroll
         for (int s = 0; s < kStep1Stages; ++s) uses[s] = 0u;
@@ -555,7 +565,7 @@ __global__ void __launch_bounds__(kStep1WsThreads, Step1WsShape<PREC>::kMinBlock
             bool live = (flags0 & kFlagActive) != 0;
             const int e = (ONE || !live) ? 0 : step1_ensemble(p, i);
             const EnsConst& C = p.ens[e];
-            const double t0 = p.t_dev[p.ens_base + static_cast<uint32_t>(e)];
+            const double t0 = ONE ? t0_one : p.t_dev[p.ens_base + static_cast<uint32_t>(e)];
             uint8_t flags = flags0;
             auto kill = [&]() {
                 flags = static_cast<uint8_t>(flags & ~kFlagActive);

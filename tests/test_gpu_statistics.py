@@ -77,10 +77,22 @@ def test_config0_observables_match_reference_cpu(golden, precision):
 
 
 def test_mixed_precision_accuracy_at_1M_ions():
+    """Also prints the measured differences (one JSON line per float form):
+    relative difference and its combined standard error for v_drift, K0,
+    D_L, D_T, and the two-sample KS p-value of the arrival times."""
+    import json
     n = 1_048_576
-    fp64, _, _ = device_run(n, 100000, capi.PREC_FP64)
+    fp64, fin64, _ = device_run(n, 100000, capi.PREC_FP64)
+    a64 = fin64.t_arrival[fin64.t_arrival >= 0]
     for prec in (capi.PREC_MIXED, capi.PREC_MIXED_HILO):
-        mix, _, _ = device_run(n, 100000, prec)
+        mix, fin, _ = device_run(n, 100000, prec)
+        row = {"form": {capi.PREC_MIXED: "mixed", capi.PREC_MIXED_HILO: "hilo"}[prec], "ions": n, "steps": 100000}
+        for key in ("v_drift", "K0", "D_L", "D_T"):
+            row[key] = {"rel_diff": (mix[key] - fp64[key]) / fp64[key],
+                        "rel_se": float(np.hypot(mix["se_" + key], fp64["se_" + key])) / abs(fp64[key])}
+        a = fin.t_arrival[fin.t_arrival >= 0]
+        row["arrivals"] = {"fp64": int(len(a64)), "form": int(len(a)), "ks_p": float(ob.ks_2samp(a, a64)[1])}
+        print("precision accuracy:", json.dumps(row))
         assert ob.rel_err(mix["K0"], fp64["K0"]) <= 3e-3, (prec, mix["K0"], fp64["K0"])
         assert ob.rel_err(mix["D_L"], fp64["D_L"]) <= 1e-2, (prec, mix["D_L"], fp64["D_L"])
         assert ob.rel_err(mix["D_T"], fp64["D_T"]) <= 1e-2, (prec, mix["D_T"], fp64["D_T"])
