@@ -734,11 +734,12 @@ int rebuild_time_fields(icb_handle* h) {
     }
     if (any != h->any_tf && !h->shape_tuned) {
         // launch shape of the time-dependent instance where neither the
-        // caller nor icb_autotune chose one (autotuner optimum on the TIMS
-        // workload: +10 %)
+        // caller nor icb_autotune chose one: the autotuner's optimum on the
+        // TIMS workload (64-thread blocks, a 6-lane deferred batch, 8 steps
+        // per vote: 1.05e11 ion-steps/s; 4 steps per vote gave 9.8e10)
         if (h->cfg.block_size <= 0) h->block = any ? 64 : 128;
         if (h->cfg.pending_threshold <= 0) h->pend = any ? 6u : 10u;
-        if (h->cfg.steps_per_vote <= 0) h->spv = any ? 4u : 8u;
+        if (h->cfg.steps_per_vote <= 0) h->spv = 8u;
     }
     h->any_tf = any;
     h->field_kind = any ? std::max(h->base_field_kind, static_cast<int>(kFieldLinearRF)) : h->base_field_kind;
