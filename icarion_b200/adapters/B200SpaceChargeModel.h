@@ -27,6 +27,7 @@ public:
         for (int a = 0; a < 3; ++a) { c.box_min_m[a] = -h; c.box_max_m[a] = h; }
         c.box_min_m[2] += d.geometry.origin_m.z + h; c.box_max_m[2] += d.geometry.origin_m.z + h;
         c.softening_m = -1.0;                    // 1e-10 m, SpaceChargeModelFactory.h:26
+        c.solver_fp32 = 1;                       // single-precision mesh under an FP64 push too
         if (icb_spacecharge_configure(s_.handle(), &c) != ICB_OK)
             throw std::runtime_error(icb_last_error());
     }
