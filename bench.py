@@ -71,6 +71,7 @@ STEPPING = {"events": 0, "per-step": 1, "events-all": 2}
 # sources the capture ran; the figures are used only while that hash matches
 # the current sources.
 PROFILE_FUSED = "profiles/k_step_mixed_fused_ims_1M.md"
+PROFILE_STEP1 = "profiles/k_step1_ws_mixed_per_step_16M.md"
 
 
 def profile_figures(rel: str, unit: str = "icb_step_mixed.cu") -> dict:
@@ -90,8 +91,9 @@ def profile_figures(rel: str, unit: str = "icb_step_mixed.cu") -> dict:
     fresh = bool(figs) and figs.get("source_sha256") == kernel_source_hash(unit)
     out = {"file": rel, "fresh": fresh}
     if fresh:
-        out["inst_per_launch"] = float(figs["inst_per_launch"])
-        out["dram_bytes_per_launch"] = float(figs["dram_bytes_per_launch"])
+        for key in ("inst_per_launch", "dram_bytes_per_launch"):
+            if key in figs:
+                out[key] = float(figs[key])
     else:
         out["note"] = ("no figures block" if not figs else
                        "stale: the summary was taken of other kernel sources; its figures are not used")
@@ -454,11 +456,14 @@ def run_ours(args) -> None:
         avg1 = r1["step_kernel_ms"] / n_launch
         ach1 = b1 * n1 / (avg1 * 1e-3) / 1e9
         sim1.close()
+        prof1 = (profile_figures(PROFILE_STEP1, unit="icb_step1_mixed.cu")
+                 if args.precision == "mixed" and n1 == 16 * 1048576 else {"fresh": False, "note": "not profiled"})
         per_step = {"bound": "hbm", "achieved": ach1, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                     "frac": ach1 / peaks["hbm_gbs"], "peak_source": peaks["source"], "avg_launch_ms": avg1,
-                    "kernel": f"k_step1<{args.precision},hss> (collision_test = PER_STEP), 1 step/launch",
-                    "ions": n1, "bytes_per_ion_step": b1, "launches_timed": n_launch,
-                    "ion_steps_per_s": n1 / (avg1 * 1e-3),
+                    "kernel": f"k_step1_ws<{args.precision},hss> (collision_test = PER_STEP), 1 step/launch",
+                    "ions": n1, "bytes_per_ion_step": b1, "bytes_per_launch": b1 * n1, "launches_timed": n_launch,
+                    "traffic": prof1.get("dram_bytes_per_launch"), "traffic_unit": "DRAM bytes per launch (ncu)",
+                    "profile": prof1, "ion_steps_per_s": n1 / (avg1 * 1e-3),
                     "collision_fraction": r1["collisions"] / (n1 * n_launch)}
 
     # The same workload in the other precision forms, each on a shorter

@@ -643,22 +643,33 @@ __global__ void __launch_bounds__(kStep1WsThreads, Step1WsShape<PREC>::kMinBlock
     }
 }
 
+// Persistent grid size of a kernel on the current device: resident CTAs
+// per SM x SMs, cached per device (a kernel's occupancy does not change).
+constexpr int kStep1MaxDevices = 64;
+template <class K>
+cudaError_t step1_grid_cap(K kernel, int threads, std::atomic<int>* cache, int& cap) {
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    std::atomic<int>* slot = (dev >= 0 && dev < kStep1MaxDevices) ? &cache[dev] : nullptr;
+    cap = slot ? slot->load(std::memory_order_relaxed) : 0;
+    if (cap > 0) return cudaSuccess;
+    int sms = 0, per_sm = 0;
+    err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+    if (err != cudaSuccess) return err;
+    cap = (per_sm < 1 ? 1 : per_sm) * (sms < 1 ? 1 : sms);
+    if (slot) slot->store(cap, std::memory_order_relaxed);
+    return cudaSuccess;
+}
+
 // Persistent grid: resident CTAs per SM (as compiled) x SMs, at most one
 // CTA per tile of the launch's range.
 template <int PREC, int COLL>
 cudaError_t launch_step1_coll(const StepParams& p, cudaStream_t s) {
-    static std::atomic<int> cached{0};           // CTAs per SM x SMs, 0 = not known yet
-    int cap_i = cached.load(std::memory_order_relaxed);
-    if (cap_i == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaError_t err = cudaGetDevice(&dev);
-        if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (err == cudaSuccess)
-            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step1<PREC, COLL>, kStep1Block, 0);
-        if (err != cudaSuccess) return err;
-        cap_i = (per_sm < 1 ? 1 : per_sm) * (sms < 1 ? 1 : sms);
-        cached.store(cap_i, std::memory_order_relaxed);
-    }
+    static std::atomic<int> cached[kStep1MaxDevices];
+    int cap_i = 0;
+    if (cudaError_t err = step1_grid_cap(k_step1<PREC, COLL>, kStep1Block, cached, cap_i)) return err;
     const uint64_t b = p.ens_off[0], en = p.ens_off[p.n_ens];
     if (en <= b) return cudaSuccess;
     const uint64_t tiles = (en + kStep1Block - 1) / kStep1Block - b / kStep1Block;
@@ -670,18 +681,9 @@ cudaError_t launch_step1_coll(const StepParams& p, cudaStream_t s) {
 
 template <int PREC, bool ONE>
 cudaError_t launch_step1_ws(const StepParams& p, cudaStream_t s) {
-    static std::atomic<int> cached{0};
-    int cap_i = cached.load(std::memory_order_relaxed);
-    if (cap_i == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaError_t err = cudaGetDevice(&dev);
-        if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (err == cudaSuccess)
-            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step1_ws<PREC, ONE>, kStep1WsThreads, 0);
-        if (err != cudaSuccess) return err;
-        cap_i = (per_sm < 1 ? 1 : per_sm) * (sms < 1 ? 1 : sms);
-        cached.store(cap_i, std::memory_order_relaxed);
-    }
+    static std::atomic<int> cached[kStep1MaxDevices];
+    int cap_i = 0;
+    if (cudaError_t err = step1_grid_cap(k_step1_ws<PREC, ONE>, kStep1WsThreads, cached, cap_i)) return err;
     const uint64_t b = p.ens_off[0], en = p.ens_off[p.n_ens];
     if (en <= b) return cudaSuccess;
     const uint64_t tiles = (en + kStep1Block - 1) / kStep1Block - b / kStep1Block;
