@@ -251,6 +251,10 @@ struct icb_handle {
     uint32_t pend = 0;      // 0 = precision default (set at create)
     uint32_t spv = 8;       // collision-free steps between warp votes
     bool shape_tuned = false;  // block / pend / spv chosen by icb_autotune
+    // per-step mode: the last launch finalized every ion and nothing wrote
+    // the state since, so every live ion is inside its domain (the next
+    // step's prepare has nothing to remove)
+    bool prep_ok = false;
     std::vector<double> sp_m, sp_q;   // per ensemble: shared ion mass / charge (0 = per ion)
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
@@ -894,6 +898,10 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
                 return fail(ICB_ERR_UNSUPPORTED, "the per-step collision test runs fused steps only (icb_advance)");
             if (h->any_tf || h->sc)
                 return fail(ICB_ERR_UNSUPPORTED, "the per-step collision test has no time-dependent field or space charge");
+            // prepare_ions_for_integration finds nothing to remove after a
+            // whole-population per-step launch (graphs replay their captured
+            // parameters, so they always prepare)
+            p.skip_prepare = (h->prep_ok && lo == 0 && hi >= h->n && !h->cfg.use_graphs) ? 1u : 0u;
             for (int e = 0; e < ne; ++e) {
                 EnsConst& E = p.ens[e];
                 E.sp_m = h->sp_m[static_cast<size_t>(e0 + e)];
@@ -904,7 +912,11 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
                     for (int a = 0; a < 3; ++a) {
                         E.sp_a64[a] = (E.E0[a] * E.sp_q) / E.sp_m;
                         E.sp_a32[a] = (E.E0[a] * E.sp_q) * inv_m;
+                        E.sp_fa[a] = static_cast<float>(E.sp_a32[a]);
                     }
+                    E.sp_fh = static_cast<float>(E.dt * 0.5);
+                    E.sp_fdt = static_cast<float>(E.dt);
+                    E.sp_fAmean = static_cast<float>(E.A * E.mean_th);
                 }
             }
             cudaError_t err1;
@@ -930,6 +942,7 @@ int launch_step(icb_handle* h, uint32_t K, int do_push, int do_collide, int do_f
                         h->cfg.precision, h->cfg.integrator, h->cfg.collision_model);
         if (err != cudaSuccess) return fail(ICB_ERR_CUDA, "step kernel launch: %s", cudaGetErrorString(err));
     }
+    if (h->cfg.collision_test == ICB_TEST_PER_STEP && lo == 0 && hi >= h->n) h->prep_ok = true;
     return ICB_OK;
 }
 
@@ -1217,6 +1230,7 @@ int icb_upload_ions(icb_handle* h, uint64_t n,
                     const uint8_t* active, const double* birth_time_s,
                     const uint64_t* ens_offsets, uint64_t first_ion_id) {
     if (int r = check_handle(h)) return r;
+    h->prep_ok = false;
     if (n == 0) return fail(ICB_ERR_INVALID_ARGUMENT, "no ions");
     if (!x || !y || !z || !vx || !vy || !vz || !mass_kg || !charge_C || !active)
         return fail(ICB_ERR_INVALID_ARGUMENT, "state arrays must not be NULL");
@@ -1343,6 +1357,7 @@ int icb_upload_ions(icb_handle* h, uint64_t n,
 int icb_update_state(icb_handle* h, const double* x, const double* y, const double* z,
                      const double* vx, const double* vy, const double* vz, const uint8_t* active) {
     if (int r = check_handle(h)) return r;
+    h->prep_ok = false;
     if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
     cudaStream_t s = h->stream;
     const uint64_t n = h->n;
@@ -1800,6 +1815,7 @@ int icb_autotune(icb_handle* h, uint64_t trial_steps, icb_tuning* out) {
 int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, double* y, double* z, double* vx,
                      double* vy, double* vz, uint8_t* active, icb_run_stats* stats) {
     if (int r = check_handle(h)) return r;
+    h->prep_ok = false;
     if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
     if (!x || !y || !z || !vx || !vy || !vz || !active) return fail(ICB_ERR_INVALID_ARGUMENT, "null state array");
     if (n_chunks < 1 || n_chunks > 64) return fail(ICB_ERR_INVALID_ARGUMENT, "n_chunks must be in [1, 64]");

@@ -76,6 +76,9 @@ struct EnsConst {
     // by the float forms' (E0 q) (1 / m)
     double sp_m, sp_q;
     double sp_a64[3], sp_a32[3];
+    // ... and the float forms' push constants: the acceleration, dt / 2, dt
+    // and A <|th|> rounded to float once
+    float sp_fa[3], sp_fh, sp_fdt, sp_fAmean;
 };
 
 // HSS gas mixture of one ensemble (read by the candidate step only):
@@ -202,6 +205,7 @@ struct StepParams {
     uint32_t jumps;                    // event-to-event drift where the kernel supports it
     uint32_t subcycles;                // collision sub-steps per step (plain form), >= 1
     uint32_t flows;                    // some ensemble of the launch has a parabolic gas flow
+    uint32_t skip_prepare;             // per-step kernel: every live ion was inside after the last step
     uint64_t ens_off[kMaxLaunchEns + 1];  // absolute ion offsets of the chunk's ensembles
     EnsConst ens[kMaxLaunchEns];
 };

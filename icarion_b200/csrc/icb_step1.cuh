@@ -48,6 +48,7 @@
 namespace icb {
 
 constexpr int kStep1Block = 256;    // ions per tile = threads per CTA
+static_assert(kStep1Block == 256, "tile index arithmetic shifts by 8");
 // Tiles loaded ahead per CTA (9.5 KB each in the float forms, 12.5 KB in
 // FP64).  Two keep the copies ahead of the push: four measured the same
 // (0.348 vs 0.342 ms per 16.8M-ion step), and five CTAs per SM with 40
@@ -62,6 +63,28 @@ template <int PREC>
 struct Step1Shape {
     static constexpr int kMinBlocks = PREC == kPrecFP64 ? 2 : 4;
 };
+
+// Position of the mixed form in the one-step kernel: the double position
+// itself.  A step adds (double) fmaf(v, dt, 0) per axis, the value the fused
+// kernel's anchor + float offset folds to, without the offset's
+// bookkeeping (one step per launch leaves nothing to accumulate).
+struct PosS {
+    double x, y, z;
+    __device__ void load(const StepParams& p, uint64_t i) { x = p.x[i]; y = p.y[i]; z = p.z[i]; }
+    __device__ void store(const StepParams& p, uint64_t i) const { p.x[i] = x; p.y[i] = y; p.z[i] = z; }
+    __device__ double gx() const { return x; }
+    __device__ double gy() const { return y; }
+    __device__ double gz() const { return z; }
+    __device__ void fold() {}
+    __device__ void drift(float vx, float vy, float vz, double, float d) {
+        x += static_cast<double>(fmaf(vx, d, 0.0f));
+        y += static_cast<double>(fmaf(vy, d, 0.0f));
+        z += static_cast<double>(fmaf(vz, d, 0.0f));
+    }
+    __device__ bool finite() const { return isfinite(x) && isfinite(y) && isfinite(z); }
+};
+template <int PREC> struct Step1Pos { using T = typename PosOf<PREC>::T; };
+template <> struct Step1Pos<kPrecMixed> { using T = PosS; };
 
 // Shared-memory image of one tile: position arrays, velocity arrays, flags.
 template <int PREC>
@@ -104,10 +127,6 @@ __device__ __forceinline__ void step1_pos_from_stage(Pos& x, const unsigned char
         x.xh = f[j]; x.xl = f[kStep1Block + j];
         x.yh = f[2 * kStep1Block + j]; x.yl = f[3 * kStep1Block + j];
         x.zh = f[4 * kStep1Block + j]; x.zl = f[5 * kStep1Block + j];
-    } else if constexpr (PREC == kPrecMixed) {
-        const double* d = reinterpret_cast<const double*>(st);
-        x.ax = d[j]; x.ay = d[kStep1Block + j]; x.az = d[2 * kStep1Block + j];
-        x.dx = x.dy = x.dz = 0.0f;
     } else {
         const double* d = reinterpret_cast<const double*>(st);
         x.x = d[j]; x.y = d[kStep1Block + j]; x.z = d[2 * kStep1Block + j];
@@ -120,16 +139,28 @@ __device__ __forceinline__ void step1_pos_from_stage(Pos& x, const unsigned char
 template <class R>
 __device__ __forceinline__ void step1_consts(Consts<R>& k, const EnsConst& C, const StepParams& p, uint64_t i) {
     if (C.sp_m > 0.0) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            k.a_uni[a] = static_cast<R>(sizeof(R) == 8 ? C.sp_a64[a] : C.sp_a32[a]);
-            k.ug[a] = static_cast<R>(C.ug[a]);
-        }
         k.dt = C.dt;
-        k.h = static_cast<R>(C.dt * 0.5);
-        k.dt_r = static_cast<R>(C.dt);
-        k.A = static_cast<R>(C.A);
-        k.Amean = static_cast<R>(C.A * C.mean_th);
+        if constexpr (sizeof(R) == 8) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                k.a_uni[a] = C.sp_a64[a];
+                k.ug[a] = C.ug[a];
+            }
+            k.h = C.dt * 0.5;
+            k.dt_r = C.dt;
+            k.A = C.A;
+            k.Amean = C.A * C.mean_th;
+        } else {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                k.a_uni[a] = C.sp_fa[a];
+                k.ug[a] = C.fug[a];
+            }
+            k.h = C.sp_fh;
+            k.dt_r = C.sp_fdt;
+            k.A = C.fA;
+            k.Amean = C.sp_fAmean;
+        }
     } else {
         load_consts<R, kFieldUniform, false>(k, C, p.charge[i], p.mass[i]);
     }
@@ -147,7 +178,7 @@ __device__ __forceinline__ int step1_ensemble(const StepParams& p, uint64_t i) {
 template <int PREC, int COLL>
 __global__ void __launch_bounds__(kStep1Block, Step1Shape<PREC>::kMinBlocks) k_step1(const __grid_constant__ StepParams p) {
     using R = typename PrecT<PREC>::R;
-    using Pos = typename PosOf<PREC>::T;
+    using Pos = typename Step1Pos<PREC>::T;
     using S = Step1Stage<PREC>;
     constexpr bool kAccumT = PREC == kPrecFP64;   // FP64: the engine clock as the sum t += dt
     constexpr bool kColl = COLL == kCollHSS;
@@ -262,7 +293,7 @@ __global__ void __launch_bounds__(kStep1Block, Step1Shape<PREC>::kMinBlocks) k_s
             live = false;
             ++n_dead;
         };
-        if (live && !inside(C, x)) kill(t0);     // prepare_ions_for_integration
+        if (live && !p.skip_prepare && !inside(C, x)) kill(t0);   // prepare_ions_for_integration
         for (uint32_t kk = 0; kk < p.n_steps; ++kk) {
             const uint32_t gs = step0 + kk;
             bool out = false;                     // outside the domain or non-finite after the push
@@ -281,7 +312,9 @@ __global__ void __launch_bounds__(kStep1Block, Step1Shape<PREC>::kMinBlocks) k_s
                     flags |= kFlagArrived;
                     ++n_arr;
                 }
-                out = !inside(C, x) || !x.finite();
+                // inside() already fails for non-finite x or y and infinite
+                // z; of a non-finite position only a NaN z passes it
+                out = !inside(C, x) || isnan(x.gz());
             }
             if constexpr (kColl) {
                 const int qp = static_cast<int>(pass & 1u);
@@ -402,7 +435,7 @@ template <int PREC, bool ONE>
 __global__ void __launch_bounds__(kStep1WsThreads, Step1WsShape<PREC>::kMinBlocks)
     k_step1_ws(const __grid_constant__ StepParams p) {
     using R = typename PrecT<PREC>::R;
-    using Pos = typename PosOf<PREC>::T;
+    using Pos = typename Step1Pos<PREC>::T;
     using S = Step1Stage<PREC>;
     constexpr int kStep1Stages = Step1Stages<PREC>::kN;
 
@@ -522,12 +555,13 @@ __global__ void __launch_bounds__(kStep1WsThreads, Step1WsShape<PREC>::kMinBlock
         uint32_t uses[kStep1Stages];
 #pragma unroll
         for (int s = 0; s < kStep1Stages; ++s) uses[s] = 0u;
-        for (uint64_t it = 0; it < n_it; ++it) {
+        // tiles wholly inside the range: [k_lo, k_hi)
+        const uint64_t k_lo = (b + kStep1Block - 1) / kStep1Block, k_hi = en / kStep1Block;
+        uint64_t k = tile_of(0);
+        for (uint64_t it = 0; it < n_it; ++it, k += gridDim.x) {
             const int s = static_cast<int>(it % kStep1Stages);
-            const uint64_t k = tile_of(it);
-            const uint64_t i = k * kStep1Block + static_cast<uint64_t>(j);
-            const bool bulk = staged(k);
-            const bool in_range = i >= b && i < en;
+            const uint64_t i = (k << 8) + static_cast<uint64_t>(j);
+            const bool bulk = k >= k_lo && k < k_hi;
             bool give_up = false;
             if (bulk) {
 #pragma unroll
@@ -552,7 +586,7 @@ __global__ void __launch_bounds__(kStep1WsThreads, Step1WsShape<PREC>::kMinBlock
                     const R* vv = reinterpret_cast<const R*>(st + S::kVelOff);
                     v[0] = vv[j]; v[1] = vv[kStep1Block + j]; v[2] = vv[2 * kStep1Block + j];
                 }
-            } else if (in_range) {
+            } else if (i >= b && i < en) {
                 flags0 = p.flags[i];
                 if (flags0 & kFlagActive) {
                     x.load(p, i);
@@ -573,7 +607,7 @@ __global__ void __launch_bounds__(kStep1WsThreads, Step1WsShape<PREC>::kMinBlock
                 live = false;
                 ++n_dead;
             };
-            if (live && !inside(C, x)) kill();   // prepare_ions_for_integration
+            if (live && !p.skip_prepare && !inside(C, x)) kill();   // prepare_ions_for_integration
             bool out = false, cand = false;
             if (live) {
                 Consts<R> kc;
@@ -587,7 +621,9 @@ __global__ void __launch_bounds__(kStep1WsThreads, Step1WsShape<PREC>::kMinBlock
                     flags |= kFlagArrived;
                     ++n_arr;
                 }
-                out = !inside(C, x) || !x.finite();
+                // inside() already fails for non-finite x or y and infinite
+                // z; of a non-finite position only a NaN z passes it
+                out = !inside(C, x) || isnan(x.gz());
                 const R wx = v[0] - kc.ug[0], wy = v[1] - kc.ug[1], wz = v[2] - kc.ug[2];
                 const R bb = m_sqrt(wx * wx + wy * wy + wz * wz);
                 R Q = kc.A * bb + kc.Amean;

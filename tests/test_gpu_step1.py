@@ -105,6 +105,38 @@ def test_per_step_kernel_tiles_across_ensembles_and_launch_chunks(precision):
     assert ta == tb and ta["collisions"] > 0
 
 
+@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_MIXED])
+def test_ions_moved_outside_between_steps_are_removed_at_the_next_prepare(precision):
+    """Once a step has finalized every ion the kernel skips the next step's
+    domain test at prepare; state written by the host (icb_update_state)
+    brings it back: ions moved outside the cylinder between two steps die at
+    the next step's start time, the others step on."""
+    e = config0_ensemble(detector_z_m=1e30)
+    e.update(radius_m=1.2e-3, length_m=4e-3, origin_m=[0.0, 0.0, -2e-3])
+    st0 = config0_ions(1000)
+    st0.x[:] *= 0.2
+    st0.y[:] *= 0.2
+    st0.z[:] *= 0.2
+    with Simulation([e], precision=precision, collision=capi.COLLISION_HSS, rng_seed=123,
+                    collision_test=capi.TEST_PER_STEP) as sim:
+        sim.upload(st0)
+        for _ in range(3):
+            sim.advance(1)
+        st = sim.download()
+        assert int(st.active.sum()) == 1000
+        moved = np.arange(0, 1000, 7)
+        st.x[moved] = 5e-3                       # beyond the 1.2 mm radius
+        sim.update_state(st)
+        _, t_before = sim.clock()
+        sim.advance(1)
+        out = sim.download()
+    assert np.all(out.active[moved] == 0)
+    assert np.all(out.t_death[moved] == t_before[0])
+    keep = np.setdiff1d(np.arange(1000), moved)
+    assert np.all(out.active[keep] == 1)
+    assert np.all(out.x[moved] == 5e-3)          # removed before the push: not moved
+
+
 def test_collision_free_per_step_kernel_is_the_reference_push(golden):
     z = golden("push_boris_ims.npz")
     out, _ = step1(golden_state(z), ensemble_from_golden(z), int(z["steps"]), collision=capi.COLLISION_NONE)
