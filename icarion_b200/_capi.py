@@ -196,6 +196,8 @@ SIGNATURES = {
     "icb_autotune": (C.c_int, [_H, C.c_uint64, _P(Tuning)]),
     "icb_spacecharge_configure": (C.c_int, [_H, _P(SpaceChargeConfig)]),
     "icb_spacecharge_field": (C.c_int, [_H, _DP, _DP, _DP]),
+    "icb_spacecharge_set_peers": (C.c_int, [_H, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint64]),
+    "icb_spacecharge_export": (C.c_int, [_H, C.c_void_p]),
     "icb_ipm_deflection": (C.c_int, [C.c_int, _P(IpmPotential), C.c_uint64, _DP, _DP, _DP]),
     "icb_ipm_configure": (C.c_int, [_H, _P(IpmConfig)]),
     "icb_ipm_table": (C.c_int, [_H, _FP]),

@@ -255,6 +255,11 @@ struct icb_handle {
     // the state since, so every live ion is inside its domain (the next
     // step's prepare has nothing to remove)
     bool prep_ok = false;
+    // space charge: the field bound is automatic (4 x the largest field);
+    // it was taken again with the peers' ions; the peers last set
+    bool sc_bound_auto = false, sc_peers_bounded = false;
+    const void* sc_peer_ptr = nullptr;
+    uint64_t sc_peer_n = 0, sc_peer_skip_b = 0, sc_peer_skip_n = 0;
     std::vector<double> sp_m, sp_q;   // per ensemble: shared ion mass / charge (0 = per ion)
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
@@ -1508,6 +1513,27 @@ int icb_advance(icb_handle* h, uint64_t n_steps, icb_run_stats* stats) {
     return ICB_OK;
 }
 
+// Field bound of the collision majorant: 4 x the largest space-charge field
+// of the current state (own ions, and the peers' ions when set).
+int sc_auto_bound(icb_handle* h) {
+    std::string err;
+    const int r = sc_solve(h->sc, h->x.p, h->y.p, h->z.p, h->charge.p, h->flags.p, h->n, h->stream, err);
+    if (r != ICB_OK) return fail(r, "space charge: %s", err.c_str());
+    std::vector<double> e[3];
+    for (int a = 0; a < 3; ++a) {
+        e[a].resize(h->n);
+        ICB_CUDA(cudaMemcpyAsync(e[a].data(), sc_field(h->sc, a), h->n * sizeof(double), cudaMemcpyDeviceToHost,
+                                 h->stream));
+    }
+    ICB_CUDA(cudaStreamSynchronize(h->stream));
+    double mx = 0.0;
+    for (uint64_t i = 0; i < h->n; ++i)
+        mx = std::max(mx, std::sqrt(e[0][i] * e[0][i] + e[1][i] * e[1][i] + e[2][i] * e[2][i]));
+    h->ens_const[0].Emax = h->sc_emax_base + 4.0 * mx;
+    ++h->gen;
+    return ICB_OK;
+}
+
 int icb_spacecharge_configure(icb_handle* h, const icb_spacecharge_config* cfg) {
     if (int r = check_handle(h)) return r;
     if (!cfg) return fail(ICB_ERR_INVALID_ARGUMENT, "null space-charge config");
@@ -1532,24 +1558,50 @@ int icb_spacecharge_configure(icb_handle* h, const icb_spacecharge_config* cfg) 
     if (r != ICB_OK) return fail(r, "space charge: %s", err.c_str());
     h->sc = sc;
     h->sc_emax_base = h->ens_const[0].Emax;
-    double bound = cfg->field_bound_V_m;
-    if (!(bound > 0.0)) {
-        // 4 x the largest field of the configured state
-        r = sc_solve(h->sc, h->x.p, h->y.p, h->z.p, h->charge.p, h->flags.p, h->n, h->stream, err);
-        if (r != ICB_OK) return fail(r, "space charge: %s", err.c_str());
-        std::vector<double> e[3];
-        for (int a = 0; a < 3; ++a) {
-            e[a].resize(h->n);
-            ICB_CUDA(cudaMemcpyAsync(e[a].data(), sc_field(h->sc, a), h->n * sizeof(double), cudaMemcpyDeviceToHost,
-                                     h->stream));
-        }
-        ICB_CUDA(cudaStreamSynchronize(h->stream));
-        double mx = 0.0;
-        for (uint64_t i = 0; i < h->n; ++i)
-            mx = std::max(mx, std::sqrt(e[0][i] * e[0][i] + e[1][i] * e[1][i] + e[2][i] * e[2][i]));
-        bound = 4.0 * mx;
+    h->sc_bound_auto = !(cfg->field_bound_V_m > 0.0);
+    h->sc_peers_bounded = false;
+    h->sc_peer_ptr = nullptr;
+    h->sc_peer_n = h->sc_peer_skip_b = h->sc_peer_skip_n = 0;
+    if (!h->sc_bound_auto) {
+        h->ens_const[0].Emax = h->sc_emax_base + cfg->field_bound_V_m;
+        return ICB_OK;
     }
-    h->ens_const[0].Emax = h->sc_emax_base + bound;
+    return sc_auto_bound(h);
+}
+
+// Space charge across devices: other devices' ions join this handle's solve.
+int icb_spacecharge_set_peers(icb_handle* h, uint64_t n, const double* xyzq_device, uint64_t skip_begin,
+                              uint64_t skip_count) {
+    if (int r = check_handle(h)) return r;
+    if (!h->sc) return fail(ICB_ERR_STATE, "space charge is not configured");
+    std::string err;
+    const int r = sc_set_peers(h->sc, xyzq_device, n, skip_begin, skip_count, h->stream, err);
+    if (r != ICB_OK) return fail(r, "space charge: %s", err.c_str());
+    const void* ptr = n ? static_cast<const void*>(xyzq_device) : nullptr;
+    if (ptr != h->sc_peer_ptr || n != h->sc_peer_n || skip_begin != h->sc_peer_skip_b ||
+        skip_count != h->sc_peer_skip_n) {
+        // a captured graph holds the solver's launch parameters
+        ++h->gen;
+        h->sc_peer_ptr = ptr;
+        h->sc_peer_n = n;
+        h->sc_peer_skip_b = skip_begin;
+        h->sc_peer_skip_n = skip_count;
+    }
+    // the automatic field bound is taken again with the peers' ions, once
+    if (n > 0 && h->sc_bound_auto && !h->sc_peers_bounded) {
+        h->sc_peers_bounded = true;
+        return sc_auto_bound(h);
+    }
+    return ICB_OK;
+}
+
+int icb_spacecharge_export(icb_handle* h, double* xyzq_device) {
+    if (int r = check_handle(h)) return r;
+    if (h->n == 0) return fail(ICB_ERR_STATE, "no ions uploaded");
+    if (h->hilo()) return fail(ICB_ERR_UNSUPPORTED, "space charge is built for the FP64 and mixed position forms");
+    std::string err;
+    const int r = sc_export(h->x.p, h->y.p, h->z.p, h->charge.p, h->flags.p, h->n, xyzq_device, h->stream, err);
+    if (r != ICB_OK) return fail(r, "space charge: %s", err.c_str());
     return ICB_OK;
 }
 

@@ -35,6 +35,10 @@ void sc_destroy(SpaceChargeSolver* sc);
 int sc_solve(SpaceChargeSolver* sc, const double* x, const double* y, const double* z, const double* q,
              const uint8_t* flags, uint64_t n, cudaStream_t s, std::string& err);
 const double* sc_field(const SpaceChargeSolver* sc, int axis);
+int sc_set_peers(SpaceChargeSolver* sc, const double* xyzq, uint64_t n, uint64_t skip_b, uint64_t skip_n,
+                 cudaStream_t s, std::string& err);
+int sc_export(const double* x, const double* y, const double* z, const double* q, const uint8_t* flags, uint64_t n,
+              double* out, cudaStream_t s, std::string& err);
 int sc_kernel_count(const SpaceChargeSolver* sc);
 
 // Interaction-potential physics (icb_ipm.cu).

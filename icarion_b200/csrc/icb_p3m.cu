@@ -21,6 +21,7 @@
 #include <cufft.h>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <climits>
@@ -57,15 +58,33 @@ __device__ __forceinline__ bool grid_coords(const MeshGeom& g, double x, double 
     return f[0] >= 0.0 && f[0] < g.n0 - 1 && f[1] >= 0.0 && f[1] < g.n1 - 1 && f[2] >= 0.0 && f[2] < g.n2 - 1;
 }
 
+// Slots [0, n_own) are this handle's ions; slots n_own + j the peers' ions j
+// (other devices' ions in the same solve: position, charge; a peer takes
+// part when its charge is nonzero and j is outside the skip range).
+struct PeerIons {
+    const double4* xyzq = nullptr;
+    uint32_t n = 0, skip_b = 0, skip_n = 0;
+};
+
 __global__ void k_sc_bin(MeshGeom g, const double* __restrict__ x, const double* __restrict__ y,
-                         const double* __restrict__ z, const uint8_t* __restrict__ flags, uint32_t n, int all_ions,
-                         uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                         const double* __restrict__ z, const uint8_t* __restrict__ flags, uint32_t n_own,
+                         PeerIons peers, int all_ions, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n_own + peers.n) return;
     uint32_t key = g.ncell;
-    const bool use = all_ions || ((flags[i] & 3u) == 3u);   // active and born
+    bool use;
+    double px, py, pz;
+    if (i < n_own) {
+        use = all_ions || ((flags[i] & 3u) == 3u);   // active and born
+        px = x[i]; py = y[i]; pz = z[i];
+    } else {
+        const uint32_t j = i - n_own;
+        const double4 v = peers.xyzq[j];
+        use = v.w != 0.0 && (j < peers.skip_b || j - peers.skip_b >= peers.skip_n);
+        px = v.x; py = v.y; pz = v.z;
+    }
     double f[3];
-    if (use && grid_coords(g, x[i], y[i], z[i], f)) {
+    if (use && grid_coords(g, px, py, pz, f)) {
         const int c0 = static_cast<int>(f[0]), c1 = static_cast<int>(f[1]), c2 = static_cast<int>(f[2]);
         key = (static_cast<uint32_t>(c0) * g.n1 + static_cast<uint32_t>(c1)) * g.n2 + static_cast<uint32_t>(c2);
     }
@@ -92,17 +111,41 @@ __global__ void k_sc_cell_start(const uint32_t* __restrict__ keys, uint32_t n, u
 // particle-particle loop's distance prefilter.
 __global__ void k_sc_permute(MeshGeom g, const double* __restrict__ x, const double* __restrict__ y,
                              const double* __restrict__ z, const double* __restrict__ q,
-                             const uint32_t* __restrict__ vals, uint32_t n, double4* __restrict__ ps,
-                             float4* __restrict__ pf) {
+                             const uint32_t* __restrict__ vals, uint32_t n, uint32_t n_own, PeerIons peers,
+                             double4* __restrict__ ps, float4* __restrict__ pf) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const uint32_t j = vals[s];
-    const double4 v = make_double4(x[j], y[j], z[j], q[j]);
+    const double4 v = j < n_own ? make_double4(x[j], y[j], z[j], q[j]) : peers.xyzq[j - n_own];
     ps[s] = v;
     // float copy for the particle-particle sums: position from the mesh
     // origin and the Coulomb constant times the charge
     pf[s] = make_float4(static_cast<float>(v.x - g.lo0), static_cast<float>(v.y - g.lo1),
                         static_cast<float>(v.z - g.lo2), static_cast<float>(kCoulomb * v.w));
+}
+
+// Sorted slots of this handle's own ions, in sorted order: a flag per slot,
+// its exclusive scan, then the scatter of the flagged slots.
+__global__ void k_sc_own_flag(const uint32_t* __restrict__ vals, uint32_t n, uint32_t n_own,
+                              uint32_t* __restrict__ flag) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) flag[s] = vals[s] < n_own ? 1u : 0u;
+}
+__global__ void k_sc_own_scatter(const uint32_t* __restrict__ vals, const uint32_t* __restrict__ pos, uint32_t n,
+                                 uint32_t n_own, uint32_t* __restrict__ slots) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n && vals[s] < n_own) slots[pos[s]] = s;
+}
+
+// This handle's ions as a peer list for other devices' solves: active, born
+// ions keep position and charge; the rest get charge 0 (they take no part).
+__global__ void k_sc_export(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                            const double* __restrict__ q, const uint8_t* __restrict__ flags, uint64_t n,
+                            double4* __restrict__ out) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool use = (flags[i] & 3u) == 3u;
+    out[i] = use ? make_double4(x[i], y[i], z[i], q[i]) : make_double4(0.0, 0.0, 0.0, 0.0);
 }
 
 // CIC weight of corner (ox, oy, oz) of a cell for fractions fr (taken left
@@ -297,9 +340,9 @@ template <bool REF_WEIGHTS, class GT>
 __global__ void __launch_bounds__(256, 4) k_sc_gather(MeshGeom g, PPParams pp, const double4* __restrict__ ps,
                             const float4* __restrict__ pf,
                             const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                            const uint32_t* __restrict__ start, uint32_t n, const GT* __restrict__ gx,
-                            const GT* __restrict__ gy, const GT* __restrict__ gz, double* __restrict__ ex,
-                            double* __restrict__ ey, double* __restrict__ ez) {
+                            const uint32_t* __restrict__ start, uint32_t n, const uint32_t* __restrict__ slots,
+                            const GT* __restrict__ gx, const GT* __restrict__ gy, const GT* __restrict__ gz,
+                            double* __restrict__ ex, double* __restrict__ ey, double* __restrict__ ez) {
     __shared__ double tab[REF_WEIGHTS ? 1 : kPPTable + 1];
     float* tabf = reinterpret_cast<float*>(tab);
     if (!REF_WEIGHTS && pp.on) {
@@ -313,8 +356,11 @@ __global__ void __launch_bounds__(256, 4) k_sc_gather(MeshGeom g, PPParams pp, c
     // Every lane of a warp reaches the particle-particle loops (they use
     // warp-wide ranges); lanes without an ion inside the mesh take part with
     // empty ranges.
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool in_range = s < n;
+    // thread t takes sorted slot t, or slots[t] (this handle's ions among
+    // peers' ions: n counts the own ions then)
+    const uint32_t tt = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in_range = tt < n;
+    const uint32_t s = in_range ? (slots ? slots[tt] : tt) : 0u;
     const uint32_t i = in_range ? vals[s] : 0u;
     const uint32_t key = in_range ? keys[s] : g.ncell;
     const bool act = key < g.ncell;
@@ -558,8 +604,20 @@ struct SpaceChargeSolver {
     float* egrid_f = nullptr;             // three grids, one block
     cufftComplex* ghat_f[3] = {nullptr, nullptr, nullptr};
     double max_field = 0.0;
+    // other devices' ions in this solve (icb_spacecharge_set_peers); cap
+    // covers own_cap own ions plus the peers
+    uint32_t own_cap = 0;
+    PeerIons peers{};
+    uint32_t* own_flag = nullptr;          // per sorted slot, then its scan
+    uint32_t* own_pos = nullptr;
+    uint32_t* own_slots = nullptr;         // sorted slots of the own ions
+    void* scan_tmp = nullptr;
+    size_t scan_bytes = 0;
 
     ~SpaceChargeSolver() {
+        for (void* p : {static_cast<void*>(own_flag), static_cast<void*>(own_pos), static_cast<void*>(own_slots),
+                        scan_tmp})
+            if (p) cudaFree(p);
         if (have_fwd) cufftDestroy(fwd);
         if (have_inv) cufftDestroy(inv);
         if (have_inv3) cufftDestroy(inv3);
@@ -670,6 +728,7 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, bool pp_float, c
         S.pp.rc2_pre = static_cast<float>(rc * rc * 1.001 + 1e-6 * 3.0 * (c.box_max_m[0] - c.box_min_m[0]) * rc);
     }
     S.cap = static_cast<uint32_t>(n_ions);
+    S.own_cap = S.cap;
     SC_CUDA(dev_alloc(&S.keys, S.cap));
     SC_CUDA(dev_alloc(&S.keys_sorted, S.cap));
     SC_CUDA(dev_alloc(&S.vals, S.cap));
@@ -764,19 +823,87 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, bool pp_float, c
 
 void sc_destroy(SpaceChargeSolver* S) { delete S; }
 
+int sc_set_peers(SpaceChargeSolver* S, const double* xyzq, uint64_t n, uint64_t skip_b, uint64_t skip_n,
+                 cudaStream_t s, std::string& err) {
+    if (n == 0) {
+        S->peers = PeerIons{};
+        return ICB_OK;
+    }
+    if (S->mode != ICB_SC_P3M_ISOLATED) {
+        err = "peer ions need the isolated P3M solver";
+        return ICB_ERR_UNSUPPORTED;
+    }
+    if (xyzq == nullptr || (reinterpret_cast<uintptr_t>(xyzq) & 15u) != 0u) {
+        err = "peer ions: null or misaligned device array (16-byte aligned x, y, z, q quadruples)";
+        return ICB_ERR_INVALID_ARGUMENT;
+    }
+    if (skip_b > n || skip_n > n - skip_b || static_cast<uint64_t>(S->own_cap) + n >= (1ull << 31)) {
+        err = "peer ions: skip range outside the list, or more than 2^31 ions in the solve";
+        return ICB_ERR_INVALID_ARGUMENT;
+    }
+    const uint64_t total = static_cast<uint64_t>(S->own_cap) + n;
+    if (total > S->cap || S->own_slots == nullptr) {
+        // grow the sort, permutation and slot buffers to own + peers
+        SC_CUDA(cudaStreamSynchronize(s));
+        const uint32_t cap = static_cast<uint32_t>(std::max<uint64_t>(total, S->cap));
+        for (void** p : {reinterpret_cast<void**>(&S->keys), reinterpret_cast<void**>(&S->keys_sorted),
+                         reinterpret_cast<void**>(&S->vals), reinterpret_cast<void**>(&S->vals_sorted),
+                         reinterpret_cast<void**>(&S->ps), reinterpret_cast<void**>(&S->pf), &S->cub_tmp,
+                         reinterpret_cast<void**>(&S->own_flag), reinterpret_cast<void**>(&S->own_pos),
+                         reinterpret_cast<void**>(&S->own_slots), &S->scan_tmp}) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+        }
+        S->cap = cap;
+        SC_CUDA(dev_alloc(&S->keys, cap));
+        SC_CUDA(dev_alloc(&S->keys_sorted, cap));
+        SC_CUDA(dev_alloc(&S->vals, cap));
+        SC_CUDA(dev_alloc(&S->vals_sorted, cap));
+        SC_CUDA(dev_alloc(&S->ps, cap));
+        SC_CUDA(dev_alloc(&S->pf, cap));
+        SC_CUDA(dev_alloc(&S->own_flag, cap));
+        SC_CUDA(dev_alloc(&S->own_pos, cap));
+        SC_CUDA(dev_alloc(&S->own_slots, S->own_cap));
+        S->cub_bytes = 0;
+        SC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, S->cub_bytes, S->keys, S->keys_sorted, S->vals,
+                                                S->vals_sorted, static_cast<int>(cap), 0, S->key_bits, s));
+        SC_CUDA(cudaMalloc(&S->cub_tmp, std::max<size_t>(S->cub_bytes, 16)));
+        S->scan_bytes = 0;
+        SC_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, S->scan_bytes, S->own_flag, S->own_pos, static_cast<int>(cap), s));
+        SC_CUDA(cudaMalloc(&S->scan_tmp, std::max<size_t>(S->scan_bytes, 16)));
+    }
+    S->peers.xyzq = reinterpret_cast<const double4*>(xyzq);
+    S->peers.n = static_cast<uint32_t>(n);
+    S->peers.skip_b = static_cast<uint32_t>(skip_b);
+    S->peers.skip_n = static_cast<uint32_t>(skip_n);
+    return ICB_OK;
+}
+
+int sc_export(const double* x, const double* y, const double* z, const double* q, const uint8_t* flags, uint64_t n,
+              double* out, cudaStream_t s, std::string& err) {
+    if (out == nullptr || (reinterpret_cast<uintptr_t>(out) & 15u) != 0u) {
+        err = "export: null or misaligned device array (16-byte aligned x, y, z, q quadruples)";
+        return ICB_ERR_INVALID_ARGUMENT;
+    }
+    k_sc_export<<<blocks_for(n, 256), 256, 0, s>>>(x, y, z, q, flags, n, reinterpret_cast<double4*>(out));
+    SC_CUDA(cudaGetLastError());
+    return ICB_OK;
+}
+
 int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const double* z, const double* q,
              const uint8_t* flags, uint64_t n, cudaStream_t s, std::string& err) {
-    if (n > S->cap) {
+    if (n > S->own_cap) {
         err = "more ions than the space-charge solver was configured for";
         return ICB_ERR_STATE;
     }
     const MeshGeom& g = S->g;
     const bool iso = S->mode == ICB_SC_P3M_ISOLATED;
-    const uint32_t nn = static_cast<uint32_t>(n);
+    const uint32_t n_own = static_cast<uint32_t>(n);
+    const uint32_t nn = n_own + S->peers.n;     // sorted slots: own ions and peers
     SC_FFT(cufftSetStream(S->fwd, s));
     if (S->have_inv) SC_FFT(cufftSetStream(S->inv, s));
     if (S->have_inv3) SC_FFT(cufftSetStream(S->inv3, s));
-    k_sc_bin<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, flags, nn, iso ? 0 : 1, S->keys, S->vals);
+    k_sc_bin<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, flags, n_own, S->peers, iso ? 0 : 1, S->keys, S->vals);
     SC_CUDA(cudaGetLastError());
     size_t bytes = S->cub_bytes;
     SC_CUDA(cub::DeviceRadixSort::SortPairs(S->cub_tmp, bytes, S->keys, S->keys_sorted, S->vals, S->vals_sorted,
@@ -784,8 +911,22 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
     k_sc_cell_start<<<blocks_for(static_cast<size_t>(g.ncell) + 1, 256), 256, 0, s>>>(S->keys_sorted, nn, g.ncell,
                                                                                       S->start);
     SC_CUDA(cudaGetLastError());
-    k_sc_permute<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, q, S->vals_sorted, nn, S->ps, S->pf);
+    k_sc_permute<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, q, S->vals_sorted, nn, n_own, S->peers, S->ps,
+                                                     S->pf);
     SC_CUDA(cudaGetLastError());
+    // with peers the gather runs over this handle's ions only, in sorted order
+    const uint32_t* slots = nullptr;
+    uint32_t n_gather = nn;
+    if (S->peers.n > 0) {
+        k_sc_own_flag<<<blocks_for(nn, 256), 256, 0, s>>>(S->vals_sorted, nn, n_own, S->own_flag);
+        SC_CUDA(cudaGetLastError());
+        size_t sb = S->scan_bytes;
+        SC_CUDA(cub::DeviceScan::ExclusiveSum(S->scan_tmp, sb, S->own_flag, S->own_pos, static_cast<int>(nn), s));
+        k_sc_own_scatter<<<blocks_for(nn, 256), 256, 0, s>>>(S->vals_sorted, S->own_pos, nn, n_own, S->own_slots);
+        SC_CUDA(cudaGetLastError());
+        slots = S->own_slots;
+        n_gather = n_own;
+    }
     const size_t mesh_nodes = static_cast<size_t>(g.n0) * g.n1 * g.n2;
     if (iso && S->f32) {
         SC_CUDA(cudaMemsetAsync(S->rho_f, 0, S->real_size() * sizeof(float), s));
@@ -797,9 +938,9 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
         SC_CUDA(cudaGetLastError());
         SC_FFT(cufftExecC2R(S->inv3, S->tmp_hat_f, S->egrid_f));
         const size_t rs = S->real_size();
-        k_sc_gather<false, float><<<blocks_for(nn, 256), 256, 0, s>>>(
-            g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted, S->start, nn, S->egrid_f, S->egrid_f + rs,
-            S->egrid_f + 2 * rs, S->esc[0], S->esc[1], S->esc[2]);
+        k_sc_gather<false, float><<<blocks_for(n_gather, 256), 256, 0, s>>>(
+            g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted, S->start, n_gather, slots, S->egrid_f,
+            S->egrid_f + rs, S->egrid_f + 2 * rs, S->esc[0], S->esc[1], S->esc[2]);
         SC_CUDA(cudaGetLastError());
     } else if (iso) {
         SC_CUDA(cudaMemsetAsync(S->rho, 0, S->real_size() * sizeof(double), s));
@@ -810,9 +951,9 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
                                                                     S->tmp_hat, S->cplx_size());
         SC_CUDA(cudaGetLastError());
         SC_FFT(cufftExecZ2D(S->inv3, S->tmp_hat, S->egrid[0]));
-        k_sc_gather<false, double><<<blocks_for(nn, 256), 256, 0, s>>>(g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted,
-                                                                S->start, nn, S->egrid[0], S->egrid[1], S->egrid[2],
-                                                                S->esc[0], S->esc[1], S->esc[2]);
+        k_sc_gather<false, double><<<blocks_for(n_gather, 256), 256, 0, s>>>(
+            g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted, S->start, n_gather, slots, S->egrid[0],
+            S->egrid[1], S->egrid[2], S->esc[0], S->esc[1], S->esc[2]);
         SC_CUDA(cudaGetLastError());
     } else {
         k_sc_deposit<true, double><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho);
@@ -826,9 +967,9 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
         k_sc_efield_ref<<<blocks_for(S->real_size(), 256), 256, 0, s>>>(g, S->h[0], S->h[1], S->h[2], scale, S->rho,
                                                                          S->egrid[0], S->egrid[1], S->egrid[2]);
         SC_CUDA(cudaGetLastError());
-        k_sc_gather<true, double><<<blocks_for(nn, 256), 256, 0, s>>>(g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted,
-                                                               S->start, nn, S->egrid[0], S->egrid[1], S->egrid[2],
-                                                               S->esc[0], S->esc[1], S->esc[2]);
+        k_sc_gather<true, double><<<blocks_for(n_gather, 256), 256, 0, s>>>(
+            g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted, S->start, n_gather, slots, S->egrid[0],
+            S->egrid[1], S->egrid[2], S->esc[0], S->esc[1], S->esc[2]);
         SC_CUDA(cudaGetLastError());
     }
     return ICB_OK;

@@ -246,6 +246,17 @@ class Simulation:
         c.solver_fp32 = 1 if solver_fp32 else 0
         capi.check(self._lib.icb_spacecharge_configure(self._h, C.byref(c)))
 
+    def spacecharge_export(self, xyzq_device_ptr: int) -> None:
+        """This handle's ions as (x, y, z, q) rows into a device buffer of
+        n rows (see icb_spacecharge_export)."""
+        capi.check(self._lib.icb_spacecharge_export(self._h, C.c_void_p(xyzq_device_ptr)))
+
+    def set_spacecharge_peers(self, xyzq_device_ptr: int, n: int, skip_begin: int = 0, skip_count: int = 0) -> None:
+        """Other devices' ions in this handle's solve (see
+        icb_spacecharge_set_peers); n = 0 removes them."""
+        capi.check(self._lib.icb_spacecharge_set_peers(self._h, int(n), C.c_void_p(xyzq_device_ptr or 0),
+                                                       int(skip_begin), int(skip_count)))
+
     def space_charge_field(self) -> np.ndarray:
         """[3, n] space-charge field (V/m) of the current state."""
         out = np.zeros((3, self.n))

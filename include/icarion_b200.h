@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define ICB_ABI_VERSION 9
+#define ICB_ABI_VERSION 10
 
 /* ---- status codes ------------------------------------------------------ */
 enum {
@@ -360,6 +360,23 @@ typedef struct icb_spacecharge_config {
     int32_t reserved[7];
 } icb_spacecharge_config;
 int icb_spacecharge_configure(struct icb_handle* h, const icb_spacecharge_config* cfg);
+/* Space charge across devices (one process per GPU, the ions sharded over
+ * the ranks): this handle's solve also deposits, and pairs with, the ions of
+ * the other ranks, given as a device array on this handle's device of n
+ * (x, y, z, q) double quadruples (16-byte aligned), e.g. an all-gather of
+ * every rank's icb_spacecharge_export.  Entries [skip_begin, skip_begin +
+ * skip_count) are this handle's own ions in that list and take no part, nor
+ * do entries with q = 0.  Every following solve reads the array as it is
+ * then (refresh it before each step, after the ranks' previous step); n = 0
+ * removes the peers.  The field is computed for this handle's ions only.
+ * With an automatic field bound (field_bound_V_m = 0) the first call with
+ * peers takes the bound again over the whole state.  Isolated P3M only. */
+int icb_spacecharge_set_peers(struct icb_handle* h, uint64_t n, const double* xyzq_device,
+                              uint64_t skip_begin, uint64_t skip_count);
+/* This handle's ions as (x, y, z, q) quadruples into a device array of
+ * n_ions entries on the handle's device (16-byte aligned), on the handle's
+ * stream: active, born ions with their charge, the others with q = 0. */
+int icb_spacecharge_export(struct icb_handle* h, double* xyzq_device);
 /* Solve the field of the current state and copy E_sc (V/m) of every ion to
  * host arrays (any may be NULL): ISpaceChargeModel::sample_electric_field. */
 int icb_spacecharge_field(struct icb_handle* h, double* ex, double* ey, double* ez);

@@ -62,7 +62,7 @@ def test_struct_sizes_match_c_layout():
 
 def test_abi_version_and_error_reporting_without_compute():
     lib = capi.lib()
-    assert lib.icb_abi_version() == 9
+    assert lib.icb_abi_version() == 10
     # invalid configuration is rejected before any device work
     h = C.c_void_p()
     c = capi.Config()
