@@ -137,6 +137,30 @@ def test_ions_moved_outside_between_steps_are_removed_at_the_next_prepare(precis
     assert np.all(out.x[moved] == 5e-3)          # removed before the push: not moved
 
 
+@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_MIXED])
+def test_per_step_advance_host_equals_separate_calls(precision):
+    """icb_advance_host in per-step mode: 4 overlapped ion chunks (their
+    launches cut tiles at the chunk ends and always prepare) give the state
+    of update_state + advance + download (one chunk) bit for bit."""
+    e = config0_ensemble(detector_z_m=3e-4)
+    e.update(radius_m=1.2e-3, length_m=4e-3, origin_m=[0.0, 0.0, -2e-3])
+    st0 = config0_ions(3000)
+    outs = []
+    for chunks in (1, 4):
+        with Simulation([e], precision=precision, collision=capi.COLLISION_HSS, rng_seed=5,
+                        collision_test=capi.TEST_PER_STEP) as sim:
+            sim.upload(st0)
+            host = st0.copy()
+            host.t_death = host.t_arrival = None
+            tot = 0
+            for _ in range(3):
+                tot += sim.advance_host(host, 50, n_chunks=chunks)["collisions"]
+            outs.append((host, tot))
+    for k in KEYS + ("active",):
+        assert np.array_equal(getattr(outs[0][0], k), getattr(outs[1][0], k)), k
+    assert outs[0][1] == outs[1][1] > 0
+
+
 def test_collision_free_per_step_kernel_is_the_reference_push(golden):
     z = golden("push_boris_ims.npz")
     out, _ = step1(golden_state(z), ensemble_from_golden(z), int(z["steps"]), collision=capi.COLLISION_NONE)
