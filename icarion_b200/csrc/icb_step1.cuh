@@ -406,29 +406,31 @@ __global__ void __launch_bounds__(kStep1Block, Step1Shape<PREC>::kMinBlocks) k_s
     }
 }
 
-// ---- the one-step form with a collision warp -------------------------------
+// ---- the one-step form with collision warps --------------------------------
 // One engine step per launch (n_steps = 1, the per-step loop) with
 // hard-sphere collisions.  Eight push warps hold a tile (one ion per
 // thread): they push, take the detector plane and the domain test, draw the
-// collision test and queue the candidates in shared memory; a ninth warp
-// works through the previous tile's queue meanwhile (the candidate law of
-// the block-synchronous kernel above, then the velocity half of finalize
-// and the stores of the candidate ions) and refills the stages.  Two queues
-// alternate; full and empty are mbarriers (eight arrivals / one).  A push
-// warp reads its tile's stage before it arrives on the tile's full queue,
-// so once the collision warp has that queue the stage is free and it
-// issues the stage's next fill: no warp waits for another's stage reads or
-// for the candidate chain of its own tile.  Every wait is bounded; a wait
-// that gives up sets the CTA's abort flag, which every other wait polls,
-// and the CTA reports a stall and returns once its copies have landed.
+// collision test and queue the candidates in shared memory; two collision
+// warps, each owning every other tile with its queue and stage, work through
+// the queues meanwhile (the candidate law of the block-synchronous kernel
+// above, then the velocity half of finalize and the stores of the candidate
+// ions) and refill their stages.  Full and empty queues are mbarriers (eight arrivals
+// / one).  A push warp reads its tile's stage before it arrives on the
+// tile's full queue, so once a collision warp has that queue the stage is
+// free and it issues the stage's next fill: no warp waits for another's
+// stage reads or for the candidate chain of its own tile.  Every wait is
+// bounded; a wait that gives up sets the CTA's abort flag, which every
+// other wait polls, and the CTA reports a stall and returns once its copies
+// have landed.
 constexpr int kStep1WsPush = 8;
-constexpr int kStep1WsThreads = 32 * (kStep1WsPush + 1);
+constexpr int kStep1WsColl = 2;          // collision warps: warp w takes the tiles it with it % 2 == w
+constexpr int kStep1WsThreads = 32 * (kStep1WsPush + kStep1WsColl);
 static_assert(kStep1WsPush * 32 == kStep1Block, "one push thread per ion of a tile");
 constexpr uint8_t kQueueOut = 0x80u;    // queue flag bit: the position failed finalize
 
 template <int PREC>
 struct Step1WsShape {
-    static constexpr int kMinBlocks = PREC == kPrecFP64 ? 2 : 4;
+    static constexpr int kMinBlocks = PREC == kPrecFP64 ? 2 : 3;
 };
 
 template <int PREC, bool ONE>
@@ -475,18 +477,22 @@ __global__ void __launch_bounds__(kStep1WsThreads, Step1WsShape<PREC>::kMinBlock
     const uint32_t step0 = static_cast<uint32_t>(*p.step_dev);
     uint32_t n_cand = 0, n_coll = 0, n_ovf = 0, n_dead = 0, n_arr = 0;
 
-    if (warp == kStep1WsPush) {
-        // ---- the collision warp (lane 0 also fills the stages) ----
+    if (warp >= kStep1WsPush) {
+        // ---- the collision warps: warp w takes the tiles (and their queue
+        // q = w and stage s = w) of the iterations it = w, w + 2, ...; its
+        // lane 0 also fills that stage ----
+        static_assert(kStep1WsColl == 2 && Step1Stages<PREC>::kN == 2, "one queue and one stage per collision warp");
+        const int w = warp - kStep1WsPush;
         uint32_t fills[kStep1Stages];
 #pragma unroll
         for (int s = 0; s < kStep1Stages; ++s) {
             fills[s] = 0u;
-            if (static_cast<uint64_t>(s) < n_it && staged(tile_of(s))) {
+            if (s == w && static_cast<uint64_t>(s) < n_it && staged(tile_of(s))) {
                 if (lane == 0) step1_issue<PREC>(p, tile_of(s) * kStep1Block, stage[s], &bar[s]);
                 fills[s] = 1u;
             }
         }
-        for (uint64_t it = 0; it < n_it; ++it) {
+        for (uint64_t it = static_cast<uint64_t>(w); it < n_it; it += 2) {
             const int q = static_cast<int>(it & 1u);
             const bool got = mbar_wait_or_abort(&q_full[q], static_cast<uint32_t>(it >> 1) & 1u, abortp);
             if (__any_sync(full, !got)) {
@@ -546,7 +552,7 @@ __global__ void __launch_bounds__(kStep1WsThreads, Step1WsShape<PREC>::kMinBlock
         if (lane == 0) {
 #pragma unroll
             for (int s = 0; s < kStep1Stages; ++s)
-                if (fills[s] > 0u) (void)mbar_wait_bounded(&bar[s], (fills[s] - 1u) & 1u);
+                if (s == w && fills[s] > 0u) (void)mbar_wait_bounded(&bar[s], (fills[s] - 1u) & 1u);
         }
     } else {
         // ---- the push warps ----
