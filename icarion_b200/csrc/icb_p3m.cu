@@ -107,21 +107,29 @@ __global__ void k_sc_cell_start(const uint32_t* __restrict__ keys, uint32_t n, u
 
 // Positions and charges in sorted (cell) order: the deposit and the
 // particle-particle loops then read contiguous memory.
-// A float copy of the positions relative to the mesh origin serves as the
-// particle-particle loop's distance prefilter.
+// A float copy (position relative to the mesh origin, Coulomb constant times
+// the charge) serves the particle-particle loop: per slot (x, y, z, kq) as
+// the FP64 loop's distance prefilter, or, for the float loop (`pairs`), per
+// slot pair k = s / 2 as two float4 {x0, x1, y0, y1}, {z0, z1, kq0, kq1}:
+// the packed (two-lane) FP32 instructions then take each pair's values as
+// loaded.
 __global__ void k_sc_permute(MeshGeom g, const double* __restrict__ x, const double* __restrict__ y,
                              const double* __restrict__ z, const double* __restrict__ q,
                              const uint32_t* __restrict__ vals, uint32_t n, uint32_t n_own, PeerIons peers,
-                             double4* __restrict__ ps, float4* __restrict__ pf) {
+                             int pairs, double4* __restrict__ ps, float4* __restrict__ pf) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const uint32_t j = vals[s];
     const double4 v = j < n_own ? make_double4(x[j], y[j], z[j], q[j]) : peers.xyzq[j - n_own];
     ps[s] = v;
-    // float copy for the particle-particle sums: position from the mesh
-    // origin and the Coulomb constant times the charge
-    pf[s] = make_float4(static_cast<float>(v.x - g.lo0), static_cast<float>(v.y - g.lo1),
-                        static_cast<float>(v.z - g.lo2), static_cast<float>(kCoulomb * v.w));
+    const float fx = static_cast<float>(v.x - g.lo0), fy = static_cast<float>(v.y - g.lo1);
+    const float fz = static_cast<float>(v.z - g.lo2), fq = static_cast<float>(kCoulomb * v.w);
+    if (pairs) {
+        float* b = reinterpret_cast<float*>(pf) + 8u * (s >> 1) + (s & 1u);
+        b[0] = fx; b[2] = fy; b[4] = fz; b[6] = fq;
+    } else {
+        pf[s] = make_float4(fx, fy, fz, fq);
+    }
 }
 
 // Sorted slots of this handle's own ions, in sorted order: a flag per slot,
@@ -216,11 +224,64 @@ __global__ void k_sc_cmul3(const CT* __restrict__ a, const CT* __restrict__ b0, 
     }
 }
 
-// Transformed kernel to single precision (the float forms' mesh).
-__global__ void k_sc_to_c32(const cufftDoubleComplex* __restrict__ in, cufftComplex* __restrict__ out, size_t n) {
-    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    out[i] = make_cuComplex(static_cast<float>(in[i].x), static_cast<float>(in[i].y));
+// Single-precision mesh of the isolated solver.  Field component c's
+// sampled kernel is real, odd along axis c and even along the other two
+// (k_sc_green), so its transform is imaginary, odd in k_c and even in the
+// other wave numbers.  Only the imaginary part on the quadrant
+// kx <= m0/2, ky <= m1/2 (all kz of the half spectrum) is kept: 1/8 of the
+// complex array, small enough to stay in L2 while the product streams.
+struct FoldGeom {
+    int hx, hy, hz;          // m0/2 + 1, m1/2 + 1, m2/2 + 1
+    size_t n;                // hx * hy * hz
+};
+__host__ __device__ inline FoldGeom fold_geom(const MeshGeom& g) {
+    FoldGeom f;
+    f.hx = g.m0 / 2 + 1; f.hy = g.m1 / 2 + 1; f.hz = g.m2 / 2 + 1;
+    f.n = static_cast<size_t>(f.hx) * f.hy * f.hz;
+    return f;
+}
+
+__global__ void k_sc_fold(MeshGeom g, const cufftDoubleComplex* __restrict__ gh, float* __restrict__ out) {
+    const FoldGeom f = fold_geom(g);
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= f.n) return;
+    const int kz = static_cast<int>(idx % f.hz);
+    const size_t t = idx / f.hz;
+    const int ky = static_cast<int>(t % f.hy);
+    const int kx = static_cast<int>(t / f.hy);
+    out[idx] = static_cast<float>(gh[(static_cast<size_t>(kx) * g.m1 + ky) * f.hz + kz].y);
+}
+
+// out_c = rho_hat * (i G_c) for the three components.  One thread per
+// folded point: it reads G_c once and serves the point's mirrors
+// (kx, m0 - kx) x (ky, m1 - ky), flipping G_0 at m0 - kx and G_1 at
+// m1 - ky (kx = 0 or m0/2, and likewise ky, are their own mirrors).
+__global__ void k_sc_cmul_fold(MeshGeom g, const cufftComplex* __restrict__ a, const float* __restrict__ gf,
+                               cufftComplex* __restrict__ out) {
+    const FoldGeom f = fold_geom(g);
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= f.n) return;
+    const int kz = static_cast<int>(idx % f.hz);
+    const size_t t = idx / f.hz;
+    const int ky = static_cast<int>(t % f.hy);
+    const int kx = static_cast<int>(t / f.hy);
+    const float G0 = gf[idx], G1 = gf[f.n + idx], G2 = gf[2 * f.n + idx];
+    const size_t plane = static_cast<size_t>(g.m1) * f.hz;
+    const size_t n = static_cast<size_t>(g.m0) * plane;
+    const int nx = (kx == 0 || 2 * kx == g.m0) ? 1 : 2;
+    const int ny = (ky == 0 || 2 * ky == g.m1) ? 1 : 2;
+    for (int mx = 0; mx < nx; ++mx) {
+        const size_t X = static_cast<size_t>(mx ? g.m0 - kx : kx);
+        const float g0 = mx ? -G0 : G0;
+        for (int my = 0; my < ny; ++my) {
+            const size_t Y = static_cast<size_t>(my ? g.m1 - ky : ky);
+            const float gc[3] = {g0, my ? -G1 : G1, G2};
+            const size_t o = X * plane + Y * f.hz + kz;
+            const cufftComplex u = a[o];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) out[c * n + o] = make_cuComplex(-u.y * gc[c], u.x * gc[c]);
+        }
+    }
 }
 
 __device__ __forceinline__ double e_long(double r, double alpha) {
@@ -327,7 +388,13 @@ struct PPParams {
     // float particle-particle arithmetic (the float forms): bounds in float
     int use_float;
     float rc2f, eps2f, min_d2f, inv_drf;
+    // the float loop's long-range term as a polynomial when it is accurate
+    // enough (sc_create checks): -L(r)/r^3 = sum_k pc[k] u^k, u = r^2 pu_s - 1
+    int poly;
+    float pu_s;
+    float pc[11];
 };
+constexpr int kPPPoly = 10;     // degree of that polynomial
 
 // Particle-particle table: L(r) = r^2 E_long(r) / k = erf(a r) - (2 a r /
 // sqrt(pi)) exp(-a^2 r^2) on kPPTable equal intervals of [0, r_c], linearly
@@ -336,16 +403,18 @@ constexpr int kPPTable = 4096;
 
 // Field of every ion: CIC interpolation of the mesh field (+ particle-
 // particle correction).  Thread s handles the ion in sorted slot s.
-template <bool REF_WEIGHTS, class GT>
+template <bool REF_WEIGHTS, class GT, bool POLY = false>
 __global__ void __launch_bounds__(256, 4) k_sc_gather(MeshGeom g, PPParams pp, const double4* __restrict__ ps,
                             const float4* __restrict__ pf,
                             const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                             const uint32_t* __restrict__ start, uint32_t n, const uint32_t* __restrict__ slots,
                             const GT* __restrict__ gx, const GT* __restrict__ gy, const GT* __restrict__ gz,
                             double* __restrict__ ex, double* __restrict__ ey, double* __restrict__ ez) {
-    __shared__ double tab[REF_WEIGHTS ? 1 : kPPTable + 1];
+    // the long-range table (the polynomial form has none; it runs with the
+    // float loop only)
+    __shared__ double tab[(REF_WEIGHTS || POLY) ? 1 : kPPTable + 1];
     float* tabf = reinterpret_cast<float*>(tab);
-    if (!REF_WEIGHTS && pp.on) {
+    if (!REF_WEIGHTS && !POLY && pp.on) {
         if (pp.use_float) {
             for (int k = threadIdx.x; k <= kPPTable; k += blockDim.x) tabf[k] = static_cast<float>(pp.table[k]);
         } else {
@@ -409,13 +478,14 @@ __global__ void __launch_bounds__(256, 4) k_sc_gather(MeshGeom g, PPParams pp, c
         }
     }
     if (!REF_WEIGHTS && pp.on) {
-        const float4 own = act ? pf[s] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float fxi = own.x, fyi = own.y, fzi = own.z;
         const int x0 = max(ci - pp.r0, 0), x1 = min(ci + pp.r0, g.n0 - 2);
         const int y0 = max(cj - pp.r1, 0), y1 = min(cj + pp.r1, g.n1 - 2);
         const int z0 = max(ck - pp.r2, 0), z1 = min(ck + pp.r2, g.n2 - 2);
         if (pp.use_float) {
-            // float arithmetic on positions relative to the mesh origin.
+            // float arithmetic on positions relative to the mesh origin,
+            // partners read as slot pairs (k_sc_permute) and evaluated two
+            // at a time on the packed FP32 pipe (sm_100 fma/add/mul .f32x2:
+            // one instruction for both).
             // Each (cx, cy) column contributes the cells whose z interval
             // reaches within r_c of the ion given the column's distance in x
             // and y (lower bounds, padded for rounding).  The warp walks the
@@ -425,54 +495,56 @@ __global__ void __launch_bounds__(256, 4) k_sc_gather(MeshGeom g, PPParams pp, c
             // warp pays the longest, with nearby loads): over the sorted
             // FT-ICR cloud this evaluates ~1.6 pairs per useful one where
             // walking unions costs ~2.2.  Pairs outside a lane's range or
-            // outside (min_d, r_c) add exactly nothing, so the sums equal a
-            // walk over every pair of the 5x5x5 cells.
+            // outside (min_d, r_c) add exactly nothing (the ion itself is at
+            // distance 0 < min_d), so the sums equal a walk over every pair
+            // of the cells within reach.
             const unsigned full = 0xffffffffu;
-            float Ef[3] = {0.f, 0.f, 0.f};
+            float fxi = 0.f, fyi = 0.f, fzi = 0.f;
+            if (act) {
+                const float* b = reinterpret_cast<const float*>(pf) + 8u * (s >> 1) + (s & 1u);
+                fxi = b[0]; fyi = b[2]; fzi = b[4];
+            }
             const float h0 = static_cast<float>(1.0 / g.ih0), h1 = static_cast<float>(1.0 / g.ih1);
             const float ih2 = static_cast<float>(g.ih2);
             const float rcpad = pp.rc2f * 1.0001f;
             const float zpad = 1e-4f * static_cast<float>(1.0 / g.ih2);
-            auto pair = [&](const float4& qf, bool take) {
-                const float dx = fxi - qf.x, dy = fyi - qf.y, dz = fzi - qf.z;
-                const float r2 = dx * dx + dy * dy + dz * dz;
-                const bool near = take && r2 < pp.rc2f && r2 >= pp.min_d2f;
-                const float rinv = rsqrtf(r2);
-                const float u = r2 * rinv * pp.inv_drf;
-                const int kt = max(min(static_cast<int>(u), kPPTable - 1), 0);
-                const float fr = u - static_cast<float>(kt);
-                const float L = fmaf(fr, tabf[kt + 1] - tabf[kt], tabf[kt]);
-                // kc q_j (1 / (r^2 + eps^2) - L / r^2) / r  (qf.w = kc q_j)
-                const float f = (__fdividef(1.f, r2 + pp.eps2f) - L * rinv * rinv) * rinv * qf.w;
-                const float sc = near ? f : 0.f;
-                Ef[0] = fmaf(dx, sc, Ef[0]);
-                Ef[1] = fmaf(dy, sc, Ef[1]);
-                Ef[2] = fmaf(dz, sc, Ef[2]);
-            };
-            // the same for two partners at once on the packed FP32 pipe
-            // (sm_100 fma/add/mul .f32x2: one instruction for both)
             const float2 m1 = make_float2(-1.f, -1.f);
             const float2 FX = make_float2(fxi, fxi), FY = make_float2(fyi, fyi), FZ = make_float2(fzi, fzi);
             const float2 INV = make_float2(pp.inv_drf, pp.inv_drf), EPS = make_float2(pp.eps2f, pp.eps2f);
+            const float2 US = make_float2(pp.pu_s, pp.pu_s);
             float2 E2x = make_float2(0.f, 0.f), E2y = E2x, E2z = E2x;
-            auto pair2 = [&](const float4& qa, const float4& qb, bool ta, bool tb) {
-                const float2 dX = __ffma2_rn(make_float2(qa.x, qb.x), m1, FX);
-                const float2 dY = __ffma2_rn(make_float2(qa.y, qb.y), m1, FY);
-                const float2 dZ = __ffma2_rn(make_float2(qa.z, qb.z), m1, FZ);
+            // partners 2k and 2k + 1 (ta, tb: inside the lane's range)
+            auto pair2 = [&](uint32_t k, bool ta, bool tb) {
+                const float4 xy = pf[2u * k], zq = pf[2u * k + 1u];
+                const float2 dX = __ffma2_rn(make_float2(xy.x, xy.y), m1, FX);
+                const float2 dY = __ffma2_rn(make_float2(xy.z, xy.w), m1, FY);
+                const float2 dZ = __ffma2_rn(make_float2(zq.x, zq.y), m1, FZ);
                 const float2 r2 = __ffma2_rn(dZ, dZ, __ffma2_rn(dY, dY, __fmul2_rn(dX, dX)));
                 const bool na = ta && r2.x < pp.rc2f && r2.x >= pp.min_d2f;
                 const bool nb = tb && r2.y < pp.rc2f && r2.y >= pp.min_d2f;
                 const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-                const float2 u = __fmul2_rn(__fmul2_rn(r2, ri), INV);
-                const int ka = max(min(static_cast<int>(u.x), kPPTable - 1), 0);
-                const int kb = max(min(static_cast<int>(u.y), kPPTable - 1), 0);
-                const float2 fr = __ffma2_rn(make_float2(static_cast<float>(ka), static_cast<float>(kb)), m1, u);
-                const float2 t0 = make_float2(tabf[ka], tabf[kb]), t1 = make_float2(tabf[ka + 1], tabf[kb + 1]);
-                const float2 L = __ffma2_rn(fr, __ffma2_rn(t0, m1, t1), t0);
                 const float2 re = __fadd2_rn(r2, EPS);
                 const float2 rc = make_float2(__fdividef(1.f, re.x), __fdividef(1.f, re.y));
-                const float2 nri2 = __fmul2_rn(ri, __fmul2_rn(ri, m1));           // -1 / r^2
-                const float2 f = __fmul2_rn(__fmul2_rn(__ffma2_rn(L, nri2, rc), ri), make_float2(qa.w, qb.w));
+                // 1 / ((r^2 + eps^2) r) - L(r) / r^3
+                float2 gsr;
+                if (POLY) {
+                    const float2 u = __ffma2_rn(r2, US, m1);
+                    float2 nP = make_float2(pp.pc[kPPPoly], pp.pc[kPPPoly]);
+#pragma unroll
+                    for (int c = kPPPoly - 1; c >= 0; --c) nP = __ffma2_rn(nP, u, make_float2(pp.pc[c], pp.pc[c]));
+                    gsr = __ffma2_rn(ri, rc, nP);
+                } else {
+                    const float2 uu = __fmul2_rn(__fmul2_rn(r2, ri), INV);
+                    const int ka = max(min(static_cast<int>(uu.x), kPPTable - 1), 0);
+                    const int kb = max(min(static_cast<int>(uu.y), kPPTable - 1), 0);
+                    const float2 fr = __ffma2_rn(make_float2(static_cast<float>(ka), static_cast<float>(kb)), m1, uu);
+                    const float2 t0 = make_float2(tabf[ka], tabf[kb]), t1 = make_float2(tabf[ka + 1], tabf[kb + 1]);
+                    const float2 L = __ffma2_rn(fr, __ffma2_rn(t0, m1, t1), t0);
+                    const float2 nri2 = __fmul2_rn(ri, __fmul2_rn(ri, m1));           // -1 / r^2
+                    gsr = __fmul2_rn(__ffma2_rn(L, nri2, rc), ri);
+                }
+                // kc q_j times that (zq.zw = kc q)
+                const float2 f = __fmul2_rn(gsr, make_float2(zq.z, zq.w));
                 const float2 sc = make_float2(na ? f.x : 0.f, nb ? f.y : 0.f);
                 E2x = __ffma2_rn(dX, sc, E2x);
                 E2y = __ffma2_rn(dY, sc, E2y);
@@ -508,24 +580,18 @@ __global__ void __launch_bounds__(256, 4) k_sc_gather(MeshGeom g, PPParams pp, c
                     if (usb <= usa) continue;                  // no lane has pairs in this column
                     const uint32_t len = __reduce_max_sync(full, sb - sa);
                     if (usb - usa <= len + (len >> 3) + 2u) {
-                        uint32_t s2 = usa;
-                        for (; s2 + 1u < usb; s2 += 2u)
-                            pair2(pf[s2], pf[s2 + 1u], s2 >= sa && s2 < sb && s2 != s,
-                                  s2 + 1u >= sa && s2 + 1u < sb && s2 + 1u != s);
-                        if (s2 < usb) pair(pf[s2], s2 >= sa && s2 < sb && s2 != s);
+                        for (uint32_t k = usa >> 1; 2u * k < usb; ++k)
+                            pair2(k, 2u * k >= sa && 2u * k < sb, 2u * k + 1u >= sa && 2u * k + 1u < sb);
                     } else {
-                        uint32_t s2 = sa;
-                        for (; s2 + 1u < sb; s2 += 2u) pair2(pf[s2], pf[s2 + 1u], s2 != s, s2 + 1u != s);
-                        if (s2 < sb) pair(pf[s2], s2 != s);
+                        for (uint32_t k = sa >> 1; 2u * k < sb; ++k) pair2(k, 2u * k >= sa, 2u * k + 1u < sb);
                     }
                 }
             }
-            Ef[0] += E2x.x + E2x.y;
-            Ef[1] += E2y.x + E2y.y;
-            Ef[2] += E2z.x + E2z.y;
+            const float Ef[3] = {E2x.x + E2x.y, E2y.x + E2y.y, E2z.x + E2z.y};
 #pragma unroll
             for (int c = 0; c < 3; ++c) E[c] += static_cast<double>(Ef[c]);
-        } else
+        } else if (!POLY) {
+        const float4 own = pf[s];
         for (int cx = x0; cx <= x1; ++cx) {
             for (int cy = y0; cy <= y1; ++cy) {
                 const uint32_t row = (static_cast<uint32_t>(cx) * g.n1 + static_cast<uint32_t>(cy)) * g.n2;
@@ -533,7 +599,7 @@ __global__ void __launch_bounds__(256, 4) k_sc_gather(MeshGeom g, PPParams pp, c
                 const uint32_t sb = start[row + static_cast<uint32_t>(z1) + 1u];
                 for (uint32_t s2 = sa; s2 < sb; ++s2) {
                     const float4 qf = pf[s2];
-                    const float ex0 = fxi - qf.x, ey0 = fyi - qf.y, ez0 = fzi - qf.z;
+                    const float ex0 = own.x - qf.x, ey0 = own.y - qf.y, ez0 = own.z - qf.z;
                     if (ex0 * ex0 + ey0 * ey0 + ez0 * ez0 >= pp.rc2_pre) continue;
                     const double4 pj = ps[s2];
                     const double dx = xi - pj.x, dy = yi - pj.y, dz = zi - pj.z;
@@ -552,12 +618,72 @@ __global__ void __launch_bounds__(256, 4) k_sc_gather(MeshGeom g, PPParams pp, c
                 }
             }
         }
+        }
     }
     if (!act) {
         if (in_range) { ex[i] = 0.0; ey[i] = 0.0; ez[i] = 0.0; }
         return;
     }
     ex[i] = E[0]; ey[i] = E[1]; ez[i] = E[2];
+}
+
+// L(r) / (a r)^3 as a function of x = (a r)^2: (erf(t) - 2t e^(-x) / sqrt(pi)) / t^3
+// with t = sqrt(x); by its series (2/sqrt(pi)) sum_{n>=1} (-1)^(n+1)
+// x^(n-1) 2n / (n! (2n+1)) below x = 1/4, where the difference cancels.
+double long_range_ratio(double x) {
+    if (x < 0.25) {
+        double sum = 0.0, term = 1.0;                 // term = x^(n-1) / n!
+        for (int n = 1; n < 24; ++n) {
+            if (n > 1) term *= x / n;
+            sum += ((n & 1) ? 1.0 : -1.0) * term * 2.0 * n / (2.0 * n + 1.0);
+        }
+        return 2.0 / std::sqrt(kPi) * sum;
+    }
+    const double t = std::sqrt(x);
+    return (std::erf(t) - 2.0 * t / std::sqrt(kPi) * std::exp(-x)) / (x * t);
+}
+
+// The float loop's long-range term -L(r)/r^3 as a degree-kPPPoly polynomial
+// in u = 2 r^2 / r_c^2 - 1: Chebyshev interpolation at kPPPoly + 1 nodes,
+// rewritten in powers of u and rounded to float.  Accepted (pp.poly = 1)
+// when, evaluated in float by Horner's rule as the kernel does, it is within
+// 1e-5 of the short-range term 1/r^3 - L(r)/r^3 at every r of 4096 points
+// in (0, r_c] (the table form's float rounding is ~2e-6 there); else the
+// loop keeps the table.
+void fit_long_range_poly(double alpha, double rc, PPParams& pp) {
+    constexpr int N = kPPPoly + 1;
+    const double X = alpha * alpha * rc * rc, a3 = alpha * alpha * alpha;
+    double cheb[N];
+    for (int k = 0; k < N; ++k) {
+        double acc = 0.0;
+        for (int j = 0; j < N; ++j) {
+            const double th = kPi * (j + 0.5) / N;
+            acc += a3 * long_range_ratio(0.5 * X * (std::cos(th) + 1.0)) * std::cos(k * th);
+        }
+        cheb[k] = (k == 0 ? 1.0 : 2.0) * acc / N;
+    }
+    // T_k in powers of u: T_0 = 1, T_1 = u, T_{k+1} = 2u T_k - T_{k-1}
+    double mono[N] = {}, tm[N] = {}, t0[N] = {}, t1[N] = {};
+    t0[0] = 1.0;
+    t1[1] = 1.0;
+    mono[0] = cheb[0];
+    mono[1] = cheb[1];
+    for (int k = 2; k < N; ++k) {
+        for (int e = 0; e < N; ++e) tm[e] = (e > 0 ? 2.0 * t1[e - 1] : 0.0) - t0[e];
+        for (int e = 0; e < N; ++e) { mono[e] += cheb[k] * tm[e]; t0[e] = t1[e]; t1[e] = tm[e]; }
+    }
+    for (int e = 0; e < N; ++e) pp.pc[e] = static_cast<float>(-mono[e]);
+    pp.pu_s = static_cast<float>(2.0 / (rc * rc));
+    double worst = 0.0;
+    for (int i = 1; i <= 4096; ++i) {
+        const double r = rc * i / 4096.0;
+        const float u = std::fmaf(static_cast<float>(r * r), pp.pu_s, -1.0f);
+        float np = pp.pc[kPPPoly];
+        for (int e = kPPPoly - 1; e >= 0; --e) np = std::fmaf(np, u, pp.pc[e]);
+        const double lr = a3 * long_range_ratio(alpha * alpha * r * r);
+        worst = std::max(worst, std::fabs(-static_cast<double>(np) - lr) / std::fabs(1.0 / (r * r * r) - lr));
+    }
+    pp.poly = worst <= 1e-5 ? 1 : 0;
 }
 
 template <class T>
@@ -596,14 +722,18 @@ struct SpaceChargeSolver {
     double* esc[3] = {nullptr, nullptr, nullptr};
     cufftHandle fwd = 0, inv = 0, inv3 = 0;
     bool have_fwd = false, have_inv = false, have_inv3 = false;
-    // single-precision mesh (isolated solver in the float forms)
+    // single-precision mesh (isolated solver in the float forms): the
+    // charge and the field grids hold the planes x < n0 only (the mesh);
+    // the transform runs as a 2D (y, z) pass over those planes and a 1D x
+    // pass over the whole spectrum, forward and inverse
     bool f32 = false;
-    float* rho_f = nullptr;
+    float* rho_f = nullptr;               // n0 x m1 x m2, zero outside the mesh
     cufftComplex* rho_hat_f = nullptr;
     cufftComplex* tmp_hat_f = nullptr;
-    float* egrid_f = nullptr;             // three grids, one block
-    cufftComplex* ghat_f[3] = {nullptr, nullptr, nullptr};
-    double max_field = 0.0;
+    float* egrid_f = nullptr;             // three grids of n0 x m1 x m2, one block
+    float* gfold_f = nullptr;             // three folded kernels, one block
+    cufftHandle xpass = 0, inv2 = 0;
+    bool have_xpass = false, have_inv2 = false;
     // other devices' ions in this solve (icb_spacecharge_set_peers); cap
     // covers own_cap own ions plus the peers
     uint32_t own_cap = 0;
@@ -621,6 +751,8 @@ struct SpaceChargeSolver {
         if (have_fwd) cufftDestroy(fwd);
         if (have_inv) cufftDestroy(inv);
         if (have_inv3) cufftDestroy(inv3);
+        if (have_xpass) cufftDestroy(xpass);
+        if (have_inv2) cufftDestroy(inv2);
         for (void* p : {static_cast<void*>(keys), static_cast<void*>(keys_sorted), static_cast<void*>(vals),
                         static_cast<void*>(vals_sorted), static_cast<void*>(start), static_cast<void*>(ps), static_cast<void*>(pf), static_cast<void*>(pp_table),
                         cub_tmp,
@@ -628,8 +760,7 @@ struct SpaceChargeSolver {
             if (p) cudaFree(p);
         if (egrid[0]) cudaFree(egrid[0]);   // one block holds the three grids
         for (void* q : {static_cast<void*>(rho_f), static_cast<void*>(rho_hat_f), static_cast<void*>(tmp_hat_f),
-                        static_cast<void*>(egrid_f), static_cast<void*>(ghat_f[0]), static_cast<void*>(ghat_f[1]),
-                        static_cast<void*>(ghat_f[2])})
+                        static_cast<void*>(egrid_f), static_cast<void*>(gfold_f)})
             if (q) cudaFree(q);
         for (int c = 0; c < 3; ++c) {
             if (ghat[c]) cudaFree(ghat[c]);
@@ -637,6 +768,7 @@ struct SpaceChargeSolver {
         }
     }
     size_t real_size() const { return static_cast<size_t>(g.m0) * g.m1 * g.m2; }
+    size_t mesh_planes_size() const { return static_cast<size_t>(g.n0) * g.m1 * g.m2; }
     size_t cplx_size() const { return static_cast<size_t>(g.m0) * g.m1 * (g.m2 / 2 + 1); }
 };
 
@@ -726,6 +858,7 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, bool pp_float, c
         // float positions relative to the mesh origin carry an absolute error
         // below 1e-7 of the box; the margin keeps every pair under r_c
         S.pp.rc2_pre = static_cast<float>(rc * rc * 1.001 + 1e-6 * 3.0 * (c.box_max_m[0] - c.box_min_m[0]) * rc);
+        if (pp_float) fit_long_range_poly(S.pp.alpha, rc, S.pp);
     }
     S.cap = static_cast<uint32_t>(n_ions);
     S.own_cap = S.cap;
@@ -735,7 +868,8 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, bool pp_float, c
     SC_CUDA(dev_alloc(&S.vals_sorted, S.cap));
     SC_CUDA(dev_alloc(&S.start, static_cast<size_t>(g.ncell) + 1));
     SC_CUDA(dev_alloc(&S.ps, S.cap));
-    SC_CUDA(dev_alloc(&S.pf, S.cap));
+    SC_CUDA(dev_alloc(&S.pf, static_cast<size_t>(S.cap) + 1));
+    SC_CUDA(cudaMemsetAsync(S.pf, 0, (static_cast<size_t>(S.cap) + 1) * sizeof(float4), s));
     if (iso) {
         std::vector<double> tab(kPPTable + 1);
         const double a = S.pp.alpha;
@@ -778,6 +912,7 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, bool pp_float, c
             SC_CUDA(dev_alloc(&S.tmp_hat, 3 * S.cplx_size()));
         } else {
             SC_CUDA(dev_alloc(&tmp, S.cplx_size()));
+            SC_CUDA(dev_alloc(&S.gfold_f, 3 * fold_geom(g).n));
         }
         for (int a = 0; a < 3; ++a) {
             cufftDoubleComplex* gh = tmp;
@@ -791,29 +926,42 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, bool pp_float, c
             k_sc_normalize<<<blocks_for(S.cplx_size(), 256), 256, 0, s>>>(g, gh);
             SC_CUDA(cudaGetLastError());
             if (f32) {
-                SC_CUDA(dev_alloc(&S.ghat_f[a], S.cplx_size()));
-                k_sc_to_c32<<<blocks_for(S.cplx_size(), 256), 256, 0, s>>>(gh, S.ghat_f[a], S.cplx_size());
+                const size_t nf = fold_geom(g).n;
+                k_sc_fold<<<blocks_for(nf, 256), 256, 0, s>>>(g, gh, S.gfold_f + a * nf);
                 SC_CUDA(cudaGetLastError());
             }
         }
         if (f32) {
-            // single-precision per-step mesh: R2C, products, batched C2R
+            // single-precision per-step mesh.  Forward: 2D R2C over (y, z)
+            // of the n0 mesh planes, then the x pass over every (y, kz)
+            // column (the planes x >= n0 are zero).  Inverse per component:
+            // the x pass, then the 2D C2R of the planes x < n0 only (the
+            // gather reads nothing else).
             SC_CUDA(cudaStreamSynchronize(s));
             cudaFree(tmp);
             cudaFree(S.rho);
             S.rho = nullptr;
             cufftDestroy(S.fwd);
             S.have_fwd = false;
-            SC_CUDA(dev_alloc(&S.rho_f, S.real_size()));
+            SC_CUDA(dev_alloc(&S.rho_f, S.mesh_planes_size()));
             SC_CUDA(dev_alloc(&S.rho_hat_f, S.cplx_size()));
             SC_CUDA(dev_alloc(&S.tmp_hat_f, 3 * S.cplx_size()));
-            SC_CUDA(dev_alloc(&S.egrid_f, 3 * S.real_size()));
-            SC_FFT(cufftPlan3d(&S.fwd, g.m0, g.m1, g.m2, CUFFT_R2C));
+            SC_CUDA(dev_alloc(&S.egrid_f, 3 * S.mesh_planes_size()));
+            // the deposit writes every mesh node; the rest stays zero (an
+            // out-of-place R2C leaves its input as it is)
+            SC_CUDA(cudaMemsetAsync(S.rho_f, 0, S.mesh_planes_size() * sizeof(float), s));
+            int n2d[2] = {g.m1, g.m2};
+            SC_FFT(cufftPlanMany(&S.fwd, 2, n2d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, g.n0));
             S.have_fwd = true;
             SC_FFT(cufftSetStream(S.fwd, s));
-            SC_FFT(cufftPlanMany(&S.inv3, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, 3));
-            S.have_inv3 = true;
-            SC_FFT(cufftSetStream(S.inv3, s));
+            int n1d[1] = {g.m0};
+            const int cols = g.m1 * (g.m2 / 2 + 1);
+            SC_FFT(cufftPlanMany(&S.xpass, 1, n1d, n1d, cols, 1, n1d, cols, 1, CUFFT_C2C, cols));
+            S.have_xpass = true;
+            SC_FFT(cufftSetStream(S.xpass, s));
+            SC_FFT(cufftPlanMany(&S.inv2, 2, n2d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, g.n0));
+            S.have_inv2 = true;
+            SC_FFT(cufftSetStream(S.inv2, s));
         }
     }
     SC_CUDA(cudaStreamSynchronize(s));
@@ -860,7 +1008,8 @@ int sc_set_peers(SpaceChargeSolver* S, const double* xyzq, uint64_t n, uint64_t 
         SC_CUDA(dev_alloc(&S->vals, cap));
         SC_CUDA(dev_alloc(&S->vals_sorted, cap));
         SC_CUDA(dev_alloc(&S->ps, cap));
-        SC_CUDA(dev_alloc(&S->pf, cap));
+        SC_CUDA(dev_alloc(&S->pf, static_cast<size_t>(cap) + 1));
+        SC_CUDA(cudaMemsetAsync(S->pf, 0, (static_cast<size_t>(cap) + 1) * sizeof(float4), s));
         SC_CUDA(dev_alloc(&S->own_flag, cap));
         SC_CUDA(dev_alloc(&S->own_pos, cap));
         SC_CUDA(dev_alloc(&S->own_slots, S->own_cap));
@@ -903,6 +1052,8 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
     SC_FFT(cufftSetStream(S->fwd, s));
     if (S->have_inv) SC_FFT(cufftSetStream(S->inv, s));
     if (S->have_inv3) SC_FFT(cufftSetStream(S->inv3, s));
+    if (S->have_xpass) SC_FFT(cufftSetStream(S->xpass, s));
+    if (S->have_inv2) SC_FFT(cufftSetStream(S->inv2, s));
     k_sc_bin<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, flags, n_own, S->peers, iso ? 0 : 1, S->keys, S->vals);
     SC_CUDA(cudaGetLastError());
     size_t bytes = S->cub_bytes;
@@ -911,8 +1062,8 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
     k_sc_cell_start<<<blocks_for(static_cast<size_t>(g.ncell) + 1, 256), 256, 0, s>>>(S->keys_sorted, nn, g.ncell,
                                                                                       S->start);
     SC_CUDA(cudaGetLastError());
-    k_sc_permute<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, q, S->vals_sorted, nn, n_own, S->peers, S->ps,
-                                                     S->pf);
+    k_sc_permute<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, q, S->vals_sorted, nn, n_own, S->peers,
+                                                     (S->pp.on && S->pp.use_float) ? 1 : 0, S->ps, S->pf);
     SC_CUDA(cudaGetLastError());
     // with peers the gather runs over this handle's ions only, in sorted order
     const uint32_t* slots = nullptr;
@@ -929,18 +1080,24 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
     }
     const size_t mesh_nodes = static_cast<size_t>(g.n0) * g.n1 * g.n2;
     if (iso && S->f32) {
-        SC_CUDA(cudaMemsetAsync(S->rho_f, 0, S->real_size() * sizeof(float), s));
+        const size_t cs = S->cplx_size(), ms = S->mesh_planes_size();
+        const size_t upper = cs / 2;           // planes x >= n0 of the (y, kz) spectrum
         k_sc_deposit<false, float><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho_f);
         SC_CUDA(cudaGetLastError());
         SC_FFT(cufftExecR2C(S->fwd, S->rho_f, S->rho_hat_f));
-        k_sc_cmul3<cufftComplex><<<blocks_for(S->cplx_size(), 256), 256, 0, s>>>(
-            S->rho_hat_f, S->ghat_f[0], S->ghat_f[1], S->ghat_f[2], S->tmp_hat_f, S->cplx_size());
+        SC_CUDA(cudaMemsetAsync(S->rho_hat_f + upper, 0, (cs - upper) * sizeof(cufftComplex), s));
+        SC_FFT(cufftExecC2C(S->xpass, S->rho_hat_f, S->rho_hat_f, CUFFT_FORWARD));
+        const size_t nf = fold_geom(g).n;
+        k_sc_cmul_fold<<<blocks_for(nf, 256), 256, 0, s>>>(g, S->rho_hat_f, S->gfold_f, S->tmp_hat_f);
         SC_CUDA(cudaGetLastError());
-        SC_FFT(cufftExecC2R(S->inv3, S->tmp_hat_f, S->egrid_f));
-        const size_t rs = S->real_size();
-        k_sc_gather<false, float><<<blocks_for(n_gather, 256), 256, 0, s>>>(
+        for (int c = 0; c < 3; ++c) {
+            SC_FFT(cufftExecC2C(S->xpass, S->tmp_hat_f + c * cs, S->tmp_hat_f + c * cs, CUFFT_INVERSE));
+            SC_FFT(cufftExecC2R(S->inv2, S->tmp_hat_f + c * cs, S->egrid_f + c * ms));
+        }
+        auto gather = S->pp.poly ? k_sc_gather<false, float, true> : k_sc_gather<false, float, false>;
+        gather<<<blocks_for(n_gather, 256), 256, 0, s>>>(
             g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted, S->start, n_gather, slots, S->egrid_f,
-            S->egrid_f + rs, S->egrid_f + 2 * rs, S->esc[0], S->esc[1], S->esc[2]);
+            S->egrid_f + ms, S->egrid_f + 2 * ms, S->esc[0], S->esc[1], S->esc[2]);
         SC_CUDA(cudaGetLastError());
     } else if (iso) {
         SC_CUDA(cudaMemsetAsync(S->rho, 0, S->real_size() * sizeof(double), s));

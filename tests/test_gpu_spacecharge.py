@@ -84,6 +84,34 @@ def test_isolated_p3m_matches_oracle(precision, tol):
     assert np.all(got[:, act == 0] == 0.0)
 
 
+@pytest.mark.parametrize("precision,tol", [(capi.PREC_FP64, 1e-6), (capi.PREC_MIXED, 1e-4)])
+def test_box_mesh_matches_oracle_and_solves_keep_no_state(precision, tol):
+    """A mesh with three different sizes (the mixed form's single-precision
+    mesh: 2D (y, z) transforms of the mesh planes, 1D x transforms of the
+    spectrum, folded kernel quadrant).  The field is within `tol` of the
+    oracle's RMS field (as on the cubic mesh), and a solve after another
+    cloud equals a fresh solver's solve bit for bit (nothing of the first
+    cloud stays in the grids' padding or the spectrum's upper planes)."""
+    n = (32, 24, 20)
+    lo, hi = np.array([-6e-3, -5e-3, -4.5e-3]), np.array([6e-3, 5e-3, 4.5e-3])
+    h = (hi - lo) / np.array(n)
+    first = _cloud(3000, seed=3, sigma=0.8e-3)
+    x, y, z, q = _cloud(3000)
+    act = np.ones(3000, dtype=np.uint8)
+    want = p3m.p3m_field(x, y, z, q, act, lo, h, n, 1.0 / h.max(), 2.0 * h.max())
+    with _sim(_state(*first), precision=precision) as sim:
+        sim.configure_space_charge(capi.SC_P3M_ISOLATED, n, lo, hi)
+        sim.space_charge_field()
+        sim.upload(_state(x, y, z, q))
+        got = sim.space_charge_field()
+    with _sim(_state(x, y, z, q), precision=precision) as sim:
+        sim.configure_space_charge(capi.SC_P3M_ISOLATED, n, lo, hi)
+        fresh = sim.space_charge_field()
+    assert np.array_equal(got, fresh)
+    rms = np.sqrt(np.mean(np.sum(want ** 2, axis=0)))
+    assert np.max(np.abs(got - want)) <= tol * rms
+
+
 def test_reference_periodic_solver_matches_oracle():
     x, y, z, q = _cloud(2000, seed=2)
     act = np.zeros(2000, dtype=np.uint8)                  # the reference solver ignores activity
