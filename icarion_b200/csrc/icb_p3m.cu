@@ -92,17 +92,22 @@ __global__ void k_sc_bin(MeshGeom g, const double* __restrict__ x, const double*
     vals[i] = i;
 }
 
-// start[c] = first sorted slot whose key is >= c, for c in [0, ncell].
+// start[c] = first sorted slot whose key is >= c, for c in [0, ncell]: one
+// binary search per group of four cells, then a forward scan over the keys
+// (a cell holds a few ions).
 __global__ void k_sc_cell_start(const uint32_t* __restrict__ keys, uint32_t n, uint32_t ncell,
                                 uint32_t* __restrict__ start) {
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c > ncell) return;
+    const uint32_t c0 = 4u * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (c0 > ncell) return;
     uint32_t lo = 0, hi = n;
     while (lo < hi) {
         const uint32_t mid = lo + ((hi - lo) >> 1);
-        if (keys[mid] < c) lo = mid + 1; else hi = mid;
+        if (keys[mid] < c0) lo = mid + 1; else hi = mid;
     }
-    start[c] = lo;
+    for (uint32_t c = c0; c < c0 + 4u && c <= ncell; ++c) {
+        while (lo < n && keys[lo] < c) ++lo;
+        start[c] = lo;
+    }
 }
 
 // Positions and charges in sorted (cell) order: the deposit and the
@@ -176,30 +181,32 @@ __global__ void k_sc_deposit(MeshGeom g, const double4* __restrict__ ps, const u
     const size_t t = idx / g.n2;
     const int b = static_cast<int>(t % g.n1);
     const int a = static_cast<int>(t / g.n1);
+    // cells (ci, cj, ck) with ck = c - 1, c are adjacent keys: one slot range
+    // per (ci, cj) column, each ion's ck taken from its position as k_sc_bin
+    // took it (the same sums in the same order as cell by cell)
+    const int kz0 = max(c - 1, 0), kz1 = min(c, g.n2 - 2);
     double acc = 0.0;
     for (int ci = a - 1; ci <= a; ++ci) {
         if (ci < 0 || ci > g.n0 - 2) continue;
         for (int cj = b - 1; cj <= b; ++cj) {
-            if (cj < 0 || cj > g.n1 - 2) continue;
-            for (int ck = c - 1; ck <= c; ++ck) {
-                if (ck < 0 || ck > g.n2 - 2) continue;
-                const uint32_t key = (static_cast<uint32_t>(ci) * g.n1 + static_cast<uint32_t>(cj)) * g.n2 +
-                                     static_cast<uint32_t>(ck);
-                const uint32_t s1 = start[key + 1];
-                for (uint32_t s = start[key]; s < s1; ++s) {
-                    const double4 pj = ps[s];
-                    const double fx = (pj.x - g.lo0) * g.ih0 - ci;
-                    const double fy = (pj.y - g.lo1) * g.ih1 - cj;
-                    const double fz = (pj.z - g.lo2) * g.ih2 - ck;
-                    double w;
-                    if (REF_WEIGHTS) {
-                        w = static_cast<double>(cic_w<float>(a - ci, b - cj, c - ck, static_cast<float>(fx),
-                                                             static_cast<float>(fy), static_cast<float>(fz)));
-                    } else {
-                        w = cic_w<double>(a - ci, b - cj, c - ck, fx, fy, fz);
-                    }
-                    acc += w * pj.w;
+            if (cj < 0 || cj > g.n1 - 2 || kz0 > kz1) continue;
+            const uint32_t row = (static_cast<uint32_t>(ci) * g.n1 + static_cast<uint32_t>(cj)) * g.n2;
+            const uint32_t s1 = start[row + static_cast<uint32_t>(kz1) + 1u];
+            for (uint32_t s = start[row + static_cast<uint32_t>(kz0)]; s < s1; ++s) {
+                const double4 pj = ps[s];
+                const double gz = (pj.z - g.lo2) * g.ih2;
+                const int ck = static_cast<int>(gz);
+                const double fx = (pj.x - g.lo0) * g.ih0 - ci;
+                const double fy = (pj.y - g.lo1) * g.ih1 - cj;
+                const double fz = gz - ck;
+                double w;
+                if (REF_WEIGHTS) {
+                    w = static_cast<double>(cic_w<float>(a - ci, b - cj, c - ck, static_cast<float>(fx),
+                                                         static_cast<float>(fy), static_cast<float>(fz)));
+                } else {
+                    w = cic_w<double>(a - ci, b - cj, c - ck, fx, fy, fz);
                 }
+                acc += w * pj.w;
             }
         }
     }
@@ -401,33 +408,22 @@ constexpr int kPPPoly = 10;     // degree of that polynomial
 // interpolated (relative error ~ (a r_c / kPPTable)^2 / 8 ~ 3e-8 at a r_c = 2).
 constexpr int kPPTable = 4096;
 
-// Field of every ion: CIC interpolation of the mesh field (+ particle-
-// particle correction).  Thread s handles the ion in sorted slot s.
-template <bool REF_WEIGHTS, class GT, bool POLY = false>
-__global__ void __launch_bounds__(256, 4) k_sc_gather(MeshGeom g, PPParams pp, const double4* __restrict__ ps,
-                            const float4* __restrict__ pf,
+// Field of one ion: CIC interpolation of the mesh field (+ particle-
+// particle correction).  Thread tt handles the ion in sorted slot tt (or
+// slots[tt]).
+template <bool REF_WEIGHTS, class GT, bool POLY>
+__device__ __forceinline__ void sc_gather_ion(uint32_t tt, const MeshGeom& g, const PPParams& pp,
+                            const double4* __restrict__ ps, const float4* __restrict__ pf,
                             const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                             const uint32_t* __restrict__ start, uint32_t n, const uint32_t* __restrict__ slots,
                             const GT* __restrict__ gx, const GT* __restrict__ gy, const GT* __restrict__ gz,
-                            double* __restrict__ ex, double* __restrict__ ey, double* __restrict__ ez) {
-    // the long-range table (the polynomial form has none; it runs with the
-    // float loop only)
-    __shared__ double tab[(REF_WEIGHTS || POLY) ? 1 : kPPTable + 1];
-    float* tabf = reinterpret_cast<float*>(tab);
-    if (!REF_WEIGHTS && !POLY && pp.on) {
-        if (pp.use_float) {
-            for (int k = threadIdx.x; k <= kPPTable; k += blockDim.x) tabf[k] = static_cast<float>(pp.table[k]);
-        } else {
-            for (int k = threadIdx.x; k <= kPPTable; k += blockDim.x) tab[k] = pp.table[k];
-        }
-        __syncthreads();
-    }
+                            double* __restrict__ ex, double* __restrict__ ey, double* __restrict__ ez,
+                            const double* tab, const float* tabf) {
     // Every lane of a warp reaches the particle-particle loops (they use
     // warp-wide ranges); lanes without an ion inside the mesh take part with
     // empty ranges.
     // thread t takes sorted slot t, or slots[t] (this handle's ions among
     // peers' ions: n counts the own ions then)
-    const uint32_t tt = blockIdx.x * blockDim.x + threadIdx.x;
     const bool in_range = tt < n;
     const uint32_t s = in_range ? (slots ? slots[tt] : tt) : 0u;
     const uint32_t i = in_range ? vals[s] : 0u;
@@ -550,30 +546,37 @@ __global__ void __launch_bounds__(256, 4) k_sc_gather(MeshGeom g, PPParams pp, c
                 E2y = __ffma2_rn(dY, sc, E2y);
                 E2z = __ffma2_rn(dZ, sc, E2z);
             };
+            // slot range [sa, sb) of column (cx, cy) for this ion (dxa: its
+            // distance to the column's x slab)
+            auto column = [&](int cx, float dxa, int cy, uint32_t& sa, uint32_t& sb) {
+                sa = 0u;
+                sb = 0u;
+                const float dya = fmaxf(0.f, fmaxf(static_cast<float>(cy) * h1 - fyi,
+                                                   fyi - static_cast<float>(cy + 1) * h1));
+                const float rem = rcpad - dxa * dxa - dya * dya;
+                if (rem > 0.f) {
+                    const float dzm = sqrtf(rem) + zpad;
+                    const int za = max(z0, static_cast<int>(floorf((fzi - dzm) * ih2)));
+                    const int zb = min(z1, static_cast<int>(floorf((fzi + dzm) * ih2)));
+                    if (za <= zb) {
+                        const uint32_t row = (static_cast<uint32_t>(cx) * g.n1 + static_cast<uint32_t>(cy)) * g.n2;
+                        sa = start[row + static_cast<uint32_t>(za)];
+                        sb = start[row + static_cast<uint32_t>(zb) + 1u];
+                    }
+                }
+            };
+            auto slab = [&](int cx) {
+                return fmaxf(0.f, fmaxf(static_cast<float>(cx) * h0 - fxi, fxi - static_cast<float>(cx + 1) * h0));
+            };
             const int wx0 = __reduce_min_sync(full, act ? x0 : INT_MAX);
             const int wx1 = __reduce_max_sync(full, act ? x1 : INT_MIN);
             const int wy0 = __reduce_min_sync(full, act ? y0 : INT_MAX);
             const int wy1 = __reduce_max_sync(full, act ? y1 : INT_MIN);
             for (int cx = wx0; cx <= wx1; ++cx) {
-                const float dxa = fmaxf(0.f, fmaxf(static_cast<float>(cx) * h0 - fxi,
-                                                   fxi - static_cast<float>(cx + 1) * h0));
+                const float dxa = slab(cx);
                 for (int cy = wy0; cy <= wy1; ++cy) {
                     uint32_t sa = 0u, sb = 0u;
-                    if (act && cx >= x0 && cx <= x1 && cy >= y0 && cy <= y1) {
-                        const float dya = fmaxf(0.f, fmaxf(static_cast<float>(cy) * h1 - fyi,
-                                                           fyi - static_cast<float>(cy + 1) * h1));
-                        const float rem = rcpad - dxa * dxa - dya * dya;
-                        if (rem > 0.f) {
-                            const float dzm = sqrtf(rem) + zpad;
-                            const int za = max(z0, static_cast<int>(floorf((fzi - dzm) * ih2)));
-                            const int zb = min(z1, static_cast<int>(floorf((fzi + dzm) * ih2)));
-                            if (za <= zb) {
-                                const uint32_t row = (static_cast<uint32_t>(cx) * g.n1 + static_cast<uint32_t>(cy)) * g.n2;
-                                sa = start[row + static_cast<uint32_t>(za)];
-                                sb = start[row + static_cast<uint32_t>(zb) + 1u];
-                            }
-                        }
-                    }
+                    if (act && cx >= x0 && cx <= x1 && cy >= y0 && cy <= y1) column(cx, dxa, cy, sa, sb);
                     const bool has = sb > sa;
                     const uint32_t usa = __reduce_min_sync(full, has ? sa : 0xffffffffu);
                     const uint32_t usb = __reduce_max_sync(full, has ? sb : 0u);
@@ -625,6 +628,33 @@ __global__ void __launch_bounds__(256, 4) k_sc_gather(MeshGeom g, PPParams pp, c
         return;
     }
     ex[i] = E[0]; ey[i] = E[1]; ez[i] = E[2];
+}
+
+// Field of every ion, one thread per ion in sorted order (blocks of
+// consecutive ions share their partners in L1).  The polynomial form runs
+// blocks of 128: finer blocks leave fewer warps waiting for their block's
+// slowest one (the cloud's dense middle costs many times its edges).
+template <bool REF_WEIGHTS, class GT, bool POLY = false>
+__global__ void __launch_bounds__(POLY ? 128 : 256, POLY ? 8 : 4) k_sc_gather(MeshGeom g, PPParams pp,
+                            const double4* __restrict__ ps, const float4* __restrict__ pf,
+                            const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                            const uint32_t* __restrict__ start, uint32_t n, const uint32_t* __restrict__ slots,
+                            const GT* __restrict__ gx, const GT* __restrict__ gy, const GT* __restrict__ gz,
+                            double* __restrict__ ex, double* __restrict__ ey, double* __restrict__ ez) {
+    // the long-range table (the polynomial form has none; it runs with the
+    // float loop only)
+    __shared__ double tab[(REF_WEIGHTS || POLY) ? 1 : kPPTable + 1];
+    float* tabf = reinterpret_cast<float*>(tab);
+    if (!REF_WEIGHTS && !POLY && pp.on) {
+        if (pp.use_float) {
+            for (int k = threadIdx.x; k <= kPPTable; k += blockDim.x) tabf[k] = static_cast<float>(pp.table[k]);
+        } else {
+            for (int k = threadIdx.x; k <= kPPTable; k += blockDim.x) tab[k] = pp.table[k];
+        }
+        __syncthreads();
+    }
+    sc_gather_ion<REF_WEIGHTS, GT, POLY>(blockIdx.x * blockDim.x + threadIdx.x, g, pp, ps, pf, keys, vals, start, n,
+                                         slots, gx, gy, gz, ex, ey, ez, tab, tabf);
 }
 
 // L(r) / (a r)^3 as a function of x = (a r)^2: (erf(t) - 2t e^(-x) / sqrt(pi)) / t^3
@@ -1059,8 +1089,8 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
     size_t bytes = S->cub_bytes;
     SC_CUDA(cub::DeviceRadixSort::SortPairs(S->cub_tmp, bytes, S->keys, S->keys_sorted, S->vals, S->vals_sorted,
                                             static_cast<int>(nn), 0, S->key_bits, s));
-    k_sc_cell_start<<<blocks_for(static_cast<size_t>(g.ncell) + 1, 256), 256, 0, s>>>(S->keys_sorted, nn, g.ncell,
-                                                                                      S->start);
+    k_sc_cell_start<<<blocks_for((static_cast<size_t>(g.ncell) + 4) / 4, 256), 256, 0, s>>>(S->keys_sorted, nn,
+                                                                                            g.ncell, S->start);
     SC_CUDA(cudaGetLastError());
     k_sc_permute<<<blocks_for(nn, 256), 256, 0, s>>>(g, x, y, z, q, S->vals_sorted, nn, n_own, S->peers,
                                                      (S->pp.on && S->pp.use_float) ? 1 : 0, S->ps, S->pf);
@@ -1095,7 +1125,8 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
             SC_FFT(cufftExecC2R(S->inv2, S->tmp_hat_f + c * cs, S->egrid_f + c * ms));
         }
         auto gather = S->pp.poly ? k_sc_gather<false, float, true> : k_sc_gather<false, float, false>;
-        gather<<<blocks_for(n_gather, 256), 256, 0, s>>>(
+        const int gb = S->pp.poly ? 128 : 256;
+        gather<<<blocks_for(n_gather, gb), gb, 0, s>>>(
             g, S->pp, S->ps, S->pf, S->keys_sorted, S->vals_sorted, S->start, n_gather, slots, S->egrid_f,
             S->egrid_f + ms, S->egrid_f + 2 * ms, S->esc[0], S->esc[1], S->esc[2]);
         SC_CUDA(cudaGetLastError());
