@@ -248,7 +248,10 @@ __host__ __device__ inline FoldGeom fold_geom(const MeshGeom& g) {
     return f;
 }
 
-__global__ void k_sc_fold(MeshGeom g, const cufftDoubleComplex* __restrict__ gh, float* __restrict__ out) {
+// Layout [kx][ky][kz], or with `kx_inner` [ky][kz][kx] (the fused x pass
+// reads a column's kx run contiguously).
+__global__ void k_sc_fold(MeshGeom g, const cufftDoubleComplex* __restrict__ gh, int kx_inner,
+                          float* __restrict__ out) {
     const FoldGeom f = fold_geom(g);
     const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= f.n) return;
@@ -256,7 +259,8 @@ __global__ void k_sc_fold(MeshGeom g, const cufftDoubleComplex* __restrict__ gh,
     const size_t t = idx / f.hz;
     const int ky = static_cast<int>(t % f.hy);
     const int kx = static_cast<int>(t / f.hy);
-    out[idx] = static_cast<float>(gh[(static_cast<size_t>(kx) * g.m1 + ky) * f.hz + kz].y);
+    const size_t o = kx_inner ? (static_cast<size_t>(ky) * f.hz + kz) * f.hx + kx : idx;
+    out[o] = static_cast<float>(gh[(static_cast<size_t>(kx) * g.m1 + ky) * f.hz + kz].y);
 }
 
 // out_c = rho_hat * (i G_c) for the three components.  One thread per
@@ -287,6 +291,157 @@ __global__ void k_sc_cmul_fold(MeshGeom g, const cufftComplex* __restrict__ a, c
             const cufftComplex u = a[o];
 #pragma unroll
             for (int c = 0; c < 3; ++c) out[c * n + o] = make_cuComplex(-u.y * gc[c], u.x * gc[c]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused x pass of the single-precision mesh for a padded x length of 256 (a
+// 128-node mesh axis).  Per (ky, kz) column of the 2D-transformed mesh
+// planes: the forward 256-point transform along x (inputs x >= 128 are the
+// zero padding), the products with i G_c of the three field components,
+// and their inverse transforms, keeping the outputs x < 128 (the mesh
+// planes the gather reads).  The unfused path's three whole spectra are
+// never written or read back.  256 = 16 x 16: a block of 256 threads takes
+// 16 columns, 16 threads a column, each thread 16 points in registers; a
+// transform is two 16-point DFTs with the 256-point twiddles between them
+// and one transpose through shared memory (rows of 17 against bank
+// conflicts; 273 float2 a column keeps the column-major staging
+// conflict-free too).
+constexpr int kXLen = 256;
+constexpr int kXCols = 16;
+constexpr int kXStride = 273;
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// 4-point DFT in place, y_k = sum_n a_n w^(n k), w = -i (forward) or +i.
+template <bool INV>
+__device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2& a3) {
+    const float2 s02 = make_float2(a0.x + a2.x, a0.y + a2.y), d02 = make_float2(a0.x - a2.x, a0.y - a2.y);
+    const float2 s13 = make_float2(a1.x + a3.x, a1.y + a3.y), d13 = make_float2(a1.x - a3.x, a1.y - a3.y);
+    const float2 r = INV ? make_float2(-d13.y, d13.x) : make_float2(d13.y, -d13.x);   // w * d13
+    a0 = make_float2(s02.x + s13.x, s02.y + s13.y);
+    a1 = make_float2(d02.x + r.x, d02.y + r.y);
+    a2 = make_float2(s02.x - s13.x, s02.y - s13.y);
+    a3 = make_float2(d02.x - r.x, d02.y - r.y);
+}
+
+// exp(-+2 pi i m / 16) for the exponents a 4 x 4 split uses (m = n2 k1)
+template <bool INV>
+__device__ __forceinline__ float2 w16(int m) {
+    constexpr float c1 = 0.923879532511286756f, s1 = 0.382683432365089772f, r2 = 0.707106781186547524f;
+    float c = 1.f, sn = 0.f;
+    switch (m) {
+        case 1: c = c1; sn = s1; break;
+        case 2: c = r2; sn = r2; break;
+        case 3: c = s1; sn = c1; break;
+        case 4: c = 0.f; sn = 1.f; break;
+        case 6: c = -r2; sn = r2; break;
+        case 9: c = -c1; sn = -s1; break;
+        default: break;
+    }
+    return make_float2(c, INV ? sn : -sn);
+}
+
+// 16-point DFT in registers, v_k = sum_n v_n w^(n k), w = exp(-+2 pi i/16):
+// n = 4 n1 + n2, k = k1 + 4 k2; 4-point DFTs over n1, twiddles w^(n2 k1),
+// 4-point DFTs over n2, then natural order.
+template <bool INV>
+__device__ __forceinline__ void dft16(float2 (&v)[16]) {
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) dft4<INV>(v[n2], v[4 + n2], v[8 + n2], v[12 + n2]);
+#pragma unroll
+    for (int n2 = 1; n2 < 4; ++n2) {
+#pragma unroll
+        for (int k1 = 1; k1 < 4; ++k1) v[4 * k1 + n2] = cmulf(v[4 * k1 + n2], w16<INV>(n2 * k1));
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) dft4<INV>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+    float2 t[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) t[k1 + 4 * k2] = v[4 * k1 + k2];
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = t[k];
+}
+
+// in: the mesh planes x < 128 of the 2D-transformed charge, [x][ky][kz];
+// gf: the folded kernels, [c][ky][kz][kx] (k_sc_fold with kx_inner);
+// out: component c's planes x < 128 after the x pass, at c * 128 * P;
+// tw: exp(-2 pi i m / 256), m < 256.
+__global__ void __launch_bounds__(256) k_sc_xconv(MeshGeom g, const float2* __restrict__ in,
+                                                  const float* __restrict__ gf, const float2* __restrict__ tw,
+                                                  float2* __restrict__ out) {
+    __shared__ float2 buf[kXCols * kXStride];
+    __shared__ float2 w[kXLen];
+    const FoldGeom f = fold_geom(g);
+    const uint32_t P = static_cast<uint32_t>(g.m1) * static_cast<uint32_t>(f.hz);    // (ky, kz) columns
+    const uint32_t j0 = blockIdx.x * kXCols;
+    const int col = threadIdx.x >> 4, t = threadIdx.x & 15;
+    w[threadIdx.x] = tw[threadIdx.x];
+    for (int e = threadIdx.x; e < (kXLen / 2) * kXCols; e += blockDim.x) {
+        const int x = e >> 4, c = e & 15;
+        const uint32_t j = j0 + c;
+        buf[c * kXStride + x] = j < P ? in[static_cast<size_t>(x) * P + j] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2* bc = buf + col * kXStride;
+    float2 v[16];
+    // forward: x = 16 x1 + t, k = k1 + 16 k2
+#pragma unroll
+    for (int x1 = 0; x1 < 16; ++x1) v[x1] = x1 < 8 ? bc[16 * x1 + t] : make_float2(0.f, 0.f);
+    __syncthreads();
+    dft16<false>(v);
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) bc[t * 17 + k1] = cmulf(v[k1], w[(t * k1) & 255]);
+    __syncthreads();
+#pragma unroll
+    for (int x2 = 0; x2 < 16; ++x2) v[x2] = bc[x2 * 17 + t];
+    dft16<false>(v);
+    float2 X[16];                                   // X[k2] = spectrum at kx = t + 16 k2
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) X[k2] = v[k2];
+    const uint32_t j = j0 + col;
+    const bool live = j < P;
+    const int ky = live ? static_cast<int>(j / f.hz) : 0, kz = live ? static_cast<int>(j % f.hz) : 0;
+    const int kyf = min(ky, g.m1 - ky);
+    const float sy = 2 * ky > g.m1 ? -1.f : 1.f;
+    for (int c = 0; c < 3; ++c) {
+        // kernel values in [ky][kz][kx] order: a column's kx run is contiguous
+        const float* gc = gf + c * f.n + (static_cast<size_t>(kyf) * f.hz + kz) * f.hx;
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2) {
+            const int kx = t + 16 * k2;
+            const int kxf = min(kx, kXLen - kx);
+            float G = live ? gc[kxf] : 0.f;
+            if (c == 0 && kx > kXLen / 2) G = -G;
+            if (c == 1) G *= sy;
+            v[k2] = make_float2(-G * X[k2].y, G * X[k2].x);
+        }
+        // inverse: k = t + 16 k2, x = r + 16 q; only q < 8 is kept
+        dft16<true>(v);
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const float2 wr = w[(r * t) & 255];
+            bc[r * 17 + t] = cmulf(v[r], make_float2(wr.x, -wr.y));
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k1 = 0; k1 < 16; ++k1) v[k1] = bc[t * 17 + k1];
+        dft16<true>(v);
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 8; ++q) bc[t + 16 * q] = v[q];
+        __syncthreads();
+        float2* oc = out + static_cast<size_t>(c) * (kXLen / 2) * P;
+        for (int e = threadIdx.x; e < (kXLen / 2) * kXCols; e += blockDim.x) {
+            const int x = e >> 4, cc = e & 15;
+            if (j0 + cc < P) oc[static_cast<size_t>(x) * P + j0 + cc] = buf[cc * kXStride + x];
         }
     }
 }
@@ -764,6 +919,10 @@ struct SpaceChargeSolver {
     float* gfold_f = nullptr;             // three folded kernels, one block
     cufftHandle xpass = 0, inv2 = 0;
     bool have_xpass = false, have_inv2 = false;
+    // a padded x length of 256 runs the fused x pass (k_sc_xconv) in place
+    // of the cuFFT x passes and the separate kernel products
+    bool xfused = false;
+    float2* tw256 = nullptr;
     // other devices' ions in this solve (icb_spacecharge_set_peers); cap
     // covers own_cap own ions plus the peers
     uint32_t own_cap = 0;
@@ -790,7 +949,7 @@ struct SpaceChargeSolver {
             if (p) cudaFree(p);
         if (egrid[0]) cudaFree(egrid[0]);   // one block holds the three grids
         for (void* q : {static_cast<void*>(rho_f), static_cast<void*>(rho_hat_f), static_cast<void*>(tmp_hat_f),
-                        static_cast<void*>(egrid_f), static_cast<void*>(gfold_f)})
+                        static_cast<void*>(egrid_f), static_cast<void*>(gfold_f), static_cast<void*>(tw256)})
             if (q) cudaFree(q);
         for (int c = 0; c < 3; ++c) {
             if (ghat[c]) cudaFree(ghat[c]);
@@ -957,7 +1116,7 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, bool pp_float, c
             SC_CUDA(cudaGetLastError());
             if (f32) {
                 const size_t nf = fold_geom(g).n;
-                k_sc_fold<<<blocks_for(nf, 256), 256, 0, s>>>(g, gh, S.gfold_f + a * nf);
+                k_sc_fold<<<blocks_for(nf, 256), 256, 0, s>>>(g, gh, g.m0 == kXLen ? 1 : 0, S.gfold_f + a * nf);
                 SC_CUDA(cudaGetLastError());
             }
         }
@@ -984,11 +1143,21 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, bool pp_float, c
             SC_FFT(cufftPlanMany(&S.fwd, 2, n2d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, g.n0));
             S.have_fwd = true;
             SC_FFT(cufftSetStream(S.fwd, s));
-            int n1d[1] = {g.m0};
-            const int cols = g.m1 * (g.m2 / 2 + 1);
-            SC_FFT(cufftPlanMany(&S.xpass, 1, n1d, n1d, cols, 1, n1d, cols, 1, CUFFT_C2C, cols));
-            S.have_xpass = true;
-            SC_FFT(cufftSetStream(S.xpass, s));
+            S.xfused = g.m0 == kXLen;
+            if (S.xfused) {
+                std::vector<float2> tw(kXLen);
+                for (int m = 0; m < kXLen; ++m)
+                    tw[m] = make_float2(static_cast<float>(std::cos(2.0 * kPi * m / kXLen)),
+                                        static_cast<float>(-std::sin(2.0 * kPi * m / kXLen)));
+                SC_CUDA(dev_alloc(&S.tw256, kXLen));
+                SC_CUDA(cudaMemcpy(S.tw256, tw.data(), kXLen * sizeof(float2), cudaMemcpyHostToDevice));
+            } else {
+                int n1d[1] = {g.m0};
+                const int cols = g.m1 * (g.m2 / 2 + 1);
+                SC_FFT(cufftPlanMany(&S.xpass, 1, n1d, n1d, cols, 1, n1d, cols, 1, CUFFT_C2C, cols));
+                S.have_xpass = true;
+                SC_FFT(cufftSetStream(S.xpass, s));
+            }
             SC_FFT(cufftPlanMany(&S.inv2, 2, n2d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, g.n0));
             S.have_inv2 = true;
             SC_FFT(cufftSetStream(S.inv2, s));
@@ -1115,6 +1284,12 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
         k_sc_deposit<false, float><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho_f);
         SC_CUDA(cudaGetLastError());
         SC_FFT(cufftExecR2C(S->fwd, S->rho_f, S->rho_hat_f));
+        if (S->xfused) {
+            const size_t P = static_cast<size_t>(g.m1) * (g.m2 / 2 + 1);
+            k_sc_xconv<<<blocks_for(P, kXCols), 256, 0, s>>>(g, S->rho_hat_f, S->gfold_f, S->tw256, S->tmp_hat_f);
+            SC_CUDA(cudaGetLastError());
+            for (int c = 0; c < 3; ++c) SC_FFT(cufftExecC2R(S->inv2, S->tmp_hat_f + c * upper, S->egrid_f + c * ms));
+        } else {
         SC_CUDA(cudaMemsetAsync(S->rho_hat_f + upper, 0, (cs - upper) * sizeof(cufftComplex), s));
         SC_FFT(cufftExecC2C(S->xpass, S->rho_hat_f, S->rho_hat_f, CUFFT_FORWARD));
         const size_t nf = fold_geom(g).n;
@@ -1123,6 +1298,7 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
         for (int c = 0; c < 3; ++c) {
             SC_FFT(cufftExecC2C(S->xpass, S->tmp_hat_f + c * cs, S->tmp_hat_f + c * cs, CUFFT_INVERSE));
             SC_FFT(cufftExecC2R(S->inv2, S->tmp_hat_f + c * cs, S->egrid_f + c * ms));
+        }
         }
         auto gather = S->pp.poly ? k_sc_gather<false, float, true> : k_sc_gather<false, float, false>;
         const int gb = S->pp.poly ? 128 : 256;
