@@ -668,20 +668,20 @@ def run_fticr(args) -> None:
     # transforms): deposit write, forward FFT read+write, 3 x (kernel
     # multiply: 2 reads + 1 write, inverse FFT read+write) of the real (8 B)
     # and half-complex (16 B x (M/2+1)/M) grids.  Single-precision mesh
-    # (4 B; transforms pruned to the mesh planes x < M/2): deposit write of
-    # those planes, 2D (y, z) R2C of them, x pass over the spectrum, the
-    # multiply (spectrum read, folded kernel quadrants read, three spectra
-    # written), three inverse x passes and three 2D C2R of the mesh planes.
-    # Plus per ion position/charge reads, keys and the 8-node x 3-component
-    # gather.
+    # (4 B; transforms pruned to the mesh planes x < M/2, the x pass fused
+    # with the kernel products at M = 256): deposit write of the mesh
+    # planes, their 2D (y, z) R2C, the fused x pass (their spectrum and the
+    # folded kernel quadrants read, three components' mesh planes written)
+    # and the three components' 2D C2R.  Plus per ion position/charge reads,
+    # keys and the 8-node x 3-component gather.
     M = 2 * cell.sc_grid[0]
     esz = 4.0 if solver_fp32 else 8.0
     real_b = esz * M ** 3
     cplx_b = 2 * esz * M * M * (M // 2 + 1)
     if solver_fp32:
         fold_b = 3 * esz * (M // 2 + 1) ** 3
-        grid_bytes = (real_b / 2 + (real_b / 2 + cplx_b / 2) + 2 * cplx_b + (cplx_b + fold_b + 3 * cplx_b)
-                      + 3 * (2 * cplx_b) + 3 * (cplx_b / 2 + real_b / 2))
+        grid_bytes = (real_b / 2 + (real_b / 2 + cplx_b / 2) + (cplx_b / 2 + fold_b + 3 * cplx_b / 2)
+                      + 3 * (cplx_b / 2 + real_b / 2))
     else:
         grid_bytes = real_b + (real_b + cplx_b) + 3 * (3 * cplx_b) + 3 * (cplx_b + real_b)
     ion_bytes = n * (33 + 32 + 24 + 192 + 24)

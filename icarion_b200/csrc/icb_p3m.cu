@@ -373,7 +373,7 @@ __device__ __forceinline__ void dft16(float2 (&v)[16]) {
 // gf: the folded kernels, [c][ky][kz][kx] (k_sc_fold with kx_inner);
 // out: component c's planes x < 128 after the x pass, at c * 128 * P;
 // tw: exp(-2 pi i m / 256), m < 256.
-__global__ void __launch_bounds__(256) k_sc_xconv(MeshGeom g, const float2* __restrict__ in,
+__global__ void __launch_bounds__(256, 3) k_sc_xconv(MeshGeom g, const float2* __restrict__ in,
                                                   const float* __restrict__ gf, const float2* __restrict__ tw,
                                                   float2* __restrict__ out) {
     __shared__ float2 buf[kXCols * kXStride];
@@ -1158,7 +1158,10 @@ int sc_create(const icb_spacecharge_config& c, uint64_t n_ions, bool pp_float, c
                 S.have_xpass = true;
                 SC_FFT(cufftSetStream(S.xpass, s));
             }
-            SC_FFT(cufftPlanMany(&S.inv2, 2, n2d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, g.n0));
+            // the fused x pass leaves the three components' mesh planes
+            // back to back: one inverse over all of them
+            SC_FFT(cufftPlanMany(&S.inv2, 2, n2d, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R,
+                                 S.xfused ? 3 * g.n0 : g.n0));
             S.have_inv2 = true;
             SC_FFT(cufftSetStream(S.inv2, s));
         }
@@ -1288,7 +1291,7 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
             const size_t P = static_cast<size_t>(g.m1) * (g.m2 / 2 + 1);
             k_sc_xconv<<<blocks_for(P, kXCols), 256, 0, s>>>(g, S->rho_hat_f, S->gfold_f, S->tw256, S->tmp_hat_f);
             SC_CUDA(cudaGetLastError());
-            for (int c = 0; c < 3; ++c) SC_FFT(cufftExecC2R(S->inv2, S->tmp_hat_f + c * upper, S->egrid_f + c * ms));
+            SC_FFT(cufftExecC2R(S->inv2, S->tmp_hat_f, S->egrid_f));
         } else {
         SC_CUDA(cudaMemsetAsync(S->rho_hat_f + upper, 0, (cs - upper) * sizeof(cufftComplex), s));
         SC_FFT(cufftExecC2C(S->xpass, S->rho_hat_f, S->rho_hat_f, CUFFT_FORWARD));
