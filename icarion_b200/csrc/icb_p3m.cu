@@ -1345,8 +1345,13 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
 const double* sc_field(const SpaceChargeSolver* S, int axis) { return S->esc[axis]; }
 
 int sc_kernel_count(const SpaceChargeSolver* S) {
-    // kernels of one solve that this library launches (cuFFT and CUB not counted)
-    return S->mode == ICB_SC_P3M_ISOLATED ? 4 + 1 + 1 + 1 : 4 + 1 + 1 + 1 + 1;
+    // kernels of one solve that this library launches (cuFFT, CUB and
+    // memsets not counted): bin, cell starts, permute, deposit, then the
+    // kernel products (or the fused x pass) and the gather, or the
+    // reference's Poisson step, its differences and the gather; with peer
+    // ions also the own-slot flag and scatter
+    const int peers = S->peers.n > 0 ? 2 : 0;
+    return (S->mode == ICB_SC_P3M_ISOLATED ? 4 + 1 + 1 : 4 + 1 + 1 + 1) + peers;
 }
 
 }  // namespace icb
