@@ -158,6 +158,36 @@ __global__ void k_flags_out(const uint8_t* __restrict__ flags, uint8_t* __restri
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i < n) active[i] = (flags[i] & kFlagActive) ? 1 : 0;
 }
+// One ion chunk of the overlapped host path, in one launch each way: the
+// staged double velocities (three arrays `stride` apart) to float when vx is
+// given, and the host activity bytes into the flags (k_to_float x 3 +
+// k_flags_update); and back (k_from_float x 3 + k_flags_out).
+__global__ void k_chunk_in(const double* __restrict__ stage, uint64_t stride, float* __restrict__ vx,
+                           float* __restrict__ vy, float* __restrict__ vz, const uint8_t* __restrict__ active,
+                           uint8_t* __restrict__ flags, uint64_t n) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (vx) {
+        vx[i] = static_cast<float>(stage[i]);
+        vy[i] = static_cast<float>(stage[stride + i]);
+        vz[i] = static_cast<float>(stage[2 * stride + i]);
+    }
+    uint8_t f = flags[i];
+    if ((f & kFlagBorn) != 0) f = active[i] ? static_cast<uint8_t>(f | kFlagActive) : static_cast<uint8_t>(f & ~kFlagActive);
+    flags[i] = f;
+}
+__global__ void k_chunk_out(const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz,
+                            double* __restrict__ stage, uint64_t stride, const uint8_t* __restrict__ flags,
+                            uint8_t* __restrict__ active, uint64_t n) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (vx) {
+        stage[i] = static_cast<double>(vx[i]);
+        stage[stride + i] = static_cast<double>(vy[i]);
+        stage[2 * stride + i] = static_cast<double>(vz[i]);
+    }
+    active[i] = (flags[i] & kFlagActive) ? 1 : 0;
+}
 
 // Moments: one block per work item (a slice of one ensemble's ions), a
 // fixed-order block reduction into partials[item], then one block per
@@ -1931,16 +1961,15 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
         const unsigned g = grid_for(cnt, 256);
         cudaStream_t ks = h->chunk_streams[static_cast<size_t>(c)];
         ICB_CUDA(cudaStreamWaitEvent(ks, h->hev[2 * c], 0));
-        if (!f64)
-            for (int k = 0; k < 3; ++k) k_to_float<<<g, 256, 0, ks>>>(h->hstage.p + k * n + a, vf[k] + a, cnt);
-        k_flags_update<<<g, 256, 0, ks>>>(h->active_stage.p + a, h->flags.p + a, cnt);
+        double* stage = f64 ? nullptr : h->hstage.p + a;
+        k_chunk_in<<<g, 256, 0, ks>>>(stage, n, f64 ? nullptr : vf[0] + a, f64 ? nullptr : vf[1] + a,
+                                      f64 ? nullptr : vf[2] + a, h->active_stage.p + a, h->flags.p + a, cnt);
         ICB_CUDA(cudaGetLastError());
         if (int r = launch_step(h, static_cast<uint32_t>(n_steps), 1, 1, 1, a, b, ks, false)) return r;
-        if (!f64)
-            for (int k = 0; k < 3; ++k) k_from_float<<<g, 256, 0, ks>>>(vf[k] + a, h->hstage.p + k * n + a, cnt);
-        k_flags_out<<<g, 256, 0, ks>>>(h->flags.p + a, h->active_stage.p + a, cnt);
+        k_chunk_out<<<g, 256, 0, ks>>>(f64 ? nullptr : vf[0] + a, f64 ? nullptr : vf[1] + a, f64 ? nullptr : vf[2] + a,
+                                       stage, n, h->flags.p + a, h->active_stage.p + a, cnt);
         ICB_CUDA(cudaGetLastError());
-        h->launches += f64 ? 2 : 8;
+        h->launches += 2;
         ICB_CUDA(cudaEventRecord(h->hev[2 * c + 1], ks));
         ICB_CUDA(cudaStreamWaitEvent(bs, h->hev[2 * c + 1], 0));
         ICB_CUDA(cudaStreamWaitEvent(s, h->hev[2 * c + 1], 0));   // the clock advance follows every chunk
