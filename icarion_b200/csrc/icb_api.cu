@@ -1903,7 +1903,9 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
     if (n_chunks < 1 || n_chunks > 64) return fail(ICB_ERR_INVALID_ARGUMENT, "n_chunks must be in [1, 64]");
     if (n_steps == 0) return fail(ICB_ERR_INVALID_ARGUMENT, "n_steps must be > 0");
     // the overlapped form needs one launch per chunk and independent ions
-    if (n_chunks == 1 || n_steps > h->K || h->sc || h->hilo() || h->cfg.use_graphs) {
+    // (its chunks launch directly, also on a handle that replays
+    // icb_advance through CUDA graphs)
+    if (n_chunks == 1 || n_steps > h->K || h->sc || h->hilo()) {
         if (int r = icb_update_state(h, x, y, z, vx, vy, vz, active)) return r;
         if (int r = icb_advance(h, n_steps, stats)) return r;
         return icb_download_ions(h, x, y, z, vx, vy, vz, active, nullptr, nullptr);

@@ -301,9 +301,10 @@ int icb_advance(struct icb_handle* h, uint64_t n_steps, icb_run_stats* stats);
  * copy-back streams, one compute stream per chunk, events, queued chunk by
  * chunk; host arrays should be pinned for the overlap; 24 chunks measured
  * best for 1M ions on a B200).  The overlapped
- * form needs n_steps <= steps_per_launch, no space charge, no CUDA graphs
- * and the double-position forms; otherwise (and for n_chunks = 1) the three
- * calls run in order.  Results equal the three separate calls bit for bit. */
+ * form needs n_steps <= steps_per_launch, no space charge and the
+ * double-position forms (on a use_graphs handle its chunks launch directly);
+ * otherwise (and for n_chunks = 1) the three calls run in order.  Results
+ * equal the three separate calls bit for bit. */
 int icb_advance_host(struct icb_handle* h, uint64_t n_steps, int n_chunks,
                      double* x, double* y, double* z, double* vx, double* vy, double* vz,
                      uint8_t* active, icb_run_stats* stats);

@@ -420,6 +420,36 @@ def test_advance_host_equals_separate_calls(precision):
     assert outs[0][1][0] == outs[1][1][0] == 1200 and outs[0][2] == outs[1][2]
 
 
+@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_MIXED])
+def test_advance_host_with_graphs_equals_separate_calls(precision):
+    """A handle that replays icb_advance through CUDA graphs runs
+    icb_advance_host as overlapped ion chunks too (plain launches), on two
+    ensembles whose boundary falls inside a chunk; mixed with graph-replayed
+    icb_advance calls it gives the state of the same calls without graphs
+    and of icb_update_state + icb_advance + icb_download_ions, bit for bit."""
+    e = config0_ensemble()
+    st0 = config0_ions(5000)
+    offsets = [0, 2900, 5000]
+    outs = []
+    for graphs, chunks in ((0, 1), (1, 4), (0, 4)):
+        with Simulation([e, e], precision=precision, collision=capi.COLLISION_HSS, rng_seed=3,
+                        steps_per_launch=400, use_graphs=graphs) as sim:
+            sim.upload(st0, ens_offsets=offsets)
+            host = st0.copy()
+            host.t_death = host.t_arrival = None
+            colls = 0
+            for _ in range(2):
+                colls += sim.advance_host(host, 400, n_chunks=chunks)["collisions"]
+            sim.update_state(host)
+            colls += sim.advance(400)["collisions"]
+            host = sim.download(host)
+            outs.append((host, sim.clock(), colls))
+    for o in outs[1:]:
+        for k in KEYS + ("active",):
+            assert np.array_equal(getattr(outs[0][0], k), getattr(o[0], k)), k
+        assert o[1][0] == outs[0][1][0] == 1200 and o[2] == outs[0][2]
+
+
 def test_unfused_plug_points_equal_fused_step():
     """push (step_batch) -> collide (handle_batch) -> finalize, one call each
     per step, gives the fused icb_advance result bit for bit (FP64)."""
