@@ -524,6 +524,8 @@ def run_ours(args) -> None:
     if world > 1:
         dist.barrier()
     # the host fast path overlaps each ion chunk's copies with the others' steps
+    if args.e2e_chunks is None:
+        args.e2e_chunks = 10 if args.workload == "en-sweep" else 24
     sim.advance_host(host, STEPS_PER_BENCH_STEP, n_chunks=args.e2e_chunks)      # warm the copy stream
     sim.upload(st0, ens_offsets=offsets, first_id=first_id)
     for k in pin:
@@ -890,7 +892,10 @@ def main():
     ap.add_argument("--per-step-ions", type=int, default=16 * 1048576,
                     help="ions of the per-step kernel's HBM roofline run (0 = skip)")
     ap.add_argument("--e2e-steps", type=int, default=20)
-    ap.add_argument("--e2e-chunks", type=int, default=24, help="ion chunks of the overlapped host path")
+    ap.add_argument("--e2e-chunks", type=int, default=None,
+                    help="ion chunks of the overlapped host path (default: 24 for ims-1M, whose steps outlast "
+                         "the copies; 10 for en-sweep, whose copies outlast the steps and whose chunks then "
+                         "pay their per-chunk host calls)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.precision is None:

@@ -1974,7 +1974,6 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
         h->launches += 2;
         ICB_CUDA(cudaEventRecord(h->hev[2 * c + 1], ks));
         ICB_CUDA(cudaStreamWaitEvent(bs, h->hev[2 * c + 1], 0));
-        ICB_CUDA(cudaStreamWaitEvent(s, h->hev[2 * c + 1], 0));   // the clock advance follows every chunk
         for (int k = 0; k < 3; ++k) {
             ICB_CUDA(cudaMemcpyAsync(pos[k] + a, pd[k] + a, cnt * sizeof(double), cudaMemcpyDeviceToHost, bs));
             const double* src = f64 ? vd[k] + a : h->hstage.p + k * n + a;
@@ -1982,13 +1981,15 @@ int icb_advance_host(icb_handle* h, uint64_t n_steps, int n_chunks, double* x, d
         }
         ICB_CUDA(cudaMemcpyAsync(active + a, h->active_stage.p + a, cnt, cudaMemcpyDeviceToHost, bs));
     }
+    // the copy-back stream has waited for every chunk's steps: the clock
+    // advance follows them (and the copies) through it
+    ICB_CUDA(cudaEventRecord(h->hev[2 * n_chunks], bs));
+    ICB_CUDA(cudaStreamWaitEvent(s, h->hev[2 * n_chunks], 0));
     const int ne = static_cast<int>(h->ens.size());
     k_clock_advance<<<(ne + 127) / 128, 128, 0, s>>>(h->step_dev.p, h->t_dev.p, h->dt_dev.p, ne,
                                                       static_cast<uint32_t>(n_steps));
     ICB_CUDA(cudaGetLastError());
     ++h->launches;
-    ICB_CUDA(cudaEventRecord(h->hev[2 * n_chunks], bs));
-    ICB_CUDA(cudaStreamWaitEvent(s, h->hev[2 * n_chunks], 0));    // the stream sees the copies done
     ICB_CUDA(cudaEventRecord(h->ev1, s));
     if (stats) return read_stats(h, stats, n_steps, 0);
     ICB_CUDA(cudaStreamSynchronize(s));
