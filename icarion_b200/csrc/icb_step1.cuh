@@ -10,7 +10,8 @@
 // per-ion arrays); the death and arrival times are written only when they
 // happen (an arrival is also recorded in the flag byte, so the per-ion
 // arrival time is never read).  No collision-clock state exists: each step
-// draws Philox(id, step, 0, 0) and a candidate occurs with probability
+// draws one Philox2x32-10 word of (step, id) (step_test_word) and a
+// candidate occurs with probability
 // Q = A (|v - u| + <|th|>) of the current relative speed; the candidate then
 // samples the neutral from the size-biased law and accepts with
 // p / (A (|v - u| + |th|)) exactly as the per-step clock does
@@ -53,6 +54,24 @@ static_assert(kStep1Block == 256, "tile index arithmetic shifts by 8");
 // FP64).  Two keep the copies ahead of the push: four measured the same
 // (0.348 vs 0.342 ms per 16.8M-ion step), and five CTAs per SM with 40
 // registers measured 0.369 ms.
+// The per-step collision test's word: Philox2x32-10 (Salmon et al., SC'11;
+// multiplier 0xD256D193, key bump 0x9E3779B9) of the counter (step, ion id)
+// under the key seed_lo ^ seed_hi (rk[0], rk[1] are the seed's words),
+// first output word.  A candidate then draws its Philox4x32-10 blocks
+// (id, step, 0 | 1) as the clock form's candidates do.  The first round's
+// product depends on the step alone: one value for every ion of a launch.
+__device__ __forceinline__ uint32_t step_test_word(uint32_t step, uint32_t id, const uint32_t* rk) {
+    uint32_t c0 = step, c1 = id, k = rk[0] ^ rk[1];
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi = __umulhi(0xD256D193u, c0), lo = 0xD256D193u * c0;
+        c0 = hi ^ k ^ c1;
+        c1 = lo;
+        k += 0x9E3779B9u;
+    }
+    return c0;
+}
+
 template <int PREC>
 struct Step1Stages {
     static constexpr int kN = 2;
@@ -282,8 +301,6 @@ __global__ void __launch_bounds__(kStep1Block, Step1Shape<PREC>::kMinBlocks) k_s
         const double dt = C.dt;
         const double t0 = p.t_dev[p.ens_base + static_cast<uint32_t>(e)];
         const uint32_t id = static_cast<uint32_t>(p.first_id + i);
-        PhiloxIon pq{};
-        if constexpr (kColl) pq = philox_ion_setup(id, p.rk);
         uint8_t flags = flags0;
         double t = t0;
         // death and arrival times are stored when they happen
@@ -324,8 +341,7 @@ __global__ void __launch_bounds__(kStep1Block, Step1Shape<PREC>::kMinBlocks) k_s
                     const R bb = m_sqrt(wx * wx + wy * wy + wz * wz);
                     R Q = kc.A * bb + kc.Amean;
                     if (Q > R(1)) { Q = R(1); ++n_ovf; }
-                    const U4 r0 = philox_ion(pq, gs, 0u, p.rk);
-                    cand = u32(r0.x, R(0)) < Q;
+                    cand = u32(step_test_word(gs, id, p.rk), R(0)) < Q;
                 }
                 // queue the candidates (warp-aggregated slots)
                 const unsigned ball = __ballot_sync(0xffffffffu, cand);
@@ -634,9 +650,7 @@ __global__ void __launch_bounds__(kStep1WsThreads, Step1WsShape<PREC>::kMinBlock
                 const R bb = m_sqrt(wx * wx + wy * wy + wz * wz);
                 R Q = kc.A * bb + kc.Amean;
                 if (Q > R(1)) { Q = R(1); ++n_ovf; }
-                const PhiloxIon pq = philox_ion_setup(static_cast<uint32_t>(p.first_id + i), p.rk);
-                const U4 r0 = philox_ion(pq, step0, 0u, p.rk);
-                cand = u32(r0.x, R(0)) < Q;
+                cand = u32(step_test_word(step0, static_cast<uint32_t>(p.first_id + i), p.rk), R(0)) < Q;
             }
             // queue the candidates once the collision warp is done with
             // this queue's previous tile

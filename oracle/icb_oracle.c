@@ -189,6 +189,30 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
     philox4x32_10(ctr, key, out);
 }
 
+/* Philox2x32-10 (Salmon, Moraes, Dror, Shaw, SC'11; the Random123 round:
+ * (hi, lo) = 0xD256D193 * c0, c0' = hi ^ key ^ c1, c1' = lo, then
+ * key += 0x9E3779B9) of the counter (c0, c1): both output words. */
+void orc_philox2x32_10(uint32_t c0, uint32_t c1, uint32_t key, uint32_t out2[2]) {
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p = (uint64_t)0xD256D193u * c0;
+        const uint32_t hi = (uint32_t)(p >> 32), lo = (uint32_t)p;
+        c0 = hi ^ key ^ c1;
+        c1 = lo;
+        key += 0x9E3779B9u;
+    }
+    out2[0] = c0;
+    out2[1] = c1;
+}
+
+/* The per-step kernel's collision test word (icb_step1.cuh,
+ * step_test_word): Philox2x32-10 of (step, ion_id) under the key
+ * seed_lo ^ seed_hi, first word. */
+uint32_t orc_step_test_word(uint64_t seed, uint32_t step, uint32_t ion_id) {
+    uint32_t out2[2];
+    orc_philox2x32_10(step, ion_id, (uint32_t)seed ^ (uint32_t)(seed >> 32), out2);
+    return out2[0];
+}
+
 void orc_philox_many(int64_t n, const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
     for (int64_t i = 0; i < n; ++i) philox4x32_10(ctr + 4 * i, key, out + 4 * i);
 }
@@ -1322,16 +1346,15 @@ int orc_run(const orc_domain* d, int integrator, int collision, uint64_t seed,
                         }
                     } else if (collision == 8) {
                         /* the per-step kernel's stateless test: a candidate
-                         * when Philox(id, step, 0).x < Q = A |v - u| + A <|th|>,
-                         * then the per-step clock's candidate with b exact */
+                         * when the Philox2x32-10 word of (step, id) is below
+                         * Q = A |v - u| + A <|th|>, then the per-step clock's
+                         * candidate with b exact */
                         const uint32_t gs = (uint32_t)(step0 + (uint64_t)k);
-                        uint32_t r0[4];
-                        philox_words(seed, id, gs, 0u, r0);
                         const double w[3] = {v[0] - Gi.ug[0], v[1] - Gi.ug[1], v[2] - Gi.ug[2]};
                         const double b = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
                         double Q = Gi.A * b + Gi.Amean;
                         if (Q > 1.0) { Q = 1.0; ++ovf_tot; }
-                        if (u32_to_unit(r0[0]) < Q) {
+                        if (u32_to_unit(orc_step_test_word(seed, gs, id)) < Q) {
                             double clk = 0.0;
                             ++cand_tot;
                             if (nullcoll_candidate(&Gi, v, m, seed, id, gs, 0, &clk, 0.0, b, 0) == 2) ++coll_tot;

@@ -173,6 +173,9 @@ def lib() -> C.CDLL:
         L.orc_mt64_uniforms.argtypes = [C.c_uint64, C.c_int64, DP]
         L.orc_philox4x32_10.argtypes = [U32P, U32P, U32P]
         L.orc_philox_many.argtypes = [C.c_int64, U32P, U32P, U32P]
+        L.orc_philox2x32_10.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, U32P]
+        L.orc_step_test_word.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32]
+        L.orc_step_test_word.restype = C.c_uint32
         L.orc_unit_uniforms.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, DP]
         L.orc_field.argtypes = [C.POINTER(Domain), DP, C.c_double, DP]
         L.orc_clock_init.argtypes = [C.c_uint64, C.c_int64, C.c_uint64, DP, DP, U32P, U32P, C.c_int]
@@ -337,6 +340,18 @@ def mt64_uniforms(seed: int, n: int) -> np.ndarray:
     out = np.zeros(n)
     lib().orc_mt64_uniforms(seed, n, _dp(out))
     return out
+
+
+def philox2x32(c0: int, c1: int, key: int) -> tuple[int, int]:
+    """Philox2x32-10 of the counter (c0, c1) under `key` (both words)."""
+    out = (C.c_uint32 * 2)()
+    lib().orc_philox2x32_10(c0, c1, key, out)
+    return int(out[0]), int(out[1])
+
+
+def step_test_word(seed: int, step: int, ion_id: int) -> int:
+    """The per-step kernel's collision-test word of (step, ion id)."""
+    return int(lib().orc_step_test_word(seed, step, ion_id))
 
 
 def philox(ctr: np.ndarray, seed: int) -> np.ndarray:

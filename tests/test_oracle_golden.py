@@ -143,7 +143,8 @@ def test_plain_per_step_form_tracks_reference_code(golden):
 
 def test_stateless_per_step_test_tracks_reference_code(golden):
     """The per-step kernel's stateless collision test (oracle collision 8:
-    Philox(id, step) against Q = A (|v - u| + <|th|>) every step, then the
+    a Philox2x32-10 word of (step, id) against Q = A (|v - u| + <|th|>)
+    every step, then the
     per-step clock's candidate) against the reference's own Boris + HSS run
     on the same cloud over 20,000 steps: collision fraction within 1 % and
     drift within 4 combined standard errors."""
@@ -164,3 +165,15 @@ def test_stateless_per_step_test_tracks_reference_code(golden):
     f_ref = float(z["collisions"]) / (n * int(z["steps"]))
     f_me = r["collisions"] / (n * steps)
     assert abs(f_me - f_ref) / f_ref < 0.01, (f_me, f_ref)
+
+
+def test_philox2x32_known_answers():
+    """The per-step test's generator, Philox2x32-10, as the oracle restates
+    it: the known-answer vectors published with the Random123 generators
+    (counter, key -> both output words), and the test word's counter
+    (step, id) and key (seed_lo ^ seed_hi)."""
+    assert orc.philox2x32(0, 0, 0) == (0xFF1DAE59, 0x6CD10DF2)
+    assert orc.philox2x32(0xFFFFFFFF, 0xFFFFFFFF, 0xFFFFFFFF) == (0x2C3F628B, 0xAB4FD7AD)
+    assert orc.philox2x32(0x243F6A88, 0x85A308D3, 0x13198A2E) == (0xDD7CE038, 0xF62A4C12)
+    seed = 0x0123456789ABCDEF
+    assert orc.step_test_word(seed, 7, 11) == orc.philox2x32(7, 11, (seed & 0xFFFFFFFF) ^ (seed >> 32))[0]
