@@ -173,7 +173,7 @@ __device__ __forceinline__ W cic_w(int ox, int oy, int oz, W fx, W fy, W fz) {
 // the mesh were zeroed before).  One thread per mesh node.
 template <bool REF_WEIGHTS, class T>
 __global__ void k_sc_deposit(MeshGeom g, const double4* __restrict__ ps, const uint32_t* __restrict__ start,
-                             const uint32_t* __restrict__ keys, T* __restrict__ rho) {
+                             T* __restrict__ rho) {
     const size_t total = static_cast<size_t>(g.n0) * g.n1 * g.n2;
     const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= total) return;
@@ -181,17 +181,6 @@ __global__ void k_sc_deposit(MeshGeom g, const double4* __restrict__ ps, const u
     const size_t t = idx / g.n2;
     const int b = static_cast<int>(t % g.n1);
     const int a = static_cast<int>(t / g.n1);
-    // nodes whose eight cells lie outside the occupied key range [first
-    // sorted key, last key of an ion in the mesh] hold no charge
-    {
-        const uint32_t nv = start[g.ncell];
-        const int64_t lo = (static_cast<int64_t>(a - 1) * g.n1 + (b - 1)) * g.n2 + (c - 1);
-        const int64_t hi = (static_cast<int64_t>(a) * g.n1 + b) * g.n2 + c;
-        if (nv == 0 || hi < static_cast<int64_t>(keys[0]) || lo > static_cast<int64_t>(keys[nv - 1])) {
-            rho[(static_cast<size_t>(a) * g.m1 + static_cast<size_t>(b)) * g.m2 + static_cast<size_t>(c)] = T(0);
-            return;
-        }
-    }
     // cells (ci, cj, ck) with ck = c - 1, c are adjacent keys: one slot range
     // per (ci, cj) column, each ion's ck taken from its position as k_sc_bin
     // took it (the same sums in the same order as cell by cell)
@@ -1295,8 +1284,7 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
     if (iso && S->f32) {
         const size_t cs = S->cplx_size(), ms = S->mesh_planes_size();
         const size_t upper = cs / 2;           // planes x >= n0 of the (y, kz) spectrum
-        k_sc_deposit<false, float><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->keys_sorted,
-                                                                                 S->rho_f);
+        k_sc_deposit<false, float><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho_f);
         SC_CUDA(cudaGetLastError());
         SC_FFT(cufftExecR2C(S->fwd, S->rho_f, S->rho_hat_f));
         if (S->xfused) {
@@ -1323,8 +1311,7 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
         SC_CUDA(cudaGetLastError());
     } else if (iso) {
         SC_CUDA(cudaMemsetAsync(S->rho, 0, S->real_size() * sizeof(double), s));
-        k_sc_deposit<false, double><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->keys_sorted,
-                                                                                  S->rho);
+        k_sc_deposit<false, double><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho);
         SC_CUDA(cudaGetLastError());
         SC_FFT(cufftExecD2Z(S->fwd, S->rho, S->rho_hat));
         k_sc_cmul3<cufftDoubleComplex><<<blocks_for(S->cplx_size(), 256), 256, 0, s>>>(S->rho_hat, S->ghat[0], S->ghat[1], S->ghat[2],
@@ -1336,8 +1323,7 @@ int sc_solve(SpaceChargeSolver* S, const double* x, const double* y, const doubl
             S->egrid[1], S->egrid[2], S->esc[0], S->esc[1], S->esc[2]);
         SC_CUDA(cudaGetLastError());
     } else {
-        k_sc_deposit<true, double><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->keys_sorted,
-                                                                                 S->rho);
+        k_sc_deposit<true, double><<<blocks_for(mesh_nodes, 256), 256, 0, s>>>(g, S->ps, S->start, S->rho);
         SC_CUDA(cudaGetLastError());
         SC_FFT(cufftExecD2Z(S->fwd, S->rho, S->rho_hat));
         k_sc_poisson_ref<<<blocks_for(S->cplx_size(), 256), 256, 0, s>>>(g, S->h[0], S->h[1], S->h[2], S->rho_hat);
